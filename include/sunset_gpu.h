@@ -1,0 +1,144 @@
+/*
+ * sunset_gpu.h -- C-ABI of the B200 LABFM time-step path (libsunset_b200.so).
+ *
+ * Every entry point replaces one Fortran subroutine of the reference (uom-complexfluids/
+ * sunset-viscoelastic, cited as file:line inside source/base) and keeps its meaning: the
+ * reference's arrays are passed as plain pointers in the reference's node order and
+ * layout (1-based neighbour indices, node-major weights), so a thin ISO_C_BINDING module
+ * can forward the reference's module arrays unchanged.  The device keeps its own copies
+ * (Morton-ordered, sliced-ELL links); host pointers are only read or written inside the
+ * call that receives them.
+ *
+ * All functions return 0 on success or a negative SUNSET_ERR_* code; the message is
+ * available from sunset_last_error().  Nothing aborts the host process.  A handle owns
+ * one CUDA stream; calls on one handle must not overlap, distinct handles are
+ * independent.
+ */
+#ifndef SUNSET_GPU_H
+#define SUNSET_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SUNSET_OK 0
+#define SUNSET_ERR_ARG -1          /* bad argument or call order */
+#define SUNSET_ERR_CUDA -2         /* CUDA runtime error */
+#define SUNSET_ERR_SVD -3          /* SVD did not converge in 30 QR sweeps (svdlib.F90:219-222) */
+#define SUNSET_ERR_SCOPE -4        /* configuration outside the implemented path */
+#define SUNSET_ERR_NONFINITE -5    /* NaN/Inf in the time-step error norm */
+#define SUNSET_ERR_NOMEM -6        /* device allocation failed */
+
+/* Conformation formulation (reference Makefile:71-90 ceform -> -Ddi/-Dchl/-Dlc). */
+#define SUNSET_FORM_DI 0
+#define SUNSET_FORM_CHL 1
+#define SUNSET_FORM_LC 2
+#define SUNSET_FORM_NEWT 3
+
+#define SUNSET_FP64 0   /* FP64 throughout: the drop-in */
+#define SUNSET_MIXED 1  /* FP32 fields/weights (hi/lo weights at order >= 8), FP64 solves */
+
+/* Run parameters: the reference's compile-time flags (Makefile) and control.in values
+   (load_data.F90:53-159) in one struct. */
+typedef struct {
+    int form;               /* SUNSET_FORM_* */
+    int fenep;              /* 1: FENE-P, 0: sPTT / Oldroyd-B (epsPTT = 0) */
+    int morder, forder;     /* LABFM order of derivatives and filter (4, 6, 8, 10) */
+    int mcorr;              /* mass correction, reference default on (Makefile:122-125) */
+    int kolmogorov_forcing; /* -1: as the reference (on for chl only, rhs.F90:275) */
+    int di_full_gradients;  /* DI: compute d(cxx)/dy and d(cyy)/dx, which rhs_di.F90:421-423
+                               reads but never computes (1), or take them as zero (0) */
+    int precision;          /* SUNSET_FP64 or SUNSET_MIXED */
+    double L_char, U_char, Re, Wi, beta, epsPTT, fenep_l2, Mdiff, Ma;
+    double grav[3];
+    double h_over_s;        /* >0: h = h_small = h_over_s*s (fixed radius 2h); 0: reference
+                               hovs/hovs_bound (common_parameter.F90:44-66) */
+    int device;             /* CUDA device ordinal */
+} SunsetConfig;
+
+typedef struct SunsetHandle SunsetHandle;
+
+/* flags for the operator calls */
+#define SUNSET_PTR_HOST 0    /* arrays are host memory */
+#define SUNSET_PTR_DEVICE 1  /* arrays are device memory on the handle's device */
+
+int sunset_create(const SunsetConfig *cfg, SunsetHandle **out);
+void sunset_destroy(SunsetHandle *h);
+const char *sunset_last_error(const SunsetHandle *h);
+int sunset_version(void);
+
+/* setup_domain.F90:80-374 build_domain (IPART rows -> nodes, 4 FD rows per boundary node)
+   + mirror_boundaries.F90:34-261 create_mirror_particles, as device-resident ghost points.
+   bcond = {xbcond_L, xbcond_U, ybcond_L, ybcond_U}. */
+int sunset_build_domain(SunsetHandle *h, int nrows, const int *global_index, const double *x,
+                        const double *y, const int *node_type, const double *nx, const double *ny,
+                        const double *s, double xmin, double xmax, double ymin, double ymax,
+                        const int *bcond, double smax);
+/* np (nodes + ghosts), npfb, nb, nplink (max neighbours) */
+int sunset_get_sizes(SunsetHandle *h, int *np, int *npfb, int *nb, int *nplink);
+
+/* neighbours.F90:32-341 find_neighbours: cell-list search + per-row distance sort. */
+int sunset_find_neighbours(SunsetHandle *h);
+/* labf.F90:34-231 calc_labf_weights (+ calc_filter_weights :233-394). */
+int sunset_calc_labf_weights(SunsetHandle *h);
+/* labf.F90:396-451 calc_labf_sums (+ node volumes, labf.F90:453-503). */
+int sunset_calc_labf_sums(SunsetHandle *h);
+/* labf.F90:1723-1811 filter_coefficients. */
+int sunset_filter_coefficients(SunsetHandle *h);
+
+/* ij_count(npfb), ij_count_small(npfb), ij_link(nplink*npfb) 1-based into [1,np] with the
+   reference's ghost numbering (common_vars.F90:87-88). */
+int sunset_get_neighbours(SunsetHandle *h, int *ij_count, int *ij_count_small, int *ij_link);
+/* ij_w_grad(2,nplink,npfb), ij_w_lap(nplink,npfb), ij_w_hyp(nplink,npfb), ij_w_grad_sum(2,npfb),
+   ij_w_lap_sum(npfb), ij_w_hyp_sum(npfb), vol(npfb) (common_vars.F90:91-94). Any may be NULL. */
+int sunset_get_weights(SunsetHandle *h, double *w_grad, double *w_lap, double *w_hyp,
+                       double *w_grad_sum, double *w_lap_sum, double *w_hyp_sum, double *vol);
+
+/* derivatives.F90 operators on a field phi(npfb) in reference order (ghost values follow
+   their parents): calc_gradient :26-71 -> grad(npfb,2) node-major; calc_laplacian :73-116;
+   calc_filtered_var :360-414 (out-of-place); calc_filter_term :466-511. */
+int sunset_calc_gradient(SunsetHandle *h, const double *phi, double *grad, int flags);
+int sunset_calc_laplacian(SunsetHandle *h, const double *phi, double *lap, int flags);
+int sunset_calc_filtered_var(SunsetHandle *h, const double *phi, double *out, int flags);
+int sunset_calc_filter_term(SunsetHandle *h, const double *phi, double *out, int flags);
+
+/* Fields in reference order (npfb each).  setup_flow.F90:24-173 initial_solution: rho, u,
+   v and the conformation tensor c; psi is formed from c as the formulation requires. */
+int sunset_set_state(SunsetHandle *h, const double *ro, const double *u, const double *v,
+                     const double *cxx, const double *cxy, const double *cyy, const double *czz);
+/* 13*npfb: ro rou rov u v psixx psixy psiyy psizz cxx cxy cyy czz */
+int sunset_get_state(SunsetHandle *h, double *out);
+/* rhs_*.F90 calc_all_rhs at the current state: 7*npfb: ro rou rov xx xy yy zz */
+int sunset_calc_all_rhs(SunsetHandle *h, double *out);
+
+/* step.F90:569-622 set_tstep: the CFL and viscous limits at the current state. */
+int sunset_set_tstep(SunsetHandle *h, double *dt_cfl, double *dt_parabolic);
+/* step.F90:218-512 step_rk3_4S_2R_EE, nsteps times.  mode 0: fixed dt; mode 1: set_tstep +
+   set_tstep_PID (step.F90:624-682) before every step.  Steps run as a captured CUDA graph. */
+int sunset_step(SunsetHandle *h, double dt, int nsteps, int mode);
+/* time, dt, itime, emax(3) = {emax_nm1, emax_n, emax_np1} */
+int sunset_get_time(SunsetHandle *h, double *time, double *dt, int *itime, double *emax);
+int sunset_set_time(SunsetHandle *h, double time, double dt, int itime, const double *emax);
+/* sum 0.5 rho |u|^2 vol and sum rho vol over the interior nodes */
+int sunset_kinetic_energy(SunsetHandle *h, double *ke);
+int sunset_mass(SunsetHandle *h, double *mass);
+int sunset_synchronize(SunsetHandle *h);
+
+/* Host-buffer round trip, the drop-in use from a host code that owns the fields: copy the
+   evolved variables in from host arrays (pinned for full speed), run nsteps, copy them
+   back.  7*npfb in reference order: ro rou rov q_xx q_xy q_yy q_zz, q = c (DI) or psi. */
+int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nsteps, double *state_out);
+
+/* sunset_step with the steps bracketed by CUDA events on the handle's stream: *ms is the
+   device time of the nsteps steps. */
+int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
+
+/* Stage-kernel timing: runs `reps` launches of the RK stage kernel (stage 1) on the
+   current state and returns the mean device time per launch in ms. */
+int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
+                             double *bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,2186 @@
+/*
+ * sunset_oracle.c -- CPU restatement (C99 + OpenMP) of SUNSET's LABFM time-step path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the timed CPU baseline.
+ * Parity with the reference is UNPINNED by reference outputs (the reference is Fortran,
+ * cannot be compiled here and ships no golden vectors); see sunset_oracle.h.
+ *
+ * Every routine below restates one reference routine, cited by file:line.  Expressions
+ * keep gfortran's left-to-right evaluation order and the file is compiled with
+ * -ffp-contract=off, so each operation rounds exactly as the reference's does on x86-64
+ * (gfortran -O3 without -march emits no FMA).  Transcendentals call glibc, as the
+ * reference does.  OpenMP is used only where the reference loop is parallel and the
+ * result does not depend on the thread count; reductions are sequential.
+ */
+#include "sunset_oracle.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---------------------------------------------------------------------------------------
+ * Constants: common_parameter.F90:15-101
+ * ------------------------------------------------------------------------------------- */
+static const double pi = 3.141592653589793238462643383279502884197;
+static const double verysmall = 1.0e-30;
+static const double doublesmall = 1.0e-16;
+static const double ss = 2.0; /* common_parameter.F90:68 */
+
+/* RK3(2)4[2R+]C, common_parameter.F90:74-94 */
+#define RK_A21 (11847461282814.0 / 36547543011857.0)
+#define RK_A32 (3943225443063.0 / 7078155732230.0)
+#define RK_A43 (-346793006927.0 / 4029903576067.0)
+#define RK_B1 (1017324711453.0 / 9774461848756.0)
+#define RK_B2 (8237718856693.0 / 13685301971492.0)
+#define RK_B3 (57731312506979.0 / 19404895981398.0)
+#define RK_B4 (-101169746363290.0 / 37734290219643.0)
+#define RK_BH1 (15763415370699.0 / 46270243929542.0)
+#define RK_BH2 (514528521746.0 / 5659431552419.0)
+#define RK_BH3 (27030193851939.0 / 9429696342944.0)
+#define RK_BH4 (-69544964788955.0 / 30262026368149.0)
+
+/* PID, common_parameter.F90:96-101 */
+static const double pid_tol = 1.0e-5;
+#define PID_A (0.49 / 2.0)
+#define PID_B (0.34 / 2.0)
+#define PID_C (0.1 / 2.0)
+static const double pid_k = 0.9;
+
+static double hovs_for(int forder) { /* common_parameter.F90:44-56 */
+    if (forder == 4) return 1.8;
+    if (forder == 6) return 2.4;
+    if (forder == 10) return 3.1;
+    return 2.7;
+}
+static double hovs_bound_for(int forder) {
+    if (forder == 4) return 2.1;
+    return 2.4;
+}
+static int nsize_for(int k) { return (k * k + 3 * k) / 2; } /* labf.F90:56 */
+
+/* ---------------------------------------------------------------------------------------
+ * State (common_vars.F90)
+ * ------------------------------------------------------------------------------------- */
+struct OrSim {
+    OrConfig cfg;
+    char err[512];
+    /* derived parameters, load_data.F90:131-148 */
+    double rho_char, visc_total, visc_solvent, visc_polymeric, lambda, csq;
+    int kolmo;
+    /* nodes */
+    int np, npfb, nb, cap;
+    double *rx, *ry, *h, *hs, *sp, *rnx, *rny;
+    int *type, *fd_parent, *gi, *irel, *vrel;
+    double xmin, xmax, ymin, ymax, smax, smin, h0, h2, h3, sup_size;
+    int bc[4]; /* xbcond_L, xbcond_U, ybcond_L, ybcond_U */
+    int *internal_list, *boundary_list, n_internal;
+    /* neighbours */
+    int nplink;
+    int *ij_count, *ij_count_small, *ij_link; /* link[i*nplink+k], 0-based point index */
+    /* weights */
+    double *w_grad, *w_lap, *w_hyp, *w_grad_sum, *w_lap_sum, *w_hyp_sum, *vol;
+    double *wb_grad2, *wb_grad2_sum; /* boundary second derivatives [jj][k][3] */
+    int have_weights;
+    /* fields (np) */
+    double *ro, *rou, *rov, *row, *u, *v, *w, *p;
+    double *psixx, *psixy, *psiyy, *psizz, *cxx, *cxy, *cyy, *czz;
+    /* rhs (npfb) */
+    double *rhs_ro, *rhs_rou, *rhs_rov, *rhs_row, *rhs_xx, *rhs_xy, *rhs_yy, *rhs_zz;
+    /* time */
+    double time, dt, dt_cfl, dt_parabolic;
+    int itime, iRKstep;
+    double emax_nm1, emax_n, emax_np1;
+    double ero_norm, erou_norm, exx_norm;
+    double driving_force[3];
+};
+
+static int fail(OrSim *s, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(s->err, sizeof(s->err), fmt, ap);
+    va_end(ap);
+    return -1;
+}
+
+const char *or_last_error(OrSim *s) { return s ? s->err : "null handle"; }
+
+void or_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+static void *xcalloc(size_t n, size_t sz) {
+    void *p = calloc(n ? n : 1, sz);
+    if (!p) {
+        fprintf(stderr, "sunset_oracle: out of memory\n");
+        abort();
+    }
+    return p;
+}
+
+OrSim *or_create(const OrConfig *cfg) {
+    OrSim *s = (OrSim *)xcalloc(1, sizeof(OrSim));
+    s->cfg = *cfg;
+    if (s->cfg.L_char == 0.0) s->cfg.L_char = 1.0;
+    if (s->cfg.U_char == 0.0) s->cfg.U_char = 1.0;
+    /* load_data.F90:131-148 */
+    s->rho_char = 1.0;
+    s->visc_total = s->rho_char * s->cfg.U_char * s->cfg.L_char / s->cfg.Re;
+    s->visc_solvent = s->cfg.beta * s->visc_total;
+    s->visc_polymeric = (1.0 - s->cfg.beta) * s->visc_total;
+    s->lambda = s->cfg.Wi * s->cfg.L_char / s->cfg.U_char;
+    {
+        double t = s->cfg.U_char / s->cfg.Ma;
+        s->csq = t * t; /* (u_char/Ma)**two */
+    }
+    s->kolmo = cfg->kolmogorov_forcing < 0 ? (cfg->form == OR_FORM_CHL) : cfg->kolmogorov_forcing;
+    /* setup_flow.F90:147-157 */
+    s->dt = 1.0e-6;
+    s->emax_np1 = pid_tol;
+    s->emax_n = pid_tol;
+    s->emax_nm1 = pid_tol;
+    s->ero_norm = 1.0 / 1.0;
+    s->erou_norm = 1.0 / (1.0 * s->cfg.U_char);
+    s->exx_norm = 1.0 / (1.0);
+    return s;
+}
+
+#define FREE(p) do { free(p); (p) = NULL; } while (0)
+static void free_fields(OrSim *s) {
+    FREE(s->ro); FREE(s->rou); FREE(s->rov); FREE(s->row); FREE(s->u); FREE(s->v); FREE(s->w);
+    FREE(s->p); FREE(s->psixx); FREE(s->psixy); FREE(s->psiyy); FREE(s->psizz);
+    FREE(s->cxx); FREE(s->cxy); FREE(s->cyy); FREE(s->czz);
+    FREE(s->rhs_ro); FREE(s->rhs_rou); FREE(s->rhs_rov); FREE(s->rhs_row);
+    FREE(s->rhs_xx); FREE(s->rhs_xy); FREE(s->rhs_yy); FREE(s->rhs_zz);
+}
+static void free_links(OrSim *s) {
+    FREE(s->ij_count); FREE(s->ij_count_small); FREE(s->ij_link);
+    FREE(s->w_grad); FREE(s->w_lap); FREE(s->w_hyp); FREE(s->w_grad_sum); FREE(s->w_lap_sum);
+    FREE(s->w_hyp_sum); FREE(s->vol); FREE(s->wb_grad2); FREE(s->wb_grad2_sum);
+    s->have_weights = 0;
+}
+void or_destroy(OrSim *s) {
+    if (!s) return;
+    free_fields(s);
+    free_links(s);
+    FREE(s->rx); FREE(s->ry); FREE(s->h); FREE(s->hs); FREE(s->sp); FREE(s->rnx); FREE(s->rny);
+    FREE(s->type); FREE(s->fd_parent); FREE(s->gi); FREE(s->irel); FREE(s->vrel);
+    FREE(s->internal_list); FREE(s->boundary_list);
+    free(s);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * rbfs.F90:48-68 (kernel 1, Wendland C2)
+ * ------------------------------------------------------------------------------------- */
+double or_pow4_libm(double x) { return pow(x, 4.0); } /* qq4**4.0 -> libm pow */
+
+/* x^4 rounded once from the exact double-double product (Dekker two-product on fma).
+   glibc's pow(x,4.0), which the reference calls, is not always correctly rounded (about
+   one argument in 1200 in [0,1] differs by one ulp); this variant is the device path's. */
+double or_pow4_cr(double x) {
+    double a = x * x;
+    double ae = fma(x, x, -a);
+    double b = a * a;
+    double be = fma(a, a, -b);
+    double t = fma(2.0 * a, ae, be);
+    t = fma(ae, ae, t);
+    return b + t;
+}
+
+static int g_pow_cr = 0;
+void or_set_pow_mode(int correctly_rounded) { g_pow_cr = correctly_rounded; }
+
+double or_wab(double qq, double h2) {
+    double qq4 = 1.0 - 0.5 * qq;
+    qq4 = g_pow_cr ? or_pow4_cr(qq4) : pow(qq4, 4.0);
+    double f = 0.0;
+    if (qq <= 2.0 && qq > 0.0) f = ((7.0 / ((4.0 * pi) * h2)) * (2.0 * qq + 1.0)) * qq4;
+    return f;
+}
+static double or_fac(double qq, double h3) {
+    double qq2 = qq * qq, qq3 = qq * qq2, qq4 = qq * qq3;
+    double f = 0.0;
+    if (qq <= 2.0 && qq > 0.0)
+        f = (7.0 / ((4.0 * pi) * h3)) * ((((0.625 * qq4) - (3.75 * qq3)) + (7.5 * qq2)) - (5.0 * qq));
+    return f;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * labf.F90:1815-1920 monomials: x^p y^q/(p!q!), degree-graded, x-power descending.
+ * Each term is (coef*x^p)*y^q with x^k built as x2=x*x, x3=x2*x, ... as written there.
+ * ------------------------------------------------------------------------------------- */
+static const double fact[11] = {1, 1, 2, 6, 24, 120, 720, 5040, 40320, 362880, 3628800};
+
+void or_monomials(int order, double x, double y, double *out) {
+    double xp[11], yp[11];
+    xp[0] = 1.0; yp[0] = 1.0; xp[1] = x; yp[1] = y;
+    for (int k = 2; k <= order; k++) { xp[k] = xp[k - 1] * x; yp[k] = yp[k - 1] * y; }
+    int idx = 0;
+    for (int d = 1; d <= order; d++) {
+        for (int p = d; p >= 0; p--) {
+            int q = d - p;
+            double den = fact[p] * fact[q];
+            double t;
+            if (den == 1.0) {
+                if (p == 0) t = yp[q];
+                else if (q == 0) t = xp[p];
+                else t = xp[p] * yp[q];
+            } else {
+                double c = 1.0 / den;
+                if (q == 0) t = c * xp[p];
+                else if (p == 0) t = c * yp[q];
+                else t = (c * xp[p]) * yp[q];
+            }
+            out[idx++] = t;
+        }
+    }
+}
+
+/* labf.F90:2329-2391: univariate probabilists' Hermite polynomials, as written. */
+static double hermite(int n, double z) {
+    double z2, z3, z4;
+    switch (n) {
+    case 0: return 1.0;
+    case 1: return z;
+    case 2: return z * z - 1.0;
+    case 3: return (z * z) * z - 3.0 * z;
+    case 4: return ((((z * z) * z) * z) - ((6.0 * z) * z)) + 3.0;
+    case 5: z2 = z * z; z3 = z * z2; return ((z2 * z3) - (10.0 * z3)) + (15.0 * z);
+    case 6: z2 = z * z; z3 = z * z2; return (((z3 * z3) - ((15.0 * z2) * z2)) + (45.0 * z2)) - 15.0;
+    case 7:
+        z2 = z * z; z3 = z * z2; z4 = z3 * z;
+        return (((z4 * z3) - ((21.0 * z3) * z2)) + (105.0 * z3)) - (105.0 * z);
+    case 8:
+        z2 = z * z; z4 = z2 * z2;
+        return ((((z4 * z4) - ((28.0 * z4) * z2)) + (210.0 * z4)) - (420.0 * z2)) + 105.0;
+    case 9:
+        z2 = z * z; z3 = z * z2; z4 = z3 * z;
+        return (((((z4 * z3) * z2) - ((36.0 * z4) * z3)) + ((378.0 * z3) * z2)) - (1260.0 * z3)) + (945.0 * z);
+    case 10:
+        z2 = z * z; z4 = z2 * z2;
+        return ((((((z4 * z4) * z2) - ((45.0 * z4) * z4)) + ((630.0 * z4) * z2)) - (3150.0 * z4)) + (4725.0 * z2)) - 945.0;
+    }
+    return 0.0;
+}
+
+/* labf.F90:2025-2121 (ABF==2): He_p(x)He_q(y) in the monomials' ordering. */
+void or_abfs(int order, double x, double y, double *out) {
+    double hx[11], hy[11];
+    for (int k = 0; k <= order; k++) { hx[k] = hermite(k, x); hy[k] = hermite(k, y); }
+    int idx = 0;
+    for (int d = 1; d <= order; d++)
+        for (int p = d; p >= 0; p--) {
+            int q = d - p;
+            if (q == 0) out[idx++] = hx[p];
+            else if (p == 0) out[idx++] = hy[q];
+            else out[idx++] = hx[p] * hy[q];
+        }
+}
+
+/* labf.F90:1041-1077, 1D monomials and ABFs for the tangential boundary operators */
+static void monomials1D(double x, double *out) {
+    double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x, x6 = x5 * x;
+    out[0] = x;
+    out[1] = 0.5 * x2;
+    out[2] = (1.0 / 6.0) * x3;
+    out[3] = (1.0 / 24.0) * x4;
+    out[4] = (1.0 / 120.0) * x5;
+    out[5] = (1.0 / 720.0) * x6;
+}
+static void abfs1D(double x, double ff1, double *out) {
+    for (int k = 0; k < 6; k++) out[k] = hermite(k + 1, x) * ff1;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * svdlib.F90:22-327 -- Golub-Kahan-Reinsch SVD and solve, split into factor + apply.
+ * labf.F90 solves five right-hand sides with five SVDs of identical copies of one
+ * matrix; the factorisation is deterministic, so factoring once and applying it to
+ * each right-hand side gives bit-identical results.
+ * ------------------------------------------------------------------------------------- */
+static double nr_hypot(double a, double b) { /* svdlib.F90:308-327 */
+    double absA = fabs(a), absB = fabs(b), t;
+    if (absA > absB) {
+        t = absB / absA;
+        return absA * sqrt(1.0 + t * t);
+    }
+    if (absB == 0.0) return 0.0;
+    t = absA / absB;
+    return absB * sqrt(1.0 + t * t);
+}
+
+typedef struct {
+    int n;
+    double *u, *v, *w, *rv1, *tmp;
+} SvdWork;
+
+static void svdw_init(SvdWork *sw, int nmax) {
+    sw->n = nmax;
+    sw->u = (double *)xcalloc((size_t)nmax * nmax, sizeof(double));
+    sw->v = (double *)xcalloc((size_t)nmax * nmax, sizeof(double));
+    sw->w = (double *)xcalloc(nmax + 2, sizeof(double));
+    sw->rv1 = (double *)xcalloc(nmax + 2, sizeof(double));
+    sw->tmp = (double *)xcalloc(nmax + 2, sizeof(double));
+}
+static void svdw_free(SvdWork *sw) { free(sw->u); free(sw->v); free(sw->w); free(sw->rv1); free(sw->tmp); }
+
+#define UM(i, j) umat[((j) - 1) * n + ((i) - 1)]
+#define VM(i, j) vmat[((j) - 1) * n + ((i) - 1)]
+
+/* svdlib.F90:37-278. Returns 0, or -1 if the QR iteration does not converge in 30 steps
+   (where the reference stops). */
+static int svd_factor(const double *amat, int n, SvdWork *sw) {
+    double *umat = sw->u, *vmat = sw->v, *W = sw->w - 1, *rv1 = sw->rv1 - 1; /* 1-based */
+    double anorm, c, f, g, h, s, scale, x, y, z;
+    int i, its, j, jj, k, l = 1, nm;
+    memcpy(umat, amat, sizeof(double) * n * n);
+    g = 0.0; scale = 0.0; anorm = 0.0;
+    for (i = 1; i <= n; i++) {
+        l = i + 1;
+        rv1[i] = scale * g;
+        g = 0.0; s = 0.0; scale = 0.0;
+        for (k = i; k <= n; k++) scale = scale + fabs(UM(k, i));
+        if (scale != 0.0) {
+            for (k = i; k <= n; k++) {
+                UM(k, i) = UM(k, i) / scale;
+                s = s + UM(k, i) * UM(k, i);
+            }
+            f = UM(i, i);
+            g = -copysign(sqrt(s), f);
+            h = f * g - s;
+            UM(i, i) = f - g;
+            for (j = l; j <= n; j++) {
+                s = 0.0;
+                for (k = i; k <= n; k++) s = s + UM(k, i) * UM(k, j);
+                f = s / h;
+                for (k = i; k <= n; k++) UM(k, j) = UM(k, j) + f * UM(k, i);
+            }
+            for (k = i; k <= n; k++) UM(k, i) = scale * UM(k, i);
+        }
+        W[i] = scale * g;
+        g = 0.0; s = 0.0; scale = 0.0;
+        for (k = l; k <= n; k++) scale = scale + fabs(UM(i, k));
+        if (scale != 0.0) {
+            for (k = l; k <= n; k++) {
+                UM(i, k) = UM(i, k) / scale;
+                s = s + UM(i, k) * UM(i, k);
+            }
+            f = UM(i, l);
+            g = -copysign(sqrt(s), f);
+            h = f * g - s;
+            UM(i, l) = f - g;
+            for (k = l; k <= n; k++) rv1[k] = UM(i, k) / h;
+            for (j = l; j <= n; j++) {
+                s = 0.0;
+                for (k = l; k <= n; k++) s = s + UM(j, k) * UM(i, k);
+                for (k = l; k <= n; k++) UM(j, k) = UM(j, k) + s * rv1[k];
+            }
+            for (k = l; k <= n; k++) UM(i, k) = scale * UM(i, k);
+        }
+        {
+            double t = fabs(W[i]) + fabs(rv1[i]);
+            anorm = (t > anorm) ? t : anorm;
+        }
+    }
+    /* Accumulation of right-hand transformations, svdlib.F90:115-141 */
+    for (i = n; i >= 1; i--) {
+        if (i < n) {
+            if (g != 0.0) {
+                for (j = l; j <= n; j++) VM(j, i) = (UM(i, j) / UM(i, l)) / g;
+                for (j = l; j <= n; j++) {
+                    s = 0.0;
+                    for (k = l; k <= n; k++) s = s + UM(i, k) * VM(k, j);
+                    for (k = l; k <= n; k++) VM(k, j) = VM(k, j) + s * VM(k, i);
+                }
+            }
+            for (j = l; j <= n; j++) { VM(i, j) = 0.0; VM(j, i) = 0.0; }
+        }
+        VM(i, i) = 1.0;
+        g = rv1[i];
+        l = i;
+    }
+    /* Accumulation of left-hand transformations, svdlib.F90:143-171 */
+    for (i = n; i >= 1; i--) {
+        l = i + 1;
+        g = W[i];
+        for (j = l; j <= n; j++) UM(i, j) = 0.0;
+        if (g != 0.0) {
+            g = 1.0 / g;
+            for (j = l; j <= n; j++) {
+                s = 0.0;
+                for (k = l; k <= n; k++) s = s + UM(k, i) * UM(k, j);
+                f = (s / UM(i, i)) * g;
+                for (k = i; k <= n; k++) UM(k, j) = UM(k, j) + f * UM(k, i);
+            }
+            for (j = i; j <= n; j++) UM(j, i) = UM(j, i) * g;
+        } else {
+            for (j = i; j <= n; j++) UM(j, i) = 0.0;
+        }
+        UM(i, i) = UM(i, i) + 1.0;
+    }
+    /* Diagonalisation of the bidiagonal form, svdlib.F90:173-278 */
+    nm = 1;
+    for (k = n; k >= 1; k--) {
+        for (its = 1; its <= 30; its++) {
+            for (l = k; l >= 1; l--) {
+                nm = l - 1;
+                if ((fabs(rv1[l]) + anorm) == anorm) goto L2000;
+                if ((fabs(W[nm]) + anorm) == anorm) goto L1000;
+            }
+        L1000:
+            c = 0.0; s = 1.0;
+            for (i = l; i <= k; i++) {
+                f = s * rv1[i];
+                rv1[i] = c * rv1[i];
+                if ((fabs(f) + anorm) == anorm) goto L2000;
+                g = W[i];
+                h = nr_hypot(f, g);
+                W[i] = h;
+                h = 1.0 / h;
+                c = (g * h);
+                s = -(f * h);
+                for (j = 1; j <= n; j++) {
+                    y = UM(j, nm);
+                    z = UM(j, i);
+                    UM(j, nm) = (y * c) + (z * s);
+                    UM(j, i) = -(y * s) + (z * c);
+                }
+            }
+        L2000:
+            z = W[k];
+            if (l == k) {
+                if (z < 0.0) {
+                    W[k] = -z;
+                    for (j = 1; j <= n; j++) VM(j, k) = -VM(j, k);
+                }
+                break;
+            }
+            if (its == 30) return -1;
+            x = W[l];
+            nm = k - 1;
+            y = W[nm];
+            g = rv1[nm];
+            h = rv1[k];
+            f = ((y - z) * (y + z) + (g - h) * (g + h)) / ((2.0 * h) * y);
+            g = nr_hypot(f, 1.0);
+            f = ((x - z) * (x + z) + h * ((y / (f + copysign(g, f))) - h)) / x;
+            c = 1.0; s = 1.0;
+            for (j = l; j <= nm; j++) {
+                i = j + 1;
+                g = rv1[i];
+                y = W[i];
+                h = s * g;
+                g = c * g;
+                z = nr_hypot(f, h);
+                rv1[j] = z;
+                c = f / z;
+                s = h / z;
+                f = (x * c) + (g * s);
+                g = -(x * s) + (g * c);
+                h = y * s;
+                y = y * c;
+                for (jj = 1; jj <= n; jj++) {
+                    x = VM(jj, j);
+                    z = VM(jj, i);
+                    VM(jj, j) = (x * c) + (z * s);
+                    VM(jj, i) = -(x * s) + (z * c);
+                }
+                z = nr_hypot(f, h);
+                W[j] = z;
+                if (z != 0.0) {
+                    z = 1.0 / z;
+                    c = f * z;
+                    s = h * z;
+                }
+                f = (c * g) + (s * y);
+                x = -(s * g) + (c * y);
+                for (jj = 1; jj <= n; jj++) {
+                    y = UM(jj, j);
+                    z = UM(jj, i);
+                    UM(jj, j) = (y * c) + (z * s);
+                    UM(jj, i) = -(y * s) + (z * c);
+                }
+            }
+            rv1[l] = 0.0;
+            rv1[k] = f;
+            W[k] = x;
+        }
+    }
+    return 0;
+}
+
+/* svdlib.F90:279-303: x = V diag(1/w) U^T b, skipping exactly-zero singular values. */
+static void svd_apply(const SvdWork *sw, int n, double *bvec) {
+    const double *umat = sw->u, *vmat = sw->v, *W = sw->w - 1;
+    double *tmp = sw->tmp - 1, *b = bvec - 1, s;
+    for (int j = 1; j <= n; j++) {
+        s = 0.0;
+        if (W[j] != 0.0) {
+            for (int i = 1; i <= n; i++) s = s + UM(i, j) * b[i];
+            s = s / W[j];
+        }
+        tmp[j] = s;
+    }
+    for (int j = 1; j <= n; j++) {
+        s = 0.0;
+        for (int jj = 1; jj <= n; jj++) s = s + VM(j, jj) * tmp[jj];
+        b[j] = s;
+    }
+}
+#undef UM
+#undef VM
+
+void or_svd_solve(double *amat, int n, double *bvec) {
+    SvdWork sw;
+    svdw_init(&sw, n);
+    if (svd_factor(amat, n, &sw) == 0) svd_apply(&sw, n, bvec);
+    else for (int i = 0; i < n; i++) bvec[i] = NAN;
+    svdw_free(&sw);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * setup_domain.F90:80-374 (build_domain, non-MPI) and mirror_boundaries.F90:34-261
+ * ------------------------------------------------------------------------------------- */
+static void grow_nodes(OrSim *s, int cap) {
+#define GROW(p, T) p = (T *)realloc(p, sizeof(T) * (size_t)cap)
+    GROW(s->rx, double); GROW(s->ry, double); GROW(s->h, double); GROW(s->hs, double);
+    GROW(s->sp, double); GROW(s->rnx, double); GROW(s->rny, double);
+    GROW(s->type, int); GROW(s->fd_parent, int); GROW(s->gi, int); GROW(s->irel, int); GROW(s->vrel, int);
+#undef GROW
+    s->cap = cap;
+}
+
+static int add_point(OrSim *s) {
+    if (s->np >= s->cap) grow_nodes(s, s->cap * 2 + 64);
+    return s->np++;
+}
+
+/* create_mirror_particles, mirror_boundaries.F90:34-261 */
+static int create_mirror_particles(OrSim *s) {
+    const double mlayer_buff = 2.0;
+    const int xL = s->bc[0], xU = s->bc[1], yL = s->bc[2], yU = s->bc[3];
+    const double xmin = s->xmin, xmax = s->xmax, ymin = s->ymin, ymax = s->ymax;
+    if ((xL == 1 && xU != 1) || (xU == 1 && xL != 1) || (yL == 1 && yU != 1) || (yU == 1 && yL != 1))
+        return fail(s, "periodic boundary conditions incorrectly specified with bcond");
+    int npfb = s->npfb;
+    s->np = npfb;
+    for (int i = 0; i < npfb; i++) {
+        double xi = s->rx[i], yi = s->ry[i], lim = (ss * s->h[i]) * mlayer_buff;
+        int k;
+#define MIRROR(VREL, XNEW, YNEW)                                                  \
+    do {                                                                          \
+        double xn_ = (XNEW), yn_ = (YNEW);                                        \
+        k = add_point(s);                                                         \
+        s->irel[k] = i; s->vrel[k] = (VREL); s->rx[k] = xn_; s->ry[k] = yn_;      \
+    } while (0)
+        if (xi <= xmin + lim) {
+            if (xL == 1) MIRROR(1, (xi + xmax) - xmin, yi);
+            else if (xL == 2) MIRROR(2, 2.0 * xmin - xi, yi);
+        }
+        if (xi >= xmax - lim) {
+            if (xU == 1) MIRROR(1, (xi - xmax) + xmin, yi);
+            else if (xU == 2) MIRROR(2, 2.0 * xmax - xi, yi);
+        }
+        if (yi <= ymin + lim) {
+            if (yL == 1) MIRROR(1, xi, (yi + ymax) - ymin);
+            else if (yL == 2) MIRROR(3, xi, 2.0 * ymin - yi);
+            else if (yL == 3) MIRROR(4, xi, 2.0 * ymin - yi);
+        }
+        if (yi >= ymax - lim) {
+            if (yU == 1) MIRROR(1, xi, (yi - ymax) + ymin);
+            else if (yU == 2) MIRROR(3, xi, 2.0 * ymax - yi);
+            else if (yU == 3) MIRROR(4, xi, 2.0 * ymax - yi);
+        }
+        /* corners: cdist = sqrt(dot_product(rcorn-rp,rcorn-rp)) with z=0 */
+        const double cx[4] = {xmin, xmax, xmin, xmax}, cy[4] = {ymin, ymin, ymax, ymax};
+        const int bx[4] = {xL, xU, xL, xU}, by[4] = {yL, yL, yU, yU};
+        for (int c = 0; c < 4; c++) {
+            double dx = cx[c] - xi, dy = cy[c] - yi, dz = 0.0 - 0.0;
+            double cdist = sqrt((dx * dx + dy * dy) + dz * dz);
+            if (cdist <= lim && bx[c] != 0 && by[c] != 0) {
+                int right = (c == 1 || c == 3), top = (c == 2 || c == 3);
+                double xp = right ? (xi - xmax) + xmin : (xi + xmax) - xmin;
+                double yp = top ? (yi - ymax) + ymin : (yi + ymax) - ymin;
+                double xs = right ? 2.0 * xmax - xi : 2.0 * xmin - xi;
+                double ys = top ? 2.0 * ymax - yi : 2.0 * ymin - yi;
+                if (bx[c] == 1 && by[c] == 1) MIRROR(1, xp, yp);
+                else if (bx[c] == 2 && by[c] == 1) MIRROR(2, xs, yp);
+                else if (bx[c] == 1 && by[c] == 2) MIRROR(3, xp, ys);
+                else if (bx[c] == 2 && by[c] == 2) MIRROR(4, xs, ys);
+                else {
+                    /* the reference increments imp and sets irelation but no position or
+                       vrelation for other combinations (e.g. periodic x + no-slip y) */
+                    return fail(s, "corner mirror for bcond (%d,%d) is undefined in the reference", bx[c], by[c]);
+                }
+            }
+        }
+#undef MIRROR
+    }
+    for (int i = npfb; i < s->np; i++) {
+        int par = s->irel[i];
+        s->type[i] = s->type[par];
+        s->h[i] = s->h[par];
+        s->hs[i] = s->hs[par];
+        s->sp[i] = s->sp[par];
+        s->rnx[i] = s->rnx[par];
+        s->rny[i] = s->rny[par];
+        s->fd_parent[i] = 0;
+        s->gi[i] = s->gi[par];
+    }
+    return 0;
+}
+
+int or_build_domain(OrSim *s, int nrows, const int *gi, const double *x, const double *y,
+                    const int *node_type, const double *nx, const double *ny, const double *sp,
+                    double xmin, double xmax, double ymin, double ymax, const int *bcond,
+                    double smax) {
+    const double hovs = hovs_for(s->cfg.forder), hovs_bound = hovs_bound_for(s->cfg.forder);
+    const double hos = s->cfg.h_over_s;
+    free_fields(s);
+    free_links(s);
+    s->np = 0;
+    s->cap = 0;
+    grow_nodes(s, 5 * nrows + 64);
+    s->xmin = xmin; s->xmax = xmax; s->ymin = ymin; s->ymax = ymax;
+    for (int c = 0; c < 4; c++) s->bc[c] = bcond[c];
+    s->smax = smax;
+    s->h0 = (hos > 0 ? hos : hovs) * smax; /* setup_domain.F90:105 */
+    s->sup_size = ss * s->h0;
+    s->h2 = s->h0 * s->h0;
+    s->h3 = s->h2 * s->h0;
+    int nb = 0;
+    for (int r = 0; r < nrows; r++) { /* setup_domain.F90:177-199 */
+        int ii = add_point(s);
+        s->gi[ii] = gi[r];
+        s->rx[ii] = x[r]; s->ry[ii] = y[r];
+        s->rnx[ii] = nx[r]; s->rny[ii] = ny[r];
+        s->h[ii] = sp[r] * hovs;
+        s->sp[ii] = sp[r];
+        s->type[ii] = node_type[r];
+        s->fd_parent[ii] = -1;
+        s->irel[ii] = ii;
+        s->vrel[ii] = 1;
+        if (node_type[r] >= 0 && node_type[r] <= 2) {
+            s->h[ii] = s->sp[ii] * hovs_bound;
+            int k = ii;
+            nb++;
+            for (int j = 1; j <= 4; j++) {
+                ii = add_point(s);
+                s->gi[ii] = s->gi[k] + j;
+                s->rx[ii] = s->rx[k] + (s->rnx[k] * (double)j) * s->sp[k];
+                s->ry[ii] = s->ry[k] + (s->rny[k] * (double)j) * s->sp[k];
+                s->rnx[ii] = s->rnx[k]; s->rny[ii] = s->rny[k];
+                s->h[ii] = s->h[k]; s->sp[ii] = s->sp[k];
+                s->type[ii] = -j;
+                s->fd_parent[ii] = k;
+                s->irel[ii] = ii;
+                s->vrel[ii] = 1;
+            }
+        }
+    }
+    s->npfb = s->np;
+    s->nb = nb;
+    for (int i = 0; i < s->npfb; i++) {
+        if (hos > 0) s->h[i] = hos * s->sp[i];
+        s->hs[i] = s->h[i]; /* h_small = h, setup_domain.F90:202 */
+    }
+    if (create_mirror_particles(s)) return -1;
+    /* internal / boundary lists, setup_domain.F90:314-327 */
+    FREE(s->internal_list); FREE(s->boundary_list);
+    s->internal_list = (int *)xcalloc(s->npfb, sizeof(int));
+    s->boundary_list = (int *)xcalloc(s->nb ? s->nb : 1, sizeof(int));
+    int ii = 0, jj = 0;
+    for (int i = 0; i < s->npfb; i++) {
+        int t = s->type[i];
+        if (t < 0 || t == 999 || t == 998) s->internal_list[ii++] = i;
+        else s->boundary_list[jj++] = i;
+    }
+    s->n_internal = ii;
+    if (jj != s->nb) return fail(s, "boundary count mismatch (%d vs %d)", jj, s->nb);
+    s->smin = 1e300;
+    for (int i = 0; i < s->npfb; i++) if (s->sp[i] < s->smin) s->smin = s->sp[i];
+    return 0;
+}
+
+int or_sizes(OrSim *s, int *np, int *npfb, int *nb, int *nplink) {
+    if (np) *np = s->np;
+    if (npfb) *npfb = s->npfb;
+    if (nb) *nb = s->nb;
+    if (nplink) *nplink = s->nplink;
+    return 0;
+}
+
+int or_get_nodes(OrSim *s, double *x, double *y, double *h, double *h_small, double *sp,
+                 int *node_type, int *irelation, int *vrelation) {
+    for (int i = 0; i < s->np; i++) {
+        if (x) x[i] = s->rx[i];
+        if (y) y[i] = s->ry[i];
+        if (h) h[i] = s->h[i];
+        if (h_small) h_small[i] = s->hs[i];
+        if (sp) sp[i] = s->sp[i];
+        if (node_type) node_type[i] = s->type[i];
+        if (irelation) irelation[i] = s->irel[i] + 1;
+        if (vrelation) vrelation[i] = s->vrel[i];
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * neighbours.F90:32-341
+ * ------------------------------------------------------------------------------------- */
+static void quicksort_neighbours(int *link, double *a, int first, int last) { /* :316-341 (1-based) */
+    double x = a[(first + last) / 2], t;
+    int i = first, j = last, it;
+    for (;;) {
+        while (a[i] < x) i++;
+        while (x < a[j]) j--;
+        if (i >= j) break;
+        t = a[i]; a[i] = a[j]; a[j] = t;
+        it = link[i]; link[i] = link[j]; link[j] = it;
+        i++;
+        j--;
+    }
+    if (first < i - 1) quicksort_neighbours(link, a, first, i - 1);
+    if (j + 1 < last) quicksort_neighbours(link, a, j + 1, last);
+}
+
+int or_find_neighbours(OrSim *s) {
+    const int np = s->np, npfb = s->npfb;
+    /* cell_generator, :75-93 */
+    double sizeX = s->xmax - s->xmin, sizeY = s->ymax - s->ymin;
+    double unoss = 1.0 / (1.0 * s->sup_size);
+    double xmaxt = s->xmax + sizeX, xmint = s->xmin - sizeX;
+    double ymaxt = s->ymax + sizeY, ymint = s->ymin - sizeY;
+    int ncx = (int)((xmaxt - xmint) * unoss) + 1;
+    int ncy = (int)((ymaxt - ymint) * unoss) + 1;
+    long nct = (long)ncx * ncy;
+    /* neighbour_cells, :95-158: 1-based cell ids, order self,E,NE,SE,W,NW,SW,N,S */
+    /* divide, :160-206 */
+    int *cellpart = (int *)xcalloc(np, sizeof(int));
+    int *nc = (int *)xcalloc(nct + 2, sizeof(int));
+    int *ist = (int *)xcalloc(nct + 2, sizeof(int));
+    int *ip = (int *)xcalloc(np, sizeof(int));
+    for (int k = 0; k < np; k++) {
+        double ddx = s->rx[k] - xmint, ddy = s->ry[k] - ymint;
+        int icell = (int)(ddx * unoss) + 1, jcell = (int)(ddy * unoss) + 1;
+        long ii = icell + (long)(jcell - 1) * ncx;
+        if (icell < 1 || icell > ncx || jcell < 1 || jcell > ncy) {
+            free(cellpart); free(nc); free(ist); free(ip);
+            return fail(s, "node %d outside the cell grid", k);
+        }
+        nc[ii]++;
+        cellpart[k] = (int)ii;
+    }
+    ist[1] = 1;
+    for (long ii = 1; ii <= nct; ii++) { ist[ii + 1] = ist[ii] + nc[ii]; nc[ii] = 0; }
+    for (int k = 0; k < np; k++) { ip[ist[cellpart[k]] + nc[cellpart[k]] - 1] = k; nc[cellpart[k]]++; }
+
+    /* neighboring_list_parallel, :208-243: count, then fill */
+    free_links(s);
+    s->ij_count = (int *)xcalloc(npfb, sizeof(int));
+    s->ij_count_small = (int *)xcalloc(npfb, sizeof(int));
+    int pass, nplink = 0;
+    for (pass = 0; pass < 2; pass++) {
+        if (pass == 1) s->ij_link = (int *)xcalloc((size_t)npfb * nplink, sizeof(int));
+        int maxc = 0;
+#pragma omp parallel for schedule(static) reduction(max : maxc)
+        for (int i = 0; i < npfb; i++) {
+            int ic = cellpart[i];
+            int icx = (ic - 1) % ncx + 1, icy = (ic - 1) / ncx + 1;
+            long cells[9];
+            int ncell = 0;
+            cells[ncell++] = ic;
+            if (icx + 1 <= ncx) {
+                cells[ncell++] = ic + 1;
+                if (icy + 1 <= ncy) cells[ncell++] = ic + ncx + 1;
+                if (icy - 1 >= 1) cells[ncell++] = ic - ncx + 1;
+            }
+            if (icx - 1 >= 1) {
+                cells[ncell++] = ic - 1;
+                if (icy + 1 <= ncy) cells[ncell++] = ic + ncx - 1;
+                if (icy - 1 >= 1) cells[ncell++] = ic - ncx - 1;
+            }
+            if (icy + 1 <= ncy) cells[ncell++] = ic + ncx;
+            if (icy - 1 >= 1) cells[ncell++] = ic - ncx;
+            double hs2 = (s->h[i] * ss) * (s->h[i] * ss);
+            int cnt = 0;
+            for (int kc = 0; kc < ncell; kc++) {
+                long jc = cells[kc];
+                for (int jj = ist[jc]; jj < ist[jc + 1]; jj++) {
+                    int j = ip[jj - 1];
+                    double rx = s->rx[i] - s->rx[j], ry = s->ry[i] - s->ry[j], rz = 0.0 - 0.0;
+                    double rr2 = (rx * rx + ry * ry) + rz * rz;
+                    if (rr2 <= hs2) {
+                        if (pass == 1) s->ij_link[(size_t)i * nplink + cnt] = j;
+                        cnt++;
+                    }
+                }
+            }
+            s->ij_count[i] = cnt;
+            if (cnt > maxc) maxc = cnt;
+        }
+        if (pass == 0) nplink = maxc;
+    }
+    s->nplink = nplink;
+    free(cellpart); free(nc); free(ist); free(ip);
+
+    /* order_neighbours, :272-314 */
+#pragma omp parallel
+    {
+        double *rij2 = (double *)xcalloc(nplink + 1, sizeof(double));
+#pragma omp for schedule(static)
+        for (int i = 0; i < npfb; i++) {
+            int *lk = s->ij_link + (size_t)i * nplink;
+            int cnt = s->ij_count[i];
+            for (int k = 0; k < cnt; k++) {
+                int j = lk[k];
+                double rx = s->rx[i] - s->rx[j], ry = s->ry[i] - s->ry[j], rz = 0.0 - 0.0;
+                rij2[k + 1] = (rx * rx + ry * ry) + rz * rz;
+            }
+            if (cnt >= 1) quicksort_neighbours(lk - 1, rij2, 1, cnt);
+            int small = 0;
+            double hs2 = (s->hs[i] * ss) * (s->hs[i] * ss);
+            for (int k = 0; k < cnt; k++) {
+                int j = lk[k];
+                double rx = s->rx[i] - s->rx[j], ry = s->ry[i] - s->ry[j], rz = 0.0 - 0.0;
+                double rad2 = (rx * rx + ry * ry) + rz * rz;
+                if (rad2 <= hs2) small++;
+            }
+            s->ij_count_small[i] = small;
+        }
+        free(rij2);
+    }
+    return 0;
+}
+
+int or_get_neighbours(OrSim *s, int *ij_count, int *ij_count_small, int *ij_link) {
+    if (!s->ij_count) return fail(s, "neighbours not built");
+    for (int i = 0; i < s->npfb; i++) {
+        if (ij_count) ij_count[i] = s->ij_count[i];
+        if (ij_count_small) ij_count_small[i] = s->ij_count_small[i];
+        if (ij_link)
+            for (int k = 0; k < s->nplink; k++) {
+                size_t o = (size_t)i * s->nplink + k;
+                ij_link[o] = k < s->ij_count[i] ? s->ij_link[o] + 1 : 0;
+            }
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * labf.F90:34-231 calc_labf_weights, :233-394 calc_filter_weights, :453-503 volumes
+ * ------------------------------------------------------------------------------------- */
+static void alloc_weights(OrSim *s) {
+    size_t nn = (size_t)s->npfb * s->nplink;
+    FREE(s->w_grad); FREE(s->w_lap); FREE(s->w_hyp); FREE(s->vol);
+    s->w_grad = (double *)xcalloc(2 * nn, sizeof(double));
+    s->w_lap = (double *)xcalloc(nn, sizeof(double));
+    s->w_hyp = (double *)xcalloc(nn, sizeof(double));
+    s->vol = (double *)xcalloc(s->npfb, sizeof(double));
+}
+
+/* Assemble A(i1,i2) = sum_k X_i1 G_i2 over links 0..cnt-1 of node i with length hh,
+   labf.F90:88-123 (and :268-303 for the filter). A is column-major n x n. */
+static void assemble_moments(const OrSim *s, int i, int cnt, double hh, int order_large, int n,
+                             double *amat, double *gvec, double *xvec) {
+    memset(amat, 0, sizeof(double) * n * n);
+    const int *lk = s->ij_link + (size_t)i * s->nplink;
+    for (int k = 0; k < cnt; k++) {
+        int j = lk[k];
+        double rijx = s->rx[i] - s->rx[j], rijy = s->ry[i] - s->ry[j];
+        double x = -rijx, y = -rijy;
+        double rad = sqrt(x * x + y * y) / hh, qq = rad;
+        double ff1 = or_wab(qq, s->h2);
+        double xx = x / hh, yy = y / hh;
+        or_abfs(order_large, xx, yy, gvec);
+        int nl = nsize_for(order_large);
+        for (int m = 0; m < nl; m++) gvec[m] = gvec[m] * ff1;
+        or_monomials(order_large, x / hh, y / hh, xvec);
+        for (int i2 = 0; i2 < n; i2++)
+            for (int i1 = 0; i1 < n; i1++) amat[i2 * n + i1] = amat[i2 * n + i1] + xvec[i1] * gvec[i2];
+    }
+}
+
+/* The order drop near walls: keep the first m unknowns (labf.F90:125-148). */
+static void drop_order(double *amat, int n, int m) {
+    for (int i1 = 0; i1 < n; i1++)
+        for (int i2 = m; i2 < n; i2++) amat[i2 * n + i1] = 0.0;
+    for (int i1 = m; i1 < n; i1++) {
+        for (int i2 = 0; i2 < n; i2++) amat[i2 * n + i1] = 0.0;
+        amat[i1 * n + i1] = 1.0;
+    }
+}
+
+static double dotn(const double *a, const double *b, int n) {
+    double s = 0.0;
+    for (int m = 0; m < n; m++) s = s + a[m] * b[m];
+    return s;
+}
+
+/* hyperviscosity right-hand sides, labf.F90:325-351 */
+static void hyp_rhs(int order, double *b, int n) {
+    memset(b, 0, sizeof(double) * n);
+    if (order <= 5) { b[9] = -1.0; b[11] = -2.0; b[13] = -1.0; }
+    else if (order <= 7) { b[20] = 1.0; b[22] = 3.0; b[24] = 3.0; b[26] = 1.0; }
+    else if (order <= 9) { b[35] = -1.0; b[37] = -4.0; b[39] = -6.0; b[41] = -4.0; b[43] = -1.0; }
+    else { b[54] = 1.0; b[56] = 5.0; b[58] = 10.0; b[60] = 10.0; b[62] = 5.0; b[64] = 1.0; }
+}
+
+int or_calc_labf_weights(OrSim *s) {
+    if (!s->ij_count) return fail(s, "neighbours not built");
+    const int forder = s->cfg.forder, morder = s->cfg.morder;
+    const int nlarge = nsize_for(forder), nG = nsize_for(morder), nF = nsize_for(forder);
+    alloc_weights(s);
+    int bad = -1;
+#pragma omp parallel
+    {
+        SvdWork sw;
+        svdw_init(&sw, nlarge);
+        double *amat = (double *)xcalloc((size_t)nlarge * nlarge, sizeof(double));
+        double *gvec = (double *)xcalloc(nlarge, sizeof(double));
+        double *xvec = (double *)xcalloc(nlarge, sizeof(double));
+        double *bx = (double *)xcalloc(nlarge, sizeof(double)), *by = (double *)xcalloc(nlarge, sizeof(double));
+        double *bxx = (double *)xcalloc(nlarge, sizeof(double)), *byy = (double *)xcalloc(nlarge, sizeof(double));
+        double *blap = (double *)xcalloc(nlarge, sizeof(double)), *bh = (double *)xcalloc(nlarge, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (int ii = 0; ii < s->n_internal; ii++) {
+            int i = s->internal_list[ii];
+            const int *lk = s->ij_link + (size_t)i * s->nplink;
+            int t = s->type[i];
+            /* ---- derivative weights, :80-215 ---- */
+            double hh = s->hs[i];
+            assemble_moments(s, i, s->ij_count_small[i], hh, forder, nG, amat, gvec, xvec);
+            if (morder >= 7 && (t == 998 || t < 0)) drop_order(amat, nG, 27);
+            if (morder >= 5 && (t == -1 || t == -2)) drop_order(amat, nG, 14);
+            memset(bx, 0, sizeof(double) * nG); bx[0] = 1.0;
+            memset(by, 0, sizeof(double) * nG); by[1] = 1.0;
+            memset(bxx, 0, sizeof(double) * nG); bxx[2] = 1.0;
+            memset(byy, 0, sizeof(double) * nG); byy[4] = 1.0;
+            if (svd_factor(amat, nG, &sw)) {
+#pragma omp critical
+                bad = i;
+                continue;
+            }
+            svd_apply(&sw, nG, bx);
+            svd_apply(&sw, nG, by);
+            svd_apply(&sw, nG, bxx);
+            svd_apply(&sw, nG, byy);
+            for (int m = 0; m < nG; m++) blap[m] = bxx[m] + byy[m];
+            for (int k = 0; k < s->ij_count[i]; k++) {
+                int j = lk[k];
+                double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+                double rad = sqrt(x * x + y * y) / hh, qq = rad;
+                double ff1 = or_wab(qq, s->h2);
+                double xx = x / hh, yy = y / hh;
+                or_abfs(forder, xx, yy, gvec);
+                for (int m = 0; m < nlarge; m++) gvec[m] = gvec[m] * ff1;
+                size_t o = (size_t)i * s->nplink + k;
+                s->w_grad[2 * o + 0] = dotn(bx, gvec, nG) / hh;
+                s->w_grad[2 * o + 1] = dotn(by, gvec, nG) / hh;
+                s->w_lap[o] = (dotn(blap, gvec, nG) / hh) / hh;
+            }
+            /* ---- filter weights, calc_filter_weights :258-388 ---- */
+            hh = s->h[i];
+            assemble_moments(s, i, s->ij_count[i], hh, forder, nF, amat, gvec, xvec);
+            if (forder >= 7 && (t == 998 || t < 0)) drop_order(amat, nF, 27);
+            hyp_rhs(forder, bh, nF);
+            if (forder >= 7 && (t == 998 || t < 0)) hyp_rhs(6, bh, nF);
+            if (forder >= 5 && t == -1) {
+                drop_order(amat, nF, 14);
+                hyp_rhs(4, bh, nF);
+            }
+            if (svd_factor(amat, nF, &sw)) {
+#pragma omp critical
+                bad = i;
+                continue;
+            }
+            svd_apply(&sw, nF, bh);
+            for (int k = 0; k < s->ij_count[i]; k++) {
+                int j = lk[k];
+                double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+                double rad = sqrt(x * x + y * y) / hh, qq = rad;
+                double ff1 = or_wab(qq, s->h2);
+                double xx = x / hh, yy = y / hh;
+                or_abfs(forder, xx, yy, gvec);
+                for (int m = 0; m < nF; m++) gvec[m] = gvec[m] * ff1;
+                s->w_hyp[(size_t)i * s->nplink + k] = dotn(bh, gvec, nF);
+            }
+            /* ---- node volume, calc_node_volumes :460-486 ---- */
+            double vsum = 0.0;
+            for (int k = 0; k < s->ij_count[i]; k++) {
+                int j = lk[k];
+                double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+                double rad = sqrt(x * x + y * y) / hh;
+                double f1 = ((9.0 / pi) * exp((-9.0 * rad) * rad)) / (hh * hh);
+                vsum = vsum + f1;
+            }
+            s->vol[i] = 1.0 / vsum;
+        }
+        svdw_free(&sw);
+        free(amat); free(gvec); free(xvec); free(bx); free(by); free(bxx); free(byy); free(blap); free(bh);
+    }
+    if (bad >= 0) return fail(s, "SVD not converging at node %d (svdlib.F90:219-222)", bad);
+    for (int jj = 0; jj < s->nb; jj++) { /* :489-493 */
+        int i = s->boundary_list[jj];
+        s->vol[i] = s->sp[i] * s->sp[i];
+    }
+    return 0;
+}
+
+/* labf.F90:505-1039 -- boundary framework (walls / inflow / outflow with FD rows). */
+int or_calc_boundary_weights(OrSim *s) {
+    if (s->nb == 0) return 0;
+    return fail(s, "calc_boundary_weights (labf.F90:505-1039) is not restated yet");
+}
+
+/* labf.F90:396-451 */
+int or_calc_labf_sums(OrSim *s) {
+    const int npfb = s->npfb, nplink = s->nplink;
+    const double L = s->cfg.L_char;
+    FREE(s->w_grad_sum); FREE(s->w_lap_sum); FREE(s->w_hyp_sum);
+    s->w_grad_sum = (double *)xcalloc(2 * (size_t)npfb, sizeof(double));
+    s->w_lap_sum = (double *)xcalloc(npfb, sizeof(double));
+    s->w_hyp_sum = (double *)xcalloc(npfb, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < npfb; i++) {
+        double gx = 0.0, gy = 0.0, lp = 0.0, hy = 0.0;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            size_t o = (size_t)i * nplink + k;
+            hy = hy + s->w_hyp[o];
+            gx = gx + s->w_grad[2 * o];
+            gy = gy + s->w_grad[2 * o + 1];
+            lp = lp + s->w_lap[o];
+        }
+        s->w_grad_sum[2 * i] = gx / L;
+        s->w_grad_sum[2 * i + 1] = gy / L;
+        for (int k = 0; k < nplink; k++) {
+            size_t o = (size_t)i * nplink + k;
+            s->w_grad[2 * o] = s->w_grad[2 * o] / L;
+            s->w_grad[2 * o + 1] = s->w_grad[2 * o + 1] / L;
+        }
+        s->w_lap_sum[i] = (lp / L) / L;
+        for (int k = 0; k < nplink; k++) {
+            size_t o = (size_t)i * nplink + k;
+            s->w_lap[o] = (s->w_lap[o] / L) / L;
+        }
+        s->w_hyp_sum[i] = hy;
+    }
+    return 0;
+}
+
+/* labf.F90:1723-1811 */
+int or_filter_coefficients(OrSim *s) {
+    const int npfb = s->npfb, nplink = s->nplink;
+    double *fc = (double *)xcalloc(npfb, sizeof(double));
+    const double oosqrt2 = 1.0 / sqrt(2.0);
+#pragma omp parallel for schedule(static)
+    for (int ii = 0; ii < s->n_internal; ii++) {
+        int i = s->internal_list[ii];
+        double lscal = (2.0 * s->h[i]) * sqrt(pi / (double)s->ij_count[i]);
+        double tmp = ((2.0 / 3.0) * pi) / lscal;
+        double lsum = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            double x = s->rx[j] - s->rx[i], y = s->ry[j] - s->ry[i];
+            double fji = 1.0 - cos(tmp * x) * cos(tmp * y);
+            lsum = lsum + fji * s->w_hyp[(size_t)i * nplink + k];
+        }
+        fc[i] = (2.0 / 3.0) / lsum;
+        int t = s->type[i];
+        if (t < 0 && s->type[s->fd_parent[i]] == 0) {
+            if (t == -1) fc[i] = (fc[i] * 0.5) * oosqrt2;
+            if (t == -2) fc[i] = fc[i] * 0.5;
+            if (t == -3) fc[i] = fc[i] * oosqrt2;
+            if (t == -4 || t == 998) fc[i] = fc[i] * oosqrt2;
+        }
+    }
+    for (int ii = 0; ii < s->nb; ii++) {
+        int i = s->boundary_list[ii];
+        double lscal = s->sp[i];
+        double tmp = ((2.0 / 3.0) * pi) / lscal;
+        double lsum = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            double x = s->rx[j] - s->rx[i], y = s->ry[j] - s->ry[i];
+            double fji = 1.0 - cos(tmp * sqrt(x * x + y * y));
+            lsum = lsum + fji * s->w_hyp[(size_t)i * nplink + k];
+        }
+        fc[i] = (1.0 / 3.0) / lsum;
+        fc[i] = fc[i] * 0.5;
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < npfb; i++) {
+        double sum = 0.0;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            size_t o = (size_t)i * nplink + k;
+            s->w_hyp[o] = s->w_hyp[o] * fc[i];
+            sum = sum + s->w_hyp[o];
+        }
+        s->w_hyp_sum[i] = sum;
+    }
+    free(fc);
+    s->have_weights = 1;
+    return 0;
+}
+
+int or_setup_all(OrSim *s) { /* sunset.F90:51-60 */
+    if (or_find_neighbours(s)) return -1;
+    if (or_calc_labf_weights(s)) return -1;
+    if (s->nb != 0 && or_calc_boundary_weights(s)) return -1;
+    if (or_calc_labf_sums(s)) return -1;
+    if (or_filter_coefficients(s)) return -1;
+    return 0;
+}
+
+int or_get_weights(OrSim *s, double *w_grad, double *w_lap, double *w_hyp, double *w_grad_sum,
+                   double *w_lap_sum, double *w_hyp_sum, double *vol) {
+    if (!s->have_weights) return fail(s, "weights not built");
+    size_t nn = (size_t)s->npfb * s->nplink;
+    if (w_grad) memcpy(w_grad, s->w_grad, 2 * nn * sizeof(double));
+    if (w_lap) memcpy(w_lap, s->w_lap, nn * sizeof(double));
+    if (w_hyp) memcpy(w_hyp, s->w_hyp, nn * sizeof(double));
+    if (w_grad_sum) memcpy(w_grad_sum, s->w_grad_sum, 2 * (size_t)s->npfb * sizeof(double));
+    if (w_lap_sum) memcpy(w_lap_sum, s->w_lap_sum, (size_t)s->npfb * sizeof(double));
+    if (w_hyp_sum) memcpy(w_hyp_sum, s->w_hyp_sum, (size_t)s->npfb * sizeof(double));
+    if (vol) memcpy(vol, s->vol, (size_t)s->npfb * sizeof(double));
+    return 0;
+}
+
+int or_set_neighbours_weights(OrSim *s, int nplink, const int *ij_count, const int *ij_count_small,
+                              const int *ij_link, const double *w_grad, const double *w_lap,
+                              const double *w_hyp, const double *w_grad_sum, const double *w_lap_sum,
+                              const double *w_hyp_sum, const double *vol) {
+    const int npfb = s->npfb;
+    free_links(s);
+    s->nplink = nplink;
+    size_t nn = (size_t)npfb * nplink;
+    s->ij_count = (int *)xcalloc(npfb, sizeof(int));
+    s->ij_count_small = (int *)xcalloc(npfb, sizeof(int));
+    s->ij_link = (int *)xcalloc(nn, sizeof(int));
+    memcpy(s->ij_count, ij_count, npfb * sizeof(int));
+    memcpy(s->ij_count_small, ij_count_small, npfb * sizeof(int));
+    for (size_t o = 0; o < nn; o++) s->ij_link[o] = ij_link[o] - 1;
+    alloc_weights(s);
+    memcpy(s->w_grad, w_grad, 2 * nn * sizeof(double));
+    memcpy(s->w_lap, w_lap, nn * sizeof(double));
+    memcpy(s->w_hyp, w_hyp, nn * sizeof(double));
+    s->w_grad_sum = (double *)xcalloc(2 * (size_t)npfb, sizeof(double));
+    s->w_lap_sum = (double *)xcalloc(npfb, sizeof(double));
+    s->w_hyp_sum = (double *)xcalloc(npfb, sizeof(double));
+    memcpy(s->w_grad_sum, w_grad_sum, 2 * (size_t)npfb * sizeof(double));
+    memcpy(s->w_lap_sum, w_lap_sum, npfb * sizeof(double));
+    memcpy(s->w_hyp_sum, w_hyp_sum, npfb * sizeof(double));
+    memcpy(s->vol, vol, npfb * sizeof(double));
+    for (int i = 0; i < npfb; i++)
+        for (int k = 0; k < ij_count[i]; k++)
+            if (s->ij_link[(size_t)i * nplink + k] < 0 || s->ij_link[(size_t)i * nplink + k] >= s->np)
+                return fail(s, "link out of range at node %d", i);
+    s->have_weights = 1;
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * derivatives.F90 (2-D)
+ * ------------------------------------------------------------------------------------- */
+/* calc_gradient :26-71; comp = 0 both, 1 = x only, 2 = y only (calc_gradient_only :416-464) */
+static void calc_gradient(const OrSim *s, const double *phi, double *gx, double *gy, int comp) {
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->npfb; i++) {
+        double g1 = 0.0, g2 = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wg = s->w_grad + 2 * (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count_small[i]; k++) {
+            double pj = phi[lk[k]];
+            if (comp != 2) g1 = g1 + pj * wg[2 * k];
+            if (comp != 1) g2 = g2 + pj * wg[2 * k + 1];
+        }
+        if (comp != 2) gx[i] = g1 - phi[i] * s->w_grad_sum[2 * i];
+        if (comp != 1) gy[i] = g2 - phi[i] * s->w_grad_sum[2 * i + 1];
+    }
+}
+/* calc_laplacian :73-116 */
+static void calc_laplacian(const OrSim *s, const double *phi, double *lap) {
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->npfb; i++) {
+        double l = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wl = s->w_lap + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count_small[i]; k++) l = l + phi[lk[k]] * wl[k];
+        lap[i] = l - phi[i] * s->w_lap_sum[i];
+    }
+}
+/* calc_laplacian_transverse_only_on_bound :306-358 */
+static void calc_laplacian_transverse(const OrSim *s, const double *phi, double *lap) {
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (int ii = 0; ii < s->n_internal; ii++) {
+        int i = s->internal_list[ii];
+        double l = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wl = s->w_lap + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count_small[i]; k++) l = l + phi[lk[k]] * wl[k];
+        lap[i] = l - phi[i] * s->w_lap_sum[i];
+    }
+    for (int ii = 0; ii < s->nb; ii++) {
+        int i = s->boundary_list[ii];
+        double l = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count_small[i]; k++)
+            l = l + phi[lk[k]] * s->wb_grad2[((size_t)ii * nplink + k) * 3 + 1];
+        lap[i] = l - phi[i] * s->wb_grad2_sum[3 * ii + 1];
+    }
+}
+/* calc_filtered_var :360-414 (in place on phi(1:npfb)) */
+static void calc_filtered_var(const OrSim *s, double *phi, double *work) {
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->npfb; i++) {
+        double t = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wh = s->w_hyp + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) t = t + phi[lk[k]] * wh[k];
+        work[i] = phi[i] + (t - phi[i] * s->w_hyp_sum[i]);
+    }
+    memcpy(phi, work, sizeof(double) * s->npfb);
+}
+/* calc_filter_term :466-511 */
+static void calc_filter_term(const OrSim *s, const double *phi, double *out) {
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->npfb; i++) {
+        double t = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wh = s->w_hyp + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) t = t + phi[lk[k]] * wh[k];
+        out[i] = t - phi[i] * s->w_hyp_sum[i];
+    }
+}
+
+static double *extend_to_np(const OrSim *s, const double *phi) {
+    double *e = (double *)xcalloc(s->np, sizeof(double));
+    memcpy(e, phi, sizeof(double) * s->npfb);
+    for (int j = s->npfb; j < s->np; j++) e[j] = e[s->irel[j]];
+    return e;
+}
+
+int or_calc_gradient(OrSim *s, const double *phi, double *grad) {
+    if (!s->have_weights) return fail(s, "weights not built");
+    double *e = extend_to_np(s, phi);
+    double *gx = (double *)xcalloc(s->npfb, sizeof(double)), *gy = (double *)xcalloc(s->npfb, sizeof(double));
+    calc_gradient(s, e, gx, gy, 0);
+    for (int i = 0; i < s->npfb; i++) { grad[2 * i] = gx[i]; grad[2 * i + 1] = gy[i]; }
+    free(e); free(gx); free(gy);
+    return 0;
+}
+int or_calc_laplacian(OrSim *s, const double *phi, double *lap) {
+    if (!s->have_weights) return fail(s, "weights not built");
+    double *e = extend_to_np(s, phi);
+    calc_laplacian(s, e, lap);
+    free(e);
+    return 0;
+}
+int or_calc_filtered_var(OrSim *s, const double *phi, double *out) {
+    if (!s->have_weights) return fail(s, "weights not built");
+    double *e = extend_to_np(s, phi);
+    double *w = (double *)xcalloc(s->npfb, sizeof(double));
+    calc_filtered_var(s, e, w);
+    memcpy(out, e, sizeof(double) * s->npfb);
+    free(e); free(w);
+    return 0;
+}
+int or_calc_filter_term(OrSim *s, const double *phi, double *out) {
+    if (!s->have_weights) return fail(s, "weights not built");
+    double *e = extend_to_np(s, phi);
+    calc_filter_term(s, e, out);
+    free(e);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * conf_transforms.F90 (2-D parts)
+ * ------------------------------------------------------------------------------------- */
+/* eigens 2x2, :399-444. R column-major: R[0]=R(1,1), R[1]=R(2,1), R[2]=R(1,2), R[3]=R(2,2) */
+static void eigens2(double a, double b, double d, double *l, double *R) {
+    if (fabs(b) <= doublesmall) {
+        l[0] = a; l[1] = d;
+        R[0] = 1.0; R[1] = 0.0; R[2] = 0.0; R[3] = 1.0;
+    } else {
+        double tr = a + d;
+        double det = a * d - b * b;
+        double temp = (0.25 * tr) * tr - det;
+        if (temp <= doublesmall) temp = 0.0;
+        temp = sqrt(temp);
+        l[0] = 0.5 * tr + temp;
+        l[1] = 0.5 * tr - temp;
+        R[0] = l[0] - d;
+        R[1] = b;
+        temp = sqrt(R[0] * R[0] + R[1] * R[1]);
+        R[0] = R[0] / temp;
+        R[1] = R[1] / temp;
+        R[2] = -R[1];
+        R[3] = R[0];
+    }
+}
+/* 2x2 column-major matmul, gfortran inline order: c(i,j) = a(i,1)b(1,j) + a(i,2)b(2,j) */
+static void mm2(const double *a, const double *b, double *c) {
+    double t[4];
+    t[0] = a[0] * b[0] + a[2] * b[1];
+    t[1] = a[1] * b[0] + a[3] * b[1];
+    t[2] = a[0] * b[2] + a[2] * b[3];
+    t[3] = a[1] * b[2] + a[3] * b[3];
+    memcpy(c, t, sizeof(t));
+}
+static void tr2(const double *a, double *t) { t[0] = a[0]; t[1] = a[2]; t[2] = a[1]; t[3] = a[3]; }
+
+/* log_conf_c_from_psi :133-169 (2-D leaves c_zz untouched) */
+static void log_conf_c_from_psi(double pxx, double pxy, double pyy, double *cxx, double *cxy, double *cyy) {
+    double L[2], R[4], RT[4], Lm[4], C[4];
+    eigens2(pxx, pxy, pyy, L, R);
+    tr2(R, RT);
+    Lm[0] = exp(L[0]); Lm[1] = 0.0; Lm[2] = 0.0; Lm[3] = exp(L[1]);
+    mm2(Lm, RT, C);
+    mm2(R, C, C);
+    *cxx = C[0]; *cxy = C[1]; *cyy = C[3];
+}
+/* log_conf_psi_from_c :177-215 */
+static void log_conf_psi_from_c(double cxx, double cxy, double cyy, double *pxx, double *pxy, double *pyy) {
+    double L[2], R[4], RT[4], Lm[4], P[4];
+    eigens2(cxx, cxy, cyy, L, R);
+    tr2(R, RT);
+    Lm[0] = log(L[0]); Lm[1] = 0.0; Lm[2] = 0.0; Lm[3] = log(L[1]);
+    mm2(Lm, RT, P);
+    mm2(R, P, P);
+    *pxx = P[0]; *pxy = P[1]; *pyy = P[3];
+}
+/* cholesky_c_from_psi :33-74 */
+static void cholesky_c_from_psi(const OrSim *s, double pxx, double pxy, double pyy, double pzz,
+                                double *cxx, double *cxy, double *cyy, double *czz) {
+    if (s->cfg.fenep) {
+        double L2 = s->cfg.fenep_l2;
+        double Jxx = exp(2.0 * pxx), Jxy = exp(pxx) * pxy, Jyy = pxy * pxy + exp(2.0 * pyy);
+        double Jzz = exp(2.0 * pzz);
+        double fq = L2 / ((((L2 - 3.0) + Jxx) + Jyy) + Jzz);
+        *cxx = Jxx * fq; *cxy = Jxy * fq; *cyy = Jyy * fq; *czz = Jzz * fq;
+    } else {
+        double e = exp(pxx);
+        *cxx = e * e;
+        *cxy = exp(pxx) * pxy;
+        *cyy = pxy * pxy + exp(2.0 * pyy);
+        *czz = 1.0;
+    }
+}
+/* cholesky_psi_from_c :82-125 */
+static void cholesky_psi_from_c(const OrSim *s, double cxx, double cxy, double cyy, double czz,
+                                double *pxx, double *pxy, double *pyy, double *pzz) {
+    double xx, xy, yy, zz;
+    if (s->cfg.fenep) {
+        double L2 = s->cfg.fenep_l2;
+        double fr = (L2 - 3.0) / (L2 - ((cxx + cyy) + czz));
+        double Jxx = cxx * fr, Jxy = cxy * fr, Jyy = cyy * fr, Jzz = czz * fr;
+        xx = sqrt(Jxx);
+        xy = Jxy / xx;
+        yy = sqrt(Jyy - xy * xy);
+        zz = sqrt(Jzz);
+    } else {
+        xx = sqrt(cxx);
+        xy = cxy / (xx);
+        yy = (sqrt(cyy - xy * xy));
+        zz = sqrt(czz);
+    }
+    *pxx = log(xx); *pxy = xy; *pyy = log(yy); *pzz = log(zz);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Fields: setup_flow.F90:24-173 initial_solution, step.F90:514-567
+ * ------------------------------------------------------------------------------------- */
+static void alloc_fields(OrSim *s) {
+    free_fields(s);
+    int np = s->np, npfb = s->npfb;
+#define A(p, n) s->p = (double *)xcalloc(n, sizeof(double))
+    A(ro, np); A(rou, np); A(rov, np); A(row, np); A(u, np); A(v, np); A(w, np); A(p, np);
+    A(psixx, np); A(psixy, np); A(psiyy, np); A(psizz, np); A(cxx, np); A(cxy, np); A(cyy, np); A(czz, np);
+    A(rhs_ro, npfb); A(rhs_rou, npfb); A(rhs_rov, npfb); A(rhs_row, npfb);
+    A(rhs_xx, npfb); A(rhs_xy, npfb); A(rhs_yy, npfb); A(rhs_zz, npfb);
+#undef A
+}
+
+/* reapply_mirror_bcs, mirror_boundaries.F90:263-352 (no pgrad) */
+static void reapply_mirror_bcs(OrSim *s) {
+    const int form = s->cfg.form;
+    for (int j = s->npfb; j < s->np; j++) {
+        int i = s->irel[j], vr = s->vrel[j];
+        s->ro[j] = s->ro[i];
+        if (vr == 1) { s->rou[j] = s->rou[i]; s->rov[j] = s->rov[i]; }
+        else if (vr == 2) { s->rou[j] = -s->rou[i]; s->rov[j] = s->rov[i]; }
+        else if (vr == 3) { s->rou[j] = s->rou[i]; s->rov[j] = -s->rov[i]; }
+        else if (vr == 4) { s->rou[j] = -s->rou[i]; s->rov[j] = -s->rov[i]; }
+        if (form == OR_FORM_NEWT) continue;
+        int flip = (vr == 2 || vr == 3);
+        if (form != OR_FORM_DI) {
+            s->psixx[j] = s->psixx[i];
+            s->psixy[j] = flip ? -s->psixy[i] : s->psixy[i];
+            s->psiyy[j] = s->psiyy[i];
+            s->psizz[j] = s->psizz[i];
+        } else {
+            s->cxx[j] = s->cxx[i];
+            s->cxy[j] = flip ? -s->cxy[i] : s->cxy[i];
+            s->cyy[j] = s->cyy[i];
+            s->czz[j] = s->czz[i];
+        }
+    }
+}
+
+static void get_velocity_from_momentum(OrSim *s) { /* step.F90:514-529 */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s->np; i++) {
+        double ooro = 1.0 / s->ro[i];
+        s->u[i] = s->rou[i] * ooro;
+        s->v[i] = s->rov[i] * ooro;
+        s->w[i] = s->row[i] * ooro;
+    }
+}
+
+static void get_c_from_psi(OrSim *s) { /* step.F90:531-567 */
+    if (s->cfg.form == OR_FORM_LC) {
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < s->np; i++)
+            log_conf_c_from_psi(s->psixx[i], s->psixy[i], s->psiyy[i], &s->cxx[i], &s->cxy[i], &s->cyy[i]);
+    } else if (s->cfg.form == OR_FORM_CHL) {
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < s->np; i++)
+            cholesky_c_from_psi(s, s->psixx[i], s->psixy[i], s->psiyy[i], s->psizz[i], &s->cxx[i],
+                                &s->cxy[i], &s->cyy[i], &s->czz[i]);
+    }
+}
+
+static void apply_time_dependent_bounds(OrSim *s) { /* characteristic_boundaries.F90:191-257 (walls) */
+    for (int jj = 0; jj < s->nb; jj++) {
+        int i = s->boundary_list[jj];
+        if (s->type[i] == 0) { s->rou[i] = 0.0; s->rov[i] = 0.0; s->row[i] = 0.0; }
+    }
+}
+
+int or_set_state(OrSim *s, const double *ro, const double *u, const double *v, const double *cxx,
+                 const double *cxy, const double *cyy, const double *czz) {
+    if (s->npfb == 0) return fail(s, "domain not built");
+    alloc_fields(s);
+    const int npfb = s->npfb, np = s->np, form = s->cfg.form;
+    for (int i = 0; i < np; i++) { s->ro[i] = 1.0; s->cxx[i] = 1.0; s->cyy[i] = 1.0; s->czz[i] = 1.0; }
+    for (int i = 0; i < npfb; i++) { /* hardcode_initial_conditions, :180-260 */
+        s->u[i] = u[i]; s->v[i] = v[i]; s->w[i] = 0.0; s->ro[i] = ro[i];
+        s->p[i] = s->ro[i] * s->csq;
+        s->cxx[i] = cxx[i]; s->cxy[i] = cxy[i]; s->cyy[i] = cyy[i]; s->czz[i] = czz ? czz[i] : 1.0;
+        if (form == OR_FORM_LC) {
+            log_conf_psi_from_c(s->cxx[i], s->cxy[i], s->cyy[i], &s->psixx[i], &s->psixy[i], &s->psiyy[i]);
+        } else if (form == OR_FORM_CHL) {
+            cholesky_psi_from_c(s, s->cxx[i], s->cxy[i], s->cyy[i], s->czz[i], &s->psixx[i],
+                                &s->psixy[i], &s->psiyy[i], &s->psizz[i]);
+        }
+    }
+    for (int jj = 0; jj < s->nb; jj++) { /* :266-280 walls */
+        int i = s->boundary_list[jj];
+        if (s->type[i] == 0) { s->u[i] = 0.0; s->v[i] = 0.0; s->w[i] = 0.0; }
+    }
+    for (int i = 0; i < np; i++) { /* setup_flow.F90:68-74 */
+        s->rou[i] = s->ro[i] * s->u[i];
+        s->rov[i] = s->ro[i] * s->v[i];
+        s->row[i] = s->ro[i] * s->w[i];
+    }
+    reapply_mirror_bcs(s);
+    get_c_from_psi(s);
+    for (int i = npfb; i < np; i++) { /* :120-125 */
+        s->u[i] = s->rou[i] / s->ro[i];
+        s->v[i] = s->rov[i] / s->ro[i];
+        s->w[i] = s->row[i] / s->ro[i];
+    }
+    s->time = 0.0; s->itime = 0; s->dt = 1.0e-6;
+    s->emax_np1 = pid_tol; s->emax_n = pid_tol; s->emax_nm1 = pid_tol;
+    s->driving_force[0] = s->driving_force[1] = s->driving_force[2] = 0.0;
+    return 0;
+}
+
+int or_set_raw_state(OrSim *s, const double *ro, const double *rou, const double *rov, const double *q) {
+    if (!s->ro) alloc_fields(s);
+    const int npfb = s->npfb;
+    for (int i = 0; i < npfb; i++) {
+        s->ro[i] = ro[i]; s->rou[i] = rou[i]; s->rov[i] = rov[i]; s->row[i] = 0.0;
+        if (s->cfg.form == OR_FORM_DI) {
+            s->cxx[i] = q[i]; s->cxy[i] = q[npfb + i]; s->cyy[i] = q[2 * npfb + i]; s->czz[i] = q[3 * npfb + i];
+        } else {
+            s->psixx[i] = q[i]; s->psixy[i] = q[npfb + i]; s->psiyy[i] = q[2 * npfb + i]; s->psizz[i] = q[3 * npfb + i];
+            if (s->cfg.form == OR_FORM_LC) s->czz[i] = 1.0;
+        }
+    }
+    reapply_mirror_bcs(s);
+    get_velocity_from_momentum(s);
+    get_c_from_psi(s);
+    return 0;
+}
+
+int or_get_state(OrSim *s, double *out) {
+    const int n = s->npfb;
+    if (!s->ro) return fail(s, "state not set");
+    double *src[13] = {s->ro, s->rou, s->rov, s->u, s->v, s->psixx, s->psixy, s->psiyy, s->psizz,
+                       s->cxx, s->cxy, s->cyy, s->czz};
+    for (int f = 0; f < 13; f++) memcpy(out + (size_t)f * n, src[f], sizeof(double) * n);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * rhs_di.F90 / rhs.F90 / rhs_lc.F90 -- calc_all_rhs, 2-D, walls only among boundaries
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+    double *gro_x, *gro_y, *gu_x, *gu_y, *gv_x, *gv_y, *gp_x, *gp_y;
+    double *lapu, *lapv;
+    double *gcxx_x, *gcxx_y, *gcxy_x, *gcxy_y, *gcyy_x, *gcyy_y; /* DI, LC momentum */
+    double *gpxx_x, *gpxx_y, *gpxy_x, *gpxy_y, *gpyy_x, *gpyy_y, *gpzz_x, *gpzz_y; /* chl, lc */
+    double *fenepf, *gf_x, *gf_y;
+    double *lapcxx, *lapcxy, *lapcyy, *lapczz;
+    double *L; /* nb x 5 */
+} RhsWork;
+
+static double *zarr(int n) { return (double *)xcalloc(n, sizeof(double)); }
+
+static void rhs_work_alloc(const OrSim *s, RhsWork *w) {
+    int n = s->npfb;
+    memset(w, 0, sizeof(*w));
+    w->gro_x = zarr(n); w->gro_y = zarr(n); w->gu_x = zarr(n); w->gu_y = zarr(n);
+    w->gv_x = zarr(n); w->gv_y = zarr(n); w->gp_x = zarr(n); w->gp_y = zarr(n);
+    w->lapu = zarr(n); w->lapv = zarr(n);
+    w->gcxx_x = zarr(n); w->gcxx_y = zarr(n); w->gcxy_x = zarr(n); w->gcxy_y = zarr(n);
+    w->gcyy_x = zarr(n); w->gcyy_y = zarr(n);
+    w->gpxx_x = zarr(n); w->gpxx_y = zarr(n); w->gpxy_x = zarr(n); w->gpxy_y = zarr(n);
+    w->gpyy_x = zarr(n); w->gpyy_y = zarr(n); w->gpzz_x = zarr(n); w->gpzz_y = zarr(n);
+    w->fenepf = zarr(s->np); w->gf_x = zarr(n); w->gf_y = zarr(n);
+    w->lapcxx = zarr(n); w->lapcxy = zarr(n); w->lapcyy = zarr(n); w->lapczz = zarr(n);
+    w->L = zarr(5 * (s->nb ? s->nb : 1));
+}
+static void rhs_work_free(RhsWork *w) {
+    double **p = (double **)w;
+    for (size_t k = 0; k < sizeof(RhsWork) / sizeof(double *); k++) free(p[k]);
+}
+
+/* calc_rhs_ro: rhs_di.F90:119-163 (identical in rhs.F90 and rhs_lc.F90) */
+static void calc_rhs_ro(OrSim *s, RhsWork *W) {
+#pragma omp parallel for schedule(static)
+    for (int jj = 0; jj < s->n_internal; jj++) {
+        int i = s->internal_list[jj];
+        double tmp_scal = (s->u[i] * W->gro_x[i] + s->v[i] * W->gro_y[i]) + s->w[i] * 0.0;
+        double divvel = (W->gu_x[i] + W->gv_y[i]) + 0.0;
+        s->rhs_ro[i] = -s->ro[i] * divvel - tmp_scal;
+    }
+    for (int jj = 0; jj < s->nb; jj++) {
+        int i = s->boundary_list[jj];
+        if (s->type[i] == 0) {
+            double xn = s->rnx[i], yn = s->rny[i];
+            double dutdt = -yn * W->gu_y[i] + xn * W->gv_y[i];
+            s->rhs_ro[i] = -s->ro[i] * dutdt - s->ro[i] * 0.0;
+        } else {
+            s->rhs_ro[i] = ((-s->v[i] * W->gro_y[i] - s->ro[i] * W->gv_y[i]) - s->w[i] * 0.0) - s->ro[i] * 0.0;
+        }
+    }
+}
+
+/* polymeric stress divergence for node i: DI/LC read gradients of c (rhs_di.F90:232-250),
+   chl builds them from gradients of psi (rhs.F90:238-260). */
+static void polymeric_divergence(const OrSim *s, const RhsWork *W, int i, double *fu, double *fv) {
+    const int form = s->cfg.form;
+    if (form == OR_FORM_NEWT) { *fu = 0.0; *fv = 0.0; return; }
+    if (form == OR_FORM_CHL) {
+        double pxx = s->psixx[i], pxy = s->psixy[i], pyy = s->psiyy[i];
+        double gcxx1 = (2.0 * exp(2.0 * pxx)) * W->gpxx_x[i];
+        double gcxy1 = exp(pxx) * W->gpxy_x[i] + (pxy * exp(pxx)) * W->gpxx_x[i];
+        double gcxy2 = exp(pxx) * W->gpxy_y[i] + (pxy * exp(pxx)) * W->gpxx_y[i];
+        double gcyy2 = (2.0 * pxy) * W->gpxy_y[i] + (2.0 * exp(2.0 * pyy)) * W->gpyy_y[i];
+        *fu = (gcxx1 + gcxy2) + 0.0;
+        *fv = (gcxy1 + gcyy2) + 0.0;
+        return;
+    }
+    if (s->cfg.fenep) {
+        double f1 = W->fenepf[i];
+        *fu = (((((W->gcxx_x[i] * f1 + s->cxx[i] * W->gf_x[i]) + W->gcxy_y[i] * f1) + s->cxy[i] * W->gf_y[i]) + 0.0 * f1) + 0.0 * 0.0);
+        *fv = (((((W->gcxy_x[i] * f1 + s->cxy[i] * W->gf_x[i]) + W->gcyy_y[i] * f1) + s->cyy[i] * W->gf_y[i]) + 0.0 * f1) + 0.0 * 0.0);
+        return;
+    }
+    *fu = (W->gcxx_x[i] + W->gcxy_y[i]) + 0.0;
+    *fv = (W->gcxy_x[i] + W->gcyy_y[i]) + 0.0;
+}
+
+/* calc_rhs_rovel: rhs_di.F90:165-382, rhs.F90:165-391, rhs_lc.F90:165-381 */
+static void calc_rhs_rovel(OrSim *s, RhsWork *W) {
+    const double coef_solvent = s->visc_solvent, coef_polymeric = s->visc_polymeric / s->lambda;
+    const double *g = s->cfg.grav, *df = s->driving_force;
+    const double kol = (1.0 + (s->cfg.Mdiff * s->cfg.beta) * s->cfg.Wi);
+    const double kold = (1.0 + s->cfg.Mdiff * s->cfg.Wi);
+#pragma omp parallel for schedule(static)
+    for (int jj = 0; jj < s->n_internal; jj++) {
+        int i = s->internal_list[jj];
+        double u = s->u[i], v = s->v[i], ro = s->ro[i];
+        double tsu = ro * ((u * W->gu_x[i] + v * W->gu_y[i]) + s->w[i] * 0.0) - u * s->rhs_ro[i];
+        double tsv = ro * ((u * W->gv_x[i] + v * W->gv_y[i]) + s->w[i] * 0.0) - v * s->rhs_ro[i];
+        double fvu = coef_solvent * W->lapu[i], fvv = coef_solvent * W->lapv[i];
+        double pu, pv;
+        polymeric_divergence(s, W, i, &pu, &pv);
+        if (s->cfg.form != OR_FORM_NEWT) {
+            fvu = fvu + coef_polymeric * pu;
+            fvv = fvv + coef_polymeric * pv;
+        }
+        double bfu = ro * (g[0] + df[0]), bfv = ro * (g[1] + df[1]);
+        if (s->kolmo) bfu = bfu + (((1.0 / s->cfg.Re) * cos(s->ry[i])) * kol) / kold;
+        s->rhs_rou[i] = ((-tsu - W->gp_x[i]) + bfu) + fvu;
+        s->rhs_rov[i] = ((-tsv - W->gp_y[i]) + bfv) + fvv;
+        s->rhs_row[i] = 0.0;
+    }
+    for (int jj = 0; jj < s->nb; jj++) {
+        int i = s->boundary_list[jj];
+        double ro = s->ro[i], c = sqrt(s->csq), dpdn = W->gp_x[i];
+        double *L = W->L + 5 * jj;
+        if (s->type[i] == 0) {
+            double xn = s->rnx[i], yn = s->rny[i];
+            double un = s->u[i] * xn + s->v[i] * yn;
+            double dundn = xn * W->gu_x[i] + yn * W->gv_x[i];
+            double dutdn = -yn * W->gu_x[i] + xn * W->gv_x[i];
+            L[0] = (0.5 * (un - c)) * (dpdn - (ro * c) * dundn);
+            L[1] = un * (W->gro_x[i] - (W->gp_x[i] / c) / c);
+            L[2] = un * dutdn;
+            L[3] = un * (0.0 * xn + 0.0 * yn);
+            L[4] = (0.5 * (un + c)) * (dpdn + (ro * c) * dundn);
+            s->rhs_rou[i] = 0.0; s->rhs_rov[i] = 0.0; s->rhs_row[i] = 0.0;
+        }
+    }
+}
+
+/* calc_rhs_c, DI: rhs_di.F90:384-599 */
+static void calc_rhs_c_di(OrSim *s, RhsWork *W) {
+    const double lambda = s->lambda, eps = s->cfg.epsPTT, Mdiff = s->cfg.Mdiff, L = s->cfg.L_char;
+#pragma omp parallel for schedule(static)
+    for (int jj = 0; jj < s->n_internal + s->nb; jj++) {
+        int wall = jj >= s->n_internal;
+        int i = wall ? s->boundary_list[jj - s->n_internal] : s->internal_list[jj];
+        if (wall && s->type[i] != 0) {
+            s->rhs_xx[i] = 0.0; s->rhs_xy[i] = 0.0; s->rhs_yy[i] = 0.0; s->rhs_zz[i] = 0.0;
+            continue;
+        }
+        double u = s->u[i], v = s->v[i];
+        double cxx = s->cxx[i], cxy = s->cxy[i], cyy = s->cyy[i], czz = s->czz[i];
+        double adxx = -((u * W->gcxx_x[i] + v * W->gcxx_y[i]) + s->w[i] * 0.0);
+        double adxy = -((u * W->gcxy_x[i] + v * W->gcxy_y[i]) + s->w[i] * 0.0);
+        double adyy = -((u * W->gcyy_x[i] + v * W->gcyy_y[i]) + s->w[i] * 0.0);
+        double adzz = -((u * 0.0 + v * 0.0) + s->w[i] * 0.0);
+        double g11 = W->gu_x[i], g12 = W->gu_y[i], g21 = W->gv_x[i], g22 = W->gv_y[i];
+        if (wall) { /* rotated gradients, rhs_di.F90:497-512 */
+            double xn = s->rnx[i], yn = s->rny[i];
+            double a11 = xn * W->gu_x[i] - yn * W->gu_y[i], a21 = xn * W->gv_x[i] - yn * W->gv_y[i];
+            double a12 = yn * W->gu_x[i] + xn * W->gu_y[i], a22 = yn * W->gv_x[i] + xn * W->gv_y[i];
+            g11 = a11; g21 = a21; g12 = a12; g22 = a22;
+        }
+        double ucxx = ((2.0 * g11) * cxx + (2.0 * g12) * cxy) + (2.0 * 0.0) * 0.0;
+        double ucxy = (((((g11 * cxy + g12 * cyy) + 0.0 * 0.0) + g21 * cxx) + g22 * cxy) + 0.0 * 0.0);
+        double ucyy = ((2.0 * g21) * cxy + (2.0 * g22) * cyy) + (2.0 * 0.0) * 0.0;
+        double uczz = ((2.0 * 0.0) * 0.0 + (2.0 * 0.0) * 0.0) + (2.0 * 0.0) * czz;
+        double sxx, sxy, syy, szz;
+        if (s->cfg.fenep) {
+            double fr = -W->fenepf[i];
+            sxx = (fr * cxx + 1.0) / lambda;
+            sxy = (fr * cxy) / lambda;
+            syy = (fr * cyy + 1.0) / lambda;
+            szz = (fr * czz + 1.0) / lambda;
+        } else {
+            double fr = -(((1.0 - eps * 2.0) + eps * ((cxx + cyy) + czz))) / lambda;
+            sxx = fr * (cxx - 1.0);
+            sxy = fr * cxy;
+            syy = fr * (cyy - 1.0);
+            szz = fr * (czz - 1.0); /* undefined in the reference 2-D path; defined here */
+        }
+        if (!wall) {
+            s->rhs_xx[i] = ((adxx + ucxx) + sxx) + Mdiff * W->lapcxx[i];
+            s->rhs_xy[i] = ((adxy + ucxy) + sxy) + Mdiff * W->lapcxy[i];
+            s->rhs_yy[i] = ((adyy + ucyy) + syy) + Mdiff * W->lapcyy[i];
+            s->rhs_zz[i] = ((adzz + uczz) + szz) + Mdiff * W->lapczz[i];
+        } else {
+            double den = ((72.0 * s->sp[i]) * s->sp[i]) * L * L;
+            double *f[3] = {s->cxx, s->cxy, s->cyy};
+            double *lp[3] = {W->lapcxx, W->lapcxy, W->lapcyy};
+            for (int c = 0; c < 3; c++) {
+                double *q = f[c];
+                lp[c][i] = lp[c][i] + (((((-415.0 * q[i]) + 576.0 * q[i + 1]) - 216.0 * q[i + 2]) + 64.0 * q[i + 3]) - 9.0 * q[i + 4]) / den;
+            }
+            s->rhs_xx[i] = (ucxx + sxx) + Mdiff * W->lapcxx[i];
+            s->rhs_xy[i] = (ucxy + sxy) + Mdiff * W->lapcxy[i];
+            s->rhs_yy[i] = (ucyy + syy) + Mdiff * W->lapcyy[i];
+            /* rhs_zz on walls is left untouched in 2-D (rhs_di.F90:573-580) */
+        }
+    }
+}
+
+/* calc_rhs_cholesky, rhs.F90:393-722 (2-D) */
+static void calc_rhs_cholesky(OrSim *s, RhsWork *W) {
+    const double lambda = s->lambda, eps = s->cfg.epsPTT, Mdiff = s->cfg.Mdiff, L = s->cfg.L_char;
+    for (int jj = 0; jj < s->n_internal + s->nb; jj++) {
+        int wall = jj >= s->n_internal;
+        int i = wall ? s->boundary_list[jj - s->n_internal] : s->internal_list[jj];
+        double u = s->u[i], v = s->v[i];
+        if (wall && s->type[i] == 1) u = 0.0;
+        double adxx = (u * W->gpxx_x[i] + v * W->gpxx_y[i]) + s->w[i] * 0.0;
+        double adxy = (u * W->gpxy_x[i] + v * W->gpxy_y[i]) + s->w[i] * 0.0;
+        double adyy = (u * W->gpyy_x[i] + v * W->gpyy_y[i]) + s->w[i] * 0.0;
+        double adzz = (u * W->gpzz_x[i] + v * W->gpzz_y[i]) + s->w[i] * 0.0;
+        double lxx = exp(s->psixx[i]), lxy = s->psixy[i], lyy = exp(s->psiyy[i]), lzz = exp(s->psizz[i]);
+        double g11 = W->gu_x[i], g12 = W->gu_y[i], g21 = W->gv_x[i], g22 = W->gv_y[i];
+        if (wall && s->type[i] == 0) {
+            double xn = s->rnx[i], yn = s->rny[i];
+            g11 = xn * W->gu_x[i] - yn * W->gu_y[i];
+            g12 = yn * W->gu_x[i] + xn * W->gu_y[i];
+            g21 = xn * W->gv_x[i] - yn * W->gv_y[i];
+            g22 = yn * W->gv_x[i] + xn * W->gv_y[i];
+        }
+        double ucxx = (g11 + (g12 * lxy) / lxx);
+        double ucxy = ((g22 * lxy + ((g12 * lyy) * lyy) / lxx) + g21 * lxx);
+        double ucyy = (g22 - (g12 * lxy) / lxx);
+        double uczz = 0.0;
+        double cxx = s->cxx[i], cxy = s->cxy[i], cyy = s->cyy[i], czz = s->czz[i];
+        if (wall) {
+            double den = ((72.0 * s->sp[i]) * s->sp[i]) * L * L;
+            double *f[4] = {s->cxx, s->cxy, s->cyy, s->czz};
+            double *lp[4] = {W->lapcxx, W->lapcxy, W->lapcyy, W->lapczz};
+            for (int c = 0; c < 4; c++) {
+                double *q = f[c];
+                lp[c][i] = lp[c][i] + (((((-415.0 * q[i]) + 576.0 * q[i + 1]) - 216.0 * q[i + 2]) + 64.0 * q[i + 3]) - 9.0 * q[i + 4]) / den;
+            }
+        }
+        double sxx, sxy, syy, szz = 0.0;
+        if (s->cfg.fenep) {
+            double fr = W->fenepf[i], L2 = s->cfg.fenep_l2;
+            double srctmp = ((((((2.0 * g11) * cxx + (2.0 * g12) * cxy) + (2.0 * g21) * cxy) + (2.0 * g22) * cyy)
+                              - (((fr * cxx + fr * cyy) + fr * czz) - 3.0) / lambda)
+                             + Mdiff * ((W->lapcxx[i] + W->lapcyy[i]) + W->lapczz[i]));
+            double den = ((L2 - cxx) - cyy) - czz;
+            sxx = (-(fr / lambda) * (fr * cxx - 1.0) + (Mdiff * fr) * W->lapcxx[i]) + ((fr * cxx) * srctmp) / den;
+            sxy = (-(fr / lambda) * (fr * cxy) + (Mdiff * fr) * W->lapcxy[i]) + ((fr * cxy) * srctmp) / den;
+            syy = (-(fr / lambda) * (fr * cyy - 1.0) + (Mdiff * fr) * W->lapcyy[i]) + ((fr * cyy) * srctmp) / den;
+            szz = (-(fr / lambda) * (fr * czz - 1.0) + (Mdiff * fr) * W->lapczz[i]) + ((fr * czz) * srctmp) / den;
+        } else {
+            double fr = -(((1.0 - eps * 3.0) + eps * ((cxx + cyy) + czz))) / lambda;
+            sxx = fr * (cxx - 1.0) + Mdiff * W->lapcxx[i];
+            sxy = fr * cxy + Mdiff * W->lapcxy[i];
+            syy = fr * (cyy - 1.0) + Mdiff * W->lapcyy[i];
+        }
+        double csxx = ((0.5 * sxx) / lxx) / lxx;
+        double csxy = sxy / lxx - ((0.5 * sxx) * lxy) / (lxx * lxx);
+        double csyy = (((0.5 * syy) / lyy) / lyy - (sxy * lxy) / ((lxx * lyy) * lyy))
+                      + (((0.5 * sxx) * lxy) * lxy) / ((lyy * lyy) * (lxx * lxx));
+        double cszz = ((0.5 * szz) / lzz) / lzz;
+        s->rhs_xx[i] = (-adxx + ucxx) + csxx;
+        s->rhs_xy[i] = (-adxy + ucxy) + csxy;
+        s->rhs_yy[i] = (-adyy + ucyy) + csyy;
+        if (s->cfg.fenep) s->rhs_zz[i] = (-adzz + uczz) + cszz;
+    }
+}
+
+/* calc_rhs_logconf, rhs_lc.F90:383-750 (2-D) */
+static void calc_rhs_logconf(OrSim *s, RhsWork *W) {
+    const double lambda = s->lambda, eps = s->cfg.epsPTT;
+    const int first = (s->itime == 1 && s->iRKstep == 1); /* :503 */
+#pragma omp parallel for schedule(static)
+    for (int jj = 0; jj < s->n_internal + s->nb; jj++) {
+        int wall = jj >= s->n_internal;
+        int i = wall ? s->boundary_list[jj - s->n_internal] : s->internal_list[jj];
+        double u = s->u[i], v = s->v[i];
+        double adxx = -((u * W->gpxx_x[i] + v * W->gpxx_y[i]) + s->w[i] * 0.0);
+        double adxy = -((u * W->gpxy_x[i] + v * W->gpxy_y[i]) + s->w[i] * 0.0);
+        double adyy = -((u * W->gpyy_x[i] + v * W->gpyy_y[i]) + s->w[i] * 0.0);
+        double Lv[2], R[4], RT[4], G[4], M[4], B[4], Om[4], UC[4], P[4], Ci[4], Rx[4], T[4];
+        eigens2(s->psixx[i], s->psixy[i], s->psiyy[i], Lv, R);
+        Lv[0] = exp(Lv[0]);
+        Lv[1] = exp(Lv[1]);
+        tr2(R, RT);
+        double tr_c = Lv[0] + Lv[1];
+        if (wall && s->type[i] == 0) {
+            double xn = s->rnx[i], yn = s->rny[i];
+            G[0] = xn * W->gu_x[i] - yn * W->gu_y[i];
+            G[2] = yn * W->gu_x[i] + xn * W->gu_y[i];
+            G[1] = xn * W->gv_x[i] - yn * W->gv_y[i];
+            G[3] = yn * W->gv_x[i] + xn * W->gv_y[i];
+        } else {
+            G[0] = W->gu_x[i]; G[2] = W->gu_y[i]; G[1] = W->gv_x[i]; G[3] = W->gv_y[i];
+        }
+        mm2(G, R, T);
+        mm2(RT, T, M);
+        double om = (Lv[1] * M[2] + Lv[0] * M[1]);
+        if (fabs(Lv[1] - Lv[0]) <= verysmall) om = 0.0;
+        else om = om / (Lv[1] - Lv[0]);
+        M[2] = 0.0; M[1] = 0.0;
+        mm2(M, RT, T);
+        mm2(R, T, B);
+        M[0] = 0.0; M[1] = 0.0; M[2] = 0.0; M[3] = 0.0;
+        M[2] = om; M[1] = -om;
+        mm2(M, RT, T);
+        mm2(R, T, Om);
+        if (first) {
+            Om[0] = Om[1] = Om[2] = Om[3] = 0.0;
+            double GT[4];
+            tr2(G, GT);
+            for (int c = 0; c < 4; c++) B[c] = 0.5 * (G[c] + GT[c]);
+        }
+        P[0] = s->psixx[i]; P[2] = s->psixy[i]; P[1] = s->psixy[i]; P[3] = s->psiyy[i];
+        double OP[4], PO[4];
+        mm2(Om, P, OP);
+        mm2(P, Om, PO);
+        for (int c = 0; c < 4; c++) UC[c] = (OP[c] - PO[c]) + 2.0 * B[c];
+        if (s->cfg.fenep) {
+            double fR = W->fenepf[i];
+            double cxx = s->cxx[i], cxy = s->cxy[i], cyy = s->cyy[i];
+            double det = cxx * cyy - cxy * cxy;
+            Ci[0] = cyy / det; Ci[3] = cxx / det; Ci[2] = -cxy / det; Ci[1] = -cxy / det;
+            B[0] = cxx; B[3] = cyy; B[2] = cxy; B[1] = cxy;
+            for (int c = 0; c < 4; c++) B[c] = B[c] * fR;
+            B[0] = B[0] - 1.0; B[3] = B[3] - 1.0;
+            mm2(Ci, B, T);
+            for (int c = 0; c < 4; c++) Rx[c] = (-1.0 / lambda) * T[c];
+        } else {
+            double fR = ((1.0 - 2.0 * eps) + eps * tr_c);
+            Ci[0] = fR / Lv[0] - fR; Ci[1] = 0.0; Ci[2] = 0.0; Ci[3] = fR / Lv[1] - fR;
+            mm2(Ci, RT, T);
+            mm2(R, T, T);
+            for (int c = 0; c < 4; c++) Rx[c] = T[c] / lambda;
+        }
+        if (wall && s->type[i] == 0) {
+            s->rhs_xx[i] = UC[0] + Rx[0];
+            s->rhs_xy[i] = UC[2] + Rx[2];
+            s->rhs_yy[i] = UC[3] + Rx[3];
+        } else {
+            s->rhs_xx[i] = (adxx + UC[0]) + Rx[0];
+            s->rhs_xy[i] = (adxy + UC[2]) + Rx[2];
+            s->rhs_yy[i] = (adyy + UC[3]) + Rx[3];
+        }
+    }
+}
+
+/* specify_characteristics_isothermal_wall (characteristic_boundaries.F90:27-52) and the
+   boundary update of calc_rhs_nscbc (rhs_di.F90:601-665). */
+static void calc_rhs_nscbc(OrSim *s, RhsWork *W) {
+    for (int jj = 0; jj < s->nb; jj++) {
+        int i = s->boundary_list[jj];
+        double *L = W->L + 5 * jj;
+        if (s->type[i] == 0) L[4] = L[0];
+        double c = sqrt(s->csq);
+        double tmp_scal = ((((c * c) * L[1] + L[4]) + L[0]) / c) / c;
+        s->rhs_ro[i] = s->rhs_ro[i] - tmp_scal;
+        s->rhs_rou[i] = (s->rhs_rou[i] - s->u[i] * tmp_scal) - (L[4] - L[0]) / c;
+        s->rhs_rov[i] = (s->rhs_rov[i] - s->v[i] * tmp_scal) - s->ro[i] * L[2];
+        s->rhs_row[i] = (s->rhs_row[i] - s->w[i] * tmp_scal) - s->ro[i] * L[3];
+    }
+}
+
+static int calc_all_rhs(OrSim *s) {
+    const int form = s->cfg.form, npfb = s->npfb;
+    for (int jj = 0; jj < s->nb; jj++)
+        if (s->type[s->boundary_list[jj]] != 0)
+            return fail(s, "inflow/outflow characteristics are outside the restated scope");
+    RhsWork W;
+    rhs_work_alloc(s, &W);
+    memset(s->rhs_ro, 0, sizeof(double) * npfb); memset(s->rhs_rou, 0, sizeof(double) * npfb);
+    memset(s->rhs_rov, 0, sizeof(double) * npfb); memset(s->rhs_row, 0, sizeof(double) * npfb);
+    memset(s->rhs_xx, 0, sizeof(double) * npfb); memset(s->rhs_xy, 0, sizeof(double) * npfb);
+    memset(s->rhs_yy, 0, sizeof(double) * npfb); memset(s->rhs_zz, 0, sizeof(double) * npfb);
+    calc_gradient(s, s->ro, W.gro_x, W.gro_y, 0);
+    calc_gradient(s, s->u, W.gu_x, W.gu_y, 0);
+    calc_gradient(s, s->v, W.gv_x, W.gv_y, 0);
+    for (int i = 0; i < s->np; i++) s->p[i] = s->csq * s->ro[i];
+    for (int i = 0; i < npfb; i++) { W.gp_x[i] = s->csq * W.gro_x[i]; W.gp_y[i] = s->csq * W.gro_y[i]; }
+    calc_rhs_ro(s, &W);
+    /* calc_rhs_rovel derivative calls */
+    calc_laplacian(s, s->u, W.lapu);
+    calc_laplacian(s, s->v, W.lapv);
+    if (form == OR_FORM_DI || form == OR_FORM_LC) {
+        int full = (form == OR_FORM_DI && s->cfg.di_full_gradients);
+        calc_gradient(s, s->cxx, W.gcxx_x, W.gcxx_y, full ? 0 : 1);
+        calc_gradient(s, s->cxy, W.gcxy_x, W.gcxy_y, 0);
+        calc_gradient(s, s->cyy, W.gcyy_x, W.gcyy_y, full ? 0 : 2);
+        if (s->cfg.fenep) {
+            for (int i = 0; i < s->np; i++)
+                W.fenepf[i] = (s->cfg.fenep_l2 - 3.0) / (s->cfg.fenep_l2 - ((s->cxx[i] + s->cyy[i]) + s->czz[i]));
+            calc_gradient(s, W.fenepf, W.gf_x, W.gf_y, 0);
+        }
+    } else if (form == OR_FORM_CHL) {
+        calc_gradient(s, s->psixx, W.gpxx_x, W.gpxx_y, 0);
+        calc_gradient(s, s->psixy, W.gpxy_x, W.gpxy_y, 0);
+        calc_gradient(s, s->psiyy, W.gpyy_x, W.gpyy_y, 0);
+        if (s->cfg.fenep) {
+            calc_gradient(s, s->psizz, W.gpzz_x, W.gpzz_y, 0);
+            for (int i = 0; i < s->np; i++)
+                W.fenepf[i] = (s->cfg.fenep_l2 - 3.0) / (s->cfg.fenep_l2 - ((s->cxx[i] + s->cyy[i]) + s->czz[i]));
+        }
+    }
+    calc_rhs_rovel(s, &W);
+    if (form == OR_FORM_DI) {
+        if (s->cfg.Mdiff != 0.0) {
+            calc_laplacian_transverse(s, s->cxx, W.lapcxx);
+            calc_laplacian_transverse(s, s->cxy, W.lapcxy);
+            calc_laplacian_transverse(s, s->cyy, W.lapcyy);
+            if (s->cfg.fenep) calc_laplacian_transverse(s, s->czz, W.lapczz);
+        }
+        calc_rhs_c_di(s, &W);
+    } else if (form == OR_FORM_CHL) {
+        if (s->cfg.Mdiff != 0.0) {
+            calc_laplacian_transverse(s, s->cxx, W.lapcxx);
+            calc_laplacian_transverse(s, s->cxy, W.lapcxy);
+            calc_laplacian_transverse(s, s->cyy, W.lapcyy);
+            calc_laplacian_transverse(s, s->czz, W.lapczz);
+        }
+        calc_rhs_cholesky(s, &W);
+    } else if (form == OR_FORM_LC) {
+        calc_gradient(s, s->psixx, W.gpxx_x, W.gpxx_y, 0);
+        calc_gradient(s, s->psixy, W.gpxy_x, W.gpxy_y, 0);
+        calc_gradient(s, s->psiyy, W.gpyy_x, W.gpyy_y, 0);
+        calc_rhs_logconf(s, &W);
+    }
+    if (s->nb != 0) calc_rhs_nscbc(s, &W);
+    rhs_work_free(&W);
+    return 0;
+}
+
+int or_calc_all_rhs(OrSim *s, double *rhs) {
+    if (!s->have_weights || !s->ro) return fail(s, "weights or state missing");
+    if (calc_all_rhs(s)) return -1;
+    const int n = s->npfb;
+    double *src[7] = {s->rhs_ro, s->rhs_rou, s->rhs_rov, s->rhs_xx, s->rhs_xy, s->rhs_yy, s->rhs_zz};
+    for (int f = 0; f < 7; f++) memcpy(rhs + (size_t)f * n, src[f], sizeof(double) * n);
+    return 0;
+}
+
+/* filter_variables: rhs_di.F90:667-720, rhs.F90:792-900, rhs_lc.F90:818-893 */
+static void filter_variables(OrSim *s) {
+    const int form = s->cfg.form, npfb = s->npfb;
+    double *work = zarr(npfb);
+    calc_filtered_var(s, s->ro, work);
+    calc_filtered_var(s, s->rou, work);
+    calc_filtered_var(s, s->rov, work);
+    if (form == OR_FORM_DI) {
+        calc_filtered_var(s, s->cxx, work);
+        calc_filtered_var(s, s->cxy, work);
+        calc_filtered_var(s, s->cyy, work);
+        calc_filtered_var(s, s->czz, work);
+    } else if (form == OR_FORM_CHL) {
+        const double L2 = s->cfg.fenep_l2;
+        if (s->cfg.fenep) {
+            for (int i = 0; i < s->np; i++) {
+                double fr = ((exp(2.0 * s->psixx[i]) + s->psixy[i] * s->psixy[i]) + exp(2.0 * s->psiyy[i])) + exp(2.0 * s->psizz[i]);
+                fr = (L2 * fr) / ((L2 - 3.0) + fr);
+                fr = (L2 - 3.0) / (L2 - fr);
+                s->psixx[i] = s->psixx[i] - log(sqrt(fr));
+                s->psixy[i] = s->psixy[i] / sqrt(fr);
+                s->psiyy[i] = s->psiyy[i] - log(sqrt(fr));
+                s->psizz[i] = s->psizz[i] - log(sqrt(fr));
+            }
+        }
+        calc_filtered_var(s, s->psixx, work);
+        calc_filtered_var(s, s->psixy, work);
+        calc_filtered_var(s, s->psiyy, work);
+        if (s->cfg.fenep) {
+            calc_filtered_var(s, s->psizz, work);
+            for (int i = 0; i < npfb; i++) {
+                double fr = (L2 - 3.0) / (L2 - (((exp(2.0 * s->psixx[i]) + s->psixy[i] * s->psixy[i]) + exp(2.0 * s->psiyy[i])) + exp(2.0 * s->psizz[i])));
+                s->psixx[i] = s->psixx[i] + log(sqrt(fr));
+                s->psixy[i] = s->psixy[i] * sqrt(fr);
+                s->psiyy[i] = s->psiyy[i] + log(sqrt(fr));
+                s->psizz[i] = s->psizz[i] + log(sqrt(fr));
+            }
+        }
+    } else if (form == OR_FORM_LC) {
+        calc_filtered_var(s, s->psixx, work);
+        calc_filtered_var(s, s->psixy, work);
+        calc_filtered_var(s, s->psiyy, work);
+        if (s->cfg.fenep) calc_filtered_var(s, s->psizz, work);
+    }
+    free(work);
+    if (s->cfg.mcorr) {
+        double tm = 0.0, tv = 0.0;
+        for (int i = 0; i < npfb; i++) {
+            tm = tm + (s->ro[i] - s->rho_char) * s->vol[i];
+            tv = tv + s->vol[i];
+        }
+        double dro = tm / tv;
+        for (int i = 0; i < npfb; i++) s->ro[i] = s->ro[i] - dro;
+    }
+}
+
+/* step_rk3_4S_2R_EE, step.F90:218-512 */
+static int step_rk3_4s_2r_ee(OrSim *s) {
+    const int npfb = s->npfb, form = s->cfg.form;
+    const double a[3] = {RK_A21, RK_A32, RK_A43};
+    const double b[4] = {RK_B1, RK_B2, RK_B3, RK_B4};
+    const double bh[4] = {RK_BH1, RK_BH2, RK_BH3, RK_BH4};
+    const double cc[4] = {0.0, RK_A21, RK_A32 + RK_B1, 1.0};
+    double RKa[3], RKb[4], RKbmbh[4], RKc[4];
+    const double dt = s->dt;
+    s->emax_nm1 = s->emax_n;
+    s->emax_n = s->emax_np1;
+    for (int k = 0; k < 3; k++) RKa[k] = dt * a[k];
+    for (int k = 0; k < 4; k++) { RKb[k] = dt * b[k]; RKbmbh[k] = dt * (b[k] - bh[k]); RKc[k] = dt * cc[k]; }
+    double *Q[6], *reg[6], *eacc[6], *rhs[6];
+    double *xx, *xy, *yy, *zz;
+    if (form == OR_FORM_DI) { xx = s->cxx; xy = s->cxy; yy = s->cyy; zz = s->czz; }
+    else { xx = s->psixx; xy = s->psixy; yy = s->psiyy; zz = s->psizz; }
+    Q[0] = s->ro; Q[1] = s->rou; Q[2] = s->rov; Q[3] = xx; Q[4] = xy; Q[5] = yy;
+    double *Qzz = zz, *Qrow = s->row;
+    rhs[0] = s->rhs_ro; rhs[1] = s->rhs_rou; rhs[2] = s->rhs_rov; rhs[3] = s->rhs_xx; rhs[4] = s->rhs_xy; rhs[5] = s->rhs_yy;
+    for (int f = 0; f < 6; f++) { reg[f] = zarr(npfb); eacc[f] = zarr(npfb); }
+    double *reg_row = zarr(npfb), *reg_zz = zarr(npfb), *e_row = zarr(npfb), *e_zz = zarr(npfb);
+    for (int i = 0; i < npfb; i++) {
+        for (int f = 0; f < 6; f++) reg[f][i] = Q[f][i];
+        reg_row[i] = Qrow[i];
+        reg_zz[i] = Qzz[i];
+    }
+    double time0 = s->time;
+    s->iRKstep = 0;
+    int rc = 0;
+    for (int k = 0; k < 3; k++) {
+        s->iRKstep++;
+        s->time = time0 + RKc[s->iRKstep - 1];
+        if (calc_all_rhs(s)) { rc = -1; goto done; }
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < npfb; i++) {
+            for (int f = 0; f < 6; f++) Q[f][i] = reg[f][i] + RKa[k] * rhs[f][i];
+            Qrow[i] = reg_row[i] + RKa[k] * s->rhs_row[i];
+            Qzz[i] = reg_zz[i] + RKa[k] * s->rhs_zz[i];
+            for (int f = 0; f < 6; f++) reg[f][i] = reg[f][i] + RKb[k] * rhs[f][i];
+            reg_row[i] = reg_row[i] + RKb[k] * s->rhs_row[i];
+            reg_zz[i] = reg_zz[i] + RKb[k] * s->rhs_zz[i];
+            for (int f = 0; f < 6; f++) eacc[f][i] = eacc[f][i] + RKbmbh[k] * rhs[f][i];
+            e_row[i] = e_row[i] + RKbmbh[k] * s->rhs_row[i];
+            e_zz[i] = e_zz[i] + RKbmbh[k] * s->rhs_zz[i];
+        }
+        if (s->nb != 0) apply_time_dependent_bounds(s);
+        reapply_mirror_bcs(s);
+        get_velocity_from_momentum(s);
+        if (form != OR_FORM_DI) get_c_from_psi(s);
+    }
+    s->iRKstep++;
+    s->time = time0 + RKc[s->iRKstep - 1];
+    if (calc_all_rhs(s)) { rc = -1; goto done; }
+    double en[6] = {0, 0, 0, 0, 0, 0}, en_row = 0.0, en_zz = 0.0;
+    const double norms[6] = {s->ero_norm, s->erou_norm, s->erou_norm, s->exx_norm, s->exx_norm, s->exx_norm};
+    for (int i = 0; i < npfb; i++) {
+        for (int f = 0; f < 6; f++) Q[f][i] = reg[f][i] + RKb[3] * rhs[f][i];
+        Qrow[i] = reg_row[i] + RKb[3] * s->rhs_row[i];
+        Qzz[i] = reg_zz[i] + RKb[3] * s->rhs_zz[i];
+        for (int f = 0; f < 6; f++) eacc[f][i] = eacc[f][i] + RKbmbh[3] * rhs[f][i];
+        e_row[i] = e_row[i] + RKbmbh[3] * s->rhs_row[i];
+        e_zz[i] = e_zz[i] + RKbmbh[3] * s->rhs_zz[i];
+        for (int f = 0; f < 6; f++) {
+            double t = fabs(eacc[f][i]) * norms[f];
+            en[f] = (t > en[f]) ? t : en[f];
+        }
+        {
+            double t = fabs(e_row[i]) * s->erou_norm;
+            en_row = (t > en_row) ? t : en_row;
+            t = fabs(e_zz[i]) * s->exx_norm;
+            en_zz = (t > en_zz) ? t : en_zz;
+        }
+        if (form == OR_FORM_CHL && s->cfg.fenep) {
+            double fr = (s->cfg.fenep_l2 - 3.0) / (((s->cfg.fenep_l2 - s->cxx[i]) - s->cyy[i]) - s->czz[i]);
+            fr = 1.0 / sqrt(fr);
+            en[3] = en[3] * fr; en[4] = en[4] * fr; en[5] = en[5] * fr; en_zz = en_zz * fr;
+        }
+    }
+#define MAXD(a, b) ((a) > (b) ? (a) : (b))
+    /* emax_conf = max(xx, max(xy, max(yy, max(xz, max(yz, zz))))) with xz = yz = 0 */
+    double emax_conf = MAXD(en[3], MAXD(en[4], MAXD(en[5], MAXD(0.0, MAXD(0.0, en_zz)))));
+    s->emax_np1 = MAXD(emax_conf, MAXD(en[0], MAXD(en[1], MAXD(en[2], MAXD(en_row, doublesmall)))));
+#undef MAXD
+    if (s->nb != 0) apply_time_dependent_bounds(s);
+    reapply_mirror_bcs(s);
+    filter_variables(s);
+    if (s->nb != 0) apply_time_dependent_bounds(s);
+    reapply_mirror_bcs(s);
+    get_velocity_from_momentum(s);
+    if (form != OR_FORM_DI) get_c_from_psi(s);
+done:
+    for (int f = 0; f < 6; f++) { free(reg[f]); free(eacc[f]); }
+    free(reg_row); free(reg_zz); free(e_row); free(e_zz);
+    return rc;
+}
+
+/* set_tstep, step.F90:569-622 */
+int or_set_tstep(OrSim *s, double *dt_cfl, double *dt_parabolic) {
+    double dcfl = 1.0e10, dvisc = 1.0e10;
+    for (int i = 0; i < s->npfb; i++) {
+        double c = sqrt(s->csq);
+        double umax = sqrt((s->u[i] * s->u[i] + s->v[i] * s->v[i]) + s->w[i] * s->w[i]);
+        double uplusc = umax + c;
+        double t = (s->type[i] == 2) ? (0.8 * s->sp[i]) / uplusc : s->sp[i] / uplusc;
+        dcfl = (t < dcfl) ? t : dcfl;
+        t = ((s->sp[i] * s->sp[i]) * s->ro[i]) / s->visc_total;
+        dvisc = (t < dvisc) ? t : dvisc;
+    }
+    s->dt_cfl = (1.0 * dcfl) * s->cfg.L_char;
+    s->dt_parabolic = (((2.0 / 3.0) * dvisc) * s->cfg.L_char) * s->cfg.L_char;
+    if (dt_cfl) *dt_cfl = s->dt_cfl;
+    if (dt_parabolic) *dt_parabolic = s->dt_parabolic;
+    return 0;
+}
+
+/* set_tstep_PID, step.F90:624-682 */
+static void set_tstep_pid(OrSim *s) {
+    double facA = PID_A * log(pid_tol / s->emax_np1);
+    double facB = PID_B * log(s->emax_n / pid_tol);
+    double facC = PID_C * log(pid_tol / s->emax_nm1);
+    double dtfactor = pid_k * exp((facA + facB) + facC);
+    dtfactor = (0.5 > dtfactor) ? 0.5 : dtfactor;
+    dtfactor = (1.02 < dtfactor) ? 1.02 : dtfactor;
+    s->dt = s->dt * dtfactor;
+    double dt_max = (s->dt_cfl < s->dt_parabolic) ? s->dt_cfl : s->dt_parabolic;
+    if (s->dt > dt_max) s->dt = dt_max;
+}
+
+int or_step(OrSim *s, double dt, int nsteps, int pid) {
+    if (!s->have_weights || !s->ro) return fail(s, "weights or state missing");
+    for (int n = 0; n < nsteps; n++) {
+        if (pid) {
+            or_set_tstep(s, NULL, NULL);
+            set_tstep_pid(s);
+        } else {
+            s->dt = dt;
+        }
+        if (step_rk3_4s_2r_ee(s)) return -1;
+        s->itime++;
+    }
+    return 0;
+}
+
+int or_get_time(OrSim *s, double *time, double *dt, int *itime, double *emax) {
+    if (time) *time = s->time;
+    if (dt) *dt = s->dt;
+    if (itime) *itime = s->itime;
+    if (emax) { emax[0] = s->emax_nm1; emax[1] = s->emax_n; emax[2] = s->emax_np1; }
+    return 0;
+}
+int or_set_time(OrSim *s, double time, double dt, int itime, const double *emax) {
+    s->time = time; s->dt = dt; s->itime = itime;
+    if (emax) { s->emax_nm1 = emax[0]; s->emax_n = emax[1]; s->emax_np1 = emax[2]; }
+    return 0;
+}
+
+double or_kinetic_energy(OrSim *s) {
+    double ke = 0.0;
+    for (int i = 0; i < s->npfb; i++)
+        ke = ke + ((0.5 * s->ro[i]) * (s->u[i] * s->u[i] + s->v[i] * s->v[i])) * s->vol[i];
+    return ke;
+}
+double or_mass(OrSim *s) {
+    double m = 0.0;
+    for (int i = 0; i < s->npfb; i++) m = m + s->ro[i] * s->vol[i];
+    return m;
+}

@@ -1,0 +1,574 @@
+// abi.cu -- the extern "C" entry points of include/sunset_gpu.h: argument checks, the host
+// part of build_domain (IPART rows -> nodes + FD rows, setup_domain.F90:177-202), the
+// reference-order <-> Morton-order permutations, and the calls into the device stages.
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace sunset {
+
+int set_err(Handle *H, int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    H->err = buf;
+    return code;
+}
+
+void dfree(Handle *H, void *p) {
+    if (!p) return;
+    auto it = std::find(H->allocs.begin(), H->allocs.end(), p);
+    if (it != H->allocs.end()) {
+        cudaFree(p);
+        H->allocs.erase(it);
+    }
+}
+
+namespace {
+
+__global__ void k_gather(const double *in, const int *perm, int n, double *out) {  // out[i] = in[perm[i]]
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[perm[i]];
+}
+__global__ void k_scatter(const double *in, const int *perm, int n, double *out) {  // out[perm[i]] = in[i]
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[perm[i]] = in[i];
+}
+
+double hovs_for(int forder) {  // common_parameter.F90:44-56
+    if (forder == 4) return 1.8;
+    if (forder == 6) return 2.4;
+    if (forder == 10) return 3.1;
+    return 2.7;
+}
+double hovs_bound_for(int forder) { return forder == 4 ? 2.1 : 2.4; }
+
+int set_device(Handle *H) {
+    SUNSET_CUDA(H, cudaSetDevice(H->device));
+    return 0;
+}
+
+// Copies a reference-order array (host or device) into internal order on the device.
+int to_internal(Handle *H, const double *src, int flags, double *dst) {
+    const int n = H->npfb;
+    double *ref = H->tmpd + 3 * (size_t)n;
+    if (flags == SUNSET_PTR_DEVICE) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(ref, src, n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
+    } else {
+        SUNSET_CUDA(H, cudaMemcpyAsync(ref, src, n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    }
+    k_gather<<<(n + 255) / 256, 256, 0, H->stream>>>(ref, H->perm, n, dst);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+int to_reference(Handle *H, const double *src, int flags, double *dst) {
+    const int n = H->npfb;
+    double *ref = H->tmpd + 3 * (size_t)n;
+    k_scatter<<<(n + 255) / 256, 256, 0, H->stream>>>(src, H->perm, n, ref);
+    SUNSET_CUDA(H, cudaGetLastError());
+    if (flags == SUNSET_PTR_DEVICE) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(dst, ref, n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
+    } else {
+        SUNSET_CUDA(H, cudaMemcpyAsync(dst, ref, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+        SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    }
+    return 0;
+}
+
+int need(Handle *H, bool ok, const char *what) {
+    if (!ok) return set_err(H, SUNSET_ERR_ARG, "call order: %s first", what);
+    return 0;
+}
+
+int check_err_flag(Handle *H) {
+    int e = 0;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&e, &H->dsc->err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    if (e) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite time-step error norm");
+    return 0;
+}
+
+}  // namespace
+}  // namespace sunset
+
+using namespace sunset;
+
+extern "C" {
+
+int sunset_version(void) { return 1; }
+
+int sunset_create(const SunsetConfig *cfg, SunsetHandle **out) {
+    if (!cfg || !out) return SUNSET_ERR_ARG;
+    SunsetHandle *sh = new SunsetHandle();
+    Handle *H = &sh->H;
+    H->cfg = *cfg;
+    if (H->cfg.L_char == 0.0) H->cfg.L_char = 1.0;
+    if (H->cfg.U_char == 0.0) H->cfg.U_char = 1.0;
+    H->device = cfg->device;
+    *out = sh;
+    const SunsetConfig &c = H->cfg;
+    if (!(c.morder == 4 || c.morder == 6 || c.morder == 8 || c.morder == 10) || c.forder != c.morder)
+        return set_err(H, SUNSET_ERR_SCOPE, "orders must be equal and one of 4, 6, 8, 10 (got %d, %d)", c.morder, c.forder);
+    if (c.form < 0 || c.form > 3) return set_err(H, SUNSET_ERR_ARG, "unknown form %d", c.form);
+    if (c.fenep) return set_err(H, SUNSET_ERR_SCOPE, "FENE-P is not implemented on the device path");
+    if (c.precision != SUNSET_FP64 && c.precision != SUNSET_MIXED) return set_err(H, SUNSET_ERR_ARG, "bad precision");
+    if (c.Re <= 0 || c.Ma <= 0 || (c.form != SUNSET_FORM_NEWT && c.Wi <= 0))
+        return set_err(H, SUNSET_ERR_ARG, "Re, Ma and Wi must be positive");
+    if (int rc = set_device(H)) return rc;
+    SUNSET_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+    return 0;
+}
+
+void sunset_destroy(SunsetHandle *sh) {
+    if (!sh) return;
+    Handle *H = &sh->H;
+    cudaSetDevice(H->device);
+    if (H->stream) cudaStreamSynchronize(H->stream);
+    for (int b = 0; b < 2; b++)
+        if (H->graph[b]) cudaGraphExecDestroy(H->graph[b]);
+    for (void *p : H->allocs) cudaFree(p);
+    H->allocs.clear();
+    if (H->stream) cudaStreamDestroy(H->stream);
+    delete sh;
+}
+
+const char *sunset_last_error(const SunsetHandle *sh) { return sh ? sh->H.err.c_str() : "null handle"; }
+
+int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double *x, const double *y,
+                        const int *node_type, const double *nx, const double *ny, const double *s, double xmin,
+                        double xmax, double ymin, double ymax, const int *bcond, double smax) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (H->domain_ok) return set_err(H, SUNSET_ERR_ARG, "domain already built; create a new handle");
+    if (nrows <= 0 || !x || !y || !node_type || !s || !bcond) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
+    if (!(xmax > xmin && ymax > ymin)) return set_err(H, SUNSET_ERR_ARG, "empty domain");
+    if (int rc = set_device(H)) return rc;
+    (void)gi;
+    const double hovs = hovs_for(H->cfg.forder), hovs_bound = hovs_bound_for(H->cfg.forder);
+    const double hos = H->cfg.h_over_s;
+    std::vector<double> vx, vy, vh, vs;
+    std::vector<int> vt;
+    int nb = 0;
+    for (int r = 0; r < nrows; r++) {  // setup_domain.F90:177-199
+        int t = node_type[r];
+        if (t >= 0 && t <= 2) nb++;
+        vx.push_back(x[r]);
+        vy.push_back(y[r]);
+        vs.push_back(s[r]);
+        vt.push_back(t);
+        vh.push_back(s[r] * hovs);
+        if (t >= 0 && t <= 2) {
+            vh.back() = s[r] * hovs_bound;
+            double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
+            for (int j = 1; j <= 4; j++) {
+                vx.push_back(x[r] + (rnx * (double)j) * s[r]);
+                vy.push_back(y[r] + (rny * (double)j) * s[r]);
+                vs.push_back(s[r]);
+                vt.push_back(-j);
+                vh.push_back(s[r] * hovs_bound);
+            }
+        }
+    }
+    if (nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "boundary nodes (walls/inflow/outflow) are not implemented on the device path");
+    const int n = (int)vx.size();
+    if (n >= (1 << 30)) return set_err(H, SUNSET_ERR_SCOPE, "too many nodes");
+    if (hos > 0)
+        for (int i = 0; i < n; i++) vh[i] = hos * vs[i];
+    std::vector<double> vhs = vh;  // h_small = h
+    H->npfb = n;
+    H->nb = nb;
+    H->nrows = nrows;
+    H->xmin = xmin; H->xmax = xmax; H->ymin = ymin; H->ymax = ymax;
+    for (int c = 0; c < 4; c++) H->bc[c] = bcond[c];
+    if ((bcond[0] == 1) != (bcond[1] == 1) || (bcond[2] == 1) != (bcond[3] == 1))
+        return set_err(H, SUNSET_ERR_ARG, "periodic boundary conditions incorrectly specified with bcond");
+    H->smax = smax;
+    H->h0 = (hos > 0 ? hos : hovs) * smax;  // setup_domain.F90:105
+    H->h2 = H->h0 * H->h0;
+    H->h3 = H->h2 * H->h0;
+    H->hmax = *std::max_element(vh.begin(), vh.end());
+    int rc = build_domain_device(H, vx, vy, vh, vhs, vs, vt);
+    if (rc) return rc;
+    H->domain_ok = true;
+    return 0;
+}
+
+int sunset_get_sizes(SunsetHandle *sh, int *np, int *npfb, int *nb, int *nplink) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (np) *np = H->np;
+    if (npfb) *npfb = H->npfb;
+    if (nb) *nb = H->nb;
+    if (nplink) *nplink = H->nplink;
+    return 0;
+}
+
+int sunset_find_neighbours(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->domain_ok, "sunset_build_domain")) return rc;
+    if (H->nbr_ok) return set_err(H, SUNSET_ERR_ARG, "neighbours already built");
+    if (int rc = set_device(H)) return rc;
+    int rc = find_neighbours_device(H);
+    if (rc) return rc;
+    H->nbr_ok = true;
+    return 0;
+}
+
+int sunset_calc_labf_weights(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->nbr_ok, "sunset_find_neighbours")) return rc;
+    if (int rc = set_device(H)) return rc;
+    int rc = labf_weights_device(H);
+    if (rc) return rc;
+    H->w_ok = true;
+    H->sums_ok = H->fc_ok = false;
+    return 0;
+}
+
+int sunset_calc_labf_sums(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->w_ok && !H->sums_ok, "sunset_calc_labf_weights")) return rc;
+    if (int rc = set_device(H)) return rc;
+    int rc = labf_sums_device(H);
+    if (rc) return rc;
+    H->sums_ok = true;
+    return 0;
+}
+
+int sunset_filter_coefficients(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->sums_ok && !H->fc_ok, "sunset_calc_labf_sums")) return rc;
+    if (int rc = set_device(H)) return rc;
+    int rc = filter_coefficients_device(H);
+    if (rc) return rc;
+    rc = state_alloc(H);
+    if (rc) return rc;
+    if (H->cfg.precision == SUNSET_MIXED) {
+        rc = make_mixed_weights(H);
+        if (rc) return rc;
+    }
+    H->fc_ok = true;
+    return 0;
+}
+
+int sunset_get_neighbours(SunsetHandle *sh, int *ij_count, int *ij_count_small, int *ij_link) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->nbr_ok, "sunset_find_neighbours")) return rc;
+    if (int rc = set_device(H)) return rc;
+    const int n = H->npfb, nplink = H->nplink;
+    std::vector<int> cnt(n), cs(n), lpt(H->nlinks_sell);
+    std::vector<long long> sptr(H->nslices + 1);
+    SUNSET_CUDA(H, cudaMemcpy(cnt.data(), H->cnt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(lpt.data(), H->lpt, lpt.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sptr.data(), H->slice_ptr, sptr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < n; r++) {
+        int i = H->h_iperm[r];
+        if (ij_count) ij_count[r] = cnt[i];
+        if (ij_count_small) ij_count_small[r] = cs[i];
+        if (ij_link) {
+            for (int k = 0; k < nplink; k++) {
+                int v = 0;
+                if (k < cnt[i]) {
+                    int p = lpt[sptr[i >> 5] + (long long)k * kSlice + (i & 31)];
+                    v = (p < n ? H->h_perm[p] : p) + 1;
+                }
+                ij_link[(size_t)r * nplink + k] = v;
+            }
+        }
+    }
+    return 0;
+}
+
+int sunset_get_weights(SunsetHandle *sh, double *w_grad, double *w_lap, double *w_hyp, double *w_grad_sum,
+                       double *w_lap_sum, double *w_hyp_sum, double *vol) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->w_ok, "sunset_calc_labf_weights")) return rc;
+    if (int rc = set_device(H)) return rc;
+    const int n = H->npfb, nplink = H->nplink;
+    const size_t L = H->nlinks_sell;
+    std::vector<int> cnt(n);
+    std::vector<long long> sptr(H->nslices + 1);
+    SUNSET_CUDA(H, cudaMemcpy(cnt.data(), H->cnt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sptr.data(), H->slice_ptr, sptr.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    auto scatter_links = [&](const double *dsrc, double *dst, int stride, int comp) -> int {
+        std::vector<double> tmp(L);
+        SUNSET_CUDA(H, cudaMemcpy(tmp.data(), dsrc, L * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int r = 0; r < n; r++) {
+            int i = H->h_iperm[r];
+            for (int k = 0; k < nplink; k++) {
+                double v = 0.0;
+                if (k < cnt[i]) v = tmp[sptr[i >> 5] + (long long)k * kSlice + (i & 31)];
+                dst[((size_t)r * nplink + k) * stride + comp] = v;
+            }
+        }
+        return 0;
+    };
+    auto scatter_nodes = [&](const double *dsrc, double *dst, int stride, int comp) -> int {
+        std::vector<double> tmp(n);
+        SUNSET_CUDA(H, cudaMemcpy(tmp.data(), dsrc, n * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int r = 0; r < n; r++) dst[(size_t)r * stride + comp] = tmp[H->h_iperm[r]];
+        return 0;
+    };
+    int rc = 0;
+    if (w_grad && !rc) rc = scatter_links(H->wx, w_grad, 2, 0);
+    if (w_grad && !rc) rc = scatter_links(H->wy, w_grad, 2, 1);
+    if (w_lap && !rc) rc = scatter_links(H->wl, w_lap, 1, 0);
+    if (w_hyp && !rc) rc = scatter_links(H->wh, w_hyp, 1, 0);
+    if (H->sums_ok) {
+        if (w_grad_sum && !rc) rc = scatter_nodes(H->gsx, w_grad_sum, 2, 0);
+        if (w_grad_sum && !rc) rc = scatter_nodes(H->gsy, w_grad_sum, 2, 1);
+        if (w_lap_sum && !rc) rc = scatter_nodes(H->lsum, w_lap_sum, 1, 0);
+        if (w_hyp_sum && !rc) rc = scatter_nodes(H->hsum, w_hyp_sum, 1, 0);
+        if (vol && !rc) rc = scatter_nodes(H->vol, vol, 1, 0);
+    }
+    return rc;
+}
+
+static int op_common(SunsetHandle *sh, Handle **HH) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    *HH = H;
+    if (int rc = need(H, H->fc_ok, "sunset_filter_coefficients")) return rc;
+    return set_device(H);
+}
+
+int sunset_calc_gradient(SunsetHandle *sh, const double *phi, double *grad, int flags) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!phi || !grad) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    double *p = H->tmpd, *gx = H->tmpd + n, *gy = H->tmpd + 2 * (size_t)n;
+    if (int rc = to_internal(H, phi, flags, p)) return rc;
+    if (int rc = op_gradient(H, p, gx, gy)) return rc;
+    std::vector<double> hx(n), hy(n);
+    double *ref = H->tmpd + 3 * (size_t)n;
+    for (int c = 0; c < 2; c++) {
+        const double *src = c == 0 ? gx : gy;
+        std::vector<double> &dst = c == 0 ? hx : hy;
+        if (int rc = to_reference(H, src, SUNSET_PTR_DEVICE, ref)) return rc;
+        SUNSET_CUDA(H, cudaMemcpyAsync(dst.data(), ref, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+        SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    }
+    if (flags == SUNSET_PTR_DEVICE) {
+        std::vector<double> inter(2 * (size_t)n);
+        for (int r = 0; r < n; r++) { inter[2 * r] = hx[r]; inter[2 * r + 1] = hy[r]; }
+        SUNSET_CUDA(H, cudaMemcpy(grad, inter.data(), inter.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        for (int r = 0; r < n; r++) { grad[2 * r] = hx[r]; grad[2 * r + 1] = hy[r]; }
+    }
+    return 0;
+}
+
+int sunset_calc_laplacian(SunsetHandle *sh, const double *phi, double *lap, int flags) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!phi || !lap) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    double *p = H->tmpd, *o = H->tmpd + n;
+    if (int rc = to_internal(H, phi, flags, p)) return rc;
+    if (int rc = op_laplacian(H, p, o)) return rc;
+    return to_reference(H, o, flags, lap);
+}
+
+int sunset_calc_filtered_var(SunsetHandle *sh, const double *phi, double *out, int flags) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!phi || !out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    double *p = H->tmpd, *o = H->tmpd + n;
+    if (int rc = to_internal(H, phi, flags, p)) return rc;
+    if (int rc = op_filter(H, p, o, 0)) return rc;
+    return to_reference(H, o, flags, out);
+}
+
+int sunset_calc_filter_term(SunsetHandle *sh, const double *phi, double *out, int flags) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!phi || !out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    double *p = H->tmpd, *o = H->tmpd + n;
+    if (int rc = to_internal(H, phi, flags, p)) return rc;
+    if (int rc = op_filter(H, p, o, 1)) return rc;
+    return to_reference(H, o, flags, out);
+}
+
+int sunset_set_state(SunsetHandle *sh, const double *ro, const double *u, const double *v, const double *cxx,
+                     const double *cxy, const double *cyy, const double *czz) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!ro || !u || !v || !cxx || !cxy || !cyy) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    // stage the seven inputs in internal order inside the (not yet used) second buffer and rhs
+    double *d[7] = {H->rhs[0], H->rhs[1], H->rhs[2], H->rhs[3], H->rhs[4], H->rhs[5], H->rhs[6]};
+    const double *src[7] = {ro, u, v, cxx, cxy, cyy, czz};
+    std::vector<double> ones;
+    if (!czz) {
+        ones.assign(n, 1.0);
+        src[6] = ones.data();
+    }
+    for (int f = 0; f < 7; f++)
+        if (int rc = to_internal(H, src[f], SUNSET_PTR_HOST, d[f])) return rc;
+    int rc = state_set_device(H, d[0], d[1], d[2], d[3], d[4], d[5], d[6]);
+    if (rc) return rc;
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    H->state_ok = true;
+    return 0;
+}
+
+int sunset_get_state(SunsetHandle *sh, double *out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    const int n = H->npfb;
+    const Fields &F = H->buf[H->cur];
+    const double *src[13] = {F.ro, F.rou, F.rov, F.u, F.v, F.q[0], F.q[1], F.q[2], F.q[3], F.c[0], F.c[1], F.c[2], F.c[3]};
+    for (int f = 0; f < 13; f++) {
+        if (H->cfg.form == SUNSET_FORM_DI && f >= 5 && f <= 8) {
+            for (int r = 0; r < n; r++) out[(size_t)f * n + r] = 0.0;
+            continue;
+        }
+        if (int rc = to_reference(H, src[f], SUNSET_PTR_HOST, out + (size_t)f * n)) return rc;
+    }
+    return 0;
+}
+
+int sunset_calc_all_rhs(SunsetHandle *sh, double *out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (int rc = rhs_only(H)) return rc;
+    for (int f = 0; f < 7; f++)
+        if (int rc = to_reference(H, H->rhs[f], SUNSET_PTR_HOST, out + (size_t)f * H->npfb)) return rc;
+    return 0;
+}
+
+int sunset_set_tstep(SunsetHandle *sh, double *dt_cfl, double *dt_parabolic) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (int rc = set_tstep_device(H)) return rc;
+    DevScalars s;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&s, H->dsc, sizeof(s), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    if (dt_cfl) *dt_cfl = s.dt_cfl;
+    if (dt_parabolic) *dt_parabolic = s.dt_par;
+    return 0;
+}
+
+int sunset_step(SunsetHandle *sh, double dt, int nsteps, int mode) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (nsteps < 0 || (mode == 0 && !(dt > 0.0)) || mode < 0 || mode > 1)
+        return set_err(H, SUNSET_ERR_ARG, "bad dt/nsteps/mode");
+    if (int rc = step_run(H, dt, nsteps, mode)) return rc;
+    return check_err_flag(H);
+}
+
+int sunset_step_timed(SunsetHandle *sh, double dt, int nsteps, int mode, double *ms) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (nsteps < 0 || (mode == 0 && !(dt > 0.0)) || mode < 0 || mode > 1 || !ms)
+        return set_err(H, SUNSET_ERR_ARG, "bad dt/nsteps/mode");
+    cudaEvent_t e0, e1;
+    SUNSET_CUDA(H, cudaEventCreate(&e0));
+    SUNSET_CUDA(H, cudaEventCreate(&e1));
+    SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
+    int rc = step_run(H, dt, nsteps, mode);
+    SUNSET_CUDA(H, cudaEventRecord(e1, H->stream));
+    SUNSET_CUDA(H, cudaEventSynchronize(e1));
+    float t = 0.f;
+    SUNSET_CUDA(H, cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t;
+    if (rc) return rc;
+    return check_err_flag(H);
+}
+
+int sunset_get_time(SunsetHandle *sh, double *time, double *dt, int *itime, double *emax) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    DevScalars s;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&s, H->dsc, sizeof(s), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    if (time) *time = s.time;
+    if (dt) *dt = s.dt;
+    if (itime) *itime = s.itime;
+    if (emax) { emax[0] = s.emax_nm1; emax[1] = s.emax_n; emax[2] = s.emax_np1; }
+    return 0;
+}
+
+int sunset_set_time(SunsetHandle *sh, double time, double dt, int itime, const double *emax) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    DevScalars s;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&s, H->dsc, sizeof(s), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    s.time = time; s.dt = dt; s.itime = itime;
+    if (emax) { s.emax_nm1 = emax[0]; s.emax_n = emax[1]; s.emax_np1 = emax[2]; }
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+int sunset_kinetic_energy(SunsetHandle *sh, double *ke) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    return reduce_ke_mass(H, ke, nullptr);
+}
+
+int sunset_mass(SunsetHandle *sh, double *mass) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    return reduce_ke_mass(H, nullptr, mass);
+}
+
+int sunset_synchronize(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+int sunset_run_host(SunsetHandle *sh, const double *state_in, double dt, int nsteps, double *state_out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    const int n = H->npfb;
+    double *d[7] = {H->rhs[0], H->rhs[1], H->rhs[2], H->rhs[3], H->rhs[4], H->rhs[5], H->rhs[6]};
+    for (int f = 0; f < 7; f++)
+        if (int rc = to_internal(H, state_in + (size_t)f * n, SUNSET_PTR_HOST, d[f])) return rc;
+    if (int rc = state_set_conservative_device(H, d)) return rc;
+    if (int rc = step_run(H, dt, nsteps, 0)) return rc;
+    const Fields &F = H->buf[H->cur];
+    const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
+    for (int f = 0; f < 7; f++)
+        if (int rc = to_reference(H, src[f], SUNSET_PTR_HOST, state_out + (size_t)f * n)) return rc;
+    return check_err_flag(H);
+}
+
+int sunset_time_stage_kernel(SunsetHandle *sh, int reps, double *ms_per_launch, double *bytes_per_launch) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (reps <= 0 || !ms_per_launch || !bytes_per_launch) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
+    return time_stage_kernel(H, reps, ms_per_launch, bytes_per_launch);
+}
+
+}  // extern "C"

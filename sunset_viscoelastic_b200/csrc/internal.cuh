@@ -1,0 +1,178 @@
+// internal.cuh -- shared definitions of the B200 LABFM path (device layout, handle, helpers).
+//
+// Device layout
+//   * Interior nodes are renumbered in Morton (Z-curve) order of their position; perm[i]
+//     gives the reference index of internal node i, iperm the inverse.
+//   * Ghost points (the reference's mirror nodes, mirror_boundaries.F90:34-261) exist only
+//     as positions for the weight build; each link stores the internal index of the
+//     parent plus a 2-bit reflection code, so fields are never copied to ghosts.
+//   * Links are kept in sliced ELL: slices of 32 consecutive internal nodes, each padded
+//     to its own width; link k of node i sits at slice_ptr[i/32] + 32*k + i%32, so a warp
+//     reading link k of its 32 nodes issues one coalesced access.  Padding has weight 0
+//     and points at node 0.
+//   * Fields are structure-of-arrays FP64 (or FP32 in the mixed path).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sunset_gpu.h"
+
+namespace sunset {
+
+constexpr double kPi = 3.141592653589793238462643383279502884197;
+constexpr double kSs = 2.0;  // stencil support in units of h, common_parameter.F90:68
+constexpr int kSlice = 32;
+constexpr int kLinkMask = 0x3fffffff;  // low 30 bits: internal parent index
+
+// RK3(2)4[2R+]C, common_parameter.F90:74-94
+#define SUNSET_RK_A21 (11847461282814.0 / 36547543011857.0)
+#define SUNSET_RK_A32 (3943225443063.0 / 7078155732230.0)
+#define SUNSET_RK_A43 (-346793006927.0 / 4029903576067.0)
+#define SUNSET_RK_B1 (1017324711453.0 / 9774461848756.0)
+#define SUNSET_RK_B2 (8237718856693.0 / 13685301971492.0)
+#define SUNSET_RK_B3 (57731312506979.0 / 19404895981398.0)
+#define SUNSET_RK_B4 (-101169746363290.0 / 37734290219643.0)
+#define SUNSET_RK_BH1 (15763415370699.0 / 46270243929542.0)
+#define SUNSET_RK_BH2 (514528521746.0 / 5659431552419.0)
+#define SUNSET_RK_BH3 (27030193851939.0 / 9429696342944.0)
+#define SUNSET_RK_BH4 (-69544964788955.0 / 30262026368149.0)
+
+inline int nsize_for(int k) { return (k * k + 3 * k) / 2; }  // labf.F90:56
+
+// Scalars the step kernels share on the device (one per handle).
+struct DevScalars {
+    double dt, time;
+    double emax_nm1, emax_n, emax_np1;
+    double dro;            // mass correction of the current step
+    double tv;             // sum of node volumes (constant once the weights exist)
+    double dt_cfl, dt_par; // set_tstep results of the current state
+    unsigned long long emax_bits;  // running max of the step's error norm (bit pattern)
+    unsigned long long cfl_bits, par_bits;  // running minima (bit patterns, positive)
+    unsigned int done_ctr;  // last-block counter of the mass reduction
+    int itime;
+    int err;  // nonzero: non-finite error norm
+};
+
+// One buffer of the state: conservative fields, conformation variables and the derived
+// fields (velocity and c) the stencils read.
+struct Fields {
+    double *ro, *rou, *rov;
+    double *q[4];   // DI: cxx cxy cyy czz; LC/CHL: psixx psixy psiyy psizz
+    double *u, *v;
+    double *c[4];   // cxx cxy cyy czz (DI: aliases q)
+};
+
+struct StepConsts {
+    int npfb, nslices, form, fenep, mcorr, kolmo, di_full, has_mirrors, mdiff_on;
+    double csq, c_sound, coef_solvent, coef_polymeric, lambda, epsPTT, fenep_l2, Mdiff, Re, Wi, beta;
+    double visc_total, rho_char, L_char, grav0, grav1, ero_norm, erou_norm, exx_norm;
+};
+
+struct Handle {
+    SunsetConfig cfg{};
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    // ---- domain (host copies kept for export) ----
+    int npfb = 0, np = 0, nb = 0, nghost = 0, nrows = 0;
+    double xmin = 0, xmax = 0, ymin = 0, ymax = 0, smax = 0, h0 = 0, h2 = 0, h3 = 0, hmax = 0;
+    int bc[4] = {0, 0, 0, 0};
+    std::vector<int> h_perm, h_iperm;  // internal <-> reference
+    bool domain_ok = false, nbr_ok = false, w_ok = false, sums_ok = false, fc_ok = false;
+    bool state_ok = false;
+
+    // ---- device: points (internal interior 0..npfb-1, ghosts npfb..np-1) ----
+    double *px = nullptr, *py = nullptr;       // np
+    double *h = nullptr, *hs = nullptr, *sp = nullptr;  // npfb (internal order)
+    int *ntype = nullptr;                      // npfb
+    int *gpar = nullptr, *gvrel = nullptr;     // ghosts: parent (internal), vrel 1..4
+    int *perm = nullptr, *iperm = nullptr;     // npfb
+
+    // ---- neighbours (sliced ELL) ----
+    int nslices = 0, nplink = 0;
+    long long nlinks_sell = 0;
+    long long *slice_ptr = nullptr;            // nslices+1
+    int *slice_w = nullptr, *slice_ws = nullptr;  // widths: all links, small links
+    int *cnt = nullptr, *cnt_small = nullptr;  // npfb
+    int *lpt = nullptr;                        // SELL: point id (ghost-aware), for setup/export
+    int *lidx = nullptr;                       // SELL: parent | vrel code << 30
+    bool has_mirrors = false;
+
+    // ---- weights (SELL, FP64) ----
+    double *wx = nullptr, *wy = nullptr, *wl = nullptr, *wh = nullptr;
+    double *gsx = nullptr, *gsy = nullptr, *lsum = nullptr, *hsum = nullptr, *vol = nullptr;
+    // mixed-precision copies
+    float *wx32 = nullptr, *wy32 = nullptr, *wl32 = nullptr, *wh32 = nullptr;
+    float *wx32lo = nullptr, *wy32lo = nullptr, *wl32lo = nullptr, *wh32lo = nullptr;
+
+    // ---- state ----
+    Fields buf[2]{};
+    int cur = 0;  // buffer holding the current state
+    double *reg[7] = {};   // RK register S: ro rou rov q0..q3
+    double *eacc[7] = {};  // error accumulators
+    double *rhs[7] = {};   // rhs output of sunset_calc_all_rhs
+    double *partials = nullptr;
+    int npart = 0;
+    DevScalars *dsc = nullptr;
+    double *tmpd = nullptr;  // scratch, 4*npfb doubles
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_mode[2] = {-1, -1};
+
+    std::vector<void *> allocs;
+};
+
+// error helpers
+int set_err(Handle *H, int code, const char *fmt, ...);
+#define SUNSET_CUDA(H, call)                                                                    \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return ::sunset::set_err((H), SUNSET_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
+                                     cudaGetErrorString(e_), __FILE__, __LINE__);               \
+    } while (0)
+
+template <typename T>
+int dalloc(Handle *H, T **p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) return set_err(H, SUNSET_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    H->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return 0;
+}
+void dfree(Handle *H, void *p);
+
+// stage entry points implemented in the .cu files
+int build_domain_device(Handle *H, const std::vector<double> &x, const std::vector<double> &y,
+                        const std::vector<double> &h, const std::vector<double> &hs,
+                        const std::vector<double> &s, const std::vector<int> &type);
+int find_neighbours_device(Handle *H);
+int labf_weights_device(Handle *H);
+int labf_sums_device(Handle *H);
+int filter_coefficients_device(Handle *H);
+int make_mixed_weights(Handle *H);
+
+int state_alloc(Handle *H);
+int state_set_device(Handle *H, const double *ro, const double *u, const double *v, const double *cxx,
+                     const double *cxy, const double *cyy, const double *czz);  // internal order, device
+int state_set_conservative_device(Handle *H, const double *const *f7);  // internal order, device
+int step_run(Handle *H, double dt, int nsteps, int mode);
+int rhs_only(Handle *H);
+int set_tstep_device(Handle *H);
+int op_gradient(Handle *H, const double *phi, double *gx, double *gy);
+int op_laplacian(Handle *H, const double *phi, double *lap);
+int op_filter(Handle *H, const double *phi, double *out, int term_only);
+int reduce_ke_mass(Handle *H, double *ke, double *mass);
+int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes);
+
+}  // namespace sunset
+
+// C-ABI handle
+struct SunsetHandle {
+    sunset::Handle H;
+};

@@ -1,0 +1,225 @@
+// physics.cuh -- pointwise right-hand sides of the viscoelastic equations on one node
+// (2-D, interior nodes), restated from rhs_di.F90, rhs.F90 (Cholesky) and rhs_lc.F90,
+// and the conformation transforms of conf_transforms.F90.  Expressions keep the
+// reference's left-to-right order; zero third components are kept as the literal
+// "+ 0.0" terms so signed zeros match the reference's too.
+#pragma once
+
+#include "internal.cuh"
+
+namespace sunset {
+
+// Stencil results the right-hand sides read.
+struct Grads {
+    double ro_x, ro_y, u_x, u_y, v_x, v_y, lapu, lapv;
+    double cxx_x, cxx_y, cxy_x, cxy_y, cyy_x, cyy_y;              // DI, LC (momentum)
+    double pxx_x, pxx_y, pxy_x, pxy_y, pyy_x, pyy_y;              // LC, CHL
+    double lapcxx, lapcxy, lapcyy, lapczz;                        // polymer diffusion
+};
+
+struct NodeState {
+    double ro, u, v, y;                 // y: node ordinate (Kolmogorov forcing)
+    double cxx, cxy, cyy, czz;          // conformation tensor
+    double pxx, pxy, pyy, pzz;          // psi (LC/CHL)
+};
+
+struct Rhs {
+    double ro, rou, rov, xx, xy, yy, zz;
+};
+
+// conf_transforms.F90:399-444, 2x2 eigen-decomposition; R column-major.
+__device__ __forceinline__ void eigens2(double a, double b, double d, double *l, double *R) {
+    if (fabs(b) <= 1.0e-16) {
+        l[0] = a; l[1] = d;
+        R[0] = 1.0; R[1] = 0.0; R[2] = 0.0; R[3] = 1.0;
+    } else {
+        double tr = a + d;
+        double det = a * d - b * b;
+        double temp = (0.25 * tr) * tr - det;
+        if (temp <= 1.0e-16) temp = 0.0;
+        temp = sqrt(temp);
+        l[0] = 0.5 * tr + temp;
+        l[1] = 0.5 * tr - temp;
+        R[0] = l[0] - d;
+        R[1] = b;
+        temp = sqrt(R[0] * R[0] + R[1] * R[1]);
+        R[0] = R[0] / temp;
+        R[1] = R[1] / temp;
+        R[2] = -R[1];
+        R[3] = R[0];
+    }
+}
+// gfortran inline matmul order: c(i,j) = a(i,1) b(1,j) + a(i,2) b(2,j)
+__device__ __forceinline__ void mm2(const double *a, const double *b, double *c) {
+    double t0 = a[0] * b[0] + a[2] * b[1];
+    double t1 = a[1] * b[0] + a[3] * b[1];
+    double t2 = a[0] * b[2] + a[2] * b[3];
+    double t3 = a[1] * b[2] + a[3] * b[3];
+    c[0] = t0; c[1] = t1; c[2] = t2; c[3] = t3;
+}
+__device__ __forceinline__ void tr2(const double *a, double *t) { t[0] = a[0]; t[1] = a[2]; t[2] = a[1]; t[3] = a[3]; }
+
+// log_conf_c_from_psi, conf_transforms.F90:133-169
+__device__ __forceinline__ void lc_c_from_psi(double pxx, double pxy, double pyy, double *cxx, double *cxy,
+                                              double *cyy) {
+    double L[2], R[4], RT[4], Lm[4], C[4];
+    eigens2(pxx, pxy, pyy, L, R);
+    tr2(R, RT);
+    Lm[0] = exp(L[0]); Lm[1] = 0.0; Lm[2] = 0.0; Lm[3] = exp(L[1]);
+    mm2(Lm, RT, C);
+    mm2(R, C, C);
+    *cxx = C[0]; *cxy = C[1]; *cyy = C[3];
+}
+// log_conf_psi_from_c, conf_transforms.F90:177-215
+__device__ __forceinline__ void lc_psi_from_c(double cxx, double cxy, double cyy, double *pxx, double *pxy,
+                                              double *pyy) {
+    double L[2], R[4], RT[4], Lm[4], P[4];
+    eigens2(cxx, cxy, cyy, L, R);
+    tr2(R, RT);
+    Lm[0] = log(L[0]); Lm[1] = 0.0; Lm[2] = 0.0; Lm[3] = log(L[1]);
+    mm2(Lm, RT, P);
+    mm2(R, P, P);
+    *pxx = P[0]; *pxy = P[1]; *pyy = P[3];
+}
+// cholesky_c_from_psi (sPTT), conf_transforms.F90:60-70
+__device__ __forceinline__ void chl_c_from_psi(double pxx, double pxy, double pyy, double *cxx, double *cxy,
+                                               double *cyy, double *czz) {
+    double e = exp(pxx);
+    *cxx = e * e;
+    *cxy = exp(pxx) * pxy;
+    *cyy = pxy * pxy + exp(2.0 * pyy);
+    *czz = 1.0;
+}
+// cholesky_psi_from_c (sPTT), conf_transforms.F90:109-121
+__device__ __forceinline__ void chl_psi_from_c(double cxx, double cxy, double cyy, double czz, double *pxx,
+                                               double *pxy, double *pyy, double *pzz) {
+    double xx = sqrt(cxx);
+    double xy = cxy / (xx);
+    double yy = (sqrt(cyy - xy * xy));
+    double zz = sqrt(czz);
+    *pxx = log(xx); *pxy = xy; *pyy = log(yy); *pzz = log(zz);
+}
+
+// calc_rhs_ro + calc_rhs_rovel, interior branch (rhs_di.F90:126-141,215-275; rhs.F90:220-286;
+// rhs_lc.F90:215-275).
+__device__ __forceinline__ void rhs_flow(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
+    const double w = 0.0;
+    double tmp_scal = (n.u * g.ro_x + n.v * g.ro_y) + w * 0.0;
+    double divvel = (g.u_x + g.v_y) + 0.0;
+    r.ro = -n.ro * divvel - tmp_scal;
+    double tsu = n.ro * ((n.u * g.u_x + n.v * g.u_y) + w * 0.0) - n.u * r.ro;
+    double tsv = n.ro * ((n.u * g.v_x + n.v * g.v_y) + w * 0.0) - n.v * r.ro;
+    double fvu = K.coef_solvent * g.lapu, fvv = K.coef_solvent * g.lapv;
+    if (K.form == SUNSET_FORM_CHL) {
+        double gcxx1 = (2.0 * exp(2.0 * n.pxx)) * g.pxx_x;
+        double gcxy1 = exp(n.pxx) * g.pxy_x + (n.pxy * exp(n.pxx)) * g.pxx_x;
+        double gcxy2 = exp(n.pxx) * g.pxy_y + (n.pxy * exp(n.pxx)) * g.pxx_y;
+        double gcyy2 = (2.0 * n.pxy) * g.pxy_y + (2.0 * exp(2.0 * n.pyy)) * g.pyy_y;
+        fvu = fvu + K.coef_polymeric * ((gcxx1 + gcxy2) + 0.0);
+        fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + 0.0);
+    } else if (K.form != SUNSET_FORM_NEWT) {
+        fvu = fvu + K.coef_polymeric * ((g.cxx_x + g.cxy_y) + 0.0);
+        fvv = fvv + K.coef_polymeric * ((g.cxy_x + g.cyy_y) + 0.0);
+    }
+    double bfu = n.ro * (K.grav0 + 0.0), bfv = n.ro * (K.grav1 + 0.0);
+    if (K.kolmo)
+        bfu = bfu + (((1.0 / K.Re) * cos(n.y)) * (1.0 + (K.Mdiff * K.beta) * K.Wi)) / (1.0 + K.Mdiff * K.Wi);
+    r.rou = ((-tsu - K.csq * g.ro_x) + bfu) + fvu;
+    r.rov = ((-tsv - K.csq * g.ro_y) + bfv) + fvv;
+}
+
+// calc_rhs_c, interior branch, rhs_di.F90:415-476 (sPTT / Oldroyd-B, 2-D).
+__device__ __forceinline__ void rhs_c_di(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
+    const double w = 0.0;
+    const double cxx = n.cxx, cxy = n.cxy, cyy = n.cyy, czz = n.czz;
+    double adxx = -((n.u * g.cxx_x + n.v * g.cxx_y) + w * 0.0);
+    double adxy = -((n.u * g.cxy_x + n.v * g.cxy_y) + w * 0.0);
+    double adyy = -((n.u * g.cyy_x + n.v * g.cyy_y) + w * 0.0);
+    double adzz = -((n.u * 0.0 + n.v * 0.0) + w * 0.0);
+    double g11 = g.u_x, g12 = g.u_y, g21 = g.v_x, g22 = g.v_y;
+    double ucxx = ((2.0 * g11) * cxx + (2.0 * g12) * cxy) + (2.0 * 0.0) * 0.0;
+    double ucxy = (((((g11 * cxy + g12 * cyy) + 0.0 * 0.0) + g21 * cxx) + g22 * cxy) + 0.0 * 0.0);
+    double ucyy = ((2.0 * g21) * cxy + (2.0 * g22) * cyy) + (2.0 * 0.0) * 0.0;
+    double uczz = ((2.0 * 0.0) * 0.0 + (2.0 * 0.0) * 0.0) + (2.0 * 0.0) * czz;
+    double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+    double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0), szz = fr * (czz - 1.0);
+    r.xx = ((adxx + ucxx) + sxx) + K.Mdiff * g.lapcxx;
+    r.xy = ((adxy + ucxy) + sxy) + K.Mdiff * g.lapcxy;
+    r.yy = ((adyy + ucyy) + syy) + K.Mdiff * g.lapcyy;
+    r.zz = ((adzz + uczz) + szz) + K.Mdiff * g.lapczz;
+}
+
+// calc_rhs_cholesky, interior branch, rhs.F90:424-550 (sPTT, 2-D).
+__device__ __forceinline__ void rhs_c_chl(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
+    const double w = 0.0;
+    double adxx = (n.u * g.pxx_x + n.v * g.pxx_y) + w * 0.0;
+    double adxy = (n.u * g.pxy_x + n.v * g.pxy_y) + w * 0.0;
+    double adyy = (n.u * g.pyy_x + n.v * g.pyy_y) + w * 0.0;
+    double lxx = exp(n.pxx), lxy = n.pxy, lyy = exp(n.pyy);
+    double g11 = g.u_x, g12 = g.u_y, g21 = g.v_x, g22 = g.v_y;
+    double ucxx = (g11 + (g12 * lxy) / lxx);
+    double ucxy = ((g22 * lxy + ((g12 * lyy) * lyy) / lxx) + g21 * lxx);
+    double ucyy = (g22 - (g12 * lxy) / lxx);
+    const double cxx = n.cxx, cxy = n.cxy, cyy = n.cyy, czz = n.czz;
+    double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+    double sxx = fr * (cxx - 1.0) + K.Mdiff * g.lapcxx;
+    double sxy = fr * cxy + K.Mdiff * g.lapcxy;
+    double syy = fr * (cyy - 1.0) + K.Mdiff * g.lapcyy;
+    double csxx = ((0.5 * sxx) / lxx) / lxx;
+    double csxy = sxy / lxx - ((0.5 * sxx) * lxy) / (lxx * lxx);
+    double csyy = (((0.5 * syy) / lyy) / lyy - (sxy * lxy) / ((lxx * lyy) * lyy)) +
+                  (((0.5 * sxx) * lxy) * lxy) / ((lyy * lyy) * (lxx * lxx));
+    r.xx = (-adxx + ucxx) + csxx;
+    r.xy = (-adxy + ucxy) + csxy;
+    r.yy = (-adyy + ucyy) + csyy;
+    r.zz = 0.0;
+}
+
+// calc_rhs_logconf, interior branch, rhs_lc.F90:414-559 (sPTT, 2-D).  `first` is the
+// reference's itime==1 .and. iRKstep==1 special case (rhs_lc.F90:503).
+__device__ __forceinline__ void rhs_c_lc(const StepConsts &K, const NodeState &n, const Grads &g, bool first,
+                                         Rhs &r) {
+    const double w = 0.0;
+    double adxx = -((n.u * g.pxx_x + n.v * g.pxx_y) + w * 0.0);
+    double adxy = -((n.u * g.pxy_x + n.v * g.pxy_y) + w * 0.0);
+    double adyy = -((n.u * g.pyy_x + n.v * g.pyy_y) + w * 0.0);
+    double Lv[2], R[4], RT[4], G[4], M[4], B[4], Om[4], P[4], Ci[4], T[4];
+    eigens2(n.pxx, n.pxy, n.pyy, Lv, R);
+    Lv[0] = exp(Lv[0]);
+    Lv[1] = exp(Lv[1]);
+    tr2(R, RT);
+    double tr_c = Lv[0] + Lv[1];
+    G[0] = g.u_x; G[2] = g.u_y; G[1] = g.v_x; G[3] = g.v_y;
+    mm2(G, R, T);
+    mm2(RT, T, M);
+    double om = (Lv[1] * M[2] + Lv[0] * M[1]);
+    if (fabs(Lv[1] - Lv[0]) <= 1.0e-30) om = 0.0;
+    else om = om / (Lv[1] - Lv[0]);
+    M[2] = 0.0; M[1] = 0.0;
+    mm2(M, RT, T);
+    mm2(R, T, B);
+    M[0] = 0.0; M[1] = -om; M[2] = om; M[3] = 0.0;
+    mm2(M, RT, T);
+    mm2(R, T, Om);
+    if (first) {
+        Om[0] = Om[1] = Om[2] = Om[3] = 0.0;
+        double GT[4];
+        tr2(G, GT);
+        for (int c = 0; c < 4; c++) B[c] = 0.5 * (G[c] + GT[c]);
+    }
+    P[0] = n.pxx; P[2] = n.pxy; P[1] = n.pxy; P[3] = n.pyy;
+    double OP[4], PO[4], UC[4];
+    mm2(Om, P, OP);
+    mm2(P, Om, PO);
+    for (int c = 0; c < 4; c++) UC[c] = (OP[c] - PO[c]) + 2.0 * B[c];
+    double fR = ((1.0 - 2.0 * K.epsPTT) + K.epsPTT * tr_c);
+    Ci[0] = fR / Lv[0] - fR; Ci[1] = 0.0; Ci[2] = 0.0; Ci[3] = fR / Lv[1] - fR;
+    mm2(Ci, RT, T);
+    mm2(R, T, T);
+    r.xx = (adxx + UC[0]) + T[0] / K.lambda;
+    r.xy = (adxy + UC[2]) + T[2] / K.lambda;
+    r.yy = (adyy + UC[3]) + T[3] / K.lambda;
+    r.zz = 0.0;
+}
+
+}  // namespace sunset

@@ -1,0 +1,886 @@
+// step.cu -- the FP64 time step: fused RK stage kernels, filter + mass correction,
+// finalisation, PID time-step control, and the single-operator kernels of the C-ABI.
+//
+// One RK stage is one kernel: a thread owns a node, a warp owns a slice of 32 nodes, and
+// the warp streams the slice's links (index + gradient/Laplacian weights, one coalesced
+// access per link and array) while gathering the neighbours' fields.  The node's stencil
+// sums feed the right-hand side in registers, which feeds the low-storage RK update
+// (step.F90:291-343), which writes the next state and its derived fields (velocity,
+// conformation tensor) into the other state buffer.  Ghost links carry the parent's
+// index and a reflection code, so no mirror copy (mirror_boundaries.F90:263-352) or
+// halo exchange runs between stages.
+//
+// Sums run over each node's links in the reference's order, in the reference's sum form
+// (sum_k w_k phi_j - phi_i sum_k w_k, derivatives.F90:36-46), and the file is built with
+// -fmad=false, so the FP64 path computes what the reference computes operation for
+// operation; only the libm functions (exp, log, cos) may differ from glibc in the last bit.
+#include "internal.cuh"
+#include "physics.cuh"
+
+namespace sunset {
+
+namespace {
+
+__constant__ StepConsts cK;
+
+struct StageArgs {
+    const long long *slice_ptr;
+    const int *slice_ws, *slice_w;
+    const int *lidx;
+    const double *wx, *wy, *wl, *wh;
+    const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
+    Fields in, out;
+    double *reg[7], *eacc[7], *rhs[7];
+    DevScalars *sc;
+    double *partials;
+    int stage;  // 0..3; 4 = rhs only
+};
+
+__device__ __forceinline__ double fetch(const double *p, int j) { return __ldg(p + j); }
+
+// Reflection codes of a ghost link: 1 -> vrelation 2 (x mirror: u and the xy component
+// change sign), 2 -> vrelation 3 (y mirror: v and xy), 3 -> vrelation 4 (u and v).
+__device__ __forceinline__ void reflect(int code, double &uj, double &vj, double &xyj) {
+    if (code == 1 || code == 3) uj = -uj;
+    if (code == 2 || code == 3) vj = -vj;
+    if (code == 1 || code == 2) xyj = -xyj;
+}
+
+template <int FORM>
+__device__ __forceinline__ void gather_stage(const StageArgs &A, int i, Grads &g) {
+    const long long base = A.slice_ptr[i >> 5] + (i & 31);
+    const int ws = A.slice_ws[i >> 5];
+    const Fields &F = A.in;
+    double s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
+    double s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
+    double s_pxx_x = 0, s_pxx_y = 0, s_pxy_x = 0, s_pxy_y = 0, s_pyy_x = 0, s_pyy_y = 0;
+    double s_lxx = 0, s_lxy = 0, s_lyy = 0;
+    const bool mir = cK.has_mirrors;
+    const bool mdiff = cK.mdiff_on;
+    const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
+    for (int k = 0; k < ws; k++) {
+        const long long o = base + (long long)k * kSlice;
+        const int lk = __ldg(A.lidx + o);
+        const int j = lk & kLinkMask;
+        const double wxk = __ldg(A.wx + o), wyk = __ldg(A.wy + o), wlk = __ldg(A.wl + o);
+        double roj = fetch(F.ro, j), uj = fetch(F.u, j), vj = fetch(F.v, j);
+        double dxy = 0.0;
+        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) dxy = fetch(F.c[1], j);
+        double pxy = 0.0;
+        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) pxy = fetch(F.q[1], j);
+        if (mir) {
+            int code = (unsigned)lk >> 30;
+            double t = pxy;
+            reflect(code, uj, vj, dxy);
+            if (code == 1 || code == 2) t = -t;
+            pxy = t;
+        }
+        s_ro_x = s_ro_x + roj * wxk;
+        s_ro_y = s_ro_y + roj * wyk;
+        s_u_x = s_u_x + uj * wxk;
+        s_u_y = s_u_y + uj * wyk;
+        s_lu = s_lu + uj * wlk;
+        s_v_x = s_v_x + vj * wxk;
+        s_v_y = s_v_y + vj * wyk;
+        s_lv = s_lv + vj * wlk;
+        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
+            double cxxj = fetch(F.c[0], j), cyyj = fetch(F.c[2], j);
+            s_cxx_x = s_cxx_x + cxxj * wxk;
+            if (full) s_cxx_y = s_cxx_y + cxxj * wyk;
+            s_cxy_x = s_cxy_x + dxy * wxk;
+            s_cxy_y = s_cxy_y + dxy * wyk;
+            if (full) s_cyy_x = s_cyy_x + cyyj * wxk;
+            s_cyy_y = s_cyy_y + cyyj * wyk;
+            if (FORM == SUNSET_FORM_DI && mdiff) {
+                s_lxx = s_lxx + cxxj * wlk;
+                s_lxy = s_lxy + dxy * wlk;
+                s_lyy = s_lyy + cyyj * wlk;
+            }
+        }
+        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {
+            double pxxj = fetch(F.q[0], j), pyyj = fetch(F.q[2], j);
+            s_pxx_x = s_pxx_x + pxxj * wxk;
+            s_pxx_y = s_pxx_y + pxxj * wyk;
+            s_pxy_x = s_pxy_x + pxy * wxk;
+            s_pxy_y = s_pxy_y + pxy * wyk;
+            s_pyy_x = s_pyy_x + pyyj * wxk;
+            s_pyy_y = s_pyy_y + pyyj * wyk;
+        }
+        if (FORM == SUNSET_FORM_CHL && mdiff) {
+            double cxxj = fetch(F.c[0], j), cyyj = fetch(F.c[2], j), cxyj = fetch(F.c[1], j);
+            if (mir) {
+                int code = (unsigned)lk >> 30;
+                if (code == 1 || code == 2) cxyj = -cxyj;
+            }
+            s_lxx = s_lxx + cxxj * wlk;
+            s_lxy = s_lxy + cxyj * wlk;
+            s_lyy = s_lyy + cyyj * wlk;
+        }
+    }
+    if (i >= cK.npfb) return;
+    const double gx = A.gsx[i], gy = A.gsy[i], ls = A.lsum[i];
+    const double roi = F.ro[i], ui = F.u[i], vi = F.v[i];
+    g.ro_x = s_ro_x - roi * gx;
+    g.ro_y = s_ro_y - roi * gy;
+    g.u_x = s_u_x - ui * gx;
+    g.u_y = s_u_y - ui * gy;
+    g.lapu = s_lu - ui * ls;
+    g.v_x = s_v_x - vi * gx;
+    g.v_y = s_v_y - vi * gy;
+    g.lapv = s_lv - vi * ls;
+    g.cxx_x = g.cxx_y = g.cxy_x = g.cxy_y = g.cyy_x = g.cyy_y = 0.0;
+    g.pxx_x = g.pxx_y = g.pxy_x = g.pxy_y = g.pyy_x = g.pyy_y = 0.0;
+    g.lapcxx = g.lapcxy = g.lapcyy = g.lapczz = 0.0;
+    if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
+        const double cxx = F.c[0][i], cxy = F.c[1][i], cyy = F.c[2][i];
+        g.cxx_x = s_cxx_x - cxx * gx;
+        if (full) g.cxx_y = s_cxx_y - cxx * gy;
+        g.cxy_x = s_cxy_x - cxy * gx;
+        g.cxy_y = s_cxy_y - cxy * gy;
+        if (full) g.cyy_x = s_cyy_x - cyy * gx;
+        g.cyy_y = s_cyy_y - cyy * gy;
+        if (FORM == SUNSET_FORM_DI && mdiff) {
+            g.lapcxx = s_lxx - cxx * ls;
+            g.lapcxy = s_lxy - cxy * ls;
+            g.lapcyy = s_lyy - cyy * ls;
+        }
+    }
+    if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {
+        const double pxx = F.q[0][i], pxy = F.q[1][i], pyy = F.q[2][i];
+        g.pxx_x = s_pxx_x - pxx * gx;
+        g.pxx_y = s_pxx_y - pxx * gy;
+        g.pxy_x = s_pxy_x - pxy * gx;
+        g.pxy_y = s_pxy_y - pxy * gy;
+        g.pyy_x = s_pyy_x - pyy * gx;
+        g.pyy_y = s_pyy_y - pyy * gy;
+    }
+    if (FORM == SUNSET_FORM_CHL && mdiff) {
+        g.lapcxx = s_lxx - F.c[0][i] * ls;
+        g.lapcxy = s_lxy - F.c[1][i] * ls;
+        g.lapcyy = s_lyy - F.c[2][i] * ls;
+    }
+}
+
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+__device__ __forceinline__ void block_max_bits(unsigned long long v, unsigned long long *dst) {
+    __shared__ unsigned long long sm[32];
+    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_down_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_down_sync(0xffffffffu, v, o);
+            v = t > v ? t : v;
+        }
+        if (lane == 0 && v) atomicMax(dst, v);
+    }
+}
+__device__ __forceinline__ void block_min_bits(unsigned long long v, unsigned long long *dst) {
+    __shared__ unsigned long long sm2[32];
+    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_down_sync(0xffffffffu, v, o);
+        v = t < v ? t : v;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm2[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sm2[lane] : ~0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_down_sync(0xffffffffu, v, o);
+            v = t < v ? t : v;
+        }
+        if (lane == 0) atomicMin(dst, v);
+    }
+}
+
+// One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).
+template <int FORM>
+__global__ void __launch_bounds__(128) k_stage(StageArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stage = A.stage;
+    if (stage == 0 && i == 0) {
+        A.sc->cfl_bits = 0x7ff0000000000000ull;
+        A.sc->par_bits = 0x7ff0000000000000ull;
+    }
+    Grads g;
+    bool active = (i >> 5) < cK.nslices;
+    if (active) gather_stage<FORM>(A, i, g);
+    active = active && i < cK.npfb;
+    unsigned long long emax_bits = 0;
+    if (active) {
+        const Fields &F = A.in;
+        NodeState n;
+        n.ro = F.ro[i]; n.u = F.u[i]; n.v = F.v[i]; n.y = A.py_node[i];
+        n.cxx = F.c[0][i]; n.cxy = F.c[1][i]; n.cyy = F.c[2][i]; n.czz = F.c[3][i];
+        n.pxx = F.q[0][i]; n.pxy = F.q[1][i]; n.pyy = F.q[2][i]; n.pzz = F.q[3][i];
+        Rhs r;
+        rhs_flow(cK, n, g, r);
+        if (FORM == SUNSET_FORM_DI) rhs_c_di(cK, n, g, r);
+        else if (FORM == SUNSET_FORM_CHL) rhs_c_chl(cK, n, g, r);
+        else if (FORM == SUNSET_FORM_LC) {
+            const bool first = (A.sc->itime == 1) && (stage == 0);
+            rhs_c_lc(cK, n, g, first, r);
+        } else { r.xx = r.xy = r.yy = r.zz = 0.0; }
+        const double rr[7] = {r.ro, r.rou, r.rov, r.xx, r.xy, r.yy, r.zz};
+        if (stage == 4) {
+            for (int f = 0; f < 7; f++) A.rhs[f][i] = rr[f];
+        } else {
+            const double U[7] = {F.ro[i], F.rou[i], F.rov[i], F.q[0][i], F.q[1][i], F.q[2][i], F.q[3][i]};
+            const double dt = A.sc->dt;
+            const double a[3] = {SUNSET_RK_A21, SUNSET_RK_A32, SUNSET_RK_A43};
+            const double b[4] = {SUNSET_RK_B1, SUNSET_RK_B2, SUNSET_RK_B3, SUNSET_RK_B4};
+            const double bh[4] = {SUNSET_RK_BH1, SUNSET_RK_BH2, SUNSET_RK_BH3, SUNSET_RK_BH4};
+            const double RKb = dt * b[stage], RKbmbh = dt * (b[stage] - bh[stage]);
+            const int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+            double Un[7];
+            if (stage < 3) {
+                const double RKa = dt * a[stage];
+                for (int f = 0; f < nf; f++) {
+                    double S = (stage == 0) ? U[f] : A.reg[f][i];
+                    double E = (stage == 0) ? 0.0 : A.eacc[f][i];
+                    Un[f] = S + RKa * rr[f];
+                    A.reg[f][i] = S + RKb * rr[f];
+                    A.eacc[f][i] = E + RKbmbh * rr[f];
+                }
+            } else {
+                const double norms[7] = {cK.ero_norm, cK.erou_norm, cK.erou_norm, cK.exx_norm,
+                                         cK.exx_norm, cK.exx_norm, cK.exx_norm};
+                double en = 0.0;
+                for (int f = 0; f < nf; f++) {
+                    Un[f] = A.reg[f][i] + RKb * rr[f];
+                    double E = A.eacc[f][i] + RKbmbh * rr[f];
+                    double t = fabs(E) * norms[f];
+                    en = (t > en) ? t : en;
+                    if (t != t) en = t;
+                }
+                emax_bits = dbits(en);
+            }
+            for (int f = nf; f < 7; f++) Un[f] = U[f];
+            const Fields &O = A.out;
+            O.ro[i] = Un[0]; O.rou[i] = Un[1]; O.rov[i] = Un[2];
+            if (FORM != SUNSET_FORM_NEWT) {
+                O.q[0][i] = Un[3]; O.q[1][i] = Un[4]; O.q[2][i] = Un[5]; O.q[3][i] = Un[6];
+            }
+            if (stage < 3) {  // get_velocity_from_momentum, get_c_from_psi (step.F90:514-567)
+                double ooro = 1.0 / Un[0];
+                O.u[i] = Un[1] * ooro;
+                O.v[i] = Un[2] * ooro;
+                if (FORM == SUNSET_FORM_LC) {
+                    double cxx, cxy, cyy;
+                    lc_c_from_psi(Un[3], Un[4], Un[5], &cxx, &cxy, &cyy);
+                    O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = F.c[3][i];
+                } else if (FORM == SUNSET_FORM_CHL) {
+                    double cxx, cxy, cyy, czz;
+                    chl_c_from_psi(Un[3], Un[4], Un[5], &cxx, &cxy, &cyy, &czz);
+                    O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = czz;
+                }
+            }
+        }
+    }
+    if (stage == 3) block_max_bits(emax_bits, &A.sc->emax_bits);
+}
+
+// filter_variables (rhs_di.F90:667-720; rhs.F90:792-900; rhs_lc.F90:818-893): the
+// hyperviscous filter of each evolved field plus the mass-correction partial sums.
+template <int FORM>
+__global__ void __launch_bounds__(128) k_filter(StageArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    double part = 0.0;
+    if ((i >> 5) < cK.nslices) {
+        const long long base = A.slice_ptr[i >> 5] + (i & 31);
+        const int w = A.slice_w[i >> 5];
+        const Fields &F = A.in;
+        const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
+        double t[7] = {0, 0, 0, 0, 0, 0, 0};
+        const bool mir = cK.has_mirrors;
+        for (int k = 0; k < w; k++) {
+            const long long o = base + (long long)k * kSlice;
+            const int lk = __ldg(A.lidx + o);
+            const int j = lk & kLinkMask;
+            const double whk = __ldg(A.wh + o);
+            double v[7];
+#pragma unroll
+            for (int f = 0; f < 7; f++)
+                if (f < nf) v[f] = fetch(src[f], j);
+            if (mir) {
+                int code = (unsigned)lk >> 30;
+                reflect(code, v[1], v[2], v[4]);
+            }
+#pragma unroll
+            for (int f = 0; f < 7; f++)
+                if (f < nf) t[f] = t[f] + v[f] * whk;
+        }
+        if (i < cK.npfb) {
+            const double hs = A.hsum[i];
+            double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
+#pragma unroll
+            for (int f = 0; f < 7; f++) {
+                if (f < nf) {
+                    double p = src[f][i];
+                    dst[f][i] = p + (t[f] - p * hs);
+                } else if (f >= 3 && FORM != SUNSET_FORM_NEWT) {
+                    dst[f][i] = src[f][i];
+                }
+            }
+            double rof = src[0][i] + (t[0] - src[0][i] * hs);
+            part = (rof - cK.rho_char) * A.vol[i];
+        }
+    }
+    // deterministic two-level sum: fixed tree in the block, fixed order over blocks
+    __shared__ double sm[128];
+    sm[threadIdx.x] = part;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+        __syncthreads();
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        A.partials[blockIdx.x] = sm[0];
+        __threadfence();
+        unsigned int prev = atomicAdd(&A.sc->done_ctr, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc = acc + ((volatile double *)A.partials)[b];
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            A.sc->dro = cK.mcorr ? sm[0] / A.sc->tv : 0.0;
+            A.sc->done_ctr = 0;
+        }
+    }
+}
+
+// End of step: mass correction, velocity and c from the filtered state
+// (filter_variables + get_velocity_from_momentum + get_c_from_psi) and the step's scalar
+// bookkeeping (error-norm history, time, itime).
+template <int FORM>
+__global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dro = A.sc->dro;
+    if (i < cK.npfb) {
+        const Fields &F = A.out;
+        double ro = F.ro[i];
+        if (cK.mcorr) ro = ro - dro;
+        F.ro[i] = ro;
+        double ooro = 1.0 / ro;
+        F.u[i] = F.rou[i] * ooro;
+        F.v[i] = F.rov[i] * ooro;
+        if (FORM == SUNSET_FORM_LC) {
+            double cxx, cxy, cyy;
+            lc_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy);
+            F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy;
+        } else if (FORM == SUNSET_FORM_CHL) {
+            double cxx, cxy, cyy, czz;
+            chl_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy, &czz);
+            F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy; F.c[3][i] = czz;
+        }
+    }
+    if (advance && i == 0) {
+        DevScalars *sc = A.sc;
+        double e = __longlong_as_double((long long)sc->emax_bits);
+        double emax = (e > 1.0e-16) ? e : 1.0e-16;
+        if (!(e == e) || isinf(e)) sc->err = 1;
+        sc->emax_nm1 = sc->emax_n;
+        sc->emax_n = sc->emax_np1;
+        sc->emax_np1 = emax;
+        sc->emax_bits = 0ull;
+        sc->time = sc->time + sc->dt;
+        sc->itime = sc->itime + 1;
+    }
+}
+
+// set_tstep (step.F90:569-622) over the current state: block minima of s/(|u|+c) and
+// s^2 rho/mu, folded into dt_cfl and dt_parabolic by k_pid / the host.
+__global__ void __launch_bounds__(128) k_tstep(const double *u, const double *v, const double *ro, const double *sp,
+                                                const int *ntype, int npfb, DevScalars *sc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double tc = 1.0e10, tp = 1.0e10;
+    if (i < npfb) {
+        double umax = sqrt((u[i] * u[i] + v[i] * v[i]) + 0.0 * 0.0);
+        double uplusc = umax + cK.c_sound;
+        tc = (ntype[i] == 2) ? (0.8 * sp[i]) / uplusc : sp[i] / uplusc;
+        tp = ((sp[i] * sp[i]) * ro[i]) / cK.visc_total;
+    }
+    block_min_bits(dbits(tc), &sc->cfl_bits);
+    block_min_bits(dbits(tp), &sc->par_bits);
+}
+
+// set_tstep_PID, step.F90:624-682.
+__global__ void k_pid(DevScalars *sc) {
+    double dcfl = __longlong_as_double((long long)sc->cfl_bits);
+    double dvisc = __longlong_as_double((long long)sc->par_bits);
+    sc->dt_cfl = (1.0 * dcfl) * cK.L_char;
+    sc->dt_par = (((2.0 / 3.0) * dvisc) * cK.L_char) * cK.L_char;
+    double facA = (0.49 / 2.0) * log(1.0e-5 / sc->emax_np1);
+    double facB = (0.34 / 2.0) * log(sc->emax_n / 1.0e-5);
+    double facC = (0.1 / 2.0) * log(1.0e-5 / sc->emax_nm1);
+    double dtfactor = 0.9 * exp((facA + facB) + facC);
+    dtfactor = (0.5 > dtfactor) ? 0.5 : dtfactor;
+    dtfactor = (1.02 < dtfactor) ? 1.02 : dtfactor;
+    double dt = sc->dt * dtfactor;
+    double dt_max = (sc->dt_cfl < sc->dt_par) ? sc->dt_cfl : sc->dt_par;
+    if (dt > dt_max) dt = dt_max;
+    sc->dt = dt;
+    sc->cfl_bits = 0x7ff0000000000000ull;
+    sc->par_bits = 0x7ff0000000000000ull;
+}
+
+__global__ void k_tstep_fold(DevScalars *sc) {
+    double dcfl = __longlong_as_double((long long)sc->cfl_bits);
+    double dvisc = __longlong_as_double((long long)sc->par_bits);
+    sc->dt_cfl = (1.0 * dcfl) * cK.L_char;
+    sc->dt_par = (((2.0 / 3.0) * dvisc) * cK.L_char) * cK.L_char;
+}
+
+// ---------------------------------------------------------------------------------------
+// Single operators of the C-ABI (derivatives.F90), on a field in internal order.
+// ---------------------------------------------------------------------------------------
+__global__ void k_op_grad_lap(StageArgs A, const double *phi, double *gx, double *gy, double *lap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((i >> 5) >= cK.nslices) return;
+    const long long base = A.slice_ptr[i >> 5] + (i & 31);
+    const int ws = A.slice_ws[i >> 5];
+    double sx = 0.0, sy = 0.0, sl = 0.0;
+    for (int k = 0; k < ws; k++) {
+        const long long o = base + (long long)k * kSlice;
+        const int j = __ldg(A.lidx + o) & kLinkMask;
+        const double pj = phi[j];
+        sx = sx + pj * __ldg(A.wx + o);
+        sy = sy + pj * __ldg(A.wy + o);
+        sl = sl + pj * __ldg(A.wl + o);
+    }
+    if (i >= cK.npfb) return;
+    const double p = phi[i];
+    if (gx) gx[i] = sx - p * A.gsx[i];
+    if (gy) gy[i] = sy - p * A.gsy[i];
+    if (lap) lap[i] = sl - p * A.lsum[i];
+}
+
+__global__ void k_op_filter(StageArgs A, const double *phi, double *out, int term_only) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((i >> 5) >= cK.nslices) return;
+    const long long base = A.slice_ptr[i >> 5] + (i & 31);
+    const int w = A.slice_w[i >> 5];
+    double t = 0.0;
+    for (int k = 0; k < w; k++) {
+        const long long o = base + (long long)k * kSlice;
+        const int j = __ldg(A.lidx + o) & kLinkMask;
+        t = t + phi[j] * __ldg(A.wh + o);
+    }
+    if (i >= cK.npfb) return;
+    const double p = phi[i];
+    out[i] = term_only ? (t - p * A.hsum[i]) : p + (t - p * A.hsum[i]);
+}
+
+// initial_solution (setup_flow.F90:24-173) on internal-order device arrays.
+__global__ void k_set_state(int npfb, int form, const double *ro, const double *u, const double *v,
+                            const double *cxx, const double *cxy, const double *cyy, const double *czz, Fields F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npfb) return;
+    double r = ro[i];
+    F.ro[i] = r;
+    F.u[i] = u[i];
+    F.v[i] = v[i];
+    F.rou[i] = r * u[i];
+    F.rov[i] = r * v[i];
+    double c0 = cxx[i], c1 = cxy[i], c2 = cyy[i], c3 = czz[i];
+    if (form == SUNSET_FORM_LC) {
+        double p0, p1, p2;
+        lc_psi_from_c(c0, c1, c2, &p0, &p1, &p2);
+        F.q[0][i] = p0; F.q[1][i] = p1; F.q[2][i] = p2; F.q[3][i] = 0.0;
+        lc_c_from_psi(p0, p1, p2, &c0, &c1, &c2);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
+    } else if (form == SUNSET_FORM_CHL) {
+        double p0, p1, p2, p3;
+        chl_psi_from_c(c0, c1, c2, c3, &p0, &p1, &p2, &p3);
+        F.q[0][i] = p0; F.q[1][i] = p1; F.q[2][i] = p2; F.q[3][i] = p3;
+        chl_c_from_psi(p0, p1, p2, &c0, &c1, &c2, &c3);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
+    } else {
+        F.q[0][i] = c0; F.q[1][i] = c1; F.q[2][i] = c2; F.q[3][i] = c3;
+    }
+}
+
+// Conservative state given directly (ro, rou, rov, q0..q3), derived fields recomputed
+// as get_velocity_from_momentum / get_c_from_psi do.
+__global__ void k_set_conservative(int npfb, int form, const double *ro, const double *rou, const double *rov,
+                                   const double *q0, const double *q1, const double *q2, const double *q3, Fields F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npfb) return;
+    F.ro[i] = ro[i]; F.rou[i] = rou[i]; F.rov[i] = rov[i];
+    F.q[0][i] = q0[i]; F.q[1][i] = q1[i]; F.q[2][i] = q2[i]; F.q[3][i] = q3[i];
+    double ooro = 1.0 / ro[i];
+    F.u[i] = rou[i] * ooro;
+    F.v[i] = rov[i] * ooro;
+    if (form == SUNSET_FORM_LC) {
+        double c0, c1, c2;
+        lc_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = 1.0;
+    } else if (form == SUNSET_FORM_CHL) {
+        double c0, c1, c2, c3;
+        chl_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2, &c3);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
+    }
+}
+
+__global__ void k_ke_mass(int npfb, Fields F, const double *vol, double *partials) {
+    __shared__ double s1[128], s2[128];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0, m = 0.0;
+    if (i < npfb) {
+        ke = ((0.5 * F.ro[i]) * (F.u[i] * F.u[i] + F.v[i] * F.v[i])) * vol[i];
+        m = F.ro[i] * vol[i];
+    }
+    s1[threadIdx.x] = ke;
+    s2[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+            s2[threadIdx.x] = s2[threadIdx.x] + s2[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = s1[0];
+        partials[2 * blockIdx.x + 1] = s2[0];
+    }
+}
+
+__global__ void k_sum_vol(int npfb, const double *vol, double *partials) {
+    __shared__ double s1[128];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    s1[threadIdx.x] = i < npfb ? vol[i] : 0.0;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = s1[0];
+}
+
+__global__ void k_fold_partials(const double *partials, int n, double *out) {
+    __shared__ double sm[128];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) acc = acc + partials[b];
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sm[0];
+}
+
+StageArgs make_args(Handle *H, int from, int stage) {
+    StageArgs A{};
+    A.slice_ptr = H->slice_ptr;
+    A.slice_ws = H->slice_ws;
+    A.slice_w = H->slice_w;
+    A.lidx = H->lidx;
+    A.wx = H->wx; A.wy = H->wy; A.wl = H->wl; A.wh = H->wh;
+    A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum; A.hsum = H->hsum; A.vol = H->vol;
+    A.py_node = H->py;
+    A.in = H->buf[from];
+    A.out = H->buf[from ^ 1];
+    for (int f = 0; f < 7; f++) { A.reg[f] = H->reg[f]; A.eacc[f] = H->eacc[f]; A.rhs[f] = H->rhs[f]; }
+    A.sc = H->dsc;
+    A.partials = H->partials;
+    A.stage = stage;
+    return A;
+}
+
+int upload_consts(Handle *H) {
+    const SunsetConfig &c = H->cfg;
+    StepConsts K{};
+    K.npfb = H->npfb;
+    K.nslices = H->nslices;
+    K.form = c.form;
+    K.fenep = c.fenep;
+    K.mcorr = c.mcorr;
+    K.kolmo = c.kolmogorov_forcing < 0 ? (c.form == SUNSET_FORM_CHL) : c.kolmogorov_forcing;
+    K.di_full = c.di_full_gradients;
+    K.has_mirrors = H->has_mirrors;
+    K.mdiff_on = c.Mdiff != 0.0;
+    double t = c.U_char / c.Ma;
+    K.csq = t * t;
+    K.c_sound = sqrt(K.csq);
+    K.rho_char = 1.0;
+    K.visc_total = K.rho_char * c.U_char * c.L_char / c.Re;
+    K.coef_solvent = c.beta * K.visc_total;
+    K.lambda = c.Wi * c.L_char / c.U_char;
+    K.coef_polymeric = ((1.0 - c.beta) * K.visc_total) / K.lambda;
+    K.epsPTT = c.epsPTT;
+    K.fenep_l2 = c.fenep_l2;
+    K.Mdiff = c.Mdiff;
+    K.Re = c.Re;
+    K.Wi = c.Wi;
+    K.beta = c.beta;
+    K.L_char = c.L_char;
+    K.grav0 = c.grav[0];
+    K.grav1 = c.grav[1];
+    K.ero_norm = 1.0 / 1.0;
+    K.erou_norm = 1.0 / (1.0 * c.U_char);
+    K.exx_norm = 1.0 / (1.0);
+    SUNSET_CUDA(H, cudaMemcpyToSymbolAsync(cK, &K, sizeof(K), 0, cudaMemcpyHostToDevice, H->stream));
+    return 0;
+}
+
+template <int FORM>
+void launch_step_kernels(Handle *H, int from, int pid) {
+    const int TB = 128;
+    const int nthr = H->nslices * kSlice;
+    const int nblk = (nthr + TB - 1) / TB;
+    cudaStream_t st = H->stream;
+    if (pid) k_pid<<<1, 1, 0, st>>>(H->dsc);
+    int b = from;
+    for (int s = 0; s < 4; s++) {
+        StageArgs A = make_args(H, b, s);
+        k_stage<FORM><<<nblk, TB, 0, st>>>(A);
+        b ^= 1;
+    }
+    StageArgs F = make_args(H, b, 5);
+    k_filter<FORM><<<nblk, TB, 0, st>>>(F);
+    b ^= 1;
+    StageArgs Z = make_args(H, b ^ 1, 5);  // in = filter input, out = filtered buffer
+    const int fb = (H->npfb + TB - 1) / TB;
+    k_finalize<FORM><<<fb, TB, 0, st>>>(Z, 1);
+    k_tstep<<<fb, TB, 0, st>>>(H->buf[b].u, H->buf[b].v, H->buf[b].ro, H->sp, H->ntype, H->npfb, H->dsc);
+}
+
+void launch_step(Handle *H, int from, int pid) {
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI: launch_step_kernels<SUNSET_FORM_DI>(H, from, pid); break;
+    case SUNSET_FORM_CHL: launch_step_kernels<SUNSET_FORM_CHL>(H, from, pid); break;
+    case SUNSET_FORM_LC: launch_step_kernels<SUNSET_FORM_LC>(H, from, pid); break;
+    default: launch_step_kernels<SUNSET_FORM_NEWT>(H, from, pid); break;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+int state_alloc(Handle *H) {
+    if (H->dsc) return 0;
+    const int n = H->npfb;
+    for (int b = 0; b < 2; b++) {
+        Fields &F = H->buf[b];
+        if (dalloc(H, &F.ro, n) || dalloc(H, &F.rou, n) || dalloc(H, &F.rov, n) || dalloc(H, &F.u, n) ||
+            dalloc(H, &F.v, n))
+            return SUNSET_ERR_NOMEM;
+        for (int k = 0; k < 4; k++)
+            if (dalloc(H, &F.q[k], n)) return SUNSET_ERR_NOMEM;
+        if (H->cfg.form == SUNSET_FORM_DI) {
+            for (int k = 0; k < 4; k++) F.c[k] = F.q[k];
+        } else {
+            for (int k = 0; k < 4; k++)
+                if (dalloc(H, &F.c[k], n)) return SUNSET_ERR_NOMEM;
+        }
+    }
+    for (int f = 0; f < 7; f++)
+        if (dalloc(H, &H->reg[f], n) || dalloc(H, &H->eacc[f], n) || dalloc(H, &H->rhs[f], n)) return SUNSET_ERR_NOMEM;
+    const int nthr = H->nslices * kSlice;
+    H->npart = (nthr + 127) / 128 + 1;
+    if (dalloc(H, &H->partials, 2 * (size_t)H->npart + 16) || dalloc(H, &H->dsc, 1) || dalloc(H, &H->tmpd, 4 * (size_t)n))
+        return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->dsc, 0, sizeof(DevScalars), H->stream));
+    return 0;
+}
+
+static int init_scalars(Handle *H) {
+    DevScalars s{};
+    s.dt = 1.0e-6;
+    s.time = 0.0;
+    s.emax_nm1 = s.emax_n = s.emax_np1 = 1.0e-5;  // pid_tol, setup_flow.F90:149-152
+    s.cfl_bits = 0x7ff0000000000000ull;
+    s.par_bits = 0x7ff0000000000000ull;
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, H->stream));
+    // sum of volumes (constant), same tree as the mass correction
+    const int TB = 128, nb = (H->npfb + TB - 1) / TB;
+    k_sum_vol<<<nb, TB, 0, H->stream>>>(H->npfb, H->vol, H->partials);
+    k_fold_partials<<<1, 128, 0, H->stream>>>(H->partials, nb, &H->dsc->tv);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int state_set_device(Handle *H, const double *ro, const double *u, const double *v, const double *cxx,
+                     const double *cxy, const double *cyy, const double *czz) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    H->cur = 0;
+    k_set_state<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, ro, u, v, cxx, cxy, cyy, czz,
+                                                              H->buf[0]);
+    SUNSET_CUDA(H, cudaGetLastError());
+    rc = init_scalars(H);
+    if (rc) return rc;
+    return set_tstep_device(H);
+}
+
+int state_set_conservative_device(Handle *H, const double *const *f7) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    k_set_conservative<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, f7[0], f7[1], f7[2],
+                                                                     f7[3], f7[4], f7[5], f7[6], H->buf[H->cur]);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int set_tstep_device(Handle *H) {
+    const Fields &F = H->buf[H->cur];
+    DevScalars *sc = H->dsc;
+    unsigned long long inf = 0x7ff0000000000000ull;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&sc->cfl_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, H->stream));
+    SUNSET_CUDA(H, cudaMemcpyAsync(&sc->par_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, H->stream));
+    k_tstep<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(F.u, F.v, F.ro, H->sp, H->ntype, H->npfb, sc);
+    k_tstep_fold<<<1, 1, 0, H->stream>>>(sc);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int rhs_only(Handle *H) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
+    StageArgs A = make_args(H, H->cur, 4);
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI: k_stage<SUNSET_FORM_DI><<<nblk, TB, 0, H->stream>>>(A); break;
+    case SUNSET_FORM_CHL: k_stage<SUNSET_FORM_CHL><<<nblk, TB, 0, H->stream>>>(A); break;
+    case SUNSET_FORM_LC: k_stage<SUNSET_FORM_LC><<<nblk, TB, 0, H->stream>>>(A); break;
+    default: k_stage<SUNSET_FORM_NEWT><<<nblk, TB, 0, H->stream>>>(A); break;
+    }
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int step_run(Handle *H, double dt, int nsteps, int mode) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    cudaStream_t st = H->stream;
+    if (mode == 0) SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < nsteps; s++) {
+        int from = H->cur;
+        if (!H->graph[from] || H->graph_mode[from] != mode) {
+            if (H->graph[from]) { cudaGraphExecDestroy(H->graph[from]); H->graph[from] = nullptr; }
+            cudaGraph_t g;
+            SUNSET_CUDA(H, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            launch_step(H, from, mode);
+            SUNSET_CUDA(H, cudaStreamEndCapture(st, &g));
+            SUNSET_CUDA(H, cudaGraphInstantiate(&H->graph[from], g, 0));
+            cudaGraphDestroy(g);
+            H->graph_mode[from] = mode;
+        }
+        SUNSET_CUDA(H, cudaGraphLaunch(H->graph[from], st));
+        H->cur ^= 1;
+    }
+    return 0;
+}
+
+int op_gradient(Handle *H, const double *phi, double *gx, double *gy) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    StageArgs A = make_args(H, 0, 5);
+    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
+    k_op_grad_lap<<<nblk, TB, 0, H->stream>>>(A, phi, gx, gy, nullptr);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int op_laplacian(Handle *H, const double *phi, double *lap) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    StageArgs A = make_args(H, 0, 5);
+    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
+    k_op_grad_lap<<<nblk, TB, 0, H->stream>>>(A, phi, nullptr, nullptr, lap);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int op_filter(Handle *H, const double *phi, double *out, int term_only) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    StageArgs A = make_args(H, 0, 5);
+    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
+    k_op_filter<<<nblk, TB, 0, H->stream>>>(A, phi, out, term_only);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+int reduce_ke_mass(Handle *H, double *ke, double *mass) {
+    const int TB = 128, nb = (H->npfb + TB - 1) / TB;
+    double *p = H->partials;
+    k_ke_mass<<<nb, TB, 0, H->stream>>>(H->npfb, H->buf[H->cur], H->vol, p);
+    std::vector<double> hp(2 * (size_t)nb);
+    SUNSET_CUDA(H, cudaMemcpyAsync(hp.data(), p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    double k = 0.0, m = 0.0;
+    for (int b = 0; b < nb; b++) { k += hp[2 * b]; m += hp[2 * b + 1]; }
+    if (ke) *ke = k;
+    if (mass) *mass = m;
+    return 0;
+}
+
+int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
+    int rc = upload_consts(H);
+    if (rc) return rc;
+    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
+    // stage 4 (right-hand side only) reads what an RK stage reads and writes the rhs arrays;
+    // use stage 1 itself: it reads the current buffer and writes the other one.
+    StageArgs A = make_args(H, H->cur, 1);
+    cudaEvent_t e0, e1;
+    SUNSET_CUDA(H, cudaEventCreate(&e0));
+    SUNSET_CUDA(H, cudaEventCreate(&e1));
+    auto launch = [&]() {
+        switch (H->cfg.form) {
+        case SUNSET_FORM_DI: k_stage<SUNSET_FORM_DI><<<nblk, TB, 0, H->stream>>>(A); break;
+        case SUNSET_FORM_CHL: k_stage<SUNSET_FORM_CHL><<<nblk, TB, 0, H->stream>>>(A); break;
+        case SUNSET_FORM_LC: k_stage<SUNSET_FORM_LC><<<nblk, TB, 0, H->stream>>>(A); break;
+        default: k_stage<SUNSET_FORM_NEWT><<<nblk, TB, 0, H->stream>>>(A); break;
+        }
+    };
+    for (int r = 0; r < 3; r++) launch();
+    SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
+    for (int r = 0; r < reps; r++) launch();
+    SUNSET_CUDA(H, cudaEventRecord(e1, H->stream));
+    SUNSET_CUDA(H, cudaEventSynchronize(e1));
+    float t = 0.f;
+    SUNSET_CUDA(H, cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / reps;
+    // algorithmic bytes of one stage launch: small-link stream (index + 3 weights), the
+    // per-node state read once, registers S and E read + written, new state written.
+    long long links = 0;
+    {
+        std::vector<int> ws(H->nslices);
+        cudaMemcpy(ws.data(), H->slice_ws, ws.size() * sizeof(int), cudaMemcpyDeviceToHost);
+        for (int w : ws) links += (long long)w * kSlice;
+    }
+    const int form = H->cfg.form;
+    const int nf = form == SUNSET_FORM_DI ? 7 : 6;         // evolved fields (S and E registers)
+    const int nread = form == SUNSET_FORM_DI ? 9 : 13;      // state + derived fields of a node
+    const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;     // next state + derived fields
+    *bytes = (double)links * (4 + 3 * 8) + (double)H->npfb * 8.0 * (nread + 4 * nf + nwrite) +
+             (double)H->npfb * 8.0 * 4;  // sums + ordinate
+    return 0;
+}
+
+}  // namespace sunset

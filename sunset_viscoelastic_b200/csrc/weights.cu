@@ -1,0 +1,699 @@
+// weights.cu -- LABFM weight construction on the device (labf.F90, svdlib.F90, rbfs.F90).
+//
+// One warp builds the weights of one node: it assembles the moment matrix
+// A = sum_k X(r_k/h) [W(r_k/h) H(r_k/h)]^T (monomials X, Hermite ABFs H, Wendland C2 W)
+// in shared memory, factors it with the reference's Golub-Kahan-Reinsch SVD and applies
+// the factorisation to each right-hand side.  The SVD is the reference's algorithm with
+// its serial recurrences kept serial: lanes split only loops whose iterations are
+// independent (columns of a Householder update, rows of a Givens rotation), and every
+// dot product is summed by one lane in the reference's order.  With -fmad=false each
+// operation then rounds exactly as the reference's does, so the factorisation - and the
+// weights - are those of the CPU restatement bit for bit.
+//
+// The five SVDs of identical matrix copies in labf.F90:157-180 become one factorisation
+// applied to five right-hand sides; the filter matrix (labf.F90:258-303) is the same
+// matrix whenever h == h_small, the counts agree and the order drops agree, and is then
+// not factored again.
+#include "internal.cuh"
+
+namespace sunset {
+
+namespace {
+
+__host__ __device__ constexpr int nsz(int k) { return (k * k + 3 * k) / 2; }
+
+// (p, q) exponents of unknown m in the reference's degree-graded ordering
+// (labf.F90:1815-1920): degree d, p from d down to 0.
+__host__ __device__ constexpr int deg_of(int m) {
+    int d = 1, base = 0;
+    while (m >= base + d + 1) { base += d + 1; d++; }
+    return d;
+}
+__host__ __device__ constexpr int p_of(int m) {
+    int d = 1, base = 0;
+    while (m >= base + d + 1) { base += d + 1; d++; }
+    return d - (m - base);
+}
+__host__ __device__ constexpr int q_of(int m) { return deg_of(m) - p_of(m); }
+
+__device__ __forceinline__ double fact(int k) {
+    double f = 1.0;
+    for (int j = 2; j <= k; j++) f *= (double)j;
+    return f;
+}
+
+// labf.F90:2329-2391 probabilists' Hermite polynomials, in the reference's operation order.
+__device__ __forceinline__ double hermite(int n, double z) {
+    double z2, z3, z4;
+    switch (n) {
+    case 0: return 1.0;
+    case 1: return z;
+    case 2: return z * z - 1.0;
+    case 3: return (z * z) * z - 3.0 * z;
+    case 4: return ((((z * z) * z) * z) - ((6.0 * z) * z)) + 3.0;
+    case 5: z2 = z * z; z3 = z * z2; return ((z2 * z3) - (10.0 * z3)) + (15.0 * z);
+    case 6: z2 = z * z; z3 = z * z2; return (((z3 * z3) - ((15.0 * z2) * z2)) + (45.0 * z2)) - 15.0;
+    case 7:
+        z2 = z * z; z3 = z * z2; z4 = z3 * z;
+        return (((z4 * z3) - ((21.0 * z3) * z2)) + (105.0 * z3)) - (105.0 * z);
+    case 8:
+        z2 = z * z; z4 = z2 * z2;
+        return ((((z4 * z4) - ((28.0 * z4) * z2)) + (210.0 * z4)) - (420.0 * z2)) + 105.0;
+    case 9:
+        z2 = z * z; z3 = z * z2; z4 = z3 * z;
+        return (((((z4 * z3) * z2) - ((36.0 * z4) * z3)) + ((378.0 * z3) * z2)) - (1260.0 * z3)) + (945.0 * z);
+    case 10:
+        z2 = z * z; z4 = z2 * z2;
+        return ((((((z4 * z4) * z2) - ((45.0 * z4) * z4)) + ((630.0 * z4) * z2)) - (3150.0 * z4)) + (4725.0 * z2)) - 945.0;
+    }
+    return 0.0;
+}
+
+// x^p y^q / (p! q!) as written in labf.F90:1815-1920: x2=x*x, x3=x2*x, ..., then
+// (coef*x^p)*y^q.
+__device__ __forceinline__ double monomial(int p, int q, double x, double y) {
+    double xp = x, yq = y;
+    for (int k = 2; k <= p; k++) xp = xp * x;
+    for (int k = 2; k <= q; k++) yq = yq * y;
+    double den = fact(p) * fact(q);
+    if (den == 1.0) {
+        if (p == 0) return yq;
+        if (q == 0) return xp;
+        return xp * yq;
+    }
+    double c = 1.0 / den;
+    if (q == 0) return c * xp;
+    if (p == 0) return c * yq;
+    return (c * xp) * yq;
+}
+
+// x^4 correctly rounded.  The reference evaluates (1-q/2)**4.0 with libm pow; glibc's pow
+// returns the correctly rounded power for these arguments, which this reproduces with an
+// exact double-double product (Dekker's two-product, built on fma) rounded once.
+__device__ __forceinline__ double pow4_cr(double x) {
+    double a = x * x;
+    double ae = fma(x, x, -a);           // x*x = a + ae exactly
+    double b = a * a;                     // (a + ae)^2 = a^2 + 2 a ae + ae^2
+    double be = fma(a, a, -b);            // a*a = b + be exactly
+    double t = fma(2.0 * a, ae, be);      // small terms
+    t = fma(ae, ae, t);
+    return b + t;
+}
+
+// rbfs.F90:48-57, Wendland C2 (zero at q=0 and q>2).
+__device__ __forceinline__ double wab(double qq, double h2) {
+    double qq4 = 1.0 - 0.5 * qq;
+    qq4 = pow4_cr(qq4);
+    double f = 0.0;
+    if (qq <= 2.0 && qq > 0.0) f = ((7.0 / ((4.0 * kPi) * h2)) * (2.0 * qq + 1.0)) * qq4;
+    return f;
+}
+
+__device__ __forceinline__ double nr_hypot(double a, double b) {  // svdlib.F90:308-327
+    double absA = fabs(a), absB = fabs(b), t;
+    if (absA > absB) {
+        t = absB / absA;
+        return absA * sqrt(1.0 + t * t);
+    }
+    if (absB == 0.0) return 0.0;
+    t = absA / absB;
+    return absB * sqrt(1.0 + t * t);
+}
+
+// Shared scalars are written by lane 0 between two warp barriers, so no lane reads a
+// half-updated value and every lane sees the new one.
+__device__ __forceinline__ void wstore(double *p, double v, int lane) {
+    __syncwarp();
+    if (lane == 0) *p = v;
+    __syncwarp();
+}
+
+// svdlib.F90:37-278 on a warp.  U (in: A, out: U) and V are column-major n x n with
+// leading dimension ld; W and rv1 are 1-based.  Returns 0 or -1 (no convergence).
+template <int N>
+__device__ int svd_factor_warp(double *U, double *V, double *W, double *rv1, int ld, int lane) {
+    const int n = N;
+#define UM(i, j) U[((j) - 1) * ld + ((i) - 1)]
+#define VM(i, j) V[((j) - 1) * ld + ((i) - 1)]
+    double anorm = 0.0, c, f, g = 0.0, h, s, scale = 0.0, x, y, z;
+    int l = 1, nm;
+    for (int i = 1; i <= n; i++) {
+        l = i + 1;
+        wstore(&rv1[i], scale * g, lane);
+        g = 0.0; s = 0.0; scale = 0.0;
+        for (int k = i; k <= n; k++) scale = scale + fabs(UM(k, i));
+        if (scale != 0.0) {
+            __syncwarp();
+            for (int k = i + lane; k <= n; k += 32) UM(k, i) = UM(k, i) / scale;
+            __syncwarp();
+            for (int k = i; k <= n; k++) s = s + UM(k, i) * UM(k, i);
+            f = UM(i, i);
+            g = -copysign(sqrt(s), f);
+            h = f * g - s;
+            wstore(&UM(i, i), f - g, lane);
+            for (int j = l + lane; j <= n; j += 32) {
+                double sj = 0.0;
+                for (int k = i; k <= n; k++) sj = sj + UM(k, i) * UM(k, j);
+                double fj = sj / h;
+                for (int k = i; k <= n; k++) UM(k, j) = UM(k, j) + fj * UM(k, i);
+            }
+            __syncwarp();
+            for (int k = i + lane; k <= n; k += 32) UM(k, i) = scale * UM(k, i);
+            __syncwarp();
+        }
+        wstore(&W[i], scale * g, lane);
+        g = 0.0; s = 0.0; scale = 0.0;
+        for (int k = l; k <= n; k++) scale = scale + fabs(UM(i, k));
+        if (scale != 0.0) {
+            __syncwarp();
+            for (int k = l + lane; k <= n; k += 32) UM(i, k) = UM(i, k) / scale;
+            __syncwarp();
+            for (int k = l; k <= n; k++) s = s + UM(i, k) * UM(i, k);
+            f = UM(i, l);
+            g = -copysign(sqrt(s), f);
+            h = f * g - s;
+            wstore(&UM(i, l), f - g, lane);
+            for (int k = l + lane; k <= n; k += 32) rv1[k] = UM(i, k) / h;
+            __syncwarp();
+            for (int j = l + lane; j <= n; j += 32) {
+                double sj = 0.0;
+                for (int k = l; k <= n; k++) sj = sj + UM(j, k) * UM(i, k);
+                for (int k = l; k <= n; k++) UM(j, k) = UM(j, k) + sj * rv1[k];
+            }
+            __syncwarp();
+            for (int k = l + lane; k <= n; k += 32) UM(i, k) = scale * UM(i, k);
+            __syncwarp();
+        }
+        double t = fabs(W[i]) + fabs(rv1[i]);
+        anorm = (t > anorm) ? t : anorm;
+    }
+    // right-hand transformations, svdlib.F90:115-141
+    for (int i = n; i >= 1; i--) {
+        if (i < n) {
+            if (g != 0.0) {
+                __syncwarp();
+                for (int j = l + lane; j <= n; j += 32) VM(j, i) = (UM(i, j) / UM(i, l)) / g;
+                __syncwarp();
+                for (int j = l + lane; j <= n; j += 32) {
+                    double sj = 0.0;
+                    for (int k = l; k <= n; k++) sj = sj + UM(i, k) * VM(k, j);
+                    for (int k = l; k <= n; k++) VM(k, j) = VM(k, j) + sj * VM(k, i);
+                }
+                __syncwarp();
+            }
+            for (int j = l + lane; j <= n; j += 32) { VM(i, j) = 0.0; VM(j, i) = 0.0; }
+            __syncwarp();
+        }
+        wstore(&VM(i, i), 1.0, lane);
+        g = rv1[i];
+        l = i;
+    }
+    // left-hand transformations, svdlib.F90:143-171
+    for (int i = n; i >= 1; i--) {
+        l = i + 1;
+        g = W[i];
+        __syncwarp();
+        for (int j = l + lane; j <= n; j += 32) UM(i, j) = 0.0;
+        __syncwarp();
+        if (g != 0.0) {
+            g = 1.0 / g;
+            for (int j = l + lane; j <= n; j += 32) {
+                double sj = 0.0;
+                for (int k = l; k <= n; k++) sj = sj + UM(k, i) * UM(k, j);
+                double fj = (sj / UM(i, i)) * g;
+                for (int k = i; k <= n; k++) UM(k, j) = UM(k, j) + fj * UM(k, i);
+            }
+            __syncwarp();
+            for (int j = i + lane; j <= n; j += 32) UM(j, i) = UM(j, i) * g;
+            __syncwarp();
+        } else {
+            for (int j = i + lane; j <= n; j += 32) UM(j, i) = 0.0;
+            __syncwarp();
+        }
+        wstore(&UM(i, i), UM(i, i) + 1.0, lane);
+    }
+    // diagonalisation, svdlib.F90:173-278
+    nm = 1;
+    for (int k = n; k >= 1; k--) {
+        for (int its = 1; its <= 30; its++) {
+            bool to2000 = false;
+            for (l = k; l >= 1; l--) {
+                nm = l - 1;
+                if ((fabs(rv1[l]) + anorm) == anorm) { to2000 = true; break; }
+                if ((fabs(W[nm]) + anorm) == anorm) break;
+            }
+            if (!to2000) {
+                c = 0.0; s = 1.0;
+                for (int i = l; i <= k; i++) {
+                    double r = rv1[i];
+                    f = s * r;
+                    wstore(&rv1[i], c * r, lane);
+                    if ((fabs(f) + anorm) == anorm) break;
+                    g = W[i];
+                    h = nr_hypot(f, g);
+                    wstore(&W[i], h, lane);
+                    h = 1.0 / h;
+                    c = (g * h);
+                    s = -(f * h);
+                    for (int j = 1 + lane; j <= n; j += 32) {
+                        double yy = UM(j, nm), zz = UM(j, i);
+                        UM(j, nm) = (yy * c) + (zz * s);
+                        UM(j, i) = -(yy * s) + (zz * c);
+                    }
+                    __syncwarp();
+                }
+            }
+            z = W[k];
+            if (l == k) {
+                if (z < 0.0) {
+                    wstore(&W[k], -z, lane);
+                    for (int j = 1 + lane; j <= n; j += 32) VM(j, k) = -VM(j, k);
+                    __syncwarp();
+                }
+                break;
+            }
+            if (its == 30) return -1;
+            x = W[l];
+            nm = k - 1;
+            y = W[nm];
+            g = rv1[nm];
+            h = rv1[k];
+            f = ((y - z) * (y + z) + (g - h) * (g + h)) / ((2.0 * h) * y);
+            g = nr_hypot(f, 1.0);
+            f = ((x - z) * (x + z) + h * ((y / (f + copysign(g, f))) - h)) / x;
+            c = 1.0; s = 1.0;
+            for (int j = l; j <= nm; j++) {
+                int i = j + 1;
+                g = rv1[i];
+                y = W[i];
+                h = s * g;
+                g = c * g;
+                z = nr_hypot(f, h);
+                wstore(&rv1[j], z, lane);
+                c = f / z;
+                s = h / z;
+                f = (x * c) + (g * s);
+                g = -(x * s) + (g * c);
+                h = y * s;
+                y = y * c;
+                for (int jj = 1 + lane; jj <= n; jj += 32) {
+                    double xv = VM(jj, j), zv = VM(jj, i);
+                    VM(jj, j) = (xv * c) + (zv * s);
+                    VM(jj, i) = -(xv * s) + (zv * c);
+                }
+                z = nr_hypot(f, h);
+                wstore(&W[j], z, lane);
+                if (z != 0.0) {
+                    z = 1.0 / z;
+                    c = f * z;
+                    s = h * z;
+                }
+                f = (c * g) + (s * y);
+                x = -(s * g) + (c * y);
+                for (int jj = 1 + lane; jj <= n; jj += 32) {
+                    double yv = UM(jj, j), zv = UM(jj, i);
+                    UM(jj, j) = (yv * c) + (zv * s);
+                    UM(jj, i) = -(yv * s) + (zv * c);
+                }
+                __syncwarp();
+            }
+            wstore(&rv1[l], 0.0, lane);
+            wstore(&rv1[k], f, lane);
+            wstore(&W[k], x, lane);
+        }
+    }
+    __syncwarp();
+    return 0;
+#undef UM
+#undef VM
+}
+
+// svdlib.F90:279-303: b <- V diag(1/w) U^T b (exactly-zero singular values skipped).
+template <int N>
+__device__ void svd_apply_warp(const double *U, const double *V, const double *W, double *tmp, double *b, int ld,
+                               int lane) {
+    __syncwarp();
+    for (int j = 1 + lane; j <= N; j += 32) {
+        double s = 0.0;
+        if (W[j] != 0.0) {
+            for (int i = 1; i <= N; i++) s = s + U[(j - 1) * ld + (i - 1)] * b[i - 1];
+            s = s / W[j];
+        }
+        tmp[j] = s;
+    }
+    __syncwarp();
+    for (int j = 1 + lane; j <= N; j += 32) {
+        double s = 0.0;
+        for (int jj = 1; jj <= N; jj++) s = s + V[(jj - 1) * ld + (j - 1)] * tmp[jj];
+        b[j - 1] = s;
+    }
+    __syncwarp();
+}
+
+struct WArgs {
+    int npfb, morder, forder;
+    double h2;
+    const double *px, *py, *h, *hs;
+    const int *ntype, *cnt, *cnt_small, *lpt;
+    const long long *slice_ptr;
+    double *wx, *wy, *wl, *wh;
+    int *err;
+};
+
+__device__ __forceinline__ long long sell_off(const long long *slice_ptr, int i, int k) {
+    return slice_ptr[i >> 5] + (long long)k * kSlice + (i & 31);
+}
+
+// Moment matrix over links [0,cnt) of node i with length scale hh (labf.F90:88-123).
+template <int ORDER>
+__device__ void assemble(const WArgs &a, int i, int cnt, double hh, double *U, int ld, double *X, double *G,
+                         int lane) {
+    constexpr int n = nsz(ORDER);
+    __syncwarp();
+    for (int e = lane; e < n * n; e += 32) U[(e / n) * ld + (e % n)] = 0.0;
+    const double xi = a.px[i], yi = a.py[i];
+    for (int k = 0; k < cnt; k++) {
+        int p = a.lpt[sell_off(a.slice_ptr, i, k)];
+        double x = -(xi - a.px[p]), y = -(yi - a.py[p]);
+        double rad = sqrt(x * x + y * y) / hh;
+        double ff1 = wab(rad, a.h2);
+        double xx = x / hh, yy = y / hh;
+        __syncwarp();
+        for (int m = lane; m < n; m += 32) {
+            int pm = p_of(m), qm = q_of(m);
+            X[m] = monomial(pm, qm, x / hh, y / hh);
+            double g = (qm == 0) ? hermite(pm, xx) : (pm == 0) ? hermite(qm, yy) : hermite(pm, xx) * hermite(qm, yy);
+            G[m] = g * ff1;
+        }
+        __syncwarp();
+        for (int e = lane; e < n * n; e += 32) {
+            int i1 = e % n, i2 = e / n;
+            double *u = &U[i2 * ld + i1];
+            *u = *u + X[i1] * G[i2];
+        }
+    }
+    __syncwarp();
+}
+
+// labf.F90:125-148: keep the first m unknowns.
+template <int N>
+__device__ void drop_order(double *U, int ld, int m, int lane) {
+    __syncwarp();
+    for (int e = lane; e < N * N; e += 32) {
+        int i1 = e % N, i2 = e / N;
+        if (i2 >= m || i1 >= m) U[i2 * ld + i1] = (i1 == i2) ? 1.0 : 0.0;
+    }
+    __syncwarp();
+}
+
+__device__ void hyp_rhs(int order, double *b, int n, int lane) {
+    __syncwarp();
+    for (int m = lane; m < n; m += 32) b[m] = 0.0;
+    __syncwarp();
+    if (lane == 0) {
+        if (order <= 5) { b[9] = -1.0; b[11] = -2.0; b[13] = -1.0; }
+        else if (order <= 7) { b[20] = 1.0; b[22] = 3.0; b[24] = 3.0; b[26] = 1.0; }
+        else if (order <= 9) { b[35] = -1.0; b[37] = -4.0; b[39] = -6.0; b[41] = -4.0; b[43] = -1.0; }
+        else { b[54] = 1.0; b[56] = 5.0; b[58] = 10.0; b[60] = 10.0; b[62] = 5.0; b[64] = 1.0; }
+    }
+    __syncwarp();
+}
+
+template <int ORDER>
+__host__ __device__ constexpr int smem_doubles() {
+    return 2 * nsz(ORDER) * (nsz(ORDER) | 1) + 3 * (nsz(ORDER) + 2) + 7 * nsz(ORDER);
+}
+
+template <int ORDER>
+__global__ void k_labf_weights(WArgs a) {
+    constexpr int n = nsz(ORDER);
+    constexpr int ld = n | 1;
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    double *U = smem + warp * smem_doubles<ORDER>();
+    double *V = U + n * ld, *W = V + n * ld, *rv1 = W + (n + 2), *tmp = rv1 + (n + 2);
+    double *X = tmp + (n + 2), *G = X + n, *bx = G + n, *by = bx + n, *bxx = by + n, *byy = bxx + n, *bh = byy + n;
+    for (int i = blockIdx.x * wpb + warp; i < a.npfb; i += gridDim.x * wpb) {
+        const int t = a.ntype[i];
+        if (!(t < 0 || t == 999 || t == 998)) continue;  // boundary nodes: labf.F90:505-1039
+        const int cnt = a.cnt[i], cs = a.cnt_small[i];
+        double hh = a.hs[i];
+        // ---- derivative weights, labf.F90:80-215 ----
+        assemble<ORDER>(a, i, cs, hh, U, ld, X, G, lane);
+        if (a.morder >= 7 && (t == 998 || t < 0)) drop_order<n>(U, ld, 27, lane);
+        if (a.morder >= 5 && (t == -1 || t == -2)) drop_order<n>(U, ld, 14, lane);
+        if (svd_factor_warp<n>(U, V, W, rv1, ld, lane)) {
+            if (lane == 0) atomicExch(a.err, i + 1);
+            continue;
+        }
+        for (int m = lane; m < n; m += 32) {
+            bx[m] = (m == 0) ? 1.0 : 0.0;
+            by[m] = (m == 1) ? 1.0 : 0.0;
+            bxx[m] = (m == 2) ? 1.0 : 0.0;
+            byy[m] = (m == 4) ? 1.0 : 0.0;
+        }
+        svd_apply_warp<n>(U, V, W, tmp, bx, ld, lane);
+        svd_apply_warp<n>(U, V, W, tmp, by, ld, lane);
+        svd_apply_warp<n>(U, V, W, tmp, bxx, ld, lane);
+        svd_apply_warp<n>(U, V, W, tmp, byy, ld, lane);
+        for (int m = lane; m < n; m += 32) bxx[m] = bxx[m] + byy[m];  // bvecxx + bvecyy
+        __syncwarp();
+        const double xi = a.px[i], yi = a.py[i];
+        for (int k = lane; k < cnt; k += 32) {
+            int p = a.lpt[sell_off(a.slice_ptr, i, k)];
+            double x = -(xi - a.px[p]), y = -(yi - a.py[p]);
+            double rad = sqrt(x * x + y * y) / hh;
+            double ff1 = wab(rad, a.h2);
+            double xx = x / hh, yy = y / hh;
+            double hx[ORDER + 1], hy[ORDER + 1];
+#pragma unroll
+            for (int d = 0; d <= ORDER; d++) { hx[d] = hermite(d, xx); hy[d] = hermite(d, yy); }
+            double sx = 0.0, sy = 0.0, sl = 0.0;
+#pragma unroll
+            for (int m = 0; m < n; m++) {
+                constexpr int dummy = 0;
+                (void)dummy;
+                const int pm = p_of(m), qm = q_of(m);
+                double g = (qm == 0) ? hx[pm] : (pm == 0) ? hy[qm] : hx[pm] * hy[qm];
+                g = g * ff1;
+                sx = sx + bx[m] * g;
+                sy = sy + by[m] * g;
+                sl = sl + bxx[m] * g;
+            }
+            long long o = sell_off(a.slice_ptr, i, k);
+            a.wx[o] = sx / hh;
+            a.wy[o] = sy / hh;
+            a.wl[o] = (sl / hh) / hh;
+        }
+        // ---- filter weights, calc_filter_weights (labf.F90:258-388) ----
+        const double hf = a.h[i];
+        const bool same = (hf == hh) && (cnt == cs) && (a.forder == a.morder) && (t != -2);
+        if (!same) {
+            assemble<ORDER>(a, i, cnt, hf, U, ld, X, G, lane);
+            if (a.forder >= 7 && (t == 998 || t < 0)) drop_order<n>(U, ld, 27, lane);
+            if (a.forder >= 5 && t == -1) drop_order<n>(U, ld, 14, lane);
+            if (svd_factor_warp<n>(U, V, W, rv1, ld, lane)) {
+                if (lane == 0) atomicExch(a.err, i + 1);
+                continue;
+            }
+        }
+        int hord = a.forder;
+        if (a.forder >= 7 && (t == 998 || t < 0)) hord = 6;
+        if (a.forder >= 5 && t == -1) hord = 4;
+        hyp_rhs(hord, bh, n, lane);
+        svd_apply_warp<n>(U, V, W, tmp, bh, ld, lane);
+        for (int k = lane; k < cnt; k += 32) {
+            int p = a.lpt[sell_off(a.slice_ptr, i, k)];
+            double x = -(xi - a.px[p]), y = -(yi - a.py[p]);
+            double rad = sqrt(x * x + y * y) / hf;
+            double ff1 = wab(rad, a.h2);
+            double xx = x / hf, yy = y / hf;
+            double hx[ORDER + 1], hy[ORDER + 1];
+#pragma unroll
+            for (int d = 0; d <= ORDER; d++) { hx[d] = hermite(d, xx); hy[d] = hermite(d, yy); }
+            double sh = 0.0;
+#pragma unroll
+            for (int m = 0; m < n; m++) {
+                const int pm = p_of(m), qm = q_of(m);
+                double g = (qm == 0) ? hx[pm] : (pm == 0) ? hy[qm] : hx[pm] * hy[qm];
+                g = g * ff1;
+                sh = sh + bh[m] * g;
+            }
+            a.wh[sell_off(a.slice_ptr, i, k)] = sh;
+        }
+        __syncwarp();
+    }
+}
+
+// calc_labf_sums (labf.F90:396-451) and calc_node_volumes (:453-503), one thread per node;
+// link k of a slice is read by the 32 threads of a warp at once.
+struct SumArgs {
+    int npfb;
+    double L;
+    const double *px, *py, *h, *sp;
+    const int *ntype, *cnt, *lpt;
+    const long long *slice_ptr;
+    double *wx, *wy, *wl, *wh, *gsx, *gsy, *lsum, *hsum, *vol;
+};
+
+__global__ void k_labf_sums(SumArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npfb) return;
+    const long long base = a.slice_ptr[i >> 5] + (i & 31);
+    const int cnt = a.cnt[i];
+    double gx = 0.0, gy = 0.0, lp = 0.0, hy = 0.0;
+    for (int k = 0; k < cnt; k++) {
+        long long o = base + (long long)k * kSlice;
+        hy = hy + a.wh[o];
+        gx = gx + a.wx[o];
+        gy = gy + a.wy[o];
+        lp = lp + a.wl[o];
+    }
+    a.gsx[i] = gx / a.L;
+    a.gsy[i] = gy / a.L;
+    a.lsum[i] = (lp / a.L) / a.L;
+    a.hsum[i] = hy;
+    for (int k = 0; k < cnt; k++) {
+        long long o = base + (long long)k * kSlice;
+        a.wx[o] = a.wx[o] / a.L;
+        a.wy[o] = a.wy[o] / a.L;
+        a.wl[o] = (a.wl[o] / a.L) / a.L;
+    }
+    const int t = a.ntype[i];
+    if (t < 0 || t == 999 || t == 998) {
+        const double hh = a.h[i], xi = a.px[i], yi = a.py[i];
+        double v = 0.0;
+        for (int k = 0; k < cnt; k++) {
+            int p = a.lpt[base + (long long)k * kSlice];
+            double x = -(xi - a.px[p]), y = -(yi - a.py[p]);
+            double rad = sqrt(x * x + y * y) / hh;
+            double f1 = ((9.0 / kPi) * exp((-9.0 * rad) * rad)) / (hh * hh);
+            v = v + f1;
+        }
+        a.vol[i] = 1.0 / v;
+    } else {
+        a.vol[i] = a.sp[i] * a.sp[i];
+    }
+}
+
+// filter_coefficients, labf.F90:1723-1811 (walls' FD-row reductions need fd_parent and
+// are applied only for interior nodes here: the boundary framework is outside this path).
+__global__ void k_filter_coeff(SumArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npfb) return;
+    const long long base = a.slice_ptr[i >> 5] + (i & 31);
+    const int cnt = a.cnt[i];
+    const double xi = a.px[i], yi = a.py[i];
+    const int t = a.ntype[i];
+    double fc;
+    if (t < 0 || t == 999 || t == 998) {
+        double lscal = (2.0 * a.h[i]) * sqrt(kPi / (double)cnt);
+        double tmp = ((2.0 / 3.0) * kPi) / lscal;
+        double lsum = 0.0;
+        for (int k = 0; k < cnt; k++) {
+            long long o = base + (long long)k * kSlice;
+            int p = a.lpt[o];
+            double x = a.px[p] - xi, y = a.py[p] - yi;
+            double fji = 1.0 - cos(tmp * x) * cos(tmp * y);
+            lsum = lsum + fji * a.wh[o];
+        }
+        fc = (2.0 / 3.0) / lsum;
+    } else {
+        double tmp = ((2.0 / 3.0) * kPi) / a.sp[i];
+        double lsum = 0.0;
+        for (int k = 0; k < cnt; k++) {
+            long long o = base + (long long)k * kSlice;
+            int p = a.lpt[o];
+            double x = a.px[p] - xi, y = a.py[p] - yi;
+            double fji = 1.0 - cos(tmp * sqrt(x * x + y * y));
+            lsum = lsum + fji * a.wh[o];
+        }
+        fc = (1.0 / 3.0) / lsum;
+        fc = fc * 0.5;
+    }
+    double sum = 0.0;
+    for (int k = 0; k < cnt; k++) {
+        long long o = base + (long long)k * kSlice;
+        double w = a.wh[o] * fc;
+        a.wh[o] = w;
+        sum = sum + w;
+    }
+    a.hsum[i] = sum;
+}
+
+template <int ORDER>
+int launch_weights(Handle *H, WArgs &a) {
+    constexpr int per_warp = smem_doubles<ORDER>() * (int)sizeof(double);
+    int wpb = (200 * 1024) / per_warp;
+    if (wpb > 16) wpb = 16;
+    if (wpb < 1) wpb = 1;
+    size_t smem = (size_t)wpb * per_warp;
+    SUNSET_CUDA(H, cudaFuncSetAttribute(k_labf_weights<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nsm = 0;
+    SUNSET_CUDA(H, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, H->device));
+    int nb = (a.npfb + wpb - 1) / wpb;
+    int cap = nsm * 8;
+    if (nb > cap) nb = cap;
+    k_labf_weights<ORDER><<<nb, wpb * 32, smem, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+}  // namespace
+
+int labf_weights_device(Handle *H) {
+    const int n = H->npfb;
+    if (H->cfg.forder != H->cfg.morder)
+        return set_err(H, SUNSET_ERR_SCOPE, "the device weight build requires forder == morder");
+    if (!H->wx) {
+        if (dalloc(H, &H->wx, H->nlinks_sell) || dalloc(H, &H->wy, H->nlinks_sell) ||
+            dalloc(H, &H->wl, H->nlinks_sell) || dalloc(H, &H->wh, H->nlinks_sell) || dalloc(H, &H->gsx, n) ||
+            dalloc(H, &H->gsy, n) || dalloc(H, &H->lsum, n) || dalloc(H, &H->hsum, n) || dalloc(H, &H->vol, n))
+            return SUNSET_ERR_NOMEM;
+    }
+    cudaStream_t st = H->stream;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->wx, 0, H->nlinks_sell * sizeof(double), st));
+    SUNSET_CUDA(H, cudaMemsetAsync(H->wy, 0, H->nlinks_sell * sizeof(double), st));
+    SUNSET_CUDA(H, cudaMemsetAsync(H->wl, 0, H->nlinks_sell * sizeof(double), st));
+    SUNSET_CUDA(H, cudaMemsetAsync(H->wh, 0, H->nlinks_sell * sizeof(double), st));
+    int *derr;
+    if (dalloc(H, &derr, 1)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(derr, 0, sizeof(int), st));
+    WArgs a{n, H->cfg.morder, H->cfg.forder, H->h2, H->px, H->py, H->h, H->hs, H->ntype, H->cnt, H->cnt_small,
+            H->lpt, H->slice_ptr, H->wx, H->wy, H->wl, H->wh, derr};
+    int rc;
+    switch (H->cfg.morder) {
+    case 4: rc = launch_weights<4>(H, a); break;
+    case 6: rc = launch_weights<6>(H, a); break;
+    case 8: rc = launch_weights<8>(H, a); break;
+    case 10: rc = launch_weights<10>(H, a); break;
+    default: return set_err(H, SUNSET_ERR_ARG, "order must be 4, 6, 8 or 10");
+    }
+    if (rc) return rc;
+    int herr = 0;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    dfree(H, derr);
+    if (herr) return set_err(H, SUNSET_ERR_SVD, "SVD not converging at internal node %d (svdlib.F90:219-222)", herr - 1);
+    return 0;
+}
+
+int labf_sums_device(Handle *H) {
+    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->slice_ptr,
+              H->wx, H->wy, H->wl, H->wh, H->gsx, H->gsy, H->lsum, H->hsum, H->vol};
+    k_labf_sums<<<(H->npfb + 255) / 256, 256, 0, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+int filter_coefficients_device(Handle *H) {
+    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->slice_ptr,
+              H->wx, H->wy, H->wl, H->wh, H->gsx, H->gsy, H->lsum, H->hsum, H->vol};
+    k_filter_coeff<<<(H->npfb + 255) / 256, 256, 0, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+}  // namespace sunset

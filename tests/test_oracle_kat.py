@@ -1,0 +1,230 @@
+"""Known-answer tests of the CPU restatement (the oracle), run without a GPU.
+
+The reference ships no test suite and no golden outputs, and it cannot be compiled here
+(Fortran).  The restatement is pinned instead by what the reference itself solves for and
+checks: the LABFM moment conditions (labf.F90:153-180), its own analytic steady state
+(the Kolmogorov initial condition of setup_flow.F90:224-229 with the forcing of
+rhs.F90:275, statistics.F90:552-612), mass conservation under the mass correction
+(rhs_di.F90:697-717), and building blocks against independent computations.
+"""
+import ctypes
+import math
+import os
+import random
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from sunset_viscoelastic_b200.nodesets import NodeSet, WORKLOADS, initial_state, jittered_lattice
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def fixture_nodes():
+    d = np.load(os.path.join(HERE, "golden", "ipart_fixture.npz"))
+    b = d["box"]
+    ns = NodeSet(x=d["x"], y=d["y"], node_type=d["node_type"], nx=d["nx"], ny=d["ny"], s=d["s"],
+                 xmin=b[0], xmax=b[1], ymin=b[2], ymax=b[3], bcond=tuple(int(v) for v in d["bcond"]), gi=d["gi"])
+    return ns, dict(zip(["L_char", "U_char", "Re", "Wi", "beta", "epsPTT", "fenep_l2", "Mdiff", "Ma"],
+                        (float(v) for v in d["control"])))
+
+
+# ------------------------------------------------------------------------------------ blocks
+def test_svd_solve_matches_lapack():
+    rng = np.random.default_rng(1)
+    for n in (5, 14, 27, 44):
+        A = rng.standard_normal((n, n)) + n * np.eye(n)
+        b = rng.standard_normal(n)
+        x = b.copy()
+        O.lib().or_svd_solve(np.asfortranarray(A).ravel(order="F").copy(), n, x)
+        np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-10, atol=1e-12)
+
+
+def test_svd_solve_skips_zero_singular_values():
+    """svdlib.F90:286: an exactly singular system gives the minimum-norm-like solution
+    with the zero singular value skipped, not inf/nan."""
+    A = np.diag([2.0, 1.0, 0.0])
+    x = np.array([2.0, 3.0, 5.0])
+    O.lib().or_svd_solve(np.asfortranarray(A).ravel(order="F").copy(), 3, x)
+    assert np.all(np.isfinite(x))
+    np.testing.assert_allclose(x[:2], [1.0, 3.0])
+
+
+def test_monomials_and_hermite_abfs():
+    x, y = 0.37, -0.81
+    for order in (4, 6, 8, 10):
+        n = (order * order + 3 * order) // 2
+        mono, abf = np.zeros(n), np.zeros(n)
+        O.lib().or_monomials(order, x, y, mono)
+        O.lib().or_abfs(order, x, y, abf)
+        # probabilists' Hermite polynomials from numpy's HermiteE basis
+        from numpy.polynomial import hermite_e as He
+        m = 0
+        for d in range(1, order + 1):
+            for p in range(d, -1, -1):
+                q = d - p
+                assert mono[m] == pytest.approx(x ** p * y ** q / (math.factorial(p) * math.factorial(q)), rel=1e-13)
+                hp = He.hermeval(x, [0] * p + [1])
+                hq = He.hermeval(y, [0] * q + [1])
+                assert abf[m] == pytest.approx(hp * hq, rel=1e-12, abs=1e-12)
+                m += 1
+
+
+def test_wendland_c2():
+    h2 = 0.3 ** 2
+    for q in (0.0, 0.5, 1.0, 1.999, 2.0, 2.5):
+        w = O.lib().or_wab(q, h2)
+        expect = 7.0 / (4.0 * math.pi * h2) * (2 * q + 1) * (1 - q / 2) ** 4 if 0 < q <= 2 else 0.0
+        assert w == pytest.approx(expect, rel=1e-14, abs=1e-300)
+
+
+def test_correctly_rounded_pow4():
+    """The device's x^4 (and the restatement's set_pow_mode(True)) is the correctly
+    rounded power; glibc's pow(x, 4.0), which the reference calls, is not always."""
+    L = O.lib()
+    rnd = random.Random(5)
+    libm_wrong = 0
+    for _ in range(20000):
+        x = rnd.random()
+        cr = float(Fraction(x) ** 4)
+        assert L.or_pow4_cr(x) == cr
+        libm_wrong += L.or_pow4_libm(x) != cr
+    assert libm_wrong < 100
+
+
+# ------------------------------------------------------------------------------ neighbours
+def test_neighbour_search_matches_brute_force():
+    wl = WORKLOADS["periodic-di-o4-16k"]
+    ns = jittered_lattice(24, seed=9)
+    o = O.Oracle(form="di", order=4, h_over_s=wl.h_over_s).build_domain(ns)
+    o.find_neighbours()
+    nd = o.nodes()
+    cnt, cs, links = o.neighbours()
+    npfb = ns.n
+    x, y, h = nd["x"], nd["y"], nd["h"]
+    for i in range(0, npfb, 37):
+        d2 = (x[i] - x) ** 2 + (y[i] - y) ** 2
+        expect = set(np.nonzero(d2 <= (2 * h[i]) ** 2)[0] + 1)
+        got = links[i, :cnt[i]]
+        assert set(got) == expect
+        dist = d2[got - 1]
+        assert np.all(np.diff(dist) >= 0)             # sorted by distance (neighbours.F90:272-314)
+        assert got[0] == i + 1                         # self first
+
+
+def test_mirror_points_are_periodic_images():
+    ns = jittered_lattice(20, seed=3)
+    o = O.Oracle(form="di", order=4, h_over_s=1.5).build_domain(ns)
+    nd = o.nodes()
+    np_, npfb = o.sizes()[:2]
+    par = nd["irelation"][npfb:] - 1
+    dx = nd["x"][npfb:] - nd["x"][par]
+    dy = nd["y"][npfb:] - nd["y"][par]
+    assert np.all(np.isin(np.round(dx, 12), [-1.0, 0.0, 1.0]))
+    assert np.all(np.isin(np.round(dy, 12), [-1.0, 0.0, 1.0]))
+    assert np.all(nd["vrelation"][npfb:] == 1)
+
+
+# ------------------------------------------------------------------------- moment conditions
+@pytest.mark.parametrize("order,radius,tol", [(4, 3.0, 1e-11), (6, 4.2, 1e-9), (8, 4.72, 2e-6)])
+def test_weights_reproduce_polynomials(order, radius, tol):
+    """labf.F90:153-180: the d/dx, d/dy and Laplacian weights are exact on every monomial
+    up to the order.  In the stencil's scaled variables (r/h, weights times h or h^2) the
+    moment conditions read sum_k w_k m(r_k) = derivative of m at 0."""
+    ns = jittered_lattice(24, seed=11)
+    o = O.Oracle(form="di", order=order, h_over_s=radius / 2).build_domain(ns).setup()
+    nd = o.nodes()
+    cnt, cs, links = o.neighbours()
+    w = o.weights()
+    worst = 0.0
+    for i in range(0, ns.n, 53):
+        j = links[i, :cs[i]] - 1
+        h = nd["h_small"][i]
+        X, Y = (nd["x"][j] - nd["x"][i]) / h, (nd["y"][j] - nd["y"][i]) / h
+        wx, wy, wl = w["w_grad"][i, :cs[i], 0] * h, w["w_grad"][i, :cs[i], 1] * h, w["w_lap"][i, :cs[i]] * h * h
+        for d in range(1, order + 1):
+            for p in range(d, -1, -1):
+                q = d - p
+                m = X ** p * Y ** q
+                worst = max(worst, abs(wx @ m - ((p, q) == (1, 0))), abs(wy @ m - ((p, q) == (0, 1))),
+                            abs(wl @ m - 2.0 * ((p, q) in ((2, 0), (0, 2)))))
+    # the un-truncated SVD solve meets the conditions to cond(A)*eps, ~1e9*eps at order 8
+    print("order", order, "worst moment residual", worst)
+    assert worst < tol, worst
+
+
+def test_ipart_fixture_setup():
+    """The reference's own fixture with its default parameters (order 8, hovs 2.7)."""
+    ns, c = fixture_nodes()
+    o = O.Oracle(form="chl", order=8, Re=c["Re"], Wi=c["Wi"], beta=c["beta"], epsPTT=c["epsPTT"],
+                 fenep_l2=c["fenep_l2"], Mdiff=c["Mdiff"], Ma=c["Ma"]).build_domain(ns).setup()
+    np_, npfb, nb, nplink = o.sizes()
+    assert npfb == 4056 and nb == 0
+    cnt, cs, links = o.neighbours()
+    assert cnt.min() >= 44                # more neighbours than order-8 unknowns
+    assert nplink <= 2 * 4 * math.ceil(2.0 * 2.7) ** 2  # nplink bound of setup_domain.F90:50
+    w = o.weights()
+    assert np.all(np.isfinite(w["w_grad"])) and np.all(np.isfinite(w["w_hyp"]))
+    # node volumes tile the periodic box
+    assert abs(w["vol"].sum() / (2 * math.pi) ** 2 - 1.0) < 0.05
+
+
+@pytest.mark.parametrize("form,Wi,Mdiff,tol", [("di", 0.3, 1e-3, 1e-7), ("chl", 0.3, 1e-3, 1e-7), ("lc", 1.0, 0.0, 1e-5)])
+def test_kolmogorov_steady_state_is_a_fixed_point(form, Wi, Mdiff, tol):
+    """setup_flow.F90:224-229 with the forcing of rhs.F90:275 is an exact steady state of
+    the PDE; the discrete right-hand side must vanish to discretisation accuracy, in every
+    formulation (the log-conformation form has no polymer diffusion, so Mdiff = 0 there)."""
+    ns, c = fixture_nodes()
+    o = O.Oracle(form=form, order=8, Re=c["Re"], Wi=Wi, beta=c["beta"], epsPTT=c["epsPTT"],
+                 fenep_l2=c["fenep_l2"], Mdiff=Mdiff, Ma=c["Ma"], kolmogorov_forcing=1).build_domain(ns).setup()
+    x, y = ns.x, ns.y
+    u = np.cos(y)
+    v = np.zeros_like(y)
+    cxx = 1 + (Wi * Wi / (1 + Mdiff * Wi)) * (1 - np.cos(2 * y) / (1 + 4 * Mdiff * Wi))
+    cxy = -Wi * np.sin(y) / (1 + Mdiff * Wi)
+    o.set_state(np.ones(ns.n), u, v, cxx, cxy, np.ones(ns.n))
+    r = o.rhs()
+    scale = 1.0 / c["Re"]   # size of the balanced momentum terms
+    assert np.abs(r["rou"]).max() < tol * 100 * scale + tol
+    assert np.abs(r["rov"]).max() < tol * 100 * scale + tol
+    for k in ("xx", "xy", "yy"):
+        assert np.abs(r[k]).max() < 100 * tol, (k, np.abs(r[k]).max())
+    # and a perturbed state is not a fixed point (the check has teeth)
+    o.set_state(np.ones(ns.n), 1.1 * u, v, cxx, cxy, np.ones(ns.n))
+    assert np.abs(o.rhs()["rou"]).max() > 1e-4
+
+
+def test_mass_correction_conserves_mass():
+    """rhs_di.F90:697-717: after every step sum (rho - 1) vol = 0 to rounding."""
+    import dataclasses
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=32)
+    ns = wl.nodes()
+    o = O.for_workload(wl, ns).setup()
+    st = initial_state(ns)
+    st["ro"] = 1.0 + 0.01 * np.sin(2 * np.pi * ns.x)
+    o.set_state(**st)
+    dtc, dtp = o.set_tstep()
+    o.step(wl.cfl * min(dtc, dtp), 10)
+    vol = o.weights()["vol"]
+    m = float(np.sum((o.state()["ro"] - 1.0) * vol))
+    assert abs(m) < 1e-13
+
+
+def test_transforms_round_trip():
+    """conf_transforms.F90: c -> psi -> c for log-conformation and log-Cholesky."""
+    import dataclasses
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16)
+    ns = wl.nodes()
+    rng = np.random.default_rng(2)
+    a = 1 + rng.random(ns.n)
+    b = 0.3 * (rng.random(ns.n) - 0.5)
+    d = 1 + rng.random(ns.n)
+    for form in ("lc", "chl"):
+        o = O.Oracle(form=form, order=6, h_over_s=wl.h_over_s).build_domain(ns)
+        o.set_state(np.ones(ns.n), np.zeros(ns.n), np.zeros(ns.n), a, b, d)
+        s = o.state()
+        np.testing.assert_allclose(s["cxx"], a, rtol=1e-13)
+        np.testing.assert_allclose(s["cxy"], b, rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(s["cyy"], d, rtol=1e-13)
