@@ -138,6 +138,19 @@ int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *
 int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
                              double *bytes_per_launch);
 
+/* Allocation-free variant of sunset_kinetic_energy/sunset_mass; it has no counterpart in
+   the reference.  For callers that cannot allocate device memory (their arrays live in
+   their own device pool, and cudaMalloc could synchronise the device or exceed a memory
+   cap): they pass device arrays they own, ro, u, v, vol (npfb each, any consistent node
+   order) and out (2 doubles, device), and get out[0] = sum 0.5 ro (u^2+v^2) vol and
+   out[1] = sum ro vol.  The partial sums use a static device array sized for at most
+   4,194,304 nodes (256 KB per GPU, held until the process exits); larger npfb returns
+   SUNSET_ERR_SCOPE.  The first call on a device looks the array's address up and should
+   come before any stream capture.  Work is enqueued on `stream` (NULL: the default
+   stream).  All calls share the array, so calls that overlap on the GPU race. */
+int sunset_kinetic_energy_noalloc(int device, int npfb, const double *ro, const double *u, const double *v,
+                                  const double *vol, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,7 +28,7 @@ ABI_SYMBOLS = [
     "sunset_calc_laplacian", "sunset_calc_filtered_var", "sunset_calc_filter_term", "sunset_set_state",
     "sunset_get_state", "sunset_calc_all_rhs", "sunset_set_tstep", "sunset_step", "sunset_get_time",
     "sunset_set_time", "sunset_kinetic_energy", "sunset_mass", "sunset_synchronize", "sunset_run_host",
-    "sunset_time_stage_kernel", "sunset_step_timed",
+    "sunset_time_stage_kernel", "sunset_step_timed", "sunset_kinetic_energy_noalloc",
 ]
 
 
@@ -91,6 +91,8 @@ def load_library(build_if_missing: bool = True):
     L.sunset_run_host.argtypes = [P, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
     L.sunset_time_stage_kernel.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.sunset_step_timed.argtypes = [P, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.sunset_kinetic_energy_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
@@ -294,6 +296,16 @@ class Sunset:
         ms, by = C.c_double(), C.c_double()
         self._chk(self.L.sunset_time_stage_kernel(self.h, int(reps), C.byref(ms), C.byref(by)))
         return ms.value, by.value
+
+
+def kinetic_energy_noalloc(device, npfb, ro_ptr, u_ptr, v_ptr, vol_ptr, out_ptr, stream_ptr=None):
+    """sunset_kinetic_energy_noalloc on device arrays the caller owns (raw device pointers);
+    out receives (kinetic energy, mass).  Allocates nothing on the device."""
+    rc = load_library().sunset_kinetic_energy_noalloc(int(device), int(npfb), C.c_void_p(ro_ptr), C.c_void_p(u_ptr),
+                                                      C.c_void_p(v_ptr), C.c_void_p(vol_ptr), C.c_void_p(out_ptr),
+                                                      C.c_void_p(stream_ptr) if stream_ptr else None)
+    if rc != 0:
+        raise SunsetError(f"sunset_kinetic_energy_noalloc failed with code {rc}")
 
 
 def for_workload(wl, ns=None, precision="fp64", device=0, **over):
