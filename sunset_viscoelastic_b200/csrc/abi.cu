@@ -218,6 +218,8 @@ int sunset_find_neighbours(SunsetHandle *sh) {
     if (int rc = set_device(H)) return rc;
     int rc = find_neighbours_device(H);
     if (rc) return rc;
+    rc = build_halos(H);
+    if (rc) return rc;
     H->nbr_ok = true;
     return 0;
 }
@@ -282,7 +284,7 @@ int sunset_get_neighbours(SunsetHandle *sh, int *ij_count, int *ij_count_small, 
             for (int k = 0; k < nplink; k++) {
                 int v = 0;
                 if (k < cnt[i]) {
-                    int p = lpt[sptr[i >> 5] + (long long)k * kSlice + (i & 31)];
+                    int p = lpt[sell_at(sptr[i >> 5], k, i & 31)];
                     v = (p < n ? H->h_perm[p] : p) + 1;
                 }
                 ij_link[(size_t)r * nplink + k] = v;
@@ -311,7 +313,7 @@ int sunset_get_weights(SunsetHandle *sh, double *w_grad, double *w_lap, double *
             int i = H->h_iperm[r];
             for (int k = 0; k < nplink; k++) {
                 double v = 0.0;
-                if (k < cnt[i]) v = tmp[sptr[i >> 5] + (long long)k * kSlice + (i & 31)];
+                if (k < cnt[i]) v = tmp[sell_at(sptr[i >> 5], k, i & 31)];
                 dst[((size_t)r * nplink + k) * stride + comp] = v;
             }
         }

@@ -7,9 +7,9 @@
 //     as positions for the weight build; each link stores the internal index of the
 //     parent plus a 2-bit reflection code, so fields are never copied to ghosts.
 //   * Links are kept in sliced ELL: slices of 32 consecutive internal nodes, each padded
-//     to its own width; link k of node i sits at slice_ptr[i/32] + 32*k + i%32, so a warp
-//     reading link k of its 32 nodes issues one coalesced access.  Padding has weight 0
-//     and points at node 0.
+//     to its own (even) width; links k = 2m, 2m+1 of node i sit next to each other at
+//     slice_ptr[i/32] + 64 m + 2 (i%32) (sell_at), so a warp reading link pair m of its 32
+//     nodes issues one coalesced 512-byte access.  Padding has weight 0 and points at node 0.
 //   * Fields are structure-of-arrays FP64 (or FP32 in the mixed path).
 #pragma once
 
@@ -27,6 +27,9 @@ constexpr double kPi = 3.141592653589793238462643383279502884197;
 constexpr double kSs = 2.0;  // stencil support in units of h, common_parameter.F90:68
 constexpr int kSlice = 32;
 constexpr int kLinkMask = 0x3fffffff;  // low 30 bits: internal parent index
+constexpr int kTileSlices = 8;         // slices per thread block of the staged stencil kernels
+constexpr int kTile = kTileSlices * 32;
+constexpr int kLocMask = 0x3fff;       // low 14 bits of a local link: position in the tile's halo
 
 // RK3(2)4[2R+]C, common_parameter.F90:74-94
 #define SUNSET_RK_A21 (11847461282814.0 / 36547543011857.0)
@@ -42,6 +45,13 @@ constexpr int kLinkMask = 0x3fffffff;  // low 30 bits: internal parent index
 #define SUNSET_RK_BH4 (-69544964788955.0 / 30262026368149.0)
 
 inline int nsize_for(int k) { return (k * k + 3 * k) / 2; }  // labf.F90:56
+
+// Position of link k of lane `lane` in the slice stored from `base`.  Links are stored in
+// pairs, so one 16-byte load brings links 2m and 2m+1 of a node and a warp's pair load is
+// 512 contiguous bytes; slice widths are even.
+__host__ __device__ __forceinline__ long long sell_at(long long base, int k, int lane) {
+    return base + ((long long)(k >> 1) << 6) + (lane << 1) + (k & 1);
+}
 
 // Scalars the step kernels share on the device (one per handle).
 struct DevScalars {
@@ -102,6 +112,11 @@ struct Handle {
     int *lpt = nullptr;                        // SELL: point id (ghost-aware), for setup/export
     int *lidx = nullptr;                       // SELL: parent | vrel code << 30
     bool has_mirrors = false;
+    // tiles of kTileSlices slices: the sorted set of nodes their links reach (the halo) and,
+    // per link, the position of its parent in that set | reflection code << 14
+    int ntiles = 0, halo_max = 0;
+    int *halo_ptr = nullptr, *halo = nullptr;
+    uint16_t *lloc = nullptr;
 
     // ---- weights (SELL, FP64) ----
     double *wx = nullptr, *wy = nullptr, *wl = nullptr, *wh = nullptr;
@@ -152,6 +167,7 @@ int build_domain_device(Handle *H, const std::vector<double> &x, const std::vect
                         const std::vector<double> &h, const std::vector<double> &hs,
                         const std::vector<double> &s, const std::vector<int> &type);
 int find_neighbours_device(Handle *H);
+int build_halos(Handle *H);
 int labf_weights_device(Handle *H);
 int labf_sums_device(Handle *H);
 int filter_coefficients_device(Handle *H);

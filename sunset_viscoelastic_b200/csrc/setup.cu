@@ -234,12 +234,12 @@ __global__ void k_fill_sell(int npfb, int nslices, const long long *rowptr, cons
     int sl = i >> 5;
     if (sl >= nslices) return;
     int lane = i & 31;
-    long long base = slice_ptr[sl] + lane;
+    long long base = slice_ptr[sl];
     int w = slice_w[sl];
     long long b = i < npfb ? rowptr[i] : 0;
     int cnt = i < npfb ? (int)(rowptr[i + 1] - b) : 0;
     for (int k = 0; k < w; k++) {
-        long long o = base + (long long)k * kSlice;
+        long long o = sell_at(base, k, lane);
         if (k < cnt) {
             int p = opt[b + k];
             lpt[o] = p;
@@ -412,6 +412,8 @@ int find_neighbours_device(Handle *H) {
             w = hcount[i] > w ? hcount[i] : w;
             ws = hsmall[i] > ws ? hsmall[i] : ws;
         }
+        w = (w + 1) & ~1;  // even widths: links are stored in pairs (sell_at)
+        ws = (ws + 1) & ~1;
         sw[sl] = w;
         sws[sl] = ws;
         sptr[sl + 1] = sptr[sl] + (long long)w * kSlice;
@@ -440,6 +442,82 @@ int find_neighbours_device(Handle *H) {
     for (void *p : {(void *)cid, (void *)cid2, (void *)pid, (void *)pid2, (void *)cstart, (void *)cend, (void *)count,
                     (void *)cnt64, (void *)rowptr, (void *)opt, (void *)or2, (void *)mflag})
         dfree(H, p);
+    return 0;
+}
+
+}  // namespace sunset
+
+// ---------------------------------------------------------------------------------------
+// Halo lists of the staged stencil kernels.  A thread block owns kTileSlices consecutive
+// slices (kTile nodes); its halo is the sorted set of parents its links reach.  The
+// kernels load the halo's fields once into shared memory (consecutive halo entries are
+// mostly consecutive nodes in Morton order, so these loads coalesce) and every link then
+// reads shared memory through a 16-bit position.  Built on the host once per node set.
+// ---------------------------------------------------------------------------------------
+#include <algorithm>
+#include <thread>
+
+namespace sunset {
+
+int build_halos(Handle *H) {
+    const int n = H->npfb, nsl = H->nslices;
+    const long long L = H->nlinks_sell;
+    std::vector<int> lidx(L), cnt(n), sw(nsl);
+    std::vector<long long> sptr(nsl + 1);
+    SUNSET_CUDA(H, cudaMemcpy(lidx.data(), H->lidx, L * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cnt.data(), H->cnt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sw.data(), H->slice_w, nsl * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sptr.data(), H->slice_ptr, (nsl + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    const int nt = (nsl + kTileSlices - 1) / kTileSlices;
+    std::vector<std::vector<int>> halos(nt);
+    std::vector<uint16_t> loc(L, 0);
+    unsigned nthr = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < nthr; w++) {
+        pool.emplace_back([&, w]() {
+            for (int t = (int)w; t < nt; t += (int)nthr) {
+                std::vector<int> &hv = halos[t];
+                for (int sl = t * kTileSlices; sl < std::min(nsl, (t + 1) * kTileSlices); sl++)
+                    for (int lane = 0; lane < kSlice; lane++) {
+                        int i = sl * kSlice + lane;
+                        if (i >= n) break;
+                        for (int k = 0; k < cnt[i]; k++) hv.push_back(lidx[sell_at(sptr[sl], k, lane)] & kLinkMask);
+                    }
+                std::sort(hv.begin(), hv.end());
+                hv.erase(std::unique(hv.begin(), hv.end()), hv.end());
+                for (int sl = t * kTileSlices; sl < std::min(nsl, (t + 1) * kTileSlices); sl++)
+                    for (int lane = 0; lane < kSlice; lane++) {
+                        int i = sl * kSlice + lane;
+                        int c = i < n ? cnt[i] : 0;
+                        for (int k = 0; k < sw[sl]; k++) {
+                            long long o = sell_at(sptr[sl], k, lane);
+                            if (k >= c) { loc[o] = 0; continue; }
+                            int p = lidx[o] & kLinkMask, code = (unsigned)lidx[o] >> 30;
+                            int pos = (int)(std::lower_bound(hv.begin(), hv.end(), p) - hv.begin());
+                            loc[o] = (uint16_t)(pos | (code << 14));
+                        }
+                    }
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
+    std::vector<int> hptr(nt + 1);
+    hptr[0] = 0;
+    int hmax = 0;
+    for (int t = 0; t < nt; t++) {
+        hptr[t + 1] = hptr[t] + (int)halos[t].size();
+        hmax = std::max(hmax, (int)halos[t].size());
+    }
+    if (hmax > kLocMask + 1) return set_err(H, SUNSET_ERR_SCOPE, "tile halo of %d nodes exceeds the 14-bit local index", hmax);
+    std::vector<int> hall(hptr[nt]);
+    for (int t = 0; t < nt; t++) std::copy(halos[t].begin(), halos[t].end(), hall.begin() + hptr[t]);
+    if (dalloc(H, &H->halo_ptr, nt + 1) || dalloc(H, &H->halo, hall.size()) || dalloc(H, &H->lloc, L))
+        return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemcpy(H->halo_ptr, hptr.data(), hptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->halo, hall.data(), hall.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->lloc, loc.data(), L * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    H->ntiles = nt;
+    H->halo_max = hmax;
     return 0;
 }
 

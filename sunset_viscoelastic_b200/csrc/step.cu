@@ -27,6 +27,9 @@ struct StageArgs {
     const long long *slice_ptr;
     const int *slice_ws, *slice_w;
     const int *lidx;
+    const uint16_t *lloc;
+    const int *halo_ptr, *halo;
+    int hmax;
     const double *wx, *wy, *wl, *wh;
     const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
     Fields in, out;
@@ -36,8 +39,6 @@ struct StageArgs {
     int stage;  // 0..3; 4 = rhs only
 };
 
-__device__ __forceinline__ double fetch(const double *p, int j) { return __ldg(p + j); }
-
 // Reflection codes of a ghost link: 1 -> vrelation 2 (x mirror: u and the xy component
 // change sign), 2 -> vrelation 3 (y mirror: v and xy), 3 -> vrelation 4 (u and v).
 __device__ __forceinline__ void reflect(int code, double &uj, double &vj, double &xyj) {
@@ -46,34 +47,75 @@ __device__ __forceinline__ void reflect(int code, double &uj, double &vj, double
     if (code == 1 || code == 2) xyj = -xyj;
 }
 
-template <int FORM>
-__device__ __forceinline__ void gather_stage(const StageArgs &A, int i, Grads &g) {
-    const long long base = A.slice_ptr[i >> 5] + (i & 31);
-    const int ws = A.slice_ws[i >> 5];
+// Fields a stage gathers from its neighbours, in shared-memory order:
+//   0 ro, 1 u, 2 v, then DI: cxx cxy cyy; LC: cxx cxy cyy psixx psixy psiyy;
+//   CHL: psixx psixy psiyy (+ cxx cxy cyy with polymer diffusion).
+__host__ __device__ constexpr int ngather(int form, bool md) {
+    return form == SUNSET_FORM_DI ? 6 : form == SUNSET_FORM_LC ? 9 : form == SUNSET_FORM_CHL ? (md ? 9 : 6) : 3;
+}
+
+template <int FORM, bool MD>
+__device__ __forceinline__ const double *gather_src(const Fields &F, int f) {
+    if (f == 0) return F.ro;
+    if (f == 1) return F.u;
+    if (f == 2) return F.v;
+    if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
+        if (f <= 5) return F.c[f - 3];
+        return F.q[f - 6];
+    }
+    if (f <= 5) return F.q[f - 3];
+    return F.c[f - 6];
+}
+
+// The block's halo (fields of every node its links reach) into shared memory, laid out
+// field-major with stride hmax.  All threads of the block take part.
+template <int NG, typename SRC>
+__device__ __forceinline__ void load_halo(const StageArgs &A, double *sm, SRC src) {
+    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
+    const int hm = A.hmax;
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        const int node = __ldg(A.halo + hb + h);
+#pragma unroll
+        for (int f = 0; f < NG; f++) sm[f * hm + h] = __ldg(src(f) + node);
+    }
+    __syncthreads();
+}
+
+// Stencil sums of one node over its small links, sum form of derivatives.F90:36-46,
+// neighbours read from the block's shared-memory halo.
+template <int FORM, bool MD>
+__device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const double *sm, Grads &g) {
+    const int hm = A.hmax;
+    const long long pb = (A.slice_ptr[i >> 5] >> 1) + (i & 31);  // link pair m of this node: pb + 32 m
+    const int npair = A.slice_ws[i >> 5] >> 1;
     const Fields &F = A.in;
     double s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
     double s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
     double s_pxx_x = 0, s_pxx_y = 0, s_pxy_x = 0, s_pxy_y = 0, s_pyy_x = 0, s_pyy_y = 0;
     double s_lxx = 0, s_lxy = 0, s_lyy = 0;
     const bool mir = cK.has_mirrors;
-    const bool mdiff = cK.mdiff_on;
     const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
-    for (int k = 0; k < ws; k++) {
-        const long long o = base + (long long)k * kSlice;
-        const int lk = __ldg(A.lidx + o);
-        const int j = lk & kLinkMask;
-        const double wxk = __ldg(A.wx + o), wyk = __ldg(A.wy + o), wlk = __ldg(A.wl + o);
-        double roj = fetch(F.ro, j), uj = fetch(F.u, j), vj = fetch(F.v, j);
-        double dxy = 0.0;
-        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) dxy = fetch(F.c[1], j);
-        double pxy = 0.0;
-        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) pxy = fetch(F.q[1], j);
+    const double2 *WX = reinterpret_cast<const double2 *>(A.wx), *WY = reinterpret_cast<const double2 *>(A.wy);
+    const double2 *WL = reinterpret_cast<const double2 *>(A.wl);
+    const unsigned *LL = reinterpret_cast<const unsigned *>(A.lloc);
+    auto link = [&](int lk, double wxk, double wyk, double wlk) {
+        const int j = lk & kLocMask;
+        double roj = sm[j], uj = sm[hm + j], vj = sm[2 * hm + j];
+        double cxxj = 0.0, cxyj = 0.0, cyyj = 0.0, pxxj = 0.0, pxyj = 0.0, pyyj = 0.0;
+        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
+            cxxj = sm[3 * hm + j]; cxyj = sm[4 * hm + j]; cyyj = sm[5 * hm + j];
+        }
+        if (FORM == SUNSET_FORM_LC) {
+            pxxj = sm[6 * hm + j]; pxyj = sm[7 * hm + j]; pyyj = sm[8 * hm + j];
+        }
+        if (FORM == SUNSET_FORM_CHL) {
+            pxxj = sm[3 * hm + j]; pxyj = sm[4 * hm + j]; pyyj = sm[5 * hm + j];
+            if (MD) { cxxj = sm[6 * hm + j]; cxyj = sm[7 * hm + j]; cyyj = sm[8 * hm + j]; }
+        }
         if (mir) {
-            int code = (unsigned)lk >> 30;
-            double t = pxy;
-            reflect(code, uj, vj, dxy);
-            if (code == 1 || code == 2) t = -t;
-            pxy = t;
+            const int code = lk >> 14;
+            reflect(code, uj, vj, cxyj);
+            if (code == 1 || code == 2) pxyj = -pxyj;
         }
         s_ro_x = s_ro_x + roj * wxk;
         s_ro_y = s_ro_y + roj * wyk;
@@ -84,38 +126,34 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, Grads &g
         s_v_y = s_v_y + vj * wyk;
         s_lv = s_lv + vj * wlk;
         if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
-            double cxxj = fetch(F.c[0], j), cyyj = fetch(F.c[2], j);
             s_cxx_x = s_cxx_x + cxxj * wxk;
             if (full) s_cxx_y = s_cxx_y + cxxj * wyk;
-            s_cxy_x = s_cxy_x + dxy * wxk;
-            s_cxy_y = s_cxy_y + dxy * wyk;
+            s_cxy_x = s_cxy_x + cxyj * wxk;
+            s_cxy_y = s_cxy_y + cxyj * wyk;
             if (full) s_cyy_x = s_cyy_x + cyyj * wxk;
             s_cyy_y = s_cyy_y + cyyj * wyk;
-            if (FORM == SUNSET_FORM_DI && mdiff) {
-                s_lxx = s_lxx + cxxj * wlk;
-                s_lxy = s_lxy + dxy * wlk;
-                s_lyy = s_lyy + cyyj * wlk;
-            }
         }
         if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {
-            double pxxj = fetch(F.q[0], j), pyyj = fetch(F.q[2], j);
             s_pxx_x = s_pxx_x + pxxj * wxk;
             s_pxx_y = s_pxx_y + pxxj * wyk;
-            s_pxy_x = s_pxy_x + pxy * wxk;
-            s_pxy_y = s_pxy_y + pxy * wyk;
+            s_pxy_x = s_pxy_x + pxyj * wxk;
+            s_pxy_y = s_pxy_y + pxyj * wyk;
             s_pyy_x = s_pyy_x + pyyj * wxk;
             s_pyy_y = s_pyy_y + pyyj * wyk;
         }
-        if (FORM == SUNSET_FORM_CHL && mdiff) {
-            double cxxj = fetch(F.c[0], j), cyyj = fetch(F.c[2], j), cxyj = fetch(F.c[1], j);
-            if (mir) {
-                int code = (unsigned)lk >> 30;
-                if (code == 1 || code == 2) cxyj = -cxyj;
-            }
+        if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) {
             s_lxx = s_lxx + cxxj * wlk;
             s_lxy = s_lxy + cxyj * wlk;
             s_lyy = s_lyy + cyyj * wlk;
         }
+    };
+    // links in order k = 2m, 2m+1: the sums keep the reference's order
+    for (int m = 0; m < npair; m++) {
+        const long long o = pb + ((long long)m << 5);
+        const double2 wx2 = __ldg(WX + o), wy2 = __ldg(WY + o), wl2 = __ldg(WL + o);
+        const unsigned l2 = __ldg(LL + o);
+        link((int)(l2 & 0xffffu), wx2.x, wy2.x, wl2.x);
+        link((int)(l2 >> 16), wx2.y, wy2.y, wl2.y);
     }
     if (i >= cK.npfb) return;
     const double gx = A.gsx[i], gy = A.gsy[i], ls = A.lsum[i];
@@ -139,11 +177,6 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, Grads &g
         g.cxy_y = s_cxy_y - cxy * gy;
         if (full) g.cyy_x = s_cyy_x - cyy * gx;
         g.cyy_y = s_cyy_y - cyy * gy;
-        if (FORM == SUNSET_FORM_DI && mdiff) {
-            g.lapcxx = s_lxx - cxx * ls;
-            g.lapcxy = s_lxy - cxy * ls;
-            g.lapcyy = s_lyy - cyy * ls;
-        }
     }
     if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {
         const double pxx = F.q[0][i], pxy = F.q[1][i], pyy = F.q[2][i];
@@ -154,7 +187,7 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, Grads &g
         g.pyy_x = s_pyy_x - pyy * gx;
         g.pyy_y = s_pyy_y - pyy * gy;
     }
-    if (FORM == SUNSET_FORM_CHL && mdiff) {
+    if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) {
         g.lapcxx = s_lxx - F.c[0][i] * ls;
         g.lapcxy = s_lxy - F.c[1][i] * ls;
         g.lapcyy = s_lyy - F.c[2][i] * ls;
@@ -202,10 +235,19 @@ __device__ __forceinline__ void block_min_bits(unsigned long long v, unsigned lo
     }
 }
 
-// One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).
-template <int FORM>
-__global__ void __launch_bounds__(128) k_stage(StageArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Resident blocks per SM the stage kernel is compiled for: the log-conformation and direct
+// forms keep their longer epilogues in registers at 3 blocks (85 registers); the
+// Cholesky form runs best at 4 (64 registers).  Measured on B200.
+__host__ __device__ constexpr int stage_min_blocks(int form) { return form == SUNSET_FORM_CHL ? 4 : 3; }
+
+// One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).  One
+// block per tile of kTile nodes; the tile's halo is staged in shared memory first.
+template <int FORM, bool MD>
+__global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageArgs A) {
+    extern __shared__ double smem[];
+    constexpr int NG = ngather(FORM, MD);
+    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD>(A.in, f); });
+    const int i = blockIdx.x * kTile + threadIdx.x;
     const int stage = A.stage;
     if (stage == 0 && i == 0) {
         A.sc->cfl_bits = 0x7ff0000000000000ull;
@@ -213,7 +255,7 @@ __global__ void __launch_bounds__(128) k_stage(StageArgs A) {
     }
     Grads g;
     bool active = (i >> 5) < cK.nslices;
-    if (active) gather_stage<FORM>(A, i, g);
+    if (active) gather_stage<FORM, MD>(A, i, smem, g);
     active = active && i < cK.npfb;
     unsigned long long emax_bits = 0;
     if (active) {
@@ -231,47 +273,50 @@ __global__ void __launch_bounds__(128) k_stage(StageArgs A) {
             rhs_c_lc(cK, n, g, first, r);
         } else { r.xx = r.xy = r.yy = r.zz = 0.0; }
         const double rr[7] = {r.ro, r.rou, r.rov, r.xx, r.xy, r.yy, r.zz};
+        constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
         if (stage == 4) {
+#pragma unroll
             for (int f = 0; f < 7; f++) A.rhs[f][i] = rr[f];
         } else {
             const double U[7] = {F.ro[i], F.rou[i], F.rov[i], F.q[0][i], F.q[1][i], F.q[2][i], F.q[3][i]};
             const double dt = A.sc->dt;
-            const double a[3] = {SUNSET_RK_A21, SUNSET_RK_A32, SUNSET_RK_A43};
-            const double b[4] = {SUNSET_RK_B1, SUNSET_RK_B2, SUNSET_RK_B3, SUNSET_RK_B4};
-            const double bh[4] = {SUNSET_RK_BH1, SUNSET_RK_BH2, SUNSET_RK_BH3, SUNSET_RK_BH4};
-            const double RKb = dt * b[stage], RKbmbh = dt * (b[stage] - bh[stage]);
-            const int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+            const double a = stage == 0 ? SUNSET_RK_A21 : stage == 1 ? SUNSET_RK_A32 : SUNSET_RK_A43;
+            const double b = stage == 0 ? SUNSET_RK_B1 : stage == 1 ? SUNSET_RK_B2 : stage == 2 ? SUNSET_RK_B3 : SUNSET_RK_B4;
+            const double bh = stage == 0 ? SUNSET_RK_BH1 : stage == 1 ? SUNSET_RK_BH2 : stage == 2 ? SUNSET_RK_BH3 : SUNSET_RK_BH4;
+            const double RKb = dt * b, RKbmbh = dt * (b - bh);
             double Un[7];
+#pragma unroll
+            for (int f = 0; f < 7; f++) Un[f] = U[f];
             if (stage < 3) {
-                const double RKa = dt * a[stage];
+                const double RKa = dt * a;
+#pragma unroll
                 for (int f = 0; f < nf; f++) {
-                    double S = (stage == 0) ? U[f] : A.reg[f][i];
-                    double E = (stage == 0) ? 0.0 : A.eacc[f][i];
+                    const double S = (stage == 0) ? U[f] : A.reg[f][i];
+                    const double E = (stage == 0) ? 0.0 : A.eacc[f][i];
                     Un[f] = S + RKa * rr[f];
                     A.reg[f][i] = S + RKb * rr[f];
                     A.eacc[f][i] = E + RKbmbh * rr[f];
                 }
             } else {
-                const double norms[7] = {cK.ero_norm, cK.erou_norm, cK.erou_norm, cK.exx_norm,
-                                         cK.exx_norm, cK.exx_norm, cK.exx_norm};
                 double en = 0.0;
+#pragma unroll
                 for (int f = 0; f < nf; f++) {
+                    const double norm = f == 0 ? cK.ero_norm : f < 3 ? cK.erou_norm : cK.exx_norm;
                     Un[f] = A.reg[f][i] + RKb * rr[f];
-                    double E = A.eacc[f][i] + RKbmbh * rr[f];
-                    double t = fabs(E) * norms[f];
+                    const double E = A.eacc[f][i] + RKbmbh * rr[f];
+                    const double t = fabs(E) * norm;
                     en = (t > en) ? t : en;
                     if (t != t) en = t;
                 }
                 emax_bits = dbits(en);
             }
-            for (int f = nf; f < 7; f++) Un[f] = U[f];
             const Fields &O = A.out;
             O.ro[i] = Un[0]; O.rou[i] = Un[1]; O.rov[i] = Un[2];
             if (FORM != SUNSET_FORM_NEWT) {
                 O.q[0][i] = Un[3]; O.q[1][i] = Un[4]; O.q[2][i] = Un[5]; O.q[3][i] = Un[6];
             }
             if (stage < 3) {  // get_velocity_from_momentum, get_c_from_psi (step.F90:514-567)
-                double ooro = 1.0 / Un[0];
+                const double ooro = 1.0 / Un[0];
                 O.u[i] = Un[1] * ooro;
                 O.v[i] = Un[2] * ooro;
                 if (FORM == SUNSET_FORM_LC) {
@@ -292,61 +337,73 @@ __global__ void __launch_bounds__(128) k_stage(StageArgs A) {
 // filter_variables (rhs_di.F90:667-720; rhs.F90:792-900; rhs_lc.F90:818-893): the
 // hyperviscous filter of each evolved field plus the mass-correction partial sums.
 template <int FORM>
-__global__ void __launch_bounds__(128) k_filter(StageArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+__global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
+    extern __shared__ double smem[];
+    constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    const Fields &F = A.in;
+    load_halo<nf>(A, smem, [&](int f) -> const double * {
+        return f == 0 ? F.ro : f == 1 ? F.rou : f == 2 ? F.rov : F.q[f - 3];
+    });
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    const int hm = A.hmax;
     double part = 0.0;
     if ((i >> 5) < cK.nslices) {
-        const long long base = A.slice_ptr[i >> 5] + (i & 31);
-        const int w = A.slice_w[i >> 5];
-        const Fields &F = A.in;
-        const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
+        const long long pb = (A.slice_ptr[i >> 5] >> 1) + (i & 31);
+        const int npair = A.slice_w[i >> 5] >> 1;
         double t[7] = {0, 0, 0, 0, 0, 0, 0};
         const bool mir = cK.has_mirrors;
-        for (int k = 0; k < w; k++) {
-            const long long o = base + (long long)k * kSlice;
-            const int lk = __ldg(A.lidx + o);
-            const int j = lk & kLinkMask;
-            const double whk = __ldg(A.wh + o);
+        const double2 *WH = reinterpret_cast<const double2 *>(A.wh);
+        const unsigned *LL = reinterpret_cast<const unsigned *>(A.lloc);
+        auto link = [&](int lk, double whk) {
+            const int j = lk & kLocMask;
             double v[7];
 #pragma unroll
-            for (int f = 0; f < 7; f++)
-                if (f < nf) v[f] = fetch(src[f], j);
+            for (int f = 0; f < nf; f++) v[f] = smem[f * hm + j];
             if (mir) {
-                int code = (unsigned)lk >> 30;
-                reflect(code, v[1], v[2], v[4]);
+                double dummy = 0.0;
+                const int code = lk >> 14;
+                reflect(code, v[1], v[2], nf > 4 ? v[4] : dummy);
             }
 #pragma unroll
-            for (int f = 0; f < 7; f++)
-                if (f < nf) t[f] = t[f] + v[f] * whk;
+            for (int f = 0; f < nf; f++) t[f] = t[f] + v[f] * whk;
+        };
+        for (int m = 0; m < npair; m++) {
+            const long long o = pb + ((long long)m << 5);
+            const double2 wh2 = __ldg(WH + o);
+            const unsigned l2 = __ldg(LL + o);
+            link((int)(l2 & 0xffffu), wh2.x);
+            link((int)(l2 >> 16), wh2.y);
         }
         if (i < cK.npfb) {
             const double hs = A.hsum[i];
+            const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
             double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
+            double rof = 0.0;
 #pragma unroll
             for (int f = 0; f < 7; f++) {
                 if (f < nf) {
-                    double p = src[f][i];
-                    dst[f][i] = p + (t[f] - p * hs);
-                } else if (f >= 3 && FORM != SUNSET_FORM_NEWT) {
+                    const double p = src[f][i];
+                    const double r = p + (t[f] - p * hs);
+                    dst[f][i] = r;
+                    if (f == 0) rof = r;
+                } else if (FORM != SUNSET_FORM_NEWT) {
                     dst[f][i] = src[f][i];
                 }
             }
-            double rof = src[0][i] + (t[0] - src[0][i] * hs);
             part = (rof - cK.rho_char) * A.vol[i];
         }
     }
     // deterministic two-level sum: fixed tree in the block, fixed order over blocks
-    __shared__ double sm[128];
-    sm[threadIdx.x] = part;
+    __shared__ double red[kTile];
+    red[threadIdx.x] = part;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+        if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
         __syncthreads();
     }
     __shared__ bool last;
     if (threadIdx.x == 0) {
-        A.partials[blockIdx.x] = sm[0];
+        A.partials[blockIdx.x] = red[0];
         __threadfence();
         unsigned int prev = atomicAdd(&A.sc->done_ctr, 1u);
         last = (prev == gridDim.x - 1);
@@ -356,14 +413,14 @@ __global__ void __launch_bounds__(128) k_filter(StageArgs A) {
         __threadfence();
         double acc = 0.0;
         for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc = acc + ((volatile double *)A.partials)[b];
-        sm[threadIdx.x] = acc;
+        red[threadIdx.x] = acc;
         __syncthreads();
         for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-            if ((int)threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+            if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
             __syncthreads();
         }
         if (threadIdx.x == 0) {
-            A.sc->dro = cK.mcorr ? sm[0] / A.sc->tv : 0.0;
+            A.sc->dro = cK.mcorr ? red[0] / A.sc->tv : 0.0;
             A.sc->done_ctr = 0;
         }
     }
@@ -457,11 +514,11 @@ __global__ void k_tstep_fold(DevScalars *sc) {
 __global__ void k_op_grad_lap(StageArgs A, const double *phi, double *gx, double *gy, double *lap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if ((i >> 5) >= cK.nslices) return;
-    const long long base = A.slice_ptr[i >> 5] + (i & 31);
+    const long long base = A.slice_ptr[i >> 5];
     const int ws = A.slice_ws[i >> 5];
     double sx = 0.0, sy = 0.0, sl = 0.0;
     for (int k = 0; k < ws; k++) {
-        const long long o = base + (long long)k * kSlice;
+        const long long o = sell_at(base, k, i & 31);
         const int j = __ldg(A.lidx + o) & kLinkMask;
         const double pj = phi[j];
         sx = sx + pj * __ldg(A.wx + o);
@@ -478,11 +535,11 @@ __global__ void k_op_grad_lap(StageArgs A, const double *phi, double *gx, double
 __global__ void k_op_filter(StageArgs A, const double *phi, double *out, int term_only) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if ((i >> 5) >= cK.nslices) return;
-    const long long base = A.slice_ptr[i >> 5] + (i & 31);
+    const long long base = A.slice_ptr[i >> 5];
     const int w = A.slice_w[i >> 5];
     double t = 0.0;
     for (int k = 0; k < w; k++) {
-        const long long o = base + (long long)k * kSlice;
+        const long long o = sell_at(base, k, i & 31);
         const int j = __ldg(A.lidx + o) & kLinkMask;
         t = t + phi[j] * __ldg(A.wh + o);
     }
@@ -597,6 +654,10 @@ StageArgs make_args(Handle *H, int from, int stage) {
     A.slice_ws = H->slice_ws;
     A.slice_w = H->slice_w;
     A.lidx = H->lidx;
+    A.lloc = H->lloc;
+    A.halo_ptr = H->halo_ptr;
+    A.halo = H->halo;
+    A.hmax = H->halo_max;
     A.wx = H->wx; A.wy = H->wy; A.wl = H->wl; A.wh = H->wh;
     A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum; A.hsum = H->hsum; A.vol = H->vol;
     A.py_node = H->py;
@@ -645,34 +706,79 @@ int upload_consts(Handle *H) {
     return 0;
 }
 
+constexpr size_t kMaxStageSmem = 200 * 1024;
+
+// Opt the staged kernels into large dynamic shared memory on the handle's device.
+int set_smem_attributes(Handle *H) {
+#define SUNSET_SMEM_ATTR(K) SUNSET_CUDA(H, cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem))
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false>));
+    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_DI>);
+    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_CHL>);
+    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_LC>);
+    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_NEWT>);
+#undef SUNSET_SMEM_ATTR
+    return 0;
+}
+
+template <int FORM, bool MD>
+int launch_stage(Handle *H, const StageArgs &A) {
+    const size_t smem = (size_t)ngather(FORM, MD) * H->halo_max * sizeof(double);
+    if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
+    k_stage<FORM, MD><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    return 0;
+}
+
+int launch_stage_any(Handle *H, const StageArgs &A) {
+    const bool md = H->cfg.Mdiff != 0.0;
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI: return md ? launch_stage<SUNSET_FORM_DI, true>(H, A) : launch_stage<SUNSET_FORM_DI, false>(H, A);
+    case SUNSET_FORM_CHL: return md ? launch_stage<SUNSET_FORM_CHL, true>(H, A) : launch_stage<SUNSET_FORM_CHL, false>(H, A);
+    case SUNSET_FORM_LC: return launch_stage<SUNSET_FORM_LC, false>(H, A);
+    default: return launch_stage<SUNSET_FORM_NEWT, false>(H, A);
+    }
+}
+
 template <int FORM>
-void launch_step_kernels(Handle *H, int from, int pid) {
+int launch_filter(Handle *H, const StageArgs &A) {
+    constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    const size_t smem = (size_t)nf * H->halo_max * sizeof(double);
+    if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
+    k_filter<FORM><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    return 0;
+}
+
+template <int FORM>
+int launch_step_kernels(Handle *H, int from, int pid) {
     const int TB = 128;
-    const int nthr = H->nslices * kSlice;
-    const int nblk = (nthr + TB - 1) / TB;
     cudaStream_t st = H->stream;
     if (pid) k_pid<<<1, 1, 0, st>>>(H->dsc);
     int b = from;
     for (int s = 0; s < 4; s++) {
         StageArgs A = make_args(H, b, s);
-        k_stage<FORM><<<nblk, TB, 0, st>>>(A);
+        if (int rc = launch_stage_any(H, A)) return rc;
         b ^= 1;
     }
     StageArgs F = make_args(H, b, 5);
-    k_filter<FORM><<<nblk, TB, 0, st>>>(F);
+    if (int rc = launch_filter<FORM>(H, F)) return rc;
     b ^= 1;
     StageArgs Z = make_args(H, b ^ 1, 5);  // in = filter input, out = filtered buffer
     const int fb = (H->npfb + TB - 1) / TB;
     k_finalize<FORM><<<fb, TB, 0, st>>>(Z, 1);
     k_tstep<<<fb, TB, 0, st>>>(H->buf[b].u, H->buf[b].v, H->buf[b].ro, H->sp, H->ntype, H->npfb, H->dsc);
+    return 0;
 }
 
-void launch_step(Handle *H, int from, int pid) {
+int launch_step(Handle *H, int from, int pid) {
     switch (H->cfg.form) {
-    case SUNSET_FORM_DI: launch_step_kernels<SUNSET_FORM_DI>(H, from, pid); break;
-    case SUNSET_FORM_CHL: launch_step_kernels<SUNSET_FORM_CHL>(H, from, pid); break;
-    case SUNSET_FORM_LC: launch_step_kernels<SUNSET_FORM_LC>(H, from, pid); break;
-    default: launch_step_kernels<SUNSET_FORM_NEWT>(H, from, pid); break;
+    case SUNSET_FORM_DI: return launch_step_kernels<SUNSET_FORM_DI>(H, from, pid);
+    case SUNSET_FORM_CHL: return launch_step_kernels<SUNSET_FORM_CHL>(H, from, pid);
+    case SUNSET_FORM_LC: return launch_step_kernels<SUNSET_FORM_LC>(H, from, pid);
+    default: return launch_step_kernels<SUNSET_FORM_NEWT>(H, from, pid);
     }
 }
 
@@ -681,6 +787,7 @@ void launch_step(Handle *H, int from, int pid) {
 // ---------------------------------------------------------------------------------------
 int state_alloc(Handle *H) {
     if (H->dsc) return 0;
+    if (int rc = set_smem_attributes(H)) return rc;
     const int n = H->npfb;
     for (int b = 0; b < 2; b++) {
         Fields &F = H->buf[b];
@@ -759,14 +866,8 @@ int set_tstep_device(Handle *H) {
 int rhs_only(Handle *H) {
     int rc = upload_consts(H);
     if (rc) return rc;
-    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
     StageArgs A = make_args(H, H->cur, 4);
-    switch (H->cfg.form) {
-    case SUNSET_FORM_DI: k_stage<SUNSET_FORM_DI><<<nblk, TB, 0, H->stream>>>(A); break;
-    case SUNSET_FORM_CHL: k_stage<SUNSET_FORM_CHL><<<nblk, TB, 0, H->stream>>>(A); break;
-    case SUNSET_FORM_LC: k_stage<SUNSET_FORM_LC><<<nblk, TB, 0, H->stream>>>(A); break;
-    default: k_stage<SUNSET_FORM_NEWT><<<nblk, TB, 0, H->stream>>>(A); break;
-    }
+    if ((rc = launch_stage_any(H, A))) return rc;
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -782,8 +883,10 @@ int step_run(Handle *H, double dt, int nsteps, int mode) {
             if (H->graph[from]) { cudaGraphExecDestroy(H->graph[from]); H->graph[from] = nullptr; }
             cudaGraph_t g;
             SUNSET_CUDA(H, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            launch_step(H, from, mode);
-            SUNSET_CUDA(H, cudaStreamEndCapture(st, &g));
+            int lrc = launch_step(H, from, mode);
+            cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (lrc) return lrc;
+            SUNSET_CUDA(H, ce);
             SUNSET_CUDA(H, cudaGraphInstantiate(&H->graph[from], g, 0));
             cudaGraphDestroy(g);
             H->graph_mode[from] = mode;
@@ -848,14 +951,7 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     cudaEvent_t e0, e1;
     SUNSET_CUDA(H, cudaEventCreate(&e0));
     SUNSET_CUDA(H, cudaEventCreate(&e1));
-    auto launch = [&]() {
-        switch (H->cfg.form) {
-        case SUNSET_FORM_DI: k_stage<SUNSET_FORM_DI><<<nblk, TB, 0, H->stream>>>(A); break;
-        case SUNSET_FORM_CHL: k_stage<SUNSET_FORM_CHL><<<nblk, TB, 0, H->stream>>>(A); break;
-        case SUNSET_FORM_LC: k_stage<SUNSET_FORM_LC><<<nblk, TB, 0, H->stream>>>(A); break;
-        default: k_stage<SUNSET_FORM_NEWT><<<nblk, TB, 0, H->stream>>>(A); break;
-        }
-    };
+    auto launch = [&]() { launch_stage_any(H, A); };
     for (int r = 0; r < 3; r++) launch();
     SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
     for (int r = 0; r < reps; r++) launch();
@@ -866,8 +962,9 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms = (double)t / reps;
-    // algorithmic bytes of one stage launch: small-link stream (index + 3 weights), the
-    // per-node state read once, registers S and E read + written, new state written.
+    // algorithmic bytes of one stage launch: small-link stream (16-bit local index + 3
+    // weights), the per-node state read once, registers S and E read + written, new state
+    // written.
     long long links = 0;
     {
         std::vector<int> ws(H->nslices);
@@ -878,7 +975,7 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     const int nf = form == SUNSET_FORM_DI ? 7 : 6;         // evolved fields (S and E registers)
     const int nread = form == SUNSET_FORM_DI ? 9 : 13;      // state + derived fields of a node
     const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;     // next state + derived fields
-    *bytes = (double)links * (4 + 3 * 8) + (double)H->npfb * 8.0 * (nread + 4 * nf + nwrite) +
+    *bytes = (double)links * (2 + 3 * 8) + (double)H->npfb * 8.0 * (nread + 4 * nf + nwrite) +
              (double)H->npfb * 8.0 * 4;  // sums + ordinate
     return 0;
 }

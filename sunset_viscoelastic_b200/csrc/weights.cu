@@ -361,7 +361,7 @@ struct WArgs {
 };
 
 __device__ __forceinline__ long long sell_off(const long long *slice_ptr, int i, int k) {
-    return slice_ptr[i >> 5] + (long long)k * kSlice + (i & 31);
+    return sell_at(slice_ptr[i >> 5], k, i & 31);
 }
 
 // Moment matrix over links [0,cnt) of node i with length scale hh (labf.F90:88-123).
@@ -539,11 +539,12 @@ struct SumArgs {
 __global__ void k_labf_sums(SumArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.npfb) return;
-    const long long base = a.slice_ptr[i >> 5] + (i & 31);
+    const long long base = a.slice_ptr[i >> 5];
+    const int lane = i & 31;
     const int cnt = a.cnt[i];
     double gx = 0.0, gy = 0.0, lp = 0.0, hy = 0.0;
     for (int k = 0; k < cnt; k++) {
-        long long o = base + (long long)k * kSlice;
+        long long o = sell_at(base, k, lane);
         hy = hy + a.wh[o];
         gx = gx + a.wx[o];
         gy = gy + a.wy[o];
@@ -554,7 +555,7 @@ __global__ void k_labf_sums(SumArgs a) {
     a.lsum[i] = (lp / a.L) / a.L;
     a.hsum[i] = hy;
     for (int k = 0; k < cnt; k++) {
-        long long o = base + (long long)k * kSlice;
+        long long o = sell_at(base, k, lane);
         a.wx[o] = a.wx[o] / a.L;
         a.wy[o] = a.wy[o] / a.L;
         a.wl[o] = (a.wl[o] / a.L) / a.L;
@@ -564,7 +565,7 @@ __global__ void k_labf_sums(SumArgs a) {
         const double hh = a.h[i], xi = a.px[i], yi = a.py[i];
         double v = 0.0;
         for (int k = 0; k < cnt; k++) {
-            int p = a.lpt[base + (long long)k * kSlice];
+            int p = a.lpt[sell_at(base, k, lane)];
             double x = -(xi - a.px[p]), y = -(yi - a.py[p]);
             double rad = sqrt(x * x + y * y) / hh;
             double f1 = ((9.0 / kPi) * exp((-9.0 * rad) * rad)) / (hh * hh);
@@ -581,7 +582,8 @@ __global__ void k_labf_sums(SumArgs a) {
 __global__ void k_filter_coeff(SumArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.npfb) return;
-    const long long base = a.slice_ptr[i >> 5] + (i & 31);
+    const long long base = a.slice_ptr[i >> 5];
+    const int lane = i & 31;
     const int cnt = a.cnt[i];
     const double xi = a.px[i], yi = a.py[i];
     const int t = a.ntype[i];
@@ -591,7 +593,7 @@ __global__ void k_filter_coeff(SumArgs a) {
         double tmp = ((2.0 / 3.0) * kPi) / lscal;
         double lsum = 0.0;
         for (int k = 0; k < cnt; k++) {
-            long long o = base + (long long)k * kSlice;
+            long long o = sell_at(base, k, lane);
             int p = a.lpt[o];
             double x = a.px[p] - xi, y = a.py[p] - yi;
             double fji = 1.0 - cos(tmp * x) * cos(tmp * y);
@@ -602,7 +604,7 @@ __global__ void k_filter_coeff(SumArgs a) {
         double tmp = ((2.0 / 3.0) * kPi) / a.sp[i];
         double lsum = 0.0;
         for (int k = 0; k < cnt; k++) {
-            long long o = base + (long long)k * kSlice;
+            long long o = sell_at(base, k, lane);
             int p = a.lpt[o];
             double x = a.px[p] - xi, y = a.py[p] - yi;
             double fji = 1.0 - cos(tmp * sqrt(x * x + y * y));
@@ -613,7 +615,7 @@ __global__ void k_filter_coeff(SumArgs a) {
     }
     double sum = 0.0;
     for (int k = 0; k < cnt; k++) {
-        long long o = base + (long long)k * kSlice;
+        long long o = sell_at(base, k, lane);
         double w = a.wh[o] * fc;
         a.wh[o] = w;
         sum = sum + w;
