@@ -42,6 +42,9 @@ def parse():
     p.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--error-steps", type=int, default=100,
+                   help="mixed precision: steps from the initial state for the per-field error report")
+    p.add_argument("--no-error-check", action="store_true")
     return p.parse_args()
 
 
@@ -77,57 +80,95 @@ def dt_for(wl, dtc, dtp):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock, its maximum and the active throttle reasons, sampled every 20 ms during the
+    timed region through NVML (read-only queries; the same counters nvidia-smi prints).
+    Falls back to nvidia-smi at 200 ms where NVML is unavailable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    MASKS = (0x8, 0x40, 0x20, 0x4)  # nvmlClocksEventReason* bits
+    SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
+    def __init__(self, cuda_device, period=0.02):
+        self.dev = cuda_device
+        self.period = period
+        self.rows = []  # (sm_mhz, sm_max_mhz, reasons bitmask)
         self.proc = None
-        self.out = os.path.join("/tmp", f"sunset_clocks_{os.getpid()}.csv")
+        self.thread = None
+        self.stop = False
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            props = torch.cuda.get_device_properties(self.dev)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(f"GPU-{props.uuid}")
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.out, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            nv, h = self._nvml_handle()
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def loop():
+                while not self.stop:
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((float(sm), float(smax), int(rs)))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            self.source = "nvml 20 ms"
+        except Exception:
+            self.out = os.path.join("/tmp", f"sunset_clocks_{os.getpid()}.csv")
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.SMI_FIELDS}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=open(self.out, "w"), stderr=subprocess.DEVNULL)
+                self.source = "nvidia-smi 200 ms"
+            except OSError:
+                self.proc = None
         return self
 
     def __exit__(self, *a):
+        self.stop = True
+        if self.thread is not None:
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+            try:
+                for r in open(self.out).read().strip().splitlines():
+                    r = [c.strip() for c in r.split(",")]
+                    if len(r) < 9:
+                        continue
+                    mask = 0
+                    for k, m in enumerate(self.MASKS):
+                        if r[5 + k].lower().startswith("active"):
+                            mask |= m
+                    self.rows.append((float(r[1]), float(r[2]), mask))
+            except (OSError, ValueError):
+                pass
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.out).read().strip().splitlines() if r.strip()]
-        except OSError:
+        if not self.rows:
             return None
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [c.strip() for c in r]
-            if len(r) < 9:
-                continue
-            try:
-                sm.append(float(r[1]))
-                smax = max(smax, float(r[2]))
-            except ValueError:
-                continue
-            for k, name in enumerate(names):
-                if r[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({n for r in self.rows for n, m in zip(self.NAMES, self.MASKS) if r[2] & m})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons,
+                "samples": len(sm), "source": self.source}
 
 
 def measured_peaks():
@@ -172,6 +213,33 @@ def oracle_setup(wl, ns, gpu=None):
         o.set_neighbours_weights(cnt, cs, links, gpu.weights())
     o.set_state(**initial_state(ns))
     return o
+
+
+ERROR_GROUPS = {"ro": ["ro"], "rou": ["rou", "rov"], "rov": ["rou", "rov"], "u": ["u", "v"], "v": ["u", "v"],
+                "cxx": ["cxx", "cxy", "cyy"], "cxy": ["cxx", "cxy", "cyy"], "cyy": ["cxx", "cxy", "cyy"]}
+
+
+def mixed_error(wl, ns, g, dt, nsteps, device):
+    """Per-field error of the mixed-precision handle g against the FP64 device path (which
+    agrees with the FP64 restatement to ~1e-14 in the parity tests), both stepped nsteps
+    from the initial state at the same dt.  Each field's error is relative to the magnitude
+    of the quantity it is a component of (rho, the momentum or velocity vector, the
+    conformation tensor): L_inf = max|d| / max_group max|f|, L_2 = ||d|| / max_group ||f||."""
+    from sunset_viscoelastic_b200 import labfm
+    ref = labfm.for_workload(wl, ns, device=device).setup()
+    st = initial_state(ns)
+    for h in (g, ref):
+        h.set_state(**st)
+        h.step(dt, nsteps)
+    a, b = g.state(), ref.state()
+    ref.close()
+    linf, l2 = {}, {}
+    for k, grp in ERROR_GROUPS.items():
+        d = a[k] - b[k]
+        linf[k] = float(np.abs(d).max() / max(max(np.abs(b[f]).max() for f in grp), 1e-300))
+        l2[k] = float(np.linalg.norm(d) / max(max(np.linalg.norm(b[f]) for f in grp), 1e-300))
+    return {"against": "FP64 device path", "steps": nsteps, "linf": linf, "l2": l2,
+            "max_linf": max(linf.values()), "max_l2": max(l2.values())}
 
 
 def run_reference(args, ws, rank):
@@ -273,6 +341,10 @@ def main():
         cpu = {"value": n * k / el, "unit": "node-steps/s", "cores": cpu_threads(), "kind": "port",
                "sample": f"{k} RK steps of the full {n}-node set (weights from the device build)"}
 
+    accuracy = None
+    if args.precision == "mixed" and not args.no_error_check:
+        accuracy = mixed_error(wl, ns, g, dt, args.error_steps, local)
+
     launches_per_step = 7
     line = {"metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -284,6 +356,8 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary()}
+    if accuracy is not None:
+        line["error_vs_fp64"] = accuracy
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()

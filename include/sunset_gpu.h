@@ -36,7 +36,8 @@ extern "C" {
 #define SUNSET_FORM_NEWT 3
 
 #define SUNSET_FP64 0   /* FP64 throughout: the drop-in */
-#define SUNSET_MIXED 1  /* FP32 fields/weights (hi/lo weights at order >= 8), FP64 solves */
+#define SUNSET_MIXED 1  /* time step streams FP32-rounded weights and keeps FP32 RK increments;
+                           weight solves, fields, stencil arithmetic and reductions stay FP64 */
 
 /* Run parameters: the reference's compile-time flags (Makefile) and control.in values
    (load_data.F90:53-159) in one struct. */

@@ -1,7 +1,7 @@
 """Builds libsunset_b200.so in-tree with nvcc for sm_100a (no JIT, no torch extension).
 
-The FP64 path (setup, weights, step) is compiled with -fmad=false so every product and
-sum rounds separately, as in the reference; the mixed-precision kernels keep FMA.
+The setup, weight and step sources are compiled with -fmad=false so every product and
+sum rounds separately, as in the reference (the mixed-precision step shares those kernels).
 """
 from __future__ import annotations
 
@@ -19,7 +19,7 @@ SOURCES = {  # file -> extra flags
     "setup.cu": ["-fmad=false"],
     "weights.cu": ["-fmad=false"],
     "step.cu": ["-fmad=false"],
-    "mixed.cu": [],
+    "stream.cu": [],
     "noalloc.cu": [],
     "abi.cu": [],
 }

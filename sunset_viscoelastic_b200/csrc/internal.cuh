@@ -10,7 +10,10 @@
 //     to its own (even) width; links k = 2m, 2m+1 of node i sit next to each other at
 //     slice_ptr[i/32] + 64 m + 2 (i%32) (sell_at), so a warp reading link pair m of its 32
 //     nodes issues one coalesced 512-byte access.  Padding has weight 0 and points at node 0.
-//   * Fields are structure-of-arrays FP64 (or FP32 in the mixed path).
+//   * The time step streams its own copy of the links (stream.cu): the same SELL slots with
+//     each node's links in a shared-memory-bank-aware order, FP64 or (mixed) FP32 weights.
+//   * Fields are structure-of-arrays FP64 in both precisions; the mixed path keeps FP32 RK
+//     increments.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -121,9 +124,15 @@ struct Handle {
     // ---- weights (SELL, FP64) ----
     double *wx = nullptr, *wy = nullptr, *wl = nullptr, *wh = nullptr;
     double *gsx = nullptr, *gsy = nullptr, *lsum = nullptr, *hsum = nullptr, *vol = nullptr;
-    // mixed-precision copies
+    // mixed precision: the weights rounded to FP32 and their stencil sums (FP64 sums of
+    // the rounded weights, so sum_k w_k phi_j - phi_i sum_k w_k is exactly the
+    // difference form of the rounded stencil)
     float *wx32 = nullptr, *wy32 = nullptr, *wl32 = nullptr, *wh32 = nullptr;
-    float *wx32lo = nullptr, *wy32lo = nullptr, *wl32lo = nullptr, *wh32lo = nullptr;
+    double *gsx32 = nullptr, *gsy32 = nullptr, *lsum32 = nullptr, *hsum32 = nullptr;
+    // the time step's link stream: local links and (FP64 step) weights in the bank-aware
+    // order of stream.cu; the arrays above stay in the reference's order
+    uint16_t *lloc_s = nullptr;
+    double *wx_s = nullptr, *wy_s = nullptr, *wl_s = nullptr, *wh_s = nullptr;
 
     // ---- state ----
     Fields buf[2]{};
@@ -131,6 +140,9 @@ struct Handle {
     double *reg[7] = {};   // RK register S: ro rou rov q0..q3
     double *eacc[7] = {};  // error accumulators
     double *rhs[7] = {};   // rhs output of sunset_calc_all_rhs
+    // mixed precision: RK register as the FP32 increment D = S - U over the stage's state,
+    // and the error accumulator in FP32
+    float *dreg32[7] = {}, *eacc32[7] = {};
     double *partials = nullptr;
     int npart = 0;
     DevScalars *dsc = nullptr;
@@ -171,7 +183,7 @@ int build_halos(Handle *H);
 int labf_weights_device(Handle *H);
 int labf_sums_device(Handle *H);
 int filter_coefficients_device(Handle *H);
-int make_mixed_weights(Handle *H);
+int make_stream_links(Handle *H);
 
 int state_alloc(Handle *H);
 int state_set_device(Handle *H, const double *ro, const double *u, const double *v, const double *cxx,

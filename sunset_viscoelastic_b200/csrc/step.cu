@@ -1,19 +1,24 @@
-// step.cu -- the FP64 time step: fused RK stage kernels, filter + mass correction,
-// finalisation, PID time-step control, and the single-operator kernels of the C-ABI.
+// step.cu -- the time step (FP64 and mixed precision): fused RK stage kernels, filter + mass
+// correction, finalisation, PID time-step control, and the single-operator kernels of the
+// C-ABI.
 //
-// One RK stage is one kernel: a thread owns a node, a warp owns a slice of 32 nodes, and
-// the warp streams the slice's links (index + gradient/Laplacian weights, one coalesced
-// access per link and array) while gathering the neighbours' fields.  The node's stencil
-// sums feed the right-hand side in registers, which feeds the low-storage RK update
+// One RK stage is one kernel: a block owns a tile of 8 slices (256 nodes), stages the
+// fields of every node the tile's links reach (its halo) in shared memory, and streams the
+// tile's links through a per-thread cp.async ring.  A thread owns a node: its stencil sums
+// feed the right-hand side in registers, which feeds the low-storage RK update
 // (step.F90:291-343), which writes the next state and its derived fields (velocity,
 // conformation tensor) into the other state buffer.  Ghost links carry the parent's
 // index and a reflection code, so no mirror copy (mirror_boundaries.F90:263-352) or
 // halo exchange runs between stages.
 //
-// Sums run over each node's links in the reference's order, in the reference's sum form
-// (sum_k w_k phi_j - phi_i sum_k w_k, derivatives.F90:36-46), and the file is built with
-// -fmad=false, so the FP64 path computes what the reference computes operation for
-// operation; only the libm functions (exp, log, cos) may differ from glibc in the last bit.
+// Sums take the reference's sum form (sum_k w_k phi_j - phi_i sum_k w_k,
+// derivatives.F90:36-46) and the file is built with -fmad=false, so each product and sum of
+// the FP64 path rounds as in the reference.  The single-operator kernels sum in the
+// reference's link order and reproduce it bit for bit; the step sums in the bank-aware
+// order of stream.cu, which changes only the rounding (and libm's exp, log, cos may differ
+// from glibc in the last bit).
+#include <type_traits>
+
 #include "internal.cuh"
 #include "physics.cuh"
 
@@ -31,9 +36,11 @@ struct StageArgs {
     const int *halo_ptr, *halo;
     int hmax;
     const double *wx, *wy, *wl, *wh;
+    const float *wx32, *wy32, *wl32, *wh32;  // mixed precision
     const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
     Fields in, out;
     double *reg[7], *eacc[7], *rhs[7];
+    float *dreg[7], *eacc32[7];  // mixed precision
     DevScalars *sc;
     double *partials;
     int stage;  // 0..3; 4 = rhs only
@@ -81,13 +88,89 @@ __device__ __forceinline__ void load_halo(const StageArgs &A, double *sm, SRC sr
     __syncthreads();
 }
 
+// cp.async (global -> shared, completion tracked per thread in commit groups), with memory
+// clobbers so the compiler keeps shared-memory reads after the wait that covers them.
+template <int N>
+__device__ __forceinline__ void cp_async(void *dst_shared, const void *src_global) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_shared);
+    const size_t g = __cvta_generic_to_global(src_global);
+    if constexpr (N == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(g), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Per-thread ring of link pairs in shared memory, filled by cp.async (LDGSTS).  Thread t
+// copies its own node's link pair m -- NA weight pairs and the pair's two 16-bit local
+// indices -- D-1 pairs ahead of the pair it works on, so D-1 pairs per thread are in flight
+// without holding registers.  A thread reads back only what it copied itself, so no barrier
+// is needed; slots are reused only after the thread has consumed them.
+template <bool MX, int NA, int D>
+struct LinkRing {
+    static_assert((D & (D - 1)) == 0, "ring depth must be a power of two");
+    using W2 = typename std::conditional<MX, float2, double2>::type;
+    W2 *w;          // [D][NA][kTile]
+    unsigned *l;    // [D][kTile]
+    const W2 *src[NA];
+    const unsigned *lsrc;
+    long long pb;   // pair index of this node's pair 0; pair m sits at pb + 32 m
+    int npair;
+
+    static constexpr size_t bytes() { return (size_t)D * kTile * (NA * sizeof(W2) + sizeof(unsigned)); }
+
+    __device__ __forceinline__ void init(double *base, const unsigned *lidx2, long long pb_, int npair_) {
+        w = reinterpret_cast<W2 *>(base);
+        l = reinterpret_cast<unsigned *>(w + (size_t)D * NA * kTile);
+        lsrc = lidx2;
+        pb = pb_;
+        npair = npair_;
+    }
+    __device__ __forceinline__ void issue(int m) {
+        if (m < npair) {
+            const int s = m & (D - 1);
+            const long long o = pb + ((long long)m << 5);
+#pragma unroll
+            for (int a = 0; a < NA; a++) cp_async<sizeof(W2)>(w + (s * NA + a) * kTile + threadIdx.x, src[a] + o);
+            cp_async<4>(l + s * kTile + threadIdx.x, lsrc + o);
+        }
+        cp_async_commit();  // empty groups keep the group count uniform
+    }
+    __device__ __forceinline__ void prologue() {
+#pragma unroll
+        for (int m = 0; m < D - 1; m++) issue(m);
+    }
+    // make pair m resident (and start pair m + D - 1)
+    __device__ __forceinline__ void next(int m) {
+        issue(m + D - 1);
+        cp_async_wait<D - 1>();
+    }
+    __device__ __forceinline__ void weights(int m, int a, double &x0, double &x1) const {
+        const W2 v = w[((m & (D - 1)) * NA + a) * kTile + threadIdx.x];
+        x0 = (double)v.x;
+        x1 = (double)v.y;
+    }
+    __device__ __forceinline__ unsigned index(int m) const { return l[(m & (D - 1)) * kTile + threadIdx.x]; }
+};
+
+// Ring depth: FP64 pairs are 52 bytes a thread, FP32 ones 28.
+__host__ __device__ constexpr int ring_depth(bool mx) { return mx ? 4 : 2; }
+
+// Doubles of the shared-memory halo, rounded up so the ring after it is 16-byte aligned.
+__host__ __device__ inline size_t halo_doubles(int ng, int hmax) { return ((size_t)ng * hmax + 1) & ~(size_t)1; }
+
 // Stencil sums of one node over its small links, sum form of derivatives.F90:36-46,
-// neighbours read from the block's shared-memory halo.
-template <int FORM, bool MD>
-__device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const double *sm, Grads &g) {
+// neighbours read from the block's shared-memory halo.  In the mixed path the weights are
+// the FP32-rounded ones and A.gsx.. hold the FP64 sums of those, so the FP64 arithmetic
+// below evaluates the difference form sum_k w_k (phi_j - phi_i) of the rounded stencil.
+template <int FORM, bool MD, bool MX, class RING>
+__device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const double *sm, RING &R, Grads &g) {
     const int hm = A.hmax;
-    const long long pb = (A.slice_ptr[i >> 5] >> 1) + (i & 31);  // link pair m of this node: pb + 32 m
-    const int npair = A.slice_ws[i >> 5] >> 1;
+    const int npair = R.npair;
     const Fields &F = A.in;
     double s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
     double s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
@@ -95,9 +178,11 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
     double s_lxx = 0, s_lxy = 0, s_lyy = 0;
     const bool mir = cK.has_mirrors;
     const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
-    const double2 *WX = reinterpret_cast<const double2 *>(A.wx), *WY = reinterpret_cast<const double2 *>(A.wy);
-    const double2 *WL = reinterpret_cast<const double2 *>(A.wl);
-    const unsigned *LL = reinterpret_cast<const unsigned *>(A.lloc);
+    // FP64 step: separate multiply and add, as the reference; mixed step: fused
+    auto mac = [](double &acc, double x, double w) {
+        if constexpr (MX) acc = __fma_rn(x, w, acc);
+        else acc = acc + x * w;
+    };
     auto link = [&](int lk, double wxk, double wyk, double wlk) {
         const int j = lk & kLocMask;
         double roj = sm[j], uj = sm[hm + j], vj = sm[2 * hm + j];
@@ -117,43 +202,46 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
             reflect(code, uj, vj, cxyj);
             if (code == 1 || code == 2) pxyj = -pxyj;
         }
-        s_ro_x = s_ro_x + roj * wxk;
-        s_ro_y = s_ro_y + roj * wyk;
-        s_u_x = s_u_x + uj * wxk;
-        s_u_y = s_u_y + uj * wyk;
-        s_lu = s_lu + uj * wlk;
-        s_v_x = s_v_x + vj * wxk;
-        s_v_y = s_v_y + vj * wyk;
-        s_lv = s_lv + vj * wlk;
+        mac(s_ro_x, roj, wxk);
+        mac(s_ro_y, roj, wyk);
+        mac(s_u_x, uj, wxk);
+        mac(s_u_y, uj, wyk);
+        mac(s_lu, uj, wlk);
+        mac(s_v_x, vj, wxk);
+        mac(s_v_y, vj, wyk);
+        mac(s_lv, vj, wlk);
         if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
-            s_cxx_x = s_cxx_x + cxxj * wxk;
-            if (full) s_cxx_y = s_cxx_y + cxxj * wyk;
-            s_cxy_x = s_cxy_x + cxyj * wxk;
-            s_cxy_y = s_cxy_y + cxyj * wyk;
-            if (full) s_cyy_x = s_cyy_x + cyyj * wxk;
-            s_cyy_y = s_cyy_y + cyyj * wyk;
+            mac(s_cxx_x, cxxj, wxk);
+            if (full) mac(s_cxx_y, cxxj, wyk);
+            mac(s_cxy_x, cxyj, wxk);
+            mac(s_cxy_y, cxyj, wyk);
+            if (full) mac(s_cyy_x, cyyj, wxk);
+            mac(s_cyy_y, cyyj, wyk);
         }
         if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {
-            s_pxx_x = s_pxx_x + pxxj * wxk;
-            s_pxx_y = s_pxx_y + pxxj * wyk;
-            s_pxy_x = s_pxy_x + pxyj * wxk;
-            s_pxy_y = s_pxy_y + pxyj * wyk;
-            s_pyy_x = s_pyy_x + pyyj * wxk;
-            s_pyy_y = s_pyy_y + pyyj * wyk;
+            mac(s_pxx_x, pxxj, wxk);
+            mac(s_pxx_y, pxxj, wyk);
+            mac(s_pxy_x, pxyj, wxk);
+            mac(s_pxy_y, pxyj, wyk);
+            mac(s_pyy_x, pyyj, wxk);
+            mac(s_pyy_y, pyyj, wyk);
         }
         if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) {
-            s_lxx = s_lxx + cxxj * wlk;
-            s_lxy = s_lxy + cxyj * wlk;
-            s_lyy = s_lyy + cyyj * wlk;
+            mac(s_lxx, cxxj, wlk);
+            mac(s_lxy, cxyj, wlk);
+            mac(s_lyy, cyyj, wlk);
         }
     };
     // links in order k = 2m, 2m+1: the sums keep the reference's order
     for (int m = 0; m < npair; m++) {
-        const long long o = pb + ((long long)m << 5);
-        const double2 wx2 = __ldg(WX + o), wy2 = __ldg(WY + o), wl2 = __ldg(WL + o);
-        const unsigned l2 = __ldg(LL + o);
-        link((int)(l2 & 0xffffu), wx2.x, wy2.x, wl2.x);
-        link((int)(l2 >> 16), wx2.y, wy2.y, wl2.y);
+        R.next(m);
+        double wx0, wx1, wy0, wy1, wl0, wl1;
+        R.weights(m, 0, wx0, wx1);
+        R.weights(m, 1, wy0, wy1);
+        R.weights(m, 2, wl0, wl1);
+        const unsigned l2 = R.index(m);
+        link((int)(l2 & 0xffffu), wx0, wy0, wl0);
+        link((int)(l2 >> 16), wx1, wy1, wl1);
     }
     if (i >= cK.npfb) return;
     const double gx = A.gsx[i], gy = A.gsy[i], ls = A.lsum[i];
@@ -235,27 +323,44 @@ __device__ __forceinline__ void block_min_bits(unsigned long long v, unsigned lo
     }
 }
 
-// Resident blocks per SM the stage kernel is compiled for: the log-conformation and direct
-// forms keep their longer epilogues in registers at 3 blocks (85 registers); the
-// Cholesky form runs best at 4 (64 registers).  Measured on B200.
-__host__ __device__ constexpr int stage_min_blocks(int form) { return form == SUNSET_FORM_CHL ? 4 : 3; }
+// Resident blocks per SM the stage kernel is compiled for (up to 85 registers a thread):
+// the tile halo plus the link ring take 55-70 KB of shared memory on the order-6 and
+// order-8 sets, so a fourth block would not fit anyway.
+__host__ __device__ constexpr int stage_min_blocks(int) { return 3; }
 
 // One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).  One
 // block per tile of kTile nodes; the tile's halo is staged in shared memory first.
-template <int FORM, bool MD>
+//
+// MX (mixed precision): FP32 weights; the register S is kept as the FP32 increment
+// D = S - U over the stage's FP64 state U (so S = U + D loses only FP32 rounding of an
+// O(dt rhs) quantity) and the error accumulator E as FP32.
+template <int FORM, bool MD, bool MX>
 __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageArgs A) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     constexpr int NG = ngather(FORM, MD);
-    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD>(A.in, f); });
     const int i = blockIdx.x * kTile + threadIdx.x;
+    bool active = (i >> 5) < cK.nslices;
+    LinkRing<MX, 3, ring_depth(MX)> R;
+    if constexpr (MX) {
+        R.src[0] = reinterpret_cast<const float2 *>(A.wx32);
+        R.src[1] = reinterpret_cast<const float2 *>(A.wy32);
+        R.src[2] = reinterpret_cast<const float2 *>(A.wl32);
+    } else {
+        R.src[0] = reinterpret_cast<const double2 *>(A.wx);
+        R.src[1] = reinterpret_cast<const double2 *>(A.wy);
+        R.src[2] = reinterpret_cast<const double2 *>(A.wl);
+    }
+    R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
+           active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
+    R.prologue();  // the first link pairs stream in while the halo is staged
+    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD>(A.in, f); });
     const int stage = A.stage;
     if (stage == 0 && i == 0) {
         A.sc->cfl_bits = 0x7ff0000000000000ull;
         A.sc->par_bits = 0x7ff0000000000000ull;
     }
     Grads g;
-    bool active = (i >> 5) < cK.nslices;
-    if (active) gather_stage<FORM, MD>(A, i, smem, g);
+    if (active) gather_stage<FORM, MD, MX>(A, i, smem, R, g);
     active = active && i < cK.npfb;
     unsigned long long emax_bits = 0;
     if (active) {
@@ -291,19 +396,33 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                 const double RKa = dt * a;
 #pragma unroll
                 for (int f = 0; f < nf; f++) {
-                    const double S = (stage == 0) ? U[f] : A.reg[f][i];
-                    const double E = (stage == 0) ? 0.0 : A.eacc[f][i];
-                    Un[f] = S + RKa * rr[f];
-                    A.reg[f][i] = S + RKb * rr[f];
-                    A.eacc[f][i] = E + RKbmbh * rr[f];
+                    if constexpr (MX) {
+                        const double S = (stage == 0) ? U[f] : U[f] + (double)A.dreg[f][i];
+                        const double E = (stage == 0) ? 0.0 : (double)A.eacc32[f][i];
+                        Un[f] = S + RKa * rr[f];
+                        A.dreg[f][i] = (float)((S + RKb * rr[f]) - Un[f]);
+                        A.eacc32[f][i] = (float)(E + RKbmbh * rr[f]);
+                    } else {
+                        const double S = (stage == 0) ? U[f] : A.reg[f][i];
+                        const double E = (stage == 0) ? 0.0 : A.eacc[f][i];
+                        Un[f] = S + RKa * rr[f];
+                        A.reg[f][i] = S + RKb * rr[f];
+                        A.eacc[f][i] = E + RKbmbh * rr[f];
+                    }
                 }
             } else {
                 double en = 0.0;
 #pragma unroll
                 for (int f = 0; f < nf; f++) {
                     const double norm = f == 0 ? cK.ero_norm : f < 3 ? cK.erou_norm : cK.exx_norm;
-                    Un[f] = A.reg[f][i] + RKb * rr[f];
-                    const double E = A.eacc[f][i] + RKbmbh * rr[f];
+                    double E;
+                    if constexpr (MX) {
+                        Un[f] = (U[f] + (double)A.dreg[f][i]) + RKb * rr[f];
+                        E = (double)A.eacc32[f][i] + RKbmbh * rr[f];
+                    } else {
+                        Un[f] = A.reg[f][i] + RKb * rr[f];
+                        E = A.eacc[f][i] + RKbmbh * rr[f];
+                    }
                     const double t = fabs(E) * norm;
                     en = (t > en) ? t : en;
                     if (t != t) en = t;
@@ -336,24 +455,28 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
 
 // filter_variables (rhs_di.F90:667-720; rhs.F90:792-900; rhs_lc.F90:818-893): the
 // hyperviscous filter of each evolved field plus the mass-correction partial sums.
-template <int FORM>
+template <int FORM, bool MX>
 __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
     const Fields &F = A.in;
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    const bool live = (i >> 5) < cK.nslices;
+    LinkRing<MX, 1, ring_depth(MX)> R;
+    if constexpr (MX) R.src[0] = reinterpret_cast<const float2 *>(A.wh32);
+    else R.src[0] = reinterpret_cast<const double2 *>(A.wh);
+    R.init(smem + halo_doubles(nf, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
+           live ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, live ? A.slice_w[i >> 5] >> 1 : 0);
+    R.prologue();
     load_halo<nf>(A, smem, [&](int f) -> const double * {
         return f == 0 ? F.ro : f == 1 ? F.rou : f == 2 ? F.rov : F.q[f - 3];
     });
-    const int i = blockIdx.x * kTile + threadIdx.x;
     const int hm = A.hmax;
     double part = 0.0;
-    if ((i >> 5) < cK.nslices) {
-        const long long pb = (A.slice_ptr[i >> 5] >> 1) + (i & 31);
-        const int npair = A.slice_w[i >> 5] >> 1;
+    if (live) {
+        const int npair = R.npair;
         double t[7] = {0, 0, 0, 0, 0, 0, 0};
         const bool mir = cK.has_mirrors;
-        const double2 *WH = reinterpret_cast<const double2 *>(A.wh);
-        const unsigned *LL = reinterpret_cast<const unsigned *>(A.lloc);
         auto link = [&](int lk, double whk) {
             const int j = lk & kLocMask;
             double v[7];
@@ -365,14 +488,18 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
                 reflect(code, v[1], v[2], nf > 4 ? v[4] : dummy);
             }
 #pragma unroll
-            for (int f = 0; f < nf; f++) t[f] = t[f] + v[f] * whk;
+            for (int f = 0; f < nf; f++) {
+                if constexpr (MX) t[f] = __fma_rn(v[f], whk, t[f]);
+                else t[f] = t[f] + v[f] * whk;
+            }
         };
         for (int m = 0; m < npair; m++) {
-            const long long o = pb + ((long long)m << 5);
-            const double2 wh2 = __ldg(WH + o);
-            const unsigned l2 = __ldg(LL + o);
-            link((int)(l2 & 0xffffu), wh2.x);
-            link((int)(l2 >> 16), wh2.y);
+            R.next(m);
+            double wh0, wh1;
+            R.weights(m, 0, wh0, wh1);
+            const unsigned l2 = R.index(m);
+            link((int)(l2 & 0xffffu), wh0);
+            link((int)(l2 >> 16), wh1);
         }
         if (i < cK.npfb) {
             const double hs = A.hsum[i];
@@ -648,22 +775,39 @@ __global__ void k_fold_partials(const double *partials, int n, double *out) {
     if (threadIdx.x == 0) *out = sm[0];
 }
 
-StageArgs make_args(Handle *H, int from, int stage) {
+// Kernel arguments over buffer `from`.  step: the time step's link stream (bank-aware order;
+// FP32 weights with their own sums in mixed precision); otherwise the reference-order FP64
+// arrays of the single-operator entry points.
+StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
+    const bool mx = step && H->cfg.precision == SUNSET_MIXED;
     StageArgs A{};
     A.slice_ptr = H->slice_ptr;
     A.slice_ws = H->slice_ws;
     A.slice_w = H->slice_w;
     A.lidx = H->lidx;
-    A.lloc = H->lloc;
+    A.lloc = step ? H->lloc_s : H->lloc;
     A.halo_ptr = H->halo_ptr;
     A.halo = H->halo;
     A.hmax = H->halo_max;
-    A.wx = H->wx; A.wy = H->wy; A.wl = H->wl; A.wh = H->wh;
-    A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum; A.hsum = H->hsum; A.vol = H->vol;
+    if (step) {
+        A.wx = H->wx_s; A.wy = H->wy_s; A.wl = H->wl_s; A.wh = H->wh_s;
+    } else {
+        A.wx = H->wx; A.wy = H->wy; A.wl = H->wl; A.wh = H->wh;
+    }
+    A.wx32 = H->wx32; A.wy32 = H->wy32; A.wl32 = H->wl32; A.wh32 = H->wh32;
+    if (mx) {
+        A.gsx = H->gsx32; A.gsy = H->gsy32; A.lsum = H->lsum32; A.hsum = H->hsum32;
+    } else {
+        A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum; A.hsum = H->hsum;
+    }
+    A.vol = H->vol;
     A.py_node = H->py;
     A.in = H->buf[from];
     A.out = H->buf[from ^ 1];
-    for (int f = 0; f < 7; f++) { A.reg[f] = H->reg[f]; A.eacc[f] = H->eacc[f]; A.rhs[f] = H->rhs[f]; }
+    for (int f = 0; f < 7; f++) {
+        A.reg[f] = H->reg[f]; A.eacc[f] = H->eacc[f]; A.rhs[f] = H->rhs[f];
+        A.dreg[f] = H->dreg32[f]; A.eacc32[f] = H->eacc32[f];
+    }
     A.sc = H->dsc;
     A.partials = H->partials;
     A.stage = stage;
@@ -711,44 +855,63 @@ constexpr size_t kMaxStageSmem = 200 * 1024;
 // Opt the staged kernels into large dynamic shared memory on the handle's device.
 int set_smem_attributes(Handle *H) {
 #define SUNSET_SMEM_ATTR(K) SUNSET_CUDA(H, cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem))
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false>));
-    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_DI>);
-    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_CHL>);
-    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_LC>);
-    SUNSET_SMEM_ATTR(k_filter<SUNSET_FORM_NEWT>);
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false, false>));
+    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false, false>));
+    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_DI, false>));
+    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_CHL, false>));
+    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_LC, false>));
+    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_NEWT, false>));
+    if (H->cfg.precision == SUNSET_MIXED) {
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false, true>));
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true, true>));
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false, true>));
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true, true>));
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false, true>));
+        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false, true>));
+        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_DI, true>));
+        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_CHL, true>));
+        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_LC, true>));
+        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_NEWT, true>));
+    }
 #undef SUNSET_SMEM_ATTR
     return 0;
 }
 
+inline bool is_mx(const Handle *H) { return H->cfg.precision == SUNSET_MIXED; }
+
 template <int FORM, bool MD>
-int launch_stage(Handle *H, const StageArgs &A) {
-    const size_t smem = (size_t)ngather(FORM, MD) * H->halo_max * sizeof(double);
+int launch_stage(Handle *H, const StageArgs &A, bool mx) {
+    const size_t smem = halo_doubles(ngather(FORM, MD), H->halo_max) * sizeof(double) +
+                        (mx ? LinkRing<true, 3, ring_depth(true)>::bytes() : LinkRing<false, 3, ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    k_stage<FORM, MD><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (mx) k_stage<FORM, MD, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    else k_stage<FORM, MD, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
     return 0;
 }
 
-int launch_stage_any(Handle *H, const StageArgs &A) {
+// A must come from make_args(..., step = true); mx is the handle's precision.
+int launch_stage_any(Handle *H, const StageArgs &A, bool mx) {
     const bool md = H->cfg.Mdiff != 0.0;
     switch (H->cfg.form) {
-    case SUNSET_FORM_DI: return md ? launch_stage<SUNSET_FORM_DI, true>(H, A) : launch_stage<SUNSET_FORM_DI, false>(H, A);
-    case SUNSET_FORM_CHL: return md ? launch_stage<SUNSET_FORM_CHL, true>(H, A) : launch_stage<SUNSET_FORM_CHL, false>(H, A);
-    case SUNSET_FORM_LC: return launch_stage<SUNSET_FORM_LC, false>(H, A);
-    default: return launch_stage<SUNSET_FORM_NEWT, false>(H, A);
+    case SUNSET_FORM_DI: return md ? launch_stage<SUNSET_FORM_DI, true>(H, A, mx) : launch_stage<SUNSET_FORM_DI, false>(H, A, mx);
+    case SUNSET_FORM_CHL: return md ? launch_stage<SUNSET_FORM_CHL, true>(H, A, mx) : launch_stage<SUNSET_FORM_CHL, false>(H, A, mx);
+    case SUNSET_FORM_LC: return launch_stage<SUNSET_FORM_LC, false>(H, A, mx);
+    default: return launch_stage<SUNSET_FORM_NEWT, false>(H, A, mx);
     }
 }
 
 template <int FORM>
-int launch_filter(Handle *H, const StageArgs &A) {
+int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
-    const size_t smem = (size_t)nf * H->halo_max * sizeof(double);
+    const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) +
+                        (mx ? LinkRing<true, 1, ring_depth(true)>::bytes() : LinkRing<false, 1, ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    k_filter<FORM><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (mx) k_filter<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    else k_filter<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
     return 0;
 }
 
@@ -756,17 +919,18 @@ template <int FORM>
 int launch_step_kernels(Handle *H, int from, int pid) {
     const int TB = 128;
     cudaStream_t st = H->stream;
+    const bool mx = is_mx(H);
     if (pid) k_pid<<<1, 1, 0, st>>>(H->dsc);
     int b = from;
     for (int s = 0; s < 4; s++) {
-        StageArgs A = make_args(H, b, s);
-        if (int rc = launch_stage_any(H, A)) return rc;
+        StageArgs A = make_args(H, b, s, true);
+        if (int rc = launch_stage_any(H, A, mx)) return rc;
         b ^= 1;
     }
-    StageArgs F = make_args(H, b, 5);
-    if (int rc = launch_filter<FORM>(H, F)) return rc;
+    StageArgs F = make_args(H, b, 5, true);
+    if (int rc = launch_filter<FORM>(H, F, mx)) return rc;
     b ^= 1;
-    StageArgs Z = make_args(H, b ^ 1, 5);  // in = filter input, out = filtered buffer
+    StageArgs Z = make_args(H, b ^ 1, 5, true);  // in = filter input, out = filtered buffer
     const int fb = (H->npfb + TB - 1) / TB;
     k_finalize<FORM><<<fb, TB, 0, st>>>(Z, 1);
     k_tstep<<<fb, TB, 0, st>>>(H->buf[b].u, H->buf[b].v, H->buf[b].ro, H->sp, H->ntype, H->npfb, H->dsc);
@@ -803,8 +967,14 @@ int state_alloc(Handle *H) {
                 if (dalloc(H, &F.c[k], n)) return SUNSET_ERR_NOMEM;
         }
     }
-    for (int f = 0; f < 7; f++)
-        if (dalloc(H, &H->reg[f], n) || dalloc(H, &H->eacc[f], n) || dalloc(H, &H->rhs[f], n)) return SUNSET_ERR_NOMEM;
+    for (int f = 0; f < 7; f++) {
+        if (dalloc(H, &H->rhs[f], n)) return SUNSET_ERR_NOMEM;
+        if (is_mx(H)) {
+            if (dalloc(H, &H->dreg32[f], n) || dalloc(H, &H->eacc32[f], n)) return SUNSET_ERR_NOMEM;
+        } else {
+            if (dalloc(H, &H->reg[f], n) || dalloc(H, &H->eacc[f], n)) return SUNSET_ERR_NOMEM;
+        }
+    }
     const int nthr = H->nslices * kSlice;
     H->npart = (nthr + 127) / 128 + 1;
     if (dalloc(H, &H->partials, 2 * (size_t)H->npart + 16) || dalloc(H, &H->dsc, 1) || dalloc(H, &H->tmpd, 4 * (size_t)n))
@@ -866,8 +1036,8 @@ int set_tstep_device(Handle *H) {
 int rhs_only(Handle *H) {
     int rc = upload_consts(H);
     if (rc) return rc;
-    StageArgs A = make_args(H, H->cur, 4);
-    if ((rc = launch_stage_any(H, A))) return rc;
+    StageArgs A = make_args(H, H->cur, 4, true);
+    if ((rc = launch_stage_any(H, A, is_mx(H)))) return rc;
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -947,11 +1117,12 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
     // stage 4 (right-hand side only) reads what an RK stage reads and writes the rhs arrays;
     // use stage 1 itself: it reads the current buffer and writes the other one.
-    StageArgs A = make_args(H, H->cur, 1);
+    const bool mx = is_mx(H);
+    StageArgs A = make_args(H, H->cur, 1, true);
     cudaEvent_t e0, e1;
     SUNSET_CUDA(H, cudaEventCreate(&e0));
     SUNSET_CUDA(H, cudaEventCreate(&e1));
-    auto launch = [&]() { launch_stage_any(H, A); };
+    auto launch = [&]() { launch_stage_any(H, A, mx); };
     for (int r = 0; r < 3; r++) launch();
     SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
     for (int r = 0; r < reps; r++) launch();
@@ -963,8 +1134,8 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     cudaEventDestroy(e1);
     *ms = (double)t / reps;
     // algorithmic bytes of one stage launch: small-link stream (16-bit local index + 3
-    // weights), the per-node state read once, registers S and E read + written, new state
-    // written.
+    // weights of 8 or 4 bytes), the per-node state read once, registers S and E read +
+    // written (8 bytes each, 4 in the mixed path), new state written.
     long long links = 0;
     {
         std::vector<int> ws(H->nslices);
@@ -975,7 +1146,8 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     const int nf = form == SUNSET_FORM_DI ? 7 : 6;         // evolved fields (S and E registers)
     const int nread = form == SUNSET_FORM_DI ? 9 : 13;      // state + derived fields of a node
     const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;     // next state + derived fields
-    *bytes = (double)links * (2 + 3 * 8) + (double)H->npfb * 8.0 * (nread + 4 * nf + nwrite) +
+    const double wb = mx ? 4.0 : 8.0;
+    *bytes = (double)links * (2 + 3 * wb) + (double)H->npfb * (8.0 * nread + 4.0 * wb * nf + 8.0 * nwrite) +
              (double)H->npfb * 8.0 * 4;  // sums + ordinate
     return 0;
 }

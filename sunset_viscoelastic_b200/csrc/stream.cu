@@ -1,0 +1,239 @@
+// stream.cu -- the link stream of the time step: bank-aware link order, and the weights the
+// stage and filter kernels stream (FP64 copies, or FP32 for the mixed precision).
+//
+// The setup, the single-operator entry points and the weight export keep the reference's
+// link order (derivatives.F90 sums over ij_link in order).  The time step sums each node's
+// links in its own order instead, chosen for the hardware: the stage and filter kernels
+// gather the tile halo from shared memory with 8-byte loads, which are served per
+// half-warp, one wavefront per bank pair (position mod 16) and distinct position.  In the
+// reference order neighbouring lanes often meet in the same bank pair at the same link slot
+// (4.9 wavefronts a load on the order-6 set against the ideal 2).  order_links_by_bank()
+// re-deals each node's links slot by slot so that the 16 lanes of a half-warp read distinct
+// bank pairs wherever a bipartite matching allows it (2.6 on that set).  Only the rounding
+// of the sums changes (relative 1e-16 a sum).
+//
+// Mixed precision: the weight solves stay FP64; the step streams the weights rounded to FP32,
+// which halves the dominant per-link traffic (26 -> 14 bytes a link with the 16-bit local
+// index), while fields, stencil arithmetic and state stay FP64.  The stencil sums sum_k w_k
+// are recomputed in FP64 from the rounded weights, so the step's sum form
+// sum_k w_k phi_j - phi_i sum_k w_k is exactly the difference form
+// sum_k w_k (phi_j - phi_i) of the rounded stencil: a constant field keeps zero derivatives
+// and the rounding never leaks a phi_i * (sum of rounding errors) term.
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace sunset {
+
+namespace {
+
+struct StreamArgs {
+    int npfb;
+    const long long *slice_ptr;
+    const int *slice_w;
+    const int *src;  // SELL entry -> SELL entry of the reference-order arrays it takes (-1: padding)
+    const uint16_t *lloc;
+    const double *wx, *wy, *wl, *wh;
+    uint16_t *lloc_s;
+    double *wx_s, *wy_s, *wl_s, *wh_s;      // FP64 step
+    float *wx32, *wy32, *wl32, *wh32;       // mixed step
+    double *gsx32, *gsy32, *lsum32, *hsum32;
+};
+
+// One thread per node: gather its links into the stream order; MX: round the weights and
+// sum the rounded weights.  Padding entries keep weight 0 and local index 0.
+template <bool MX>
+__global__ void k_stream_weights(StreamArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npfb) return;
+    const long long base = a.slice_ptr[i >> 5];
+    const int lane = i & 31;
+    double gx = 0.0, gy = 0.0, lp = 0.0, hy = 0.0;
+    for (int k = 0; k < a.slice_w[i >> 5]; k++) {
+        const long long o = sell_at(base, k, lane);
+        const int q = a.src[o];
+        a.lloc_s[o] = q < 0 ? 0 : a.lloc[q];
+        if constexpr (MX) {
+            const float fx = q < 0 ? 0.0f : (float)a.wx[q], fy = q < 0 ? 0.0f : (float)a.wy[q];
+            const float fl = q < 0 ? 0.0f : (float)a.wl[q], fh = q < 0 ? 0.0f : (float)a.wh[q];
+            a.wx32[o] = fx;
+            a.wy32[o] = fy;
+            a.wl32[o] = fl;
+            a.wh32[o] = fh;
+            gx = gx + (double)fx;
+            gy = gy + (double)fy;
+            lp = lp + (double)fl;
+            hy = hy + (double)fh;
+        } else {
+            a.wx_s[o] = q < 0 ? 0.0 : a.wx[q];
+            a.wy_s[o] = q < 0 ? 0.0 : a.wy[q];
+            a.wl_s[o] = q < 0 ? 0.0 : a.wl[q];
+            a.wh_s[o] = q < 0 ? 0.0 : a.wh[q];
+        }
+    }
+    if constexpr (MX) {
+        a.gsx32[i] = gx;
+        a.gsy32[i] = gy;
+        a.lsum32[i] = lp;
+        a.hsum32[i] = hy;
+    }
+}
+
+// Matching of one half-warp's 16 lanes to the 16 bank pairs for one link slot.
+// cand[r]: the lane's remaining links (SELL entries) valid in this slot; bank(e) their bank
+// pair.  Returns the chosen entry per lane (-1 for lanes without candidates).
+struct HalfWarpMatcher {
+    int owner[16];
+    int choice[16];
+    const std::vector<int> *cand[16];
+    const std::vector<uint16_t> *loc;
+
+    int bank(int e) const { return ((*loc)[e] & kLocMask) & 15; }
+
+    bool augment(int r, unsigned &seen) {
+        for (int e : *cand[r]) {
+            const int b = bank(e);
+            if (seen & (1u << b)) continue;
+            seen |= 1u << b;
+            if (owner[b] < 0 || (owner[b] < 16 && augment(owner[b], seen))) {
+                owner[b] = r;
+                choice[r] = e;
+                return true;
+            }
+        }
+        return false;
+    }
+
+    // padding lanes read local position 0 (bank pair 0)
+    void run(bool pad0) {
+        for (int b = 0; b < 16; b++) owner[b] = -1;
+        if (pad0) owner[0] = 16;  // held by the padding lanes
+        for (int r = 0; r < 16; r++) choice[r] = -1;
+        int order[16], n = 0;
+        unsigned banks[16];
+        for (int r = 0; r < 16; r++) {
+            banks[r] = 0;
+            if (!cand[r]) continue;
+            for (int e : *cand[r]) banks[r] |= 1u << bank(e);
+            order[n++] = r;
+        }
+        // most constrained lanes first
+        std::sort(order, order + n, [&](int a, int b) { return __builtin_popcount(banks[a]) < __builtin_popcount(banks[b]); });
+        for (int q = 0; q < n; q++) {
+            unsigned seen = 0;
+            augment(order[q], seen);
+        }
+        // unmatched lanes: the link in the least used bank
+        int used[16] = {0};
+        for (int b = 0; b < 16; b++) used[b] = owner[b] >= 0 ? 1 : 0;
+        for (int q = 0; q < n; q++) {
+            const int r = order[q];
+            if (choice[r] >= 0) continue;
+            int best = -1, bu = 1 << 30;
+            for (int e : *cand[r])
+                if (used[bank(e)] < bu) { bu = used[bank(e)]; best = e; }
+            choice[r] = best;
+            used[bank(best)]++;
+        }
+    }
+};
+
+}  // namespace
+
+// New SELL order of the links for the time step: src[o] = the SELL entry (in the reference
+// order) whose link goes to entry o, or -1 for padding.  Small links stay in the slots
+// [0, cnt_small) and the other links in [cnt_small, cnt), so the stage kernel (small links)
+// and the filter (all links) see the same sets as in the reference order.
+static int order_links_by_bank(Handle *H, std::vector<int> &src) {
+    const int n = H->npfb, nsl = H->nslices;
+    const long long L = H->nlinks_sell;
+    std::vector<uint16_t> loc(L);
+    std::vector<int> cnt(n), cs(n), sw(nsl);
+    std::vector<long long> sptr(nsl + 1);
+    SUNSET_CUDA(H, cudaMemcpy(loc.data(), H->lloc, L * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cnt.data(), H->cnt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sw.data(), H->slice_w, nsl * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sptr.data(), H->slice_ptr, (nsl + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    src.assign(L, -1);
+    const unsigned nthr = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < nthr; w++) {
+        pool.emplace_back([&, w]() {
+            std::vector<int> small[kSlice], large[kSlice];
+            HalfWarpMatcher M;
+            M.loc = &loc;
+            for (int sl = (int)w; sl < nsl; sl += (int)nthr) {
+                int c[kSlice], c_s[kSlice];
+                for (int lane = 0; lane < kSlice; lane++) {
+                    const int i = sl * kSlice + lane;
+                    c[lane] = i < n ? cnt[i] : 0;
+                    c_s[lane] = i < n ? std::min(cs[i], c[lane]) : 0;
+                    small[lane].clear();
+                    large[lane].clear();
+                    for (int k = 0; k < c[lane]; k++)
+                        (k < c_s[lane] ? small[lane] : large[lane]).push_back((int)sell_at(sptr[sl], k, lane));
+                }
+                for (int k = 0; k < sw[sl]; k++) {
+                    for (int h = 0; h < 2; h++) {
+                        bool pad = false;
+                        for (int r = 0; r < 16; r++) {
+                            const int lane = 16 * h + r;
+                            std::vector<int> *v = k < c_s[lane] ? &small[lane] : k < c[lane] ? &large[lane] : nullptr;
+                            M.cand[r] = (v && !v->empty()) ? v : nullptr;
+                            if (!M.cand[r]) pad = true;
+                        }
+                        M.run(pad);
+                        for (int r = 0; r < 16; r++) {
+                            if (M.choice[r] < 0) continue;
+                            const int lane = 16 * h + r;
+                            std::vector<int> &v = k < c_s[lane] ? small[lane] : large[lane];
+                            v.erase(std::find(v.begin(), v.end(), M.choice[r]));
+                            src[sell_at(sptr[sl], k, lane)] = M.choice[r];
+                        }
+                    }
+                }
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
+    return 0;
+}
+
+// Called once the FP64 weights, their sums and the filter coefficients exist.
+int make_stream_links(Handle *H) {
+    const long long L = H->nlinks_sell;
+    const int n = H->npfb;
+    const bool mx = H->cfg.precision == SUNSET_MIXED;
+    if (L >= (1ll << 31)) return set_err(H, SUNSET_ERR_SCOPE, "the link stream supports at most 2^31 link slots");
+    if (!H->lloc_s) {
+        if (dalloc(H, &H->lloc_s, L)) return SUNSET_ERR_NOMEM;
+        if (mx) {
+            if (dalloc(H, &H->wx32, L) || dalloc(H, &H->wy32, L) || dalloc(H, &H->wl32, L) ||
+                dalloc(H, &H->wh32, L) || dalloc(H, &H->gsx32, n) || dalloc(H, &H->gsy32, n) ||
+                dalloc(H, &H->lsum32, n) || dalloc(H, &H->hsum32, n))
+                return SUNSET_ERR_NOMEM;
+        } else {
+            if (dalloc(H, &H->wx_s, L) || dalloc(H, &H->wy_s, L) || dalloc(H, &H->wl_s, L) || dalloc(H, &H->wh_s, L))
+                return SUNSET_ERR_NOMEM;
+        }
+    }
+    std::vector<int> src;
+    if (int rc = order_links_by_bank(H, src)) return rc;
+    int *d_src = nullptr;
+    if (dalloc(H, &d_src, L)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemcpy(d_src, src.data(), L * sizeof(int), cudaMemcpyHostToDevice));
+    StreamArgs a{n, H->slice_ptr, H->slice_w, d_src, H->lloc, H->wx, H->wy, H->wl, H->wh, H->lloc_s,
+                 H->wx_s, H->wy_s, H->wl_s, H->wh_s, H->wx32, H->wy32, H->wl32, H->wh32,
+                 H->gsx32, H->gsy32, H->lsum32, H->hsum32};
+    if (mx) k_stream_weights<true><<<(n + 255) / 256, 256, 0, H->stream>>>(a);
+    else k_stream_weights<false><<<(n + 255) / 256, 256, 0, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    dfree(H, d_src);
+    return 0;
+}
+
+}  // namespace sunset

@@ -150,16 +150,18 @@ class Workload:
 # Radii.  The reference adapts each node's stencil (labf.F90:1079-1721); with one fixed
 # radius on jittered nodes the nominal radii are too small: at 2.6 s (order 4), 3.2 s
 # (order 6) and 4.2 s (order 8) some nodes get near-singular moment matrices (max
-# |w_lap| s^2 ~ 1e4) and the reference algorithm diverges within a few steps.  Taking
-# the radius from the stated neighbour counts, r = s sqrt(K/pi), works at order 8
-# (K ~ 70 -> 4.72 s); at order 6 the 512^2 set still holds a few stencils whose filter
-# row sums exceed 2 at K ~ 45 (3.78 s) and 4.0 s, and the step diverges within 200
-# steps, so order 6 uses 4.2 s (K ~ 55).  Order 4 uses 3.0 s (K ~ 28).
+# |w_lap| s^2 ~ 1e4) and the reference algorithm diverges within a few steps.  At order 6
+# the 512^2 set still holds a few stencils whose filter row sums exceed 2 at K ~ 45
+# (3.78 s) and 4.0 s, and the step diverges within 200 steps, so order 6 uses 4.2 s
+# (K ~ 55).  At order 8 the radius from the stated neighbour count, r = s sqrt(K/pi) with
+# K ~ 70 (4.72 s), keeps 100 steps finite but grows an unstable mode that overflows before
+# step 500 (max |rho - 1| 4e-9 at step 50, 3e-4 at step 400); the reference's own initial
+# stencil for order 8, h = 2.7 s (common_parameter.F90:55, radius ss*h = 5.4 s, K ~ 92),
+# stays bounded through 500 steps.  Order 4 uses 3.0 s (K ~ 28).
 WORKLOADS = {
     "periodic-di-o4-16k": Workload("periodic-di-o4-16k", 128, 4, 3.0, "di", steps=100),
     "periodic-lc-o6-262k": Workload("periodic-lc-o6-262k", 512, 6, 4.2, "lc", epsPTT=0.25, steps=200),
-    "periodic-chl-o8-1m": Workload("periodic-chl-o8-1m", 1024, 8, math.sqrt(70.0 / math.pi), "chl",
-                                   Wi=2.0, beta=0.1, steps=500),
+    "periodic-chl-o8-1m": Workload("periodic-chl-o8-1m", 1024, 8, 5.4, "chl", Wi=2.0, beta=0.1, steps=500),
 }
 
 
