@@ -180,12 +180,14 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload):
-    """dram bytes per stage-kernel launch from the committed ncu summary, if present."""
+def profiled_traffic(workload, precision):
+    """DRAM bytes (read + write) per stage-kernel launch from the committed ncu summary of
+    the same workload and precision, if present."""
     path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.md")
+    key = f"traffic_bytes_per_launch[{workload}/{precision}]:"
     try:
         for line in open(path):
-            if line.startswith(f"traffic_bytes_per_launch[{workload}]:"):
+            if line.startswith(key):
                 return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
@@ -300,14 +302,17 @@ def main():
     ms_max = max_over_ranks(dist, ms, device=f"cuda:{local}")
     value = ws * ns.n * args.steps / (ms_max * 1e-3)
 
-    # kernel roofline: the RK stage kernel, timed alone with CUDA events on its stream
-    stage_ms, stage_bytes = g.time_stage_kernel(20)
+    # kernel roofline: the RK stage kernel inside real steps (the same step sequence launched
+    # kernel by kernel, CUDA events on the handle's stream around every stage launch)
+    roof_steps = max(3, min(args.steps, 50))
+    stage_ms, stage_bytes = g.time_stage_kernel(roof_steps)
     peak, peak_kind = measured_peaks()
     achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
-    traffic = profiled_traffic(wl.name)
+    traffic = profiled_traffic(wl.name, args.precision)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_stage (one RK stage: stencils + rhs + update)",
-                "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms, "peak_source": peak_kind}
+                "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms, "peak_source": peak_kind,
+                "method": f"CUDA events around each of the 4 stage launches of {roof_steps} steps"}
 
     # end to end through the C-ABI with host buffers: per step, copy the evolved fields in
     # from pinned host memory, run the step, copy them back

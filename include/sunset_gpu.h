@@ -134,8 +134,10 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
    device time of the nsteps steps. */
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
-/* Stage-kernel timing: runs `reps` launches of the RK stage kernel (stage 1) on the
-   current state and returns the mean device time per launch in ms. */
+/* Stage-kernel timing: runs `reps` fixed-dt steps at the current dt, launched kernel by
+   kernel (not as a graph) with CUDA events on the handle's stream around each RK stage
+   launch, and returns the mean stage-kernel time per launch in ms and its algorithmic
+   bytes per launch.  Advances the state by `reps` steps. */
 int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
                              double *bytes_per_launch);
 

@@ -74,19 +74,6 @@ __device__ __forceinline__ const double *gather_src(const Fields &F, int f) {
     return F.c[f - 6];
 }
 
-// The block's halo (fields of every node its links reach) into shared memory, laid out
-// field-major with stride hmax.  All threads of the block take part.
-template <int NG, typename SRC>
-__device__ __forceinline__ void load_halo(const StageArgs &A, double *sm, SRC src) {
-    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
-    const int hm = A.hmax;
-    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
-        const int node = __ldg(A.halo + hb + h);
-#pragma unroll
-        for (int f = 0; f < NG; f++) sm[f * hm + h] = __ldg(src(f) + node);
-    }
-    __syncthreads();
-}
 
 // cp.async (global -> shared, completion tracked per thread in commit groups), with memory
 // clobbers so the compiler keeps shared-memory reads after the wait that covers them.
@@ -103,6 +90,24 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The block's halo (fields of every node its links reach) into shared memory, laid out
+// field-major with stride hmax, by cp.async so all of a thread's copies are in flight at
+// once.  All threads of the block take part; the wait also covers any copies the thread
+// issued before.
+template <int NG, typename SRC>
+__device__ __forceinline__ void load_halo(const StageArgs &A, double *sm, SRC src) {
+    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
+    const int hm = A.hmax;
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        const int node = __ldg(A.halo + hb + h);
+#pragma unroll
+        for (int f = 0; f < NG; f++) cp_async<8>(&sm[f * hm + h], src(f) + node);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
 }
 
 // Per-thread ring of link pairs in shared memory, filled by cp.async (LDGSTS).  Thread t
@@ -158,7 +163,13 @@ struct LinkRing {
 };
 
 // Ring depth: FP64 pairs are 52 bytes a thread, FP32 ones 28.
-__host__ __device__ constexpr int ring_depth(bool mx) { return mx ? 4 : 2; }
+#ifndef SUNSET_RING_FP64
+#define SUNSET_RING_FP64 2
+#endif
+#ifndef SUNSET_RING_MIXED
+#define SUNSET_RING_MIXED 4
+#endif
+__host__ __device__ constexpr int ring_depth(bool mx) { return mx ? SUNSET_RING_MIXED : SUNSET_RING_FP64; }
 
 // Doubles of the shared-memory halo, rounded up so the ring after it is 16-byte aligned.
 __host__ __device__ inline size_t halo_doubles(int ng, int hmax) { return ((size_t)ng * hmax + 1) & ~(size_t)1; }
@@ -326,7 +337,10 @@ __device__ __forceinline__ void block_min_bits(unsigned long long v, unsigned lo
 // Resident blocks per SM the stage kernel is compiled for (up to 85 registers a thread):
 // the tile halo plus the link ring take 55-70 KB of shared memory on the order-6 and
 // order-8 sets, so a fourth block would not fit anyway.
-__host__ __device__ constexpr int stage_min_blocks(int) { return 3; }
+#ifndef SUNSET_STAGE_BLOCKS
+#define SUNSET_STAGE_BLOCKS 3
+#endif
+__host__ __device__ constexpr int stage_min_blocks(int) { return SUNSET_STAGE_BLOCKS; }
 
 // One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).  One
 // block per tile of kTile nodes; the tile's halo is staged in shared memory first.
@@ -915,8 +929,10 @@ int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     return 0;
 }
 
+// The kernels of one step.  stage_ev (optional, 8 events): recorded before and after each
+// of the four RK stage launches, for timing the stage kernel inside a real step sequence.
 template <int FORM>
-int launch_step_kernels(Handle *H, int from, int pid) {
+int launch_step_kernels(Handle *H, int from, int pid, cudaEvent_t *stage_ev) {
     const int TB = 128;
     cudaStream_t st = H->stream;
     const bool mx = is_mx(H);
@@ -924,7 +940,9 @@ int launch_step_kernels(Handle *H, int from, int pid) {
     int b = from;
     for (int s = 0; s < 4; s++) {
         StageArgs A = make_args(H, b, s, true);
+        if (stage_ev) SUNSET_CUDA(H, cudaEventRecord(stage_ev[2 * s], st));
         if (int rc = launch_stage_any(H, A, mx)) return rc;
+        if (stage_ev) SUNSET_CUDA(H, cudaEventRecord(stage_ev[2 * s + 1], st));
         b ^= 1;
     }
     StageArgs F = make_args(H, b, 5, true);
@@ -937,12 +955,12 @@ int launch_step_kernels(Handle *H, int from, int pid) {
     return 0;
 }
 
-int launch_step(Handle *H, int from, int pid) {
+int launch_step(Handle *H, int from, int pid, cudaEvent_t *stage_ev = nullptr) {
     switch (H->cfg.form) {
-    case SUNSET_FORM_DI: return launch_step_kernels<SUNSET_FORM_DI>(H, from, pid);
-    case SUNSET_FORM_CHL: return launch_step_kernels<SUNSET_FORM_CHL>(H, from, pid);
-    case SUNSET_FORM_LC: return launch_step_kernels<SUNSET_FORM_LC>(H, from, pid);
-    default: return launch_step_kernels<SUNSET_FORM_NEWT>(H, from, pid);
+    case SUNSET_FORM_DI: return launch_step_kernels<SUNSET_FORM_DI>(H, from, pid, stage_ev);
+    case SUNSET_FORM_CHL: return launch_step_kernels<SUNSET_FORM_CHL>(H, from, pid, stage_ev);
+    case SUNSET_FORM_LC: return launch_step_kernels<SUNSET_FORM_LC>(H, from, pid, stage_ev);
+    default: return launch_step_kernels<SUNSET_FORM_NEWT>(H, from, pid, stage_ev);
     }
 }
 
@@ -1111,44 +1129,51 @@ int reduce_ke_mass(Handle *H, double *ke, double *mass) {
     return 0;
 }
 
+// Average duration of the RK stage kernel inside real steps: `reps` steps at the current dt
+// (fixed-dt mode), each launched directly rather than as a graph, with CUDA events on the
+// handle's stream around each of the four stage launches.  Advances the state by reps
+// steps.  Also returns the stage kernel's algorithmic bytes per launch.
 int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     int rc = upload_consts(H);
     if (rc) return rc;
-    const int TB = 128, nblk = (H->nslices * kSlice + TB - 1) / TB;
-    // stage 4 (right-hand side only) reads what an RK stage reads and writes the rhs arrays;
-    // use stage 1 itself: it reads the current buffer and writes the other one.
+    if (reps < 1) reps = 1;
     const bool mx = is_mx(H);
-    StageArgs A = make_args(H, H->cur, 1, true);
-    cudaEvent_t e0, e1;
-    SUNSET_CUDA(H, cudaEventCreate(&e0));
-    SUNSET_CUDA(H, cudaEventCreate(&e1));
-    auto launch = [&]() { launch_stage_any(H, A, mx); };
-    for (int r = 0; r < 3; r++) launch();
-    SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
-    for (int r = 0; r < reps; r++) launch();
-    SUNSET_CUDA(H, cudaEventRecord(e1, H->stream));
-    SUNSET_CUDA(H, cudaEventSynchronize(e1));
-    float t = 0.f;
-    SUNSET_CUDA(H, cudaEventElapsedTime(&t, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    *ms = (double)t / reps;
-    // algorithmic bytes of one stage launch: small-link stream (16-bit local index + 3
-    // weights of 8 or 4 bytes), the per-node state read once, registers S and E read +
-    // written (8 bytes each, 4 in the mixed path), new state written.
+    std::vector<cudaEvent_t> ev(8 * (size_t)reps);
+    for (auto &e : ev) SUNSET_CUDA(H, cudaEventCreate(&e));
+    for (int r = 0; r < reps; r++) {
+        if ((rc = launch_step(H, H->cur, 0, ev.data() + 8 * r))) break;
+        H->cur ^= 1;
+    }
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    double tot = 0.0;
+    for (int k = 0; k < 4 * reps && !rc; k++) {
+        float t = 0.f;
+        SUNSET_CUDA(H, cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]));
+        tot += t;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    *ms = tot / (4.0 * reps);
+    // Algorithmic bytes of one stage launch, averaged over the four stages: each node's
+    // small links once (16-bit local index + 3 weights of 8 bytes, 4 in the mixed path;
+    // links, not padded SELL slots), its state and derived fields read once (the halo
+    // copies of neighbours' values are re-reads), the RK registers S and E read in stages
+    // 1-3 and written in stages 0-2 (8 bytes, 4 in the mixed path), the next state with
+    // its derived fields written (conservative fields only after stage 3), and the stencil
+    // sums and ordinate read.
     long long links = 0;
     {
-        std::vector<int> ws(H->nslices);
-        cudaMemcpy(ws.data(), H->slice_ws, ws.size() * sizeof(int), cudaMemcpyDeviceToHost);
-        for (int w : ws) links += (long long)w * kSlice;
+        std::vector<int> cs(H->npfb);
+        SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int c : cs) links += c;
     }
     const int form = H->cfg.form;
-    const int nf = form == SUNSET_FORM_DI ? 7 : 6;         // evolved fields (S and E registers)
-    const int nread = form == SUNSET_FORM_DI ? 9 : 13;      // state + derived fields of a node
-    const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;     // next state + derived fields
+    const int nf = form == SUNSET_FORM_DI ? 7 : 6;      // evolved fields (S and E registers)
+    const int nread = form == SUNSET_FORM_DI ? 9 : 13;   // state + derived fields of a node
+    const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;  // next state + derived fields (stages 0-2)
     const double wb = mx ? 4.0 : 8.0;
-    *bytes = (double)links * (2 + 3 * wb) + (double)H->npfb * (8.0 * nread + 4.0 * wb * nf + 8.0 * nwrite) +
-             (double)H->npfb * 8.0 * 4;  // sums + ordinate
+    *bytes = (double)links * (2 + 3 * wb) +
+             (double)H->npfb * (8.0 * nread + 3.0 * nf * wb + 8.0 * (3.0 * nwrite + 7.0) / 4.0 + 8.0 * 4);
     return 0;
 }
 

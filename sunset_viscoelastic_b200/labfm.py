@@ -293,6 +293,8 @@ class Sunset:
                                          C.c_void_p(state_out_ptr)))
 
     def time_stage_kernel(self, reps=20):
+        """(mean ms per RK stage launch inside `reps` real steps, algorithmic bytes per launch);
+        advances the state by reps steps."""
         ms, by = C.c_double(), C.c_double()
         self._chk(self.L.sunset_time_stage_kernel(self.h, int(reps), C.byref(ms), C.byref(by)))
         return ms.value, by.value
