@@ -285,18 +285,25 @@ void or_abfs(int order, double x, double y, double *out) {
         }
 }
 
-/* labf.F90:1041-1077, 1D monomials and ABFs for the tangential boundary operators */
-static void monomials1D(double x, double *out) {
-    double x2 = x * x, x3 = x2 * x, x4 = x3 * x, x5 = x4 * x, x6 = x5 * x;
-    out[0] = x;
-    out[1] = 0.5 * x2;
-    out[2] = (1.0 / 6.0) * x3;
-    out[3] = (1.0 / 24.0) * x4;
-    out[4] = (1.0 / 120.0) * x5;
-    out[5] = (1.0 / 720.0) * x6;
+/* labf.F90:1041-1048, 1-D monomials of the tangential boundary operators, as written */
+static void monomials1D(double z, double *out) {
+    double z2 = z * z;
+    out[0] = z;
+    out[1] = 0.5 * z2;
+    out[2] = ((1.0 / 6.0) * z) * z2;
+    out[3] = (z2 * z2) / 24.0;
+    out[4] = ((z2 * z2) * z) / 120.0;
+    out[5] = ((z2 * z2) * z2) / 720.0;
 }
-static void abfs1D(double x, double ff1, double *out) {
-    for (int k = 0; k < 6; k++) out[k] = hermite(k + 1, x) * ff1;
+/* labf.F90:1050-1077 (ABF==2): Hermite ABFs of the 1-D operators */
+static void abfs1D(double z, double ff1, double *out) {
+    const double oosqrt2 = 1.0 / sqrt(2.0);
+    out[0] = ff1 * hermite(1, z);
+    out[1] = ff1 * hermite(2, z);
+    out[2] = (ff1 * oosqrt2) * hermite(3, z);
+    out[3] = ff1 * hermite(4, z);
+    out[4] = ff1 * hermite(5, z);
+    out[5] = ff1 * hermite(6, z);
 }
 
 /* ---------------------------------------------------------------------------------------
@@ -1034,10 +1041,271 @@ int or_calc_labf_weights(OrSim *s) {
     return 0;
 }
 
-/* labf.F90:505-1039 -- boundary framework (walls / inflow / outflow with FD rows). */
+/* ---------------------------------------------------------------------------------------
+ * labf.F90:505-1039 -- calc_boundary_weights.  Boundary node i0 and its four FD rows
+ * i1..i4 (the nodes that follow it): normal derivatives by 5-point finite differences,
+ * tangential ones by 6th-order 1-D LABFM on the same layer, curvature correction, and the
+ * rotation of rows 1-2 into the x-y frame.  Wall first derivatives stay in the
+ * normal-tangent frame (the wall equations are solved there).
+ * ------------------------------------------------------------------------------------- */
+static double dot6(const double *a, const double *b) { /* dot_product, summed in order */
+    double t = 0.0;
+    for (int k = 0; k < 6; k++) t = t + a[k] * b[k];
+    return t;
+}
+
+/* 1-D LABFM along the tangent (xt,yt) of node i, over the links on i's own layer:
+   assemble the 6x6 moment matrix (labf.F90:696-722 and the row variants). */
+static void assemble_1d(const OrSim *s, int i, double xt, double yt, double hh, double *amat) {
+    const int *lk = s->ij_link + (size_t)i * s->nplink;
+    double xvec[6], gvec[6];
+    memset(amat, 0, sizeof(double) * 36);
+    for (int k = 0; k < s->ij_count[i]; k++) {
+        int j = lk[k];
+        if (s->type[j] != s->type[i]) continue;
+        double rijx = s->rx[i] - s->rx[j], rijy = s->ry[i] - s->ry[j];
+        double x = -(rijx * xt + rijy * yt);
+        if (i == j) x = 0.0;
+        monomials1D(x / hh, xvec);
+        double ff1 = or_fac(fabs(x / hh), s->h3);
+        x = x / hh;
+        abfs1D(x, ff1, gvec);
+        for (int i1 = 0; i1 < 6; i1++)
+            for (int i2 = 0; i2 < 6; i2++) amat[i1 + 6 * i2] = amat[i1 + 6 * i2] + xvec[i1] * gvec[i2];
+    }
+}
+
+/* the 1-D ABF vector of link j of node i (labf.F90:737-748) */
+static void abf_1d_link(const OrSim *s, int i, int j, double xt, double yt, double hh, double *gvec) {
+    double rijx = s->rx[i] - s->rx[j], rijy = s->ry[i] - s->ry[j];
+    double x = -(rijx * xt + rijy * yt);
+    if (i == j) x = 0.0;
+    double ff1 = or_fac(fabs(x / hh), s->h3);
+    x = x / hh;
+    abfs1D(x, ff1, gvec);
+}
+
 int or_calc_boundary_weights(OrSim *s) {
     if (s->nb == 0) return 0;
-    return fail(s, "calc_boundary_weights (labf.F90:505-1039) is not restated yet");
+    const int npfb = s->npfb, nplink = s->nplink, nb = s->nb;
+    FREE(s->wb_grad2);
+    s->wb_grad2 = (double *)xcalloc((size_t)3 * nplink * nb, sizeof(double));
+#define WB(jj, k, c) s->wb_grad2[((size_t)(jj) * nplink + (k)) * 3 + (c)]
+#define WG(i, k, c) s->w_grad[2 * ((size_t)(i) * nplink + (k)) + (c)]
+#define WL(i, k) s->w_lap[(size_t)(i) * nplink + (k)]
+#define WH(i, k) s->w_hyp[(size_t)(i) * nplink + (k)]
+    /* preface, :541-565: boundary nodes keep only links on their own layer and their FD
+       children */
+    int *tmp = (int *)xcalloc(nplink, sizeof(int));
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        int kk = s->type[i], nsize = s->ij_count[i];
+        int *lk = s->ij_link + (size_t)i * nplink;
+        memcpy(tmp, lk, sizeof(int) * nsize);
+        for (int k = 0; k < nplink; k++) lk[k] = -1;
+        s->ij_count[i] = 0;
+        for (int k = 0; k < nsize; k++) {
+            int j = tmp[k];
+            if (s->type[j] == kk) lk[s->ij_count[i]++] = j;
+            if (j < npfb && s->fd_parent[j] == i) lk[s->ij_count[i]++] = j;
+        }
+        s->ij_count_small[i] = s->ij_count[i];
+    }
+    free(tmp);
+
+    /* boundary node: normal operators, :572-612 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        double dx = s->sp[i], dx2 = dx * dx;
+        for (int k = 0; k < nplink; k++) {
+            WG(i, k, 0) = 0.0; WG(i, k, 1) = 0.0; WH(i, k) = 0.0;
+            WB(jj, k, 0) = 0.0; WB(jj, k, 1) = 0.0; WB(jj, k, 2) = 0.0;
+        }
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            if (j >= npfb) continue;
+            if (s->fd_parent[j] != i) continue;
+            int t = s->type[j];
+            if (j == i) WG(i, k, 0) = 0.0;
+            if (t == -1) WG(i, k, 0) = 4.0 / dx;
+            if (t == -2) WG(i, k, 0) = -(3.0 / dx);
+            if (t == -3) WG(i, k, 0) = (4.0 / 3.0) / dx;
+            if (t == -4) WG(i, k, 0) = -(0.25 / dx);
+            if (j == i) WB(jj, k, 0) = 0.0;
+            if (t == -1) WB(jj, k, 0) = -((104.0 / 12.0) / dx2);
+            if (t == -2) WB(jj, k, 0) = (114.0 / 12.0) / dx2;
+            if (t == -3) WB(jj, k, 0) = -((56.0 / 12.0) / dx2);
+            if (t == -4) WB(jj, k, 0) = (11.0 / 12.0) / dx2;
+        }
+    }
+    /* first row: normal operators, :615-645 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj] + 1;
+        double dx = s->sp[i], dx2 = dx * dx; /* dx2 of the boundary node's row: same s */
+        for (int k = 0; k < nplink; k++) { WG(i, k, 0) = 0.0; WG(i, k, 1) = 0.0; WL(i, k) = 0.0; }
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        int par = s->fd_parent[i];
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            if (j >= npfb) continue;
+            int t = s->type[j], same = s->fd_parent[j] == par;
+            if (j == par) WG(i, k, 0) = -(0.25 / dx);
+            if (j == i) WG(i, k, 0) = 0.0;
+            if (t == -2 && same) WG(i, k, 0) = 1.5 / dx;
+            if (t == -3 && same) WG(i, k, 0) = -(0.5 / dx);
+            if (t == -4 && same) WG(i, k, 0) = (1.0 / 12.0) / dx;
+            if (j == par) WL(i, k) = (11.0 / 12.0) / dx2;
+            if (j == i) WL(i, k) = 0.0;
+            if (t == -2 && same) WL(i, k) = (6.0 / 12.0) / dx2;
+            if (t == -3 && same) WL(i, k) = (4.0 / 12.0) / dx2;
+            if (t == -4 && same) WL(i, k) = -((1.0 / 12.0) / dx2);
+        }
+    }
+    /* second row: normal operators, :648-676 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj] + 2;
+        double dx = s->sp[i], dx2 = dx * dx;
+        for (int k = 0; k < nplink; k++) { WG(i, k, 0) = 0.0; WG(i, k, 1) = 0.0; WL(i, k) = 0.0; }
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        int par = s->fd_parent[i];
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            if (j >= npfb) continue;
+            int t = s->type[j], same = s->fd_parent[j] == par;
+            if (j == par) WG(i, k, 0) = (1.0 / 12.0) / dx;
+            if (t == -1 && same) WG(i, k, 0) = -((8.0 / 12.0) / dx);
+            if (j == i) WG(i, k, 0) = (0.0 / 12.0) / dx;
+            if (t == -3 && same) WG(i, k, 0) = (8.0 / 12.0) / dx;
+            if (t == -4 && same) WG(i, k, 0) = -((1.0 / 12.0) / dx);
+            if (j == par) WL(i, k) = -((1.0 / 12.0) / dx2);
+            if (t == -1 && same) WL(i, k) = (16.0 / 12.0) / dx2;
+            if (j == i) WL(i, k) = (0.0 / 12.0) / dx2;
+            if (t == -3 && same) WL(i, k) = (16.0 / 12.0) / dx2;
+            if (t == -4 && same) WL(i, k) = -((1.0 / 12.0) / dx2);
+        }
+    }
+
+    SvdWork sw;
+    svdw_init(&sw, 6);
+    double amat[36], bvect[6], bvectt[6], bvecthyp[6], gvec[6];
+    /* boundary node: transverse operators, :688-755 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        double xt = -s->rny[i], yt = s->rnx[i], hh = s->h[i];
+        assemble_1d(s, i, xt, yt, hh, amat);
+        memset(bvect, 0, sizeof bvect); bvect[0] = 1.0;
+        memset(bvectt, 0, sizeof bvectt); bvectt[1] = 1.0;
+        memset(bvecthyp, 0, sizeof bvecthyp); bvecthyp[3] = -1.0;
+        if (svd_factor(amat, 6, &sw)) { svdw_free(&sw); return fail(s, "svd_solve: no convergence (boundary node %d)", i); }
+        svd_apply(&sw, 6, bvect);
+        svd_apply(&sw, 6, bvectt);
+        svd_apply(&sw, 6, bvecthyp);
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            if (s->type[j] != s->type[i]) continue;
+            abf_1d_link(s, i, j, xt, yt, hh, gvec);
+            WG(i, k, 1) = dot6(bvect, gvec) / hh;
+            WB(jj, k, 1) = (dot6(bvectt, gvec) / hh) / hh;
+            WH(i, k) = WH(i, k) + dot6(bvecthyp, gvec);
+        }
+    }
+    /* first and second rows: transverse operators on a tangent rotated by the tangential
+       gradient of the resolution, :758-955 */
+    for (int row = 1; row <= 2; row++) {
+        for (int jj = 0; jj < nb; jj++) {
+            int i = s->boundary_list[jj] + row;
+            double hh = s->h[i];
+            int ii = s->fd_parent[i];
+            double grads = 0.0;
+            const int *lp = s->ij_link + (size_t)ii * nplink;
+            for (int k = 0; k < s->ij_count[ii]; k++) {
+                int j = lp[k];
+                grads = grads + (s->sp[j] - s->sp[ii]) * WG(ii, k, 1);
+            }
+            grads = -atan(grads);
+            double xt = cos(grads) * (-s->rny[i]) - sin(grads) * s->rnx[i];
+            double yt = sin(grads) * (-s->rny[i]) + cos(grads) * s->rnx[i];
+            assemble_1d(s, i, xt, yt, hh, amat);
+            memset(bvect, 0, sizeof bvect); bvect[0] = 1.0;
+            memset(bvectt, 0, sizeof bvectt); bvectt[1] = 1.0;
+            if (svd_factor(amat, 6, &sw)) { svdw_free(&sw); return fail(s, "svd_solve: no convergence (row node %d)", i); }
+            svd_apply(&sw, 6, bvect);
+            svd_apply(&sw, 6, bvectt);
+            const int *lk = s->ij_link + (size_t)i * nplink;
+            for (int k = 0; k < s->ij_count[i]; k++) {
+                int j = lk[k];
+                if (s->type[j] != s->type[i]) continue;
+                abf_1d_link(s, i, j, xt, yt, hh, gvec);
+                WG(i, k, 1) = dot6(bvect, gvec) / hh;
+                WL(i, k) = WL(i, k) + (dot6(bvectt, gvec) / hh) / hh;
+            }
+            for (int k = 0; k < s->ij_count[i]; k++)
+                WG(i, k, 1) = (1.0 / cos(grads)) * WG(i, k, 1) - tan(grads) * WG(i, k, 0);
+        }
+    }
+    svdw_free(&sw);
+
+    /* wall curvature 1/R, :965-982 */
+    double *ooR = (double *)xcalloc(nb, sizeof(double));
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        if (s->type[i] != 0) continue;
+        double tmp_t = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            int j = lk[k];
+            if (s->type[j] != s->type[i]) continue;
+            double tmp_n = ((s->rnx[j] * s->rnx[i] + s->rny[j] * s->rny[i]) + 0.0 * 0.0) - 1.0;
+            tmp_t = tmp_t + WB(jj, k, 1) * tmp_n;
+        }
+        ooR[jj] = sqrt(fabs(tmp_t));
+    }
+    /* outflow: reverse the first-derivative weights, :986-991 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        if (s->type[i] == 2)
+            for (int k = 0; k < nplink; k++) { WG(i, k, 0) = -WG(i, k, 0); WG(i, k, 1) = -WG(i, k, 1); }
+    }
+    /* divergence term in the Laplacian of rows 1 and 2, :994-1003 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj] + 1;
+        if (s->type[i - 1] == 0)
+            for (int k = 0; k < nplink; k++) WL(i, k) = WL(i, k) + (WG(i, k, 0) * ooR[jj]) / (1.0 + ooR[jj] * s->sp[i]);
+        i = s->boundary_list[jj] + 2;
+        if (s->type[i - 2] == 0)
+            for (int k = 0; k < nplink; k++)
+                WL(i, k) = WL(i, k) + (WG(i, k, 0) * ooR[jj]) / (1.0 + (2.0 * ooR[jj]) * s->sp[i]);
+    }
+    /* walls: second normal derivative with the curvature term, Laplacian = sum, :1007-1016 */
+    for (int jj = 0; jj < nb; jj++) {
+        int i = s->boundary_list[jj];
+        if (s->type[i] != 0) continue;
+        for (int k = 0; k < s->ij_count[i]; k++) {
+            WB(jj, k, 0) = WB(jj, k, 0) + WG(i, k, 0) * ooR[jj];
+            WL(i, k) = WB(jj, k, 0) + WB(jj, k, 1);
+        }
+    }
+    /* rows 1 and 2: first derivatives from the normal-tangent frame to x-y, :1019-1035 */
+    for (int jj = 0; jj < nb; jj++) {
+        int ib = s->boundary_list[jj];
+        double xn = s->rnx[ib], yn = s->rny[ib];
+        for (int row = 1; row <= 2; row++) {
+            int i = ib + row;
+            for (int k = 0; k < s->ij_count[i]; k++) {
+                double g1 = WG(i, k, 0), g2 = WG(i, k, 1);
+                WG(i, k, 0) = (0.0 + xn * g1) + (-yn) * g2;
+                WG(i, k, 1) = (0.0 + yn * g1) + xn * g2;
+            }
+        }
+    }
+    free(ooR);
+#undef WB
+#undef WG
+#undef WL
+#undef WH
+    return 0;
 }
 
 /* labf.F90:396-451 */
@@ -1071,6 +1339,23 @@ int or_calc_labf_sums(OrSim *s) {
             s->w_lap[o] = (s->w_lap[o] / L) / L;
         }
         s->w_hyp_sum[i] = hy;
+    }
+    /* second derivatives on the boundary, :426-446 */
+    if (s->nb != 0) {
+        FREE(s->wb_grad2_sum);
+        s->wb_grad2_sum = (double *)xcalloc(3 * (size_t)s->nb, sizeof(double));
+        for (int jj = 0; jj < s->nb; jj++) {
+            int i = s->boundary_list[jj];
+            double *sum = s->wb_grad2_sum + 3 * jj;
+            for (int k = 0; k < s->ij_count[i]; k++)
+                for (int c = 0; c < 3; c++) sum[c] = sum[c] + s->wb_grad2[((size_t)jj * nplink + k) * 3 + c];
+            for (int c = 0; c < 3; c++) sum[c] = (sum[c] / L) / L;
+            for (int k = 0; k < nplink; k++)
+                for (int c = 0; c < 3; c++) {
+                    double *w = &s->wb_grad2[((size_t)jj * nplink + k) * 3 + c];
+                    *w = (*w / L) / L;
+                }
+        }
     }
     return 0;
 }

@@ -79,6 +79,50 @@ def jittered_lattice(nside: int, jitter: float = 0.3, seed: int = 12345,
                    s=np.full(n, s), xmin=0.0, xmax=length, ymin=0.0, ymax=length, bcond=(1, 1, 1, 1))
 
 
+def _with_gaps(types: np.ndarray) -> np.ndarray:
+    """Global indices leaving room for the four FD rows the reader adds after each boundary
+    node (it numbers them global_index + 1..4, setup_domain.F90:183-190)."""
+    step = np.where((types >= 0) & (types <= 2), 5, 1)
+    return (np.cumsum(step) - step + 1).astype(np.int32)
+
+
+def channel(ny_cells: int, lx: float = 1.0, ly: float = 1.0, jitter: float = 0.3,
+            seed: int = 12345) -> NodeSet:
+    """Walled channel, periodic in x on [0, lx), walls (node_type 0) at y = 0 and y = ly
+    with normals into the fluid.  Spacing s = ly / ny_cells.  Wall nodes sit at
+    x = (i + 1/2) s; the reader adds their FD rows at 1..4 s along the normal.  The interior
+    is the jittered lattice (+-jitter s per axis, default_rng(seed)) on the rows 5..ny_cells-5,
+    which keeps it clear of the FD rows."""
+    s = ly / ny_cells
+    nxc = int(round(lx / s))
+    xs = (np.arange(nxc) + 0.5) * s
+    rng = np.random.default_rng(seed)
+    yj = np.arange(5, ny_cells - 4) * s
+    ix, iy = np.meshgrid(xs, yj, indexing="xy")
+    n_int = ix.size
+    xi = ix.ravel() + rng.uniform(-jitter * s, jitter * s, n_int)
+    yi = iy.ravel() + rng.uniform(-jitter * s, jitter * s, n_int)
+    x = np.concatenate([xs, xi, xs])
+    y = np.concatenate([np.zeros(nxc), yi, np.full(nxc, ly)])
+    t = np.concatenate([np.zeros(nxc, np.int32), np.full(n_int, 999, np.int32), np.zeros(nxc, np.int32)])
+    nx = np.zeros(len(x))
+    ny = np.concatenate([np.ones(nxc), np.zeros(n_int), -np.ones(nxc)])
+    return NodeSet(x=x, y=y, node_type=t, nx=nx, ny=ny, s=np.full(len(x), s), xmin=0.0, xmax=lx,
+                   ymin=0.0, ymax=ly, bcond=(1, 1, 0, 0), gi=_with_gaps(t))
+
+
+def poiseuille_state(ns: NodeSet, G: float, mu_total: float, lam: float, ly: float = 1.0):
+    """Steady Oldroyd-B Poiseuille flow driven by a body force G in x between walls at
+    y = 0 and ly: u = G y (ly - y) / (2 mu_total), v = 0, rho = 1, c_xy = lam u',
+    c_xx = 1 + 2 (lam u')^2, c_yy = c_zz = 1.  (Values at the FD rows follow from the
+    reader's positions, so they are returned for the reader's node list.)"""
+    u = G * ns.y * (ly - ns.y) / (2.0 * mu_total)
+    du = G * (ly - 2.0 * ns.y) / (2.0 * mu_total)
+    n = ns.n
+    return dict(ro=np.ones(n), u=u, v=np.zeros(n), cxx=1.0 + 2.0 * (lam * du) ** 2, cxy=lam * du,
+                cyy=np.ones(n), czz=np.ones(n))
+
+
 def read_ipart(path: str) -> NodeSet:
     """Reader following setup_domain.F90:93-199 (non-MPI branch)."""
     with open(path) as f:

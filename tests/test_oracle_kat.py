@@ -16,7 +16,8 @@ from fractions import Fraction
 import numpy as np
 import pytest
 
-from sunset_viscoelastic_b200.nodesets import NodeSet, WORKLOADS, initial_state, jittered_lattice
+from sunset_viscoelastic_b200.nodesets import (NodeSet, WORKLOADS, channel, initial_state, jittered_lattice,
+                                               poiseuille_state)
 import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -228,3 +229,60 @@ def test_transforms_round_trip():
         np.testing.assert_allclose(s["cxx"], a, rtol=1e-13)
         np.testing.assert_allclose(s["cxy"], b, rtol=1e-10, atol=1e-12)
         np.testing.assert_allclose(s["cyy"], d, rtol=1e-13)
+
+
+# ------------------------------------------------------------------------------- wall closures
+def channel_oracle(order, form="di", ncell=32, G=8.0, Wi=0.5, beta=0.59):
+    o = O.Oracle(form=form, order=order, Re=1.0, Wi=Wi, beta=beta, Ma=0.1, grav=(G, 0.0, 0.0),
+                 kolmogorov_forcing=0)
+    o.build_domain(channel(ncell)).setup()
+    return o
+
+
+@pytest.mark.parametrize("order", [6, 8])
+def test_boundary_operators_reproduce_polynomials(order):
+    """labf.F90:505-1039 on a straight walled channel.  Wall nodes: first derivatives in the
+    normal-tangent frame, the normal one a 5-point one-sided difference (exact to degree 4),
+    the tangential one 6th-order 1-D LABFM (exact on polynomials in x up to degree 6).  FD
+    rows 1 and 2: the same operators rotated to x-y.  Checked away from the periodic seam,
+    where x^p is not periodic."""
+    o = channel_oracle(order)
+    nd = o.nodes()
+    npfb = o.sizes()[1]
+    x, y, t = nd["x"][:npfb], nd["y"][:npfb], nd["node_type"][:npfb]
+    inner = (x > 0.3) & (x < 0.7)
+    wall, rows = (t == 0) & inner, ((t == -1) | (t == -2)) & inner
+    nsgn = np.where(y[wall] < 0.5, 1.0, -1.0)  # wall normal is +y at the bottom, -y at the top
+    tsgn = -nsgn  # tangent (-n_y, n_x): -x at the bottom, +x at the top
+    worst = 0.0
+    for p in range(1, 5):  # normal direction
+        g = o.gradient(y ** p)
+        d = p * y ** (p - 1)
+        worst = max(worst, np.abs(g[wall, 0] - nsgn * d[wall]).max(), np.abs(g[rows, 1] - d[rows]).max() / max(1, p))
+    for p in range(1, 7):  # tangential direction
+        g = o.gradient((x - 0.5) ** p)
+        d = p * (x - 0.5) ** (p - 1)
+        worst = max(worst, np.abs(g[wall, 1] - tsgn * d[wall]).max(), np.abs(g[rows, 0] - d[rows]).max())
+    print("order", order, "worst boundary residual", worst)
+    assert worst < 1e-7, worst
+
+
+@pytest.mark.parametrize("order,form,tol", [(6, "di", 1e-9), (8, "di", 1e-9), (8, "lc", 1e-9)])
+def test_poiseuille_is_a_fixed_point(order, form, tol):
+    """Steady Oldroyd-B channel flow driven by a body force (the reference checks Poiseuille
+    flow in statistics.F90:444-550): u = G y (1-y)/(2 mu), c_xy = lam u', c_xx = 1+2(lam u')^2
+    is polynomial, so interior LABFM, FD rows, 1-D LABFM and the wall closure
+    (rhs_di.F90:146-158,291-309,497-512; calc_rhs_nscbc, characteristic_boundaries.F90:27-52)
+    must all return a zero right-hand side to rounding.  (The log-conformation form evolves
+    psi = log c, which is not polynomial, so only its momentum right-hand side is checked.)"""
+    G = 8.0
+    o = channel_oracle(order, form, G=G)
+    nd = o.nodes()
+    npfb = o.sizes()[1]
+    st = poiseuille_state(type("P", (), {"y": nd["y"][:npfb], "n": npfb}), G, 1.0, 0.5)
+    o.set_state(**st)
+    r = o.rhs()
+    keys = ["ro", "rou", "rov"] + (["xx", "xy", "yy"] if form == "di" else [])
+    worst = max(np.abs(r[k]).max() for k in keys) / G
+    print(order, form, "max |rhs| / G", worst)
+    assert worst < tol, worst
