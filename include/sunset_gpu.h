@@ -82,6 +82,11 @@ int sunset_get_sizes(SunsetHandle *h, int *np, int *npfb, int *nb, int *nplink);
 int sunset_find_neighbours(SunsetHandle *h);
 /* labf.F90:34-231 calc_labf_weights (+ calc_filter_weights :233-394). */
 int sunset_calc_labf_weights(SunsetHandle *h);
+/* labf.F90:505-1039 calc_boundary_weights: prunes the links of boundary nodes to their own
+   layer and FD children, then FD normal and 1-D LABFM tangential operators for boundary
+   nodes and FD rows 1-2, curvature and frame rotations.  A no-op without boundary nodes;
+   required between sunset_calc_labf_weights and sunset_calc_labf_sums when there are. */
+int sunset_calc_boundary_weights(SunsetHandle *h);
 /* labf.F90:396-451 calc_labf_sums (+ node volumes, labf.F90:453-503). */
 int sunset_calc_labf_sums(SunsetHandle *h);
 /* labf.F90:1723-1811 filter_coefficients. */

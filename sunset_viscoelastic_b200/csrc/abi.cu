@@ -153,30 +153,41 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
     (void)gi;
     const double hovs = hovs_for(H->cfg.forder), hovs_bound = hovs_bound_for(H->cfg.forder);
     const double hos = H->cfg.h_over_s;
-    std::vector<double> vx, vy, vh, vs;
-    std::vector<int> vt;
+    std::vector<double> vx, vy, vh, vs, vnx, vny;
+    std::vector<int> vt, vfd, vb;
     int nb = 0;
     for (int r = 0; r < nrows; r++) {  // setup_domain.F90:177-199
         int t = node_type[r];
-        if (t >= 0 && t <= 2) nb++;
+        if (t == 1 || t == 2)
+            return set_err(H, SUNSET_ERR_SCOPE, "inflow/outflow boundary nodes are not on the device path (walls are)");
+        const double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
         vx.push_back(x[r]);
         vy.push_back(y[r]);
         vs.push_back(s[r]);
         vt.push_back(t);
         vh.push_back(s[r] * hovs);
+        vnx.push_back(rnx);
+        vny.push_back(rny);
+        vfd.push_back(-1);
         if (t >= 0 && t <= 2) {
+            nb++;
+            const int k = (int)vx.size() - 1;
+            vb.push_back(k);
             vh.back() = s[r] * hovs_bound;
-            double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
             for (int j = 1; j <= 4; j++) {
                 vx.push_back(x[r] + (rnx * (double)j) * s[r]);
                 vy.push_back(y[r] + (rny * (double)j) * s[r]);
                 vs.push_back(s[r]);
                 vt.push_back(-j);
                 vh.push_back(s[r] * hovs_bound);
+                vnx.push_back(rnx);
+                vny.push_back(rny);
+                vfd.push_back(k);
             }
         }
     }
-    if (nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "boundary nodes (walls/inflow/outflow) are not implemented on the device path");
+    if (nb > 0 && H->cfg.Mdiff != 0.0)
+        return set_err(H, SUNSET_ERR_SCOPE, "polymer diffusion (Mdiff) with walls is not on the device path");
     const int n = (int)vx.size();
     if (n >= (1 << 30)) return set_err(H, SUNSET_ERR_SCOPE, "too many nodes");
     if (hos > 0)
@@ -195,6 +206,8 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
     H->h3 = H->h2 * H->h0;
     H->hmax = *std::max_element(vh.begin(), vh.end());
     int rc = build_domain_device(H, vx, vy, vh, vhs, vs, vt);
+    if (rc) return rc;
+    rc = upload_boundary(H, vnx, vny, vfd, vb, vt);
     if (rc) return rc;
     H->domain_ok = true;
     return 0;
@@ -232,14 +245,29 @@ int sunset_calc_labf_weights(SunsetHandle *sh) {
     int rc = labf_weights_device(H);
     if (rc) return rc;
     H->w_ok = true;
+    H->bw_ok = H->nb == 0;
     H->sums_ok = H->fc_ok = false;
+    return 0;
+}
+
+int sunset_calc_boundary_weights(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (H->nb == 0) return 0;
+    if (int rc = need(H, H->w_ok && !H->bw_ok, "sunset_calc_labf_weights")) return rc;
+    if (int rc = set_device(H)) return rc;
+    int rc = boundary_prune_links(H);
+    if (rc) return rc;
+    rc = boundary_weights_device(H);
+    if (rc) return rc;
+    H->bw_ok = true;
     return 0;
 }
 
 int sunset_calc_labf_sums(SunsetHandle *sh) {
     if (!sh) return SUNSET_ERR_ARG;
     Handle *H = &sh->H;
-    if (int rc = need(H, H->w_ok && !H->sums_ok, "sunset_calc_labf_weights")) return rc;
+    if (int rc = need(H, H->w_ok && H->bw_ok && !H->sums_ok, H->w_ok ? "sunset_calc_boundary_weights" : "sunset_calc_labf_weights")) return rc;
     if (int rc = set_device(H)) return rc;
     int rc = labf_sums_device(H);
     if (rc) return rc;

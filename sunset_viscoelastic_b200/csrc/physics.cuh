@@ -128,8 +128,47 @@ __device__ __forceinline__ void rhs_flow(const StepConsts &K, const NodeState &n
     r.rov = ((-tsv - K.csq * g.ro_y) + bfv) + fvv;
 }
 
-// calc_rhs_c, interior branch, rhs_di.F90:415-476 (sPTT / Oldroyd-B, 2-D).
-__device__ __forceinline__ void rhs_c_di(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
+// Walls (node_type 0).  Wall nodes' first-derivative weights are in the wall's
+// normal-tangent frame, so there g.*_x is the normal and g.*_y the tangential derivative.
+// wall_velocity_gradient: the rotated velocity gradient the conformation equations use on
+// walls (rhs_di.F90:497-512, rhs.F90 and rhs_lc.F90 alike).
+__device__ __forceinline__ Grads wall_velocity_gradient(const Grads &g, double xn, double yn) {
+    Grads w = g;
+    w.u_x = xn * g.u_x - yn * g.u_y;
+    w.v_x = xn * g.v_x - yn * g.v_y;
+    w.u_y = yn * g.u_x + xn * g.u_y;
+    w.v_y = yn * g.v_x + xn * g.v_y;
+    return w;
+}
+
+// Mass and momentum on a wall: calc_rhs_ro wall branch (rhs_di.F90:146-158), the
+// characteristic amplitudes of calc_rhs_rovel (:291-309; the momentum right-hand side is
+// zero), specify_characteristics_isothermal_wall (characteristic_boundaries.F90:27-52,
+// acoustic reflection L5 = L1) and calc_rhs_nscbc (rhs_di.F90:601-665).
+__device__ __forceinline__ void rhs_flow_wall(const StepConsts &K, const NodeState &n, const Grads &g, double xn,
+                                              double yn, Rhs &r) {
+    const double c = K.c_sound;
+    const double dutdt = -yn * g.u_y + xn * g.v_y;
+    r.ro = -n.ro * dutdt - n.ro * 0.0;
+    const double dpdn = K.csq * g.ro_x;
+    const double un = n.u * xn + n.v * yn;
+    const double dundn = xn * g.u_x + yn * g.v_x;
+    const double dutdn = -yn * g.u_x + xn * g.v_x;
+    const double L1 = (0.5 * (un - c)) * (dpdn - (n.ro * c) * dundn);
+    const double L2 = un * (g.ro_x - (dpdn / c) / c);
+    const double L3 = un * dutdn;
+    const double L5 = L1;
+    const double tmp_scal = ((((c * c) * L2 + L5) + L1) / c) / c;
+    r.ro = r.ro - tmp_scal;
+    r.rou = (0.0 - n.u * tmp_scal) - (L5 - L1) / c;
+    r.rov = (0.0 - n.v * tmp_scal) - n.ro * L3;
+}
+
+// calc_rhs_c, interior branch, rhs_di.F90:415-476 (sPTT / Oldroyd-B, 2-D); on walls
+// (rhs_di.F90:490-580) without advection, with the rotated velocity gradient, and rhs_zz
+// left at zero.
+__device__ __forceinline__ void rhs_c_di(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r,
+                                         bool wall = false) {
     const double w = 0.0;
     const double cxx = n.cxx, cxy = n.cxy, cyy = n.cyy, czz = n.czz;
     double adxx = -((n.u * g.cxx_x + n.v * g.cxx_y) + w * 0.0);
@@ -143,6 +182,13 @@ __device__ __forceinline__ void rhs_c_di(const StepConsts &K, const NodeState &n
     double uczz = ((2.0 * 0.0) * 0.0 + (2.0 * 0.0) * 0.0) + (2.0 * 0.0) * czz;
     double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
     double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0), szz = fr * (czz - 1.0);
+    if (wall) {
+        r.xx = (ucxx + sxx) + K.Mdiff * g.lapcxx;
+        r.xy = (ucxy + sxy) + K.Mdiff * g.lapcxy;
+        r.yy = (ucyy + syy) + K.Mdiff * g.lapcyy;
+        r.zz = 0.0;
+        return;
+    }
     r.xx = ((adxx + ucxx) + sxx) + K.Mdiff * g.lapcxx;
     r.xy = ((adxy + ucxy) + sxy) + K.Mdiff * g.lapcxy;
     r.yy = ((adyy + ucyy) + syy) + K.Mdiff * g.lapcyy;
@@ -176,9 +222,10 @@ __device__ __forceinline__ void rhs_c_chl(const StepConsts &K, const NodeState &
 }
 
 // calc_rhs_logconf, interior branch, rhs_lc.F90:414-559 (sPTT, 2-D).  `first` is the
-// reference's itime==1 .and. iRKstep==1 special case (rhs_lc.F90:503).
+// reference's itime==1 .and. iRKstep==1 special case (rhs_lc.F90:503).  On walls (with the
+// rotated velocity gradient) there is no advection term.
 __device__ __forceinline__ void rhs_c_lc(const StepConsts &K, const NodeState &n, const Grads &g, bool first,
-                                         Rhs &r) {
+                                         Rhs &r, bool wall = false) {
     const double w = 0.0;
     double adxx = -((n.u * g.pxx_x + n.v * g.pxx_y) + w * 0.0);
     double adxy = -((n.u * g.pxy_x + n.v * g.pxy_y) + w * 0.0);
@@ -216,6 +263,13 @@ __device__ __forceinline__ void rhs_c_lc(const StepConsts &K, const NodeState &n
     Ci[0] = fR / Lv[0] - fR; Ci[1] = 0.0; Ci[2] = 0.0; Ci[3] = fR / Lv[1] - fR;
     mm2(Ci, RT, T);
     mm2(R, T, T);
+    if (wall) {
+        r.xx = UC[0] + T[0] / K.lambda;
+        r.xy = UC[2] + T[2] / K.lambda;
+        r.yy = UC[3] + T[3] / K.lambda;
+        r.zz = 0.0;
+        return;
+    }
     r.xx = (adxx + UC[0]) + T[0] / K.lambda;
     r.xy = (adxy + UC[2]) + T[2] / K.lambda;
     r.yy = (adyy + UC[3]) + T[3] / K.lambda;

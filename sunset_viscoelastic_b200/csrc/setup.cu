@@ -194,36 +194,93 @@ __global__ void k_search(SearchArgs a, int *count, const long long *rowptr, int 
 // Reference numbering of a point, used to order links at equal distance deterministically.
 __device__ __forceinline__ int ref_point(int p, int npfb, const int *perm) { return p < npfb ? perm[p] : p; }
 
-// order_neighbours (neighbours.F90:272-314): sort each row by squared distance; links at
-// exactly equal distance are ordered by reference point number.  ij_count_small counts the
-// links inside ss*h_small.
+// The reference's search grid (cell_generator, neighbours.F90:75-93): square cells of side
+// ss*h0 over the domain tripled in each direction.
+struct RefGrid {
+    double xmint, ymint, unoss;
+};
+
+// Position of the cell (dx, dy) relative to a node's own cell in the reference's scan of the
+// neighbouring cells (neighbour_cells, neighbours.F90:95-158): self, E, NE, SE, W, NW, SW, N, S.
+__device__ __forceinline__ int scan_position(int dx, int dy) {
+    if (dx == 0 && dy == 0) return 0;
+    if (dx == 1) return dy == 0 ? 1 : dy == 1 ? 2 : 3;
+    if (dx == -1) return dy == 0 ? 4 : dy == 1 ? 5 : 6;
+    return dy == 1 ? 7 : 8;
+}
+
+constexpr int kMaxRowSort = 1024;  // longest row the reference-order sort accepts
+
+// order_neighbours (neighbours.F90:272-341), reproducing where links at exactly equal
+// distance end up (straight walls, FD rows and their periodic images give such ties): the
+// row is first put in the order in which the reference's cell scan finds the links (scan
+// position of the link's cell, then point number within a cell, as divide() fills the
+// cells), then sorted by squared distance with the reference's quicksort
+// (quicksort_neighbours), run with an explicit stack.  ij_count_small counts the links
+// inside ss*h_small.
 __global__ void k_sort_rows(int npfb, const long long *rowptr, int *opt, double *or2, const double *hs,
-                            const int *perm, int *cnt_small) {
+                            const int *perm, const double *px, const double *py, RefGrid rg, int *cnt_small,
+                            int *err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
     long long b = rowptr[i], e = rowptr[i + 1];
-    for (long long a = b + 1; a < e; a++) {
+    const int n = (int)(e - b);
+    if (n > kMaxRowSort) {
+        atomicExch(err, i + 1);
+        return;
+    }
+    const int ci = (int)((px[i] - rg.xmint) * rg.unoss), cj = (int)((py[i] - rg.ymint) * rg.unoss);
+    auto scan_key = [&](int p) -> long long {
+        int dx = (int)((px[p] - rg.xmint) * rg.unoss) - ci, dy = (int)((py[p] - rg.ymint) * rg.unoss) - cj;
+        // links beyond the reference's 3x3 cells (only when a node's h exceeds the grid's)
+        // go last, by point number
+        int pos = (dx < -1 || dx > 1 || dy < -1 || dy > 1) ? 9 : scan_position(dx, dy);
+        return ((long long)pos << 32) | (unsigned)ref_point(p, npfb, perm);
+    };
+    for (long long a = b + 1; a < e; a++) {  // insertion sort into scan order
         double key = or2[a];
-        int p = opt[a], rp = ref_point(p, npfb, perm);
+        int p = opt[a];
+        long long kp = scan_key(p);
         long long c = a - 1;
-        while (c >= b) {
-            double kc = or2[c];
-            int rc = ref_point(opt[c], npfb, perm);
-            if (kc > key || (kc == key && rc > rp)) {
-                or2[c + 1] = kc;
-                opt[c + 1] = opt[c];
-                c--;
-            } else {
-                break;
-            }
+        while (c >= b && scan_key(opt[c]) > kp) {
+            or2[c + 1] = or2[c];
+            opt[c + 1] = opt[c];
+            c--;
         }
         or2[c + 1] = key;
         opt[c + 1] = p;
     }
+    // quicksort_neighbours on the 1-based range [1, n] of this row
+    double *a = or2 + b - 1;
+    int *lk = opt + b - 1;
+    int stk[2 * 64];
+    int top = 0;
+    if (n >= 1) { stk[0] = 1; stk[1] = n; top = 1; }
+    while (top > 0) {
+        top--;
+        const int first = stk[2 * top], last = stk[2 * top + 1];
+        const double x = a[(first + last) / 2];
+        int ii = first, jj = last;
+        for (;;) {
+            while (a[ii] < x) ii++;
+            while (x < a[jj]) jj--;
+            if (ii >= jj) break;
+            double t = a[ii]; a[ii] = a[jj]; a[jj] = t;
+            int it = lk[ii]; lk[ii] = lk[jj]; lk[jj] = it;
+            ii++;
+            jj--;
+        }
+        if (top + 2 > 64) {  // deeper than any row of kMaxRowSort links needs in practice
+            atomicExch(err, i + 1);
+            return;
+        }
+        if (first < ii - 1) { stk[2 * top] = first; stk[2 * top + 1] = ii - 1; top++; }
+        if (jj + 1 < last) { stk[2 * top] = jj + 1; stk[2 * top + 1] = last; top++; }
+    }
     double t = hs[i] * kSs, hs2 = t * t;
     int small = 0;
-    for (long long a = b; a < e; a++)
-        if (or2[a] <= hs2) small++;
+    for (long long q = b; q < e; q++)
+        if (or2[q] <= hs2) small++;
     cnt_small[i] = small;
 }
 
@@ -396,7 +453,17 @@ int find_neighbours_device(Handle *H) {
     if (dalloc(H, &opt, nl) || dalloc(H, &or2, nl)) return SUNSET_ERR_NOMEM;
     k_search<true><<<(n + TB - 1) / TB, TB, 0, st>>>(sa, nullptr, rowptr, opt, or2);
     if (!H->cnt_small && dalloc(H, &H->cnt_small, n)) return SUNSET_ERR_NOMEM;
-    k_sort_rows<<<(n + TB - 1) / TB, TB, 0, st>>>(n, rowptr, opt, or2, H->hs, H->perm, H->cnt_small);
+    int *serr;
+    if (dalloc(H, &serr, 1)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(serr, 0, sizeof(int), st));
+    RefGrid rg{H->xmin - (H->xmax - H->xmin), H->ymin - (H->ymax - H->ymin), 1.0 / (1.0 * (kSs * H->h0))};
+    k_sort_rows<<<(n + TB - 1) / TB, TB, 0, st>>>(n, rowptr, opt, or2, H->hs, H->perm, H->px, H->py, rg,
+                                                  H->cnt_small, serr);
+    int hserr = 0;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&hserr, serr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    dfree(H, serr);
+    if (hserr) return set_err(H, SUNSET_ERR_SCOPE, "neighbour row of node %d too long to sort", hserr - 1);
     std::vector<int> hsmall(n);
     SUNSET_CUDA(H, cudaMemcpyAsync(hsmall.data(), H->cnt_small, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
@@ -458,6 +525,47 @@ int find_neighbours_device(Handle *H) {
 #include <thread>
 
 namespace sunset {
+
+// Boundary framework data in internal order: normals, FD parents, the boundary list in
+// the reference's order (setup_domain.F90:314-327 builds it in node order) with each
+// boundary node's four FD rows (the reader places them right after their parent), and the
+// boundary index of each node.  Inputs are in the reference's node order.
+int upload_boundary(Handle *H, const std::vector<double> &nx, const std::vector<double> &ny,
+                    const std::vector<int> &fdpar_ref, const std::vector<int> &blist_ref,
+                    const std::vector<int> &type) {
+    const int n = H->npfb, nb = (int)blist_ref.size();
+    const std::vector<int> &perm = H->h_perm, &iperm = H->h_iperm;
+    std::vector<double> inx(n), iny(n);
+    std::vector<int> ifd(n), ibidx(n, -1), ibl(nb), ibrow(4 * (size_t)(nb ? nb : 1), 0);
+    for (int i = 0; i < n; i++) {
+        const int r = perm[i];
+        inx[i] = nx[r];
+        iny[i] = ny[r];
+        ifd[i] = fdpar_ref[r] >= 0 ? iperm[fdpar_ref[r]] : -1;
+    }
+    H->h_btype.resize(nb);
+    for (int jj = 0; jj < nb; jj++) {
+        const int r = blist_ref[jj];
+        ibl[jj] = iperm[r];
+        ibidx[iperm[r]] = jj;
+        H->h_btype[jj] = type[r];
+        for (int j = 1; j <= 4; j++) ibrow[4 * jj + j - 1] = iperm[r + j];
+    }
+    if (dalloc(H, &H->rnx, n) || dalloc(H, &H->rny, n) || dalloc(H, &H->fdpar, n) || dalloc(H, &H->bidx, n) ||
+        dalloc(H, &H->blist, nb ? nb : 1) || dalloc(H, &H->brow, 4 * (size_t)(nb ? nb : 1)))
+        return SUNSET_ERR_NOMEM;
+    cudaStream_t st = H->stream;
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->rnx, inx.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->rny, iny.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->fdpar, ifd.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->bidx, ibidx.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (nb) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->blist, ibl.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st));
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->brow, ibrow.data(), 4 * (size_t)nb * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    return 0;
+}
 
 int build_halos(Handle *H) {
     const int n = H->npfb, nsl = H->nslices;

@@ -38,6 +38,8 @@ struct StageArgs {
     const double *wx, *wy, *wl, *wh;
     const float *wx32, *wy32, *wl32, *wh32;  // mixed precision
     const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
+    const int *ntype;            // node types (walls: 0)
+    const double *rnx, *rny;     // wall normals into the fluid
     Fields in, out;
     double *reg[7], *eacc[7], *rhs[7];
     float *dreg[7], *eacc32[7];  // mixed precision
@@ -384,12 +386,23 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         n.cxx = F.c[0][i]; n.cxy = F.c[1][i]; n.cyy = F.c[2][i]; n.czz = F.c[3][i];
         n.pxx = F.q[0][i]; n.pxy = F.q[1][i]; n.pyy = F.q[2][i]; n.pzz = F.q[3][i];
         Rhs r;
-        rhs_flow(cK, n, g, r);
-        if (FORM == SUNSET_FORM_DI) rhs_c_di(cK, n, g, r);
+        const bool wall = cK.has_walls && A.ntype[i] == 0;
+        if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
+            const double xn = A.rnx[i], yn = A.rny[i];
+            rhs_flow_wall(cK, n, g, xn, yn, r);
+            const double gux = g.u_x, guy = g.u_y, gvx = g.v_x, gvy = g.v_y;
+            g.u_x = xn * gux - yn * guy;
+            g.v_x = xn * gvx - yn * gvy;
+            g.u_y = yn * gux + xn * guy;
+            g.v_y = yn * gvx + xn * gvy;
+        } else {
+            rhs_flow(cK, n, g, r);
+        }
+        if (FORM == SUNSET_FORM_DI) rhs_c_di(cK, n, g, r, wall);
         else if (FORM == SUNSET_FORM_CHL) rhs_c_chl(cK, n, g, r);
         else if (FORM == SUNSET_FORM_LC) {
             const bool first = (A.sc->itime == 1) && (stage == 0);
-            rhs_c_lc(cK, n, g, first, r);
+            rhs_c_lc(cK, n, g, first, r, wall);
         } else { r.xx = r.xy = r.yy = r.zz = 0.0; }
         const double rr[7] = {r.ro, r.rou, r.rov, r.xx, r.xy, r.yy, r.zz};
         constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
@@ -443,6 +456,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                 }
                 emax_bits = dbits(en);
             }
+            if (wall) { Un[1] = 0.0; Un[2] = 0.0; }  // apply_time_dependent_bounds, characteristic_boundaries.F90:200-206
             const Fields &O = A.out;
             O.ro[i] = Un[0]; O.rou[i] = Un[1]; O.rov[i] = Un[2];
             if (FORM != SUNSET_FORM_NEWT) {
@@ -520,11 +534,13 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
             const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
             double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
             double rof = 0.0;
+            const bool wall = cK.has_walls && A.ntype[i] == 0;
 #pragma unroll
             for (int f = 0; f < 7; f++) {
                 if (f < nf) {
                     const double p = src[f][i];
-                    const double r = p + (t[f] - p * hs);
+                    double r = p + (t[f] - p * hs);
+                    if (wall && (f == 1 || f == 2)) r = 0.0;  // apply_time_dependent_bounds after the filter
                     dst[f][i] = r;
                     if (f == 0) rof = r;
                 } else if (FORM != SUNSET_FORM_NEWT) {
@@ -690,16 +706,20 @@ __global__ void k_op_filter(StageArgs A, const double *phi, double *out, int ter
 }
 
 // initial_solution (setup_flow.F90:24-173) on internal-order device arrays.
+// Wall nodes get zero velocity (setup_flow.F90:266-280).
 __global__ void k_set_state(int npfb, int form, const double *ro, const double *u, const double *v,
-                            const double *cxx, const double *cxy, const double *cyy, const double *czz, Fields F) {
+                            const double *cxx, const double *cxy, const double *cyy, const double *czz,
+                            const int *ntype, int has_walls, Fields F) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
     double r = ro[i];
+    double ui = u[i], vi = v[i];
+    if (has_walls && ntype[i] == 0) { ui = 0.0; vi = 0.0; }
     F.ro[i] = r;
-    F.u[i] = u[i];
-    F.v[i] = v[i];
-    F.rou[i] = r * u[i];
-    F.rov[i] = r * v[i];
+    F.u[i] = ui;
+    F.v[i] = vi;
+    F.rou[i] = r * ui;
+    F.rov[i] = r * vi;
     double c0 = cxx[i], c1 = cxy[i], c2 = cyy[i], c3 = czz[i];
     if (form == SUNSET_FORM_LC) {
         double p0, p1, p2;
@@ -816,6 +836,9 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     }
     A.vol = H->vol;
     A.py_node = H->py;
+    A.ntype = H->ntype;
+    A.rnx = H->rnx;
+    A.rny = H->rny;
     A.in = H->buf[from];
     A.out = H->buf[from ^ 1];
     for (int f = 0; f < 7; f++) {
@@ -839,6 +862,7 @@ int upload_consts(Handle *H) {
     K.kolmo = c.kolmogorov_forcing < 0 ? (c.form == SUNSET_FORM_CHL) : c.kolmogorov_forcing;
     K.di_full = c.di_full_gradients;
     K.has_mirrors = H->has_mirrors;
+    K.has_walls = H->nb > 0;
     K.mdiff_on = c.Mdiff != 0.0;
     double t = c.U_char / c.Ma;
     K.csq = t * t;
@@ -1023,7 +1047,7 @@ int state_set_device(Handle *H, const double *ro, const double *u, const double 
     if (rc) return rc;
     H->cur = 0;
     k_set_state<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, ro, u, v, cxx, cxy, cyy, czz,
-                                                              H->buf[0]);
+                                                              H->ntype, H->nb > 0, H->buf[0]);
     SUNSET_CUDA(H, cudaGetLastError());
     rc = init_scalars(H);
     if (rc) return rc;

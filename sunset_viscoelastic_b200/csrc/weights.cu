@@ -531,7 +531,7 @@ struct SumArgs {
     int npfb;
     double L;
     const double *px, *py, *h, *sp;
-    const int *ntype, *cnt, *lpt;
+    const int *ntype, *cnt, *lpt, *fdpar;
     const long long *slice_ptr;
     double *wx, *wy, *wl, *wh, *gsx, *gsy, *lsum, *hsum, *vol;
 };
@@ -577,8 +577,7 @@ __global__ void k_labf_sums(SumArgs a) {
     }
 }
 
-// filter_coefficients, labf.F90:1723-1811 (walls' FD-row reductions need fd_parent and
-// are applied only for interior nodes here: the boundary framework is outside this path).
+// filter_coefficients, labf.F90:1723-1811, with the reduction of the FD rows of walls.
 __global__ void k_filter_coeff(SumArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.npfb) return;
@@ -600,6 +599,13 @@ __global__ void k_filter_coeff(SumArgs a) {
             lsum = lsum + fji * a.wh[o];
         }
         fc = (2.0 / 3.0) / lsum;
+        if (t < 0 && a.ntype[a.fdpar[i]] == 0) {
+            const double oosqrt2 = 1.0 / sqrt(2.0);
+            if (t == -1) fc = (fc * 0.5) * oosqrt2;
+            if (t == -2) fc = fc * 0.5;
+            if (t == -3) fc = fc * oosqrt2;
+            if (t == -4) fc = fc * oosqrt2;
+        }
     } else {
         double tmp = ((2.0 / 3.0) * kPi) / a.sp[i];
         double lsum = 0.0;
@@ -621,6 +627,327 @@ __global__ void k_filter_coeff(SumArgs a) {
         sum = sum + w;
     }
     a.hsum[i] = sum;
+}
+
+// ---------------------------------------------------------------------------------------
+// calc_boundary_weights (labf.F90:505-1039): boundary node i0 and its FD rows i1..i4.
+// Normal first and second derivatives of i0, i1, i2 are the reference's 5-point finite
+// differences; tangential ones come from 6th-order 1-D LABFM on the node's own layer (a
+// 6 x 6 moment matrix, factored by the warp SVD above, so bit for bit the restatement's);
+// then the wall curvature, the divergence term of rows 1-2 and the rotation of rows 1-2 to
+// the x-y frame.  Wall first derivatives stay in the normal-tangent frame: the wall
+// equations are written there.
+// ---------------------------------------------------------------------------------------
+struct BndArgs {
+    int npfb, nb, nplink;
+    double h3;
+    const double *px, *py, *h, *sp, *rnx, *rny;
+    const int *ntype, *gpar, *fdpar, *blist, *brow;
+    int *cnt, *cnt_small, *lpt, *lidx;
+    uint16_t *lloc;
+    const long long *slice_ptr;
+    const int *slice_w;
+    double *wx, *wy, *wl, *wh;
+    double *wb2;  // nb x nplink x 2: second derivatives (normal, tangential) of boundary nodes
+    int *err;
+};
+
+// point p (interior or ghost) -> the interior node whose data it carries
+__device__ __forceinline__ int bnd_owner(const BndArgs &a, int p) { return p < a.npfb ? p : a.gpar[p - a.npfb]; }
+
+// rbfs.F90:58-68 (the kernel derivative `fac` of the 1-D operators; it uses the global h3)
+__device__ __forceinline__ double fac(double qq, double h3) {
+    double qq2 = qq * qq, qq3 = qq * qq2, qq4 = qq * qq3;
+    double f = 0.0;
+    if (qq <= 2.0 && qq > 0.0)
+        f = (7.0 / ((4.0 * kPi) * h3)) * ((((0.625 * qq4) - (3.75 * qq3)) + (7.5 * qq2)) - (5.0 * qq));
+    return f;
+}
+
+// labf.F90:1041-1048
+__device__ __forceinline__ double monomial1d(int m, double z) {
+    double z2 = z * z;
+    switch (m) {
+    case 0: return z;
+    case 1: return 0.5 * z2;
+    case 2: return ((1.0 / 6.0) * z) * z2;
+    case 3: return (z2 * z2) / 24.0;
+    case 4: return ((z2 * z2) * z) / 120.0;
+    default: return ((z2 * z2) * z2) / 720.0;
+    }
+}
+
+// labf.F90:1050-1077 (ABF==2)
+__device__ __forceinline__ double abf1d(int m, double z, double ff1) {
+    if (m == 2) return (ff1 * (1.0 / sqrt(2.0))) * hermite(3, z);
+    return ff1 * hermite(m + 1, z);
+}
+
+// tangential coordinate (scaled by hh) of point p relative to node i, and its kernel value
+__device__ __forceinline__ void tangential(const BndArgs &a, int i, int p, double xt, double yt, double hh,
+                                           double &z, double &ff1) {
+    double rijx = a.px[i] - a.px[p], rijy = a.py[i] - a.py[p];
+    double x = -(rijx * xt + rijy * yt);
+    if (i == p) x = 0.0;
+    ff1 = fac(fabs(x / hh), a.h3);
+    z = x / hh;
+}
+
+__device__ __forceinline__ double dot6(const double *b, const double *g) {
+    double t = 0.0;
+    for (int k = 0; k < 6; k++) t = t + b[k] * g[k];
+    return t;
+}
+
+constexpr int kBndWarpDoubles = 2 * 6 * 7 + 3 * 8 + 3 * 6;  // U, V, W/rv1/tmp, three right-hand sides
+
+// 1-D moment matrix of node i along (xt, yt) over its links on its own layer, then its
+// factorisation; lanes 0..35 each own one matrix entry and sum it over the links in order.
+__device__ int bnd_factor_1d(const BndArgs &a, int i, double xt, double yt, double hh, double *U, double *V,
+                             double *W, double *rv1, int lane) {
+    const long long base = a.slice_ptr[i >> 5];
+    const int ti = a.ntype[i], cnt = a.cnt[i];
+    for (int e = lane; e < 36; e += 32) {
+        const int i1 = e % 6, i2 = e / 6;
+        double acc = 0.0;
+        for (int k = 0; k < cnt; k++) {
+            const int p = a.lpt[sell_at(base, k, i & 31)];
+            if (a.ntype[bnd_owner(a, p)] != ti) continue;
+            double rijx = a.px[i] - a.px[p], rijy = a.py[i] - a.py[p];
+            double x = -(rijx * xt + rijy * yt);
+            if (i == p) x = 0.0;
+            const double xv = monomial1d(i1, x / hh);
+            double z, ff1;
+            tangential(a, i, p, xt, yt, hh, z, ff1);
+            acc = acc + xv * abf1d(i2, z, ff1);
+        }
+        U[i2 * 7 + i1] = acc;
+    }
+    __syncwarp();
+    return svd_factor_warp<6>(U, V, W, rv1, 7, lane);
+}
+
+// Drop every link of boundary node jj that is neither on its own layer nor one of its FD
+// children (labf.F90:541-565), compacting the SELL slots in order; the freed slots become
+// padding.
+__global__ void k_prune_boundary_links(BndArgs a) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= a.nb) return;
+    const int i = a.blist[jj], kk = a.ntype[i], c = a.cnt[i];
+    const long long base = a.slice_ptr[i >> 5];
+    const int ln = i & 31;
+    int w = 0;
+    for (int k = 0; k < c; k++) {
+        const long long o = sell_at(base, k, ln);
+        const int p = a.lpt[o];
+        const bool keep = (a.ntype[bnd_owner(a, p)] == kk) || (p < a.npfb && a.fdpar[p] == i);
+        if (!keep) continue;
+        const long long o2 = sell_at(base, w, ln);
+        a.lpt[o2] = p;
+        a.lidx[o2] = a.lidx[o];
+        a.lloc[o2] = a.lloc[o];
+        w++;
+    }
+    for (int k = w; k < c; k++) {
+        const long long o = sell_at(base, k, ln);
+        a.lpt[o] = 0;
+        a.lidx[o] = 0;
+        a.lloc[o] = 0;
+    }
+    a.cnt[i] = w;
+    a.cnt_small[i] = w;
+}
+
+// Boundary nodes: normal FD operators (labf.F90:572-612) and tangential 1-D LABFM
+// (:688-755).  One warp per boundary node.
+__global__ void k_boundary_node_weights(BndArgs a) {
+    __shared__ double sm[4][kBndWarpDoubles];
+    const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
+    const int jj = blockIdx.x * 4 + wrp;
+    if (jj >= a.nb) return;
+    double *U = sm[wrp], *V = U + 42, *W = V + 42, *rv1 = W + 8, *tmp = rv1 + 8, *bt = tmp + 8, *btt = bt + 6,
+           *bh = btt + 6;
+    const int i = a.blist[jj];
+    const long long base = a.slice_ptr[i >> 5];
+    const int ln = i & 31, cnt = a.cnt[i];
+    const double dx = a.sp[i], dx2 = dx * dx;
+    double *wb = a.wb2 + (size_t)jj * a.nplink * 2;
+    for (int k = lane; k < a.slice_w[i >> 5]; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        a.wx[o] = 0.0; a.wy[o] = 0.0; a.wl[o] = 0.0; a.wh[o] = 0.0;
+    }
+    for (int k = lane; k < a.nplink; k += 32) { wb[2 * k] = 0.0; wb[2 * k + 1] = 0.0; }
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        const int p = a.lpt[o];
+        if (p >= a.npfb || a.fdpar[p] != i) continue;
+        const int t = a.ntype[p];
+        if (t == -1) { a.wx[o] = 4.0 / dx; wb[2 * k] = -((104.0 / 12.0) / dx2); }
+        if (t == -2) { a.wx[o] = -(3.0 / dx); wb[2 * k] = (114.0 / 12.0) / dx2; }
+        if (t == -3) { a.wx[o] = (4.0 / 3.0) / dx; wb[2 * k] = -((56.0 / 12.0) / dx2); }
+        if (t == -4) { a.wx[o] = -(0.25 / dx); wb[2 * k] = (11.0 / 12.0) / dx2; }
+    }
+    const double xt = -a.rny[i], yt = a.rnx[i], hh = a.h[i];
+    __syncwarp();
+    if (bnd_factor_1d(a, i, xt, yt, hh, U, V, W, rv1, lane)) {
+        if (lane == 0) atomicExch(a.err, i + 1);
+        return;
+    }
+    for (int m = lane; m < 6; m += 32) {
+        bt[m] = (m == 0) ? 1.0 : 0.0;
+        btt[m] = (m == 1) ? 1.0 : 0.0;
+        bh[m] = (m == 3) ? -1.0 : 0.0;
+    }
+    svd_apply_warp<6>(U, V, W, tmp, bt, 7, lane);
+    svd_apply_warp<6>(U, V, W, tmp, btt, 7, lane);
+    svd_apply_warp<6>(U, V, W, tmp, bh, 7, lane);
+    const int ti = a.ntype[i];
+    for (int k = lane; k < cnt; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        const int p = a.lpt[o];
+        if (a.ntype[bnd_owner(a, p)] != ti) continue;
+        double z, ff1, g[6];
+        tangential(a, i, p, xt, yt, hh, z, ff1);
+        for (int m = 0; m < 6; m++) g[m] = abf1d(m, z, ff1);
+        a.wy[o] = dot6(bt, g) / hh;
+        wb[2 * k + 1] = (dot6(btt, g) / hh) / hh;
+        a.wh[o] = a.wh[o] + dot6(bh, g);
+    }
+}
+
+// FD rows 1 and 2: normal FD operators (labf.F90:615-676) and tangential 1-D LABFM on a
+// tangent rotated by the tangential gradient of the resolution (:758-955).  One warp per
+// (boundary node, row).
+__global__ void k_boundary_row_weights(BndArgs a) {
+    __shared__ double sm[4][kBndWarpDoubles];
+    const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
+    const int w = blockIdx.x * 4 + wrp;
+    if (w >= 2 * a.nb) return;
+    const int jj = w >> 1, row = 1 + (w & 1);
+    double *U = sm[wrp], *V = U + 42, *W = V + 42, *rv1 = W + 8, *tmp = rv1 + 8, *bt = tmp + 8, *btt = bt + 6;
+    const int i = a.brow[4 * jj + row - 1], par = a.blist[jj];
+    const long long base = a.slice_ptr[i >> 5];
+    const int ln = i & 31, cnt = a.cnt[i];
+    const double dx = a.sp[i], dx2 = dx * dx;
+    for (int k = lane; k < a.slice_w[i >> 5]; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        a.wx[o] = 0.0; a.wy[o] = 0.0; a.wl[o] = 0.0;
+    }
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        const int p = a.lpt[o];
+        if (p >= a.npfb) continue;
+        const int t = a.ntype[p];
+        const bool same = a.fdpar[p] == par;
+        if (row == 1) {
+            if (p == par) { a.wx[o] = -(0.25 / dx); a.wl[o] = (11.0 / 12.0) / dx2; }
+            if (t == -2 && same) { a.wx[o] = 1.5 / dx; a.wl[o] = (6.0 / 12.0) / dx2; }
+            if (t == -3 && same) { a.wx[o] = -(0.5 / dx); a.wl[o] = (4.0 / 12.0) / dx2; }
+            if (t == -4 && same) { a.wx[o] = (1.0 / 12.0) / dx; a.wl[o] = -((1.0 / 12.0) / dx2); }
+        } else {
+            if (p == par) { a.wx[o] = (1.0 / 12.0) / dx; a.wl[o] = -((1.0 / 12.0) / dx2); }
+            if (t == -1 && same) { a.wx[o] = -((8.0 / 12.0) / dx); a.wl[o] = (16.0 / 12.0) / dx2; }
+            if (t == -3 && same) { a.wx[o] = (8.0 / 12.0) / dx; a.wl[o] = (16.0 / 12.0) / dx2; }
+            if (t == -4 && same) { a.wx[o] = -((1.0 / 12.0) / dx); a.wl[o] = -((1.0 / 12.0) / dx2); }
+        }
+    }
+    // tangential gradient of the resolution at the boundary node, in the order of its links
+    double grads = 0.0;
+    {
+        const long long pb = a.slice_ptr[par >> 5];
+        for (int k = 0; k < a.cnt[par]; k++) {
+            const long long o = sell_at(pb, k, par & 31);
+            const int p = a.lpt[o];
+            grads = grads + (a.sp[bnd_owner(a, p)] - a.sp[par]) * a.wy[o];
+        }
+    }
+    grads = -atan(grads);
+    const double xt = cos(grads) * (-a.rny[i]) - sin(grads) * a.rnx[i];
+    const double yt = sin(grads) * (-a.rny[i]) + cos(grads) * a.rnx[i];
+    const double hh = a.h[i];
+    __syncwarp();
+    if (bnd_factor_1d(a, i, xt, yt, hh, U, V, W, rv1, lane)) {
+        if (lane == 0) atomicExch(a.err, i + 1);
+        return;
+    }
+    for (int m = lane; m < 6; m += 32) {
+        bt[m] = (m == 0) ? 1.0 : 0.0;
+        btt[m] = (m == 1) ? 1.0 : 0.0;
+    }
+    svd_apply_warp<6>(U, V, W, tmp, bt, 7, lane);
+    svd_apply_warp<6>(U, V, W, tmp, btt, 7, lane);
+    const int ti = a.ntype[i];
+    const double sec = 1.0 / cos(grads), tn = tan(grads);
+    for (int k = lane; k < cnt; k += 32) {
+        const long long o = sell_at(base, k, ln);
+        const int p = a.lpt[o];
+        if (a.ntype[bnd_owner(a, p)] == ti) {
+            double z, ff1, g[6];
+            tangential(a, i, p, xt, yt, hh, z, ff1);
+            for (int m = 0; m < 6; m++) g[m] = abf1d(m, z, ff1);
+            a.wy[o] = dot6(bt, g) / hh;
+            a.wl[o] = a.wl[o] + (dot6(btt, g) / hh) / hh;
+        }
+        a.wy[o] = sec * a.wy[o] - tn * a.wx[o];
+    }
+}
+
+// Wall curvature, outflow sign, divergence term of rows 1-2, wall Laplacian, rows 1-2 to
+// the x-y frame (labf.F90:965-1035).  One thread per boundary node.
+__global__ void k_boundary_frame(BndArgs a) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= a.nb) return;
+    const int i = a.blist[jj], ti = a.ntype[i];
+    const long long base = a.slice_ptr[i >> 5];
+    const int ln = i & 31;
+    double *wb = a.wb2 + (size_t)jj * a.nplink * 2;
+    double ooR = 0.0;
+    if (ti == 0) {
+        double tmp_t = 0.0;
+        for (int k = 0; k < a.cnt[i]; k++) {
+            const int p = a.lpt[sell_at(base, k, ln)];
+            const int q = bnd_owner(a, p);
+            if (a.ntype[q] != ti) continue;
+            const double tmp_n = ((a.rnx[q] * a.rnx[i] + a.rny[q] * a.rny[i]) + 0.0 * 0.0) - 1.0;
+            tmp_t = tmp_t + wb[2 * k + 1] * tmp_n;
+        }
+        ooR = sqrt(fabs(tmp_t));
+    }
+    if (ti == 2)
+        for (int k = 0; k < a.slice_w[i >> 5]; k++) {
+            const long long o = sell_at(base, k, ln);
+            a.wx[o] = -a.wx[o];
+            a.wy[o] = -a.wy[o];
+        }
+    for (int row = 1; row <= 2; row++) {
+        if (ti != 0) break;
+        const int r = a.brow[4 * jj + row - 1];
+        const long long rb = a.slice_ptr[r >> 5];
+        const double den = row == 1 ? 1.0 + ooR * a.sp[r] : 1.0 + (2.0 * ooR) * a.sp[r];
+        for (int k = 0; k < a.slice_w[r >> 5]; k++) {
+            const long long o = sell_at(rb, k, r & 31);
+            a.wl[o] = a.wl[o] + (a.wx[o] * ooR) / den;
+        }
+    }
+    if (ti == 0)
+        for (int k = 0; k < a.cnt[i]; k++) {
+            const long long o = sell_at(base, k, ln);
+            wb[2 * k] = wb[2 * k] + a.wx[o] * ooR;
+            a.wl[o] = wb[2 * k] + wb[2 * k + 1];
+        }
+    const double xn = a.rnx[i], yn = a.rny[i];
+    for (int row = 1; row <= 2; row++) {
+        const int r = a.brow[4 * jj + row - 1];
+        const long long rb = a.slice_ptr[r >> 5];
+        for (int k = 0; k < a.cnt[r]; k++) {
+            const long long o = sell_at(rb, k, r & 31);
+            const double g1 = a.wx[o], g2 = a.wy[o];
+            a.wx[o] = (0.0 + xn * g1) + (-yn) * g2;
+            a.wy[o] = (0.0 + yn * g1) + xn * g2;
+        }
+    }
 }
 
 template <int ORDER>
@@ -680,8 +1007,46 @@ int labf_weights_device(Handle *H) {
     return 0;
 }
 
+int boundary_prune_links(Handle *H);
+
+// calc_boundary_weights (labf.F90:505-1039); the links of the boundary nodes are pruned by
+// boundary_prune_links() first.
+int boundary_weights_device(Handle *H) {
+    if (H->nb == 0) return 0;
+    const int nb = H->nb;
+    if (!H->wb2 && dalloc(H, &H->wb2, (size_t)nb * H->nplink * 2)) return SUNSET_ERR_NOMEM;
+    int *derr;
+    if (dalloc(H, &derr, 1)) return SUNSET_ERR_NOMEM;
+    cudaStream_t st = H->stream;
+    SUNSET_CUDA(H, cudaMemsetAsync(derr, 0, sizeof(int), st));
+    BndArgs a{H->npfb, nb, H->nplink, H->h3, H->px, H->py, H->h, H->sp, H->rnx, H->rny, H->ntype, H->gpar,
+              H->fdpar, H->blist, H->brow, H->cnt, H->cnt_small, H->lpt, H->lidx, H->lloc, H->slice_ptr,
+              H->slice_w, H->wx, H->wy, H->wl, H->wh, H->wb2, derr};
+    k_boundary_node_weights<<<(nb + 3) / 4, 128, 0, st>>>(a);
+    k_boundary_row_weights<<<(2 * nb + 3) / 4, 128, 0, st>>>(a);
+    k_boundary_frame<<<(nb + 127) / 128, 128, 0, st>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    int herr = 0;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    dfree(H, derr);
+    if (herr) return set_err(H, SUNSET_ERR_SVD, "SVD not converging at boundary node or row %d", herr - 1);
+    return 0;
+}
+
+int boundary_prune_links(Handle *H) {
+    if (H->nb == 0) return 0;
+    BndArgs a{H->npfb, H->nb, H->nplink, H->h3, H->px, H->py, H->h, H->sp, H->rnx, H->rny, H->ntype, H->gpar,
+              H->fdpar, H->blist, H->brow, H->cnt, H->cnt_small, H->lpt, H->lidx, H->lloc, H->slice_ptr,
+              H->slice_w, H->wx, H->wy, H->wl, H->wh, H->wb2, nullptr};
+    k_prune_boundary_links<<<(H->nb + 127) / 128, 128, 0, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
 int labf_sums_device(Handle *H) {
-    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->slice_ptr,
+    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->fdpar, H->slice_ptr,
               H->wx, H->wy, H->wl, H->wh, H->gsx, H->gsy, H->lsum, H->hsum, H->vol};
     k_labf_sums<<<(H->npfb + 255) / 256, 256, 0, H->stream>>>(a);
     SUNSET_CUDA(H, cudaGetLastError());
@@ -690,7 +1055,7 @@ int labf_sums_device(Handle *H) {
 }
 
 int filter_coefficients_device(Handle *H) {
-    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->slice_ptr,
+    SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->fdpar, H->slice_ptr,
               H->wx, H->wy, H->wl, H->wh, H->gsx, H->gsy, H->lsum, H->hsum, H->vol};
     k_filter_coeff<<<(H->npfb + 255) / 256, 256, 0, H->stream>>>(a);
     SUNSET_CUDA(H, cudaGetLastError());

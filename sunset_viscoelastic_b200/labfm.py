@@ -23,7 +23,8 @@ RHS_FIELDS = ["ro", "rou", "rov", "xx", "xy", "yy", "zz"]
 # C-ABI symbols declared in include/sunset_gpu.h
 ABI_SYMBOLS = [
     "sunset_version", "sunset_create", "sunset_destroy", "sunset_last_error", "sunset_build_domain",
-    "sunset_get_sizes", "sunset_find_neighbours", "sunset_calc_labf_weights", "sunset_calc_labf_sums",
+    "sunset_get_sizes", "sunset_find_neighbours", "sunset_calc_labf_weights", "sunset_calc_boundary_weights",
+    "sunset_calc_labf_sums",
     "sunset_filter_coefficients", "sunset_get_neighbours", "sunset_get_weights", "sunset_calc_gradient",
     "sunset_calc_laplacian", "sunset_calc_filtered_var", "sunset_calc_filter_term", "sunset_set_state",
     "sunset_get_state", "sunset_calc_all_rhs", "sunset_set_tstep", "sunset_step", "sunset_get_time",
@@ -72,8 +73,8 @@ def load_library(build_if_missing: bool = True):
     L.sunset_build_domain.argtypes = [P, C.c_int, ip, dp, dp, ip, dp, dp, dp, C.c_double, C.c_double, C.c_double,
                                       C.c_double, ip, C.c_double]
     L.sunset_get_sizes.argtypes = [P] + [C.POINTER(C.c_int)] * 4
-    for n in ["sunset_find_neighbours", "sunset_calc_labf_weights", "sunset_calc_labf_sums",
-              "sunset_filter_coefficients", "sunset_synchronize"]:
+    for n in ["sunset_find_neighbours", "sunset_calc_labf_weights", "sunset_calc_boundary_weights",
+              "sunset_calc_labf_sums", "sunset_filter_coefficients", "sunset_synchronize"]:
         getattr(L, n).argtypes = [P]
     L.sunset_get_neighbours.argtypes = [P, ip, ip, ip]
     L.sunset_get_weights.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
@@ -160,6 +161,9 @@ class Sunset:
     def calc_labf_weights(self):
         self._chk(self.L.sunset_calc_labf_weights(self.h))
 
+    def calc_boundary_weights(self):
+        self._chk(self.L.sunset_calc_boundary_weights(self.h))
+
     def calc_labf_sums(self):
         self._chk(self.L.sunset_calc_labf_sums(self.h))
 
@@ -167,9 +171,11 @@ class Sunset:
         self._chk(self.L.sunset_filter_coefficients(self.h))
 
     def setup(self):
-        """sunset.F90:51-60: find_neighbours, calc_labf_weights, calc_labf_sums, filter_coefficients."""
+        """sunset.F90:51-60: find_neighbours, calc_labf_weights, calc_boundary_weights (with
+        boundary nodes), calc_labf_sums, filter_coefficients."""
         self.find_neighbours()
         self.calc_labf_weights()
+        self.calc_boundary_weights()
         self.calc_labf_sums()
         self.filter_coefficients()
         return self
