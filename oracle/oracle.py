@@ -283,8 +283,7 @@ class Oracle:
 
 def for_workload(wl, ns=None, **over):
     """Oracle configured for a nodesets.Workload."""
-    kw = dict(form=wl.form, order=wl.order, Re=wl.Re, Wi=wl.Wi, beta=wl.beta, epsPTT=wl.epsPTT, Ma=wl.Ma,
-              h_over_s=wl.h_over_s)
+    kw = wl.params()
     kw.update(over)
     o = Oracle(**kw)
     o.build_domain(ns if ns is not None else wl.nodes())

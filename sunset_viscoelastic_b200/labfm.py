@@ -317,8 +317,7 @@ def kinetic_energy_noalloc(device, npfb, ro_ptr, u_ptr, v_ptr, vol_ptr, out_ptr,
 
 
 def for_workload(wl, ns=None, precision="fp64", device=0, **over):
-    kw = dict(form=wl.form, order=wl.order, Re=wl.Re, Wi=wl.Wi, beta=wl.beta, epsPTT=wl.epsPTT, Ma=wl.Ma,
-              h_over_s=wl.h_over_s, precision=precision, device=device)
+    kw = dict(wl.params(), precision=precision, device=device)
     kw.update(over)
     s = Sunset(**kw)
     s.build_domain(ns if ns is not None else wl.nodes())

@@ -79,6 +79,21 @@ def jittered_lattice(nside: int, jitter: float = 0.3, seed: int = 12345,
                    s=np.full(n, s), xmin=0.0, xmax=length, ymin=0.0, ymax=length, bcond=(1, 1, 1, 1))
 
 
+def reader_nodes(ns: NodeSet):
+    """Positions and types of the node list the reference's reader builds from IPART rows:
+    each boundary node (node_type 0..2) is followed by four FD rows at j s along its normal,
+    node_type -j (setup_domain.F90:177-199)."""
+    x, y, t = [], [], []
+    for k in range(ns.n):
+        x.append(ns.x[k]); y.append(ns.y[k]); t.append(int(ns.node_type[k]))
+        if 0 <= ns.node_type[k] <= 2:
+            for j in range(1, 5):
+                x.append(ns.x[k] + (ns.nx[k] * float(j)) * ns.s[k])
+                y.append(ns.y[k] + (ns.ny[k] * float(j)) * ns.s[k])
+                t.append(-j)
+    return np.array(x), np.array(y), np.array(t, np.int32)
+
+
 def _with_gaps(types: np.ndarray) -> np.ndarray:
     """Global indices leaving room for the four FD rows the reader adds after each boundary
     node (it numbers them global_index + 1..4, setup_domain.F90:183-190)."""
@@ -109,6 +124,77 @@ def channel(ny_cells: int, lx: float = 1.0, ly: float = 1.0, jitter: float = 0.3
     ny = np.concatenate([np.ones(nxc), np.zeros(n_int), -np.ones(nxc)])
     return NodeSet(x=x, y=y, node_type=t, nx=nx, ny=ny, s=np.full(len(x), s), xmin=0.0, xmax=lx,
                    ymin=0.0, ymax=ly, bcond=(1, 1, 0, 0), gi=_with_gaps(t))
+
+
+def cylinder_channel(R: float = 1.0, half_length: float = 15.0, half_height: float = 2.0, s_min_frac: float = 1 / 64,
+                     s_max_frac: float = 1 / 16, growth: float = 0.1, jitter: float = 0.3,
+                     seed: int = 12345) -> NodeSet:
+    """Channel [-half_length, half_length] x [-half_height, half_height], periodic in x, with
+    no-slip walls (node_type 0) at y = +-half_height and a cylinder of radius R at the
+    origin.  Local spacing s(r) = s_min + growth (r - R'), capped at s_max, with
+    s_min = s_min_frac R, s_max = s_max_frac R and R' = R + 4 s_min: the law is measured from
+    the cylinder's last FD row, so the first fluid layers continue the rows' spacing (measured
+    from R itself the first ring already sits at 1.4 s_min, and the order-6 stencils of the
+    fourth FD row, which then see mostly the regular polar grid of the rows, reach condition
+    numbers of 1e9).
+
+    Boundary nodes: the cylinder at spacing ~s_min with outward normals, the walls at s_max
+    with normals into the channel; the reader adds their FD rows at 1..4 s along the normal.
+    Fluid nodes: rings around the cylinder, from just outside its FD rows, each ring one
+    local spacing further out, while the spacing grows; beyond them the jittered lattice at
+    s_max, kept clear of the rings and of the walls' FD rows.  Every fluid node is moved by
+    U(-jitter s, jitter s) per axis (default_rng(seed))."""
+    rng = np.random.default_rng(seed)
+    s_min, s_max = s_min_frac * R, s_max_frac * R
+    r_fd = R + 4.0 * s_min  # the cylinder's last FD row: the fluid continues at s_min from there
+    sfun = lambda r: np.minimum(s_min + growth * np.maximum(r - r_fd, 0.0), s_max)
+    xs, ys, ts, nxs, nys, ss = [], [], [], [], [], []
+
+    def add(x, y, t, nx, ny, sp):
+        xs.append(np.atleast_1d(x)); ys.append(np.atleast_1d(y)); ts.append(np.atleast_1d(t).astype(np.int32))
+        nxs.append(np.atleast_1d(nx)); nys.append(np.atleast_1d(ny)); ss.append(np.atleast_1d(sp))
+
+    # cylinder wall
+    nb = int(round(2 * np.pi * R / s_min))
+    th = 2 * np.pi * np.arange(nb) / nb
+    sb = 2 * np.pi * R / nb
+    add(R * np.cos(th), R * np.sin(th), np.zeros(nb), np.cos(th), np.sin(th), np.full(nb, sb))
+    # channel walls
+    nw = int(round(2 * half_length / s_max))
+    sw = 2 * half_length / nw
+    xw = -half_length + (np.arange(nw) + 0.5) * sw
+    for y0, ny0 in ((-half_height, 1.0), (half_height, -1.0)):
+        add(xw, np.full(nw, y0), np.zeros(nw), np.zeros(nw), np.full(nw, ny0), np.full(nw, sw))
+    # rings
+    r = R + 4.0 * sb + sfun(R + 4.0 * sb)  # = R + 5 s_min
+    k = 0
+    ring_out = R
+    while True:
+        sr = float(sfun(r))
+        m = int(round(2 * np.pi * r / sr))
+        if r + sr > half_height - 4.5 * sw or (sr >= s_max and r > r_fd + (s_max - s_min) / growth + 2 * s_max):
+            break
+        a = 2 * np.pi * (np.arange(m) + 0.5 * (k % 2)) / m
+        sp = 2 * np.pi * r / m
+        x = r * np.cos(a) + rng.uniform(-jitter * sp, jitter * sp, m)
+        y = r * np.sin(a) + rng.uniform(-jitter * sp, jitter * sp, m)
+        add(x, y, np.full(m, 999), np.zeros(m), np.zeros(m), np.full(m, sp))
+        ring_out = r
+        r = r + sr
+        k += 1
+    # lattice beyond the rings and clear of the walls' FD rows
+    ny_rows = int(round(2 * half_height / sw))
+    yj = -half_height + np.arange(5, ny_rows - 4) * sw
+    ix, iy = np.meshgrid(xw, yj, indexing="xy")
+    keep = np.hypot(ix, iy) > ring_out + 0.75 * s_max
+    n = int(keep.sum())
+    x = ix[keep] + rng.uniform(-jitter * sw, jitter * sw, n)
+    y = iy[keep] + rng.uniform(-jitter * sw, jitter * sw, n)
+    add(x, y, np.full(n, 999), np.zeros(n), np.zeros(n), np.full(n, sw))
+    cat = lambda v: np.concatenate(v)
+    t = cat(ts)
+    return NodeSet(x=cat(xs), y=cat(ys), node_type=t, nx=cat(nxs), ny=cat(nys), s=cat(ss), xmin=-half_length,
+                   xmax=half_length, ymin=-half_height, ymax=half_height, bcond=(1, 1, 0, 0), gi=_with_gaps(t))
 
 
 def poiseuille_state(ns: NodeSet, G: float, mu_total: float, lam: float, ly: float = 1.0):
@@ -178,17 +264,38 @@ class Workload:
     epsPTT: float = 0.0
     steps: int = 100
     cfl: float = 0.3
+    geometry: str = "periodic"   # "periodic" (jittered lattice) | "cylinder" (walled channel)
+    grav_x: float = 0.0          # body force in x
+    kolmogorov_forcing: int = -1  # the reference's default (Cholesky form only)
 
     @property
     def n(self) -> int:
-        return self.nside * self.nside
+        return self.nside * self.nside if self.geometry == "periodic" else self.nodes().n
 
     @property
     def h_over_s(self) -> float:
-        return self.radius_over_s / 2.0  # support radius = ss*h with ss = 2
+        # support radius = ss*h with ss = 2; 0 keeps the reference's own hovs / hovs_bound
+        return self.radius_over_s / 2.0
 
     def nodes(self) -> NodeSet:
+        if self.geometry == "cylinder":
+            return cylinder_channel()
         return jittered_lattice(self.nside)
+
+    def params(self) -> dict:
+        """Keyword arguments of labfm.Sunset / oracle.Oracle for this workload."""
+        return dict(form=self.form, order=self.order, Re=self.Re, Wi=self.Wi, beta=self.beta, epsPTT=self.epsPTT,
+                    Ma=self.Ma, h_over_s=self.h_over_s, grav=(self.grav_x, 0.0, 0.0),
+                    kolmogorov_forcing=self.kolmogorov_forcing)
+
+    def initial(self, ns: NodeSet) -> dict:
+        """Initial state on the reader's node list (FD rows included)."""
+        if self.geometry == "cylinder":
+            x, y, _ = reader_nodes(ns)
+            n = len(x)
+            z, one = np.zeros(n), np.ones(n)
+            return dict(ro=one, u=z, v=z, cxx=one, cxy=z, cyy=one, czz=one)
+        return initial_state(ns)
 
 
 # Radii.  The reference adapts each node's stencil (labf.F90:1079-1721); with one fixed
@@ -202,10 +309,15 @@ class Workload:
 # step 500 (max |rho - 1| 4e-9 at step 50, 3e-4 at step 400); the reference's own initial
 # stencil for order 8, h = 2.7 s (common_parameter.F90:55, radius ss*h = 5.4 s, K ~ 92),
 # stays bounded through 500 steps.  Order 4 uses 3.0 s (K ~ 28).
+# The walled cylinder channel: Oldroyd-B (direct form) at Re 0.01, Wi 0.5, beta 0.59,
+# Ma 0.05, driven by a body force of 50 (a centreline speed near 1 in the empty channel), from
+# rest; the reference's own stencil sizes (hovs 2.7, hovs_bound 2.4 at order 8).
 WORKLOADS = {
     "periodic-di-o4-16k": Workload("periodic-di-o4-16k", 128, 4, 3.0, "di", steps=100),
     "periodic-lc-o6-262k": Workload("periodic-lc-o6-262k", 512, 6, 4.2, "lc", epsPTT=0.25, steps=200),
     "periodic-chl-o8-1m": Workload("periodic-chl-o8-1m", 1024, 8, 5.4, "chl", Wi=2.0, beta=0.1, steps=500),
+    "cylinder-channel-o8": Workload("cylinder-channel-o8", 0, 8, 0.0, "di", Re=0.01, Wi=0.5, beta=0.59, Ma=0.05,
+                                    steps=2000, geometry="cylinder", grav_x=50.0, kolmogorov_forcing=0),
 }
 
 
