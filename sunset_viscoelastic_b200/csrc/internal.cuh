@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include <string>
@@ -84,6 +85,42 @@ struct StepConsts {
     double csq, c_sound, coef_solvent, coef_polymeric, lambda, epsPTT, fenep_l2, Mdiff, Re, Wi, beta;
     double visc_total, rho_char, L_char, grav0, grav1, ero_norm, erou_norm, exx_norm;
 };
+
+// Derived parameters of a run (load_data.F90:131-148) and the switches of the step kernels.
+inline StepConsts step_consts(const SunsetConfig &c, int npfb, int nslices, bool has_mirrors, bool has_walls) {
+    StepConsts K{};
+    K.npfb = npfb;
+    K.nslices = nslices;
+    K.form = c.form;
+    K.fenep = c.fenep;
+    K.mcorr = c.mcorr;
+    K.kolmo = c.kolmogorov_forcing < 0 ? (c.form == SUNSET_FORM_CHL) : c.kolmogorov_forcing;
+    K.di_full = c.di_full_gradients;
+    K.has_mirrors = has_mirrors;
+    K.has_walls = has_walls;
+    K.mdiff_on = c.Mdiff != 0.0;
+    double t = c.U_char / c.Ma;
+    K.csq = t * t;
+    K.c_sound = sqrt(K.csq);
+    K.rho_char = 1.0;
+    K.visc_total = K.rho_char * c.U_char * c.L_char / c.Re;
+    K.coef_solvent = c.beta * K.visc_total;
+    K.lambda = c.Wi * c.L_char / c.U_char;
+    K.coef_polymeric = ((1.0 - c.beta) * K.visc_total) / K.lambda;
+    K.epsPTT = c.epsPTT;
+    K.fenep_l2 = c.fenep_l2;
+    K.Mdiff = c.Mdiff;
+    K.Re = c.Re;
+    K.Wi = c.Wi;
+    K.beta = c.beta;
+    K.L_char = c.L_char;
+    K.grav0 = c.grav[0];
+    K.grav1 = c.grav[1];
+    K.ero_norm = 1.0 / 1.0;
+    K.erou_norm = 1.0 / (1.0 * c.U_char);
+    K.exx_norm = 1.0 / (1.0);
+    return K;
+}
 
 struct Handle {
     SunsetConfig cfg{};

@@ -852,38 +852,7 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
 }
 
 int upload_consts(Handle *H) {
-    const SunsetConfig &c = H->cfg;
-    StepConsts K{};
-    K.npfb = H->npfb;
-    K.nslices = H->nslices;
-    K.form = c.form;
-    K.fenep = c.fenep;
-    K.mcorr = c.mcorr;
-    K.kolmo = c.kolmogorov_forcing < 0 ? (c.form == SUNSET_FORM_CHL) : c.kolmogorov_forcing;
-    K.di_full = c.di_full_gradients;
-    K.has_mirrors = H->has_mirrors;
-    K.has_walls = H->nb > 0;
-    K.mdiff_on = c.Mdiff != 0.0;
-    double t = c.U_char / c.Ma;
-    K.csq = t * t;
-    K.c_sound = sqrt(K.csq);
-    K.rho_char = 1.0;
-    K.visc_total = K.rho_char * c.U_char * c.L_char / c.Re;
-    K.coef_solvent = c.beta * K.visc_total;
-    K.lambda = c.Wi * c.L_char / c.U_char;
-    K.coef_polymeric = ((1.0 - c.beta) * K.visc_total) / K.lambda;
-    K.epsPTT = c.epsPTT;
-    K.fenep_l2 = c.fenep_l2;
-    K.Mdiff = c.Mdiff;
-    K.Re = c.Re;
-    K.Wi = c.Wi;
-    K.beta = c.beta;
-    K.L_char = c.L_char;
-    K.grav0 = c.grav[0];
-    K.grav1 = c.grav[1];
-    K.ero_norm = 1.0 / 1.0;
-    K.erou_norm = 1.0 / (1.0 * c.U_char);
-    K.exx_norm = 1.0 / (1.0);
+    const StepConsts K = step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, H->nb > 0);
     SUNSET_CUDA(H, cudaMemcpyToSymbolAsync(cK, &K, sizeof(K), 0, cudaMemcpyHostToDevice, H->stream));
     return 0;
 }
