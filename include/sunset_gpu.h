@@ -146,6 +146,24 @@ int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *
 int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
                              double *bytes_per_launch);
 
+/* Adjoint of the fixed-dt time step (log-conformation form, FP64, node sets without walls).
+   From the current state it runs nsteps steps of size dt (the handle ends at the final
+   state), evaluates J = sum_i 1/2 rho_i |u_i|^2 vol_i at the final state, and returns dJ/dWi
+   and dJ/dbeta in dJ_dparams[2] and, unless dJ_dstate0 is NULL, dJ with respect to the
+   initial state (7*npfb host doubles in reference order: ro rou rov psixx psixy psiyy psizz).
+   The reverse sweep recomputes the stage inputs from states stored every checkpoint_every
+   steps.  The adjoint is of the discrete step as computed (step.F90:218-512 with the filter
+   and the mass correction); SUNSET_ERR_SCOPE for other forms, mixed precision, walls or
+   Mdiff != 0.  No reference counterpart (the reference has no adjoint). */
+int sunset_adjoint_run(SunsetHandle *h, double dt, int nsteps, int checkpoint_every, double *J,
+                       double *dJ_dparams, double *dJ_dstate0);
+
+/* Transposed single operators: out = D^T gbar with D the operator of sunset_calc_gradient
+   (which 0: d/dx, 1: d/dy), sunset_calc_laplacian (2) or sunset_calc_filter_term (3),
+   npfb values in reference order, flags as for the operators.  A gather over the reverse
+   neighbour lists (deterministic, no atomics).  No reference counterpart. */
+int sunset_adjoint_apply_D(SunsetHandle *h, int which, const double *gbar, double *out, int flags);
+
 /* Allocation-free variant of sunset_kinetic_energy/sunset_mass; it has no counterpart in
    the reference.  For callers that cannot allocate device memory (their arrays live in
    their own device pool, and cudaMalloc could synchronise the device or exceed a memory

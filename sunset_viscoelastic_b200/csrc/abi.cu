@@ -591,6 +591,36 @@ int sunset_run_host(SunsetHandle *sh, const double *state_in, double dt, int nst
     return check_err_flag(H);
 }
 
+int sunset_adjoint_apply_D(SunsetHandle *sh, int which, const double *gbar, double *out, int flags) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!gbar || !out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (which < 0 || which > 3) return set_err(H, SUNSET_ERR_ARG, "which must be 0 (d/dx), 1 (d/dy), 2 (Laplacian) or 3 (filter)");
+    const int n = H->npfb;
+    double *p = H->tmpd, *o = H->tmpd + n;
+    if (int rc = to_internal(H, gbar, flags, p)) return rc;
+    if (int rc = adjoint_apply_D(H, which, p, o)) return rc;
+    return to_reference(H, o, flags, out);
+}
+
+int sunset_adjoint_run(SunsetHandle *sh, double dt, int nsteps, int checkpoint_every, double *J,
+                       double *dJ_dparams, double *dJ_dstate0) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!J || !dJ_dparams) return set_err(H, SUNSET_ERR_ARG, "null output");
+    if (!(dt > 0.0)) return set_err(H, SUNSET_ERR_ARG, "dt must be positive");
+    const int n = H->npfb;
+    double *du = nullptr;
+    if (dalloc(H, &du, 7 * (size_t)n)) return SUNSET_ERR_NOMEM;
+    int rc = adjoint_run(H, dt, nsteps, checkpoint_every, J, dJ_dparams, du);
+    if (!rc && dJ_dstate0)
+        for (int f = 0; f < 7 && !rc; f++)
+            rc = to_reference(H, du + (size_t)f * n, SUNSET_PTR_HOST, dJ_dstate0 + (size_t)f * n);
+    dfree(H, du);
+    return rc;
+}
+
 int sunset_time_stage_kernel(SunsetHandle *sh, int reps, double *ms_per_launch, double *bytes_per_launch) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;

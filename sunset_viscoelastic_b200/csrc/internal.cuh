@@ -194,6 +194,16 @@ struct Handle {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_mode[2] = {-1, -1};
 
+    // ---- adjoint (step.cu) ----
+    long long *rptr = nullptr;                 // reverse links of each node (npfb + 1)
+    int *rslot = nullptr, *rnode = nullptr;    // their SELL slots and owning nodes
+    unsigned char *rcode = nullptr;            // reflection code | small-link flag << 2
+    double *adj_gb[18] = {}, *adj_sb[6] = {}, *adj_sbar[7] = {}, *adj_ua[7] = {}, *adj_ub[7] = {};
+    double *adj_tpart = nullptr, *adj_acc = nullptr, *adj_cp = nullptr;
+    std::vector<Fields> adj_store;             // stage inputs of one checkpoint segment
+    int adj_ckpt = 0, adj_nseg = 0;
+    bool adj_ready = false;
+
     std::vector<void *> allocs;
 };
 
@@ -246,6 +256,8 @@ int op_laplacian(Handle *H, const double *phi, double *lap);
 int op_filter(Handle *H, const double *phi, double *out, int term_only);
 int reduce_ke_mass(Handle *H, double *ke, double *mass);
 int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes);
+int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *dtheta, double *dU0);
+int adjoint_apply_D(Handle *H, int which, const double *gbar, double *out);
 
 }  // namespace sunset
 

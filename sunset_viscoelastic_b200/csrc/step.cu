@@ -19,6 +19,7 @@
 // from glibc in the last bit).
 #include <type_traits>
 
+#include "adjoint.cuh"
 #include "internal.cuh"
 #include "physics.cuh"
 
@@ -1167,6 +1168,437 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     const double wb = mx ? 4.0 : 8.0;
     *bytes = (double)links * (2 + 3 * wb) +
              (double)H->npfb * (8.0 * nread + 3.0 * nf * wb + 8.0 * (3.0 * nwrite + 7.0) / 4.0 + 8.0 * 4);
+    return 0;
+}
+
+
+// =======================================================================================
+// Adjoint of the fixed-dt time step (log-conformation form, periodic node sets, FP64).
+//
+// The forward map of one step is U_{n+1} = mcorr(filter(U4)), with the four stages
+// U_{s+1} = S_s + alpha_s dt R(U_s), S_{s+1} = S_s + beta_s dt R(U_s), S_0 = U_0
+// (alpha = a21, a32, a43, b4; beta = b1, b2, b3; step.F90:291-343).  Its reverse, given the
+// adjoint of U_{n+1}: the filter's transpose (with the mass correction's), then for
+// s = 3..0: R_bar = dt (alpha_s U_bar_{s+1} + beta_s S_bar_{s+1}), S_bar_s = U_bar_{s+1} +
+// S_bar_{s+1}, U_bar_s = dR(U_s)^T R_bar (+ S_bar_0 at s = 0).  dR^T is the pointwise reverse
+// of adjoint.cuh followed by the transposed stencils: node j collects w_ij g_bar_i from every
+// node i whose links reach it, through a reverse-neighbour list built once (a gather, in a
+// fixed order, without atomics), plus its own -sum(w) g_bar_j terms, and the derived fields
+// (u = rho u / rho, c from psi) are reversed into the conservative state.
+//
+// Stage inputs are recomputed per segment of `checkpoint_every` steps from the state stored
+// at the segment's start, and kept (13 fields per stage) for that segment's reverse sweep.
+// =======================================================================================
+namespace {
+
+struct AdjArgs {
+    int npfb;
+    const long long *rptr;      // reverse links of node j: [rptr[j], rptr[j+1])
+    const int *rslot, *rnode;   // SELL slot (reference order) and the node owning it
+    const unsigned char *rcode; // bits 0-1: reflection code, bit 2: a small link (stencils of the stage)
+    const double *wx, *wy, *wl, *wh;
+    const double *gsx, *gsy, *lsum, *hsum, *vol;
+    double *gb[kAdjG];
+    double *sb[kAdjS];
+    double *ub_in[7], *ub_out[7], *sbar[7];
+    double *tpart;
+    const double *mc_sum, *mc_tv;  // sum of rho_bar and of the volumes (mass correction)
+    double dt, alpha, beta;
+    int first, add_sbar, mcorr;
+};
+
+__device__ __forceinline__ double sgn_u(int c) { return (c == 1 || c == 3) ? -1.0 : 1.0; }
+__device__ __forceinline__ double sgn_v(int c) { return (c == 2 || c == 3) ? -1.0 : 1.0; }
+__device__ __forceinline__ double sgn_xy(int c) { return (c == 1 || c == 2) ? -1.0 : 1.0; }
+
+// Stage adjoint, part 1: the stage's stencil sums g at its input state (the forward gather),
+// R_bar and S_bar of each node, and the pointwise reverse: g_bar, the node's direct state
+// adjoint and block sums of the parameter adjoint.
+__global__ void __launch_bounds__(kTile, 2) k_adj_point_lc(StageArgs A, AdjArgs B) {
+    extern __shared__ __align__(16) double smem[];
+    constexpr int NG = ngather(SUNSET_FORM_LC, false);
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    bool active = (i >> 5) < cK.nslices;
+    LinkRing<false, 3, ring_depth(false)> R;
+    R.src[0] = reinterpret_cast<const double2 *>(A.wx);
+    R.src[1] = reinterpret_cast<const double2 *>(A.wy);
+    R.src[2] = reinterpret_cast<const double2 *>(A.wl);
+    R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
+           active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
+    R.prologue();
+    load_halo<NG>(A, smem, [&](int f) { return gather_src<SUNSET_FORM_LC, false>(A.in, f); });
+    Grads g;
+    if (active) gather_stage<SUNSET_FORM_LC, false, false>(A, i, smem, R, g);
+    double t0 = 0.0, t1 = 0.0;
+    if (active && i < B.npfb) {
+        const Fields &F = A.in;
+        const double s[kAdjS] = {F.ro[i], F.rou[i], F.rov[i], F.q[0][i], F.q[1][i], F.q[2][i]};
+        const double gv[kAdjG] = {g.ro_x, g.ro_y, g.u_x, g.u_y, g.lapu, g.v_x, g.v_y, g.lapv, g.cxx_x, g.cxy_x,
+                                  g.cxy_y, g.cyy_y, g.pxx_x, g.pxx_y, g.pxy_x, g.pxy_y, g.pyy_x, g.pyy_y};
+        double rb[kAdjR];
+        for (int f = 0; f < kAdjR; f++) {
+            const double ui = B.ub_in[f][i], si = B.sbar[f][i];
+            rb[f] = B.dt * (B.alpha * ui + B.beta * si);
+            B.sbar[f][i] = ui + si;
+        }
+        double sbv[kAdjS] = {0, 0, 0, 0, 0, 0}, gbv[kAdjG], tb[2] = {0.0, 0.0};
+        for (int k = 0; k < kAdjG; k++) gbv[k] = 0.0;
+        p_adjoint_lc(cK, s, gv, B.first != 0, rb, sbv, gbv, tb);
+        for (int k = 0; k < kAdjG; k++) B.gb[k][i] = gbv[k];
+        for (int k = 0; k < kAdjS; k++) B.sb[k][i] = sbv[k];
+        t0 = tb[0];
+        t1 = tb[1];
+    }
+    __shared__ double red[2][kTile];
+    red[0][threadIdx.x] = t0;
+    red[1][threadIdx.x] = t1;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) {
+            red[0][threadIdx.x] = red[0][threadIdx.x] + red[0][threadIdx.x + st];
+            red[1][threadIdx.x] = red[1][threadIdx.x] + red[1][threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        B.tpart[2 * blockIdx.x] = red[0][0];
+        B.tpart[2 * blockIdx.x + 1] = red[1][0];
+    }
+}
+
+// Stage adjoint, part 2: the transposed stencils and the reverse of the derived fields;
+// writes U_bar of the stage's input state (+ S_bar at the first stage).
+__global__ void __launch_bounds__(128) k_adj_transpose_lc(StageArgs A, AdjArgs B) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= B.npfb) return;
+    double ph[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // rho, u, v, cxx, cxy, cyy, psixx, psixy, psiyy
+    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) {
+        const int code = B.rcode[e];
+        if (!(code & 4)) continue;
+        const int o = B.rslot[e], i = B.rnode[e], rc = code & 3;
+        const double wx = B.wx[o], wy = B.wy[o], wl = B.wl[o];
+        ph[0] += wx * B.gb[G_RO_X][i] + wy * B.gb[G_RO_Y][i];
+        ph[1] += sgn_u(rc) * (wx * B.gb[G_U_X][i] + wy * B.gb[G_U_Y][i] + wl * B.gb[G_LAPU][i]);
+        ph[2] += sgn_v(rc) * (wx * B.gb[G_V_X][i] + wy * B.gb[G_V_Y][i] + wl * B.gb[G_LAPV][i]);
+        ph[3] += wx * B.gb[G_CXX_X][i];
+        ph[4] += sgn_xy(rc) * (wx * B.gb[G_CXY_X][i] + wy * B.gb[G_CXY_Y][i]);
+        ph[5] += wy * B.gb[G_CYY_Y][i];
+        ph[6] += wx * B.gb[G_PXX_X][i] + wy * B.gb[G_PXX_Y][i];
+        ph[7] += sgn_xy(rc) * (wx * B.gb[G_PXY_X][i] + wy * B.gb[G_PXY_Y][i]);
+        ph[8] += wx * B.gb[G_PYY_X][i] + wy * B.gb[G_PYY_Y][i];
+    }
+    const double gx = B.gsx[j], gy = B.gsy[j], ls = B.lsum[j];
+    ph[0] -= gx * B.gb[G_RO_X][j] + gy * B.gb[G_RO_Y][j];
+    ph[1] -= gx * B.gb[G_U_X][j] + gy * B.gb[G_U_Y][j] + ls * B.gb[G_LAPU][j];
+    ph[2] -= gx * B.gb[G_V_X][j] + gy * B.gb[G_V_Y][j] + ls * B.gb[G_LAPV][j];
+    ph[3] -= gx * B.gb[G_CXX_X][j];
+    ph[4] -= gx * B.gb[G_CXY_X][j] + gy * B.gb[G_CXY_Y][j];
+    ph[5] -= gy * B.gb[G_CYY_Y][j];
+    ph[6] -= gx * B.gb[G_PXX_X][j] + gy * B.gb[G_PXX_Y][j];
+    ph[7] -= gx * B.gb[G_PXY_X][j] + gy * B.gb[G_PXY_Y][j];
+    ph[8] -= gx * B.gb[G_PYY_X][j] + gy * B.gb[G_PYY_Y][j];
+    const Fields &F = A.in;
+    const double ooro = 1.0 / F.ro[j];
+    const double u = F.rou[j] * ooro, v = F.rov[j] * ooro;
+    double pb[3] = {0.0, 0.0, 0.0};
+    const double cb[3] = {ph[3], ph[4], ph[5]};
+    lc_c_from_psi_adj(F.q[0][j], F.q[1][j], F.q[2][j], cb, pb);
+    double U[7];
+    U[0] = B.sb[0][j] + ph[0] - (ph[1] * u + ph[2] * v) * ooro;
+    U[1] = B.sb[1][j] + ph[1] * ooro;
+    U[2] = B.sb[2][j] + ph[2] * ooro;
+    U[3] = B.sb[3][j] + ph[6] + pb[0];
+    U[4] = B.sb[4][j] + ph[7] + pb[1];
+    U[5] = B.sb[5][j] + ph[8] + pb[2];
+    U[6] = 0.0;
+    for (int f = 0; f < 7; f++) B.ub_out[f][j] = B.add_sbar ? U[f] + B.sbar[f][j] : U[f];
+}
+
+// Filter and mass correction reversed (rhs_lc.F90:818-893): U4_bar_j = Uf_bar_j (1 - hsum_j)
+// + sum over reverse links w_h Uf_bar_i, with Uf_bar = U_bar and, for rho,
+// rho_f_bar_i = rho_bar_i - vol_i sum(rho_bar) / sum(vol) when the mass is corrected.
+__global__ void __launch_bounds__(128) k_adj_filter_lc(AdjArgs B) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= B.npfb) return;
+    const double mc = B.mcorr ? *B.mc_sum / *B.mc_tv : 0.0;
+    auto uf = [&](int f, int i) { return f == 0 ? B.ub_in[0][i] - B.vol[i] * mc : B.ub_in[f][i]; };
+    double acc[6];
+    const double own = 1.0 - B.hsum[j];
+    for (int f = 0; f < 6; f++) acc[f] = uf(f, j) * own;
+    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) {
+        const int o = B.rslot[e], i = B.rnode[e], rc = B.rcode[e] & 3;
+        const double w = B.wh[o];
+        acc[0] += w * uf(0, i);
+        acc[1] += w * sgn_u(rc) * uf(1, i);
+        acc[2] += w * sgn_v(rc) * uf(2, i);
+        acc[3] += w * uf(3, i);
+        acc[4] += w * sgn_xy(rc) * uf(4, i);
+        acc[5] += w * uf(5, i);
+    }
+    for (int f = 0; f < 6; f++) B.ub_out[f][j] = acc[f];
+    B.ub_out[6][j] = 0.0;
+}
+
+// Adjoint of J = sum 1/2 rho |u|^2 vol at the final state.
+__global__ void k_adj_objective(int npfb, Fields F, const double *vol, AdjArgs B) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npfb) return;
+    const double u = F.u[i], v = F.v[i], w = vol[i];
+    B.ub_out[0][i] = -0.5 * (u * u + v * v) * w;
+    B.ub_out[1][i] = u * w;
+    B.ub_out[2][i] = v * w;
+    for (int f = 3; f < 7; f++) B.ub_out[f][i] = 0.0;
+}
+
+// Sum of rho_bar (block partials) for the mass correction's adjoint.
+__global__ void k_adj_sum(int npfb, const double *x, double *partials) {
+    __shared__ double sm[128];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    sm[threadIdx.x] = i < npfb ? x[i] : 0.0;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+}
+
+// acc[c] += sum_b partials[stride b + c] (c < stride), in block order.
+__global__ void k_adj_fold(const double *partials, int n, int stride, double *acc, int accumulate) {
+    __shared__ double sm[128];
+    for (int c = 0; c < stride; c++) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < n; b += blockDim.x) a = a + partials[stride * b + c];
+        sm[threadIdx.x] = a;
+        __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if ((int)threadIdx.x < st) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) acc[c] = accumulate ? acc[c] + sm[0] : sm[0];
+        __syncthreads();
+    }
+}
+
+// Transposed single operators (the adjoint of derivative application): out_j =
+// sum over reverse links w_ij gbar_i - sum_k w_jk gbar_j, for d/dx, d/dy, Laplacian or filter.
+__global__ void k_adj_apply_D(AdjArgs B, int which, const double *gbar, double *out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= B.npfb) return;
+    const double *w = which == 0 ? B.wx : which == 1 ? B.wy : which == 2 ? B.wl : B.wh;
+    const double *sum = which == 0 ? B.gsx : which == 1 ? B.gsy : which == 2 ? B.lsum : B.hsum;
+    double acc = 0.0;
+    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) {
+        if (which < 3 && !(B.rcode[e] & 4)) continue;
+        acc += w[B.rslot[e]] * gbar[B.rnode[e]];
+    }
+    out[j] = acc - sum[j] * gbar[j];
+}
+
+StageArgs make_args_io(Handle *H, const Fields &in, const Fields &out, int stage) {
+    StageArgs A = make_args(H, 0, stage, true);
+    A.in = in;
+    A.out = out;
+    return A;
+}
+
+}  // namespace
+
+// Reverse-neighbour lists (host build): for every node j the SELL slots, in the order of
+// (owning node, link), whose link points at j.
+static int adjoint_build_reverse(Handle *H) {
+    if (H->rptr) return 0;
+    const int n = H->npfb, nsl = H->nslices;
+    const long long L = H->nlinks_sell;
+    std::vector<int> lidx(L), cnt(n), cs(n);
+    std::vector<long long> sptr(nsl + 1);
+    SUNSET_CUDA(H, cudaMemcpy(lidx.data(), H->lidx, L * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cnt.data(), H->cnt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, n * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(sptr.data(), H->slice_ptr, (nsl + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    std::vector<long long> rptr(n + 1, 0);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < cnt[i]; k++) rptr[(lidx[sell_at(sptr[i >> 5], k, i & 31)] & kLinkMask) + 1]++;
+    for (int j = 0; j < n; j++) rptr[j + 1] += rptr[j];
+    const long long ne = rptr[n];
+    std::vector<int> rslot(ne), rnode(ne);
+    std::vector<unsigned char> rcode(ne);
+    std::vector<long long> fill(rptr.begin(), rptr.end() - 1);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < cnt[i]; k++) {
+            const long long o = sell_at(sptr[i >> 5], k, i & 31);
+            const int p = lidx[o] & kLinkMask, code = (unsigned)lidx[o] >> 30;
+            const long long e = fill[p]++;
+            rslot[e] = (int)o;
+            rnode[e] = i;
+            rcode[e] = (unsigned char)(code | (k < cs[i] ? 4 : 0));
+        }
+    if (dalloc(H, &H->rptr, n + 1) || dalloc(H, &H->rslot, ne ? ne : 1) || dalloc(H, &H->rnode, ne ? ne : 1) ||
+        dalloc(H, &H->rcode, ne ? ne : 1))
+        return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemcpy(H->rptr, rptr.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rslot, rslot.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rnode, rnode.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rcode, rcode.data(), ne * sizeof(unsigned char), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static AdjArgs adj_args(Handle *H) {
+    AdjArgs B{};
+    B.npfb = H->npfb;
+    B.rptr = H->rptr; B.rslot = H->rslot; B.rnode = H->rnode; B.rcode = H->rcode;
+    B.wx = H->wx; B.wy = H->wy; B.wl = H->wl; B.wh = H->wh;
+    B.gsx = H->gsx; B.gsy = H->gsy; B.lsum = H->lsum; B.hsum = H->hsum; B.vol = H->vol;
+    for (int k = 0; k < kAdjG; k++) B.gb[k] = H->adj_gb[k];
+    for (int k = 0; k < kAdjS; k++) B.sb[k] = H->adj_sb[k];
+    for (int f = 0; f < 7; f++) B.sbar[f] = H->adj_sbar[f];
+    B.tpart = H->adj_tpart;
+    return B;
+}
+
+int adjoint_apply_D(Handle *H, int which, const double *gbar, double *out) {
+    if (int rc = adjoint_build_reverse(H)) return rc;
+    AdjArgs B = adj_args(H);
+    k_adj_apply_D<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(B, which, gbar, out);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+static int alloc_fields(Handle *H, Fields &F) {
+    const int n = H->npfb;
+    if (dalloc(H, &F.ro, n) || dalloc(H, &F.rou, n) || dalloc(H, &F.rov, n) || dalloc(H, &F.u, n) || dalloc(H, &F.v, n))
+        return SUNSET_ERR_NOMEM;
+    for (int k = 0; k < 4; k++)
+        if (dalloc(H, &F.q[k], n) || dalloc(H, &F.c[k], n)) return SUNSET_ERR_NOMEM;
+    return 0;
+}
+
+int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *dtheta, double *dU0) {
+    if (H->cfg.form != SUNSET_FORM_LC)
+        return set_err(H, SUNSET_ERR_SCOPE, "the adjoint is built for the log-conformation form");
+    if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint runs the FP64 step");
+    if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers node sets without walls");
+    if (H->cfg.Mdiff != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint assumes Mdiff = 0");
+    if (nsteps < 1 || ckpt < 1) return set_err(H, SUNSET_ERR_ARG, "nsteps and checkpoint_every must be positive");
+    const int n = H->npfb;
+    cudaStream_t st = H->stream;
+    if (int rc = adjoint_build_reverse(H)) return rc;
+    if (int rc = upload_consts(H)) return rc;
+    const int nseg = (nsteps + ckpt - 1) / ckpt;
+    // storage: checkpoints (7 conservative fields), the stage inputs of one segment, scratch
+    if (!H->adj_ready || H->adj_ckpt != ckpt || H->adj_nseg < nseg) {
+        if (H->adj_ready) return set_err(H, SUNSET_ERR_ARG, "the adjoint storage of this handle was sized for other step counts");
+        H->adj_ckpt = ckpt;
+        H->adj_nseg = nseg;
+        H->adj_store.resize(4 * (size_t)ckpt + 2);
+        for (auto &F : H->adj_store)
+            if (int rc = alloc_fields(H, F)) return rc;
+        if (dalloc(H, &H->adj_cp, (size_t)7 * n * nseg)) return SUNSET_ERR_NOMEM;
+        for (int k = 0; k < kAdjG; k++)
+            if (dalloc(H, &H->adj_gb[k], n)) return SUNSET_ERR_NOMEM;
+        for (int k = 0; k < kAdjS; k++)
+            if (dalloc(H, &H->adj_sb[k], n)) return SUNSET_ERR_NOMEM;
+        for (int f = 0; f < 7; f++)
+            if (dalloc(H, &H->adj_sbar[f], n) || dalloc(H, &H->adj_ua[f], n) || dalloc(H, &H->adj_ub[f], n))
+                return SUNSET_ERR_NOMEM;
+        if (dalloc(H, &H->adj_tpart, 2 * (size_t)H->ntiles + 2 * (size_t)((n + 127) / 128) + 8) ||
+            dalloc(H, &H->adj_acc, 4))
+            return SUNSET_ERR_NOMEM;
+        H->adj_ready = true;
+        SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_point_lc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
+    }
+    DevScalars sc0;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&sc0, H->dsc, sizeof(sc0), cudaMemcpyDeviceToHost, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
+    // ---- forward with checkpoints ----
+    for (int sg = 0; sg < nseg; sg++) {
+        const Fields &F = H->buf[H->cur];
+        double *cp = H->adj_cp + (size_t)7 * n * sg;
+        double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
+        for (int f = 0; f < 7; f++)
+            SUNSET_CUDA(H, cudaMemcpyAsync(cp + (size_t)f * n, src[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        const int len = std::min(ckpt, nsteps - sg * ckpt);
+        if (int rc = step_run(H, dt, len, 0)) return rc;
+    }
+    if (int rc = reduce_ke_mass(H, J, nullptr)) return rc;
+    DevScalars scN;
+    SUNSET_CUDA(H, cudaMemcpyAsync(&scN, H->dsc, sizeof(scN), cudaMemcpyDeviceToHost, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    if (scN.err) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite error norm in the forward run");
+    // ---- reverse ----
+    const int TB = 128, nb = (n + TB - 1) / TB;
+    AdjArgs B = adj_args(H);
+    double **ua = H->adj_ua, **ubb = H->adj_ub;
+    for (int f = 0; f < 7; f++) B.ub_out[f] = ua[f];
+    k_adj_objective<<<nb, TB, 0, st>>>(n, H->buf[H->cur], H->vol, B);
+    SUNSET_CUDA(H, cudaMemsetAsync(H->adj_acc, 0, 4 * sizeof(double), st));
+    const double alpha[4] = {SUNSET_RK_A21, SUNSET_RK_A32, SUNSET_RK_A43, SUNSET_RK_B4};
+    const double beta[4] = {SUNSET_RK_B1, SUNSET_RK_B2, SUNSET_RK_B3, 0.0};
+    const size_t smem = halo_doubles(ngather(SUNSET_FORM_LC, false), H->halo_max) * sizeof(double) +
+                        LinkRing<false, 3, ring_depth(false)>::bytes();
+    double *part2 = H->adj_tpart + 2 * (size_t)H->ntiles;
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
+        // recompute the segment, keeping the stage inputs
+        {
+            Fields &F0 = H->adj_store[0];
+            const double *cp = H->adj_cp + (size_t)7 * n * sg;
+            k_set_conservative<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, cp, cp + n, cp + 2 * (size_t)n, cp + 3 * (size_t)n,
+                                                  cp + 4 * (size_t)n, cp + 5 * (size_t)n, cp + 6 * (size_t)n, F0);
+            const int it = sc0.itime + n0;
+            SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->itime, &it, sizeof(int), cudaMemcpyHostToDevice, st));
+            Fields &T = H->adj_store[4 * (size_t)ckpt], &X = H->adj_store[4 * (size_t)ckpt + 1];
+            for (int k = 0; k < len; k++) {
+                for (int s = 0; s < 4; s++) {
+                    StageArgs A = make_args_io(H, H->adj_store[4 * k + s], s < 3 ? H->adj_store[4 * k + s + 1] : T, s);
+                    if (int rc = launch_stage_any(H, A, false)) return rc;
+                }
+                Fields &next = k + 1 < len ? H->adj_store[4 * (k + 1)] : X;
+                StageArgs Fa = make_args_io(H, T, next, 5);
+                if (int rc = launch_filter<SUNSET_FORM_LC>(H, Fa, false)) return rc;
+                k_finalize<SUNSET_FORM_LC><<<nb, TB, 0, st>>>(Fa, 1);
+            }
+        }
+        // reverse sweep over the segment
+        for (int k = len - 1; k >= 0; k--) {
+            // filter and mass correction: ua (adjoint of U_{k+1}) -> ubb
+            for (int f = 0; f < 7; f++) { B.ub_in[f] = ua[f]; B.ub_out[f] = ubb[f]; }
+            if (H->cfg.mcorr) {
+                k_adj_sum<<<nb, TB, 0, st>>>(n, ua[0], part2);
+                k_adj_fold<<<1, 128, 0, st>>>(part2, nb, 1, H->adj_acc + 2, 0);
+            }
+            B.mcorr = H->cfg.mcorr;
+            B.mc_sum = H->adj_acc + 2;
+            B.mc_tv = &H->dsc->tv;
+            k_adj_filter_lc<<<nb, TB, 0, st>>>(B);
+            std::swap(ua, ubb);
+            for (int f = 0; f < 7; f++) SUNSET_CUDA(H, cudaMemsetAsync(B.sbar[f], 0, n * sizeof(double), st));
+            for (int s = 3; s >= 0; s--) {
+                StageArgs A = make_args_io(H, H->adj_store[4 * k + s], H->adj_store[4 * k + s], s);
+                for (int f = 0; f < 7; f++) { B.ub_in[f] = ua[f]; B.ub_out[f] = ubb[f]; }
+                B.dt = dt;
+                B.alpha = alpha[s];
+                B.beta = beta[s];
+                B.first = (s == 0) && (sc0.itime + n0 + k == 1);
+                B.add_sbar = s == 0;
+                k_adj_point_lc<<<H->ntiles, kTile, smem, st>>>(A, B);
+                k_adj_fold<<<1, 128, 0, st>>>(H->adj_tpart, H->ntiles, 2, H->adj_acc, 1);
+                k_adj_transpose_lc<<<nb, TB, 0, st>>>(A, B);
+                std::swap(ua, ubb);
+            }
+        }
+    }
+    SUNSET_CUDA(H, cudaGetLastError());
+    double acc[2];
+    SUNSET_CUDA(H, cudaMemcpyAsync(acc, H->adj_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    for (int f = 0; f < 7; f++)
+        SUNSET_CUDA(H, cudaMemcpyAsync(dU0 + (size_t)f * n, ua[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // the handle keeps the final state and its time
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &scN, sizeof(scN), cudaMemcpyHostToDevice, st));
+    SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    dtheta[0] = acc[0];
+    dtheta[1] = acc[1];
     return 0;
 }
 

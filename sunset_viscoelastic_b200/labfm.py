@@ -30,6 +30,7 @@ ABI_SYMBOLS = [
     "sunset_get_state", "sunset_calc_all_rhs", "sunset_set_tstep", "sunset_step", "sunset_get_time",
     "sunset_set_time", "sunset_kinetic_energy", "sunset_mass", "sunset_synchronize", "sunset_run_host",
     "sunset_time_stage_kernel", "sunset_step_timed", "sunset_kinetic_energy_noalloc",
+    "sunset_adjoint_run", "sunset_adjoint_apply_D",
 ]
 
 
@@ -91,6 +92,8 @@ def load_library(build_if_missing: bool = True):
     L.sunset_mass.argtypes = [P, C.POINTER(C.c_double)]
     L.sunset_run_host.argtypes = [P, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
     L.sunset_time_stage_kernel.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.sunset_adjoint_run.argtypes = [P, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double), dp, C.c_void_p]
+    L.sunset_adjoint_apply_D.argtypes = [P, C.c_int, dp, dp, C.c_int]
     L.sunset_step_timed.argtypes = [P, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.sunset_kinetic_energy_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                 C.c_void_p, C.c_void_p]
@@ -297,6 +300,28 @@ class Sunset:
         """Host-buffer round trip (7*npfb doubles in and out, pointers to pinned memory)."""
         self._chk(self.L.sunset_run_host(self.h, C.c_void_p(state_in_ptr), float(dt), int(nsteps),
                                          C.c_void_p(state_out_ptr)))
+
+    # ---- adjoint (no reference counterpart) ----
+    def adjoint_run(self, dt, nsteps, checkpoint_every=20, state_gradient=True):
+        """From the current state: J = final kinetic energy after nsteps steps of dt, and
+        (dJ/dWi, dJ/dbeta), and dJ/d(initial state) as a dict of 7 fields (ro rou rov
+        psixx psixy psiyy psizz), or None."""
+        J = C.c_double()
+        dp_ = np.zeros(2)
+        n = self.sizes()[1]
+        ds = np.zeros(7 * n) if state_gradient else None
+        self._chk(self.L.sunset_adjoint_run(self.h, float(dt), int(nsteps), int(checkpoint_every), C.byref(J), dp_,
+                                            ds.ctypes.data if ds is not None else None))
+        grads = None
+        if ds is not None:
+            grads = {k: ds[f * n:(f + 1) * n].copy() for f, k in
+                     enumerate(["ro", "rou", "rov", "psixx", "psixy", "psiyy", "psizz"])}
+        return J.value, (dp_[0], dp_[1]), grads
+
+    def adjoint_apply_D(self, which, gbar):
+        out = np.zeros(self.sizes()[1])
+        self._chk(self.L.sunset_adjoint_apply_D(self.h, int(which), np.ascontiguousarray(gbar, np.float64), out, 0))
+        return out
 
     def time_stage_kernel(self, reps=20):
         """(mean ms per RK stage launch inside `reps` real steps, algorithmic bytes per launch);
