@@ -45,6 +45,11 @@ def parse():
     p.add_argument("--error-steps", type=int, default=100,
                    help="mixed precision: steps from the initial state for the per-field error report")
     p.add_argument("--no-error-check", action="store_true")
+    p.add_argument("--adjoint", action="store_true",
+                   help="time sunset_adjoint_run against the forward run (differentiation workload by default)")
+    p.add_argument("--checkpoint", type=int, default=20, help="--adjoint: checkpoint every N steps")
+    p.add_argument("--fd-check", action="store_true",
+                   help="--adjoint: check dJ/dWi, dJ/dbeta and 8 Gaussian psi0 directions by central differences")
     return p.parse_args()
 
 
@@ -277,11 +282,96 @@ def run_reference(args, ws, rank):
     return 0
 
 
+def run_adjoint(args, local):
+    """Adjoint/forward cost ratio of sunset_adjoint_run (J = final kinetic energy; gradients
+    with respect to Wi, beta and the initial state) and, with --fd-check, its agreement with
+    central finite differences (h = 1e-6) of the forward solver."""
+    import torch
+    from sunset_viscoelastic_b200 import labfm
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload if args.workload != DEFAULT_WORKLOAD else "periodic-lc-o6-262k-adjoint"]
+    ns = wl.nodes()
+    steps = args.steps
+    g = labfm.for_workload(wl, ns, device=local).setup()
+    st = wl.initial(ns)
+    g.set_state(**st)
+    dtc, dtp = g.set_tstep()
+    dt = dt_for(wl, dtc, dtp)
+    nodes = g.sizes()[1]
+    # warm up both paths (graphs, adjoint storage), then time each from the initial state
+    g.step(dt, args.warmup)
+    g.set_state(**st)
+    g.adjoint_run(dt, min(steps, args.checkpoint), args.checkpoint, state_gradient=False)
+    g.set_state(**st)
+    g.synchronize()
+    t = time.perf_counter()
+    g.step(dt, steps)
+    g.synchronize()
+    fwd = time.perf_counter() - t
+    g.set_state(**st)
+    ms_fwd_events = g.step_timed(dt, steps)
+    g.set_state(**st)
+    g.synchronize()
+    t = time.perf_counter()
+    J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, args.checkpoint)
+    adj = time.perf_counter() - t
+    line = {"metric": "adjoint/forward cost", "value": adj / fwd, "unit": "x", "higher_is_better": False,
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic (seeded jittered lattice)",
+            "config": {"workload": wl.name, "nodes": nodes, "order": wl.order, "form": wl.form, "Wi": wl.Wi,
+                       "beta": wl.beta, "checkpoint_every": args.checkpoint,
+                       "objective": "sum 1/2 rho |u|^2 vol after the run"},
+            "forward_s": fwd, "forward_ms_events": ms_fwd_events, "adjoint_s": adj,
+            "J": J, "dJ_dWi": dWi, "dJ_dbeta": dbeta}
+    if args.fd_check:
+        keys = ["ro", "rou", "rov", "psixx", "psixy", "psiyy", "psizz"]
+
+        def fj(state=None, **over):
+            h = labfm.for_workload(wl, ns, device=local, **over).setup() if over else g
+            h.set_state(**st)
+            if state is not None:
+                buf = torch.from_numpy(np.concatenate([state[k] for k in keys])).pin_memory()
+                out = torch.empty_like(buf).pin_memory()
+                h.run_host(buf.data_ptr(), dt, 0, out.data_ptr())
+            h.step(dt, steps)
+            J1 = h.kinetic_energy()
+            if over:
+                h.close()
+            return J1
+        g.set_state(**st)
+        s0 = g.state()
+        base = {k: s0[k] for k in keys}
+        fd = {}
+        for name, ad in (("Wi", dWi), ("beta", dbeta)):
+            p0 = getattr(wl, name)
+            hstep = 1e-6 * p0
+            f = (fj(**{name: p0 + hstep}) - fj(**{name: p0 - hstep})) / (2 * hstep)
+            fd[name] = {"adjoint": ad, "fd": f, "rel": abs(ad - f) / abs(f)}
+        rng = np.random.default_rng(12345)
+        dirs = []
+        for r in range(8):
+            d = {k: rng.standard_normal(nodes) for k in ("psixx", "psixy", "psiyy")}
+            ad = sum(float(grads[k] @ d[k]) for k in d)
+            sp, sm = dict(base), dict(base)
+            for k in d:
+                sp[k] = base[k] + 1e-6 * d[k]
+                sm[k] = base[k] - 1e-6 * d[k]
+            f = (fj(sp) - fj(sm)) / 2e-6
+            dirs.append({"adjoint": ad, "fd": f, "rel": abs(ad - f) / abs(f)})
+        fd["psi0_directions"] = dirs
+        fd["max_rel"] = max([v["rel"] for k, v in fd.items() if k in ("Wi", "beta")] + [d["rel"] for d in dirs])
+        line["fd_check"] = fd
+    print(json.dumps(line), flush=True)
+    g.close()
+    return 0
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    if args.adjoint:
+        return run_adjoint(args, local)
     import torch
     from sunset_viscoelastic_b200 import labfm
     torch.cuda.set_device(local)

@@ -1486,14 +1486,19 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     if (int rc = upload_consts(H)) return rc;
     const int nseg = (nsteps + ckpt - 1) / ckpt;
     // storage: checkpoints (7 conservative fields), the stage inputs of one segment, scratch
-    if (!H->adj_ready || H->adj_ckpt != ckpt || H->adj_nseg < nseg) {
-        if (H->adj_ready) return set_err(H, SUNSET_ERR_ARG, "the adjoint storage of this handle was sized for other step counts");
-        H->adj_ckpt = ckpt;
+    if (H->adj_ready && H->adj_ckpt != ckpt)
+        return set_err(H, SUNSET_ERR_ARG, "checkpoint_every must stay the same for a handle (%d)", H->adj_ckpt);
+    if (H->adj_nseg < nseg) {  // checkpoint store: grows with the number of segments
+        if (H->adj_cp) dfree(H, H->adj_cp);
+        H->adj_cp = nullptr;
+        if (dalloc(H, &H->adj_cp, (size_t)7 * n * nseg)) return SUNSET_ERR_NOMEM;
         H->adj_nseg = nseg;
+    }
+    if (!H->adj_ready) {
+        H->adj_ckpt = ckpt;
         H->adj_store.resize(4 * (size_t)ckpt + 2);
         for (auto &F : H->adj_store)
             if (int rc = alloc_fields(H, F)) return rc;
-        if (dalloc(H, &H->adj_cp, (size_t)7 * n * nseg)) return SUNSET_ERR_NOMEM;
         for (int k = 0; k < kAdjG; k++)
             if (dalloc(H, &H->adj_gb[k], n)) return SUNSET_ERR_NOMEM;
         for (int k = 0; k < kAdjS; k++)

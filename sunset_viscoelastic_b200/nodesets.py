@@ -270,7 +270,7 @@ class Workload:
 
     @property
     def n(self) -> int:
-        return self.nside * self.nside if self.geometry == "periodic" else self.nodes().n
+        return self.nside * self.nside if self.geometry != "cylinder" else self.nodes().n
 
     @property
     def h_over_s(self) -> float:
@@ -282,6 +282,10 @@ class Workload:
             return cylinder_channel()
         return jittered_lattice(self.nside)
 
+    @property
+    def periodic(self) -> bool:
+        return self.geometry != "cylinder"
+
     def params(self) -> dict:
         """Keyword arguments of labfm.Sunset / oracle.Oracle for this workload."""
         return dict(form=self.form, order=self.order, Re=self.Re, Wi=self.Wi, beta=self.beta, epsPTT=self.epsPTT,
@@ -290,6 +294,8 @@ class Workload:
 
     def initial(self, ns: NodeSet) -> dict:
         """Initial state on the reader's node list (FD rows included)."""
+        if self.geometry == "periodic-psi0":
+            return initial_state_psi0(ns)
         if self.geometry == "cylinder":
             x, y, _ = reader_nodes(ns)
             n = len(x)
@@ -318,7 +324,34 @@ WORKLOADS = {
     "periodic-chl-o8-1m": Workload("periodic-chl-o8-1m", 1024, 8, 5.4, "chl", Wi=2.0, beta=0.1, steps=500),
     "cylinder-channel-o8": Workload("cylinder-channel-o8", 0, 8, 0.0, "di", Re=0.01, Wi=0.5, beta=0.59, Ma=0.05,
                                     steps=2000, geometry="cylinder", grav_x=50.0, kolmogorov_forcing=0),
+    # the differentiation configuration: the order-6 set, Oldroyd-B in log-conformation form,
+    # from a non-degenerate log-conformation field (initial_state_psi0)
+    "periodic-lc-o6-262k-adjoint": Workload("periodic-lc-o6-262k-adjoint", 512, 6, 4.2, "lc", Wi=1.0, beta=0.5,
+                                            steps=200, geometry="periodic-psi0"),
 }
+
+
+def psi0_field(x, y):
+    """A smooth, non-degenerate initial log-conformation field psi = log c."""
+    return (0.2 + 0.1 * np.sin(2 * np.pi * x), 0.1 * np.cos(2 * np.pi * y),
+            -0.1 + 0.05 * np.sin(2 * np.pi * (x + y)))
+
+
+def initial_state_psi0(ns: NodeSet):
+    """Taylor-Green velocity, rho = 1, c = exp(psi0) (psi0_field).  At c = I the eigenvalues
+    of psi coincide and the log-conformation right-hand side's omega branch
+    (rhs_lc.F90:465-469) is degenerate, so the differentiation runs start from here."""
+    st = initial_state(ns)
+    a, b, d = psi0_field(ns.x, ns.y)
+    # exp of the symmetric 2x2 matrix [[a, b], [b, d]]
+    m, r = 0.5 * (a + d), np.sqrt(0.25 * (a - d) ** 2 + b * b)
+    e1, e2 = np.exp(m + r), np.exp(m - r)
+    sh = np.where(r > 0, (e1 - e2) / np.where(r > 0, 2 * r, 1.0), e1)
+    ch = 0.5 * (e1 + e2)
+    st["cxx"] = ch + sh * 0.5 * (a - d)
+    st["cyy"] = ch - sh * 0.5 * (a - d)
+    st["cxy"] = sh * b
+    return st
 
 
 def initial_state(ns: NodeSet):
