@@ -301,7 +301,7 @@ def run_adjoint(args, local):
     # warm up both paths (graphs, adjoint storage), then time each from the initial state
     g.step(dt, args.warmup)
     g.set_state(**st)
-    g.adjoint_run(dt, min(steps, args.checkpoint), args.checkpoint, state_gradient=False)
+    g.adjoint_run(dt, steps, args.checkpoint, state_gradient=False)  # sizes the checkpoint store
     g.set_state(**st)
     g.synchronize()
     t = time.perf_counter()
@@ -340,25 +340,41 @@ def run_adjoint(args, local):
         g.set_state(**st)
         s0 = g.state()
         base = {k: s0[k] for k in keys}
-        fd = {}
+        # Central differences at h = 1e-6 (relative for the parameters) and, because J's
+        # rounding (about 1e-16 J per evaluation) divided by 2h is not small against some
+        # directional derivatives, also at h = 1e-4, whose truncation error O(h^2) is far
+        # below that noise.  noise = 2e-16 J / (2h) is the rounding floor of each difference.
+        fd = {"steps": [1e-6, 1e-4]}
         for name, ad in (("Wi", dWi), ("beta", dbeta)):
             p0 = getattr(wl, name)
-            hstep = 1e-6 * p0
-            f = (fj(**{name: p0 + hstep}) - fj(**{name: p0 - hstep})) / (2 * hstep)
-            fd[name] = {"adjoint": ad, "fd": f, "rel": abs(ad - f) / abs(f)}
+            ent = {"adjoint": ad}
+            for hrel in fd["steps"]:
+                hstep = hrel * p0
+                f = (fj(**{name: p0 + hstep}) - fj(**{name: p0 - hstep})) / (2 * hstep)
+                ent[f"fd_h{hrel:g}"] = f
+                ent[f"rel_h{hrel:g}"] = abs(ad - f) / abs(f)
+                ent[f"noise_h{hrel:g}"] = 2e-16 * J / (2 * hstep) / abs(f)
+            fd[name] = ent
         rng = np.random.default_rng(12345)
         dirs = []
         for r in range(8):
             d = {k: rng.standard_normal(nodes) for k in ("psixx", "psixy", "psiyy")}
             ad = sum(float(grads[k] @ d[k]) for k in d)
-            sp, sm = dict(base), dict(base)
-            for k in d:
-                sp[k] = base[k] + 1e-6 * d[k]
-                sm[k] = base[k] - 1e-6 * d[k]
-            f = (fj(sp) - fj(sm)) / 2e-6
-            dirs.append({"adjoint": ad, "fd": f, "rel": abs(ad - f) / abs(f)})
+            ent = {"adjoint": ad}
+            for hstep in fd["steps"]:
+                sp, sm = dict(base), dict(base)
+                for k in d:
+                    sp[k] = base[k] + hstep * d[k]
+                    sm[k] = base[k] - hstep * d[k]
+                f = (fj(sp) - fj(sm)) / (2 * hstep)
+                ent[f"fd_h{hstep:g}"] = f
+                ent[f"rel_h{hstep:g}"] = abs(ad - f) / abs(f)
+                ent[f"noise_h{hstep:g}"] = 2e-16 * J / (2 * hstep) / abs(f)
+            dirs.append(ent)
         fd["psi0_directions"] = dirs
-        fd["max_rel"] = max([v["rel"] for k, v in fd.items() if k in ("Wi", "beta")] + [d["rel"] for d in dirs])
+        ents = [fd["Wi"], fd["beta"]] + dirs
+        for hstep in fd["steps"]:
+            fd[f"max_rel_h{hstep:g}"] = max(e[f"rel_h{hstep:g}"] for e in ents)
         line["fd_check"] = fd
     print(json.dumps(line), flush=True)
     g.close()

@@ -17,6 +17,8 @@
 // reference's link order and reproduce it bit for bit; the step sums in the bank-aware
 // order of stream.cu, which changes only the rounding (and libm's exp, log, cos may differ
 // from glibc in the last bit).
+#include <algorithm>
+#include <thread>
 #include <type_traits>
 
 #include "adjoint.cuh"
@@ -46,6 +48,8 @@ struct StageArgs {
     float *dreg[7], *eacc32[7];  // mixed precision
     DevScalars *sc;
     double *partials;
+    double *gsave;  // log-conformation FP64 stages of the adjoint's recording: the 18 stencil
+                    // sums of each node (adjoint.cuh order, arrays of npfb), else null
     int stage;  // 0..3; 4 = rhs only
 };
 
@@ -380,6 +384,14 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
     if (active) gather_stage<FORM, MD, MX>(A, i, smem, R, g);
     active = active && i < cK.npfb;
     unsigned long long emax_bits = 0;
+    if constexpr (FORM == SUNSET_FORM_LC && !MX) {
+        if (active && A.gsave) {
+            const double gv[kAdjG] = {g.ro_x, g.ro_y, g.u_x, g.u_y, g.lapu, g.v_x, g.v_y, g.lapv, g.cxx_x, g.cxy_x,
+                                      g.cxy_y, g.cyy_y, g.pxx_x, g.pxx_y, g.pxy_x, g.pxy_y, g.pyy_x, g.pyy_y};
+#pragma unroll
+            for (int k = 0; k < kAdjG; k++) A.gsave[(size_t)k * cK.npfb + i] = gv[k];
+        }
+    }
     if (active) {
         const Fields &F = A.in;
         NodeState n;
@@ -1186,181 +1198,357 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
 // fixed order, without atomics), plus its own -sum(w) g_bar_j terms, and the derived fields
 // (u = rho u / rho, c from psi) are reversed into the conservative state.
 //
-// Stage inputs are recomputed per segment of `checkpoint_every` steps from the state stored
-// at the segment's start, and kept (13 fields per stage) for that segment's reverse sweep.
+// Checkpoints: the state every `checkpoint_every` steps.  A segment's forward stages are
+// recorded -- the stage input states (13 fields) and the 18 stencil sums g of every node
+// and stage, written by the stage kernel itself -- while it is recomputed from its
+// checkpoint (the last segment is recorded during the forward run), so the reverse sweep
+// runs no forward gather.  Per step the reverse runs five kernels, each over tiles of 256
+// nodes j with a shared-memory halo of the nodes whose links reach the tile and a cp.async
+// stream of the reverse links (the owners' weights gathered once into that order):
+//   filter:       U4_bar = (filter + mass correction)^T U_bar_{n+1}, then the pointwise
+//                 reverse of stage 3 (S_bar_3, g_bar_3 and the state's own s_bar_3);
+//   stage 3, 2, 1: U_bar_s = transposed stencils of g_bar_s + s_bar_s + the derived
+//                 fields reversed, then the pointwise reverse of stage s - 1;
+//   stage 0:      U_bar_0 (+ S_bar_0), the adjoint of the step's input, and its per-tile
+//                 sums of rho_bar for the next mass-correction reverse.
+// The parameter adjoint accumulates per tile and folds once at the end, so, like the
+// gathers, its result does not depend on scheduling.
 // =======================================================================================
 namespace {
 
+// CSR reverse lists: the single transposed operators and the source of the link stream.
 struct AdjArgs {
     int npfb;
     const long long *rptr;      // reverse links of node j: [rptr[j], rptr[j+1])
     const int *rslot, *rnode;   // SELL slot (reference order) and the node owning it
     const unsigned char *rcode; // bits 0-1: reflection code, bit 2: a small link (stencils of the stage)
     const double *wx, *wy, *wl, *wh;
-    const double *gsx, *gsy, *lsum, *hsum, *vol;
-    double *gb[kAdjG];
-    double *sb[kAdjS];
-    double *ub_in[7], *ub_out[7], *sbar[7];
-    double *tpart;
-    const double *mc_sum, *mc_tv;  // sum of rho_bar and of the volumes (mass correction)
-    double dt, alpha, beta;
-    int first, add_sbar, mcorr;
+    const double *gsx, *gsy, *lsum, *hsum;
 };
 
-__device__ __forceinline__ double sgn_u(int c) { return (c == 1 || c == 3) ? -1.0 : 1.0; }
-__device__ __forceinline__ double sgn_v(int c) { return (c == 2 || c == 3) ? -1.0 : 1.0; }
-__device__ __forceinline__ double sgn_xy(int c) { return (c == 1 || c == 2) ? -1.0 : 1.0; }
+// Kernels of the reverse sweep.
+struct RevArgs {
+    const long long *sptr;      // reverse link streams: slice starts (links)
+    const int *sw, *sws;        // slice widths: all links (filter), small links (stage stencils)
+    const uint16_t *locs, *locf;  // halo position | reflection code << 14: stage, filter order
+    const int *hptr, *halo;     // tile halos of the reverse stream
+    int hmax;
+    const double *wx, *wy, *wl, *wh;  // owners' weights: wx wy wl in the stage order, wh in the filter's
+    const double *tvol;         // filter transpose of the volumes (mass correction)
+    const double *gsx, *gsy, *lsum, *hsum;
+    Fields cur;                 // input state of the stage whose stencils are transposed
+    Fields prev;                // input state of the stage whose pointwise reverse follows
+    const double *gprev;        // that stage's recorded stencil sums (18 arrays of npfb)
+    const double2 *gb_in;       // g_bar of the transposed stage (9 pair arrays of npfb)
+    double2 *gb_out;            // g_bar of the stage whose pointwise reverse follows
+    double *sb[kAdjS];          // the state's own adjoint from the pointwise reverse
+    double *sbar[kAdjS];        // S_bar, the adjoint of the RK register
+    double *ua[kAdjS];          // U_bar of a step's input state
+    double *tacc;               // per-tile sums of the parameter adjoint (Wi, beta)
+    double *rpart;              // per-tile sums of rho_bar of ua
+    const double *tv;           // sum of the volumes
+    double dt, alpha, beta;     // RK coefficients of the stage whose pointwise reverse follows
+    int first;                  // that stage is the log-conformation first step (itime 1, stage 0)
+    int mcorr;
+};
 
-// Stage adjoint, part 1: the stage's stencil sums g at its input state (the forward gather),
-// R_bar and S_bar of each node, and the pointwise reverse: g_bar, the node's direct state
-// adjoint and block sums of the parameter adjoint.
-__global__ void __launch_bounds__(kTile, 2) k_adj_point_lc(StageArgs A, AdjArgs B) {
-    extern __shared__ __align__(16) double smem[];
-    constexpr int NG = ngather(SUNSET_FORM_LC, false);
-    const int i = blockIdx.x * kTile + threadIdx.x;
-    bool active = (i >> 5) < cK.nslices;
-    LinkRing<false, 3, ring_depth(false)> R;
-    R.src[0] = reinterpret_cast<const double2 *>(A.wx);
-    R.src[1] = reinterpret_cast<const double2 *>(A.wy);
-    R.src[2] = reinterpret_cast<const double2 *>(A.wl);
-    R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
-           active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
-    R.prologue();
-    load_halo<NG>(A, smem, [&](int f) { return gather_src<SUNSET_FORM_LC, false>(A.in, f); });
-    Grads g;
-    if (active) gather_stage<SUNSET_FORM_LC, false, false>(A, i, smem, R, g);
-    double t0 = 0.0, t1 = 0.0;
-    if (active && i < B.npfb) {
-        const Fields &F = A.in;
-        const double s[kAdjS] = {F.ro[i], F.rou[i], F.rov[i], F.q[0][i], F.q[1][i], F.q[2][i]};
-        const double gv[kAdjG] = {g.ro_x, g.ro_y, g.u_x, g.u_y, g.lapu, g.v_x, g.v_y, g.lapv, g.cxx_x, g.cxy_x,
-                                  g.cxy_y, g.cyy_y, g.pxx_x, g.pxx_y, g.pxy_x, g.pxy_y, g.pyy_x, g.pyy_y};
-        double rb[kAdjR];
-        for (int f = 0; f < kAdjR; f++) {
-            const double ui = B.ub_in[f][i], si = B.sbar[f][i];
-            rb[f] = B.dt * (B.alpha * ui + B.beta * si);
-            B.sbar[f][i] = ui + si;
-        }
-        double sbv[kAdjS] = {0, 0, 0, 0, 0, 0}, gbv[kAdjG], tb[2] = {0.0, 0.0};
-        for (int k = 0; k < kAdjG; k++) gbv[k] = 0.0;
-        p_adjoint_lc(cK, s, gv, B.first != 0, rb, sbv, gbv, tb);
-        for (int k = 0; k < kAdjG; k++) B.gb[k][i] = gbv[k];
-        for (int k = 0; k < kAdjS; k++) B.sb[k][i] = sbv[k];
-        t0 = tb[0];
-        t1 = tb[1];
-    }
+// g_bar as 9 pair arrays, so the transposed gather reads 16 bytes a load:
+//   0 (ro_x, ro_y)  1 (u_x, u_y)  2 (v_x, v_y)  3 (lap u, lap v)  4 (cxx_x, cyy_y)
+//   5 (cxy_x, cxy_y)  6 (pxx_x, pxx_y)  7 (pxy_x, pxy_y)  8 (pyy_x, pyy_y)
+constexpr int kAdjPairs = 9;
+
+__device__ __forceinline__ void store_gbar(double2 *out, int n, int j, const double *gb) {
+    out[j] = make_double2(gb[G_RO_X], gb[G_RO_Y]);
+    out[(size_t)n + j] = make_double2(gb[G_U_X], gb[G_U_Y]);
+    out[2 * (size_t)n + j] = make_double2(gb[G_V_X], gb[G_V_Y]);
+    out[3 * (size_t)n + j] = make_double2(gb[G_LAPU], gb[G_LAPV]);
+    out[4 * (size_t)n + j] = make_double2(gb[G_CXX_X], gb[G_CYY_Y]);
+    out[5 * (size_t)n + j] = make_double2(gb[G_CXY_X], gb[G_CXY_Y]);
+    out[6 * (size_t)n + j] = make_double2(gb[G_PXX_X], gb[G_PXX_Y]);
+    out[7 * (size_t)n + j] = make_double2(gb[G_PXY_X], gb[G_PXY_Y]);
+    out[8 * (size_t)n + j] = make_double2(gb[G_PYY_X], gb[G_PYY_Y]);
+}
+
+// Sums over the block's threads in a fixed tree (a, b: two sums at once).
+__device__ __forceinline__ void tile_sum2(double &a, double &b) {
     __shared__ double red[2][kTile];
-    red[0][threadIdx.x] = t0;
-    red[1][threadIdx.x] = t1;
+    red[0][threadIdx.x] = a;
+    red[1][threadIdx.x] = b;
     __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    for (int st = kTile / 2; st > 0; st >>= 1) {
         if ((int)threadIdx.x < st) {
             red[0][threadIdx.x] = red[0][threadIdx.x] + red[0][threadIdx.x + st];
             red[1][threadIdx.x] = red[1][threadIdx.x] + red[1][threadIdx.x + st];
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        B.tpart[2 * blockIdx.x] = red[0][0];
-        B.tpart[2 * blockIdx.x + 1] = red[1][0];
-    }
-}
-
-// Stage adjoint, part 2: the transposed stencils and the reverse of the derived fields;
-// writes U_bar of the stage's input state (+ S_bar at the first stage).
-__global__ void __launch_bounds__(128) k_adj_transpose_lc(StageArgs A, AdjArgs B) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= B.npfb) return;
-    double ph[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // rho, u, v, cxx, cxy, cyy, psixx, psixy, psiyy
-    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) {
-        const int code = B.rcode[e];
-        if (!(code & 4)) continue;
-        const int o = B.rslot[e], i = B.rnode[e], rc = code & 3;
-        const double wx = B.wx[o], wy = B.wy[o], wl = B.wl[o];
-        ph[0] += wx * B.gb[G_RO_X][i] + wy * B.gb[G_RO_Y][i];
-        ph[1] += sgn_u(rc) * (wx * B.gb[G_U_X][i] + wy * B.gb[G_U_Y][i] + wl * B.gb[G_LAPU][i]);
-        ph[2] += sgn_v(rc) * (wx * B.gb[G_V_X][i] + wy * B.gb[G_V_Y][i] + wl * B.gb[G_LAPV][i]);
-        ph[3] += wx * B.gb[G_CXX_X][i];
-        ph[4] += sgn_xy(rc) * (wx * B.gb[G_CXY_X][i] + wy * B.gb[G_CXY_Y][i]);
-        ph[5] += wy * B.gb[G_CYY_Y][i];
-        ph[6] += wx * B.gb[G_PXX_X][i] + wy * B.gb[G_PXX_Y][i];
-        ph[7] += sgn_xy(rc) * (wx * B.gb[G_PXY_X][i] + wy * B.gb[G_PXY_Y][i]);
-        ph[8] += wx * B.gb[G_PYY_X][i] + wy * B.gb[G_PYY_Y][i];
-    }
-    const double gx = B.gsx[j], gy = B.gsy[j], ls = B.lsum[j];
-    ph[0] -= gx * B.gb[G_RO_X][j] + gy * B.gb[G_RO_Y][j];
-    ph[1] -= gx * B.gb[G_U_X][j] + gy * B.gb[G_U_Y][j] + ls * B.gb[G_LAPU][j];
-    ph[2] -= gx * B.gb[G_V_X][j] + gy * B.gb[G_V_Y][j] + ls * B.gb[G_LAPV][j];
-    ph[3] -= gx * B.gb[G_CXX_X][j];
-    ph[4] -= gx * B.gb[G_CXY_X][j] + gy * B.gb[G_CXY_Y][j];
-    ph[5] -= gy * B.gb[G_CYY_Y][j];
-    ph[6] -= gx * B.gb[G_PXX_X][j] + gy * B.gb[G_PXX_Y][j];
-    ph[7] -= gx * B.gb[G_PXY_X][j] + gy * B.gb[G_PXY_Y][j];
-    ph[8] -= gx * B.gb[G_PYY_X][j] + gy * B.gb[G_PYY_Y][j];
-    const Fields &F = A.in;
-    const double ooro = 1.0 / F.ro[j];
-    const double u = F.rou[j] * ooro, v = F.rov[j] * ooro;
-    double pb[3] = {0.0, 0.0, 0.0};
-    const double cb[3] = {ph[3], ph[4], ph[5]};
-    lc_c_from_psi_adj(F.q[0][j], F.q[1][j], F.q[2][j], cb, pb);
-    double U[7];
-    U[0] = B.sb[0][j] + ph[0] - (ph[1] * u + ph[2] * v) * ooro;
-    U[1] = B.sb[1][j] + ph[1] * ooro;
-    U[2] = B.sb[2][j] + ph[2] * ooro;
-    U[3] = B.sb[3][j] + ph[6] + pb[0];
-    U[4] = B.sb[4][j] + ph[7] + pb[1];
-    U[5] = B.sb[5][j] + ph[8] + pb[2];
-    U[6] = 0.0;
-    for (int f = 0; f < 7; f++) B.ub_out[f][j] = B.add_sbar ? U[f] + B.sbar[f][j] : U[f];
-}
-
-// Filter and mass correction reversed (rhs_lc.F90:818-893): U4_bar_j = Uf_bar_j (1 - hsum_j)
-// + sum over reverse links w_h Uf_bar_i, with Uf_bar = U_bar and, for rho,
-// rho_f_bar_i = rho_bar_i - vol_i sum(rho_bar) / sum(vol) when the mass is corrected.
-__global__ void __launch_bounds__(128) k_adj_filter_lc(AdjArgs B) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= B.npfb) return;
-    const double mc = B.mcorr ? *B.mc_sum / *B.mc_tv : 0.0;
-    auto uf = [&](int f, int i) { return f == 0 ? B.ub_in[0][i] - B.vol[i] * mc : B.ub_in[f][i]; };
-    double acc[6];
-    const double own = 1.0 - B.hsum[j];
-    for (int f = 0; f < 6; f++) acc[f] = uf(f, j) * own;
-    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) {
-        const int o = B.rslot[e], i = B.rnode[e], rc = B.rcode[e] & 3;
-        const double w = B.wh[o];
-        acc[0] += w * uf(0, i);
-        acc[1] += w * sgn_u(rc) * uf(1, i);
-        acc[2] += w * sgn_v(rc) * uf(2, i);
-        acc[3] += w * uf(3, i);
-        acc[4] += w * sgn_xy(rc) * uf(4, i);
-        acc[5] += w * uf(5, i);
-    }
-    for (int f = 0; f < 6; f++) B.ub_out[f][j] = acc[f];
-    B.ub_out[6][j] = 0.0;
-}
-
-// Adjoint of J = sum 1/2 rho |u|^2 vol at the final state.
-__global__ void k_adj_objective(int npfb, Fields F, const double *vol, AdjArgs B) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npfb) return;
-    const double u = F.u[i], v = F.v[i], w = vol[i];
-    B.ub_out[0][i] = -0.5 * (u * u + v * v) * w;
-    B.ub_out[1][i] = u * w;
-    B.ub_out[2][i] = v * w;
-    for (int f = 3; f < 7; f++) B.ub_out[f][i] = 0.0;
-}
-
-// Sum of rho_bar (block partials) for the mass correction's adjoint.
-__global__ void k_adj_sum(int npfb, const double *x, double *partials) {
-    __shared__ double sm[128];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    sm[threadIdx.x] = i < npfb ? x[i] : 0.0;
+    a = red[0][0];
+    b = red[1][0];
     __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + st];
-        __syncthreads();
+}
+
+// Pointwise reverse of a stage at node j, given U_bar of its output ub: R_bar = dt (alpha
+// U_bar + beta S_bar), S_bar <- U_bar + S_bar (sbar_zero: S_bar of the output is zero), then
+// adjoint.cuh's reverse of the right-hand side at the recorded state and stencil sums.
+__device__ __forceinline__ void point_reverse(const RevArgs &B, int j, const double *ub, bool sbar_zero, double &t0,
+                                              double &t1) {
+    const int n = cK.npfb;
+    double rb[kAdjR];
+#pragma unroll
+    for (int f = 0; f < kAdjR; f++) {
+        const double si = sbar_zero ? 0.0 : B.sbar[f][j];
+        rb[f] = B.dt * (B.alpha * ub[f] + B.beta * si);
+        B.sbar[f][j] = ub[f] + si;
     }
-    if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+    const Fields &P = B.prev;
+    const double s[kAdjS] = {P.ro[j], P.rou[j], P.rov[j], P.q[0][j], P.q[1][j], P.q[2][j]};
+    double g[kAdjG], gbv[kAdjG], sbv[kAdjS] = {0, 0, 0, 0, 0, 0}, tb[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < kAdjG; k++) {
+        g[k] = B.gprev[(size_t)k * n + j];
+        gbv[k] = 0.0;
+    }
+    p_adjoint_lc(cK, s, g, B.first != 0, rb, sbv, gbv, tb);
+    store_gbar(B.gb_out, n, j, gbv);
+#pragma unroll
+    for (int k = 0; k < kAdjS; k++) B.sb[k][j] = sbv[k];
+    t0 += tb[0];
+    t1 += tb[1];
+}
+
+// Stage a tile's reverse halo: NA arrays of T per node (T = double2: the g_bar pairs).
+template <int NA, typename T, typename SRC>
+__device__ __forceinline__ void load_rev_halo(const RevArgs &B, T *sm, SRC src) {
+    const int hb = B.hptr[blockIdx.x], hn = B.hptr[blockIdx.x + 1] - hb;
+    const int hm = B.hmax;
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        const int node = __ldg(B.halo + hb + h);
+#pragma unroll
+        for (int a = 0; a < NA; a++) cp_async<sizeof(T)>(&sm[a * hm + h], src(a) + node);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+__host__ __device__ constexpr size_t rev_stage_smem(int hmax) {
+    return (size_t)2 * kAdjPairs * hmax * sizeof(double) + LinkRing<false, 3, ring_depth(false)>::bytes();
+}
+__host__ __device__ inline size_t rev_filter_smem(int hmax) {
+    return halo_doubles(kAdjS, hmax) * sizeof(double) + LinkRing<false, 1, ring_depth(false)>::bytes();
+}
+
+// Reverse of the filter and the mass correction (rhs_lc.F90:818-893), fused with the
+// pointwise reverse of stage 3.  The filter's output is Uf_j = U4_j (1 - hsum_j) + sum_k
+// w_jk U4_k; the mass correction subtracts vol_i (sum_k rho_f,k vol_k - M) / sum(vol) from
+// rho, so rho_f_bar_i = rho_bar_i - vol_i sum(rho_bar) / sum(vol), and
+// U4_bar_j = Uf_bar_j (1 - hsum_j) + sum over reverse links w_ij Uf_bar_i, whose rho part
+// is (filter^T rho_bar)_j - tvol_j sum(rho_bar) / sum(vol).
+__global__ void __launch_bounds__(kTile, 2) k_adj_filter_lc(RevArgs B) {
+    extern __shared__ __align__(16) double smem[];
+    const int n = cK.npfb;
+    const int j = blockIdx.x * kTile + threadIdx.x;
+    const bool in_slice = (j >> 5) < cK.nslices;
+    LinkRing<false, 1, ring_depth(false)> R;
+    R.src[0] = reinterpret_cast<const double2 *>(B.wh);
+    R.init(smem + halo_doubles(kAdjS, B.hmax), reinterpret_cast<const unsigned *>(B.locf),
+           in_slice ? (B.sptr[j >> 5] >> 1) + (j & 31) : 0, in_slice ? B.sw[j >> 5] >> 1 : 0);
+    R.prologue();
+    load_rev_halo<kAdjS>(B, smem, [&](int f) { return (const double *)B.ua[f]; });
+    // sum of rho_bar over all tiles, in the same order in every block
+    double rs = 0.0, dummy = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kTile) rs = rs + B.rpart[b];
+    tile_sum2(rs, dummy);
+    const double mc = B.mcorr ? rs / *B.tv : 0.0;
+    const int hm = B.hmax;
+    const bool mir = cK.has_mirrors;
+    double acc[kAdjS] = {0, 0, 0, 0, 0, 0};
+    auto link = [&](int lk, double w) {
+        const int h = lk & kLocMask;
+        double a1 = smem[hm + h], a2 = smem[2 * hm + h], a4 = smem[4 * hm + h];
+        if (mir) {
+            const int code = lk >> 14;
+            if (code == 1 || code == 3) a1 = -a1;
+            if (code == 2 || code == 3) a2 = -a2;
+            if (code == 1 || code == 2) a4 = -a4;
+        }
+        acc[0] = __fma_rn(w, smem[h], acc[0]);
+        acc[1] = __fma_rn(w, a1, acc[1]);
+        acc[2] = __fma_rn(w, a2, acc[2]);
+        acc[3] = __fma_rn(w, smem[3 * hm + h], acc[3]);
+        acc[4] = __fma_rn(w, a4, acc[4]);
+        acc[5] = __fma_rn(w, smem[5 * hm + h], acc[5]);
+    };
+    for (int m = 0; m < R.npair; m++) {
+        R.next(m);
+        double w0, w1;
+        R.weights(m, 0, w0, w1);
+        const unsigned l2 = R.index(m);
+        link((int)(l2 & 0xffffu), w0);
+        link((int)(l2 >> 16), w1);
+    }
+    double t0 = 0.0, t1 = 0.0;
+    if (in_slice && j < n) {
+        const double own = 1.0 - B.hsum[j];
+#pragma unroll
+        for (int f = 0; f < kAdjS; f++) acc[f] = __fma_rn(own, B.ua[f][j], acc[f]);
+        acc[0] = acc[0] - mc * B.tvol[j];
+        point_reverse(B, j, acc, true, t0, t1);
+    }
+    tile_sum2(t0, t1);
+    if (threadIdx.x == 0) {
+        B.tacc[2 * blockIdx.x] += t0;
+        B.tacc[2 * blockIdx.x + 1] += t1;
+    }
+}
+
+// Transposed stencils of stage s (the small links): node j collects w_ij g_bar_i from the
+// owners i of its reverse links and -sum_k w_jk g_bar_j from its own, then reverses the
+// derived fields (u = rho u / rho, v, c from psi) into the conservative state:
+// U_bar_s = s_bar_s + that.  FUSE: the pointwise reverse of stage s - 1 follows (s > 0);
+// otherwise (s = 0) U_bar_0 + S_bar_0 is the adjoint of the step's input.
+template <bool FUSE>
+__global__ void __launch_bounds__(kTile, 2) k_adj_stage_lc(RevArgs B) {
+    extern __shared__ __align__(16) double smem[];
+    const int n = cK.npfb;
+    const int j = blockIdx.x * kTile + threadIdx.x;
+    const bool in_slice = (j >> 5) < cK.nslices;
+    double2 *sm = reinterpret_cast<double2 *>(smem);
+    LinkRing<false, 3, ring_depth(false)> R;
+    R.src[0] = reinterpret_cast<const double2 *>(B.wx);
+    R.src[1] = reinterpret_cast<const double2 *>(B.wy);
+    R.src[2] = reinterpret_cast<const double2 *>(B.wl);
+    R.init(smem + 2 * (size_t)kAdjPairs * B.hmax, reinterpret_cast<const unsigned *>(B.locs),
+           in_slice ? (B.sptr[j >> 5] >> 1) + (j & 31) : 0, in_slice ? B.sws[j >> 5] >> 1 : 0);
+    R.prologue();
+    load_rev_halo<kAdjPairs>(B, sm, [&](int p) { return B.gb_in + (size_t)p * n; });
+    const int hm = B.hmax;
+    const bool mir = cK.has_mirrors;
+    // rho, u, v, cxx, cxy, cyy, psixx, psixy, psiyy
+    double ph0 = 0, ph1 = 0, ph2 = 0, ph3 = 0, ph4 = 0, ph5 = 0, ph6 = 0, ph7 = 0, ph8 = 0;
+    auto link = [&](int lk, double wx, double wy, double wl) {
+        const int h = lk & kLocMask;
+        const double2 a = sm[h], gu = sm[hm + h], gv = sm[2 * hm + h], lp = sm[3 * hm + h], c1 = sm[4 * hm + h];
+        const double2 c2 = sm[5 * hm + h], p0 = sm[6 * hm + h], p1 = sm[7 * hm + h], p2 = sm[8 * hm + h];
+        double tu = __fma_rn(wx, gu.x, __fma_rn(wy, gu.y, wl * lp.x));
+        double tv = __fma_rn(wx, gv.x, __fma_rn(wy, gv.y, wl * lp.y));
+        double txy = __fma_rn(wx, c2.x, wy * c2.y);
+        double tpxy = __fma_rn(wx, p1.x, wy * p1.y);
+        if (mir) {
+            const int code = lk >> 14;
+            if (code == 1 || code == 3) tu = -tu;
+            if (code == 2 || code == 3) tv = -tv;
+            if (code == 1 || code == 2) { txy = -txy; tpxy = -tpxy; }
+        }
+        ph0 = __fma_rn(wx, a.x, __fma_rn(wy, a.y, ph0));
+        ph1 = ph1 + tu;
+        ph2 = ph2 + tv;
+        ph3 = __fma_rn(wx, c1.x, ph3);
+        ph4 = ph4 + txy;
+        ph5 = __fma_rn(wy, c1.y, ph5);
+        ph6 = __fma_rn(wx, p0.x, __fma_rn(wy, p0.y, ph6));
+        ph7 = ph7 + tpxy;
+        ph8 = __fma_rn(wx, p2.x, __fma_rn(wy, p2.y, ph8));
+    };
+    for (int m = 0; m < R.npair; m++) {
+        R.next(m);
+        double wx0, wx1, wy0, wy1, wl0, wl1;
+        R.weights(m, 0, wx0, wx1);
+        R.weights(m, 1, wy0, wy1);
+        R.weights(m, 2, wl0, wl1);
+        const unsigned l2 = R.index(m);
+        link((int)(l2 & 0xffffu), wx0, wy0, wl0);
+        link((int)(l2 >> 16), wx1, wy1, wl1);
+    }
+    double t0 = 0.0, t1 = 0.0;
+    if (in_slice && j < n) {
+        const double gx = B.gsx[j], gy = B.gsy[j], ls = B.lsum[j];
+        const double2 *G = B.gb_in;
+        const double2 a = G[j], gu = G[(size_t)n + j], gv = G[2 * (size_t)n + j], lp = G[3 * (size_t)n + j];
+        const double2 c1 = G[4 * (size_t)n + j], c2 = G[5 * (size_t)n + j], p0 = G[6 * (size_t)n + j];
+        const double2 p1 = G[7 * (size_t)n + j], p2 = G[8 * (size_t)n + j];
+        ph0 = ph0 - __fma_rn(gx, a.x, gy * a.y);
+        ph1 = ph1 - __fma_rn(gx, gu.x, __fma_rn(gy, gu.y, ls * lp.x));
+        ph2 = ph2 - __fma_rn(gx, gv.x, __fma_rn(gy, gv.y, ls * lp.y));
+        ph3 = ph3 - gx * c1.x;
+        ph4 = ph4 - __fma_rn(gx, c2.x, gy * c2.y);
+        ph5 = ph5 - gy * c1.y;
+        ph6 = ph6 - __fma_rn(gx, p0.x, gy * p0.y);
+        ph7 = ph7 - __fma_rn(gx, p1.x, gy * p1.y);
+        ph8 = ph8 - __fma_rn(gx, p2.x, gy * p2.y);
+        const Fields &F = B.cur;
+        const double ooro = 1.0 / F.ro[j];
+        const double u = F.rou[j] * ooro, v = F.rov[j] * ooro;
+        double pb[3] = {0.0, 0.0, 0.0};
+        const double cb[3] = {ph3, ph4, ph5};
+        lc_c_from_psi_adj(F.q[0][j], F.q[1][j], F.q[2][j], cb, pb);
+        double U[kAdjS];
+        U[0] = B.sb[0][j] + ph0 - (ph1 * u + ph2 * v) * ooro;
+        U[1] = B.sb[1][j] + ph1 * ooro;
+        U[2] = B.sb[2][j] + ph2 * ooro;
+        U[3] = B.sb[3][j] + ph6 + pb[0];
+        U[4] = B.sb[4][j] + ph7 + pb[1];
+        U[5] = B.sb[5][j] + ph8 + pb[2];
+        if constexpr (FUSE) {
+            point_reverse(B, j, U, false, t0, t1);
+        } else {
+#pragma unroll
+            for (int f = 0; f < kAdjS; f++) {
+                const double x = U[f] + B.sbar[f][j];
+                B.ua[f][j] = x;
+                if (f == 0) t0 = x;
+            }
+        }
+    }
+    tile_sum2(t0, t1);
+    if (threadIdx.x == 0) {
+        if constexpr (FUSE) {
+            B.tacc[2 * blockIdx.x] += t0;
+            B.tacc[2 * blockIdx.x + 1] += t1;
+        } else {
+            B.rpart[blockIdx.x] = t0;
+        }
+    }
+}
+
+// Adjoint of J = sum 1/2 rho |u|^2 vol at the final state, and its per-tile sums of rho_bar.
+__global__ void __launch_bounds__(kTile) k_adj_objective(Fields F, const double *vol, RevArgs B) {
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    double r = 0.0, dummy = 0.0;
+    if (i < cK.npfb) {
+        const double u = F.u[i], v = F.v[i], w = vol[i];
+        r = -0.5 * (u * u + v * v) * w;
+        B.ua[0][i] = r;
+        B.ua[1][i] = u * w;
+        B.ua[2][i] = v * w;
+        for (int f = 3; f < kAdjS; f++) B.ua[f][i] = 0.0;
+    }
+    tile_sum2(r, dummy);
+    if (threadIdx.x == 0) B.rpart[blockIdx.x] = r;
+}
+
+// The filter's transpose applied to the volumes: tvol_j = vol_j (1 - hsum_j) + sum over
+// reverse links w_ij vol_i.
+__global__ void k_adj_tvol(AdjArgs B, const double *vol, double *tvol) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= B.npfb) return;
+    double acc = vol[j] * (1.0 - B.hsum[j]);
+    for (long long e = B.rptr[j]; e < B.rptr[j + 1]; e++) acc += B.wh[B.rslot[e]] * vol[B.rnode[e]];
+    tvol[j] = acc;
+}
+
+// The reverse streams' weights: the owner's weights at its forward SELL slot (-1: padding,
+// weight 0), wx wy wl in the stage order, wh in the filter's.
+__global__ void k_adj_stream_weights(long long L, const int *slot_s, const int *slot_f, const double *wx,
+                                     const double *wy, const double *wl, const double *wh, double *ox,
+                                     double *oy, double *ol, double *oh) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= L) return;
+    const int s = slot_s[e], f = slot_f[e];
+    ox[e] = s < 0 ? 0.0 : wx[s];
+    oy[e] = s < 0 ? 0.0 : wy[s];
+    ol[e] = s < 0 ? 0.0 : wl[s];
+    oh[e] = f < 0 ? 0.0 : wh[f];
 }
 
 // acc[c] += sum_b partials[stride b + c] (c < stride), in block order.
@@ -1448,11 +1636,164 @@ static AdjArgs adj_args(Handle *H) {
     B.npfb = H->npfb;
     B.rptr = H->rptr; B.rslot = H->rslot; B.rnode = H->rnode; B.rcode = H->rcode;
     B.wx = H->wx; B.wy = H->wy; B.wl = H->wl; B.wh = H->wh;
-    B.gsx = H->gsx; B.gsy = H->gsy; B.lsum = H->lsum; B.hsum = H->hsum; B.vol = H->vol;
-    for (int k = 0; k < kAdjG; k++) B.gb[k] = H->adj_gb[k];
-    for (int k = 0; k < kAdjS; k++) B.sb[k] = H->adj_sb[k];
-    for (int f = 0; f < 7; f++) B.sbar[f] = H->adj_sbar[f];
-    B.tpart = H->adj_tpart;
+    B.gsx = H->gsx; B.gsy = H->gsy; B.lsum = H->lsum; B.hsum = H->hsum;
+    return B;
+}
+
+// The reverse link streams (host build from the CSR lists): node j's reverse links in sliced
+// ELL over the forward's slices, tiles of kTileSlices slices with the sorted set of owners
+// as their halo.  Two orders of the links, each dealt slot by slot so that the lanes reading
+// the halo together meet distinct shared-memory banks (deal_slice_by_bank): the small links
+// for the stage kernel's 16-byte loads (groups of 8 lanes), all links for the filter's
+// 8-byte loads (groups of 16).  Then the owners' weights are gathered into those orders on
+// the device, and the filter transpose of the volumes is formed.
+static int adjoint_build_stream(Handle *H) {
+    if (H->rv_sptr) return 0;
+    const int n = H->npfb, nsl = H->nslices;
+    std::vector<long long> rptr(n + 1);
+    SUNSET_CUDA(H, cudaMemcpy(rptr.data(), H->rptr, (n + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    const long long ne = rptr[n];
+    std::vector<int> rslot(ne), rnode(ne);
+    std::vector<unsigned char> rcode(ne);
+    SUNSET_CUDA(H, cudaMemcpy(rslot.data(), H->rslot, ne * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(rnode.data(), H->rnode, ne * sizeof(int), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(rcode.data(), H->rcode, ne * sizeof(unsigned char), cudaMemcpyDeviceToHost));
+    std::vector<long long> sptr(nsl + 1, 0);
+    std::vector<int> sw(nsl), sws(nsl);
+    for (int sl = 0; sl < nsl; sl++) {
+        int w = 0, ws = 0;
+        for (int j = sl * kSlice; j < std::min(n, (sl + 1) * kSlice); j++) {
+            int c = 0;
+            for (long long e = rptr[j]; e < rptr[j + 1]; e++) c += (rcode[e] & 4) ? 1 : 0;
+            w = std::max(w, (int)(rptr[j + 1] - rptr[j]));
+            ws = std::max(ws, c);
+        }
+        sw[sl] = (w + 1) & ~1;
+        sws[sl] = (ws + 1) & ~1;
+        sptr[sl + 1] = sptr[sl] + (long long)sw[sl] * kSlice;
+    }
+    const long long L = sptr[nsl];
+    if (ne >= 0x7fffffffLL) return set_err(H, SUNSET_ERR_SCOPE, "too many links for the reverse stream");
+    const int nt = (nsl + kTileSlices - 1) / kTileSlices;
+    std::vector<int> slot_s(L, -1), slot_f(L, -1);
+    std::vector<uint16_t> loc_s(L, 0), loc_f(L, 0), pos(ne);
+    std::vector<std::vector<int>> halos(nt);
+    unsigned nthr = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < nthr; w++) {
+        pool.emplace_back([&, w]() {
+            std::vector<int> small[kSlice], large[kSlice], chosen;
+            for (int t = (int)w; t < nt; t += (int)nthr) {
+                std::vector<int> &hv = halos[t];
+                const int j0 = t * kTileSlices * kSlice, j1 = std::min(n, (t + 1) * kTileSlices * kSlice);
+                for (int j = j0; j < j1; j++)
+                    for (long long e = rptr[j]; e < rptr[j + 1]; e++) hv.push_back(rnode[e]);
+                std::sort(hv.begin(), hv.end());
+                hv.erase(std::unique(hv.begin(), hv.end()), hv.end());
+                for (int j = j0; j < j1; j++)
+                    for (long long e = rptr[j]; e < rptr[j + 1]; e++) {
+                        const int p = (int)(std::lower_bound(hv.begin(), hv.end(), rnode[e]) - hv.begin());
+                        pos[e] = (uint16_t)((p & kLocMask) | ((rcode[e] & 3) << 14));
+                    }
+                for (int sl = t * kTileSlices; sl < std::min(nsl, (t + 1) * kTileSlices); sl++) {
+                    int c[kSlice], c_s[kSlice];
+                    // stage order: the small links
+                    for (int lane = 0; lane < kSlice; lane++) {
+                        const int j = sl * kSlice + lane;
+                        small[lane].clear();
+                        large[lane].clear();
+                        if (j < n)
+                            for (long long e = rptr[j]; e < rptr[j + 1]; e++)
+                                if (rcode[e] & 4) small[lane].push_back((int)e);
+                        c[lane] = c_s[lane] = (int)small[lane].size();
+                    }
+                    chosen.assign((size_t)sws[sl] * kSlice, -1);
+                    deal_slice_by_bank(8, pos.data(), small, large, c_s, c, sws[sl], chosen.data());
+                    for (int k = 0; k < sws[sl]; k++)
+                        for (int lane = 0; lane < kSlice; lane++) {
+                            const int e = chosen[k * kSlice + lane];
+                            if (e < 0) continue;
+                            const long long o = sell_at(sptr[sl], k, lane);
+                            slot_s[o] = rslot[e];
+                            loc_s[o] = pos[e];
+                        }
+                    // filter order: all links
+                    for (int lane = 0; lane < kSlice; lane++) {
+                        const int j = sl * kSlice + lane;
+                        small[lane].clear();
+                        if (j < n)
+                            for (long long e = rptr[j]; e < rptr[j + 1]; e++) small[lane].push_back((int)e);
+                        c[lane] = c_s[lane] = (int)small[lane].size();
+                    }
+                    chosen.assign((size_t)sw[sl] * kSlice, -1);
+                    deal_slice_by_bank(16, pos.data(), small, large, c_s, c, sw[sl], chosen.data());
+                    for (int k = 0; k < sw[sl]; k++)
+                        for (int lane = 0; lane < kSlice; lane++) {
+                            const int e = chosen[k * kSlice + lane];
+                            if (e < 0) continue;
+                            const long long o = sell_at(sptr[sl], k, lane);
+                            slot_f[o] = rslot[e];
+                            loc_f[o] = pos[e];
+                        }
+                }
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
+    std::vector<int> hptr(nt + 1, 0);
+    int hmax = 0;
+    for (int t = 0; t < nt; t++) {
+        hptr[t + 1] = hptr[t] + (int)halos[t].size();
+        hmax = std::max(hmax, (int)halos[t].size());
+    }
+    if (hmax > kLocMask + 1)
+        return set_err(H, SUNSET_ERR_SCOPE, "reverse tile halo of %d nodes exceeds the 14-bit local index", hmax);
+    std::vector<int> hall(std::max(1, hptr[nt]));
+    for (int t = 0; t < nt; t++) std::copy(halos[t].begin(), halos[t].end(), hall.begin() + hptr[t]);
+    int *dslot = nullptr;
+    const size_t Lz = L ? (size_t)L : 1;
+    if (dalloc(H, &H->rv_sptr, nsl + 1) || dalloc(H, &H->rv_sw, nsl) || dalloc(H, &H->rv_sws, nsl) ||
+        dalloc(H, &H->rv_loc_s, Lz) || dalloc(H, &H->rv_loc_f, Lz) || dalloc(H, &H->rv_hptr, nt + 1) ||
+        dalloc(H, &H->rv_halo, hall.size()) || dalloc(H, &H->rv_wx, Lz) || dalloc(H, &H->rv_wy, Lz) ||
+        dalloc(H, &H->rv_wl, Lz) || dalloc(H, &H->rv_wh, Lz) || dalloc(H, &H->rv_tvol, n) || dalloc(H, &dslot, 2 * Lz))
+        return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_sptr, sptr.data(), (nsl + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_sw, sw.data(), nsl * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_sws, sws.data(), nsl * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_loc_s, loc_s.data(), L * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_loc_f, loc_f.data(), L * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_hptr, hptr.data(), (nt + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->rv_halo, hall.data(), hall.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(dslot, slot_s.data(), L * sizeof(int), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(dslot + Lz, slot_f.data(), L * sizeof(int), cudaMemcpyHostToDevice));
+    H->rv_hmax = hmax;
+    if (L)
+        k_adj_stream_weights<<<(unsigned)((L + 255) / 256), 256, 0, H->stream>>>(
+            L, dslot, dslot + Lz, H->wx, H->wy, H->wl, H->wh, H->rv_wx, H->rv_wy, H->rv_wl, H->rv_wh);
+    AdjArgs A = adj_args(H);
+    k_adj_tvol<<<(n + 127) / 128, 128, 0, H->stream>>>(A, H->vol, H->rv_tvol);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    dfree(H, dslot);
+    return 0;
+}
+
+static RevArgs rev_args(Handle *H) {
+    RevArgs B{};
+    B.sptr = H->rv_sptr; B.sw = H->rv_sw; B.sws = H->rv_sws;
+    B.locs = H->rv_loc_s; B.locf = H->rv_loc_f;
+    B.hptr = H->rv_hptr; B.halo = H->rv_halo; B.hmax = H->rv_hmax;
+    B.wx = H->rv_wx; B.wy = H->rv_wy; B.wl = H->rv_wl; B.wh = H->rv_wh; B.tvol = H->rv_tvol;
+    B.gsx = H->gsx; B.gsy = H->gsy; B.lsum = H->lsum; B.hsum = H->hsum;
+    for (int k = 0; k < kAdjS; k++) {
+        B.sb[k] = H->adj_sb[k];
+        B.sbar[k] = H->adj_sbar[k];
+        B.ua[k] = H->adj_ua[k];
+    }
+    B.tacc = H->adj_tacc;
+    B.rpart = H->adj_rpart;
+    B.tv = &H->dsc->tv;
+    B.mcorr = H->cfg.mcorr;
     return B;
 }
 
@@ -1483,9 +1824,13 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     const int n = H->npfb;
     cudaStream_t st = H->stream;
     if (int rc = adjoint_build_reverse(H)) return rc;
+    if (int rc = adjoint_build_stream(H)) return rc;
     if (int rc = upload_consts(H)) return rc;
     const int nseg = (nsteps + ckpt - 1) / ckpt;
-    // storage: checkpoints (7 conservative fields), the stage inputs of one segment, scratch
+    const size_t smem_stage = rev_stage_smem(H->rv_hmax), smem_filter = rev_filter_smem(H->rv_hmax);
+    if (smem_stage > kMaxStageSmem || smem_filter > kMaxStageSmem)
+        return set_err(H, SUNSET_ERR_SCOPE, "reverse tile halo too large for shared memory");
+    // storage: checkpoints (7 conservative fields), the recorded stages of one segment, scratch
     if (H->adj_ready && H->adj_ckpt != ckpt)
         return set_err(H, SUNSET_ERR_ARG, "checkpoint_every must stay the same for a handle (%d)", H->adj_ckpt);
     if (H->adj_nseg < nseg) {  // checkpoint store: grows with the number of segments
@@ -1499,24 +1844,52 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
         H->adj_store.resize(4 * (size_t)ckpt + 2);
         for (auto &F : H->adj_store)
             if (int rc = alloc_fields(H, F)) return rc;
-        for (int k = 0; k < kAdjG; k++)
-            if (dalloc(H, &H->adj_gb[k], n)) return SUNSET_ERR_NOMEM;
+        if (dalloc(H, &H->adj_g, (size_t)4 * ckpt * kAdjG * n) || dalloc(H, &H->adj_gp[0], (size_t)2 * kAdjPairs * n) ||
+            dalloc(H, &H->adj_gp[1], (size_t)2 * kAdjPairs * n))
+            return SUNSET_ERR_NOMEM;
         for (int k = 0; k < kAdjS; k++)
-            if (dalloc(H, &H->adj_sb[k], n)) return SUNSET_ERR_NOMEM;
+            if (dalloc(H, &H->adj_sb[k], n) || dalloc(H, &H->adj_sbar[k], n)) return SUNSET_ERR_NOMEM;
         for (int f = 0; f < 7; f++)
-            if (dalloc(H, &H->adj_sbar[f], n) || dalloc(H, &H->adj_ua[f], n) || dalloc(H, &H->adj_ub[f], n))
-                return SUNSET_ERR_NOMEM;
-        if (dalloc(H, &H->adj_tpart, 2 * (size_t)H->ntiles + 2 * (size_t)((n + 127) / 128) + 8) ||
+            if (dalloc(H, &H->adj_ua[f], n)) return SUNSET_ERR_NOMEM;
+        if (dalloc(H, &H->adj_tacc, 2 * (size_t)H->ntiles) || dalloc(H, &H->adj_rpart, (size_t)H->ntiles) ||
             dalloc(H, &H->adj_acc, 4))
             return SUNSET_ERR_NOMEM;
+        SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_stage_lc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
+        SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_stage_lc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
+        SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_filter_lc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
         H->adj_ready = true;
-        SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_point_lc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
     }
     DevScalars sc0;
     SUNSET_CUDA(H, cudaMemcpyAsync(&sc0, H->dsc, sizeof(sc0), cudaMemcpyDeviceToHost, st));
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
     SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
-    // ---- forward with checkpoints ----
+    const int TB = 128, nb = (n + TB - 1) / TB;
+    // Records segment sg from its checkpoint: stage inputs in adj_store[4 k + s], their stencil
+    // sums in adj_g, the state after the segment in adj_store[4 ckpt + 1].
+    auto record = [&](int sg) -> int {
+        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
+        Fields &F0 = H->adj_store[0];
+        const double *cp = H->adj_cp + (size_t)7 * n * sg;
+        k_set_conservative<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, cp, cp + n, cp + 2 * (size_t)n, cp + 3 * (size_t)n,
+                                              cp + 4 * (size_t)n, cp + 5 * (size_t)n, cp + 6 * (size_t)n, F0);
+        const int it = sc0.itime + n0;
+        SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->itime, &it, sizeof(int), cudaMemcpyHostToDevice, st));
+        Fields &T = H->adj_store[4 * (size_t)ckpt], &X = H->adj_store[4 * (size_t)ckpt + 1];
+        for (int k = 0; k < len; k++) {
+            for (int s = 0; s < 4; s++) {
+                StageArgs A = make_args_io(H, H->adj_store[4 * k + s], s < 3 ? H->adj_store[4 * k + s + 1] : T, s);
+                A.gsave = H->adj_g + (size_t)(4 * k + s) * kAdjG * n;
+                if (int rc = launch_stage_any(H, A, false)) return rc;
+            }
+            Fields &next = k + 1 < len ? H->adj_store[4 * (k + 1)] : X;
+            StageArgs Fa = make_args_io(H, T, next, 5);
+            if (int rc = launch_filter<SUNSET_FORM_LC>(H, Fa, false)) return rc;
+            k_finalize<SUNSET_FORM_LC><<<nb, TB, 0, st>>>(Fa, 1);
+        }
+        SUNSET_CUDA(H, cudaGetLastError());
+        return 0;
+    };
+    // ---- forward with checkpoints; the last segment is recorded as it runs ----
     for (int sg = 0; sg < nseg; sg++) {
         const Fields &F = H->buf[H->cur];
         double *cp = H->adj_cp + (size_t)7 * n * sg;
@@ -1524,81 +1897,72 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
         for (int f = 0; f < 7; f++)
             SUNSET_CUDA(H, cudaMemcpyAsync(cp + (size_t)f * n, src[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         const int len = std::min(ckpt, nsteps - sg * ckpt);
-        if (int rc = step_run(H, dt, len, 0)) return rc;
+        if (sg + 1 < nseg) {
+            if (int rc = step_run(H, dt, len, 0)) return rc;
+        } else {
+            if (int rc = record(sg)) return rc;
+            const Fields &X = H->adj_store[4 * (size_t)ckpt + 1];
+            const Fields &D = H->buf[H->cur];
+            const double *xs[13] = {X.ro, X.rou, X.rov, X.u, X.v, X.q[0], X.q[1], X.q[2], X.q[3],
+                                    X.c[0], X.c[1], X.c[2], X.c[3]};
+            double *ds[13] = {D.ro, D.rou, D.rov, D.u, D.v, D.q[0], D.q[1], D.q[2], D.q[3], D.c[0], D.c[1], D.c[2], D.c[3]};
+            for (int f = 0; f < 13; f++)
+                SUNSET_CUDA(H, cudaMemcpyAsync(ds[f], xs[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
     }
+    if (int rc = set_tstep_device(H)) return rc;
     if (int rc = reduce_ke_mass(H, J, nullptr)) return rc;
     DevScalars scN;
     SUNSET_CUDA(H, cudaMemcpyAsync(&scN, H->dsc, sizeof(scN), cudaMemcpyDeviceToHost, st));
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
     if (scN.err) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite error norm in the forward run");
     // ---- reverse ----
-    const int TB = 128, nb = (n + TB - 1) / TB;
-    AdjArgs B = adj_args(H);
-    double **ua = H->adj_ua, **ubb = H->adj_ub;
-    for (int f = 0; f < 7; f++) B.ub_out[f] = ua[f];
-    k_adj_objective<<<nb, TB, 0, st>>>(n, H->buf[H->cur], H->vol, B);
-    SUNSET_CUDA(H, cudaMemsetAsync(H->adj_acc, 0, 4 * sizeof(double), st));
+    RevArgs B = rev_args(H);
+    B.dt = dt;
+    k_adj_objective<<<H->ntiles, kTile, 0, st>>>(H->buf[H->cur], H->vol, B);
+    SUNSET_CUDA(H, cudaMemsetAsync(H->adj_tacc, 0, 2 * (size_t)H->ntiles * sizeof(double), st));
     const double alpha[4] = {SUNSET_RK_A21, SUNSET_RK_A32, SUNSET_RK_A43, SUNSET_RK_B4};
     const double beta[4] = {SUNSET_RK_B1, SUNSET_RK_B2, SUNSET_RK_B3, 0.0};
-    const size_t smem = halo_doubles(ngather(SUNSET_FORM_LC, false), H->halo_max) * sizeof(double) +
-                        LinkRing<false, 3, ring_depth(false)>::bytes();
-    double *part2 = H->adj_tpart + 2 * (size_t)H->ntiles;
+    auto gstage = [&](int k, int s) { return H->adj_g + (size_t)(4 * k + s) * kAdjG * n; };
+    auto gpair = [&](int b) { return reinterpret_cast<double2 *>(H->adj_gp[b]); };
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
-        // recompute the segment, keeping the stage inputs
-        {
-            Fields &F0 = H->adj_store[0];
-            const double *cp = H->adj_cp + (size_t)7 * n * sg;
-            k_set_conservative<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, cp, cp + n, cp + 2 * (size_t)n, cp + 3 * (size_t)n,
-                                                  cp + 4 * (size_t)n, cp + 5 * (size_t)n, cp + 6 * (size_t)n, F0);
-            const int it = sc0.itime + n0;
-            SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->itime, &it, sizeof(int), cudaMemcpyHostToDevice, st));
-            Fields &T = H->adj_store[4 * (size_t)ckpt], &X = H->adj_store[4 * (size_t)ckpt + 1];
-            for (int k = 0; k < len; k++) {
-                for (int s = 0; s < 4; s++) {
-                    StageArgs A = make_args_io(H, H->adj_store[4 * k + s], s < 3 ? H->adj_store[4 * k + s + 1] : T, s);
-                    if (int rc = launch_stage_any(H, A, false)) return rc;
-                }
-                Fields &next = k + 1 < len ? H->adj_store[4 * (k + 1)] : X;
-                StageArgs Fa = make_args_io(H, T, next, 5);
-                if (int rc = launch_filter<SUNSET_FORM_LC>(H, Fa, false)) return rc;
-                k_finalize<SUNSET_FORM_LC><<<nb, TB, 0, st>>>(Fa, 1);
-            }
-        }
-        // reverse sweep over the segment
+        if (sg + 1 < nseg)
+            if (int rc = record(sg)) return rc;
         for (int k = len - 1; k >= 0; k--) {
-            // filter and mass correction: ua (adjoint of U_{k+1}) -> ubb
-            for (int f = 0; f < 7; f++) { B.ub_in[f] = ua[f]; B.ub_out[f] = ubb[f]; }
-            if (H->cfg.mcorr) {
-                k_adj_sum<<<nb, TB, 0, st>>>(n, ua[0], part2);
-                k_adj_fold<<<1, 128, 0, st>>>(part2, nb, 1, H->adj_acc + 2, 0);
+            // filter + mass correction reversed, then the pointwise reverse of stage 3
+            B.prev = H->adj_store[4 * k + 3];
+            B.gprev = gstage(k, 3);
+            B.gb_out = gpair(0);
+            B.alpha = alpha[3];
+            B.beta = beta[3];
+            B.first = 0;
+            k_adj_filter_lc<<<H->ntiles, kTile, smem_filter, st>>>(B);
+            int cur = 0;
+            for (int s = 3; s >= 1; s--) {  // stencils of stage s, pointwise reverse of stage s - 1
+                B.cur = H->adj_store[4 * k + s];
+                B.gb_in = gpair(cur);
+                B.gb_out = gpair(cur ^ 1);
+                B.prev = H->adj_store[4 * k + s - 1];
+                B.gprev = gstage(k, s - 1);
+                B.alpha = alpha[s - 1];
+                B.beta = beta[s - 1];
+                B.first = (s == 1) && (sc0.itime + n0 + k == 1);
+                k_adj_stage_lc<true><<<H->ntiles, kTile, smem_stage, st>>>(B);
+                cur ^= 1;
             }
-            B.mcorr = H->cfg.mcorr;
-            B.mc_sum = H->adj_acc + 2;
-            B.mc_tv = &H->dsc->tv;
-            k_adj_filter_lc<<<nb, TB, 0, st>>>(B);
-            std::swap(ua, ubb);
-            for (int f = 0; f < 7; f++) SUNSET_CUDA(H, cudaMemsetAsync(B.sbar[f], 0, n * sizeof(double), st));
-            for (int s = 3; s >= 0; s--) {
-                StageArgs A = make_args_io(H, H->adj_store[4 * k + s], H->adj_store[4 * k + s], s);
-                for (int f = 0; f < 7; f++) { B.ub_in[f] = ua[f]; B.ub_out[f] = ubb[f]; }
-                B.dt = dt;
-                B.alpha = alpha[s];
-                B.beta = beta[s];
-                B.first = (s == 0) && (sc0.itime + n0 + k == 1);
-                B.add_sbar = s == 0;
-                k_adj_point_lc<<<H->ntiles, kTile, smem, st>>>(A, B);
-                k_adj_fold<<<1, 128, 0, st>>>(H->adj_tpart, H->ntiles, 2, H->adj_acc, 1);
-                k_adj_transpose_lc<<<nb, TB, 0, st>>>(A, B);
-                std::swap(ua, ubb);
-            }
+            B.cur = H->adj_store[4 * k];
+            B.gb_in = gpair(cur);
+            k_adj_stage_lc<false><<<H->ntiles, kTile, smem_stage, st>>>(B);
         }
     }
     SUNSET_CUDA(H, cudaGetLastError());
+    k_adj_fold<<<1, 128, 0, st>>>(H->adj_tacc, H->ntiles, 2, H->adj_acc, 0);
     double acc[2];
     SUNSET_CUDA(H, cudaMemcpyAsync(acc, H->adj_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    for (int f = 0; f < 7; f++)
-        SUNSET_CUDA(H, cudaMemcpyAsync(dU0 + (size_t)f * n, ua[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    for (int f = 0; f < kAdjS; f++)
+        SUNSET_CUDA(H, cudaMemcpyAsync(dU0 + (size_t)f * n, H->adj_ua[f], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    SUNSET_CUDA(H, cudaMemsetAsync(dU0 + (size_t)6 * n, 0, n * sizeof(double), st));
     // the handle keeps the final state and its time
     SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &scN, sizeof(scN), cudaMemcpyHostToDevice, st));
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
