@@ -340,41 +340,44 @@ def run_adjoint(args, local):
         g.set_state(**st)
         s0 = g.state()
         base = {k: s0[k] for k in keys}
-        # Central differences at h = 1e-6 (relative for the parameters) and, because J's
-        # rounding (about 1e-16 J per evaluation) divided by 2h is not small against some
-        # directional derivatives, also at h = 1e-4, whose truncation error O(h^2) is far
-        # below that noise.  noise = 2e-16 J / (2h) is the rounding floor of each difference.
-        fd = {"steps": [1e-6, 1e-4]}
+        # Central differences D(h) at h = 1e-6 (relative for the parameters), 1e-4, 1e-3 and
+        # 2e-3.  The rounding of J (a few 1e-16 J an evaluation, from the whole run) divided
+        # by 2h is not small against the directional derivatives at h = 1e-6; noise =
+        # 2e-16 J / (2h) / |D| is a lower bound of that floor.  The errors fall from 1e-6 to
+        # 1e-3 (rounding) and rise again at 2e-3 (truncation, O(h^2)).
+        hsteps = [1e-6, 1e-4, 1e-3, 2e-3]
+        fd = {"steps": hsteps}
+
+        def entry(ad, diff):
+            ent = {"adjoint": ad}
+            D = {}
+            for h in hsteps:
+                D[h] = diff(h)
+                ent[f"fd_h{h:g}"] = D[h]
+                ent[f"rel_h{h:g}"] = abs(ad - D[h]) / abs(D[h])
+                ent[f"noise_h{h:g}"] = 2e-16 * J / (2 * h) / abs(D[h])
+            return ent
+
         for name, ad in (("Wi", dWi), ("beta", dbeta)):
             p0 = getattr(wl, name)
-            ent = {"adjoint": ad}
-            for hrel in fd["steps"]:
-                hstep = hrel * p0
-                f = (fj(**{name: p0 + hstep}) - fj(**{name: p0 - hstep})) / (2 * hstep)
-                ent[f"fd_h{hrel:g}"] = f
-                ent[f"rel_h{hrel:g}"] = abs(ad - f) / abs(f)
-                ent[f"noise_h{hrel:g}"] = 2e-16 * J / (2 * hstep) / abs(f)
-            fd[name] = ent
+            fd[name] = entry(ad, lambda h: (fj(**{name: p0 * (1 + h)}) - fj(**{name: p0 * (1 - h)})) / (2 * h * p0))
         rng = np.random.default_rng(12345)
         dirs = []
         for r in range(8):
             d = {k: rng.standard_normal(nodes) for k in ("psixx", "psixy", "psiyy")}
             ad = sum(float(grads[k] @ d[k]) for k in d)
-            ent = {"adjoint": ad}
-            for hstep in fd["steps"]:
+
+            def diff(h):
                 sp, sm = dict(base), dict(base)
                 for k in d:
-                    sp[k] = base[k] + hstep * d[k]
-                    sm[k] = base[k] - hstep * d[k]
-                f = (fj(sp) - fj(sm)) / (2 * hstep)
-                ent[f"fd_h{hstep:g}"] = f
-                ent[f"rel_h{hstep:g}"] = abs(ad - f) / abs(f)
-                ent[f"noise_h{hstep:g}"] = 2e-16 * J / (2 * hstep) / abs(f)
-            dirs.append(ent)
+                    sp[k] = base[k] + h * d[k]
+                    sm[k] = base[k] - h * d[k]
+                return (fj(sp) - fj(sm)) / (2 * h)
+            dirs.append(entry(ad, diff))
         fd["psi0_directions"] = dirs
         ents = [fd["Wi"], fd["beta"]] + dirs
-        for hstep in fd["steps"]:
-            fd[f"max_rel_h{hstep:g}"] = max(e[f"rel_h{hstep:g}"] for e in ents)
+        for h in hsteps:
+            fd[f"max_rel_h{h:g}"] = max(e[f"rel_h{h:g}"] for e in ents)
         line["fd_check"] = fd
     print(json.dumps(line), flush=True)
     g.close()

@@ -151,8 +151,10 @@ int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
    state), evaluates J = sum_i 1/2 rho_i |u_i|^2 vol_i at the final state, and returns dJ/dWi
    and dJ/dbeta in dJ_dparams[2] and, unless dJ_dstate0 is NULL, dJ with respect to the
    initial state (7*npfb host doubles in reference order: ro rou rov psixx psixy psiyy psizz).
-   The reverse sweep recomputes the stage inputs from states stored every checkpoint_every
-   steps.  The adjoint is of the discrete step as computed (step.F90:218-512 with the filter
+   The reverse sweep recomputes each segment of checkpoint_every steps from its stored state,
+   recording the stage inputs and stencil sums (device memory: about
+   (124 * checkpoint_every + 7 * nsteps / checkpoint_every) doubles a node, plus the reverse
+   link streams).  The adjoint is of the discrete step as computed (step.F90:218-512 with the filter
    and the mass correction); SUNSET_ERR_SCOPE for other forms, mixed precision, walls or
    Mdiff != 0.  No reference counterpart (the reference has no adjoint). */
 int sunset_adjoint_run(SunsetHandle *h, double dt, int nsteps, int checkpoint_every, double *J,
