@@ -2364,20 +2364,25 @@ static int step_rk3_4s_2r_ee(OrSim *s) {
         for (int f = 0; f < 6; f++) eacc[f][i] = eacc[f][i] + RKbmbh[3] * rhs[f][i];
         e_row[i] = e_row[i] + RKbmbh[3] * s->rhs_row[i];
         e_zz[i] = e_zz[i] + RKbmbh[3] * s->rhs_zz[i];
+        /* Cholesky FENE-P (step.F90:442-452): the conformation errors are scaled by
+           1/sqrt(f).  The reference rescales its running maxima by each node's factor in
+           turn, which makes the result depend on the node order; here each node's own
+           errors are scaled by its own factor before the maximum (decision, order-free). */
+        double sc = 1.0;
+        if (form == OR_FORM_CHL && s->cfg.fenep) {
+            double fr = (s->cfg.fenep_l2 - 3.0) / (((s->cfg.fenep_l2 - s->cxx[i]) - s->cyy[i]) - s->czz[i]);
+            sc = 1.0 / sqrt(fr);
+        }
         for (int f = 0; f < 6; f++) {
             double t = fabs(eacc[f][i]) * norms[f];
+            if (f >= 3) t = t * sc;
             en[f] = (t > en[f]) ? t : en[f];
         }
         {
             double t = fabs(e_row[i]) * s->erou_norm;
             en_row = (t > en_row) ? t : en_row;
-            t = fabs(e_zz[i]) * s->exx_norm;
+            t = (fabs(e_zz[i]) * s->exx_norm) * sc;
             en_zz = (t > en_zz) ? t : en_zz;
-        }
-        if (form == OR_FORM_CHL && s->cfg.fenep) {
-            double fr = (s->cfg.fenep_l2 - 3.0) / (((s->cfg.fenep_l2 - s->cxx[i]) - s->cyy[i]) - s->czz[i]);
-            fr = 1.0 / sqrt(fr);
-            en[3] = en[3] * fr; en[4] = en[4] * fr; en[5] = en[5] * fr; en_zz = en_zz * fr;
         }
     }
 #define MAXD(a, b) ((a) > (b) ? (a) : (b))

@@ -117,10 +117,12 @@ int sunset_create(const SunsetConfig *cfg, SunsetHandle **out) {
     if (!(c.morder == 4 || c.morder == 6 || c.morder == 8 || c.morder == 10) || c.forder != c.morder)
         return set_err(H, SUNSET_ERR_SCOPE, "orders must be equal and one of 4, 6, 8, 10 (got %d, %d)", c.morder, c.forder);
     if (c.form < 0 || c.form > 3) return set_err(H, SUNSET_ERR_ARG, "unknown form %d", c.form);
-    if (c.fenep) return set_err(H, SUNSET_ERR_SCOPE, "FENE-P is not implemented on the device path");
     if (c.precision != SUNSET_FP64 && c.precision != SUNSET_MIXED) return set_err(H, SUNSET_ERR_ARG, "bad precision");
     if (c.Re <= 0 || c.Ma <= 0 || (c.form != SUNSET_FORM_NEWT && c.Wi <= 0))
         return set_err(H, SUNSET_ERR_ARG, "Re, Ma and Wi must be positive");
+    if (c.form == SUNSET_FORM_NEWT) H->cfg.fenep = 0;  // no polymer
+    if (H->cfg.fenep && !(c.fenep_l2 > 3.0))
+        return set_err(H, SUNSET_ERR_ARG, "FENE-P needs L^2 > 3 (got %g)", c.fenep_l2);
     if (int rc = set_device(H)) return rc;
     SUNSET_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
     return 0;

@@ -15,13 +15,21 @@ struct Grads {
     double cxx_x, cxx_y, cxy_x, cxy_y, cyy_x, cyy_y;              // DI, LC (momentum)
     double pxx_x, pxx_y, pxy_x, pxy_y, pyy_x, pyy_y;              // LC, CHL
     double lapcxx, lapcxy, lapcyy, lapczz;                        // polymer diffusion
+    double f_x, f_y;                                              // FENE-P function (DI, LC)
+    double pzz_x, pzz_y;                                          // CHL, FENE-P
 };
 
 struct NodeState {
     double ro, u, v, y;                 // y: node ordinate (Kolmogorov forcing)
     double cxx, cxy, cyy, czz;          // conformation tensor
     double pxx, pxy, pyy, pzz;          // psi (LC/CHL)
+    double f;                           // FENE-P function (L^2 - 3) / (L^2 - tr c)
 };
+
+// The FENE-P function fenepf (rhs_di.F90:201-203, rhs.F90:207-209, rhs_lc.F90:201-203).
+__host__ __device__ __forceinline__ double fenep_f(double L2, double cxx, double cyy, double czz) {
+    return (L2 - 3.0) / (L2 - ((cxx + cyy) + czz));
+}
 
 struct Rhs {
     double ro, rou, rov, xx, xy, yy, zz;
@@ -90,6 +98,15 @@ __host__ __device__ __forceinline__ void chl_c_from_psi(double pxx, double pxy, 
     *cyy = pxy * pxy + exp(2.0 * pyy);
     *czz = 1.0;
 }
+// cholesky_c_from_psi (FENE-P), conf_transforms.F90:39-55: psi holds the Cholesky factor of
+// J = f c, and c = J L^2 / (L^2 - 3 + tr J).
+__host__ __device__ __forceinline__ void chl_c_from_psi_fenep(double L2, double pxx, double pxy, double pyy, double pzz,
+                                                     double *cxx, double *cxy, double *cyy, double *czz) {
+    const double Jxx = exp(2.0 * pxx), Jxy = exp(pxx) * pxy, Jyy = pxy * pxy + exp(2.0 * pyy);
+    const double Jzz = exp(2.0 * pzz);
+    const double fq = L2 / ((((L2 - 3.0) + Jxx) + Jyy) + Jzz);
+    *cxx = Jxx * fq; *cxy = Jxy * fq; *cyy = Jyy * fq; *czz = Jzz * fq;
+}
 // cholesky_psi_from_c (sPTT), conf_transforms.F90:109-121
 __host__ __device__ __forceinline__ void chl_psi_from_c(double cxx, double cxy, double cyy, double czz, double *pxx,
                                                double *pxy, double *pyy, double *pzz) {
@@ -98,6 +115,37 @@ __host__ __device__ __forceinline__ void chl_psi_from_c(double cxx, double cxy, 
     double yy = (sqrt(cyy - xy * xy));
     double zz = sqrt(czz);
     *pxx = log(xx); *pxy = xy; *pyy = log(yy); *pzz = log(zz);
+}
+// cholesky_psi_from_c (FENE-P), conf_transforms.F90:89-101
+__host__ __device__ __forceinline__ void chl_psi_from_c_fenep(double L2, double cxx, double cxy, double cyy, double czz,
+                                                     double *pxx, double *pxy, double *pyy, double *pzz) {
+    const double fr = (L2 - 3.0) / (L2 - ((cxx + cyy) + czz));
+    const double Jxx = cxx * fr, Jxy = cxy * fr, Jyy = cyy * fr, Jzz = czz * fr;
+    const double xx = sqrt(Jxx);
+    const double xy = Jxy / xx;
+    const double yy = sqrt(Jyy - xy * xy);
+    const double zz = sqrt(Jzz);
+    *pxx = log(xx); *pxy = xy; *pyy = log(yy); *pzz = log(zz);
+}
+// The conversions around the filter of the Cholesky FENE-P form (rhs.F90:815-869): the
+// factor of J = f c to the factor of c before filtering, and back after it.
+__host__ __device__ __forceinline__ void chl_fenep_to_c_factor(double L2, double &pxx, double &pxy, double &pyy,
+                                                      double &pzz) {
+    double fr = ((exp(2.0 * pxx) + pxy * pxy) + exp(2.0 * pyy)) + exp(2.0 * pzz);
+    fr = (L2 * fr) / ((L2 - 3.0) + fr);
+    fr = (L2 - 3.0) / (L2 - fr);
+    pxx = pxx - log(sqrt(fr));
+    pxy = pxy / sqrt(fr);
+    pyy = pyy - log(sqrt(fr));
+    pzz = pzz - log(sqrt(fr));
+}
+__host__ __device__ __forceinline__ void chl_fenep_to_j_factor(double L2, double &pxx, double &pxy, double &pyy,
+                                                      double &pzz) {
+    const double fr = (L2 - 3.0) / (L2 - (((exp(2.0 * pxx) + pxy * pxy) + exp(2.0 * pyy)) + exp(2.0 * pzz)));
+    pxx = pxx + log(sqrt(fr));
+    pxy = pxy * sqrt(fr);
+    pyy = pyy + log(sqrt(fr));
+    pzz = pzz + log(sqrt(fr));
 }
 
 // calc_rhs_ro + calc_rhs_rovel, interior branch (rhs_di.F90:126-141,215-275; rhs.F90:220-286;
@@ -117,6 +165,10 @@ __host__ __device__ __forceinline__ void rhs_flow(const StepConsts &K, const Nod
         double gcyy2 = (2.0 * n.pxy) * g.pxy_y + (2.0 * exp(2.0 * n.pyy)) * g.pyy_y;
         fvu = fvu + K.coef_polymeric * ((gcxx1 + gcxy2) + 0.0);
         fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + 0.0);
+    } else if (K.form != SUNSET_FORM_NEWT && K.fenep) {  // rhs_di.F90:234-245, rhs_lc.F90:234-245
+        const double f1 = n.f;
+        fvu = fvu + K.coef_polymeric * (((((g.cxx_x * f1 + n.cxx * g.f_x) + g.cxy_y * f1) + n.cxy * g.f_y) + 0.0 * f1) + 0.0 * 0.0);
+        fvv = fvv + K.coef_polymeric * (((((g.cxy_x * f1 + n.cxy * g.f_x) + g.cyy_y * f1) + n.cyy * g.f_y) + 0.0 * f1) + 0.0 * 0.0);
     } else if (K.form != SUNSET_FORM_NEWT) {
         fvu = fvu + K.coef_polymeric * ((g.cxx_x + g.cxy_y) + 0.0);
         fvv = fvv + K.coef_polymeric * ((g.cxy_x + g.cyy_y) + 0.0);
@@ -180,8 +232,17 @@ __host__ __device__ __forceinline__ void rhs_c_di(const StepConsts &K, const Nod
     double ucxy = (((((g11 * cxy + g12 * cyy) + 0.0 * 0.0) + g21 * cxx) + g22 * cxy) + 0.0 * 0.0);
     double ucyy = ((2.0 * g21) * cxy + (2.0 * g22) * cyy) + (2.0 * 0.0) * 0.0;
     double uczz = ((2.0 * 0.0) * 0.0 + (2.0 * 0.0) * 0.0) + (2.0 * 0.0) * czz;
-    double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
-    double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0), szz = fr * (czz - 1.0);
+    double sxx, sxy, syy, szz;
+    if (K.fenep) {  // rhs_di.F90:444-449
+        const double fr = -n.f;
+        sxx = (fr * cxx + 1.0) / K.lambda;
+        sxy = (fr * cxy) / K.lambda;
+        syy = (fr * cyy + 1.0) / K.lambda;
+        szz = (fr * czz + 1.0) / K.lambda;
+    } else {
+        const double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+        sxx = fr * (cxx - 1.0); sxy = fr * cxy; syy = fr * (cyy - 1.0); szz = fr * (czz - 1.0);
+    }
     if (wall) {
         r.xx = (ucxx + sxx) + K.Mdiff * g.lapcxx;
         r.xy = (ucxy + sxy) + K.Mdiff * g.lapcxy;
@@ -207,10 +268,23 @@ __host__ __device__ __forceinline__ void rhs_c_chl(const StepConsts &K, const No
     double ucxy = ((g22 * lxy + ((g12 * lyy) * lyy) / lxx) + g21 * lxx);
     double ucyy = (g22 - (g12 * lxy) / lxx);
     const double cxx = n.cxx, cxy = n.cxy, cyy = n.cyy, czz = n.czz;
-    double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
-    double sxx = fr * (cxx - 1.0) + K.Mdiff * g.lapcxx;
-    double sxy = fr * cxy + K.Mdiff * g.lapcxy;
-    double syy = fr * (cyy - 1.0) + K.Mdiff * g.lapcyy;
+    double sxx, sxy, syy, szz = 0.0;
+    if (K.fenep) {  // rhs.F90:480-495: psi factors J = f c
+        const double fr = n.f, L2 = K.fenep_l2, lam = K.lambda;
+        const double srctmp = ((((((2.0 * g11) * cxx + (2.0 * g12) * cxy) + (2.0 * g21) * cxy) + (2.0 * g22) * cyy) -
+                                (((fr * cxx + fr * cyy) + fr * czz) - 3.0) / lam) +
+                               K.Mdiff * ((g.lapcxx + g.lapcyy) + g.lapczz));
+        const double den = ((L2 - cxx) - cyy) - czz;
+        sxx = (-(fr / lam) * (fr * cxx - 1.0) + (K.Mdiff * fr) * g.lapcxx) + ((fr * cxx) * srctmp) / den;
+        sxy = (-(fr / lam) * (fr * cxy) + (K.Mdiff * fr) * g.lapcxy) + ((fr * cxy) * srctmp) / den;
+        syy = (-(fr / lam) * (fr * cyy - 1.0) + (K.Mdiff * fr) * g.lapcyy) + ((fr * cyy) * srctmp) / den;
+        szz = (-(fr / lam) * (fr * czz - 1.0) + (K.Mdiff * fr) * g.lapczz) + ((fr * czz) * srctmp) / den;
+    } else {
+        const double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+        sxx = fr * (cxx - 1.0) + K.Mdiff * g.lapcxx;
+        sxy = fr * cxy + K.Mdiff * g.lapcxy;
+        syy = fr * (cyy - 1.0) + K.Mdiff * g.lapcyy;
+    }
     double csxx = ((0.5 * sxx) / lxx) / lxx;
     double csxy = sxy / lxx - ((0.5 * sxx) * lxy) / (lxx * lxx);
     double csyy = (((0.5 * syy) / lyy) / lyy - (sxy * lxy) / ((lxx * lyy) * lyy)) +
@@ -219,6 +293,12 @@ __host__ __device__ __forceinline__ void rhs_c_chl(const StepConsts &K, const No
     r.xy = (-adxy + ucxy) + csxy;
     r.yy = (-adyy + ucyy) + csyy;
     r.zz = 0.0;
+    if (K.fenep) {  // rhs.F90:539-541: psi_zz evolves
+        const double lzz = exp(n.pzz);
+        const double adzz = (n.u * g.pzz_x + n.v * g.pzz_y) + w * 0.0;
+        const double cszz = ((0.5 * szz) / lzz) / lzz;
+        r.zz = (-adzz + 0.0) + cszz;
+    }
 }
 
 // calc_rhs_logconf, interior branch, rhs_lc.F90:414-559 (sPTT, 2-D).  `first` is the
@@ -259,20 +339,32 @@ __host__ __device__ __forceinline__ void rhs_c_lc(const StepConsts &K, const Nod
     mm2(Om, P, OP);
     mm2(P, Om, PO);
     for (int c = 0; c < 4; c++) UC[c] = (OP[c] - PO[c]) + 2.0 * B[c];
-    double fR = ((1.0 - 2.0 * K.epsPTT) + K.epsPTT * tr_c);
-    Ci[0] = fR / Lv[0] - fR; Ci[1] = 0.0; Ci[2] = 0.0; Ci[3] = fR / Lv[1] - fR;
-    mm2(Ci, RT, T);
-    mm2(R, T, T);
+    double Rx[4];
+    if (K.fenep) {  // rhs_lc.F90:520-535: (-1/lambda) c^-1 (f c - I)
+        const double cxx = n.cxx, cxy = n.cxy, cyy = n.cyy;
+        const double det = cxx * cyy - cxy * cxy;
+        Ci[0] = cyy / det; Ci[3] = cxx / det; Ci[2] = -cxy / det; Ci[1] = -cxy / det;
+        B[0] = cxx * n.f; B[3] = cyy * n.f; B[2] = cxy * n.f; B[1] = cxy * n.f;
+        B[0] = B[0] - 1.0; B[3] = B[3] - 1.0;
+        mm2(Ci, B, T);
+        for (int c = 0; c < 4; c++) Rx[c] = (-1.0 / K.lambda) * T[c];
+    } else {
+        double fR = ((1.0 - 2.0 * K.epsPTT) + K.epsPTT * tr_c);
+        Ci[0] = fR / Lv[0] - fR; Ci[1] = 0.0; Ci[2] = 0.0; Ci[3] = fR / Lv[1] - fR;
+        mm2(Ci, RT, T);
+        mm2(R, T, T);
+        for (int c = 0; c < 4; c++) Rx[c] = T[c] / K.lambda;
+    }
     if (wall) {
-        r.xx = UC[0] + T[0] / K.lambda;
-        r.xy = UC[2] + T[2] / K.lambda;
-        r.yy = UC[3] + T[3] / K.lambda;
+        r.xx = UC[0] + Rx[0];
+        r.xy = UC[2] + Rx[2];
+        r.yy = UC[3] + Rx[3];
         r.zz = 0.0;
         return;
     }
-    r.xx = (adxx + UC[0]) + T[0] / K.lambda;
-    r.xy = (adxy + UC[2]) + T[2] / K.lambda;
-    r.yy = (adyy + UC[3]) + T[3] / K.lambda;
+    r.xx = (adxx + UC[0]) + Rx[0];
+    r.xy = (adxy + UC[2]) + Rx[2];
+    r.yy = (adyy + UC[3]) + Rx[3];
     r.zz = 0.0;
 }
 

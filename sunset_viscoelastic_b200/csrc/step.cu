@@ -64,15 +64,28 @@ __device__ __forceinline__ void reflect(int code, double &uj, double &vj, double
 // Fields a stage gathers from its neighbours, in shared-memory order:
 //   0 ro, 1 u, 2 v, then DI: cxx cxy cyy; LC: cxx cxy cyy psixx psixy psiyy;
 //   CHL: psixx psixy psiyy (+ cxx cxy cyy with polymer diffusion).
-__host__ __device__ constexpr int ngather(int form, bool md) {
-    return form == SUNSET_FORM_DI ? 6 : form == SUNSET_FORM_LC ? 9 : form == SUNSET_FORM_CHL ? (md ? 9 : 6) : 3;
+// FENE-P (FP) appends the FENE-P function f (DI, LC) or psizz (CHL), and with polymer
+// diffusion czz (DI, CHL).
+__host__ __device__ constexpr int ngather(int form, bool md, bool fp = false) {
+    return form == SUNSET_FORM_DI    ? 6 + (fp ? 1 : 0) + (fp && md ? 1 : 0)
+           : form == SUNSET_FORM_LC  ? 9 + (fp ? 1 : 0)
+           : form == SUNSET_FORM_CHL ? (md ? 9 : 6) + (fp ? 1 : 0) + (fp && md ? 1 : 0)
+                                     : 3;
+}
+// Positions of the FENE-P fields: f (DI, LC) or psizz (CHL), then czz (polymer diffusion).
+__host__ __device__ constexpr int fp_slot(int form, bool md) {
+    return form == SUNSET_FORM_DI ? 6 : form == SUNSET_FORM_LC ? 9 : (md ? 9 : 6);
 }
 
-template <int FORM, bool MD>
+template <int FORM, bool MD, bool FP = false>
 __device__ __forceinline__ const double *gather_src(const Fields &F, int f) {
     if (f == 0) return F.ro;
     if (f == 1) return F.u;
     if (f == 2) return F.v;
+    if (FP && f >= fp_slot(FORM, MD)) {
+        if (f == fp_slot(FORM, MD)) return FORM == SUNSET_FORM_CHL ? F.q[3] : F.f;
+        return F.c[3];
+    }
     if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
         if (f <= 5) return F.c[f - 3];
         return F.q[f - 6];
@@ -185,7 +198,7 @@ __host__ __device__ inline size_t halo_doubles(int ng, int hmax) { return ((size
 // neighbours read from the block's shared-memory halo.  In the mixed path the weights are
 // the FP32-rounded ones and A.gsx.. hold the FP64 sums of those, so the FP64 arithmetic
 // below evaluates the difference form sum_k w_k (phi_j - phi_i) of the rounded stencil.
-template <int FORM, bool MD, bool MX, class RING>
+template <int FORM, bool MD, bool MX, bool FP, class RING>
 __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const double *sm, RING &R, Grads &g) {
     const int hm = A.hmax;
     const int npair = R.npair;
@@ -194,6 +207,8 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
     double s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
     double s_pxx_x = 0, s_pxx_y = 0, s_pxy_x = 0, s_pxy_y = 0, s_pyy_x = 0, s_pyy_y = 0;
     double s_lxx = 0, s_lxy = 0, s_lyy = 0;
+    double s_f_x = 0, s_f_y = 0, s_lzz = 0;  // FENE-P: f or psizz gradient, czz Laplacian
+    constexpr int kFp = fp_slot(FORM, MD);
     const bool mir = cK.has_mirrors;
     const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
     // FP64 step: separate multiply and add, as the reference; mixed step: fused
@@ -249,6 +264,12 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
             mac(s_lxy, cxyj, wlk);
             mac(s_lyy, cyyj, wlk);
         }
+        if constexpr (FP && FORM != SUNSET_FORM_NEWT) {  // scalar or zz fields: no reflection sign
+            const double fj = sm[kFp * hm + j];
+            mac(s_f_x, fj, wxk);
+            mac(s_f_y, fj, wyk);
+            if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) mac(s_lzz, sm[(kFp + 1) * hm + j], wlk);
+        }
     };
     // links in order k = 2m, 2m+1: the sums keep the reference's order
     for (int m = 0; m < npair; m++) {
@@ -275,6 +296,14 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
     g.cxx_x = g.cxx_y = g.cxy_x = g.cxy_y = g.cyy_x = g.cyy_y = 0.0;
     g.pxx_x = g.pxx_y = g.pxy_x = g.pxy_y = g.pyy_x = g.pyy_y = 0.0;
     g.lapcxx = g.lapcxy = g.lapcyy = g.lapczz = 0.0;
+    g.f_x = g.f_y = g.pzz_x = g.pzz_y = 0.0;
+    if constexpr (FP && FORM != SUNSET_FORM_NEWT) {
+        const double fi = FORM == SUNSET_FORM_CHL ? F.q[3][i] : F.f[i];
+        const double gfx = s_f_x - fi * gx, gfy = s_f_y - fi * gy;
+        if (FORM == SUNSET_FORM_CHL) { g.pzz_x = gfx; g.pzz_y = gfy; }
+        else { g.f_x = gfx; g.f_y = gfy; }
+        if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) g.lapczz = s_lzz - F.c[3][i] * ls;
+    }
     if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {
         const double cxx = F.c[0][i], cxy = F.c[1][i], cyy = F.c[2][i];
         g.cxx_x = s_cxx_x - cxx * gx;
@@ -355,10 +384,10 @@ __host__ __device__ constexpr int stage_min_blocks(int) { return SUNSET_STAGE_BL
 // MX (mixed precision): FP32 weights; the register S is kept as the FP32 increment
 // D = S - U over the stage's FP64 state U (so S = U + D loses only FP32 rounding of an
 // O(dt rhs) quantity) and the error accumulator E as FP32.
-template <int FORM, bool MD, bool MX>
+template <int FORM, bool MD, bool MX, bool FP>
 __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageArgs A) {
     extern __shared__ __align__(16) double smem[];
-    constexpr int NG = ngather(FORM, MD);
+    constexpr int NG = ngather(FORM, MD, FP);
     const int i = blockIdx.x * kTile + threadIdx.x;
     bool active = (i >> 5) < cK.nslices;
     LinkRing<MX, 3, ring_depth(MX)> R;
@@ -374,14 +403,14 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
     R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
            active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
     R.prologue();  // the first link pairs stream in while the halo is staged
-    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD>(A.in, f); });
+    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD, FP>(A.in, f); });
     const int stage = A.stage;
     if (stage == 0 && i == 0) {
         A.sc->cfl_bits = 0x7ff0000000000000ull;
         A.sc->par_bits = 0x7ff0000000000000ull;
     }
     Grads g;
-    if (active) gather_stage<FORM, MD, MX>(A, i, smem, R, g);
+    if (active) gather_stage<FORM, MD, MX, FP>(A, i, smem, R, g);
     active = active && i < cK.npfb;
     unsigned long long emax_bits = 0;
     if constexpr (FORM == SUNSET_FORM_LC && !MX) {
@@ -398,6 +427,8 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         n.ro = F.ro[i]; n.u = F.u[i]; n.v = F.v[i]; n.y = A.py_node[i];
         n.cxx = F.c[0][i]; n.cxy = F.c[1][i]; n.cyy = F.c[2][i]; n.czz = F.c[3][i];
         n.pxx = F.q[0][i]; n.pxy = F.q[1][i]; n.pyy = F.q[2][i]; n.pzz = F.q[3][i];
+        n.f = 0.0;
+        if constexpr (FP) n.f = FORM == SUNSET_FORM_CHL ? fenep_f(cK.fenep_l2, n.cxx, n.cyy, n.czz) : F.f[i];
         Rhs r;
         const bool wall = cK.has_walls && A.ntype[i] == 0;
         if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
@@ -418,7 +449,8 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
             rhs_c_lc(cK, n, g, first, r, wall);
         } else { r.xx = r.xy = r.yy = r.zz = 0.0; }
         const double rr[7] = {r.ro, r.rou, r.rov, r.xx, r.xy, r.yy, r.zz};
-        constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+        // evolved fields: DI 7 (czz), CHL FENE-P 7 (psizz), otherwise 6 (3 Newtonian)
+        constexpr int nf = (FORM == SUNSET_FORM_DI || (FORM == SUNSET_FORM_CHL && FP)) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
         if (stage == 4) {
 #pragma unroll
             for (int f = 0; f < 7; f++) A.rhs[f][i] = rr[f];
@@ -452,6 +484,11 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                 }
             } else {
                 double en = 0.0;
+                // Cholesky FENE-P: the conformation errors scaled by the node's 1/sqrt(f)
+                // (step.F90:442-452, applied per node; see the design notes)
+                double conf_scale = 1.0;
+                if constexpr (FORM == SUNSET_FORM_CHL && FP)
+                    conf_scale = 1.0 / sqrt((cK.fenep_l2 - 3.0) / (((cK.fenep_l2 - n.cxx) - n.cyy) - n.czz));
 #pragma unroll
                 for (int f = 0; f < nf; f++) {
                     const double norm = f == 0 ? cK.ero_norm : f < 3 ? cK.erou_norm : cK.exx_norm;
@@ -463,7 +500,8 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                         Un[f] = A.reg[f][i] + RKb * rr[f];
                         E = A.eacc[f][i] + RKbmbh * rr[f];
                     }
-                    const double t = fabs(E) * norm;
+                    double t = fabs(E) * norm;
+                    if (f >= 3) t = t * conf_scale;
                     en = (t > en) ? t : en;
                     if (t != t) en = t;
                 }
@@ -485,8 +523,15 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                     O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = F.c[3][i];
                 } else if (FORM == SUNSET_FORM_CHL) {
                     double cxx, cxy, cyy, czz;
-                    chl_c_from_psi(Un[3], Un[4], Un[5], &cxx, &cxy, &cyy, &czz);
+                    if constexpr (FP) chl_c_from_psi_fenep(cK.fenep_l2, Un[3], Un[4], Un[5], Un[6], &cxx, &cxy, &cyy, &czz);
+                    else chl_c_from_psi(Un[3], Un[4], Un[5], &cxx, &cxy, &cyy, &czz);
                     O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = czz;
+                }
+                if constexpr (FP && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC)) {
+                    // DI: c is the state itself (czz = Un[6]); LC: czz is carried
+                    const double czz = FORM == SUNSET_FORM_DI ? Un[6] : F.c[3][i];
+                    O.f[i] = fenep_f(cK.fenep_l2, FORM == SUNSET_FORM_DI ? Un[3] : O.c[0][i],
+                                     FORM == SUNSET_FORM_DI ? Un[5] : O.c[2][i], czz);
                 }
             }
         }
@@ -496,10 +541,15 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
 
 // filter_variables (rhs_di.F90:667-720; rhs.F90:792-900; rhs_lc.F90:818-893): the
 // hyperviscous filter of each evolved field plus the mass-correction partial sums.
-template <int FORM, bool MX>
+//
+// FP (Cholesky FENE-P): psizz is filtered too, and the psi factors of J = f c are converted to
+// factors of c before filtering and back after it (rhs.F90:815-869) -- in shared memory for
+// the halo, in registers for the node itself.
+template <int FORM, bool MX, bool FP = false>
 __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
     extern __shared__ __align__(16) double smem[];
-    constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    constexpr bool CF = FP && FORM == SUNSET_FORM_CHL;
+    constexpr int nf = (FORM == SUNSET_FORM_DI || CF) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
     const Fields &F = A.in;
     const int i = blockIdx.x * kTile + threadIdx.x;
     const bool live = (i >> 5) < cK.nslices;
@@ -513,6 +563,12 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
         return f == 0 ? F.ro : f == 1 ? F.rou : f == 2 ? F.rov : F.q[f - 3];
     });
     const int hm = A.hmax;
+    if constexpr (CF) {
+        const int hn = A.halo_ptr[blockIdx.x + 1] - A.halo_ptr[blockIdx.x];
+        for (int h = threadIdx.x; h < hn; h += blockDim.x)
+            chl_fenep_to_c_factor(cK.fenep_l2, smem[3 * hm + h], smem[4 * hm + h], smem[5 * hm + h], smem[6 * hm + h]);
+        __syncthreads();
+    }
     double part = 0.0;
     if (live) {
         const int npair = R.npair;
@@ -548,17 +604,25 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
             double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
             double rof = 0.0;
             const bool wall = cK.has_walls && A.ntype[i] == 0;
+            double own[7], res[7];
+#pragma unroll
+            for (int f = 0; f < 7; f++) own[f] = f < nf ? src[f][i] : 0.0;
+            if constexpr (CF) chl_fenep_to_c_factor(cK.fenep_l2, own[3], own[4], own[5], own[6]);
 #pragma unroll
             for (int f = 0; f < 7; f++) {
                 if (f < nf) {
-                    const double p = src[f][i];
+                    const double p = own[f];
                     double r = p + (t[f] - p * hs);
                     if (wall && (f == 1 || f == 2)) r = 0.0;  // apply_time_dependent_bounds after the filter
-                    dst[f][i] = r;
+                    res[f] = r;
                     if (f == 0) rof = r;
-                } else if (FORM != SUNSET_FORM_NEWT) {
-                    dst[f][i] = src[f][i];
                 }
+            }
+            if constexpr (CF) chl_fenep_to_j_factor(cK.fenep_l2, res[3], res[4], res[5], res[6]);
+#pragma unroll
+            for (int f = 0; f < 7; f++) {
+                if (f < nf) dst[f][i] = res[f];
+                else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = src[f][i];
             }
             part = (rof - cK.rho_char) * A.vol[i];
         }
@@ -617,9 +681,11 @@ __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
             F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy;
         } else if (FORM == SUNSET_FORM_CHL) {
             double cxx, cxy, cyy, czz;
-            chl_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy, &czz);
+            if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, F.q[0][i], F.q[1][i], F.q[2][i], F.q[3][i], &cxx, &cxy, &cyy, &czz);
+            else chl_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy, &czz);
             F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy; F.c[3][i] = czz;
         }
+        if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
     }
     if (advance && i == 0) {
         DevScalars *sc = A.sc;
@@ -742,13 +808,20 @@ __global__ void k_set_state(int npfb, int form, const double *ro, const double *
         F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
     } else if (form == SUNSET_FORM_CHL) {
         double p0, p1, p2, p3;
-        chl_psi_from_c(c0, c1, c2, c3, &p0, &p1, &p2, &p3);
-        F.q[0][i] = p0; F.q[1][i] = p1; F.q[2][i] = p2; F.q[3][i] = p3;
-        chl_c_from_psi(p0, p1, p2, &c0, &c1, &c2, &c3);
+        if (cK.fenep) {
+            chl_psi_from_c_fenep(cK.fenep_l2, c0, c1, c2, c3, &p0, &p1, &p2, &p3);
+            F.q[0][i] = p0; F.q[1][i] = p1; F.q[2][i] = p2; F.q[3][i] = p3;
+            chl_c_from_psi_fenep(cK.fenep_l2, p0, p1, p2, p3, &c0, &c1, &c2, &c3);
+        } else {
+            chl_psi_from_c(c0, c1, c2, c3, &p0, &p1, &p2, &p3);
+            F.q[0][i] = p0; F.q[1][i] = p1; F.q[2][i] = p2; F.q[3][i] = p3;
+            chl_c_from_psi(p0, p1, p2, &c0, &c1, &c2, &c3);
+        }
         F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
     } else {
         F.q[0][i] = c0; F.q[1][i] = c1; F.q[2][i] = c2; F.q[3][i] = c3;
     }
+    if (F.f) F.f[i] = fenep_f(cK.fenep_l2, c0, c2, c3);
 }
 
 // Conservative state given directly (ro, rou, rov, q0..q3), derived fields recomputed
@@ -768,9 +841,11 @@ __global__ void k_set_conservative(int npfb, int form, const double *ro, const d
         F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = 1.0;
     } else if (form == SUNSET_FORM_CHL) {
         double c0, c1, c2, c3;
-        chl_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2, &c3);
+        if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, q0[i], q1[i], q2[i], q3[i], &c0, &c1, &c2, &c3);
+        else chl_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2, &c3);
         F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
     }
+    if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
 }
 
 __global__ void k_ke_mass(int npfb, Fields F, const double *vol, double *partials) {
@@ -872,66 +947,89 @@ int upload_consts(Handle *H) {
 
 constexpr size_t kMaxStageSmem = 200 * 1024;
 
-// Opt the staged kernels into large dynamic shared memory on the handle's device.
-int set_smem_attributes(Handle *H) {
 #define SUNSET_SMEM_ATTR(K) SUNSET_CUDA(H, cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem))
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false, false>));
-    SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false, false>));
-    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_DI, false>));
-    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_CHL, false>));
-    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_LC, false>));
-    SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_NEWT, false>));
-    if (H->cfg.precision == SUNSET_MIXED) {
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, false, true>));
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_DI, true, true>));
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, false, true>));
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_CHL, true, true>));
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_LC, false, true>));
-        SUNSET_SMEM_ATTR((k_stage<SUNSET_FORM_NEWT, false, true>));
-        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_DI, true>));
-        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_CHL, true>));
-        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_LC, true>));
-        SUNSET_SMEM_ATTR((k_filter<SUNSET_FORM_NEWT, true>));
-    }
-#undef SUNSET_SMEM_ATTR
+template <int FORM, bool MD, bool FP>
+int stage_smem_attributes(Handle *H, bool mx) {
+    SUNSET_SMEM_ATTR((k_stage<FORM, MD, false, FP>));
+    if (mx) SUNSET_SMEM_ATTR((k_stage<FORM, MD, true, FP>));
+    return 0;
+}
+template <int FORM, bool FP>
+int filter_smem_attributes(Handle *H, bool mx) {
+    SUNSET_SMEM_ATTR((k_filter<FORM, false, FP>));
+    if (mx) SUNSET_SMEM_ATTR((k_filter<FORM, true, FP>));
     return 0;
 }
 
+// Opt the staged kernels of the handle's configuration into large dynamic shared memory.
+int set_smem_attributes(Handle *H) {
+    const bool mx = H->cfg.precision == SUNSET_MIXED, md = H->cfg.Mdiff != 0.0, fp = H->cfg.fenep != 0;
+    int rc = 0;
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI:
+        rc = md ? (fp ? stage_smem_attributes<SUNSET_FORM_DI, true, true>(H, mx) : stage_smem_attributes<SUNSET_FORM_DI, true, false>(H, mx))
+                : (fp ? stage_smem_attributes<SUNSET_FORM_DI, false, true>(H, mx) : stage_smem_attributes<SUNSET_FORM_DI, false, false>(H, mx));
+        if (!rc) rc = filter_smem_attributes<SUNSET_FORM_DI, false>(H, mx);
+        break;
+    case SUNSET_FORM_CHL:
+        rc = md ? (fp ? stage_smem_attributes<SUNSET_FORM_CHL, true, true>(H, mx) : stage_smem_attributes<SUNSET_FORM_CHL, true, false>(H, mx))
+                : (fp ? stage_smem_attributes<SUNSET_FORM_CHL, false, true>(H, mx) : stage_smem_attributes<SUNSET_FORM_CHL, false, false>(H, mx));
+        if (!rc) rc = fp ? filter_smem_attributes<SUNSET_FORM_CHL, true>(H, mx) : filter_smem_attributes<SUNSET_FORM_CHL, false>(H, mx);
+        break;
+    case SUNSET_FORM_LC:
+        rc = fp ? stage_smem_attributes<SUNSET_FORM_LC, false, true>(H, mx) : stage_smem_attributes<SUNSET_FORM_LC, false, false>(H, mx);
+        if (!rc) rc = filter_smem_attributes<SUNSET_FORM_LC, false>(H, mx);
+        break;
+    default:
+        rc = stage_smem_attributes<SUNSET_FORM_NEWT, false, false>(H, mx);
+        if (!rc) rc = filter_smem_attributes<SUNSET_FORM_NEWT, false>(H, mx);
+    }
+    return rc;
+}
+#undef SUNSET_SMEM_ATTR
+
 inline bool is_mx(const Handle *H) { return H->cfg.precision == SUNSET_MIXED; }
 
-template <int FORM, bool MD>
+template <int FORM, bool MD, bool FP>
 int launch_stage(Handle *H, const StageArgs &A, bool mx) {
-    const size_t smem = halo_doubles(ngather(FORM, MD), H->halo_max) * sizeof(double) +
+    const size_t smem = halo_doubles(ngather(FORM, MD, FP), H->halo_max) * sizeof(double) +
                         (mx ? LinkRing<true, 3, ring_depth(true)>::bytes() : LinkRing<false, 3, ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    if (mx) k_stage<FORM, MD, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-    else k_stage<FORM, MD, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (mx) k_stage<FORM, MD, true, FP><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    else k_stage<FORM, MD, false, FP><<<H->ntiles, kTile, smem, H->stream>>>(A);
     return 0;
 }
 
 // A must come from make_args(..., step = true); mx is the handle's precision.
 int launch_stage_any(Handle *H, const StageArgs &A, bool mx) {
-    const bool md = H->cfg.Mdiff != 0.0;
+    const bool md = H->cfg.Mdiff != 0.0, fp = H->cfg.fenep != 0;
     switch (H->cfg.form) {
-    case SUNSET_FORM_DI: return md ? launch_stage<SUNSET_FORM_DI, true>(H, A, mx) : launch_stage<SUNSET_FORM_DI, false>(H, A, mx);
-    case SUNSET_FORM_CHL: return md ? launch_stage<SUNSET_FORM_CHL, true>(H, A, mx) : launch_stage<SUNSET_FORM_CHL, false>(H, A, mx);
-    case SUNSET_FORM_LC: return launch_stage<SUNSET_FORM_LC, false>(H, A, mx);
-    default: return launch_stage<SUNSET_FORM_NEWT, false>(H, A, mx);
+    case SUNSET_FORM_DI:
+        if (md) return fp ? launch_stage<SUNSET_FORM_DI, true, true>(H, A, mx) : launch_stage<SUNSET_FORM_DI, true, false>(H, A, mx);
+        return fp ? launch_stage<SUNSET_FORM_DI, false, true>(H, A, mx) : launch_stage<SUNSET_FORM_DI, false, false>(H, A, mx);
+    case SUNSET_FORM_CHL:
+        if (md) return fp ? launch_stage<SUNSET_FORM_CHL, true, true>(H, A, mx) : launch_stage<SUNSET_FORM_CHL, true, false>(H, A, mx);
+        return fp ? launch_stage<SUNSET_FORM_CHL, false, true>(H, A, mx) : launch_stage<SUNSET_FORM_CHL, false, false>(H, A, mx);
+    case SUNSET_FORM_LC:
+        return fp ? launch_stage<SUNSET_FORM_LC, false, true>(H, A, mx) : launch_stage<SUNSET_FORM_LC, false, false>(H, A, mx);
+    default: return launch_stage<SUNSET_FORM_NEWT, false, false>(H, A, mx);
     }
 }
 
 template <int FORM>
 int launch_filter(Handle *H, const StageArgs &A, bool mx) {
-    constexpr int nf = (FORM == SUNSET_FORM_DI) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    const bool cf = FORM == SUNSET_FORM_CHL && H->cfg.fenep;  // Cholesky FENE-P: psizz and the conversions
+    const int nf = (FORM == SUNSET_FORM_DI || cf) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
     const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) +
                         (mx ? LinkRing<true, 1, ring_depth(true)>::bytes() : LinkRing<false, 1, ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    if (mx) k_filter<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-    else k_filter<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (cf) {
+        if (mx) k_filter<FORM, true, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        else k_filter<FORM, false, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    } else {
+        if (mx) k_filter<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        else k_filter<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    }
     return 0;
 }
 
@@ -990,6 +1088,8 @@ int state_alloc(Handle *H) {
             for (int k = 0; k < 4; k++)
                 if (dalloc(H, &F.c[k], n)) return SUNSET_ERR_NOMEM;
         }
+        if (H->cfg.fenep && (H->cfg.form == SUNSET_FORM_DI || H->cfg.form == SUNSET_FORM_LC) && dalloc(H, &F.f, n))
+            return SUNSET_ERR_NOMEM;
     }
     for (int f = 0; f < 7; f++) {
         if (dalloc(H, &H->rhs[f], n)) return SUNSET_ERR_NOMEM;
@@ -1820,6 +1920,7 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint runs the FP64 step");
     if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers node sets without walls");
     if (H->cfg.Mdiff != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint assumes Mdiff = 0");
+    if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers Oldroyd-B and sPTT, not FENE-P");
     if (nsteps < 1 || ckpt < 1) return set_err(H, SUNSET_ERR_ARG, "nsteps and checkpoint_every must be positive");
     const int n = H->npfb;
     cudaStream_t st = H->stream;

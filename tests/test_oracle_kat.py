@@ -8,6 +8,7 @@ rhs.F90:275, statistics.F90:552-612), mass conservation under the mass correctio
 (rhs_di.F90:697-717), and building blocks against independent computations.
 """
 import ctypes
+import dataclasses
 import math
 import os
 import random
@@ -310,3 +311,43 @@ def test_cylinder_channel_stencils_and_first_steps():
     assert all(np.all(np.isfinite(st[k])) for k in ("ro", "u", "v", "cxx"))
     assert np.all(st["rou"][t == 0] == 0.0)
     assert st["u"].max() > 0.0
+
+
+@pytest.mark.parametrize("form", ["di", "chl", "lc"])
+def test_fenep_relaxation_agrees_across_forms(form):
+    """FENE-P at rest with a uniform conformation tensor: every form must give
+    dc/dt = -(f c - I) / lambda with f = (L^2 - 3) / (L^2 - tr c) (rhs_di.F90:444-449).
+    The Cholesky form evolves factors of J = f c (rhs.F90:480-541, conf_transforms.F90:39-101)
+    and the log-conformation form log c (rhs_lc.F90:520-535), so their right-hand sides are
+    mapped back to dc/dt through the restatement's own transforms by a central difference."""
+    L2, Wi = 50.0, 1.0
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=16, form=form, Wi=Wi, epsPTT=0.0,
+                             kolmogorov_forcing=0)
+    ns = wl.nodes()
+    o = O.for_workload(wl, ns, fenep=True, fenep_l2=L2).setup()
+    n = ns.n
+    c = dict(cxx=2.0, cxy=0.5, cyy=1.5, czz=1.0 if form == "lc" else 1.2)
+    one, zero = np.ones(n), np.zeros(n)
+    o.set_state(ro=one, u=zero, v=zero, **{k: v * one for k, v in c.items()})
+    r = o.rhs()
+    f = (L2 - 3.0) / (L2 - (c["cxx"] + c["cyy"] + c["czz"]))
+    expect = {"cxx": -(f * c["cxx"] - 1.0) / Wi, "cxy": -(f * c["cxy"]) / Wi, "cyy": -(f * c["cyy"] - 1.0) / Wi,
+              "czz": -(f * c["czz"] - 1.0) / Wi}
+    if form == "di":
+        got = {"cxx": r["xx"], "cxy": r["xy"], "cyy": r["yy"], "czz": r["zz"]}
+    else:
+        st = o.state()
+        q = np.array([st["psixx"], st["psixy"], st["psiyy"], st["psizz"]])
+        rq = np.array([r["xx"], r["xy"], r["yy"], r["zz"]])
+        eps = 1e-6
+        cs = []
+        for sgn in (1.0, -1.0):
+            o.set_raw_state(one, zero, zero, q + sgn * eps * rq)
+            cs.append(o.state())
+        got = {k: (cs[0][k] - cs[1][k]) / (2 * eps) for k in expect}
+    keys = ["cxx", "cxy", "cyy"] + ([] if form == "lc" else ["czz"])
+    for k in keys:
+        err = np.abs(got[k] - expect[k]).max()
+        print(form, k, "dc/dt", got[k][0], "expected", expect[k], "error", err)
+        assert err <= 1e-8 * max(1.0, abs(expect[k])), (k, err)
+    assert np.abs(r["ro"]).max() < 1e-12 and np.abs(r["rou"]).max() < 1e-10
