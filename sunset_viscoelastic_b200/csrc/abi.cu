@@ -188,8 +188,6 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
             }
         }
     }
-    if (nb > 0 && H->cfg.Mdiff != 0.0)
-        return set_err(H, SUNSET_ERR_SCOPE, "polymer diffusion (Mdiff) with walls is not on the device path");
     const int n = (int)vx.size();
     if (n >= (1 << 30)) return set_err(H, SUNSET_ERR_SCOPE, "too many nodes");
     if (hos > 0)

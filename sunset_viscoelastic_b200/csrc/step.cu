@@ -43,6 +43,12 @@ struct StageArgs {
     const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
     const int *ntype;            // node types (walls: 0)
     const double *rnx, *rny;     // wall normals into the fluid
+    // polymer diffusion on walls: reference-order local links, small-link counts, boundary
+    // index and FD rows, tangential second-derivative weights and their sums, spacings
+    const uint16_t *lloc_ref;
+    const int *cnt_small, *bidx, *brow;
+    const double *wbt, *wbt_sum, *sp;
+    int nplink;
     Fields in, out;
     double *reg[7], *eacc[7], *rhs[7];
     float *dreg[7], *eacc32[7];  // mixed precision
@@ -329,6 +335,45 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
     }
 }
 
+// Polymer diffusion on a wall node: the transverse Laplacian of c over the node's small links
+// with the tangential second-derivative weights (calc_laplacian_transverse_only_on_bound,
+// derivatives.F90:306-358), plus the one-sided normal second derivative from its four FD rows
+// (rhs_di.F90:556-568; rhs.F90 likewise, there for c_zz too).  Links in the reference's
+// order, neighbours from the tile's shared-memory halo.
+template <int FORM, bool MD, bool FP>
+__device__ __forceinline__ void wall_conformation_laplacian(const StageArgs &A, int i, const double *sm, Grads &g) {
+    const int jj = A.bidx[i], hm = A.hmax;
+    const long long base = A.slice_ptr[i >> 5];
+    const int ln = i & 31, cs = A.cnt_small[i];
+    constexpr int c0 = FORM == SUNSET_FORM_DI ? 3 : 6;  // halo slots of cxx, cxy, cyy
+    constexpr bool zz = FORM == SUNSET_FORM_CHL && FP;   // c_zz enters the Cholesky FENE-P source
+    constexpr int cz = fp_slot(FORM, MD) + 1;
+    const double *w = A.wbt + (size_t)jj * A.nplink;
+    double l0 = 0.0, l1 = 0.0, l2 = 0.0, l3 = 0.0;
+    for (int k = 0; k < cs; k++) {
+        const unsigned lk = A.lloc_ref[sell_at(base, k, ln)];
+        const int h = lk & kLocMask, code = lk >> 14;
+        double cxy = sm[(c0 + 1) * hm + h];
+        if (code == 1 || code == 2) cxy = -cxy;
+        const double wk = w[k];
+        l0 = l0 + sm[c0 * hm + h] * wk;
+        l1 = l1 + cxy * wk;
+        l2 = l2 + sm[(c0 + 2) * hm + h] * wk;
+        if (zz) l3 = l3 + sm[cz * hm + h] * wk;
+    }
+    const Fields &F = A.in;
+    const double ws = A.wbt_sum[jj], L = cK.L_char;
+    const double den = (((72.0 * A.sp[i]) * A.sp[i]) * L) * L;
+    const int *r = A.brow + 4 * jj;
+    auto fd = [&](const double *q) {
+        return (((((-415.0 * q[i]) + 576.0 * q[r[0]]) - 216.0 * q[r[1]]) + 64.0 * q[r[2]]) - 9.0 * q[r[3]]) / den;
+    };
+    g.lapcxx = (l0 - F.c[0][i] * ws) + fd(F.c[0]);
+    g.lapcxy = (l1 - F.c[1][i] * ws) + fd(F.c[1]);
+    g.lapcyy = (l2 - F.c[2][i] * ws) + fd(F.c[2]);
+    if (zz) g.lapczz = (l3 - F.c[3][i] * ws) + fd(F.c[3]);
+}
+
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
 
 __device__ __forceinline__ void block_max_bits(unsigned long long v, unsigned long long *dst) {
@@ -432,6 +477,8 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         Rhs r;
         const bool wall = cK.has_walls && A.ntype[i] == 0;
         if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
+            if constexpr (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL))
+                wall_conformation_laplacian<FORM, MD, FP>(A, i, smem, g);
             const double xn = A.rnx[i], yn = A.rny[i];
             rhs_flow_wall(cK, n, g, xn, yn, r);
             const double gux = g.u_x, guy = g.u_y, gvx = g.v_x, gvy = g.v_y;
@@ -927,6 +974,14 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     A.ntype = H->ntype;
     A.rnx = H->rnx;
     A.rny = H->rny;
+    A.lloc_ref = H->lloc;
+    A.cnt_small = H->cnt_small;
+    A.bidx = H->bidx;
+    A.brow = H->brow;
+    A.wbt = H->wbt;
+    A.wbt_sum = H->wbt_sum;
+    A.sp = H->sp;
+    A.nplink = H->nplink;
     A.in = H->buf[from];
     A.out = H->buf[from ^ 1];
     for (int f = 0; f < 7; f++) {

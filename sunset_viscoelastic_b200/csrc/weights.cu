@@ -1045,10 +1045,30 @@ int boundary_prune_links(Handle *H) {
     return 0;
 }
 
+// The tangential second-derivative weights of boundary nodes scaled by 1/L^2 and their sums
+// over all links (calc_labf_sums, labf.F90:426-446): the transverse Laplacian of the
+// conformation tensor on walls (derivatives.F90:306-358).  One thread per boundary node.
+__global__ void k_boundary_tangential_sums(int nb, int nplink, double L, const int *blist, const int *cnt,
+                                           const double *wb2, double *wbt, double *wbt_sum) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= nb) return;
+    const double *w = wb2 + (size_t)jj * nplink * 2;
+    double sum = 0.0;
+    for (int k = 0; k < cnt[blist[jj]]; k++) sum = sum + w[2 * k + 1];
+    wbt_sum[jj] = (sum / L) / L;
+    for (int k = 0; k < nplink; k++) wbt[(size_t)jj * nplink + k] = (w[2 * k + 1] / L) / L;
+}
+
 int labf_sums_device(Handle *H) {
     SumArgs a{H->npfb, H->cfg.L_char, H->px, H->py, H->h, H->sp, H->ntype, H->cnt, H->lpt, H->fdpar, H->slice_ptr,
               H->wx, H->wy, H->wl, H->wh, H->gsx, H->gsy, H->lsum, H->hsum, H->vol};
     k_labf_sums<<<(H->npfb + 255) / 256, 256, 0, H->stream>>>(a);
+    if (H->nb > 0) {
+        if (!H->wbt && (dalloc(H, &H->wbt, (size_t)H->nb * H->nplink) || dalloc(H, &H->wbt_sum, H->nb)))
+            return SUNSET_ERR_NOMEM;
+        k_boundary_tangential_sums<<<(H->nb + 127) / 128, 128, 0, H->stream>>>(H->nb, H->nplink, H->cfg.L_char, H->blist,
+                                                                             H->cnt, H->wb2, H->wbt, H->wbt_sum);
+    }
     SUNSET_CUDA(H, cudaGetLastError());
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
     return 0;

@@ -218,3 +218,61 @@ def test_cylinder_channel_against_restatement():
         e = rel(sg[k], sr[k])
         print(f"cylinder {k} after 50 steps: {e:.2e}")
         assert e <= F_TOL, (k, e)
+
+
+# Polymer diffusion next to walls: the transverse Laplacian of c on wall nodes
+# (derivatives.F90:306-358) with the one-sided FD normal correction (rhs_di.F90:556-568;
+# rhs.F90 also for c_zz, which the Cholesky FENE-P source reads).
+MD_CASES = [("di", 8, False), ("chl", 8, False), ("chl", 8, True), ("di", 6, True)]
+
+
+@pytest.fixture(scope="module", params=MD_CASES, ids=[f"{f}-o{o}{'-fenep' if p else ''}" for f, o, p in MD_CASES])
+def md_pair(request):
+    form, order, fenep = request.param
+    ns = channel(32)
+    kw = dict(PARAMS, Mdiff=1e-2, fenep=fenep, fenep_l2=100.0)
+    O.set_pow_mode(True)
+    try:
+        ref = O.Oracle(form=form, order=order, **kw).build_domain(ns).setup()
+    finally:
+        O.set_pow_mode(False)
+    gpu = labfm.Sunset(form=form, order=order, **kw)
+    gpu.build_domain(ns)
+    gpu.setup()
+    nd = ref.nodes()
+    npfb = ref.sizes()[1]
+    return form, order, ref, gpu, nd["x"][:npfb], nd["y"][:npfb], nd["node_type"][:npfb]
+
+
+def test_rhs_with_walls_and_polymer_diffusion(md_pair):
+    form, order, ref, gpu, x, y, t = md_pair
+    st = perturbed_state(y, x)
+    st["czz"] = 1.0 + 0.05 * np.sin(2 * np.pi * x) * np.cos(np.pi * y)
+    for o in (ref, gpu):
+        o.set_state(**st)
+    rr, rg = ref.rhs(), gpu.rhs()
+    gu = np.abs(ref.gradient(st["u"])).max()
+    cmax = max(np.abs(st["cxx"]).max(), np.abs(st["cyy"]).max())
+    for k in ["ro", "rou", "rov", "xx", "xy", "yy", "zz"]:
+        scale = max(gu * cmax, np.abs(rr[k]).max(), 1e-300)
+        e = rel(rg[k], rr[k], scale)
+        ew = rel(rg[k][t == 0], rr[k][t == 0], scale)
+        print(f"{form}-o{order} Mdiff rhs_{k}: {e:.2e} (walls {ew:.2e})")
+        assert e <= W_TOL, (k, e)
+
+
+def test_steps_with_walls_and_polymer_diffusion(md_pair):
+    form, order, ref, gpu, x, y, t = md_pair
+    st = perturbed_state(y, x)
+    for o in (ref, gpu):
+        o.set_state(**st)
+    dtc, dtp = ref.set_tstep()
+    dt = 0.3 * min(dtc, dtp)
+    for o in (ref, gpu):
+        o.step(dt, 100)
+    sr, sg = ref.state(), gpu.state()
+    for k in ["ro", "rou", "rov", "u", "v", "cxx", "cxy", "cyy", "czz"]:
+        e = rel(sg[k], sr[k])
+        print(f"{form}-o{order} Mdiff {k} after 100 steps: {e:.2e}")
+        assert e <= F_TOL, (k, e)
+    assert np.all(sg["rou"][t == 0] == 0.0)
