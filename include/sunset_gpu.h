@@ -80,6 +80,15 @@ int sunset_get_sizes(SunsetHandle *h, int *np, int *npfb, int *nb, int *nplink);
 
 /* neighbours.F90:32-341 find_neighbours: cell-list search + per-row distance sort. */
 int sunset_find_neighbours(SunsetHandle *h);
+/* labf.F90:1079-1721 adapt_stencils + adapt_stencils_main: per interior node (node_type 999)
+   the smoothing length h, and then h_small, shrink by 2% steps while the Laplacian system's
+   residual, the stencils' amplification of wavenumbers up to Nyquist and the reduction count
+   stay within the reference's limits; then the neighbour lists are rebuilt with the new
+   lengths (sunset.F90:43-51).  Call after sunset_find_neighbours, before the weights. */
+int sunset_adapt_stencils(SunsetHandle *h);
+/* The smoothing lengths h and h_small of the npfb nodes (reference order), the module
+   arrays of common_vars.F90 that sunset_adapt_stencils changes. */
+int sunset_get_lengths(SunsetHandle *h, double *h_out, double *h_small_out);
 /* labf.F90:34-231 calc_labf_weights (+ calc_filter_weights :233-394). */
 int sunset_calc_labf_weights(SunsetHandle *h);
 /* labf.F90:505-1039 calc_boundary_weights: prunes the links of boundary nodes to their own

@@ -54,7 +54,7 @@ def lib():
         L.or_build_domain.argtypes = [P, C.c_int, ip, dp, dp, ip, dp, dp, dp, C.c_double, C.c_double,
                                       C.c_double, C.c_double, ip, C.c_double]
         L.or_sizes.argtypes = [P, C.POINTER(C.c_int)] * 1 + [C.POINTER(C.c_int)] * 3
-        for name in ["or_find_neighbours", "or_calc_labf_weights", "or_calc_boundary_weights",
+        for name in ["or_find_neighbours", "or_adapt_stencils", "or_calc_labf_weights", "or_calc_boundary_weights",
                      "or_calc_labf_sums", "or_filter_coefficients", "or_setup_all"]:
             getattr(L, name).argtypes = [P]
         L.or_get_nodes.argtypes = [P, dp, dp, dp, dp, dp, ip, ip, ip]
@@ -164,6 +164,10 @@ class Oracle:
 
     def find_neighbours(self):
         self._chk(self.L.or_find_neighbours(self.h))
+
+    def adapt_stencils(self):
+        """labf.F90:1079-1721 on the current lists, then the neighbour search again."""
+        self._chk(self.L.or_adapt_stencils(self.h))
 
     def calc_labf_weights(self):
         self._chk(self.L.or_calc_labf_weights(self.h))

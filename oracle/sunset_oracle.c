@@ -14,6 +14,7 @@
  */
 #include "sunset_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -1083,6 +1084,156 @@ static void abf_1d_link(const OrSim *s, int i, int j, double xt, double yt, doub
     double ff1 = or_fac(fabs(x / hh), s->h3);
     x = x / hh;
     abfs1D(x, ff1, gvec);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * adapt_stencils (labf.F90:1079-1412) and adapt_stencils_main (:1414-1721), 2-D, Hermite ABFs.
+ * For every plain interior node (node_type > 2 and not 998) the length scale shrinks by the
+ * reference's factor 0.98 -- a default-real (single-precision) literal -- while
+ *   1. the residual of the Laplacian system, sqrt(|A b_L - C_L|^2 h^2 / n), stays below
+ *      res_tol / h,
+ *   2. no wavenumber q = i pi / (32 s), i = 1..33, is amplified by the d/dx, d/dy or
+ *      Laplacian stencil beyond 1.0001 (or turned negative, for the Laplacian), and
+ *   3. at most log(0.6) / log(0.98) reductions (log(0.6) in single precision) have been made.
+ * The first pass reduces h (and h_small with it) over the node's list, keeping the links
+ * within 2 h; the second reduces h_small over the small list.  A moment matrix whose SVD does
+ * not converge (the reference stops) ends the node's reduction here.  The caller rebuilds the
+ * neighbour lists with the new lengths (sunset.F90:43-51).
+ * ------------------------------------------------------------------------------------- */
+static double adapt_res_tol(int order) {
+    const int n = nsize_for(order);
+    const double c = order == 4 ? 1.0e-3 : order == 6 ? 5.0e-3 : order == 8 ? 3.0e-2 : 1.0;
+    return ((c * (double)(n * n * n * n)) * DBL_EPSILON) / (double)order;
+}
+
+typedef struct {
+    SvdWork sw;
+    double *amat, *gvec, *xvec, *bl, *bx, *by, *res, *dl, *dx, *dy;
+    int *tl;
+} AdaptWork;
+
+static void adapt_node(OrSim *s, int i, int main_pass, AdaptWork *w) {
+    const int order = main_pass ? s->cfg.morder : s->cfg.forder;
+    const int n = nsize_for(order), nl = nsize_for(s->cfg.forder);
+    const double rf = (double)0.98f, amp_tol = 1.0001;
+    const double limit = (double)logf(0.6f) / log(rf);
+    const double res_tol = adapt_res_tol(order);
+    const int nk = 32;
+    int *lk = s->ij_link + (size_t)i * s->nplink;
+    for (int ii = 0;; ii++) {
+        const double hh = (main_pass ? s->hs[i] : s->h[i]) * rf;
+        const int cur = main_pass ? s->ij_count_small[i] : s->ij_count[i];
+        int cnt = 0;
+        for (int k = 0; k < cur; k++) {
+            const int j = lk[k];
+            const double rx = s->rx[i] - s->rx[j], ry = s->ry[i] - s->ry[j];
+            if (sqrt(rx * rx + ry * ry) <= hh * ss) w->tl[cnt++] = j;
+        }
+        /* moment matrix over the temporary list, as in calc_labf_weights */
+        memset(w->amat, 0, sizeof(double) * n * n);
+        for (int k = 0; k < cnt; k++) {
+            const int j = w->tl[k];
+            const double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+            const double qq = sqrt(x * x + y * y) / hh;
+            const double ff1 = or_wab(qq, s->h2);
+            or_abfs(s->cfg.forder, x / hh, y / hh, w->gvec);
+            for (int m = 0; m < nl; m++) w->gvec[m] = w->gvec[m] * ff1;
+            or_monomials(s->cfg.forder, x / hh, y / hh, w->xvec);
+            for (int i2 = 0; i2 < n; i2++)
+                for (int i1 = 0; i1 < n; i1++) w->amat[i2 * n + i1] = w->amat[i2 * n + i1] + w->xvec[i1] * w->gvec[i2];
+        }
+        const double thr = res_tol / hh;
+        double hc;
+        if (svd_factor(w->amat, n, &w->sw)) {
+            hc = (2.0 * res_tol) / hh;
+        } else {
+            memset(w->bl, 0, sizeof(double) * n); w->bl[2] = (1.0 / hh) / hh; w->bl[4] = (1.0 / hh) / hh;
+            memset(w->bx, 0, sizeof(double) * n); w->bx[0] = 1.0 / hh;
+            memset(w->by, 0, sizeof(double) * n); w->by[1] = 1.0 / hh;
+            svd_apply(&w->sw, n, w->bl);
+            svd_apply(&w->sw, n, w->bx);
+            svd_apply(&w->sw, n, w->by);
+            /* residual of the Laplacian system */
+            hc = 0.0;
+            for (int i1 = 0; i1 < n; i1++) {
+                double r = (i1 == 2 || i1 == 4) ? (-1.0 / hh) / hh : 0.0;
+                for (int i2 = 0; i2 < n; i2++) r = r + w->amat[i2 * n + i1] * w->bl[i2];
+                hc = hc + r * r;
+            }
+            hc = (hc * hh) * hh;
+            hc = sqrt(hc / (double)n);
+            if (hc < thr) {
+                /* stencil amplification: the dot products of each link do not depend on q */
+                for (int k = 0; k < cnt; k++) {
+                    const int j = w->tl[k];
+                    const double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+                    const double qq = sqrt(x * x + y * y) / hh;
+                    const double ff1 = or_wab(qq, s->h2);
+                    or_abfs(s->cfg.forder, x / hh, y / hh, w->gvec);
+                    for (int m = 0; m < nl; m++) w->gvec[m] = w->gvec[m] * ff1;
+                    w->dl[k] = dotn(w->bl, w->gvec, n);
+                    w->dx[k] = dotn(w->bx, w->gvec, n);
+                    w->dy[k] = dotn(w->by, w->gvec, n);
+                }
+                for (int i1 = 1; i1 <= nk + 1 && hc < thr; i1++) {
+                    const double q = (((double)i1 * pi) / s->sp[i]) / (double)nk;
+                    double hl = 0.0, hx = 0.0, hy = 0.0;
+                    for (int k = 0; k < cnt; k++) {
+                        const int j = w->tl[k];
+                        const double x = -(s->rx[i] - s->rx[j]), y = -(s->ry[i] - s->ry[j]);
+                        hl = hl + (0.5 - (0.5 * cos(x * q)) * cos(y * q)) * w->dl[k];
+                        hx = hx + (cos(y * q) * sin(x * q)) * w->dx[k];
+                        hy = hy + (cos(x * q) * sin(y * q)) * w->dy[k];
+                    }
+                    hl = hl / (q * q);
+                    hx = hx / q;
+                    hy = hy / q;
+                    if (hl > amp_tol || hl < 0.0) hc = (2.0 * res_tol) / hh;
+                    if (fabs(hx) > amp_tol) hc = (2.0 * res_tol) / hh;
+                    if (fabs(hy) > amp_tol) hc = (2.0 * res_tol) / hh;
+                    if (isnan(hc)) hc = (2.0 * res_tol) / hh;
+                }
+            }
+        }
+        if ((double)ii > limit) hc = (2.0 * res_tol) / hh;
+        if (hc >= thr) break; /* (a NaN residual compares false and is accepted, as there) */
+        if (main_pass) {
+            s->hs[i] = hh;
+            s->ij_count_small[i] = cnt;
+        } else {
+            s->h[i] = hh;
+            s->hs[i] = hh;
+            for (int k = 0; k < cnt; k++) lk[k] = w->tl[k];
+            s->ij_count[i] = cnt;
+            s->ij_count_small[i] = cnt;
+        }
+    }
+}
+
+int or_adapt_stencils(OrSim *s) {
+    if (!s->ij_count) return fail(s, "neighbours not built");
+    const int nmax = nsize_for(s->cfg.forder > s->cfg.morder ? s->cfg.forder : s->cfg.morder);
+#pragma omp parallel
+    {
+        AdaptWork w;
+        svdw_init(&w.sw, nmax);
+        w.amat = (double *)xcalloc((size_t)nmax * nmax, sizeof(double));
+        w.gvec = (double *)xcalloc(nmax, sizeof(double)); w.xvec = (double *)xcalloc(nmax, sizeof(double));
+        w.bl = (double *)xcalloc(nmax, sizeof(double)); w.bx = (double *)xcalloc(nmax, sizeof(double));
+        w.by = (double *)xcalloc(nmax, sizeof(double)); w.res = NULL;
+        w.dl = (double *)xcalloc(s->nplink + 1, sizeof(double)); w.dx = (double *)xcalloc(s->nplink + 1, sizeof(double));
+        w.dy = (double *)xcalloc(s->nplink + 1, sizeof(double)); w.tl = (int *)xcalloc(s->nplink + 1, sizeof(int));
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < s->npfb; i++) {
+            if (s->type[i] <= 2 || s->type[i] == 998) continue;
+            adapt_node(s, i, 0, &w);
+            adapt_node(s, i, 1, &w);
+        }
+        svdw_free(&w.sw);
+        free(w.amat); free(w.gvec); free(w.xvec); free(w.bl); free(w.bx); free(w.by);
+        free(w.dl); free(w.dx); free(w.dy); free(w.tl);
+    }
+    return or_find_neighbours(s);
 }
 
 int or_calc_boundary_weights(OrSim *s) {

@@ -59,6 +59,7 @@ int or_get_nodes(OrSim *s, double *x, double *y, double *h, double *h_small, dou
                  int *node_type, int *irelation, int *vrelation);
 
 int or_find_neighbours(OrSim *s);
+int or_adapt_stencils(OrSim *s);        /* labf.F90:1079-1721, then the neighbour search again */
 int or_calc_labf_weights(OrSim *s);      /* + calc_filter_weights + calc_node_volumes */
 int or_calc_boundary_weights(OrSim *s);
 int or_calc_labf_sums(OrSim *s);

@@ -237,6 +237,45 @@ int sunset_find_neighbours(SunsetHandle *sh) {
     return 0;
 }
 
+int sunset_adapt_stencils(SunsetHandle *sh) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->nbr_ok, "sunset_find_neighbours")) return rc;
+    if (H->w_ok) return set_err(H, SUNSET_ERR_ARG, "adapt the stencils before building the weights");
+    if (int rc = set_device(H)) return rc;
+    if (int rc = adapt_stencils_device(H)) return rc;
+    // the neighbour lists again with the new lengths (sunset.F90:43-51)
+    void **lists[] = {(void **)&H->slice_ptr, (void **)&H->slice_w, (void **)&H->slice_ws, (void **)&H->lpt,
+                      (void **)&H->lidx, (void **)&H->halo_ptr, (void **)&H->halo, (void **)&H->lloc};
+    for (void **p : lists) {
+        dfree(H, *p);
+        *p = nullptr;
+    }
+    H->nbr_ok = false;
+    int rc = find_neighbours_device(H);
+    if (rc) return rc;
+    rc = build_halos(H);
+    if (rc) return rc;
+    H->nbr_ok = true;
+    return 0;
+}
+
+int sunset_get_lengths(SunsetHandle *sh, double *h, double *h_small) {
+    if (!sh || !h || !h_small) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->domain_ok, "sunset_build_domain")) return rc;
+    if (int rc = set_device(H)) return rc;
+    const int n = H->npfb;
+    std::vector<double> hv(n), hsv(n);
+    SUNSET_CUDA(H, cudaMemcpy(hv.data(), H->h, n * sizeof(double), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(hsv.data(), H->hs, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {  // internal node i is reference node perm[i]
+        h[H->h_perm[i]] = hv[i];
+        h_small[H->h_perm[i]] = hsv[i];
+    }
+    return 0;
+}
+
 int sunset_calc_labf_weights(SunsetHandle *sh) {
     if (!sh) return SUNSET_ERR_ARG;
     Handle *H = &sh->H;

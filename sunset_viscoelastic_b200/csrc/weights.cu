@@ -950,6 +950,155 @@ __global__ void k_boundary_frame(BndArgs a) {
     }
 }
 
+// adapt_stencils + adapt_stencils_main (labf.F90:1079-1721), 2-D, Hermite ABFs.  One warp
+// per plain interior node (node_type > 2, not 998).  The length scale shrinks by the
+// reference's single-precision factor 0.98 while the Laplacian system's residual stays below
+// res_tol / h, no wavenumber q = i pi / (32 s), i = 1..33, is amplified beyond 1.0001 by the
+// d/dx, d/dy or Laplacian stencil (nor turned negative by the Laplacian), and at most
+// `limit` reductions have been made.  Pass 0 reduces h (h_small with it) over the node's
+// list, pass 1 h_small over its small list.  The lists are sorted by distance, so the links
+// within 2 h are a prefix of each.  The arithmetic follows the CPU restatement operation for
+// operation (the same moment matrix, warp SVD and sums in the same order); the amplification
+// sums run one wavenumber per lane, each over the links in order.  A moment matrix whose SVD
+// does not converge ends the node's reduction (the reference stops).
+struct AdaptArgs {
+    WArgs w;
+    double *h, *hs;
+    const double *sp;
+    int nplink, per_warp;
+    double rf, limit, res_tol[2];
+};
+
+template <int ORDER>
+__host__ __device__ constexpr int adapt_fixed_doubles() {
+    return 2 * nsz(ORDER) * (nsz(ORDER) | 1) + 3 * (nsz(ORDER) + 2) + nsz(ORDER) * (nsz(ORDER) | 1) + 6 * nsz(ORDER);
+}
+
+template <int ORDER>
+__global__ void k_adapt_stencils(AdaptArgs a) {
+    constexpr int n = nsz(ORDER);
+    constexpr int ld = n | 1;
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    double *U = smem + (size_t)warp * a.per_warp;
+    double *V = U + n * ld, *W = V + n * ld, *rv1 = W + (n + 2), *tmp = rv1 + (n + 2), *M = tmp + (n + 2);
+    double *X = M + n * ld, *G = X + n, *bl = G + n, *bx = bl + n, *by = bx + n, *R = by + n;
+    double *lx = R + n, *ly = lx + a.nplink, *dl = ly + a.nplink, *dxv = dl + a.nplink, *dyv = dxv + a.nplink;
+    const WArgs &wa = a.w;
+    constexpr double amp_tol = 1.0001;
+    constexpr int nk = 32;
+    for (int i = blockIdx.x * wpb + warp; i < wa.npfb; i += gridDim.x * wpb) {
+        const int t = wa.ntype[i];
+        if (t <= 2 || t == 998) continue;
+        const double xi = wa.px[i], yi = wa.py[i], si = a.sp[i];
+        int c_all = wa.cnt[i], c_small = wa.cnt_small[i];
+        double h_i = a.h[i], hs_i = a.hs[i];
+        for (int pass = 0; pass < 2; pass++) {
+            const double res_tol = a.res_tol[pass];
+            for (int ii = 0;; ii++) {
+                const double hh = (pass ? hs_i : h_i) * a.rf;
+                const int cur = pass ? c_small : c_all;
+                int cnt = cur;  // leading links within hh * ss
+                for (int b = 0; b < cur; b += 32) {
+                    const int k = b + lane;
+                    bool out = false;
+                    if (k < cur) {
+                        const int p = wa.lpt[sell_off(wa.slice_ptr, i, k)];
+                        const double rx = xi - wa.px[p], ry = yi - wa.py[p];
+                        out = !(sqrt(rx * rx + ry * ry) <= hh * kSs);
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, out);
+                    if (m) { cnt = b + __ffs(m) - 1; break; }
+                }
+                assemble<ORDER>(wa, i, cnt, hh, U, ld, X, G, lane);
+                for (int e = lane; e < n * ld; e += 32) M[e] = U[e];
+                __syncwarp();
+                const double thr = res_tol / hh;
+                double hc;
+                if (svd_factor_warp<n>(U, V, W, rv1, ld, lane)) {
+                    hc = (2.0 * res_tol) / hh;
+                } else {
+                    for (int m = lane; m < n; m += 32) {
+                        bl[m] = (m == 2 || m == 4) ? (1.0 / hh) / hh : 0.0;
+                        bx[m] = m == 0 ? 1.0 / hh : 0.0;
+                        by[m] = m == 1 ? 1.0 / hh : 0.0;
+                    }
+                    svd_apply_warp<n>(U, V, W, tmp, bl, ld, lane);
+                    svd_apply_warp<n>(U, V, W, tmp, bx, ld, lane);
+                    svd_apply_warp<n>(U, V, W, tmp, by, ld, lane);
+                    // residual of the Laplacian system, rows in parallel, sums in order
+                    for (int r = lane; r < n; r += 32) {
+                        double v = (r == 2 || r == 4) ? (-1.0 / hh) / hh : 0.0;
+                        for (int c = 0; c < n; c++) v = v + M[c * ld + r] * bl[c];
+                        R[r] = v;
+                    }
+                    __syncwarp();
+                    hc = 0.0;
+                    if (lane == 0) {
+                        for (int r = 0; r < n; r++) hc = hc + R[r] * R[r];
+                        hc = (hc * hh) * hh;
+                        hc = sqrt(hc / (double)n);
+                    }
+                    hc = __shfl_sync(0xffffffffu, hc, 0);
+                    if (hc < thr) {
+                        // each link's dot products with the three solutions (independent of q)
+                        for (int k = lane; k < cnt; k += 32) {
+                            const int p = wa.lpt[sell_off(wa.slice_ptr, i, k)];
+                            const double x = -(xi - wa.px[p]), y = -(yi - wa.py[p]);
+                            const double qq = sqrt(x * x + y * y) / hh;
+                            const double ff1 = wab(qq, wa.h2);
+                            const double xx = x / hh, yy = y / hh;
+                            double sl = 0.0, sx = 0.0, sy = 0.0;
+                            for (int m = 0; m < n; m++) {
+                                const int pm = p_of(m), qm = q_of(m);
+                                const double g = ((qm == 0) ? hermite(pm, xx) : (pm == 0) ? hermite(qm, yy)
+                                                                                          : hermite(pm, xx) * hermite(qm, yy)) * ff1;
+                                sl = sl + bl[m] * g;
+                                sx = sx + bx[m] * g;
+                                sy = sy + by[m] * g;
+                            }
+                            lx[k] = x; ly[k] = y; dl[k] = sl; dxv[k] = sx; dyv[k] = sy;
+                        }
+                        __syncwarp();
+                        bool fail = false;
+                        for (int i1 = lane + 1; i1 <= nk + 1; i1 += 32) {
+                            const double q = (((double)i1 * kPi) / si) / (double)nk;
+                            double hl = 0.0, hx = 0.0, hy = 0.0;
+                            for (int k = 0; k < cnt; k++) {
+                                const double x = lx[k], y = ly[k];
+                                hl = hl + (0.5 - (0.5 * cos(x * q)) * cos(y * q)) * dl[k];
+                                hx = hx + (cos(y * q) * sin(x * q)) * dxv[k];
+                                hy = hy + (cos(x * q) * sin(y * q)) * dyv[k];
+                            }
+                            hl = hl / (q * q);
+                            hx = hx / q;
+                            hy = hy / q;
+                            if (hl > amp_tol || hl < 0.0 || fabs(hx) > amp_tol || fabs(hy) > amp_tol) fail = true;
+                        }
+                        if (__any_sync(0xffffffffu, fail)) hc = (2.0 * res_tol) / hh;
+                    }
+                }
+                if ((double)ii > a.limit) hc = (2.0 * res_tol) / hh;
+                if (hc >= thr) break;  // a NaN residual compares false and is accepted, as in the reference
+                if (pass == 0) {
+                    h_i = hh;
+                    hs_i = hh;
+                    c_all = cnt;
+                    c_small = cnt;
+                } else {
+                    hs_i = hh;
+                    c_small = cnt;
+                }
+                __syncwarp();
+            }
+        }
+        if (lane == 0) {
+            a.h[i] = h_i;
+            a.hs[i] = hs_i;
+        }
+    }
+}
+
 template <int ORDER>
 int launch_weights(Handle *H, WArgs &a) {
     constexpr int per_warp = smem_doubles<ORDER>() * (int)sizeof(double);
@@ -969,6 +1118,59 @@ int launch_weights(Handle *H, WArgs &a) {
 }
 
 }  // namespace
+
+template <int ORDER>
+int launch_adapt(Handle *H, AdaptArgs &a) {
+    const int per_warp = (adapt_fixed_doubles<ORDER>() + 5 * a.nplink + 1) & ~1;
+    const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
+    int wpb = (int)((200 * 1024) / per_warp_bytes);
+    if (wpb > 16) wpb = 16;
+    if (wpb < 1) return set_err(H, SUNSET_ERR_SCOPE, "neighbour lists too long for the stencil adaptation");
+    a.per_warp = per_warp;
+    const size_t smem = (size_t)wpb * per_warp_bytes;
+    SUNSET_CUDA(H, cudaFuncSetAttribute(k_adapt_stencils<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nsm = 0;
+    SUNSET_CUDA(H, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, H->device));
+    int nb = (a.w.npfb + wpb - 1) / wpb;
+    if (nb > nsm * 8) nb = nsm * 8;
+    k_adapt_stencils<ORDER><<<nb, wpb * 32, smem, H->stream>>>(a);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+// The residual tolerance of the adaptation, labf.F90:1126-1139 (Hermite ABFs).
+static double adapt_res_tol(int order) {
+    const int n = (order * order + 3 * order) / 2;
+    const double c = order == 4 ? 1.0e-3 : order == 6 ? 5.0e-3 : order == 8 ? 3.0e-2 : 1.0;
+    return ((c * (double)(n * n * n * n)) * 2.220446049250313080847e-16) / (double)order;
+}
+
+int adapt_stencils_device(Handle *H) {
+    if (H->cfg.forder != H->cfg.morder)
+        return set_err(H, SUNSET_ERR_SCOPE, "the device stencil adaptation requires forder == morder");
+    AdaptArgs a{};
+    a.w = WArgs{H->npfb, H->cfg.morder, H->cfg.forder, H->h2, H->px, H->py, H->h, H->hs, H->ntype, H->cnt,
+                H->cnt_small, H->lpt, H->slice_ptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    a.h = H->h;
+    a.hs = H->hs;
+    a.sp = H->sp;
+    a.nplink = H->nplink;
+    a.rf = (double)0.98f;                          // reduction_factor = 0.98, a default-real literal
+    a.limit = (double)logf(0.6f) / log(a.rf);      // log(0.6) of a default-real literal
+    a.res_tol[0] = adapt_res_tol(H->cfg.forder);  // adapt_stencils
+    a.res_tol[1] = adapt_res_tol(H->cfg.morder);  // adapt_stencils_main
+    int rc;
+    switch (H->cfg.morder) {
+    case 4: rc = launch_adapt<4>(H, a); break;
+    case 6: rc = launch_adapt<6>(H, a); break;
+    case 8: rc = launch_adapt<8>(H, a); break;
+    case 10: rc = launch_adapt<10>(H, a); break;
+    default: return set_err(H, SUNSET_ERR_SCOPE, "order %d", H->cfg.morder);
+    }
+    if (rc) return rc;
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
 
 int labf_weights_device(Handle *H) {
     const int n = H->npfb;

@@ -30,7 +30,7 @@ ABI_SYMBOLS = [
     "sunset_get_state", "sunset_calc_all_rhs", "sunset_set_tstep", "sunset_step", "sunset_get_time",
     "sunset_set_time", "sunset_kinetic_energy", "sunset_mass", "sunset_synchronize", "sunset_run_host",
     "sunset_time_stage_kernel", "sunset_step_timed", "sunset_kinetic_energy_noalloc",
-    "sunset_adjoint_run", "sunset_adjoint_apply_D",
+    "sunset_adjoint_run", "sunset_adjoint_apply_D", "sunset_adapt_stencils", "sunset_get_lengths",
 ]
 
 
@@ -75,8 +75,9 @@ def load_library(build_if_missing: bool = True):
                                       C.c_double, ip, C.c_double]
     L.sunset_get_sizes.argtypes = [P] + [C.POINTER(C.c_int)] * 4
     for n in ["sunset_find_neighbours", "sunset_calc_labf_weights", "sunset_calc_boundary_weights",
-              "sunset_calc_labf_sums", "sunset_filter_coefficients", "sunset_synchronize"]:
+              "sunset_calc_labf_sums", "sunset_filter_coefficients", "sunset_synchronize", "sunset_adapt_stencils"]:
         getattr(L, n).argtypes = [P]
+    L.sunset_get_lengths.argtypes = [P, dp, dp]
     L.sunset_get_neighbours.argtypes = [P, ip, ip, ip]
     L.sunset_get_weights.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
     for n in ["sunset_calc_gradient", "sunset_calc_laplacian", "sunset_calc_filtered_var", "sunset_calc_filter_term"]:
@@ -182,6 +183,17 @@ class Sunset:
         self.calc_labf_sums()
         self.filter_coefficients()
         return self
+
+    def adapt_stencils(self):
+        """labf.F90:1079-1721 on the current lists, then the neighbour search again."""
+        self._chk(self.L.sunset_adapt_stencils(self.h))
+
+    def lengths(self):
+        """(h, h_small) of the npfb nodes in reference order."""
+        n = self.sizes()[1]
+        h, hs = np.zeros(n), np.zeros(n)
+        self._chk(self.L.sunset_get_lengths(self.h, h, hs))
+        return h, hs
 
     def neighbours(self):
         _, npfb, _, nplink = self.sizes()

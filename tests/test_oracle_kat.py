@@ -351,3 +351,37 @@ def test_fenep_relaxation_agrees_across_forms(form):
         print(form, k, "dc/dt", got[k][0], "expected", expect[k], "error", err)
         assert err <= 1e-8 * max(1.0, abs(expect[k])), (k, err)
     assert np.abs(r["ro"]).max() < 1e-12 and np.abs(r["rou"]).max() < 1e-10
+
+
+def test_adapt_stencils_invariants():
+    """adapt_stencils + adapt_stencils_main (labf.F90:1079-1721) restated, from the reference's
+    own initial lengths: h and h_small never grow and shrink in whole steps of the
+    single-precision factor 0.98, at most 26 times; only plain interior nodes change (walls and
+    FD rows keep theirs); the rebuilt lists hold exactly the points within 2 h of each node;
+    and the adapted stencils are well conditioned."""
+    rf = float(np.float32(0.98))
+    for ns, form, order in [(jittered_lattice(32, 0.3, seed=5), "lc", 6), (channel(16), "di", 8)]:
+        o = O.Oracle(form=form, order=order, h_over_s=0.0).build_domain(ns)
+        o.find_neighbours()
+        nd0 = o.nodes()
+        n = o.sizes()[1]
+        h0 = nd0["h"][:n].copy()
+        o.adapt_stencils()
+        nd = o.nodes()
+        h, hs, t = nd["h"][:n], nd["h_small"][:n], nd["node_type"][:n]
+        assert np.all(h <= h0) and np.all(hs <= h)
+        steps = np.log(h / h0) / np.log(rf)
+        assert np.all(np.abs(steps - np.round(steps)) < 1e-6) and steps.max() <= 26
+        assert np.all(h[t <= 2] == h0[t <= 2])
+        assert np.sum(h < h0) > 0
+        c, cs, lk = o.neighbours()
+        x, y = nd["x"], nd["y"]
+        for i in range(0, n, 37):
+            d2 = (x - x[i]) ** 2 + (y - y[i]) ** 2
+            assert c[i] == int(np.sum(d2 <= (2.0 * h[i]) ** 2)), i
+        o.setup()  # the neighbour search again (same lists), weights, boundary weights, sums
+        w = o.weights()
+        lap = np.abs(w["w_lap"][t > 2]).max(axis=1) * nd["s"][:n][t > 2] ** 2
+        print(form, order, "reduced", int(np.sum(h < h0)), "of", n, "max steps", int(steps.max()),
+              "max |w_lap| s^2 interior", lap.max())
+        assert lap.max() < 10.0
