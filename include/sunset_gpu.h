@@ -17,6 +17,8 @@
 #ifndef SUNSET_GPU_H
 #define SUNSET_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -147,6 +149,33 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
 /* sunset_step with the steps bracketed by CUDA events on the handle's stream: *ms is the
    device time of the nsteps steps. */
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
+
+/* ---- Dumps, restart, checkpoints ---- */
+/* output.F90:184-370 output_layer: the columns of a fields dump, 10*npfb in reference order
+   (rho - rho_char, u, v, vorticity, Q criterion, alpha_out = the node's error norm of the
+   last step, cxx, cxy, cyy, czz; vorticity and Q rotated on walls as :229-241), and the
+   header's 9 values (eflow_nm1, sum_eflow, driving_force(3) -- zero: the flow-rate controller
+   of statistics.F90 is not on this path -- emax_np1, emax_n, emax_nm1, dt). */
+int sunset_get_dump(SunsetHandle *h, double *columns, double *header);
+/* The same as files in the reference's layout: <directory>/fields_10000_<n_out>, with
+   <directory>/nodes_10000 (output_nodes, output.F90:421-476: global index, x, y, s, h,
+   h_small, node type) when n_out == 1, and a line "time 2 npfb n_out 1" appended to
+   <directory>/time.out.  Readable by the reference's restart loader and vtk_conv. */
+int sunset_write_dump(SunsetHandle *h, const char *directory, int n_out, double time);
+/* Restart (-Drestart): setup_domain.F90:206-242 loads h and h_small from the nodes file
+   before the neighbour search (adapt_stencils is skipped); load_restart_file,
+   setup_flow.F90:448-552, sets rho, u, v and c (psi formed from c) and the error-norm history
+   and dt from a fields dump (columns and header as sunset_get_dump returns them).  Time and
+   step count restart at 0, as there. */
+int sunset_set_lengths(SunsetHandle *h, const double *h_lengths, const double *h_small);
+int sunset_set_restart(SunsetHandle *h, const double *columns, const double *header);
+/* Binary checkpoint of the device state between steps (no counterpart in the reference):
+   the fields, the step's scalars (time, dt, step count, error-norm history) and the per-node
+   error, bit for bit, into a caller buffer of sunset_checkpoint_size bytes.  Loading it into
+   a handle built on the same node set and configuration resumes the run exactly. */
+int sunset_checkpoint_size(SunsetHandle *h, size_t *bytes);
+int sunset_save_checkpoint(SunsetHandle *h, void *buffer, size_t bytes);
+int sunset_load_checkpoint(SunsetHandle *h, const void *buffer, size_t bytes);
 
 /* Stage-kernel timing: runs `reps` fixed-dt steps at the current dt, launched kernel by
    kernel (not as a graph) with CUDA events on the handle's stream around each RK stage

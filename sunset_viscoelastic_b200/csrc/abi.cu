@@ -152,7 +152,6 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
     if (nrows <= 0 || !x || !y || !node_type || !s || !bcond) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
     if (!(xmax > xmin && ymax > ymin)) return set_err(H, SUNSET_ERR_ARG, "empty domain");
     if (int rc = set_device(H)) return rc;
-    (void)gi;
     const double hovs = hovs_for(H->cfg.forder), hovs_bound = hovs_bound_for(H->cfg.forder);
     const double hos = H->cfg.h_over_s;
     std::vector<double> vx, vy, vh, vs, vnx, vny;
@@ -163,6 +162,7 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
         if (t == 1 || t == 2)
             return set_err(H, SUNSET_ERR_SCOPE, "inflow/outflow boundary nodes are not on the device path (walls are)");
         const double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
+        H->h_gi.push_back(gi ? gi[r] : r + 1);
         vx.push_back(x[r]);
         vy.push_back(y[r]);
         vs.push_back(s[r]);
@@ -185,6 +185,7 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
                 vnx.push_back(rnx);
                 vny.push_back(rny);
                 vfd.push_back(k);
+                H->h_gi.push_back(H->h_gi[k] + j);  // setup_domain.F90:190
             }
         }
     }
@@ -658,6 +659,148 @@ int sunset_adjoint_run(SunsetHandle *sh, double dt, int nsteps, int checkpoint_e
             rc = to_reference(H, du + (size_t)f * n, SUNSET_PTR_HOST, dJ_dstate0 + (size_t)f * n);
     dfree(H, du);
     return rc;
+}
+
+int sunset_set_lengths(SunsetHandle *sh, const double *h, const double *h_small) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->domain_ok, "sunset_build_domain")) return rc;
+    if (H->nbr_ok) return set_err(H, SUNSET_ERR_ARG, "set the lengths before sunset_find_neighbours");
+    if (!h || !h_small) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (int rc = set_device(H)) return rc;
+    const int n = H->npfb;
+    std::vector<double> hv(n), hsv(n);
+    for (int i = 0; i < n; i++) {
+        const int r = H->h_perm[i];
+        if (!(h[r] > 0.0) || !(h_small[r] > 0.0) || h_small[r] > h[r])
+            return set_err(H, SUNSET_ERR_ARG, "node %d: need 0 < h_small <= h", r + 1);
+        hv[i] = h[r];
+        hsv[i] = h_small[r];
+        H->hmax = std::max(H->hmax, h[r]);
+    }
+    SUNSET_CUDA(H, cudaMemcpy(H->h, hv.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    SUNSET_CUDA(H, cudaMemcpy(H->hs, hsv.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int sunset_get_dump(SunsetHandle *sh, double *columns, double *header) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!columns || !header) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    double *cols = nullptr;
+    if (dalloc(H, &cols, 10 * (size_t)n)) return SUNSET_ERR_NOMEM;
+    int rc = dump_columns(H, cols);
+    for (int f = 0; f < 10 && !rc; f++) rc = to_reference(H, cols + (size_t)f * n, SUNSET_PTR_HOST, columns + (size_t)f * n);
+    dfree(H, cols);
+    if (rc) return rc;
+    DevScalars sc;
+    SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
+    // eflow_nm1, sum_eflow, driving_force(3): the flow-rate controller of statistics.F90 is
+    // not part of this path, so they are zero; then emax_np1, emax_n, emax_nm1, dt
+    const double hd[9] = {0.0, 0.0, 0.0, 0.0, 0.0, sc.emax_np1, sc.emax_n, sc.emax_nm1, sc.dt};
+    for (int k = 0; k < 9; k++) header[k] = hd[k];
+    return 0;
+}
+
+int sunset_write_dump(SunsetHandle *sh, const char *directory, int n_out, double time) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!directory || n_out < 0) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
+    const int n = H->npfb;
+    std::vector<double> cols(10 * (size_t)n), hd(9);
+    if (int rc = sunset_get_dump(sh, cols.data(), hd.data())) return rc;
+    const std::string dir(directory);
+    const std::string fname = dir + "/fields_10000_" + std::to_string(n_out);
+    FILE *f = fopen(fname.c_str(), "w");
+    if (!f) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", fname.c_str());
+    // output.F90:272-310, list-directed layout
+    fprintf(f, " !! header !!\n %d\n", n);
+    fprintf(f, " %.17E %.17E %.17E %.17E %.17E\n", hd[0], hd[1], hd[2], hd[3], hd[4]);
+    fprintf(f, " %.17E %.17E %.17E %.17E\n", hd[5], hd[6], hd[7], hd[8]);
+    fprintf(f, " !! end header !!\n");
+    for (int i = 0; i < n; i++) {
+        for (int c = 0; c < 10; c++) fprintf(f, " %.17E", cols[(size_t)c * n + i]);
+        fputc('\n', f);
+    }
+    const bool ok = fclose(f) == 0;
+    if (!ok) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", fname.c_str());
+    if (n_out == 1) {  // output_nodes, output.F90:421-476
+        std::vector<double> x(n), y(n), sp(n), hv(n), hsv(n);
+        std::vector<int> t(n);
+        SUNSET_CUDA(H, cudaMemcpy(x.data(), H->px, n * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(y.data(), H->py, n * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(sp.data(), H->sp, n * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(hv.data(), H->h, n * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(hsv.data(), H->hs, n * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(t.data(), H->ntype, n * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int> at(n);  // reference index -> internal
+        for (int i = 0; i < n; i++) at[H->h_perm[i]] = i;
+        const std::string nname = dir + "/nodes_10000";
+        FILE *g = fopen(nname.c_str(), "w");
+        if (!g) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", nname.c_str());
+        fprintf(g, " %d\n", n);
+        for (int r = 0; r < n; r++) {
+            const int i = at[r];
+            fprintf(g, " %d %.17E %.17E %.17E %.17E %.17E %d\n", H->h_gi[r], x[i], y[i], sp[i], hv[i], hsv[i], t[i]);
+        }
+        if (fclose(g) != 0) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", nname.c_str());
+    }
+    const std::string tname = dir + "/time.out";  // unit 21: time, dims, npfb, n_out, nprocs
+    FILE *tf = fopen(tname.c_str(), "a");
+    if (!tf) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", tname.c_str());
+    fprintf(tf, " %.17E 2 %d %d 1\n", time, n, n_out);
+    if (fclose(tf) != 0) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", tname.c_str());
+    return 0;
+}
+
+int sunset_set_restart(SunsetHandle *sh, const double *columns, const double *header) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!columns || !header) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const int n = H->npfb;
+    // load_restart_file, setup_flow.F90:448-552: rho = (rho - rho_char) + rho_char, u, v, c
+    std::vector<double> ro(n);
+    for (int i = 0; i < n; i++) ro[i] = columns[i] + 1.0;
+    const double *c = columns;
+    if (int rc = sunset_set_state(sh, ro.data(), c + n, c + 2 * (size_t)n, c + 6 * (size_t)n, c + 7 * (size_t)n,
+                                  c + 8 * (size_t)n, c + 9 * (size_t)n))
+        return rc;
+    DevScalars sc;
+    SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
+    sc.emax_np1 = header[5];
+    sc.emax_n = header[6];
+    sc.emax_nm1 = header[7];
+    sc.dt = header[8];
+    SUNSET_CUDA(H, cudaMemcpy(H->dsc, &sc, sizeof(sc), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int sunset_checkpoint_size(SunsetHandle *sh, size_t *bytes) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!bytes) return set_err(H, SUNSET_ERR_ARG, "null pointer");
+    *bytes = checkpoint_bytes(H);
+    return 0;
+}
+
+int sunset_save_checkpoint(SunsetHandle *sh, void *buffer, size_t bytes) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!buffer || bytes < checkpoint_bytes(H)) return set_err(H, SUNSET_ERR_ARG, "checkpoint buffer too small");
+    return checkpoint_save(H, buffer);
+}
+
+int sunset_load_checkpoint(SunsetHandle *sh, const void *buffer, size_t bytes) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (!buffer) return set_err(H, SUNSET_ERR_ARG, "null buffer");
+    if (int rc = state_alloc(H)) return rc;
+    if (int rc = checkpoint_load(H, buffer, bytes)) return rc;
+    H->state_ok = true;
+    return 0;
 }
 
 int sunset_time_stage_kernel(SunsetHandle *sh, int reps, double *ms_per_launch, double *bytes_per_launch) {

@@ -135,6 +135,7 @@ struct Handle {
     double xmin = 0, xmax = 0, ymin = 0, ymax = 0, smax = 0, h0 = 0, h2 = 0, h3 = 0, hmax = 0;
     int bc[4] = {0, 0, 0, 0};
     std::vector<int> h_perm, h_iperm;  // internal <-> reference
+    std::vector<int> h_gi;             // global index of each node (reference order; FD rows: parent's + j)
     bool domain_ok = false, nbr_ok = false, w_ok = false, bw_ok = false, sums_ok = false, fc_ok = false;
     bool state_ok = false;
 
@@ -192,6 +193,7 @@ struct Handle {
     // and the error accumulator in FP32
     float *dreg32[7] = {}, *eacc32[7] = {};
     double *partials = nullptr;
+    double *alpha = nullptr;  // per-node step error of the last step (output.F90 alpha_out)
     int npart = 0;
     DevScalars *dsc = nullptr;
     double *tmpd = nullptr;  // scratch, 4*npfb doubles
@@ -281,6 +283,11 @@ int op_gradient(Handle *H, const double *phi, double *gx, double *gy);
 int op_laplacian(Handle *H, const double *phi, double *lap);
 int op_filter(Handle *H, const double *phi, double *out, int term_only);
 int reduce_ke_mass(Handle *H, double *ke, double *mass);
+// Field dumps and checkpoints (step.cu)
+int dump_columns(Handle *H, double *out);  // 10 x npfb, internal order, on the device
+size_t checkpoint_bytes(const Handle *H);
+int checkpoint_save(Handle *H, void *buf);
+int checkpoint_load(Handle *H, const void *buf, size_t bytes);
 int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes);
 int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *dtheta, double *dU0);
 int adjoint_apply_D(Handle *H, int which, const double *gbar, double *out);

@@ -18,6 +18,7 @@
 // order of stream.cu, which changes only the rounding (and libm's exp, log, cos may differ
 // from glibc in the last bit).
 #include <algorithm>
+#include <cstring>
 #include <thread>
 #include <type_traits>
 
@@ -54,6 +55,7 @@ struct StageArgs {
     float *dreg[7], *eacc32[7];  // mixed precision
     DevScalars *sc;
     double *partials;
+    double *alpha;  // per-node step error (stage 3), or null
     double *gsave;  // log-conformation FP64 stages of the adjoint's recording: the 18 stencil
                     // sums of each node (adjoint.cuh order, arrays of npfb), else null
     int stage;  // 0..3; 4 = rhs only
@@ -530,7 +532,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                     }
                 }
             } else {
-                double en = 0.0;
+                double en = 0.0, al = 0.0;
                 // Cholesky FENE-P: the conformation errors scaled by the node's 1/sqrt(f)
                 // (step.F90:442-452, applied per node; see the design notes)
                 double conf_scale = 1.0;
@@ -548,11 +550,13 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                         E = A.eacc[f][i] + RKbmbh * rr[f];
                     }
                     double t = fabs(E) * norm;
+                    if (f < 6) al = (t > al) ? t : al;  // alpha_out: rho, momentum, xx, xy, yy (step.F90:455-457)
                     if (f >= 3) t = t * conf_scale;
                     en = (t > en) ? t : en;
                     if (t != t) en = t;
                 }
                 emax_bits = dbits(en);
+                if (A.alpha) A.alpha[i] = al;
             }
             if (wall) { Un[1] = 0.0; Un[2] = 0.0; }  // apply_time_dependent_bounds, characteristic_boundaries.F90:200-206
             const Fields &O = A.out;
@@ -990,6 +994,7 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     }
     A.sc = H->dsc;
     A.partials = H->partials;
+    A.alpha = H->alpha;
     A.stage = stage;
     return A;
 }
@@ -1154,6 +1159,8 @@ int state_alloc(Handle *H) {
             if (dalloc(H, &H->reg[f], n) || dalloc(H, &H->eacc[f], n)) return SUNSET_ERR_NOMEM;
         }
     }
+    if (dalloc(H, &H->alpha, n)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->alpha, 0, n * sizeof(double), H->stream));
     const int nthr = H->nslices * kSlice;
     H->npart = (nthr + 127) / 128 + 1;
     if (dalloc(H, &H->partials, 2 * (size_t)H->npart + 16) || dalloc(H, &H->dsc, 1) || dalloc(H, &H->tmpd, 4 * (size_t)n))
@@ -1338,6 +1345,140 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     return 0;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Field dumps (output.F90:184-370): per node rho - rho_char, u, v, vorticity, Q criterion,
+// the step error alpha_out, cxx, cxy, cyy, czz.  On wall nodes the velocity gradient is in
+// the wall's normal-tangent frame, so vorticity and Q are rotated as output.F90:229-241 does.
+// ---------------------------------------------------------------------------------------
+namespace {
+__global__ void k_dump(int n, Fields F, const double *gux, const double *guy, const double *gvx, const double *gvy,
+                       const int *ntype, const double *rnx, const double *rny, int has_walls, const double *alpha,
+                       double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double ux = gux[i], uy = guy[i], vx = gvx[i], vy = gvy[i];
+    double vort = vx - uy;
+    double q = (-(0.5 * (ux * ux)) - 0.5 * (vy * vy)) - uy * vx;
+    if (has_walls && ntype[i] == 0) {
+        const double xn = rnx[i], yn = rny[i];
+        vort = xn * (vx - uy) - yn * (ux + vy);
+        const double a = xn * ux - yn * uy, b = yn * vx + xn * vy;
+        q = (-(0.5 * (a * a)) - 0.5 * (b * b)) - (yn * ux + xn * uy) * (xn * vx - yn * vy);
+    }
+    const double col[10] = {-cK.rho_char + F.ro[i], F.u[i], F.v[i], vort, q, alpha ? alpha[i] : 0.0,
+                            F.c[0][i], F.c[1][i], F.c[2][i], F.c[3][i]};
+#pragma unroll
+    for (int f = 0; f < 10; f++) out[(size_t)f * n + i] = col[f];
+}
+
+struct CheckpointHeader {
+    char magic[8];
+    int version, npfb, form, precision, fenep, nfields;
+    double xsum, ysum;  // fingerprint of the node set
+};
+}  // namespace
+
+int dump_columns(Handle *H, double *out) {
+    const int n = H->npfb;
+    const Fields &F = H->buf[H->cur];
+    double *g = H->tmpd;  // 4 x npfb scratch
+    if (int rc = op_gradient(H, F.u, g, g + n)) return rc;
+    if (int rc = op_gradient(H, F.v, g + 2 * (size_t)n, g + 3 * (size_t)n)) return rc;
+    k_dump<<<(n + 127) / 128, 128, 0, H->stream>>>(n, F, g, g + n, g + 2 * (size_t)n, g + 3 * (size_t)n, H->ntype,
+                                                   H->rnx, H->rny, H->nb > 0, H->alpha, out);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+// Checkpoint: the device state between steps, bit for bit -- the 13 fields of the current
+// buffer (and the FENE-P function where it is kept), the step's scalars (time, dt, itime,
+// error-norm history) and the per-node step error, in the internal node order, behind a
+// header that names the configuration and fingerprints the node set.  The RK registers are
+// rebuilt by every step, so they are not part of it.
+static void checkpoint_arrays(const Handle *H, double *const *&arr, int &na, double *tmp[16]) {
+    const Fields &F = H->buf[H->cur];
+    na = 0;
+    const double *src[14] = {F.ro, F.rou, F.rov, F.u, F.v, F.q[0], F.q[1], F.q[2], F.q[3], F.c[0], F.c[1], F.c[2], F.c[3], F.f};
+    for (int k = 0; k < 13; k++) {
+        if (H->cfg.form == SUNSET_FORM_DI && k >= 9) break;  // DI: c aliases q
+        tmp[na++] = const_cast<double *>(src[k]);
+    }
+    if (F.f) tmp[na++] = F.f;
+    tmp[na++] = H->alpha;
+    arr = tmp;
+}
+
+size_t checkpoint_bytes(const Handle *H) {
+    double *tmp[16];
+    double *const *arr;
+    int na;
+    checkpoint_arrays(H, arr, na, tmp);
+    return sizeof(CheckpointHeader) + sizeof(DevScalars) + (size_t)na * H->npfb * sizeof(double);
+}
+
+static int node_fingerprint(Handle *H, double *xs, double *ys) {
+    std::vector<double> x(H->npfb), y(H->npfb);
+    SUNSET_CUDA(H, cudaMemcpy(x.data(), H->px, H->npfb * sizeof(double), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(y.data(), H->py, H->npfb * sizeof(double), cudaMemcpyDeviceToHost));
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < H->npfb; i++) { a = a + x[i]; b = b + y[i]; }
+    *xs = a;
+    *ys = b;
+    return 0;
+}
+
+int checkpoint_save(Handle *H, void *buf) {
+    double *tmp[16];
+    double *const *arr;
+    int na;
+    checkpoint_arrays(H, arr, na, tmp);
+    CheckpointHeader hd{};
+    memcpy(hd.magic, "SUNSETCK", 8);
+    hd.version = 1;
+    hd.npfb = H->npfb;
+    hd.form = H->cfg.form;
+    hd.precision = H->cfg.precision;
+    hd.fenep = H->cfg.fenep;
+    hd.nfields = na;
+    if (int rc = node_fingerprint(H, &hd.xsum, &hd.ysum)) return rc;
+    char *p = static_cast<char *>(buf);
+    memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    SUNSET_CUDA(H, cudaMemcpyAsync(p, H->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, H->stream));
+    p += sizeof(DevScalars);
+    for (int k = 0; k < na; k++) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(p, arr[k], H->npfb * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+        p += H->npfb * sizeof(double);
+    }
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+int checkpoint_load(Handle *H, const void *buf, size_t bytes) {
+    double *tmp[16];
+    double *const *arr;
+    int na;
+    checkpoint_arrays(H, arr, na, tmp);
+    if (bytes != checkpoint_bytes(H)) return set_err(H, SUNSET_ERR_ARG, "checkpoint of %zu bytes, expected %zu", bytes, checkpoint_bytes(H));
+    CheckpointHeader hd;
+    const char *p = static_cast<const char *>(buf);
+    memcpy(&hd, p, sizeof(hd));
+    double xs, ys;
+    if (int rc = node_fingerprint(H, &xs, &ys)) return rc;
+    if (memcmp(hd.magic, "SUNSETCK", 8) != 0 || hd.version != 1 || hd.npfb != H->npfb || hd.form != H->cfg.form ||
+        hd.precision != H->cfg.precision || hd.fenep != H->cfg.fenep || hd.nfields != na || hd.xsum != xs || hd.ysum != ys)
+        return set_err(H, SUNSET_ERR_ARG, "checkpoint written for another configuration or node set");
+    p += sizeof(hd);
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, p, sizeof(DevScalars), cudaMemcpyHostToDevice, H->stream));
+    p += sizeof(DevScalars);
+    for (int k = 0; k < na; k++) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(arr[k], p, H->npfb * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+        p += H->npfb * sizeof(double);
+    }
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return upload_consts(H);
+}
 
 // =======================================================================================
 // Adjoint of the fixed-dt time step (log-conformation form, periodic node sets, FP64).

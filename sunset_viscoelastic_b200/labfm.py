@@ -19,6 +19,8 @@ FORMS = {"di": 0, "chl": 1, "lc": 2, "newt": 3}
 PRECISION = {"fp64": 0, "mixed": 1}
 STATE_FIELDS = ["ro", "rou", "rov", "u", "v", "psixx", "psixy", "psiyy", "psizz", "cxx", "cxy", "cyy", "czz"]
 RHS_FIELDS = ["ro", "rou", "rov", "xx", "xy", "yy", "zz"]
+# columns of a fields dump (output.F90:299-301)
+DUMP_COLUMNS = ["ro_minus_rho_char", "u", "v", "vort", "qcrit", "alpha", "cxx", "cxy", "cyy", "czz"]
 
 # C-ABI symbols declared in include/sunset_gpu.h
 ABI_SYMBOLS = [
@@ -31,6 +33,8 @@ ABI_SYMBOLS = [
     "sunset_set_time", "sunset_kinetic_energy", "sunset_mass", "sunset_synchronize", "sunset_run_host",
     "sunset_time_stage_kernel", "sunset_step_timed", "sunset_kinetic_energy_noalloc",
     "sunset_adjoint_run", "sunset_adjoint_apply_D", "sunset_adapt_stencils", "sunset_get_lengths",
+    "sunset_set_lengths", "sunset_get_dump", "sunset_write_dump", "sunset_set_restart", "sunset_checkpoint_size",
+    "sunset_save_checkpoint", "sunset_load_checkpoint",
 ]
 
 
@@ -78,6 +82,13 @@ def load_library(build_if_missing: bool = True):
               "sunset_calc_labf_sums", "sunset_filter_coefficients", "sunset_synchronize", "sunset_adapt_stencils"]:
         getattr(L, n).argtypes = [P]
     L.sunset_get_lengths.argtypes = [P, dp, dp]
+    L.sunset_set_lengths.argtypes = [P, dp, dp]
+    L.sunset_get_dump.argtypes = [P, dp, dp]
+    L.sunset_write_dump.argtypes = [P, C.c_char_p, C.c_int, C.c_double]
+    L.sunset_set_restart.argtypes = [P, dp, dp]
+    L.sunset_checkpoint_size.argtypes = [P, C.POINTER(C.c_size_t)]
+    L.sunset_save_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
+    L.sunset_load_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
     L.sunset_get_neighbours.argtypes = [P, ip, ip, ip]
     L.sunset_get_weights.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
     for n in ["sunset_calc_gradient", "sunset_calc_laplacian", "sunset_calc_filtered_var", "sunset_calc_filter_term"]:
@@ -194,6 +205,41 @@ class Sunset:
         h, hs = np.zeros(n), np.zeros(n)
         self._chk(self.L.sunset_get_lengths(self.h, h, hs))
         return h, hs
+
+    def set_lengths(self, h, h_small):
+        """Restart: h and h_small of the npfb nodes (reference order), before find_neighbours."""
+        f = lambda a: np.ascontiguousarray(a, np.float64)
+        self._chk(self.L.sunset_set_lengths(self.h, f(h), f(h_small)))
+
+    def dump(self):
+        """(columns dict of output_layer's 10 columns, header array of 9) in reference order."""
+        n = self.sizes()[1]
+        cols, hd = np.zeros(10 * n), np.zeros(9)
+        self._chk(self.L.sunset_get_dump(self.h, cols, hd))
+        cols = cols.reshape(10, n)
+        return {k: cols[i].copy() for i, k in enumerate(DUMP_COLUMNS)}, hd
+
+    def write_dump(self, directory, n_out, time=0.0):
+        self._chk(self.L.sunset_write_dump(self.h, str(directory).encode(), int(n_out), float(time)))
+
+    def set_restart(self, columns, header):
+        """load_restart_file from dump columns (dict or 10 x npfb array) and header."""
+        if isinstance(columns, dict):
+            columns = np.stack([columns[k] for k in DUMP_COLUMNS])
+        self._chk(self.L.sunset_set_restart(self.h, np.ascontiguousarray(columns, np.float64).ravel(),
+                                            np.ascontiguousarray(header, np.float64)))
+
+    def save_checkpoint(self):
+        """The device state between steps, bit for bit, as bytes."""
+        nb = C.c_size_t()
+        self._chk(self.L.sunset_checkpoint_size(self.h, C.byref(nb)))
+        buf = C.create_string_buffer(nb.value)
+        self._chk(self.L.sunset_save_checkpoint(self.h, buf, nb.value))
+        return buf.raw
+
+    def load_checkpoint(self, data):
+        buf = C.create_string_buffer(data, len(data))
+        self._chk(self.L.sunset_load_checkpoint(self.h, buf, len(data)))
 
     def neighbours(self):
         _, npfb, _, nplink = self.sizes()
