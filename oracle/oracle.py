@@ -25,7 +25,9 @@ class OrConfig(C.Structure):
                 ("L_char", C.c_double), ("U_char", C.c_double), ("Re", C.c_double), ("Wi", C.c_double),
                 ("beta", C.c_double), ("epsPTT", C.c_double), ("fenep_l2", C.c_double),
                 ("Mdiff", C.c_double), ("Ma", C.c_double), ("grav", C.c_double * 3),
-                ("h_over_s", C.c_double)]
+                ("h_over_s", C.c_double), ("inflow_type", C.c_int), ("inflow_velocity_control", C.c_int),
+                ("u_inflow_start", C.c_double), ("u_inflow_end", C.c_double), ("ramp_time", C.c_double),
+                ("vpid", C.c_int)]
 
 
 def build() -> str:
@@ -71,6 +73,8 @@ def lib():
         L.or_step.argtypes = [P, C.c_double, C.c_int, C.c_int]
         L.or_get_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), dp]
         L.or_set_time.argtypes = [P, C.c_double, C.c_double, C.c_int, dp]
+        L.or_get_flow_control.argtypes = [P, dp]
+        L.or_set_flow_control.argtypes = [P, dp]
         L.or_kinetic_energy.restype = C.c_double
         L.or_kinetic_energy.argtypes = [P]
         L.or_mass.restype = C.c_double
@@ -112,7 +116,9 @@ class Oracle:
 
     def __init__(self, form="di", order=4, forder=None, Re=1.0, Wi=1.0, beta=0.5, epsPTT=0.0, Ma=0.1,
                  fenep=False, fenep_l2=1e30, Mdiff=0.0, grav=(0.0, 0.0, 0.0), mcorr=True,
-                 kolmogorov_forcing=-1, di_full_gradients=True, h_over_s=0.0, L_char=1.0, U_char=1.0):
+                 kolmogorov_forcing=-1, di_full_gradients=True, h_over_s=0.0, L_char=1.0, U_char=1.0,
+                 inflow_type=1, inflow_velocity_control=0, u_inflow_start=0.0, u_inflow_end=1.0, ramp_time=1.0,
+                 vpid=False):
         cfg = OrConfig()
         cfg.form = FORMS[form]
         cfg.fenep = int(fenep)
@@ -126,6 +132,9 @@ class Oracle:
         for k in range(3):
             cfg.grav[k] = grav[k]
         cfg.h_over_s = h_over_s
+        cfg.inflow_type, cfg.inflow_velocity_control = int(inflow_type), int(inflow_velocity_control)
+        cfg.u_inflow_start, cfg.u_inflow_end, cfg.ramp_time = u_inflow_start, u_inflow_end, ramp_time
+        cfg.vpid = int(bool(vpid))
         self.cfg = cfg
         self.L = lib()
         self.h = self.L.or_create(C.byref(cfg))
@@ -277,6 +286,15 @@ class Oracle:
 
     def set_time(self, time, dt, itime, emax):
         self.L.or_set_time(self.h, float(time), float(dt), int(itime), np.ascontiguousarray(emax, np.float64))
+
+    def flow_control(self):
+        out = np.zeros(5)
+        self.L.or_get_flow_control(self.h, out)
+        return dict(eflow_nm1=out[0], sum_eflow=out[1], driving_force=out[2:5].copy())
+
+    def set_flow_control(self, eflow_nm1, sum_eflow, driving_force):
+        v = np.array([eflow_nm1, sum_eflow, *np.asarray(driving_force, np.float64)[:3]])
+        self.L.or_set_flow_control(self.h, v)
 
     def kinetic_energy(self):
         return self.L.or_kinetic_energy(self.h)

@@ -98,6 +98,8 @@ struct OrSim {
     double emax_nm1, emax_n, emax_np1;
     double ero_norm, erou_norm, exx_norm;
     double driving_force[3];
+    double *u_inflow_local; /* nb: inflow velocity of each boundary node (common_vars.F90:111) */
+    double eflow_nm1, sum_eflow; /* flow-rate controller (common_vars.F90:82) */
 };
 
 static int fail(OrSim *s, const char *fmt, ...) {
@@ -174,7 +176,7 @@ void or_destroy(OrSim *s) {
     free_links(s);
     FREE(s->rx); FREE(s->ry); FREE(s->h); FREE(s->hs); FREE(s->sp); FREE(s->rnx); FREE(s->rny);
     FREE(s->type); FREE(s->fd_parent); FREE(s->gi); FREE(s->irel); FREE(s->vrel);
-    FREE(s->internal_list); FREE(s->boundary_list);
+    FREE(s->internal_list); FREE(s->boundary_list); FREE(s->u_inflow_local);
     free(s);
 }
 
@@ -1900,10 +1902,41 @@ static void get_c_from_psi(OrSim *s) { /* step.F90:531-567 */
     }
 }
 
-static void apply_time_dependent_bounds(OrSim *s) { /* characteristic_boundaries.F90:191-257 (walls) */
+/* update_u_inflow, characteristic_boundaries.F90:262-300: with velocity control the inflow
+   velocity ramps linearly to u_inflow_end over ramp_time; it is updated only while
+   time <= ramp_time, so it keeps its last ramp value after that */
+static void update_u_inflow(OrSim *s) {
+    if (s->cfg.inflow_velocity_control != 1) return;
+    const double t = s->time, rt = s->cfg.ramp_time;
+    double um;
+    if (t <= rt) um = s->cfg.u_inflow_start + ((s->cfg.u_inflow_end - s->cfg.u_inflow_start) * t) / rt;
+    else um = s->cfg.u_inflow_end;
+    if (t <= rt)
+        for (int jj = 0; jj < s->nb; jj++)
+            if (s->type[s->boundary_list[jj]] == 1) s->u_inflow_local[jj] = um;
+}
+
+static void apply_time_dependent_bounds(OrSim *s) { /* characteristic_boundaries.F90:191-257 */
+    update_u_inflow(s);
     for (int jj = 0; jj < s->nb; jj++) {
         int i = s->boundary_list[jj];
         if (s->type[i] == 0) { s->rou[i] = 0.0; s->rov[i] = 0.0; s->row[i] = 0.0; }
+        else if (s->type[i] == 1 && s->cfg.inflow_type == 1) { /* hard inflow: prescribed velocity */
+            s->rou[i] = s->u_inflow_local[jj] * s->ro[i];
+            s->rov[i] = 0.0;
+            s->row[i] = 0.0;
+        }
+    }
+}
+
+/* initial_solution, setup_flow.F90:48-50,128-138: u_char everywhere, then the initial u of
+   each inflow node */
+static void init_u_inflow(OrSim *s) {
+    free(s->u_inflow_local);
+    s->u_inflow_local = (double *)xcalloc(s->nb > 0 ? s->nb : 1, sizeof(double));
+    for (int jj = 0; jj < s->nb; jj++) {
+        int i = s->boundary_list[jj];
+        s->u_inflow_local[jj] = s->type[i] == 1 ? s->u[i] : s->cfg.U_char;
     }
 }
 
@@ -1943,6 +1976,8 @@ int or_set_state(OrSim *s, const double *ro, const double *u, const double *v, c
     s->time = 0.0; s->itime = 0; s->dt = 1.0e-6;
     s->emax_np1 = pid_tol; s->emax_n = pid_tol; s->emax_nm1 = pid_tol;
     s->driving_force[0] = s->driving_force[1] = s->driving_force[2] = 0.0;
+    s->eflow_nm1 = 1.0; s->sum_eflow = 0.0; /* setup_flow.F90:165-169 */
+    init_u_inflow(s);
     return 0;
 }
 
@@ -1961,6 +1996,7 @@ int or_set_raw_state(OrSim *s, const double *ro, const double *rou, const double
     reapply_mirror_bcs(s);
     get_velocity_from_momentum(s);
     get_c_from_psi(s);
+    if (!s->u_inflow_local) init_u_inflow(s);
     return 0;
 }
 
@@ -2093,6 +2129,25 @@ static void calc_rhs_rovel(OrSim *s, RhsWork *W) {
             L[3] = un * (0.0 * xn + 0.0 * yn);
             L[4] = (0.5 * (un + c)) * (dpdn + (ro * c) * dundn);
             s->rhs_rou[i] = 0.0; s->rhs_rov[i] = 0.0; s->rhs_row[i] = 0.0;
+        } else { /* inflow/outflow in the x-y frame, rhs_di.F90:311-359 (rhs.F90, rhs_lc.F90 alike;
+                    no Kolmogorov forcing there) */
+            const double u = s->u[i], v = s->v[i], w = s->w[i];
+            L[0] = (0.5 * (u - c)) * (dpdn - (ro * c) * W->gu_x[i]);
+            L[1] = u * (W->gro_x[i] - (W->gp_x[i] / c) / c);
+            L[2] = u * W->gv_x[i];
+            L[3] = u * 0.0;
+            L[4] = (0.5 * (u + c)) * (dpdn + (ro * c) * W->gu_x[i]);
+            double fvu = coef_solvent * W->lapu[i], fvv = coef_solvent * W->lapv[i];
+            if (s->cfg.form != OR_FORM_NEWT) {
+                double pu, pv;
+                polymeric_divergence(s, W, i, &pu, &pv);
+                fvu = fvu + coef_polymeric * pu;
+                fvv = fvv + coef_polymeric * pv;
+            }
+            const double bfu = ro * (g[0] + df[0]), bfv = ro * (g[1] + df[1]), bfw = ro * (g[2] + df[2]);
+            s->rhs_rou[i] = ((-(v * W->gu_y[i]) - w * 0.0) + fvu) + bfu;
+            s->rhs_rov[i] = (((-(v * W->gv_y[i]) - w * 0.0) - W->gp_y[i]) + fvv) + bfv;
+            s->rhs_row[i] = (((-(v * 0.0) - w * 0.0) - 0.0) + coef_solvent * 0.0) + bfw;
         }
     }
 }
@@ -2306,11 +2361,42 @@ static void calc_rhs_logconf(OrSim *s, RhsWork *W) {
 /* specify_characteristics_isothermal_wall (characteristic_boundaries.F90:27-52) and the
    boundary update of calc_rhs_nscbc (rhs_di.F90:601-665). */
 static void calc_rhs_nscbc(OrSim *s, RhsWork *W) {
+    const double nscbc = 2.87e-1;                                  /* common_parameter.F90:71 */
+    const double Lx = (s->xmax - s->xmin) * s->cfg.L_char;         /* setup_domain.F90:98 */
+    const double p_in = s->rho_char * s->csq, p_out = s->rho_char * s->csq; /* load_data.F90:147-148 */
     for (int jj = 0; jj < s->nb; jj++) {
         int i = s->boundary_list[jj];
         double *L = W->L + 5 * jj;
-        if (s->type[i] == 0) L[4] = L[0];
-        double c = sqrt(s->csq);
+        const double c = sqrt(s->csq), u = s->u[i], v = s->v[i], w = s->w[i], p = s->p[i], ro = s->ro[i];
+        const double uin = s->u_inflow_local[jj];
+        if (s->type[i] == 0) {
+            L[4] = L[0]; /* specify_characteristics_isothermal_wall, :27-52 */
+        } else if (s->type[i] == 1) {
+            if (s->cfg.inflow_type == 1) { /* specify_characteristics_hard_inflow, :82-110 */
+                L[1] = 0.0; L[2] = 0.0; L[3] = 0.0; L[4] = L[0];
+            } else if (s->cfg.inflow_type == 2) { /* specify_characteristics_inflow_outflow, :112-150 */
+                if (u > 0.0) {
+                    L[1] = 0.0;
+                    L[2] = ((v * nscbc) * c) / Lx;
+                    L[3] = ((w * nscbc) * c) / Lx;
+                    L[4] = ((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx;
+                } else {
+                    L[1] = 0.0;
+                    L[4] = (((((p - p_in) * nscbc) * c) * 1.0) / 2.0) / Lx;
+                }
+            } else { /* specify_characteristics_soft_inflow, :54-80 */
+                L[1] = 0.0;
+                L[2] = (((((v * nscbc) * c) / Lx) - v * W->gv_y[i]) - w * 0.0) - W->gp_y[i] / ro;
+                L[3] = ((w * nscbc) * c) / Lx + s->rhs_row[i];
+                L[4] = (((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx -
+                        0.5 * (((v * W->gp_y[i]) + (p * W->gv_y[i])) + (((ro * c) * v) * W->gu_y[i]))) -
+                       0.5 * (((w * 0.0) + (p * 0.0)) + (((ro * c) * w) * 0.0));
+            }
+        } else if (s->type[i] == 2) { /* specify_characteristics_outflow, :152-189 */
+            if (u < c) L[0] = (((((p - p_out) * nscbc) * c) * 1.0) / 2.0) / Lx;
+            L[1] = 0.0;
+            if (u <= 0.0) { L[1] = 0.0; L[2] = 0.0; L[3] = 0.0; }
+        }
         double tmp_scal = ((((c * c) * L[1] + L[4]) + L[0]) / c) / c;
         s->rhs_ro[i] = s->rhs_ro[i] - tmp_scal;
         s->rhs_rou[i] = (s->rhs_rou[i] - s->u[i] * tmp_scal) - (L[4] - L[0]) / c;
@@ -2321,9 +2407,7 @@ static void calc_rhs_nscbc(OrSim *s, RhsWork *W) {
 
 static int calc_all_rhs(OrSim *s) {
     const int form = s->cfg.form, npfb = s->npfb;
-    for (int jj = 0; jj < s->nb; jj++)
-        if (s->type[s->boundary_list[jj]] != 0)
-            return fail(s, "inflow/outflow characteristics are outside the restated scope");
+    if (!s->u_inflow_local) init_u_inflow(s);
     RhsWork W;
     rhs_work_alloc(s, &W);
     memset(s->rhs_ro, 0, sizeof(double) * npfb); memset(s->rhs_rou, 0, sizeof(double) * npfb);
@@ -2586,6 +2670,42 @@ static void set_tstep_pid(OrSim *s) {
     if (s->dt > dt_max) s->dt = dt_max;
 }
 
+/* velocity_control with -Dvpid (statistics.F90:214-303), called after every step
+   (sunset.F90:104, statistics.F90:80-82): a PID controller drives the volume-mean x velocity
+   to L_domain_y L_domain_x / tot_vol through driving_force(1).  The reference sums over the
+   nodes in an OpenMP reduction (order unspecified); here in node order. */
+static void velocity_control(OrSim *s) {
+    double tot_vol = 0.0, tot_u = 0.0;
+    for (int i = 0; i < s->npfb; i++) {
+        const double dvi = s->vol[i];
+        tot_vol = tot_vol + dvi;
+        tot_u = tot_u + s->u[i] * dvi;
+    }
+    tot_u = tot_u / tot_vol;
+    const double Lx = (s->xmax - s->xmin) * s->cfg.L_char, Ly = (s->ymax - s->ymin) * s->cfg.L_char;
+    const double eflow_n = 1.0 - (tot_u * tot_vol) / (Ly * Lx);
+    s->sum_eflow = s->sum_eflow + eflow_n * s->dt;
+    const double deflowdt = (eflow_n - s->eflow_nm1) / s->dt;
+    const double facA = ((((0.5 * 0.5) * 0.5) * 1.0) * 2.0) * 2.0;
+    const double facB = facA / 0.4, facC = facA * 0.02;
+    double df = ((facA * eflow_n) + facB * s->sum_eflow) + facC * deflowdt;
+    df = (500.0 < df) ? 500.0 : df;
+    df = (-500.0 > df) ? -500.0 : df;
+    s->driving_force[0] = df;
+    s->eflow_nm1 = eflow_n;
+}
+
+int or_get_flow_control(OrSim *s, double *out) {
+    out[0] = s->eflow_nm1; out[1] = s->sum_eflow;
+    out[2] = s->driving_force[0]; out[3] = s->driving_force[1]; out[4] = s->driving_force[2];
+    return 0;
+}
+int or_set_flow_control(OrSim *s, const double *in) {
+    s->eflow_nm1 = in[0]; s->sum_eflow = in[1];
+    s->driving_force[0] = in[2]; s->driving_force[1] = in[3]; s->driving_force[2] = in[4];
+    return 0;
+}
+
 int or_step(OrSim *s, double dt, int nsteps, int pid) {
     if (!s->have_weights || !s->ro) return fail(s, "weights or state missing");
     for (int n = 0; n < nsteps; n++) {
@@ -2597,6 +2717,10 @@ int or_step(OrSim *s, double dt, int nsteps, int pid) {
         }
         if (step_rk3_4s_2r_ee(s)) return -1;
         s->itime++;
+        /* statistics_control after the step: the controller with -Dvpid, else the driving
+           force zeroed (statistics.F90:80-90,288; a restart may have loaded one) */
+        if (s->cfg.vpid) velocity_control(s);
+        else s->driving_force[0] = s->driving_force[1] = s->driving_force[2] = 0.0;
     }
     return 0;
 }

@@ -40,6 +40,13 @@ typedef struct {
     double grav[3];
     double h_over_s;        /* >0: h = h_small = h_over_s*s for every node (fixed-radius
                                harness); 0: reference hovs/hovs_bound (common_parameter.F90:44-66) */
+    /* inflow boundaries (control.in, load_data.F90:150-152): inflow_type 0 soft
+       (non-reflecting), 1 hard, 2 pressure-tracking inflow-outflow; inflow_velocity_control 1
+       ramps the inflow velocity from u_inflow_start to u_inflow_end over ramp_time */
+    int inflow_type, inflow_velocity_control;
+    double u_inflow_start, u_inflow_end, ramp_time;
+    int vpid;               /* -Dvpid: PID control of the mean x velocity through driving_force(1)
+                               after every step (statistics.F90:214-303) */
 } OrConfig;
 
 typedef struct OrSim OrSim;
@@ -96,6 +103,9 @@ int or_set_tstep(OrSim *s, double *dt_cfl, double *dt_parabolic);
 int or_step(OrSim *s, double dt, int nsteps, int pid);
 int or_get_time(OrSim *s, double *time, double *dt, int *itime, double *emax /* 3 */);
 int or_set_time(OrSim *s, double time, double dt, int itime, const double *emax /* 3 */);
+/* the flow-rate controller's state: eflow_nm1, sum_eflow, driving_force(1:3) */
+int or_get_flow_control(OrSim *s, double *out /* 5 */);
+int or_set_flow_control(OrSim *s, const double *in /* 5 */);
 double or_kinetic_energy(OrSim *s);
 double or_mass(OrSim *s);
 

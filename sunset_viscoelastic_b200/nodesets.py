@@ -126,6 +126,47 @@ def channel(ny_cells: int, lx: float = 1.0, ly: float = 1.0, jitter: float = 0.3
                    ymin=0.0, ymax=ly, bcond=(1, 1, 0, 0), gi=_with_gaps(t))
 
 
+def inflow_channel(ny_cells: int, lx: float = 2.0, ly: float = 1.0, ybc: int = 1, jitter: float = 0.3,
+                   seed: int = 12345) -> NodeSet:
+    """Inflow/outflow tube [0, lx] x [0, ly] in the layout of the reference generator's
+    in/out cases (gen/datclass.F90 cases 5 and 6): an inflow (node_type 1, normal +x) at
+    x = 0, an outflow (node_type 2, normal -x) at x = lx, and periodic (ybc = 1) or symmetric
+    (ybc = 2) conditions in y, so no wall meets an inflow.  Spacing s = ly / ny_cells; the
+    inflow and outflow nodes sit at y = (j + 1/2) s and the reader adds their FD rows at
+    1..4 s along the normal; the interior is a jittered lattice on the x cells 5 .. n - 6."""
+    if ybc not in (1, 2):
+        raise ValueError("ybc must be 1 (periodic) or 2 (symmetric)")
+    s = ly / ny_cells
+    nxc = int(round(lx / s))
+    ys = (np.arange(ny_cells) + 0.5) * s
+    rng = np.random.default_rng(seed)
+    xj = (np.arange(5, nxc - 5) + 0.5) * s
+    ix, iy = np.meshgrid(xj, ys, indexing="xy")
+    n_int = ix.size
+    xi = ix.ravel() + rng.uniform(-jitter * s, jitter * s, n_int)
+    yi = iy.ravel() + rng.uniform(-jitter * s, jitter * s, n_int)
+    ni = len(ys)
+    x = np.concatenate([np.zeros(ni), xi, np.full(ni, lx)])
+    y = np.concatenate([ys, yi, ys])
+    t = np.concatenate([np.ones(ni, np.int32), np.full(n_int, 999, np.int32), np.full(ni, 2, np.int32)])
+    nx = np.concatenate([np.ones(ni), np.zeros(n_int), -np.ones(ni)])
+    ny = np.zeros(len(x))
+    return NodeSet(x=x, y=y, node_type=t, nx=nx, ny=ny, s=np.full(len(x), s), xmin=0.0, xmax=lx,
+                   ymin=0.0, ymax=ly, bcond=(0, 0, ybc, ybc), gi=_with_gaps(t))
+
+
+def inflow_state(ns, u0: float = 1.0, amp: float = 0.05, ly: float = 1.0):
+    """Uniform stream u0 in x with a smooth perturbation that respects both y conditions
+    (v odd about y = 0 and y = ly, everything else even), and a smooth positive-definite
+    conformation: u = u0 (1 + amp cos(2 pi y / ly) cos(pi x)), v = amp u0 sin(2 pi y / ly)
+    sin(pi x), rho = 1 + amp/10 cos(pi x).  ns: any object with the reader's x, y."""
+    x, y = ns.x, ns.y
+    ky = 2.0 * np.pi / ly
+    return dict(ro=1.0 + 0.1 * amp * np.cos(np.pi * x), u=u0 * (1.0 + amp * np.cos(ky * y) * np.cos(np.pi * x)),
+                v=amp * u0 * np.sin(ky * y) * np.sin(np.pi * x), cxx=1.2 + 0.1 * np.cos(ky * y),
+                cxy=0.05 * np.sin(ky * y) * np.cos(np.pi * x), cyy=1.1 + 0.05 * np.cos(np.pi * x), czz=np.ones(len(x)))
+
+
 def cylinder_channel(R: float = 1.0, half_length: float = 15.0, half_height: float = 2.0, s_min_frac: float = 1 / 64,
                      s_max_frac: float = 1 / 16, growth: float = 0.1, jitter: float = 0.3,
                      seed: int = 12345) -> NodeSet:
