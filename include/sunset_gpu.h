@@ -57,6 +57,15 @@ typedef struct {
     double h_over_s;        /* >0: h = h_small = h_over_s*s (fixed radius 2h); 0: reference
                                hovs/hovs_bound (common_parameter.F90:44-66) */
     int device;             /* CUDA device ordinal */
+    /* inflow boundaries (control.in, load_data.F90:150-152): inflow_type 0 soft
+       (non-reflecting), 1 hard (prescribed velocity), 2 pressure-tracking inflow-outflow;
+       inflow_velocity_control 1 ramps the inflow velocity linearly from u_inflow_start to
+       u_inflow_end over ramp_time (characteristic_boundaries.F90:262-300), 0 keeps each inflow
+       node's initial u */
+    int inflow_type, inflow_velocity_control;
+    double u_inflow_start, u_inflow_end, ramp_time;
+    int vpid;               /* -Dvpid: after every step a PID controller drives the volume-mean x
+                               velocity through driving_force(1) (statistics.F90:214-303) */
 } SunsetConfig;
 
 typedef struct SunsetHandle SunsetHandle;
@@ -154,8 +163,8 @@ int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *
 /* output.F90:184-370 output_layer: the columns of a fields dump, 10*npfb in reference order
    (rho - rho_char, u, v, vorticity, Q criterion, alpha_out = the node's error norm of the
    last step, cxx, cxy, cyy, czz; vorticity and Q rotated on walls as :229-241), and the
-   header's 9 values (eflow_nm1, sum_eflow, driving_force(3) -- zero: the flow-rate controller
-   of statistics.F90 is not on this path -- emax_np1, emax_n, emax_nm1, dt). */
+   header's 9 values (eflow_nm1, sum_eflow, driving_force(3) of the flow-rate controller,
+   emax_np1, emax_n, emax_nm1, dt). */
 int sunset_get_dump(SunsetHandle *h, double *columns, double *header);
 /* The same as files in the reference's layout: <directory>/fields_10000_<n_out>, with
    <directory>/nodes_10000 (output_nodes, output.F90:421-476: global index, x, y, s, h,
@@ -165,10 +174,15 @@ int sunset_write_dump(SunsetHandle *h, const char *directory, int n_out, double 
 /* Restart (-Drestart): setup_domain.F90:206-242 loads h and h_small from the nodes file
    before the neighbour search (adapt_stencils is skipped); load_restart_file,
    setup_flow.F90:448-552, sets rho, u, v and c (psi formed from c) and the error-norm history
-   and dt from a fields dump (columns and header as sunset_get_dump returns them).  Time and
-   step count restart at 0, as there. */
+   and dt and the flow-rate controller's state from a fields dump (columns and header as
+   sunset_get_dump returns them; driving_force(2:3) must be zero).  Time and step count
+   restart at 0, as there. */
 int sunset_set_lengths(SunsetHandle *h, const double *h_lengths, const double *h_small);
 int sunset_set_restart(SunsetHandle *h, const double *columns, const double *header);
+/* The flow-rate controller's state (common_vars.F90:82, statistics.F90:214-303): eflow_nm1,
+   sum_eflow, driving_force(1:3), 5 values. */
+int sunset_get_flow_control(SunsetHandle *h, double *out);
+int sunset_set_flow_control(SunsetHandle *h, const double *in);
 /* Binary checkpoint of the device state between steps (no counterpart in the reference):
    the fields, the step's scalars (time, dt, step count, error-norm history) and the per-node
    error, bit for bit, into a caller buffer of sunset_checkpoint_size bytes.  Loading it into

@@ -123,6 +123,10 @@ int sunset_create(const SunsetConfig *cfg, SunsetHandle **out) {
     if (c.form == SUNSET_FORM_NEWT) H->cfg.fenep = 0;  // no polymer
     if (H->cfg.fenep && !(c.fenep_l2 > 3.0))
         return set_err(H, SUNSET_ERR_ARG, "FENE-P needs L^2 > 3 (got %g)", c.fenep_l2);
+    if (c.inflow_type < 0 || c.inflow_type > 2) return set_err(H, SUNSET_ERR_ARG, "inflow_type must be 0, 1 or 2");
+    if (c.inflow_velocity_control == 1 && !(c.ramp_time > 0.0))
+        return set_err(H, SUNSET_ERR_ARG, "inflow velocity control needs ramp_time > 0");
+    if (c.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero on this 2-D path");
     if (int rc = set_device(H)) return rc;
     SUNSET_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
     return 0;
@@ -159,8 +163,6 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
     int nb = 0;
     for (int r = 0; r < nrows; r++) {  // setup_domain.F90:177-199
         int t = node_type[r];
-        if (t == 1 || t == 2)
-            return set_err(H, SUNSET_ERR_SCOPE, "inflow/outflow boundary nodes are not on the device path (walls are)");
         const double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
         H->h_gi.push_back(gi ? gi[r] : r + 1);
         vx.push_back(x[r]);
@@ -697,9 +699,9 @@ int sunset_get_dump(SunsetHandle *sh, double *columns, double *header) {
     if (rc) return rc;
     DevScalars sc;
     SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
-    // eflow_nm1, sum_eflow, driving_force(3): the flow-rate controller of statistics.F90 is
-    // not part of this path, so they are zero; then emax_np1, emax_n, emax_nm1, dt
-    const double hd[9] = {0.0, 0.0, 0.0, 0.0, 0.0, sc.emax_np1, sc.emax_n, sc.emax_nm1, sc.dt};
+    // eflow_nm1, sum_eflow, driving_force(3) (only its x component is ever set), emax_np1,
+    // emax_n, emax_nm1, dt (output.F90:272-276)
+    const double hd[9] = {sc.eflow_nm1, sc.sum_eflow, sc.df, 0.0, 0.0, sc.emax_np1, sc.emax_n, sc.emax_nm1, sc.dt};
     for (int k = 0; k < 9; k++) header[k] = hd[k];
     return 0;
 }
@@ -759,6 +761,8 @@ int sunset_set_restart(SunsetHandle *sh, const double *columns, const double *he
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (!columns || !header) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (header[3] != 0.0 || header[4] != 0.0)
+        return set_err(H, SUNSET_ERR_SCOPE, "driving_force(2:3) must be zero on this 2-D path");
     const int n = H->npfb;
     // load_restart_file, setup_flow.F90:448-552: rho = (rho - rho_char) + rho_char, u, v, c
     std::vector<double> ro(n);
@@ -769,10 +773,43 @@ int sunset_set_restart(SunsetHandle *sh, const double *columns, const double *he
         return rc;
     DevScalars sc;
     SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
+    sc.eflow_nm1 = header[0];
+    sc.sum_eflow = header[1];
+    sc.df = header[2];
     sc.emax_np1 = header[5];
     sc.emax_n = header[6];
     sc.emax_nm1 = header[7];
     sc.dt = header[8];
+    SUNSET_CUDA(H, cudaMemcpy(H->dsc, &sc, sizeof(sc), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int sunset_get_flow_control(SunsetHandle *sh, double *out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    DevScalars sc;
+    SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
+    out[0] = sc.eflow_nm1;
+    out[1] = sc.sum_eflow;
+    out[2] = sc.df;
+    out[3] = 0.0;
+    out[4] = 0.0;
+    return 0;
+}
+
+int sunset_set_flow_control(SunsetHandle *sh, const double *in) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!in) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (in[3] != 0.0 || in[4] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "driving_force(2:3) must be zero on this 2-D path");
+    DevScalars sc;
+    SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
+    sc.eflow_nm1 = in[0];
+    sc.sum_eflow = in[1];
+    sc.df = in[2];
     SUNSET_CUDA(H, cudaMemcpy(H->dsc, &sc, sizeof(sc), cudaMemcpyHostToDevice));
     return 0;
 }

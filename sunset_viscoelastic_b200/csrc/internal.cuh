@@ -69,6 +69,8 @@ struct DevScalars {
     unsigned int done_ctr;  // last-block counter of the mass reduction
     int itime;
     int err;  // nonzero: non-finite error norm
+    // flow-rate controller (statistics.F90:214-303): driving_force(1), eflow_nm1, sum_eflow
+    double df, eflow_nm1, sum_eflow;
 };
 
 // One buffer of the state: conservative fields, conformation variables and the derived
@@ -86,10 +88,15 @@ struct StepConsts {
     int npfb, nslices, form, fenep, mcorr, kolmo, di_full, has_mirrors, mdiff_on, has_walls;
     double csq, c_sound, coef_solvent, coef_polymeric, lambda, epsPTT, fenep_l2, Mdiff, Re, Wi, beta;
     double visc_total, rho_char, L_char, grav0, grav1, ero_norm, erou_norm, exx_norm;
+    // inflow/outflow closures and the flow-rate controller (load_data.F90:145-152,
+    // setup_domain.F90:98-99, common_parameter.F90:71)
+    int inflow_type, inflow_control, vpid;
+    double u_in_start, u_in_end, ramp_time, nscbc, Lx, Ly, p_in, p_out;
 };
 
 // Derived parameters of a run (load_data.F90:131-148) and the switches of the step kernels.
-inline StepConsts step_consts(const SunsetConfig &c, int npfb, int nslices, bool has_mirrors, bool has_walls) {
+inline StepConsts step_consts(const SunsetConfig &c, int npfb, int nslices, bool has_mirrors, bool has_walls,
+                              double xlen = 1.0, double ylen = 1.0) {
     StepConsts K{};
     K.npfb = npfb;
     K.nslices = nslices;
@@ -121,6 +128,17 @@ inline StepConsts step_consts(const SunsetConfig &c, int npfb, int nslices, bool
     K.ero_norm = 1.0 / 1.0;
     K.erou_norm = 1.0 / (1.0 * c.U_char);
     K.exx_norm = 1.0 / (1.0);
+    K.inflow_type = c.inflow_type;
+    K.inflow_control = c.inflow_velocity_control;
+    K.vpid = c.vpid;
+    K.u_in_start = c.u_inflow_start;
+    K.u_in_end = c.u_inflow_end;
+    K.ramp_time = c.ramp_time;
+    K.nscbc = 2.87e-1;
+    K.Lx = xlen * c.L_char;
+    K.Ly = ylen * c.L_char;
+    K.p_in = K.rho_char * K.csq;
+    K.p_out = K.rho_char * K.csq;
     return K;
 }
 
@@ -194,6 +212,8 @@ struct Handle {
     float *dreg32[7] = {}, *eacc32[7] = {};
     double *partials = nullptr;
     double *alpha = nullptr;  // per-node step error of the last step (output.F90 alpha_out)
+    double *uin = nullptr;    // nb: u_inflow_local of each boundary node (common_vars.F90:111)
+    bool uin_set = false;     // uin initialised from a state
     int npart = 0;
     DevScalars *dsc = nullptr;
     double *tmpd = nullptr;  // scratch, 4*npfb doubles

@@ -24,6 +24,7 @@ struct NodeState {
     double cxx, cxy, cyy, czz;          // conformation tensor
     double pxx, pxy, pyy, pzz;          // psi (LC/CHL)
     double f;                           // FENE-P function (L^2 - 3) / (L^2 - tr c)
+    double df;                          // driving_force(1) of the flow-rate controller
 };
 
 // The FENE-P function fenepf (rhs_di.F90:201-203, rhs.F90:207-209, rhs_lc.F90:201-203).
@@ -150,14 +151,11 @@ __host__ __device__ __forceinline__ void chl_fenep_to_j_factor(double L2, double
 
 // calc_rhs_ro + calc_rhs_rovel, interior branch (rhs_di.F90:126-141,215-275; rhs.F90:220-286;
 // rhs_lc.F90:215-275).
-__host__ __device__ __forceinline__ void rhs_flow(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
-    const double w = 0.0;
-    double tmp_scal = (n.u * g.ro_x + n.v * g.ro_y) + w * 0.0;
-    double divvel = (g.u_x + g.v_y) + 0.0;
-    r.ro = -n.ro * divvel - tmp_scal;
-    double tsu = n.ro * ((n.u * g.u_x + n.v * g.u_y) + w * 0.0) - n.u * r.ro;
-    double tsv = n.ro * ((n.u * g.v_x + n.v * g.v_y) + w * 0.0) - n.v * r.ro;
-    double fvu = K.coef_solvent * g.lapu, fvv = K.coef_solvent * g.lapv;
+// The stress divergence f_visc: solvent Laplacian plus the polymeric term of each form.
+__host__ __device__ __forceinline__ void viscous_force(const StepConsts &K, const NodeState &n, const Grads &g,
+                                                       double &fvu, double &fvv) {
+    fvu = K.coef_solvent * g.lapu;
+    fvv = K.coef_solvent * g.lapv;
     if (K.form == SUNSET_FORM_CHL) {
         double gcxx1 = (2.0 * exp(2.0 * n.pxx)) * g.pxx_x;
         double gcxy1 = exp(n.pxx) * g.pxy_x + (n.pxy * exp(n.pxx)) * g.pxx_x;
@@ -173,7 +171,18 @@ __host__ __device__ __forceinline__ void rhs_flow(const StepConsts &K, const Nod
         fvu = fvu + K.coef_polymeric * ((g.cxx_x + g.cxy_y) + 0.0);
         fvv = fvv + K.coef_polymeric * ((g.cxy_x + g.cyy_y) + 0.0);
     }
-    double bfu = n.ro * (K.grav0 + 0.0), bfv = n.ro * (K.grav1 + 0.0);
+}
+
+__host__ __device__ __forceinline__ void rhs_flow(const StepConsts &K, const NodeState &n, const Grads &g, Rhs &r) {
+    const double w = 0.0;
+    double tmp_scal = (n.u * g.ro_x + n.v * g.ro_y) + w * 0.0;
+    double divvel = (g.u_x + g.v_y) + 0.0;
+    r.ro = -n.ro * divvel - tmp_scal;
+    double tsu = n.ro * ((n.u * g.u_x + n.v * g.u_y) + w * 0.0) - n.u * r.ro;
+    double tsv = n.ro * ((n.u * g.v_x + n.v * g.v_y) + w * 0.0) - n.v * r.ro;
+    double fvu, fvv;
+    viscous_force(K, n, g, fvu, fvv);
+    double bfu = n.ro * (K.grav0 + n.df), bfv = n.ro * (K.grav1 + 0.0);
     if (K.kolmo)
         bfu = bfu + (((1.0 / K.Re) * cos(n.y)) * (1.0 + (K.Mdiff * K.beta) * K.Wi)) / (1.0 + K.Mdiff * K.Wi);
     r.rou = ((-tsu - K.csq * g.ro_x) + bfu) + fvu;
@@ -214,6 +223,70 @@ __host__ __device__ __forceinline__ void rhs_flow_wall(const StepConsts &K, cons
     r.ro = r.ro - tmp_scal;
     r.rou = (0.0 - n.u * tmp_scal) - (L5 - L1) / c;
     r.rov = (0.0 - n.v * tmp_scal) - n.ro * L3;
+}
+
+// Inflow (node_type 1) and outflow (node_type 2) nodes, in the x-y frame (the outflow's
+// first-derivative weights are reversed at set-up, labf.F90:986-991, so g.*_x is d/dx on
+// both): calc_rhs_ro's in/out branch (rhs_di.F90:155-157), the characteristic amplitudes and
+// the transverse, viscous and body-force terms of calc_rhs_rovel (:311-359; no Kolmogorov
+// forcing there), the closure of characteristic_boundaries.F90 for the node's type -- soft
+// inflow :54-80, hard inflow :82-110, pressure-tracking inflow-outflow :112-150, partially
+// non-reflecting outflow :152-189 -- and the update of calc_rhs_nscbc (rhs_di.F90:601-665).
+// uin: the node's u_inflow_local.  rhs.F90 and rhs_lc.F90 have the same branches.
+__host__ __device__ __forceinline__ void rhs_flow_inout(const StepConsts &K, const NodeState &n, const Grads &g,
+                                                        int type, double uin, Rhs &r) {
+    const double w = 0.0;
+    const double c = K.c_sound, ro = n.ro, u = n.u, v = n.v;
+    r.ro = ((-v * g.ro_y - ro * g.v_y) - w * 0.0) - ro * 0.0;
+    const double gp_x = K.csq * g.ro_x, gp_y = K.csq * g.ro_y, p = K.csq * ro;
+    const double dpdn = gp_x;
+    double L1 = (0.5 * (u - c)) * (dpdn - (ro * c) * g.u_x);
+    double L2 = u * (g.ro_x - (gp_x / c) / c);
+    double L3 = u * g.v_x;
+    double L5 = (0.5 * (u + c)) * (dpdn + (ro * c) * g.u_x);
+    double fvu, fvv;
+    viscous_force(K, n, g, fvu, fvv);
+    const double bfu = ro * (K.grav0 + n.df), bfv = ro * (K.grav1 + 0.0);
+    const double rou = ((-(v * g.u_y) - w * 0.0) + fvu) + bfu;
+    const double rov = (((-(v * g.v_y) - w * 0.0) - gp_y) + fvv) + bfv;
+    const double nscbc = K.nscbc, Lx = K.Lx;
+    if (type == 1) {
+        if (K.inflow_type == 1) {  // hard inflow
+            L2 = 0.0; L3 = 0.0; L5 = L1;
+        } else if (K.inflow_type == 2) {  // inflow-outflow
+            if (u > 0.0) {
+                L2 = 0.0;
+                L3 = ((v * nscbc) * c) / Lx;
+                L5 = ((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx;
+            } else {
+                L2 = 0.0;
+                L5 = (((((p - K.p_in) * nscbc) * c) * 1.0) / 2.0) / Lx;
+            }
+        } else {  // soft inflow (its L4, of w, has no effect in 2-D)
+            L2 = 0.0;
+            L3 = (((((v * nscbc) * c) / Lx) - v * g.v_y) - w * 0.0) - gp_y / ro;
+            L5 = (((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx -
+                  0.5 * (((v * gp_y) + (p * g.v_y)) + (((ro * c) * v) * g.u_y))) -
+                 0.5 * (((w * 0.0) + (p * 0.0)) + (((ro * c) * w) * 0.0));
+        }
+    } else {  // outflow
+        if (u < c) L1 = (((((p - K.p_out) * nscbc) * c) * 1.0) / 2.0) / Lx;
+        L2 = 0.0;
+        if (u <= 0.0) { L2 = 0.0; L3 = 0.0; }
+    }
+    const double tmp_scal = ((((c * c) * L2 + L5) + L1) / c) / c;
+    r.ro = r.ro - tmp_scal;
+    r.rou = (rou - u * tmp_scal) - (L5 - L1) / c;
+    r.rov = (rov - v * tmp_scal) - ro * L3;
+}
+
+// u_inflow_local at time t (update_u_inflow, characteristic_boundaries.F90:262-300): with
+// velocity control, the ramp from u_inflow_start to u_inflow_end while t <= ramp_time; the
+// value is left as it is after that (and always without control).
+__host__ __device__ __forceinline__ double inflow_velocity(const StepConsts &K, double t, double uin) {
+    if (K.inflow_control != 1) return uin;
+    if (t <= K.ramp_time) return K.u_in_start + ((K.u_in_end - K.u_in_start) * t) / K.ramp_time;
+    return uin;
 }
 
 // calc_rhs_c, interior branch, rhs_di.F90:415-476 (sPTT / Oldroyd-B, 2-D); on walls

@@ -152,10 +152,17 @@ __global__ void k_cell_bounds(const int *cid_sorted, int np, int *cstart, int *c
     if (p == np - 1 || cid_sorted[p + 1] != c) cend[c] = p + 1;
 }
 
+// The reference's search grid (cell_generator, neighbours.F90:75-93): square cells of side
+// ss*h0 over the domain tripled in each direction.
+struct RefGrid {
+    double xmint, ymint, unoss;
+};
+
 struct SearchArgs {
     const double *px, *py, *h;
     const int *cstart, *cend, *pts;
     Grid g;
+    RefGrid rg;
     int npfb;
 };
 
@@ -167,6 +174,11 @@ __global__ void k_search(SearchArgs a, int *count, const long long *rowptr, int 
     const double hh = a.h[i] * kSs, hs2 = hh * hh;
     int cx = min(max((int)((xi - a.g.x0) * a.g.inv), 0), a.g.ncx - 1);
     int cy = min(max((int)((yi - a.g.y0) * a.g.inv), 0), a.g.ncy - 1);
+    // the reference scans only the 3x3 block of its own cells around the node
+    // (neighbour_cells, neighbours.F90:95-158), so where a node's ss*h exceeds the cell side
+    // ss*h0 (boundary nodes at order 4: hovs_bound > hovs) the points further out are not its
+    // neighbours even inside the radius
+    const int ci = (int)((xi - a.rg.xmint) * a.rg.unoss), cj = (int)((yi - a.rg.ymint) * a.rg.unoss);
     long long o = FILL ? rowptr[i] : 0;
     int cnt = 0;
     for (int dy = -1; dy <= 1; dy++) {
@@ -182,6 +194,9 @@ __global__ void k_search(SearchArgs a, int *count, const long long *rowptr, int 
                 double rx = xi - a.px[p], ry = yi - a.py[p], rz = 0.0 - 0.0;
                 double rr2 = (rx * rx + ry * ry) + rz * rz;
                 if (rr2 <= hs2) {
+                    const int dcx = (int)((a.px[p] - a.rg.xmint) * a.rg.unoss) - ci;
+                    const int dcy = (int)((a.py[p] - a.rg.ymint) * a.rg.unoss) - cj;
+                    if (dcx < -1 || dcx > 1 || dcy < -1 || dcy > 1) continue;
                     if (FILL) { opt[o + cnt] = p; or2[o + cnt] = rr2; }
                     cnt++;
                 }
@@ -193,12 +208,6 @@ __global__ void k_search(SearchArgs a, int *count, const long long *rowptr, int 
 
 // Reference numbering of a point, used to order links at equal distance deterministically.
 __device__ __forceinline__ int ref_point(int p, int npfb, const int *perm) { return p < npfb ? perm[p] : p; }
-
-// The reference's search grid (cell_generator, neighbours.F90:75-93): square cells of side
-// ss*h0 over the domain tripled in each direction.
-struct RefGrid {
-    double xmint, ymint, unoss;
-};
 
 // Position of the cell (dx, dy) relative to a node's own cell in the reference's scan of the
 // neighbouring cells (neighbour_cells, neighbours.F90:95-158): self, E, NE, SE, W, NW, SW, N, S.
@@ -232,8 +241,7 @@ __global__ void k_sort_rows(int npfb, const long long *rowptr, int *opt, double 
     const int ci = (int)((px[i] - rg.xmint) * rg.unoss), cj = (int)((py[i] - rg.ymint) * rg.unoss);
     auto scan_key = [&](int p) -> long long {
         int dx = (int)((px[p] - rg.xmint) * rg.unoss) - ci, dy = (int)((py[p] - rg.ymint) * rg.unoss) - cj;
-        // links beyond the reference's 3x3 cells (only when a node's h exceeds the grid's)
-        // go last, by point number
+        // (k_search keeps no link beyond the 3x3 cells; such a link would go last)
         int pos = (dx < -1 || dx > 1 || dy < -1 || dy > 1) ? 9 : scan_position(dx, dy);
         return ((long long)pos << 32) | (unsigned)ref_point(p, npfb, perm);
     };
@@ -431,7 +439,8 @@ int find_neighbours_device(Handle *H) {
     SUNSET_CUDA(H, cudaMemsetAsync(cend, 0, ncell * sizeof(int), st));
     k_cell_bounds<<<(np + TB - 1) / TB, TB, 0, st>>>(cid2, np, cstart, cend);
 
-    SearchArgs sa{H->px, H->py, H->h, cstart, cend, pid2, g, n};
+    const RefGrid rg{H->xmin - (H->xmax - H->xmin), H->ymin - (H->ymax - H->ymin), 1.0 / (1.0 * (kSs * H->h0))};
+    SearchArgs sa{H->px, H->py, H->h, cstart, cend, pid2, g, rg, n};
     int *count;
     long long *cnt64, *rowptr;
     if (dalloc(H, &count, n) || dalloc(H, &cnt64, n + 1) || dalloc(H, &rowptr, n + 1)) return SUNSET_ERR_NOMEM;
@@ -456,7 +465,6 @@ int find_neighbours_device(Handle *H) {
     int *serr;
     if (dalloc(H, &serr, 1)) return SUNSET_ERR_NOMEM;
     SUNSET_CUDA(H, cudaMemsetAsync(serr, 0, sizeof(int), st));
-    RefGrid rg{H->xmin - (H->xmax - H->xmin), H->ymin - (H->ymax - H->ymin), 1.0 / (1.0 * (kSs * H->h0))};
     k_sort_rows<<<(n + TB - 1) / TB, TB, 0, st>>>(n, rowptr, opt, or2, H->hs, H->perm, H->px, H->py, rg,
                                                   H->cnt_small, serr);
     int hserr = 0;

@@ -56,6 +56,7 @@ struct StageArgs {
     DevScalars *sc;
     double *partials;
     double *alpha;  // per-node step error (stage 3), or null
+    double *uin;    // nb: u_inflow_local of the boundary nodes (inflow/outflow sets), or null
     double *gsave;  // log-conformation FP64 stages of the adjoint's recording: the 18 stencil
                     // sums of each node (adjoint.cuh order, arrays of npfb), else null
     int stage;  // 0..3; 4 = rhs only
@@ -431,7 +432,9 @@ __host__ __device__ constexpr int stage_min_blocks(int) { return SUNSET_STAGE_BL
 // MX (mixed precision): FP32 weights; the register S is kept as the FP32 increment
 // D = S - U over the stage's FP64 state U (so S = U + D loses only FP32 rounding of an
 // O(dt rhs) quantity) and the error accumulator E as FP32.
-template <int FORM, bool MD, bool MX, bool FP>
+// BND: the node set has boundary nodes (walls, inflows, outflows); without them the
+// closures are compiled out, which keeps them from costing the periodic sets registers.
+template <int FORM, bool MD, bool MX, bool FP, bool BND>
 __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageArgs A) {
     extern __shared__ __align__(16) double smem[];
     constexpr int NG = ngather(FORM, MD, FP);
@@ -476,9 +479,17 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         n.pxx = F.q[0][i]; n.pxy = F.q[1][i]; n.pyy = F.q[2][i]; n.pzz = F.q[3][i];
         n.f = 0.0;
         if constexpr (FP) n.f = FORM == SUNSET_FORM_CHL ? fenep_f(cK.fenep_l2, n.cxx, n.cyy, n.czz) : F.f[i];
+        n.df = A.sc->df;
         Rhs r;
-        const bool wall = cK.has_walls && A.ntype[i] == 0;
-        if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
+        const int ty = BND ? A.ntype[i] : 999;
+        const bool wall = ty == 0, inout = ty == 1 || ty == 2;
+        const int jb = inout ? A.bidx[i] : 0;
+        double uin = inout ? A.uin[jb] : 0.0;
+        if (inout) {  // inflow/outflow closure in the x-y frame
+            if constexpr (MD && FORM == SUNSET_FORM_CHL)  // rhs.F90:624-636: the same one-sided flux closure
+                wall_conformation_laplacian<FORM, MD, FP>(A, i, smem, g);
+            rhs_flow_inout(cK, n, g, ty, uin, r);
+        } else if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
             if constexpr (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL))
                 wall_conformation_laplacian<FORM, MD, FP>(A, i, smem, g);
             const double xn = A.rnx[i], yn = A.rny[i];
@@ -491,9 +502,18 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         } else {
             rhs_flow(cK, n, g, r);
         }
-        if (FORM == SUNSET_FORM_DI) rhs_c_di(cK, n, g, r, wall);
-        else if (FORM == SUNSET_FORM_CHL) rhs_c_chl(cK, n, g, r);
-        else if (FORM == SUNSET_FORM_LC) {
+        if (FORM == SUNSET_FORM_DI) {
+            rhs_c_di(cK, n, g, r, wall);
+            if (inout) r.xx = r.xy = r.yy = r.zz = 0.0;  // rhs_di.F90:582-590 (left to be completed there)
+        } else if (FORM == SUNSET_FORM_CHL) {
+            if (ty == 1) {  // inflow: no streamwise advection of psi (rhs.F90:562-564)
+                NodeState m = n;
+                m.u = 0.0;
+                rhs_c_chl(cK, m, g, r);
+            } else {
+                rhs_c_chl(cK, n, g, r);
+            }
+        } else if (FORM == SUNSET_FORM_LC) {
             const bool first = (A.sc->itime == 1) && (stage == 0);
             rhs_c_lc(cK, n, g, first, r, wall);
         } else { r.xx = r.xy = r.yy = r.zz = 0.0; }
@@ -558,7 +578,16 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
                 emax_bits = dbits(en);
                 if (A.alpha) A.alpha[i] = al;
             }
-            if (wall) { Un[1] = 0.0; Un[2] = 0.0; }  // apply_time_dependent_bounds, characteristic_boundaries.F90:200-206
+            // apply_time_dependent_bounds (characteristic_boundaries.F90:191-257) at the stage's
+            // time time0 + c_s dt (step.F90:285, c = 0, a21, a32 + b1, 1): walls at rest; on
+            // inflow nodes u_inflow_local follows its ramp, and a hard inflow prescribes u
+            if (wall) { Un[1] = 0.0; Un[2] = 0.0; }
+            if (ty == 1) {
+                const double cs = stage == 0 ? 0.0 : stage == 1 ? SUNSET_RK_A21 : stage == 2 ? (SUNSET_RK_A32 + SUNSET_RK_B1) : 1.0;
+                uin = inflow_velocity(cK, A.sc->time + dt * cs, uin);
+                A.uin[jb] = uin;
+                if (cK.inflow_type == 1) { Un[1] = uin * Un[0]; Un[2] = 0.0; }
+            }
             const Fields &O = A.out;
             O.ro[i] = Un[0]; O.rou[i] = Un[1]; O.rov[i] = Un[2];
             if (FORM != SUNSET_FORM_NEWT) {
@@ -718,11 +747,18 @@ template <int FORM>
 __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double dro = A.sc->dro;
+    double uvol = 0.0;
     if (i < cK.npfb) {
         const Fields &F = A.out;
         double ro = F.ro[i];
         if (cK.mcorr) ro = ro - dro;
         F.ro[i] = ro;
+        if (cK.has_walls && cK.inflow_type == 1 && A.ntype[i] == 1) {
+            // the bounds again after the filter (step.F90:498): the hard inflow's momentum
+            // from the corrected density, at the step's end time (u_inflow_local unchanged)
+            F.rou[i] = A.uin[A.bidx[i]] * ro;
+            F.rov[i] = 0.0;
+        }
         double ooro = 1.0 / ro;
         F.u[i] = F.rou[i] * ooro;
         F.v[i] = F.rov[i] * ooro;
@@ -737,6 +773,54 @@ __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
             F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy; F.c[3][i] = czz;
         }
         if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
+        if (cK.vpid) uvol = F.u[i] * A.vol[i];
+    }
+    if (cK.vpid && advance) {
+        // velocity_control with -Dvpid (statistics.F90:214-303), after the step: the volume
+        // sum of u (fixed tree in the block, blocks in order), then the PID update of
+        // driving_force(1) by the last block
+        __shared__ double red[128];
+        __shared__ bool last;
+        red[threadIdx.x] = uvol;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            A.partials[blockIdx.x] = red[0];
+            __threadfence();
+            const unsigned int prev = atomicAdd(&A.sc->done_ctr, 1u);
+            last = (prev == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            double acc = 0.0;
+            for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc = acc + ((volatile double *)A.partials)[b];
+            red[threadIdx.x] = acc;
+            __syncthreads();
+            for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+                if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                DevScalars *sc = A.sc;
+                const double tot_vol = sc->tv, dt = sc->dt;
+                const double tot_u = red[0] / tot_vol;
+                const double eflow_n = 1.0 - (tot_u * tot_vol) / (cK.Ly * cK.Lx);
+                sc->sum_eflow = sc->sum_eflow + eflow_n * dt;
+                const double deflowdt = (eflow_n - sc->eflow_nm1) / dt;
+                const double facA = ((((0.5 * 0.5) * 0.5) * 1.0) * 2.0) * 2.0;
+                const double facB = facA / 0.4, facC = facA * 0.02;
+                double df = ((facA * eflow_n) + facB * sc->sum_eflow) + facC * deflowdt;
+                df = (500.0 < df) ? 500.0 : df;
+                df = (-500.0 > df) ? -500.0 : df;
+                sc->df = df;
+                sc->eflow_nm1 = eflow_n;
+                sc->done_ctr = 0;
+            }
+        }
     }
     if (advance && i == 0) {
         DevScalars *sc = A.sc;
@@ -749,6 +833,9 @@ __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
         sc->emax_bits = 0ull;
         sc->time = sc->time + sc->dt;
         sc->itime = sc->itime + 1;
+        // without -Dvpid the statistics call after the step zeroes the driving force
+        // (statistics.F90:288; a restart may have loaded one for the first step)
+        if (!cK.vpid) sc->df = 0.0;
     }
 }
 
@@ -995,12 +1082,14 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     A.sc = H->dsc;
     A.partials = H->partials;
     A.alpha = H->alpha;
+    A.uin = H->uin;
     A.stage = stage;
     return A;
 }
 
 int upload_consts(Handle *H) {
-    const StepConsts K = step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, H->nb > 0);
+    const StepConsts K = step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, H->nb > 0, H->xmax - H->xmin,
+                                     H->ymax - H->ymin);
     SUNSET_CUDA(H, cudaMemcpyToSymbolAsync(cK, &K, sizeof(K), 0, cudaMemcpyHostToDevice, H->stream));
     return 0;
 }
@@ -1010,8 +1099,13 @@ constexpr size_t kMaxStageSmem = 200 * 1024;
 #define SUNSET_SMEM_ATTR(K) SUNSET_CUDA(H, cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem))
 template <int FORM, bool MD, bool FP>
 int stage_smem_attributes(Handle *H, bool mx) {
-    SUNSET_SMEM_ATTR((k_stage<FORM, MD, false, FP>));
-    if (mx) SUNSET_SMEM_ATTR((k_stage<FORM, MD, true, FP>));
+    if (H->nb > 0) {
+        SUNSET_SMEM_ATTR((k_stage<FORM, MD, false, FP, true>));
+        if (mx) SUNSET_SMEM_ATTR((k_stage<FORM, MD, true, FP, true>));
+    } else {
+        SUNSET_SMEM_ATTR((k_stage<FORM, MD, false, FP, false>));
+        if (mx) SUNSET_SMEM_ATTR((k_stage<FORM, MD, true, FP, false>));
+    }
     return 0;
 }
 template <int FORM, bool FP>
@@ -1055,8 +1149,13 @@ int launch_stage(Handle *H, const StageArgs &A, bool mx) {
     const size_t smem = halo_doubles(ngather(FORM, MD, FP), H->halo_max) * sizeof(double) +
                         (mx ? LinkRing<true, 3, ring_depth(true)>::bytes() : LinkRing<false, 3, ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    if (mx) k_stage<FORM, MD, true, FP><<<H->ntiles, kTile, smem, H->stream>>>(A);
-    else k_stage<FORM, MD, false, FP><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (H->nb > 0) {
+        if (mx) k_stage<FORM, MD, true, FP, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        else k_stage<FORM, MD, false, FP, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    } else {
+        if (mx) k_stage<FORM, MD, true, FP, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        else k_stage<FORM, MD, false, FP, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    }
     return 0;
 }
 
@@ -1130,6 +1229,24 @@ int launch_step(Handle *H, int from, int pid, cudaEvent_t *stage_ev = nullptr) {
 
 }  // namespace
 
+// u_inflow_local of the initial state (setup_flow.F90:48-50,128-138): u of each inflow node,
+// U_char elsewhere.
+__global__ void k_init_uin(int nb, const int *blist, const int *ntype, const double *u, double uchar, double *uin) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= nb) return;
+    const int i = blist[jj];
+    uin[jj] = ntype[i] == 1 ? u[i] : uchar;
+}
+
+int init_inflow(Handle *H) {
+    if (H->nb == 0) return 0;
+    k_init_uin<<<(H->nb + 127) / 128, 128, 0, H->stream>>>(H->nb, H->blist, H->ntype, H->buf[H->cur].u, H->cfg.U_char,
+                                                          H->uin);
+    SUNSET_CUDA(H, cudaGetLastError());
+    H->uin_set = true;
+    return 0;
+}
+
 // ---------------------------------------------------------------------------------------
 int state_alloc(Handle *H) {
     if (H->dsc) return 0;
@@ -1161,6 +1278,7 @@ int state_alloc(Handle *H) {
     }
     if (dalloc(H, &H->alpha, n)) return SUNSET_ERR_NOMEM;
     SUNSET_CUDA(H, cudaMemsetAsync(H->alpha, 0, n * sizeof(double), H->stream));
+    if (H->nb > 0 && dalloc(H, &H->uin, H->nb)) return SUNSET_ERR_NOMEM;
     const int nthr = H->nslices * kSlice;
     H->npart = (nthr + 127) / 128 + 1;
     if (dalloc(H, &H->partials, 2 * (size_t)H->npart + 16) || dalloc(H, &H->dsc, 1) || dalloc(H, &H->tmpd, 4 * (size_t)n))
@@ -1174,6 +1292,7 @@ static int init_scalars(Handle *H) {
     s.dt = 1.0e-6;
     s.time = 0.0;
     s.emax_nm1 = s.emax_n = s.emax_np1 = 1.0e-5;  // pid_tol, setup_flow.F90:149-152
+    s.eflow_nm1 = 1.0;  // flow-rate controller, setup_flow.F90:165-169 (sum_eflow, df = 0)
     s.cfl_bits = 0x7ff0000000000000ull;
     s.par_bits = 0x7ff0000000000000ull;
     SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, H->stream));
@@ -1195,6 +1314,7 @@ int state_set_device(Handle *H, const double *ro, const double *u, const double 
     SUNSET_CUDA(H, cudaGetLastError());
     rc = init_scalars(H);
     if (rc) return rc;
+    if ((rc = init_inflow(H))) return rc;
     return set_tstep_device(H);
 }
 
@@ -1204,6 +1324,7 @@ int state_set_conservative_device(Handle *H, const double *const *f7) {
     k_set_conservative<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, f7[0], f7[1], f7[2],
                                                                      f7[3], f7[4], f7[5], f7[6], H->buf[H->cur]);
     SUNSET_CUDA(H, cudaGetLastError());
+    if (!H->uin_set) return init_inflow(H);
     return 0;
 }
 
@@ -1414,7 +1535,7 @@ size_t checkpoint_bytes(const Handle *H) {
     double *const *arr;
     int na;
     checkpoint_arrays(H, arr, na, tmp);
-    return sizeof(CheckpointHeader) + sizeof(DevScalars) + (size_t)na * H->npfb * sizeof(double);
+    return sizeof(CheckpointHeader) + sizeof(DevScalars) + ((size_t)na * H->npfb + (size_t)H->nb) * sizeof(double);
 }
 
 static int node_fingerprint(Handle *H, double *xs, double *ys) {
@@ -1435,7 +1556,7 @@ int checkpoint_save(Handle *H, void *buf) {
     checkpoint_arrays(H, arr, na, tmp);
     CheckpointHeader hd{};
     memcpy(hd.magic, "SUNSETCK", 8);
-    hd.version = 1;
+    hd.version = 2;
     hd.npfb = H->npfb;
     hd.form = H->cfg.form;
     hd.precision = H->cfg.precision;
@@ -1451,6 +1572,7 @@ int checkpoint_save(Handle *H, void *buf) {
         SUNSET_CUDA(H, cudaMemcpyAsync(p, arr[k], H->npfb * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
         p += H->npfb * sizeof(double);
     }
+    if (H->nb > 0) SUNSET_CUDA(H, cudaMemcpyAsync(p, H->uin, H->nb * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
     return 0;
 }
@@ -1466,7 +1588,7 @@ int checkpoint_load(Handle *H, const void *buf, size_t bytes) {
     memcpy(&hd, p, sizeof(hd));
     double xs, ys;
     if (int rc = node_fingerprint(H, &xs, &ys)) return rc;
-    if (memcmp(hd.magic, "SUNSETCK", 8) != 0 || hd.version != 1 || hd.npfb != H->npfb || hd.form != H->cfg.form ||
+    if (memcmp(hd.magic, "SUNSETCK", 8) != 0 || hd.version != 2 || hd.npfb != H->npfb || hd.form != H->cfg.form ||
         hd.precision != H->cfg.precision || hd.fenep != H->cfg.fenep || hd.nfields != na || hd.xsum != xs || hd.ysum != ys)
         return set_err(H, SUNSET_ERR_ARG, "checkpoint written for another configuration or node set");
     p += sizeof(hd);
@@ -1476,7 +1598,9 @@ int checkpoint_load(Handle *H, const void *buf, size_t bytes) {
         SUNSET_CUDA(H, cudaMemcpyAsync(arr[k], p, H->npfb * sizeof(double), cudaMemcpyHostToDevice, H->stream));
         p += H->npfb * sizeof(double);
     }
+    if (H->nb > 0) SUNSET_CUDA(H, cudaMemcpyAsync(H->uin, p, H->nb * sizeof(double), cudaMemcpyHostToDevice, H->stream));
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    H->uin_set = true;
     return upload_consts(H);
 }
 
@@ -2114,7 +2238,8 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     if (H->cfg.form != SUNSET_FORM_LC)
         return set_err(H, SUNSET_ERR_SCOPE, "the adjoint is built for the log-conformation form");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint runs the FP64 step");
-    if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers node sets without walls");
+    if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers node sets without boundaries");
+    if (H->cfg.vpid) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers runs without the flow-rate controller");
     if (H->cfg.Mdiff != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint assumes Mdiff = 0");
     if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint covers Oldroyd-B and sPTT, not FENE-P");
     if (nsteps < 1 || ckpt < 1) return set_err(H, SUNSET_ERR_ARG, "nsteps and checkpoint_every must be positive");

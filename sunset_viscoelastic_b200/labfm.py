@@ -34,7 +34,7 @@ ABI_SYMBOLS = [
     "sunset_time_stage_kernel", "sunset_step_timed", "sunset_kinetic_energy_noalloc",
     "sunset_adjoint_run", "sunset_adjoint_apply_D", "sunset_adapt_stencils", "sunset_get_lengths",
     "sunset_set_lengths", "sunset_get_dump", "sunset_write_dump", "sunset_set_restart", "sunset_checkpoint_size",
-    "sunset_save_checkpoint", "sunset_load_checkpoint",
+    "sunset_save_checkpoint", "sunset_load_checkpoint", "sunset_get_flow_control", "sunset_set_flow_control",
 ]
 
 
@@ -44,7 +44,9 @@ class SunsetConfig(C.Structure):
                 ("precision", C.c_int), ("L_char", C.c_double), ("U_char", C.c_double), ("Re", C.c_double),
                 ("Wi", C.c_double), ("beta", C.c_double), ("epsPTT", C.c_double), ("fenep_l2", C.c_double),
                 ("Mdiff", C.c_double), ("Ma", C.c_double), ("grav", C.c_double * 3), ("h_over_s", C.c_double),
-                ("device", C.c_int)]
+                ("device", C.c_int), ("inflow_type", C.c_int), ("inflow_velocity_control", C.c_int),
+                ("u_inflow_start", C.c_double), ("u_inflow_end", C.c_double), ("ramp_time", C.c_double),
+                ("vpid", C.c_int)]
 
 
 class SunsetError(RuntimeError):
@@ -86,6 +88,8 @@ def load_library(build_if_missing: bool = True):
     L.sunset_get_dump.argtypes = [P, dp, dp]
     L.sunset_write_dump.argtypes = [P, C.c_char_p, C.c_int, C.c_double]
     L.sunset_set_restart.argtypes = [P, dp, dp]
+    L.sunset_get_flow_control.argtypes = [P, dp]
+    L.sunset_set_flow_control.argtypes = [P, dp]
     L.sunset_checkpoint_size.argtypes = [P, C.POINTER(C.c_size_t)]
     L.sunset_save_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
     L.sunset_load_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
@@ -118,7 +122,9 @@ class Sunset:
 
     def __init__(self, form="di", order=4, forder=None, Re=1.0, Wi=1.0, beta=0.5, epsPTT=0.0, Ma=0.1,
                  fenep=False, fenep_l2=1e30, Mdiff=0.0, grav=(0.0, 0.0, 0.0), mcorr=True, kolmogorov_forcing=-1,
-                 di_full_gradients=True, h_over_s=0.0, L_char=1.0, U_char=1.0, precision="fp64", device=0):
+                 di_full_gradients=True, h_over_s=0.0, L_char=1.0, U_char=1.0, precision="fp64", device=0,
+                 inflow_type=1, inflow_velocity_control=0, u_inflow_start=0.0, u_inflow_end=1.0, ramp_time=1.0,
+                 vpid=False):
         self.L = load_library()
         cfg = SunsetConfig()
         cfg.form = FORMS[form]
@@ -135,6 +141,9 @@ class Sunset:
             cfg.grav[k] = grav[k]
         cfg.h_over_s = h_over_s
         cfg.device = device
+        cfg.inflow_type, cfg.inflow_velocity_control = int(inflow_type), int(inflow_velocity_control)
+        cfg.u_inflow_start, cfg.u_inflow_end, cfg.ramp_time = u_inflow_start, u_inflow_end, ramp_time
+        cfg.vpid = int(bool(vpid))
         self.cfg = cfg
         self.h = C.c_void_p()
         rc = self.L.sunset_create(C.byref(cfg), C.byref(self.h))
@@ -228,6 +237,16 @@ class Sunset:
             columns = np.stack([columns[k] for k in DUMP_COLUMNS])
         self._chk(self.L.sunset_set_restart(self.h, np.ascontiguousarray(columns, np.float64).ravel(),
                                             np.ascontiguousarray(header, np.float64)))
+
+    def flow_control(self):
+        """The flow-rate controller's state: eflow_nm1, sum_eflow, driving_force(1:3)."""
+        out = np.zeros(5)
+        self._chk(self.L.sunset_get_flow_control(self.h, out))
+        return dict(eflow_nm1=out[0], sum_eflow=out[1], driving_force=out[2:5].copy())
+
+    def set_flow_control(self, eflow_nm1, sum_eflow, driving_force):
+        v = np.array([eflow_nm1, sum_eflow, *np.asarray(driving_force, np.float64)[:3]])
+        self._chk(self.L.sunset_set_flow_control(self.h, v))
 
     def save_checkpoint(self):
         """The device state between steps, bit for bit, as bytes."""
