@@ -42,6 +42,26 @@ __global__ void k_scatter(const double *in, const int *perm, int n, double *out)
     if (i < n) out[perm[i]] = in[i];
 }
 
+// The seven evolved fields at once, between the reference-order staging block (7 x n,
+// field-major) and the internal-order field arrays.
+struct Fields7 {
+    double *p[7];
+};
+__global__ void k_gather7(const double *in, const int *perm, int n, Fields7 out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = perm[i];
+#pragma unroll
+    for (int f = 0; f < 7; f++) out.p[f][i] = in[(size_t)f * n + r];
+}
+__global__ void k_scatter7(Fields7 in, const int *perm, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = perm[i];
+#pragma unroll
+    for (int f = 0; f < 7; f++) out[(size_t)f * n + r] = in.p[f][i];
+}
+
 double hovs_for(int forder) {  // common_parameter.F90:44-56
     if (forder == 4) return 1.8;
     if (forder == 6) return 2.4;
@@ -620,16 +640,23 @@ int sunset_run_host(SunsetHandle *sh, const double *state_in, double dt, int nst
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (!state_in || !state_out) return set_err(H, SUNSET_ERR_ARG, "null array");
     const int n = H->npfb;
-    double *d[7] = {H->rhs[0], H->rhs[1], H->rhs[2], H->rhs[3], H->rhs[4], H->rhs[5], H->rhs[6]};
-    for (int f = 0; f < 7; f++)
-        if (int rc = to_internal(H, state_in + (size_t)f * n, SUNSET_PTR_HOST, d[f])) return rc;
-    if (int rc = state_set_conservative_device(H, d)) return rc;
+    // one copy each way through a 7 x npfb staging block (allocated on the first call), with
+    // the permutation between reference and internal order done on the device
+    if (!H->io && dalloc(H, &H->io, 7 * (size_t)n)) return SUNSET_ERR_NOMEM;
+    const int nb = (n + 255) / 256;
+    Fields7 d{{H->rhs[0], H->rhs[1], H->rhs[2], H->rhs[3], H->rhs[4], H->rhs[5], H->rhs[6]}};
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->io, state_in, 7 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    k_gather7<<<nb, 256, 0, H->stream>>>(H->io, H->perm, n, d);
+    SUNSET_CUDA(H, cudaGetLastError());
+    if (int rc = state_set_conservative_device(H, d.p)) return rc;
     if (int rc = step_run(H, dt, nsteps, 0)) return rc;
     const Fields &F = H->buf[H->cur];
-    const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
-    for (int f = 0; f < 7; f++)
-        if (int rc = to_reference(H, src[f], SUNSET_PTR_HOST, state_out + (size_t)f * n)) return rc;
+    Fields7 src{{F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]}};
+    k_scatter7<<<nb, 256, 0, H->stream>>>(src, H->perm, n, H->io);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaMemcpyAsync(state_out, H->io, 7 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
     return check_err_flag(H);
 }
 

@@ -217,6 +217,7 @@ struct Handle {
     int npart = 0;
     DevScalars *dsc = nullptr;
     double *tmpd = nullptr;  // scratch, 4*npfb doubles
+    double *io = nullptr;    // 7*npfb staging block of sunset_run_host
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_mode[2] = {-1, -1};
 
