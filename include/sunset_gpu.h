@@ -159,6 +159,26 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
    device time of the nsteps steps. */
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
+/* ---- 3-D (-Ddim3): direct and Newtonian forms, FP64, node sets without boundary nodes ---- */
+/* build_3rd_dimension (setup_domain.F90:435-547) and calc_fd_weights (fd.F90:27-256): after
+   sunset_build_domain, the node set becomes nz layers in z over L_domain_z (the control file's
+   value): dz from the mean spacing, nz = ceiling(L_domain_z/dz), at least ij_count_fd/2 + 2,
+   z-derivatives by periodic central differences of forder + 1 points.  The neighbour lists and
+   weights are built for the layer (the same calls as in 2-D) and serve every layer.  Then
+   sunset_set_state_3d, and sunset_step / sunset_set_tstep / sunset_get_time act on the 3-D
+   state.  Arrays are npfb*nz, layer-major (node iz*npfb + i, reference order in the layer). */
+int sunset_set_layers(SunsetHandle *h, double L_domain_z);
+int sunset_get_layers(SunsetHandle *h, int *nz, double *dz);
+/* initial_solution in 3-D: rho, u, v, w and the six c components (all NULL: c = I) */
+int sunset_set_state_3d(SunsetHandle *h, const double *ro, const double *u, const double *v, const double *w,
+                        const double *cxx, const double *cxy, const double *cyy, const double *cxz,
+                        const double *cyz, const double *czz);
+/* 13*npfb*nz: ro, rou, rov, row, u, v, w, cxx, cxy, cyy, cxz, cyz, czz */
+int sunset_get_state_3d(SunsetHandle *h, double *out);
+/* calc_all_rhs with the dim3 terms (rhs_di.F90): 10*npfb*nz: ro, rou, rov, row, xx, xy, yy,
+   xz, yz, zz */
+int sunset_calc_all_rhs_3d(SunsetHandle *h, double *out);
+
 /* ---- Dumps, restart, checkpoints ---- */
 /* output.F90:184-370 output_layer: the columns of a fields dump, 10*npfb in reference order
    (rho - rho_char, u, v, vorticity, Q criterion, alpha_out = the node's error norm of the

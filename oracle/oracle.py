@@ -89,6 +89,16 @@ def lib():
         L.or_pow4_cr.restype = C.c_double
         L.or_pow4_cr.argtypes = [C.c_double]
         L.or_set_pow_mode.argtypes = [C.c_int]
+        L.or3_create.restype = P
+        L.or3_create.argtypes = [P, C.c_double]
+        L.or3_destroy.argtypes = [P]
+        L.or3_sizes.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.or3_set_state.argtypes = [P, dp, dp, dp, dp, C.c_void_p]
+        L.or3_get_state.argtypes = [P, dp]
+        L.or3_rhs.argtypes = [P, dp]
+        L.or3_set_tstep.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.or3_step.argtypes = [P, C.c_double, C.c_int, C.c_int]
+        L.or3_get_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), dp]
         _lib = L
     return _lib
 
@@ -310,3 +320,67 @@ def for_workload(wl, ns=None, **over):
     o = Oracle(**kw)
     o.build_domain(ns if ns is not None else wl.nodes())
     return o
+
+
+STATE3_FIELDS = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+RHS3_FIELDS = ["ro", "rou", "rov", "row", "xx", "xy", "yy", "xz", "yz", "zz"]
+C3_FIELDS = ["cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+
+
+class Oracle3:
+    """The 3-D (-Ddim3) run built on a set-up 2-D layer (direct and Newtonian forms, node sets
+    without boundary nodes).  Arrays are nl*nz, layer-major."""
+
+    def __init__(self, layer: Oracle, Lz: float):
+        self.layer = layer
+        self.L = layer.L
+        self.h = self.L.or3_create(layer.h, float(Lz))
+        if not self.h:
+            raise OracleError("or3_create: needs weights, no boundary nodes, the direct or Newtonian form, no FENE-P")
+        nl, nz, dz = C.c_int(), C.c_int(), C.c_double()
+        self.L.or3_sizes(self.h, C.byref(nl), C.byref(nz), C.byref(dz))
+        self.nl, self.nz, self.dz = nl.value, nz.value, dz.value
+        self.n = self.nl * self.nz
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.or3_destroy(self.h)
+            self.h = None
+
+    def set_state(self, ro, u, v, w, cxx=None, cxy=None, cyy=None, cxz=None, cyz=None, czz=None):
+        f = lambda a: np.ascontiguousarray(a, np.float64)
+        keep = [f(ro), f(u), f(v), f(w)]
+        ptr = None
+        if cxx is not None:
+            cs = [f(a) for a in (cxx, cxy, cyy, cxz, cyz, czz)]
+            arr = (C.c_void_p * 6)(*[a.ctypes.data for a in cs])
+            keep += cs + [arr]
+            ptr = C.cast(arr, C.c_void_p)
+        self._keep = keep
+        self.L.or3_set_state(self.h, keep[0], keep[1], keep[2], keep[3], ptr)
+
+    def state(self):
+        out = np.zeros(13 * self.n)
+        self.L.or3_get_state(self.h, out)
+        out = out.reshape(13, self.n)
+        return {k: out[i].copy() for i, k in enumerate(STATE3_FIELDS)}
+
+    def rhs(self):
+        out = np.zeros(10 * self.n)
+        self.L.or3_rhs(self.h, out)
+        out = out.reshape(10, self.n)
+        return {k: out[i].copy() for i, k in enumerate(RHS3_FIELDS)}
+
+    def set_tstep(self):
+        a, b = C.c_double(), C.c_double()
+        self.L.or3_set_tstep(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def step(self, dt, nsteps=1, pid=False):
+        self.L.or3_step(self.h, float(dt), int(nsteps), int(pid))
+
+    def time(self):
+        t, dt, it = C.c_double(), C.c_double(), C.c_int()
+        em = np.zeros(3)
+        self.L.or3_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it), em)
+        return dict(time=t.value, dt=dt.value, itime=it.value, emax=em)

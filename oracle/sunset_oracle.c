@@ -2749,3 +2749,438 @@ double or_mass(OrSim *s) {
     for (int i = 0; i < s->npfb; i++) m = m + s->ro[i] * s->vol[i];
     return m;
 }
+
+/* =========================================================================================
+ * 3-D (-Ddim3): build_3rd_dimension (setup_domain.F90:435-547), calc_fd_weights
+ * (fd.F90:27-256), the z parts of derivatives.F90 (:48-63, :96-108, :145-157, :340-352,
+ * :387-405, :441-453) and the dim3 branches of rhs_di.F90 and step.F90, for the direct and
+ * Newtonian forms on node sets without boundary nodes.
+ *
+ * The 3-D node set is nz copies of the 2-D one, layer-major: node k = iz*nl + i at
+ * z = iz*dz.  The reference searches neighbours per layer (neighbours.F90:180-183,223-233,
+ * cells of the node's own layer) over identical positions, and the LABFM weights, sums,
+ * volumes and filter coefficients depend only on those positions, so every layer's lists and
+ * weights are the layer's own (the 2-D OrSim below), used with an offset of iz*nl.  Mirror
+ * images take their parent's value in the same layer; u and v flip with the mirror as in 2-D,
+ * w and c_xz, c_yz are copied unchanged (mirror_boundaries.F90:302-303,324-341).
+ * ========================================================================================= */
+struct Or3 {
+    OrSim *s;                /* the layer */
+    int nl, nz, ncfd;
+    size_t n3;
+    double dz, fdg[13], fdl[13], fdh[13];
+    double *ro, *rou, *rov, *row, *u, *v, *w, *c[6]; /* n3 each; c: xx xy yy xz yz zz */
+    double time, dt, dt_cfl, dt_par;
+    int itime, iRKstep;
+    double emax_nm1, emax_n, emax_np1;
+    char err[256];
+};
+
+/* calc_fd_weights, fd.F90:52-172 (ij_count_fd = forder + 1), then the L_char scaling of
+   :246-247 */
+static int fd_tables(int ncfd, double dz, double L, double *g, double *g2, double *h) {
+    const double one = 1.0, two = 2.0;
+    if (ncfd == 5) {
+        g[0] = (one / 12.0) / dz; g[1] = -((8.0 / 12.0) / dz); g[2] = 0.0; g[3] = (8.0 / 12.0) / dz; g[4] = -((one / 12.0) / dz);
+        g2[0] = -(((one / 12.0) / dz) / dz); g2[1] = ((16.0 / 12.0) / dz) / dz; g2[2] = -(((30.0 / 12.0) / dz) / dz);
+        g2[3] = ((16.0 / 12.0) / dz) / dz; g2[4] = -(((one / 12.0) / dz) / dz);
+        h[0] = -(one / 16.0); h[1] = 4.0 / 16.0; h[2] = -(6.0 / 16.0); h[3] = 4.0 / 16.0; h[4] = -(one / 16.0);
+    } else if (ncfd == 7) {
+        g[0] = -((one / 60.0) / dz); g[1] = (9.0 / 60.0) / dz; g[2] = -((45.0 / 60.0) / dz); g[3] = 0.0;
+        g[4] = (45.0 / 60.0) / dz; g[5] = -((9.0 / 60.0) / dz); g[6] = (one / 60.0) / dz;
+        g2[0] = ((two / 180.0) / dz) / dz; g2[1] = -(((27.0 / 180.0) / dz) / dz); g2[2] = ((270.0 / 180.0) / dz) / dz;
+        g2[3] = -(((490.0 / 180.0) / dz) / dz); g2[4] = ((270.0 / 180.0) / dz) / dz; g2[5] = -(((27.0 / 180.0) / dz) / dz);
+        g2[6] = ((two / 180.0) / dz) / dz;
+        h[0] = one / 64.0; h[1] = -(6.0 / 64.0); h[2] = 15.0 / 64.0; h[3] = -(20.0 / 64.0); h[4] = 15.0 / 64.0;
+        h[5] = -(6.0 / 64.0); h[6] = one / 64.0;
+    } else if (ncfd == 9) {
+        g[0] = (3.0 / 840.0) / dz; g[1] = -((32.0 / 840.0) / dz); g[2] = (168.0 / 840.0) / dz; g[3] = -((672.0 / 840.0) / dz);
+        g[4] = 0.0; g[5] = (672.0 / 840.0) / dz; g[6] = -((168.0 / 840.0) / dz); g[7] = (32.0 / 840.0) / dz;
+        g[8] = -((3.0 / 840.0) / dz);
+        g2[0] = -(((9.0 / 5040.0) / dz) / dz); g2[1] = ((128.0 / 5040.0) / dz) / dz; g2[2] = -(((1008.0 / 5040.0) / dz) / dz);
+        g2[3] = ((8064.0 / 5040.0) / dz) / dz; g2[4] = -(((14350.0 / 5040.0) / dz) / dz); g2[5] = ((8064.0 / 5040.0) / dz) / dz;
+        g2[6] = -(((1008.0 / 5040.0) / dz) / dz); g2[7] = ((128.0 / 5040.0) / dz) / dz; g2[8] = -(((9.0 / 5040.0) / dz) / dz);
+        h[0] = -(one / 256.0); h[1] = 8.0 / 256.0; h[2] = -(28.0 / 256.0); h[3] = 56.0 / 256.0; h[4] = -(70.0 / 256.0);
+        h[5] = 56.0 / 256.0; h[6] = -(28.0 / 256.0); h[7] = 8.0 / 256.0; h[8] = -(one / 256.0);
+    } else if (ncfd == 11) {
+        g[0] = -((one / 1260.0) / dz); g[1] = (5.0 / 504.0) / dz; g[2] = -((5.0 / 84.0) / dz); g[3] = (5.0 / 21.0) / dz;
+        g[4] = -((5.0 / 6.0) / dz); g[5] = 0.0; g[6] = (5.0 / 6.0) / dz; g[7] = -((5.0 / 21.0) / dz); g[8] = (5.0 / 84.0) / dz;
+        g[9] = -((5.0 / 504.0) / dz); g[10] = (one / 1260.0) / dz;
+        g2[0] = ((one / 3150.0) / dz) / dz; g2[1] = -(((5.0 / 1008.0) / dz) / dz); g2[2] = ((5.0 / 126.0) / dz) / dz;
+        g2[3] = -(((5.0 / 21.0) / dz) / dz); g2[4] = ((5.0 / 3.0) / dz) / dz; g2[5] = -(((1086.0 / 371.0) / dz) / dz);
+        g2[6] = ((5.0 / 3.0) / dz) / dz; g2[7] = -(((5.0 / 21.0) / dz) / dz); g2[8] = ((5.0 / 126.0) / dz) / dz;
+        g2[9] = -(((5.0 / 1008.0) / dz) / dz); g2[10] = ((one / 3150.0) / dz) / dz;
+        h[0] = one / 1024.0; h[1] = -(10.0 / 1024.0); h[2] = 45.0 / 1024.0; h[3] = -(120.0 / 1024.0); h[4] = 210.0 / 1024.0;
+        h[5] = -(252.0 / 1024.0); h[6] = 210.0 / 1024.0; h[7] = -(120.0 / 1024.0); h[8] = 45.0 / 1024.0;
+        h[9] = -(10.0 / 1024.0); h[10] = one / 1024.0;
+    } else {
+        return -1;
+    }
+    for (int k = 0; k < ncfd; k++) { g[k] = g[k] / L; g2[k] = (g2[k] / L) / L; }
+    return 0;
+}
+
+Or3 *or3_create(OrSim *s, double Lz) {
+    if (!s || !s->have_weights || s->nb != 0 || !(s->cfg.form == OR_FORM_DI || s->cfg.form == OR_FORM_NEWT) ||
+        s->cfg.fenep || !(Lz > 0.0))
+        return NULL;
+    Or3 *o = (Or3 *)xcalloc(1, sizeof(Or3));
+    o->s = s;
+    o->nl = s->npfb;
+    o->ncfd = s->cfg.forder + 1;
+    /* build_3rd_dimension, :444-483 (mean_alpha = 1, one process in z) */
+    double dzl = 0.0, sv = 0.0;
+    for (int i = 0; i < s->npfb; i++) {
+        sv = sv + s->sp[i] * s->sp[i];
+        dzl = dzl + (s->sp[i] * s->sp[i]) * s->sp[i];
+    }
+    double dz = dzl / sv;
+    const double L = s->cfg.L_char, Lzd = (Lz * L) / L;
+    int nz = (int)ceil((Lzd / dz) / 1.0);
+    dz = (Lzd / (double)nz) / 1.0;
+    if (nz < o->ncfd / 2 + 2) {
+        nz = o->ncfd / 2 + 2;
+        dz = Lzd / (double)(o->ncfd / 2 + 2);
+    }
+    o->nz = nz;
+    o->dz = dz;
+    if (fd_tables(o->ncfd, dz, L, o->fdg, o->fdl, o->fdh)) { free(o); return NULL; }
+    o->n3 = (size_t)o->nl * nz;
+    double **a[] = {&o->ro, &o->rou, &o->rov, &o->row, &o->u, &o->v, &o->w, &o->c[0], &o->c[1], &o->c[2], &o->c[3], &o->c[4], &o->c[5]};
+    for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) *a[k] = (double *)xcalloc(o->n3, sizeof(double));
+    return o;
+}
+
+void or3_destroy(Or3 *o) {
+    if (!o) return;
+    double *a[] = {o->ro, o->rou, o->rov, o->row, o->u, o->v, o->w, o->c[0], o->c[1], o->c[2], o->c[3], o->c[4], o->c[5]};
+    for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) free(a[k]);
+    free(o);
+}
+
+int or3_sizes(Or3 *o, int *nl, int *nz, double *dz) {
+    if (nl) *nl = o->nl;
+    if (nz) *nz = o->nz;
+    if (dz) *dz = o->dz;
+    return 0;
+}
+
+/* sign classes of a field at a mirror image: 0 none, 1 like u, 2 like v, 3 like c_xy */
+static double val3(const Or3 *o, const double *f, int j, size_t off, int cls) {
+    const OrSim *s = o->s;
+    if (j < o->nl) return f[off + j];
+    const int vr = s->vrel[j];
+    const double x = f[off + s->irel[j]];
+    const int flip = (cls == 1 && (vr == 2 || vr == 4)) || (cls == 2 && (vr == 3 || vr == 4)) ||
+                     (cls == 3 && (vr == 2 || vr == 3));
+    return flip ? -x : x;
+}
+/* layer of the m-th point of the z stencil (fd.F90:62-66, periodic in z) */
+static size_t zoff(const Or3 *o, int iz, int m) {
+    int l = (iz + m - o->ncfd / 2) % o->nz;
+    if (l < 0) l += o->nz;
+    return (size_t)l * o->nl;
+}
+
+/* calc_gradient / calc_gradient_only in 3-D: comp bits 1 = x, 2 = y, 4 = z */
+static void grad3(const Or3 *o, const double *f, int cls, int comp, double *gx, double *gy, double *gz) {
+    const OrSim *s = o->s;
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < o->n3; k++) {
+        const int iz = (int)(k / o->nl), i = (int)(k % o->nl);
+        const size_t off = (size_t)iz * o->nl;
+        if (comp & 3) {
+            double g1 = 0.0, g2 = 0.0;
+            const int *lk = s->ij_link + (size_t)i * nplink;
+            const double *wg = s->w_grad + 2 * (size_t)i * nplink;
+            for (int q = 0; q < s->ij_count_small[i]; q++) {
+                const double pj = val3(o, f, lk[q], off, cls);
+                if (comp & 1) g1 = g1 + pj * wg[2 * q];
+                if (comp & 2) g2 = g2 + pj * wg[2 * q + 1];
+            }
+            if (comp & 1) gx[k] = g1 - f[k] * s->w_grad_sum[2 * i];
+            if (comp & 2) gy[k] = g2 - f[k] * s->w_grad_sum[2 * i + 1];
+        }
+        if (comp & 4) {
+            double t = 0.0;
+            for (int m = 0; m < o->ncfd; m++) t = t + f[zoff(o, iz, m) + i] * o->fdg[m];
+            gz[k] = t;
+        }
+    }
+}
+/* calc_laplacian in 3-D (:73-108) */
+static void lap3(const Or3 *o, const double *f, int cls, double *lap) {
+    const OrSim *s = o->s;
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < o->n3; k++) {
+        const int iz = (int)(k / o->nl), i = (int)(k % o->nl);
+        const size_t off = (size_t)iz * o->nl;
+        double l = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wl = s->w_lap + (size_t)i * nplink;
+        for (int q = 0; q < s->ij_count_small[i]; q++) l = l + val3(o, f, lk[q], off, cls) * wl[q];
+        double r = l - f[k] * s->w_lap_sum[i];
+        double t = 0.0;
+        for (int m = 0; m < o->ncfd; m++) t = t + f[zoff(o, iz, m) + i] * o->fdl[m];
+        lap[k] = r + t;
+    }
+}
+/* calc_filtered_var in 3-D (:360-405): the x-y filter, then the z filter of the result */
+static void filter3(const Or3 *o, double *f, int cls, double *work) {
+    const OrSim *s = o->s;
+    const int nplink = s->nplink;
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < o->n3; k++) {
+        const int iz = (int)(k / o->nl), i = (int)(k % o->nl);
+        const size_t off = (size_t)iz * o->nl;
+        double t = 0.0;
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        const double *wh = s->w_hyp + (size_t)i * nplink;
+        for (int q = 0; q < s->ij_count[i]; q++) t = t + val3(o, f, lk[q], off, cls) * wh[q];
+        work[k] = f[k] + (t - f[k] * s->w_hyp_sum[i]);
+    }
+    memcpy(f, work, sizeof(double) * o->n3);
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < o->n3; k++) {
+        const int iz = (int)(k / o->nl), i = (int)(k % o->nl);
+        double t = 0.0;
+        for (int m = 0; m < o->ncfd; m++) t = t + f[zoff(o, iz, m) + i] * o->fdh[m];
+        work[k] = f[k] + t;
+    }
+    memcpy(f, work, sizeof(double) * o->n3);
+}
+
+/* hardcode_initial_conditions in 3-D: rho, u, v, w and c given; rho u = rho * u ... */
+int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, const double *w,
+                  const double *const *c6) {
+    for (size_t k = 0; k < o->n3; k++) {
+        o->ro[k] = ro[k]; o->u[k] = u[k]; o->v[k] = v[k]; o->w[k] = w[k];
+        o->rou[k] = o->ro[k] * o->u[k]; o->rov[k] = o->ro[k] * o->v[k]; o->row[k] = o->ro[k] * o->w[k];
+        for (int q = 0; q < 6; q++) o->c[q][k] = c6 ? c6[q][k] : ((q == 0 || q == 2 || q == 5) ? 1.0 : 0.0);
+    }
+    o->time = 0.0; o->itime = 0; o->dt = 1.0e-6;
+    o->emax_np1 = o->emax_n = o->emax_nm1 = pid_tol;
+    return 0;
+}
+int or3_get_state(Or3 *o, double *out /* 13 x n3: ro rou rov row u v w cxx cxy cyy cxz cyz czz */) {
+    const double *a[13] = {o->ro, o->rou, o->rov, o->row, o->u, o->v, o->w, o->c[0], o->c[1], o->c[2], o->c[3], o->c[4], o->c[5]};
+    for (int f = 0; f < 13; f++) memcpy(out + (size_t)f * o->n3, a[f], sizeof(double) * o->n3);
+    return 0;
+}
+
+/* calc_all_rhs in 3-D (rhs_di.F90:45-599, interior branches with the dim3 terms):
+   r[10] = ro, rou, rov, row, xx, xy, yy, xz, yz, zz */
+static void rhs3(Or3 *o, double *const *r) {
+    const OrSim *s = o->s;
+    const size_t n = o->n3;
+    const int di = s->cfg.form == OR_FORM_DI, full = s->cfg.di_full_gradients;
+    enum { ROX, ROY, ROZ, UX, UY, UZ, VX, VY, VZ, WX, WY, WZ, LU, LV, LW, NG0 };
+    double *G[NG0];
+    for (int q = 0; q < NG0; q++) G[q] = zarr((int)n);
+    grad3(o, o->ro, 0, 7, G[ROX], G[ROY], G[ROZ]);
+    grad3(o, o->u, 1, 7, G[UX], G[UY], G[UZ]);
+    grad3(o, o->v, 2, 7, G[VX], G[VY], G[VZ]);
+    grad3(o, o->w, 0, 7, G[WX], G[WY], G[WZ]);
+    lap3(o, o->u, 1, G[LU]);
+    lap3(o, o->v, 2, G[LV]);
+    lap3(o, o->w, 0, G[LW]);
+    /* conformation gradients: c_xx x only, c_xy, c_xz, c_yz full, c_yy y only, c_zz z only
+       (rhs_di.F90:186-194), the others computed only with full gradients (else zero) */
+    double *gc[6][3], *lc[6];
+    static const int ccls[6] = {0, 3, 0, 0, 0, 0};
+    static const int cmask[6] = {1, 7, 2, 7, 7, 4};
+    for (int q = 0; q < 6; q++) {
+        for (int d = 0; d < 3; d++) gc[q][d] = zarr((int)n);
+        lc[q] = zarr((int)n);
+        if (!di) continue;
+        grad3(o, o->c[q], ccls[q], full ? 7 : cmask[q], gc[q][0], gc[q][1], gc[q][2]);
+        if (s->cfg.Mdiff != 0.0) lap3(o, o->c[q], ccls[q], lc[q]);
+    }
+    const double csq = s->csq, cs = s->visc_solvent, cp = s->visc_polymeric / s->lambda;
+    const double *g = s->cfg.grav, *df = s->driving_force;
+    const double kol = (1.0 + (s->cfg.Mdiff * s->cfg.beta) * s->cfg.Wi), kold = (1.0 + s->cfg.Mdiff * s->cfg.Wi);
+    const double lambda = s->lambda, eps = s->cfg.epsPTT, Md = s->cfg.Mdiff;
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < n; k++) {
+        const int i = (int)(k % o->nl);
+        const double ro = o->ro[k], u = o->u[k], v = o->v[k], w = o->w[k];
+        const double gpx = csq * G[ROX][k], gpy = csq * G[ROY][k], gpz = csq * G[ROZ][k];
+        /* calc_rhs_ro, :128-139 */
+        const double tmp = ((u * G[ROX][k] + v * G[ROY][k]) + w * G[ROZ][k]);
+        const double divv = (G[UX][k] + G[VY][k]) + G[WZ][k];
+        const double rr = -ro * divv - tmp;
+        /* calc_rhs_rovel, :215-275 */
+        const double tsu = ro * ((u * G[UX][k] + v * G[UY][k]) + w * G[UZ][k]) - u * rr;
+        const double tsv = ro * ((u * G[VX][k] + v * G[VY][k]) + w * G[VZ][k]) - v * rr;
+        const double tsw = ro * ((u * G[WX][k] + v * G[WY][k]) + w * G[WZ][k]) - w * rr;
+        double fvu = cs * G[LU][k], fvv = cs * G[LV][k], fvw = cs * G[LW][k];
+        if (di) {
+            fvu = fvu + cp * ((gc[0][0][k] + gc[1][1][k]) + gc[3][2][k]);
+            fvv = fvv + cp * ((gc[1][0][k] + gc[2][1][k]) + gc[4][2][k]);
+            fvw = fvw + cp * ((gc[3][0][k] + gc[4][1][k]) + gc[5][2][k]);
+        }
+        double bfu = ro * (g[0] + df[0]), bfv = ro * (g[1] + df[1]), bfw = ro * (g[2] + df[2]);
+        if (s->kolmo) bfu = bfu + (((1.0 / s->cfg.Re) * cos(s->ry[i])) * kol) / kold;
+        r[0][k] = rr;
+        r[1][k] = ((-tsu - gpx) + bfu) + fvu;
+        r[2][k] = ((-tsv - gpy) + bfv) + fvv;
+        r[3][k] = ((-tsw - gpz) + bfw) + fvw;
+        for (int q = 4; q < 10; q++) r[q][k] = 0.0;
+        if (!di) continue;
+        /* calc_rhs_c, :415-476 */
+        const double cxx = o->c[0][k], cxy = o->c[1][k], cyy = o->c[2][k], cxz = o->c[3][k], cyz = o->c[4][k], czz = o->c[5][k];
+        double ad[6];
+        for (int q = 0; q < 6; q++) ad[q] = -((u * gc[q][0][k] + v * gc[q][1][k]) + w * gc[q][2][k]);
+        const double ux = G[UX][k], uy = G[UY][k], uz = G[UZ][k], vx = G[VX][k], vy = G[VY][k], vz = G[VZ][k];
+        const double wx = G[WX][k], wy = G[WY][k], wz = G[WZ][k];
+        const double ucxx = ((2.0 * ux) * cxx + (2.0 * uy) * cxy) + (2.0 * uz) * cxz;
+        const double ucxy = (((((ux * cxy + uy * cyy) + uz * cyz) + vx * cxx) + vy * cxy) + vz * cxz);
+        const double ucyy = ((2.0 * vx) * cxy + (2.0 * vy) * cyy) + (2.0 * vz) * cyz;
+        const double uczz = ((2.0 * wx) * cxz + (2.0 * wy) * cyz) + (2.0 * wz) * czz;
+        const double ucxz = (((((ux * cxz + uy * cyz) + uz * czz) + wx * cxx) + wy * cxy) + wz * cxz);
+        const double ucyz = (((((vx * cxz + vy * cyz) + vz * czz) + wx * cxy) + wy * cyy) + wz * cyz);
+        const double fr = -(((1.0 - eps * 2.0) + eps * ((cxx + cyy) + czz))) / lambda;
+        const double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0);
+        const double sxz = fr * cxz, syz = fr * cyz, szz = fr * (czz - 1.0);
+        r[4][k] = ((ad[0] + ucxx) + sxx) + Md * lc[0][k];
+        r[5][k] = ((ad[1] + ucxy) + sxy) + Md * lc[1][k];
+        r[6][k] = ((ad[2] + ucyy) + syy) + Md * lc[2][k];
+        r[7][k] = ((ad[3] + ucxz) + sxz) + Md * lc[3][k];
+        r[8][k] = ((ad[4] + ucyz) + syz) + Md * lc[4][k];
+        r[9][k] = ((ad[5] + uczz) + szz) + Md * lc[5][k];
+    }
+    for (int q = 0; q < NG0; q++) free(G[q]);
+    for (int q = 0; q < 6; q++) { for (int d = 0; d < 3; d++) free(gc[q][d]); free(lc[q]); }
+}
+
+int or3_rhs(Or3 *o, double *out /* 10 x n3 */) {
+    double *r[10];
+    for (int q = 0; q < 10; q++) r[q] = out + (size_t)q * o->n3;
+    rhs3(o, r);
+    return 0;
+}
+
+/* set_tstep (step.F90:569-622) over the 3-D nodes */
+int or3_set_tstep(Or3 *o, double *dt_cfl, double *dt_par) {
+    const OrSim *s = o->s;
+    double dcfl = 1.0e10, dvisc = 1.0e10;
+    for (size_t k = 0; k < o->n3; k++) {
+        const int i = (int)(k % o->nl);
+        const double c = sqrt(s->csq);
+        const double um = sqrt((o->u[k] * o->u[k] + o->v[k] * o->v[k]) + o->w[k] * o->w[k]);
+        const double t = s->sp[i] / (um + c);
+        dcfl = (t < dcfl) ? t : dcfl;
+        const double tv = ((s->sp[i] * s->sp[i]) * o->ro[k]) / s->visc_total;
+        dvisc = (tv < dvisc) ? tv : dvisc;
+    }
+    o->dt_cfl = (1.0 * dcfl) * s->cfg.L_char;
+    o->dt_par = (((2.0 / 3.0) * dvisc) * s->cfg.L_char) * s->cfg.L_char;
+    if (dt_cfl) *dt_cfl = o->dt_cfl;
+    if (dt_par) *dt_par = o->dt_par;
+    return 0;
+}
+
+/* step_rk3_4S_2R_EE (step.F90:218-512) in 3-D, without boundary nodes */
+static void step3(Or3 *o) {
+    const OrSim *s = o->s;
+    const size_t n = o->n3;
+    const int di = s->cfg.form == OR_FORM_DI, nf = di ? 10 : 4;
+    const double a[3] = {RK_A21, RK_A32, RK_A43}, b[4] = {RK_B1, RK_B2, RK_B3, RK_B4};
+    const double bh[4] = {RK_BH1, RK_BH2, RK_BH3, RK_BH4};
+    const double cc[4] = {0.0, RK_A21, RK_A32 + RK_B1, 1.0};
+    const double dt = o->dt;
+    o->emax_nm1 = o->emax_n;
+    o->emax_n = o->emax_np1;
+    double *Q[10] = {o->ro, o->rou, o->rov, o->row, o->c[0], o->c[1], o->c[2], o->c[3], o->c[4], o->c[5]};
+    double *reg[10], *eacc[10], *r[10];
+    for (int f = 0; f < 10; f++) { reg[f] = zarr((int)n); eacc[f] = zarr((int)n); r[f] = zarr((int)n); }
+    for (int f = 0; f < nf; f++) memcpy(reg[f], Q[f], sizeof(double) * n);
+    const double time0 = o->time;
+    o->iRKstep = 0;
+    for (int st = 0; st < 4; st++) {
+        o->iRKstep++;
+        o->time = time0 + dt * cc[st];
+        rhs3(o, r);
+        const double RKb = dt * b[st], RKbmbh = dt * (b[st] - bh[st]);
+        if (st < 3) {
+            const double RKa = dt * a[st];
+#pragma omp parallel for schedule(static)
+            for (size_t k = 0; k < n; k++)
+                for (int f = 0; f < nf; f++) {
+                    Q[f][k] = reg[f][k] + RKa * r[f][k];
+                    reg[f][k] = reg[f][k] + RKb * r[f][k];
+                    eacc[f][k] = eacc[f][k] + RKbmbh * r[f][k];
+                }
+            for (size_t k = 0; k < n; k++) { /* get_velocity_from_momentum */
+                const double oo = 1.0 / o->ro[k];
+                o->u[k] = o->rou[k] * oo; o->v[k] = o->rov[k] * oo; o->w[k] = o->row[k] * oo;
+            }
+        } else {
+            double en[10] = {0};
+            const double norms[10] = {1.0, 1.0 / (1.0 * s->cfg.U_char), 1.0 / (1.0 * s->cfg.U_char), 1.0 / (1.0 * s->cfg.U_char),
+                                      1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+            for (size_t k = 0; k < n; k++)
+                for (int f = 0; f < nf; f++) {
+                    Q[f][k] = reg[f][k] + RKb * r[f][k];
+                    eacc[f][k] = eacc[f][k] + RKbmbh * r[f][k];
+                    const double t = fabs(eacc[f][k]) * norms[f];
+                    en[f] = (t > en[f]) ? t : en[f];
+                }
+#define MAXD(x, y) ((x) > (y) ? (x) : (y))
+            /* :475-483 (xx xy yy xz yz zz; ro rou rov row) */
+            const double econf = MAXD(en[4], MAXD(en[5], MAXD(en[6], MAXD(en[7], MAXD(en[8], en[9])))));
+            o->emax_np1 = MAXD(econf, MAXD(en[0], MAXD(en[1], MAXD(en[2], MAXD(en[3], doublesmall)))));
+#undef MAXD
+        }
+    }
+    /* filter_variables (rhs_di.F90:667-720): ro, rou, rov, row, then c; the mass correction */
+    static const int cls[10] = {0, 1, 2, 0, 0, 3, 0, 0, 0, 0};
+    for (int f = 0; f < nf; f++) filter3(o, Q[f], cls[f], r[0]);
+    if (s->cfg.mcorr) {
+        double tm = 0.0, tv = 0.0;
+        for (size_t k = 0; k < n; k++) {
+            const int i = (int)(k % o->nl);
+            tm = tm + (o->ro[k] - s->rho_char) * s->vol[i];
+            tv = tv + s->vol[i];
+        }
+        const double dro = tm / tv;
+        for (size_t k = 0; k < n; k++) o->ro[k] = o->ro[k] - dro;
+    }
+    for (size_t k = 0; k < n; k++) {
+        const double oo = 1.0 / o->ro[k];
+        o->u[k] = o->rou[k] * oo; o->v[k] = o->rov[k] * oo; o->w[k] = o->row[k] * oo;
+    }
+    for (int f = 0; f < 10; f++) { free(reg[f]); free(eacc[f]); free(r[f]); }
+}
+
+int or3_step(Or3 *o, double dt, int nsteps, int pid) {
+    for (int q = 0; q < nsteps; q++) {
+        if (pid) {
+            or3_set_tstep(o, NULL, NULL);
+            double facA = PID_A * log(pid_tol / o->emax_np1);
+            double facB = PID_B * log(o->emax_n / pid_tol);
+            double facC = PID_C * log(pid_tol / o->emax_nm1);
+            double f = pid_k * exp((facA + facB) + facC);
+            f = (0.5 > f) ? 0.5 : f;
+            f = (1.02 < f) ? 1.02 : f;
+            o->dt = o->dt * f;
+            const double dmax = (o->dt_cfl < o->dt_par) ? o->dt_cfl : o->dt_par;
+            if (o->dt > dmax) o->dt = dmax;
+        } else {
+            o->dt = dt;
+        }
+        step3(o);
+        o->itime++;
+    }
+    return 0;
+}
+
+int or3_get_time(Or3 *o, double *time, double *dt, int *itime, double *emax) {
+    if (time) *time = o->time;
+    if (dt) *dt = o->dt;
+    if (itime) *itime = o->itime;
+    if (emax) { emax[0] = o->emax_nm1; emax[1] = o->emax_n; emax[2] = o->emax_np1; }
+    return 0;
+}

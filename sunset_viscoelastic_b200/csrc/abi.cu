@@ -501,6 +501,7 @@ int sunset_set_state(SunsetHandle *sh, const double *ro, const double *u, const 
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (!ro || !u || !v || !cxx || !cxy || !cyy) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (H->nz > 0) return set_err(H, SUNSET_ERR_ARG, "a 3-D handle: use sunset_set_state_3d");
     const int n = H->npfb;
     // stage the seven inputs in internal order inside the (not yet used) second buffer and rhs
     double *d[7] = {H->rhs[0], H->rhs[1], H->rhs[2], H->rhs[3], H->rhs[4], H->rhs[5], H->rhs[6]};
@@ -536,6 +537,55 @@ int sunset_get_state(SunsetHandle *sh, double *out) {
     return 0;
 }
 
+int sunset_set_layers(SunsetHandle *sh, double L_domain_z) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->domain_ok, "sunset_build_domain")) return rc;
+    if (H->state_ok || H->state3_ok || H->nz > 0) return set_err(H, SUNSET_ERR_ARG, "set the layers once, before the state");
+    if (int rc = set_device(H)) return rc;
+    return layers_set(H, L_domain_z);
+}
+
+int sunset_get_layers(SunsetHandle *sh, int *nz, double *dz) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (nz) *nz = H->nz;
+    if (dz) *dz = H->dz;
+    return 0;
+}
+
+int sunset_set_state_3d(SunsetHandle *sh, const double *ro, const double *u, const double *v, const double *w,
+                        const double *cxx, const double *cxy, const double *cyy, const double *cxz, const double *cyz,
+                        const double *czz) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (H->nz == 0) return set_err(H, SUNSET_ERR_ARG, "call order: sunset_set_layers first");
+    if (!ro || !u || !v || !w) return set_err(H, SUNSET_ERR_ARG, "null array");
+    const bool anyc = cxx || cxy || cyy || cxz || cyz || czz, allc = cxx && cxy && cyy && cxz && cyz && czz;
+    if (anyc && !allc) return set_err(H, SUNSET_ERR_ARG, "give all six c components or none");
+    const double *f[10] = {ro, u, v, w, cxx, cxy, cyy, cxz, cyz, czz};
+    if (int rc = state3_set(H, f)) return rc;
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    H->state3_ok = true;
+    return 0;
+}
+
+int sunset_get_state_3d(SunsetHandle *sh, double *out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+    if (!out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    return state3_get(H, out);
+}
+
+int sunset_calc_all_rhs_3d(SunsetHandle *sh, double *out) {
+    Handle *H;
+    if (int rc = op_common(sh, &H)) return rc;
+    if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+    if (!out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    return rhs3_calc(H, out);
+}
+
 int sunset_calc_all_rhs(SunsetHandle *sh, double *out) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
@@ -549,8 +599,13 @@ int sunset_calc_all_rhs(SunsetHandle *sh, double *out) {
 int sunset_set_tstep(SunsetHandle *sh, double *dt_cfl, double *dt_parabolic) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
-    if (int rc = set_tstep_device(H)) return rc;
+    if (H->nz > 0) {
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        if (int rc = tstep3(H)) return rc;
+    } else {
+        if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+        if (int rc = set_tstep_device(H)) return rc;
+    }
     DevScalars s;
     SUNSET_CUDA(H, cudaMemcpyAsync(&s, H->dsc, sizeof(s), cudaMemcpyDeviceToHost, H->stream));
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
@@ -562,9 +617,14 @@ int sunset_set_tstep(SunsetHandle *sh, double *dt_cfl, double *dt_parabolic) {
 int sunset_step(SunsetHandle *sh, double dt, int nsteps, int mode) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (nsteps < 0 || (mode == 0 && !(dt > 0.0)) || mode < 0 || mode > 1)
         return set_err(H, SUNSET_ERR_ARG, "bad dt/nsteps/mode");
+    if (H->nz > 0) {
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        if (int rc = step3_run(H, dt, nsteps, mode)) return rc;
+        return check_err_flag(H);
+    }
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (int rc = step_run(H, dt, nsteps, mode)) return rc;
     return check_err_flag(H);
 }

@@ -155,7 +155,7 @@ struct Handle {
     std::vector<int> h_perm, h_iperm;  // internal <-> reference
     std::vector<int> h_gi;             // global index of each node (reference order; FD rows: parent's + j)
     bool domain_ok = false, nbr_ok = false, w_ok = false, bw_ok = false, sums_ok = false, fc_ok = false;
-    bool state_ok = false;
+    bool state_ok = false, state3_ok = false;
 
     // ---- device: points (internal interior 0..npfb-1, ghosts npfb..np-1) ----
     double *px = nullptr, *py = nullptr;       // np
@@ -218,6 +218,13 @@ struct Handle {
     DevScalars *dsc = nullptr;
     double *tmpd = nullptr;  // scratch, 4*npfb doubles
     double *io = nullptr;    // 7*npfb staging block of sunset_run_host
+
+    // ---- 3-D (step3d.cu): nz layers of the node set, z stencils of fd.F90 ----
+    int nz = 0, ncfd = 0, cur3 = 0;
+    double dz = 0.0, fdg[13] = {}, fdl[13] = {}, fdh[13] = {};
+    double *f3[2][13] = {};  // per buffer: ro rou rov row u v w cxx cxy cyy cxz cyz czz (layer-major)
+    double *reg3[10] = {}, *eacc3[10] = {}, *rhs3[10] = {};
+    double *g3 = nullptr, *tmp3 = nullptr, *partials3 = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_mode[2] = {-1, -1};
 
@@ -297,6 +304,13 @@ int state_alloc(Handle *H);
 int state_set_device(Handle *H, const double *ro, const double *u, const double *v, const double *cxx,
                      const double *cxy, const double *cyy, const double *czz);  // internal order, device
 int state_set_conservative_device(Handle *H, const double *const *f7);  // internal order, device
+// 3-D (step3d.cu)
+int layers_set(Handle *H, double Lz);
+int state3_set(Handle *H, const double *const *fields10);
+int state3_get(Handle *H, double *out13);
+int rhs3_calc(Handle *H, double *out10);
+int tstep3(Handle *H);
+int step3_run(Handle *H, double dt, int nsteps, int mode);
 int step_run(Handle *H, double dt, int nsteps, int mode);
 int rhs_only(Handle *H);
 int set_tstep_device(Handle *H);

@@ -1,0 +1,656 @@
+// step3d.cu -- the 3-D (-Ddim3) time step of the direct and Newtonian forms on node sets
+// without boundary nodes.
+//
+// The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
+// setup_domain.F90:435-547), layer-major: node k = iz*nl + i at z = iz*dz.  The reference builds
+// the neighbour lists per layer from identical positions (neighbours.F90:180-183,223-233), so
+// every layer uses the layer's lists and LABFM weights (built once, 2-D); only the state is
+// 3-D.  z-derivatives are the periodic central differences of fd.F90 (ij_count_fd = forder+1
+// points) over the same node in the neighbouring layers.  Mirror images take their parent's
+// value in the same layer, u and v with the mirror's sign, w, c_xz and c_yz unchanged
+// (mirror_boundaries.F90:302-303,324-341).
+//
+// Structure, as calc_all_rhs: one gather kernel per field and derivative set (x-y LABFM sums
+// in the reference's link order, then the z stencil), then a pointwise kernel for the
+// right-hand side and the RK update; the filter as the x-y filter followed by the z filter of
+// its result (derivatives.F90:387-405); the mass correction and the derived fields; all FP64.
+#include "internal.cuh"
+
+namespace sunset {
+
+namespace {
+
+constexpr int kMaxFd = 13;
+constexpr int kG3 = 39;  // derivative arrays, see enum G3
+
+struct Layer3 {
+    int nl, nz, ncfd;
+    const long long *slice_ptr;
+    const int *cnt, *cnt_small, *lidx;
+    const double *wx, *wy, *wl, *wh, *gsx, *gsy, *lsum, *hsum;
+    double fdg[kMaxFd], fdl[kMaxFd], fdh[kMaxFd];
+};
+
+// derivative arrays (each nl*nz)
+enum G3 {
+    ROX, ROY, ROZ, UX, UY, UZ, VX, VY, VZ, WX, WY, WZ, LU, LV, LW,
+    CG0 = 15,  // c grads: CG0 + 3*q + d, q = xx xy yy xz yz zz, d = x y z
+    LC0 = 33   // c Laplacians: LC0 + q
+};
+
+// sign class of a field at a mirror image: 0 none, 1 like u (x mirrors), 2 like v (y
+// mirrors), 3 like c_xy (one of the two); code = vrelation - 1 (1 x, 2 y, 3 both)
+__device__ __forceinline__ double mirror_value(double x, int cls, int code) {
+    const bool flip = (cls == 1 && (code == 1 || code == 3)) || (cls == 2 && (code == 2 || code == 3)) ||
+                      (cls == 3 && (code == 1 || code == 2));
+    return flip ? -x : x;
+}
+
+__device__ __forceinline__ size_t zlayer(const Layer3 &L, int iz, int m) {
+    int l = (iz + m - L.ncfd / 2) % L.nz;
+    if (l < 0) l += L.nz;
+    return (size_t)l * L.nl;
+}
+
+// calc_gradient / calc_gradient_only / calc_laplacian in 3-D (derivatives.F90:26-116,416-464):
+// comp bits 1 = d/dx, 2 = d/dy, 4 = d/dz; lap: the x-y Laplacian plus the z second difference.
+__global__ void k3_deriv(Layer3 L, const double *f, int cls, int comp, double *gx, double *gy, double *gz,
+                         double *lap) {
+    const size_t n = (size_t)L.nl * L.nz;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
+    const size_t off = (size_t)iz * L.nl;
+    if ((comp & 3) || lap) {
+        const long long base = L.slice_ptr[i >> 5];
+        double sx = 0.0, sy = 0.0, sl = 0.0;
+        const int cs = L.cnt_small[i];
+        for (int q = 0; q < cs; q++) {
+            const long long o = sell_at(base, q, i & 31);
+            const int l = __ldg(L.lidx + o);
+            const double pj = mirror_value(f[off + (l & kLinkMask)], cls, (int)((unsigned)l >> 30));
+            if (comp & 1) sx = sx + pj * __ldg(L.wx + o);
+            if (comp & 2) sy = sy + pj * __ldg(L.wy + o);
+            if (lap) sl = sl + pj * __ldg(L.wl + o);
+        }
+        const double p = f[k];
+        if (comp & 1) gx[k] = sx - p * L.gsx[i];
+        if (comp & 2) gy[k] = sy - p * L.gsy[i];
+        if (lap) {
+            const double r = sl - p * L.lsum[i];
+            double t = 0.0;
+            for (int m = 0; m < L.ncfd; m++) t = t + f[zlayer(L, iz, m) + i] * L.fdl[m];
+            lap[k] = r + t;
+        }
+    }
+    if (comp & 4) {
+        double t = 0.0;
+        for (int m = 0; m < L.ncfd; m++) t = t + f[zlayer(L, iz, m) + i] * L.fdg[m];
+        gz[k] = t;
+    }
+}
+
+// calc_filtered_var in 3-D: the x-y filter (into out) ...
+__global__ void k3_filter_xy(Layer3 L, const double *f, int cls, double *out) {
+    const size_t n = (size_t)L.nl * L.nz;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
+    const size_t off = (size_t)iz * L.nl;
+    const long long base = L.slice_ptr[i >> 5];
+    double t = 0.0;
+    for (int q = 0; q < L.cnt[i]; q++) {
+        const long long o = sell_at(base, q, i & 31);
+        const int l = __ldg(L.lidx + o);
+        t = t + mirror_value(f[off + (l & kLinkMask)], cls, (int)((unsigned)l >> 30)) * __ldg(L.wh + o);
+    }
+    const double p = f[k];
+    out[k] = p + (t - p * L.hsum[i]);
+}
+// ... then the z filter of that result (back into the field)
+__global__ void k3_filter_z(Layer3 L, const double *in, double *out) {
+    const size_t n = (size_t)L.nl * L.nz;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
+    double t = 0.0;
+    for (int m = 0; m < L.ncfd; m++) t = t + in[zlayer(L, iz, m) + i] * L.fdh[m];
+    out[k] = in[k] + t;
+}
+
+struct Point3 {
+    StepConsts K;
+    int nl, nz, di, full, md;
+    const double *py;                     // node ordinate (Kolmogorov forcing)
+    const double *G;                      // kG3 derivative arrays
+    const double *in[13];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz
+    double *out[13];
+    double *reg[10], *eacc[10], *rhs[10];
+    DevScalars *sc;
+    int stage;                            // 0..3, 4 = right-hand side only
+};
+
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
+// 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).
+__global__ void __launch_bounds__(128) k3_point(Point3 P) {
+    const size_t n = (size_t)P.nl * P.nz;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long eb = 0;
+    if (k < n) {
+        const StepConsts &K = P.K;
+        const double *G = P.G;
+        auto g = [&](int a) { return G[(size_t)a * n + k]; };
+        const int i = (int)(k % P.nl);
+        const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
+        const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
+        const double tmp = ((u * g(ROX) + v * g(ROY)) + w * g(ROZ));
+        const double divv = (g(UX) + g(VY)) + g(WZ);
+        const double rr = -ro * divv - tmp;
+        const double tsu = ro * ((u * g(UX) + v * g(UY)) + w * g(UZ)) - u * rr;
+        const double tsv = ro * ((u * g(VX) + v * g(VY)) + w * g(VZ)) - v * rr;
+        const double tsw = ro * ((u * g(WX) + v * g(WY)) + w * g(WZ)) - w * rr;
+        double fvu = K.coef_solvent * g(LU), fvv = K.coef_solvent * g(LV), fvw = K.coef_solvent * g(LW);
+        if (P.di) {
+            fvu = fvu + K.coef_polymeric * ((g(CG0 + 0) + g(CG0 + 3 + 1)) + g(CG0 + 9 + 2));
+            fvv = fvv + K.coef_polymeric * ((g(CG0 + 3 + 0) + g(CG0 + 6 + 1)) + g(CG0 + 12 + 2));
+            fvw = fvw + K.coef_polymeric * ((g(CG0 + 9 + 0) + g(CG0 + 12 + 1)) + g(CG0 + 15 + 2));
+        }
+        double bfu = ro * (K.grav0 + P.sc->df), bfv = ro * (K.grav1 + 0.0), bfw = ro * (0.0 + 0.0);
+        if (K.kolmo)
+            bfu = bfu + (((1.0 / K.Re) * cos(P.py[i])) * (1.0 + (K.Mdiff * K.beta) * K.Wi)) / (1.0 + K.Mdiff * K.Wi);
+        double r[10];
+        r[0] = rr;
+        r[1] = ((-tsu - gpx) + bfu) + fvu;
+        r[2] = ((-tsv - gpy) + bfv) + fvv;
+        r[3] = ((-tsw - gpz) + bfw) + fvw;
+        for (int q = 4; q < 10; q++) r[q] = 0.0;
+        if (P.di) {
+            const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
+                         czz = P.in[12][k];
+            double ad[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) ad[q] = -((u * g(CG0 + 3 * q) + v * g(CG0 + 3 * q + 1)) + w * g(CG0 + 3 * q + 2));
+            const double ux = g(UX), uy = g(UY), uz = g(UZ), vx = g(VX), vy = g(VY), vz = g(VZ);
+            const double wx = g(WX), wy = g(WY), wz = g(WZ);
+            const double ucxx = ((2.0 * ux) * cxx + (2.0 * uy) * cxy) + (2.0 * uz) * cxz;
+            const double ucxy = (((((ux * cxy + uy * cyy) + uz * cyz) + vx * cxx) + vy * cxy) + vz * cxz);
+            const double ucyy = ((2.0 * vx) * cxy + (2.0 * vy) * cyy) + (2.0 * vz) * cyz;
+            const double uczz = ((2.0 * wx) * cxz + (2.0 * wy) * cyz) + (2.0 * wz) * czz;
+            const double ucxz = (((((ux * cxz + uy * cyz) + uz * czz) + wx * cxx) + wy * cxy) + wz * cxz);
+            const double ucyz = (((((vx * cxz + vy * cyz) + vz * czz) + wx * cxy) + wy * cyy) + wz * cyz);
+            const double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+            const double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0);
+            const double sxz = fr * cxz, syz = fr * cyz, szz = fr * (czz - 1.0);
+            const double Md = K.Mdiff;
+            auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
+            r[4] = ((ad[0] + ucxx) + sxx) + Md * lc(0);
+            r[5] = ((ad[1] + ucxy) + sxy) + Md * lc(1);
+            r[6] = ((ad[2] + ucyy) + syy) + Md * lc(2);
+            r[7] = ((ad[3] + ucxz) + sxz) + Md * lc(3);
+            r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
+            r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
+        }
+        const int nf = P.di ? 10 : 4;
+        if (P.stage == 4) {
+            for (int q = 0; q < 10; q++) P.rhs[q][k] = r[q];
+        } else {
+            static constexpr int src[10] = {0, 1, 2, 3, 7, 8, 9, 10, 11, 12};
+            const int stage = P.stage;
+            const double dt = P.sc->dt;
+            const double a = stage == 0 ? SUNSET_RK_A21 : stage == 1 ? SUNSET_RK_A32 : SUNSET_RK_A43;
+            const double b = stage == 0 ? SUNSET_RK_B1 : stage == 1 ? SUNSET_RK_B2 : stage == 2 ? SUNSET_RK_B3 : SUNSET_RK_B4;
+            const double bh = stage == 0 ? SUNSET_RK_BH1 : stage == 1 ? SUNSET_RK_BH2 : stage == 2 ? SUNSET_RK_BH3 : SUNSET_RK_BH4;
+            const double RKb = dt * b, RKbmbh = dt * (b - bh);
+            double Un[10];
+            double en = 0.0;
+            for (int q = 0; q < 10; q++) Un[q] = P.in[src[q]][k];
+            for (int q = 0; q < nf; q++) {
+                const double S = stage == 0 ? P.in[src[q]][k] : P.reg[q][k];
+                const double E = stage == 0 ? 0.0 : P.eacc[q][k];
+                if (stage < 3) {
+                    Un[q] = S + (dt * a) * r[q];
+                    P.reg[q][k] = S + RKb * r[q];
+                    P.eacc[q][k] = E + RKbmbh * r[q];
+                } else {
+                    Un[q] = S + RKb * r[q];
+                    const double norm = q == 0 ? K.ero_norm : q < 4 ? K.erou_norm : K.exx_norm;
+                    const double t = fabs(E + RKbmbh * r[q]) * norm;
+                    en = (t > en) ? t : en;
+                    if (t != t) en = t;
+                }
+            }
+            if (stage == 3) eb = dbits(en);
+            for (int q = 0; q < 10; q++) P.out[src[q]][k] = Un[q];
+            const double oo = 1.0 / Un[0];  // get_velocity_from_momentum
+            P.out[4][k] = Un[1] * oo;
+            P.out[5][k] = Un[2] * oo;
+            P.out[6][k] = Un[3] * oo;
+        }
+    }
+    if (P.stage == 3) {  // block max, then one atomic
+        __shared__ unsigned long long sm[4];
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long t = __shfl_down_sync(0xffffffffu, eb, o);
+            eb = t > eb ? t : eb;
+        }
+        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = eb;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long m = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = sm[w] > m ? sm[w] : m;
+            if (m) atomicMax(&P.sc->emax_bits, m);
+        }
+    }
+}
+
+// Block sums of (rho - rho_char) vol (or of vol), in a fixed tree; folded in block order.
+__global__ void k3_mass_partials(int nl, size_t n, const double *ro, const double *vol, double rho_char, int volume_only,
+                                 double *partials) {
+    __shared__ double red[128];
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (k < n) {
+        const double vi = vol[k % nl];
+        v = volume_only ? vi : (ro[k] - rho_char) * vi;
+    }
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+__global__ void k3_fold(const double *partials, int nblk, double *out, const double *divisor, int enabled) {
+    __shared__ double red[128];
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) a = a + partials[b];
+    red[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = divisor ? (enabled ? red[0] / *divisor : 0.0) : red[0];
+}
+
+// End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
+__global__ void k3_finalize(size_t n, double *ro, const double *rou, const double *rov, const double *row, double *u,
+                            double *v, double *w, DevScalars *sc, int vpid) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        const double r = ro[k] - sc->dro;
+        ro[k] = r;
+        const double oo = 1.0 / r;
+        u[k] = rou[k] * oo;
+        v[k] = rov[k] * oo;
+        w[k] = row[k] * oo;
+    }
+    if (k == 0) {
+        const double e = __longlong_as_double((long long)sc->emax_bits);
+        const double emax = (e > 1.0e-16) ? e : 1.0e-16;
+        if (!(e == e) || isinf(e)) sc->err = 1;
+        sc->emax_nm1 = sc->emax_n;
+        sc->emax_n = sc->emax_np1;
+        sc->emax_np1 = emax;
+        sc->emax_bits = 0ull;
+        sc->time = sc->time + sc->dt;
+        sc->itime = sc->itime + 1;
+        if (!vpid) sc->df = 0.0;
+    }
+}
+
+// set_tstep (step.F90:569-622) over the 3-D nodes: block minima as bit patterns
+__global__ void k3_tstep(int nl, size_t n, const double *u, const double *v, const double *w, const double *ro,
+                         const double *sp, double csq, double visc_total, DevScalars *sc) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double tc = 1.0e10, tp = 1.0e10;
+    if (k < n) {
+        const int i = (int)(k % nl);
+        const double c = sqrt(csq);
+        const double um = sqrt((u[k] * u[k] + v[k] * v[k]) + w[k] * w[k]);
+        tc = sp[i] / (um + c);
+        tp = ((sp[i] * sp[i]) * ro[k]) / visc_total;
+    }
+    unsigned long long bc = dbits(tc), bp = dbits(tp);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_down_sync(0xffffffffu, bc, o), y = __shfl_down_sync(0xffffffffu, bp, o);
+        bc = x < bc ? x : bc;
+        bp = y < bp ? y : bp;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&sc->cfl_bits, bc);
+        atomicMin(&sc->par_bits, bp);
+    }
+}
+// fold the minima into dt_cfl, dt_parabolic; with pid, set_tstep_PID (step.F90:624-682)
+__global__ void k3_tstep_fold(DevScalars *sc, double L, int pid) {
+    const double dcfl = __longlong_as_double((long long)sc->cfl_bits);
+    const double dvisc = __longlong_as_double((long long)sc->par_bits);
+    sc->dt_cfl = (1.0 * dcfl) * L;
+    sc->dt_par = (((2.0 / 3.0) * dvisc) * L) * L;
+    sc->cfl_bits = 0x7ff0000000000000ull;
+    sc->par_bits = 0x7ff0000000000000ull;
+    if (!pid) return;
+    const double facA = (0.49 / 2.0) * log(1.0e-5 / sc->emax_np1);
+    const double facB = (0.34 / 2.0) * log(sc->emax_n / 1.0e-5);
+    const double facC = (0.1 / 2.0) * log(1.0e-5 / sc->emax_nm1);
+    double f = 0.9 * exp((facA + facB) + facC);
+    f = (0.5 > f) ? 0.5 : f;
+    f = (1.02 < f) ? 1.02 : f;
+    double dt = sc->dt * f;
+    const double dmax = (sc->dt_cfl < sc->dt_par) ? sc->dt_cfl : sc->dt_par;
+    if (dt > dmax) dt = dmax;
+    sc->dt = dt;
+}
+
+// reference layer-major arrays <-> internal layer-major arrays
+__global__ void k3_gather(const double *in, const int *perm, int nl, size_t n, double *out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t iz = k / nl;
+    out[k] = in[iz * nl + perm[k - iz * nl]];
+}
+__global__ void k3_scatter(const double *in, const int *perm, int nl, size_t n, double *out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t iz = k / nl;
+    out[iz * nl + perm[k - iz * nl]] = in[k];
+}
+__global__ void k3_fill(size_t n, double v, double *out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = v;
+}
+// hardcode_initial_conditions in 3-D: rho u = rho * u, rho v, rho w
+__global__ void k3_momentum(size_t n, const double *ro, const double *u, const double *v, const double *w, double *rou,
+                            double *rov, double *row) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    rou[k] = ro[k] * u[k];
+    rov[k] = ro[k] * v[k];
+    row[k] = ro[k] * w[k];
+}
+
+// calc_fd_weights, fd.F90:52-172, then the L_char scaling of :246-247
+int fd_tables(int ncfd, double dz, double L, double *g, double *g2, double *h) {
+    const double one = 1.0, two = 2.0;
+    if (ncfd == 5) {
+        const double G[5] = {(one / 12.0) / dz, -((8.0 / 12.0) / dz), 0.0, (8.0 / 12.0) / dz, -((one / 12.0) / dz)};
+        const double G2[5] = {-(((one / 12.0) / dz) / dz), ((16.0 / 12.0) / dz) / dz, -(((30.0 / 12.0) / dz) / dz),
+                              ((16.0 / 12.0) / dz) / dz, -(((one / 12.0) / dz) / dz)};
+        const double Hh[5] = {-(one / 16.0), 4.0 / 16.0, -(6.0 / 16.0), 4.0 / 16.0, -(one / 16.0)};
+        for (int k = 0; k < 5; k++) { g[k] = G[k]; g2[k] = G2[k]; h[k] = Hh[k]; }
+    } else if (ncfd == 7) {
+        const double G[7] = {-((one / 60.0) / dz), (9.0 / 60.0) / dz, -((45.0 / 60.0) / dz), 0.0,
+                             (45.0 / 60.0) / dz, -((9.0 / 60.0) / dz), (one / 60.0) / dz};
+        const double G2[7] = {((two / 180.0) / dz) / dz, -(((27.0 / 180.0) / dz) / dz), ((270.0 / 180.0) / dz) / dz,
+                              -(((490.0 / 180.0) / dz) / dz), ((270.0 / 180.0) / dz) / dz, -(((27.0 / 180.0) / dz) / dz),
+                              ((two / 180.0) / dz) / dz};
+        const double Hh[7] = {one / 64.0, -(6.0 / 64.0), 15.0 / 64.0, -(20.0 / 64.0), 15.0 / 64.0, -(6.0 / 64.0), one / 64.0};
+        for (int k = 0; k < 7; k++) { g[k] = G[k]; g2[k] = G2[k]; h[k] = Hh[k]; }
+    } else if (ncfd == 9) {
+        const double G[9] = {(3.0 / 840.0) / dz, -((32.0 / 840.0) / dz), (168.0 / 840.0) / dz, -((672.0 / 840.0) / dz), 0.0,
+                             (672.0 / 840.0) / dz, -((168.0 / 840.0) / dz), (32.0 / 840.0) / dz, -((3.0 / 840.0) / dz)};
+        const double G2[9] = {-(((9.0 / 5040.0) / dz) / dz), ((128.0 / 5040.0) / dz) / dz, -(((1008.0 / 5040.0) / dz) / dz),
+                              ((8064.0 / 5040.0) / dz) / dz, -(((14350.0 / 5040.0) / dz) / dz), ((8064.0 / 5040.0) / dz) / dz,
+                              -(((1008.0 / 5040.0) / dz) / dz), ((128.0 / 5040.0) / dz) / dz, -(((9.0 / 5040.0) / dz) / dz)};
+        const double Hh[9] = {-(one / 256.0), 8.0 / 256.0, -(28.0 / 256.0), 56.0 / 256.0, -(70.0 / 256.0),
+                              56.0 / 256.0, -(28.0 / 256.0), 8.0 / 256.0, -(one / 256.0)};
+        for (int k = 0; k < 9; k++) { g[k] = G[k]; g2[k] = G2[k]; h[k] = Hh[k]; }
+    } else if (ncfd == 11) {
+        const double G[11] = {-((one / 1260.0) / dz), (5.0 / 504.0) / dz, -((5.0 / 84.0) / dz), (5.0 / 21.0) / dz,
+                              -((5.0 / 6.0) / dz), 0.0, (5.0 / 6.0) / dz, -((5.0 / 21.0) / dz), (5.0 / 84.0) / dz,
+                              -((5.0 / 504.0) / dz), (one / 1260.0) / dz};
+        const double G2[11] = {((one / 3150.0) / dz) / dz, -(((5.0 / 1008.0) / dz) / dz), ((5.0 / 126.0) / dz) / dz,
+                               -(((5.0 / 21.0) / dz) / dz), ((5.0 / 3.0) / dz) / dz, -(((1086.0 / 371.0) / dz) / dz),
+                               ((5.0 / 3.0) / dz) / dz, -(((5.0 / 21.0) / dz) / dz), ((5.0 / 126.0) / dz) / dz,
+                               -(((5.0 / 1008.0) / dz) / dz), ((one / 3150.0) / dz) / dz};
+        const double Hh[11] = {one / 1024.0, -(10.0 / 1024.0), 45.0 / 1024.0, -(120.0 / 1024.0), 210.0 / 1024.0,
+                               -(252.0 / 1024.0), 210.0 / 1024.0, -(120.0 / 1024.0), 45.0 / 1024.0, -(10.0 / 1024.0),
+                               one / 1024.0};
+        for (int k = 0; k < 11; k++) { g[k] = G[k]; g2[k] = G2[k]; h[k] = Hh[k]; }
+    } else {
+        return -1;
+    }
+    for (int k = 0; k < ncfd; k++) {
+        g[k] = g[k] / L;
+        g2[k] = (g2[k] / L) / L;
+    }
+    return 0;
+}
+
+Layer3 layer3(const Handle *H) {
+    Layer3 L{};
+    L.nl = H->npfb;
+    L.nz = H->nz;
+    L.ncfd = H->ncfd;
+    L.slice_ptr = H->slice_ptr;
+    L.cnt = H->cnt;
+    L.cnt_small = H->cnt_small;
+    L.lidx = H->lidx;
+    L.wx = H->wx; L.wy = H->wy; L.wl = H->wl; L.wh = H->wh;
+    L.gsx = H->gsx; L.gsy = H->gsy; L.lsum = H->lsum; L.hsum = H->hsum;
+    for (int m = 0; m < kMaxFd; m++) { L.fdg[m] = H->fdg[m]; L.fdl[m] = H->fdl[m]; L.fdh[m] = H->fdh[m]; }
+    return L;
+}
+
+inline size_t n3(const Handle *H) { return (size_t)H->npfb * H->nz; }
+inline unsigned nblk(size_t n) { return (unsigned)((n + 127) / 128); }
+
+// all the derivatives the right-hand side reads, of buffer b
+int derivs3(Handle *H, int b) {
+    const Layer3 L = layer3(H);
+    const size_t n = n3(H);
+    double *const *f = H->f3[b];
+    double *G = H->g3;
+    auto A = [&](int a) { return G + (size_t)a * n; };
+    cudaStream_t st = H->stream;
+    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[0], 0, 7, A(ROX), A(ROY), A(ROZ), nullptr);
+    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[4], 1, 7, A(UX), A(UY), A(UZ), A(LU));
+    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[5], 2, 7, A(VX), A(VY), A(VZ), A(LV));
+    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[6], 0, 7, A(WX), A(WY), A(WZ), A(LW));
+    if (H->cfg.form == SUNSET_FORM_DI) {
+        // rhs_di.F90:186-194: c_xx x only, c_xy c_xz c_yz full, c_yy y only, c_zz z only; the
+        // rest with full gradients, else zero (set once at allocation)
+        static const int cls[6] = {0, 3, 0, 0, 0, 0}, mask[6] = {1, 7, 2, 7, 7, 4};
+        const bool md = H->cfg.Mdiff != 0.0;
+        for (int q = 0; q < 6; q++)
+            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], H->cfg.di_full_gradients ? 7 : mask[q],
+                                              A(CG0 + 3 * q), A(CG0 + 3 * q + 1), A(CG0 + 3 * q + 2),
+                                              md ? A(LC0 + q) : nullptr);
+    }
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+Point3 point3(Handle *H, int b, int stage) {
+    Point3 P{};
+    P.K = step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, false, H->xmax - H->xmin, H->ymax - H->ymin);
+    P.nl = H->npfb;
+    P.nz = H->nz;
+    P.di = H->cfg.form == SUNSET_FORM_DI;
+    P.full = H->cfg.di_full_gradients;
+    P.md = H->cfg.Mdiff != 0.0;
+    P.py = H->py;
+    P.G = H->g3;
+    for (int f = 0; f < 13; f++) {
+        P.in[f] = H->f3[b][f];
+        P.out[f] = H->f3[b ^ 1][f];
+    }
+    for (int q = 0; q < 10; q++) { P.reg[q] = H->reg3[q]; P.eacc[q] = H->eacc3[q]; P.rhs[q] = H->rhs3[q]; }
+    P.sc = H->dsc;
+    P.stage = stage;
+    return P;
+}
+
+int tstep3_launch(Handle *H, int b, int pid) {
+    const size_t n = n3(H);
+    const double *const *f = H->f3[b];
+    k3_tstep<<<nblk(n), 128, 0, H->stream>>>(H->npfb, n, f[4], f[5], f[6], f[0], H->sp, step_consts(H->cfg, 1, 1, false, false).csq,
+                                             step_consts(H->cfg, 1, 1, false, false).visc_total, H->dsc);
+    k3_tstep_fold<<<1, 1, 0, H->stream>>>(H->dsc, H->cfg.L_char, pid);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+int layers_set(Handle *H, double Lz) {
+    if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
+    if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
+    if (!(H->cfg.form == SUNSET_FORM_DI || H->cfg.form == SUNSET_FORM_NEWT))
+        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers the direct and Newtonian forms");
+    if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers sPTT / Oldroyd-B, not FENE-P");
+    if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
+    if (H->cfg.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero");
+    const int ncfd = H->cfg.forder + 1;
+    // build_3rd_dimension, setup_domain.F90:444-483: dz from the mean spacing (s^3 over s^2,
+    // summed in the reference's node order), then nz layers over L_domain_z
+    std::vector<double> sp(H->npfb);
+    SUNSET_CUDA(H, cudaMemcpy(sp.data(), H->sp, H->npfb * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<double> sref(H->npfb);
+    for (int i = 0; i < H->npfb; i++) sref[H->h_perm[i]] = sp[i];
+    double dzl = 0.0, sv = 0.0;
+    for (int r = 0; r < H->npfb; r++) {
+        sv = sv + sref[r] * sref[r];
+        dzl = dzl + (sref[r] * sref[r]) * sref[r];
+    }
+    double dz = dzl / sv;
+    const double L = H->cfg.L_char, Lzd = (Lz * L) / L;
+    int nz = (int)ceil((Lzd / dz) / 1.0);
+    dz = (Lzd / (double)nz) / 1.0;
+    if (nz < ncfd / 2 + 2) {
+        nz = ncfd / 2 + 2;
+        dz = Lzd / (double)(ncfd / 2 + 2);
+    }
+    if ((double)nz * H->npfb >= 2.0e9) return set_err(H, SUNSET_ERR_SCOPE, "too many 3-D nodes");
+    H->nz = nz;
+    H->dz = dz;
+    H->ncfd = ncfd;
+    for (int m = 0; m < 13; m++) H->fdg[m] = H->fdl[m] = H->fdh[m] = 0.0;
+    if (fd_tables(ncfd, dz, L, H->fdg, H->fdl, H->fdh)) return set_err(H, SUNSET_ERR_SCOPE, "no z stencil for this order");
+    return 0;
+}
+
+static int state3_alloc(Handle *H) {
+    if (H->g3) return 0;
+    const size_t n = n3(H);
+    for (int b = 0; b < 2; b++)
+        for (int f = 0; f < 13; f++)
+            if (dalloc(H, &H->f3[b][f], n)) return SUNSET_ERR_NOMEM;
+    for (int q = 0; q < 10; q++)
+        if (dalloc(H, &H->reg3[q], n) || dalloc(H, &H->eacc3[q], n) || dalloc(H, &H->rhs3[q], n)) return SUNSET_ERR_NOMEM;
+    if (dalloc(H, &H->g3, (size_t)kG3 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->g3, 0, (size_t)kG3 * n * sizeof(double), H->stream));
+    for (int b = 0; b < 2; b++)
+        for (int f = 7; f < 13; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
+    const unsigned nb = nblk(n);
+    if (!H->partials3 && dalloc(H, &H->partials3, (size_t)nb + 16)) return SUNSET_ERR_NOMEM;
+    if (!H->dsc) {
+        if (dalloc(H, &H->dsc, 1)) return SUNSET_ERR_NOMEM;
+    }
+    return 0;
+}
+
+// fields10: ro u v w cxx cxy cyy cxz cyz czz, reference layer-major, host memory (c may be null: c = I)
+int state3_set(Handle *H, const double *const *fields10) {
+    if (int rc = state3_alloc(H)) return rc;
+    const size_t n = n3(H);
+    cudaStream_t st = H->stream;
+    H->cur3 = 0;
+    double *const *f = H->f3[0];
+    static const int dst[10] = {0, 4, 5, 6, 7, 8, 9, 10, 11, 12};
+    for (int q = 0; q < 10; q++) {
+        double *d = f[dst[q]];
+        if (!fields10[q]) {  // c = I
+            k3_fill<<<nblk(n), 128, 0, st>>>(n, (q == 4 || q == 6 || q == 9) ? 1.0 : 0.0, d);
+            continue;
+        }
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->tmp3, fields10[q], n * sizeof(double), cudaMemcpyHostToDevice, st));
+        k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, n, d);
+    }
+    k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
+    SUNSET_CUDA(H, cudaGetLastError());
+    DevScalars s{};
+    s.dt = 1.0e-6;
+    s.emax_nm1 = s.emax_n = s.emax_np1 = 1.0e-5;  // pid_tol
+    s.eflow_nm1 = 1.0;
+    s.cfl_bits = 0x7ff0000000000000ull;
+    s.par_bits = 0x7ff0000000000000ull;
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, st));
+    // sum of the 3-D nodes' volumes, for the mass correction
+    k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->npfb, n, f[0], H->vol, 1.0, 1, H->partials3);
+    k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->tv, nullptr, 1);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return tstep3_launch(H, 0, 0);
+}
+
+// out13: ro rou rov row u v w cxx cxy cyy cxz cyz czz, reference layer-major, host memory
+int state3_get(Handle *H, double *out13) {
+    const size_t n = n3(H);
+    cudaStream_t st = H->stream;
+    for (int f = 0; f < 13; f++) {
+        k3_scatter<<<nblk(n), 128, 0, st>>>(H->f3[H->cur3][f], H->perm, H->npfb, n, H->tmp3);
+        SUNSET_CUDA(H, cudaMemcpyAsync(out13 + (size_t)f * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SUNSET_CUDA(H, cudaStreamSynchronize(st));
+    }
+    return 0;
+}
+
+// out10: the right-hand sides ro rou rov row xx xy yy xz yz zz, reference layer-major, host
+int rhs3_calc(Handle *H, double *out10) {
+    const size_t n = n3(H);
+    if (int rc = derivs3(H, H->cur3)) return rc;
+    Point3 P = point3(H, H->cur3, 4);
+    k3_point<<<nblk(n), 128, 0, H->stream>>>(P);
+    SUNSET_CUDA(H, cudaGetLastError());
+    for (int q = 0; q < 10; q++) {
+        k3_scatter<<<nblk(n), 128, 0, H->stream>>>(H->rhs3[q], H->perm, H->npfb, n, H->tmp3);
+        SUNSET_CUDA(H, cudaMemcpyAsync(out10 + (size_t)q * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+        SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    }
+    return 0;
+}
+
+int tstep3(Handle *H) { return tstep3_launch(H, H->cur3, 0); }
+
+// mode 0: fixed dt; 1: set_tstep + set_tstep_PID before each step (sunset.F90:82-83)
+int step3_run(Handle *H, double dt, int nsteps, int mode) {
+    const size_t n = n3(H);
+    cudaStream_t st = H->stream;
+    const Layer3 L = layer3(H);
+    const bool di = H->cfg.form == SUNSET_FORM_DI;
+    if (mode == 0) SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < nsteps; s++) {
+        if (mode == 1) {
+            if (int rc = tstep3_launch(H, H->cur3, 1)) return rc;
+        }
+        int b = H->cur3;
+        for (int stage = 0; stage < 4; stage++) {
+            if (int rc = derivs3(H, b)) return rc;
+            Point3 P = point3(H, b, stage);
+            k3_point<<<nblk(n), 128, 0, st>>>(P);
+            b ^= 1;
+        }
+        // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694); the mass correction
+        static const int cls[10] = {0, 1, 2, 0, 0, 3, 0, 0, 0, 0};
+        static const int fld[10] = {0, 1, 2, 3, 7, 8, 9, 10, 11, 12};
+        for (int q = 0; q < (di ? 10 : 4); q++) {
+            double *f = H->f3[b][fld[q]];
+            k3_filter_xy<<<nblk(n), 128, 0, st>>>(L, f, cls[q], H->tmp3);
+            k3_filter_z<<<nblk(n), 128, 0, st>>>(L, H->tmp3, f);
+        }
+        k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->npfb, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
+        k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
+        double *const *f = H->f3[b];
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], H->dsc, H->cfg.vpid);
+        SUNSET_CUDA(H, cudaGetLastError());
+        H->cur3 = b;
+    }
+    return tstep3_launch(H, H->cur3, 0);
+}
+
+}  // namespace sunset

@@ -35,6 +35,7 @@ ABI_SYMBOLS = [
     "sunset_adjoint_run", "sunset_adjoint_apply_D", "sunset_adapt_stencils", "sunset_get_lengths",
     "sunset_set_lengths", "sunset_get_dump", "sunset_write_dump", "sunset_set_restart", "sunset_checkpoint_size",
     "sunset_save_checkpoint", "sunset_load_checkpoint", "sunset_get_flow_control", "sunset_set_flow_control",
+    "sunset_set_layers", "sunset_get_layers", "sunset_set_state_3d", "sunset_get_state_3d", "sunset_calc_all_rhs_3d",
 ]
 
 
@@ -89,6 +90,11 @@ def load_library(build_if_missing: bool = True):
     L.sunset_write_dump.argtypes = [P, C.c_char_p, C.c_int, C.c_double]
     L.sunset_set_restart.argtypes = [P, dp, dp]
     L.sunset_get_flow_control.argtypes = [P, dp]
+    L.sunset_set_layers.argtypes = [P, C.c_double]
+    L.sunset_get_layers.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.sunset_set_state_3d.argtypes = [P] + [C.c_void_p] * 10
+    L.sunset_get_state_3d.argtypes = [P, dp]
+    L.sunset_calc_all_rhs_3d.argtypes = [P, dp]
     L.sunset_set_flow_control.argtypes = [P, dp]
     L.sunset_checkpoint_size.argtypes = [P, C.POINTER(C.c_size_t)]
     L.sunset_save_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
@@ -237,6 +243,42 @@ class Sunset:
             columns = np.stack([columns[k] for k in DUMP_COLUMNS])
         self._chk(self.L.sunset_set_restart(self.h, np.ascontiguousarray(columns, np.float64).ravel(),
                                             np.ascontiguousarray(header, np.float64)))
+
+    # ---- 3-D (-Ddim3) ----
+    def set_layers(self, L_domain_z):
+        """build_3rd_dimension: nz layers over L_domain_z; returns (nz, dz)."""
+        self._chk(self.L.sunset_set_layers(self.h, float(L_domain_z)))
+        return self.layers()
+
+    def layers(self):
+        nz, dz = C.c_int(), C.c_double()
+        self._chk(self.L.sunset_get_layers(self.h, C.byref(nz), C.byref(dz)))
+        return nz.value, dz.value
+
+    def set_state_3d(self, ro, u, v, w, cxx=None, cxy=None, cyy=None, cxz=None, cyz=None, czz=None):
+        arrs = [np.ascontiguousarray(a, np.float64) if a is not None else None
+                for a in (ro, u, v, w, cxx, cxy, cyy, cxz, cyz, czz)]
+        self._keep3 = arrs
+        ptrs = [a.ctypes.data if a is not None else None for a in arrs]
+        self._chk(self.L.sunset_set_state_3d(self.h, *ptrs))
+
+    def state_3d(self):
+        nz, _ = self.layers()
+        n = self.sizes()[1] * nz
+        out = np.zeros(13 * n)
+        self._chk(self.L.sunset_get_state_3d(self.h, out))
+        out = out.reshape(13, n)
+        keys = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+        return {k: out[i].copy() for i, k in enumerate(keys)}
+
+    def rhs_3d(self):
+        nz, _ = self.layers()
+        n = self.sizes()[1] * nz
+        out = np.zeros(10 * n)
+        self._chk(self.L.sunset_calc_all_rhs_3d(self.h, out))
+        out = out.reshape(10, n)
+        keys = ["ro", "rou", "rov", "row", "xx", "xy", "yy", "xz", "yz", "zz"]
+        return {k: out[i].copy() for i, k in enumerate(keys)}
 
     def flow_control(self):
         """The flow-rate controller's state: eflow_nm1, sum_eflow, driving_force(1:3)."""
