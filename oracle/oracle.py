@@ -322,21 +322,22 @@ def for_workload(wl, ns=None, **over):
     return o
 
 
-STATE3_FIELDS = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+STATE3_FIELDS = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz",
+                 "psixx", "psixy", "psiyy", "psixz", "psiyz", "psizz"]
 RHS3_FIELDS = ["ro", "rou", "rov", "row", "xx", "xy", "yy", "xz", "yz", "zz"]
 C3_FIELDS = ["cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
 
 
 class Oracle3:
-    """The 3-D (-Ddim3) run built on a set-up 2-D layer (direct and Newtonian forms, node sets
-    without boundary nodes).  Arrays are nl*nz, layer-major."""
+    """The 3-D (-Ddim3) run built on a set-up 2-D layer (direct, Cholesky (sPTT) and Newtonian
+    forms, node sets without boundary nodes).  Arrays are nl*nz, layer-major."""
 
     def __init__(self, layer: Oracle, Lz: float):
         self.layer = layer
         self.L = layer.L
         self.h = self.L.or3_create(layer.h, float(Lz))
         if not self.h:
-            raise OracleError("or3_create: needs weights, no boundary nodes, the direct or Newtonian form, no FENE-P")
+            raise OracleError("or3_create: needs weights, no boundary nodes, the direct, Cholesky or Newtonian form, no FENE-P")
         nl, nz, dz = C.c_int(), C.c_int(), C.c_double()
         self.L.or3_sizes(self.h, C.byref(nl), C.byref(nz), C.byref(dz))
         self.nl, self.nz, self.dz = nl.value, nz.value, dz.value
@@ -360,9 +361,9 @@ class Oracle3:
         self.L.or3_set_state(self.h, keep[0], keep[1], keep[2], keep[3], ptr)
 
     def state(self):
-        out = np.zeros(13 * self.n)
+        out = np.zeros(19 * self.n)
         self.L.or3_get_state(self.h, out)
-        out = out.reshape(13, self.n)
+        out = out.reshape(19, self.n)
         return {k: out[i].copy() for i, k in enumerate(STATE3_FIELDS)}
 
     def rhs(self):

@@ -120,7 +120,7 @@ double or_pow4_cr(double x);
    rounded x^4, as the device path evaluates it. */
 void or_set_pow_mode(int correctly_rounded);
 
-/* 3-D (-Ddim3), direct and Newtonian forms, node sets without boundary nodes: nz copies of
+/* 3-D (-Ddim3), direct, Cholesky (sPTT) and Newtonian forms, node sets without boundary nodes: nz copies of
    the layer in z (build_3rd_dimension, setup_domain.F90:435-547), z derivatives by the periodic
    central differences of fd.F90.  Create after or_setup_all on the layer; Lz is the control
    file's L_domain_z.  Arrays are nl*nz, layer-major (node iz*nl + i). */
@@ -130,7 +130,7 @@ void or3_destroy(Or3 *o);
 int or3_sizes(Or3 *o, int *nl, int *nz, double *dz);
 int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, const double *w,
                   const double *const *c6 /* cxx cxy cyy cxz cyz czz, or NULL: c = I */);
-int or3_get_state(Or3 *o, double *out /* 13 x n: ro rou rov row u v w cxx cxy cyy cxz cyz czz */);
+int or3_get_state(Or3 *o, double *out /* 19 x n: ro rou rov row u v w cxx cxy cyy cxz cyz czz, then psixx psixy psiyy psixz psiyz psizz */);
 int or3_rhs(Or3 *o, double *out /* 10 x n: ro rou rov row xx xy yy xz yz zz */);
 int or3_set_tstep(Or3 *o, double *dt_cfl, double *dt_parabolic);
 int or3_step(Or3 *o, double dt, int nsteps, int pid);

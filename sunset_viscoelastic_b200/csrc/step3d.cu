@@ -1,5 +1,5 @@
-// step3d.cu -- the 3-D (-Ddim3) time step of the direct and Newtonian forms on node sets
-// without boundary nodes.
+// step3d.cu -- the 3-D (-Ddim3) time step of the direct, Cholesky (sPTT) and Newtonian forms
+// on node sets without boundary nodes.
 //
 // The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
 // setup_domain.F90:435-547), layer-major: node k = iz*nl + i at z = iz*dz.  The reference builds
@@ -123,14 +123,35 @@ struct Point3 {
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
     const double *G;                      // kG3 derivative arrays
-    const double *in[13];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz
-    double *out[13];
+    int chl;
+    const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
+    double *out[19];
     double *reg[10], *eacc[10], *rhs[10];
     DevScalars *sc;
     int stage;                            // 0..3, 4 = right-hand side only
 };
 
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// cholesky_c_from_psi / cholesky_psi_from_c in 3-D, sPTT (conf_transforms.F90:60-71,108-121)
+__device__ __forceinline__ void chl3_c_from_psi(const double *p, double *c) {
+    const double e = exp(p[0]);
+    c[0] = e * e;
+    c[1] = exp(p[0]) * p[1];
+    c[2] = p[1] * p[1] + exp(2.0 * p[2]);
+    c[3] = exp(p[0]) * p[3];
+    c[4] = p[1] * p[3] + exp(p[2]) * p[4];
+    c[5] = (exp(2.0 * p[5]) + p[3] * p[3]) + p[4] * p[4];
+}
+__device__ __forceinline__ void chl3_psi_from_c(const double *c, double *p) {
+    const double xx = sqrt(c[0]);
+    const double xy = c[1] / (xx);
+    const double yy = (sqrt(c[2] - xy * xy));
+    const double xz = c[3] / xx;
+    const double yz = (c[4] - xy * xz) / yy;
+    const double zz = sqrt((c[5] - xz * xz) - yz * yz);
+    p[0] = log(xx); p[1] = xy; p[2] = log(yy); p[3] = xz; p[4] = yz; p[5] = log(zz);
+}
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
 // 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).
@@ -152,6 +173,23 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         const double tsv = ro * ((u * g(VX) + v * g(VY)) + w * g(VZ)) - v * rr;
         const double tsw = ro * ((u * g(WX) + v * g(WY)) + w * g(WZ)) - w * rr;
         double fvu = K.coef_solvent * g(LU), fvv = K.coef_solvent * g(LV), fvw = K.coef_solvent * g(LW);
+        auto gp = [&](int q, int d) { return g(CG0 + 3 * q + d); };  // Cholesky: psi gradients
+        if (P.chl) {  // grad c from grad psi, rhs.F90:245-262
+            const double pxx = P.in[13][k], pxy = P.in[14][k], pyy = P.in[15][k], pxz = P.in[16][k], pyz = P.in[17][k],
+                         pzz = P.in[18][k];
+            const double gcxx1 = (2.0 * exp(2.0 * pxx)) * gp(0, 0);
+            const double gcxy1 = exp(pxx) * gp(1, 0) + (pxy * exp(pxx)) * gp(0, 0);
+            const double gcxy2 = exp(pxx) * gp(1, 1) + (pxy * exp(pxx)) * gp(0, 1);
+            const double gcyy2 = (2.0 * pxy) * gp(1, 1) + (2.0 * exp(2.0 * pyy)) * gp(2, 1);
+            const double gcxz1 = exp(pxx) * gp(3, 0) + (pxz * exp(pxx)) * gp(0, 0);
+            const double gcxz3 = exp(pxx) * gp(3, 2) + (pxz * exp(pxx)) * gp(0, 2);
+            const double gcyz2 = (pxy * gp(3, 1) + pxz * gp(1, 1)) + exp(pyy) * (gp(4, 1) + pyz * gp(2, 1));
+            const double gcyz3 = (pxy * gp(3, 2) + pxz * gp(1, 2)) + exp(pyy) * (gp(4, 2) + pyz * gp(2, 2));
+            const double gczz3 = ((2.0 * exp(2.0 * pzz)) * gp(5, 2) + (2.0 * pxz) * gp(3, 2)) + (2.0 * pyz) * gp(4, 2);
+            fvu = fvu + K.coef_polymeric * ((gcxx1 + gcxy2) + gcxz3);
+            fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + gcyz3);
+            fvw = fvw + K.coef_polymeric * ((gcxz1 + gcyz2) + gczz3);
+        }
         if (P.di) {
             fvu = fvu + K.coef_polymeric * ((g(CG0 + 0) + g(CG0 + 3 + 1)) + g(CG0 + 9 + 2));
             fvv = fvv + K.coef_polymeric * ((g(CG0 + 3 + 0) + g(CG0 + 6 + 1)) + g(CG0 + 12 + 2));
@@ -166,6 +204,50 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         r[2] = ((-tsv - gpy) + bfv) + fvv;
         r[3] = ((-tsw - gpz) + bfw) + fvw;
         for (int q = 4; q < 10; q++) r[q] = 0.0;
+        if (P.chl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D)
+            const double ux = g(UX), uy = g(UY), uz = g(UZ), vx = g(VX), vy = g(VY), vz = g(VZ);
+            const double wx = g(WX), wy = g(WY), wz = g(WZ);
+            double ad[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) ad[q] = (u * gp(q, 0) + v * gp(q, 1)) + w * gp(q, 2);
+            const double lxx = exp(P.in[13][k]), lxy = P.in[14][k], lyy = exp(P.in[15][k]), lzz = exp(P.in[18][k]);
+            const double lxz = P.in[16][k], lyz = P.in[17][k];
+            double ucxx = (ux + (uy * lxy) / lxx);
+            double ucxy = ((vy * lxy + ((uy * lyy) * lyy) / lxx) + vx * lxx);
+            double ucyy = (vy - (uy * lxy) / lxx);
+            ucxx = ucxx + (uz * lxz) / lxx;
+            ucxy = (ucxy + vz * lxz) + ((uz * lyy) * lyz) / lxx;
+            ucyy = (ucyy + vz * lyz) - ((uz * lxy) * lyz) / lxx;
+            const double ucxz = (((wx * lxx + wy * lxy) + wz * lxz) + ((uy * lyy) * lyz) / lxx) + (uz * ((lyz * lyz) + (lzz * lzz))) / lxx;
+            const double ucyz = (((((wy * lyy + wz * lyz) - ((uy * lxz) * lyy) / lxx) + ((uz * lxz) * lyz) / lxx) +
+                                  ((vz * lzz) * lzz) / lyy) - (((uz * lxy) * lzz) * lzz) / (lxx * lyy));
+            const double uczz = ((wz - (uz * lxz) / lxx) - (vz * lyz) / lyy) + ((uz * lxy) * lyz) / (lxx * lyy);
+            const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
+                         czz = P.in[12][k];
+            const double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+            const double Md = K.Mdiff;
+            auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
+            const double sxx = fr * (cxx - 1.0) + Md * lc(0), sxy = fr * cxy + Md * lc(1);
+            const double syy = fr * (cyy - 1.0) + Md * lc(2), sxz = fr * cxz + Md * lc(3);
+            const double syz = fr * cyz + Md * lc(4), szz = fr * (czz - 1.0) + Md * lc(5);
+            const double csxx = ((0.5 * sxx) / lxx) / lxx;
+            const double csxy = sxy / lxx - ((0.5 * sxx) * lxy) / (lxx * lxx);
+            const double csyy = (((0.5 * syy) / lyy) / lyy - (sxy * lxy) / ((lxx * lyy) * lyy)) +
+                                (((0.5 * sxx) * lxy) * lxy) / ((lyy * lyy) * (lxx * lxx));
+            double cszz = ((0.5 * szz) / lzz) / lzz;
+            const double csxz = sxz / lxx - ((0.5 * sxx) * lxz) / (lxx * lxx);
+            const double csyz = ((((syz / lyy - (sxz * lxy) / (lxx * lyy)) +
+                                   (((0.5 * sxx) * lxy) * (((2.0 * lxz) * lyy) - lxy * lyz)) / (((lxx * lxx) * lyy) * lyy)) -
+                                  ((0.5 * syy) * lyz) / (lyy * lyy)) +
+                                 (sxy * ((lxy * lyz) - (lxz * lyy))) / ((lxx * lyy) * lyy));
+            cszz = (cszz - ((csxz * lxz) / lzz) / lzz) - ((csyz * lyz) / lzz) / lzz;
+            r[4] = (-ad[0] + ucxx) + csxx;
+            r[5] = (-ad[1] + ucxy) + csxy;
+            r[6] = (-ad[2] + ucyy) + csyy;
+            r[7] = (-ad[3] + ucxz) + csxz;
+            r[8] = (-ad[4] + ucyz) + csyz;
+            r[9] = (-ad[5] + uczz) + cszz;
+        }
         if (P.di) {
             const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
                          czz = P.in[12][k];
@@ -192,11 +274,13 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
             r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
         }
-        const int nf = P.di ? 10 : 4;
+        const int nf = (P.di || P.chl) ? 10 : 4;
         if (P.stage == 4) {
             for (int q = 0; q < 10; q++) P.rhs[q][k] = r[q];
         } else {
-            static constexpr int src[10] = {0, 1, 2, 3, 7, 8, 9, 10, 11, 12};
+            // evolved fields: rho, rho u, rho v, rho w, then c (direct) or psi (Cholesky)
+            const int c0 = P.chl ? 13 : 7;
+            const int src[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
             const int stage = P.stage;
             const double dt = P.sc->dt;
             const double a = stage == 0 ? SUNSET_RK_A21 : stage == 1 ? SUNSET_RK_A32 : SUNSET_RK_A43;
@@ -227,6 +311,11 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             P.out[4][k] = Un[1] * oo;
             P.out[5][k] = Un[2] * oo;
             P.out[6][k] = Un[3] * oo;
+            if (P.chl) {  // get_c_from_psi
+                double c[6];
+                chl3_c_from_psi(Un + 4, c);
+                for (int q = 0; q < 6; q++) P.out[7 + q][k] = c[q];
+            }
         }
     }
     if (P.stage == 3) {  // block max, then one atomic
@@ -277,16 +366,24 @@ __global__ void k3_fold(const double *partials, int nblk, double *out, const dou
 }
 
 // End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
-__global__ void k3_finalize(size_t n, double *ro, const double *rou, const double *rov, const double *row, double *u,
-                            double *v, double *w, DevScalars *sc, int vpid) {
+struct Fields19 {
+    double *p[19];
+};
+__global__ void k3_finalize(size_t n, Fields19 F, int chl, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
-        const double r = ro[k] - sc->dro;
-        ro[k] = r;
+        const double r = F.p[0][k] - sc->dro;
+        F.p[0][k] = r;
         const double oo = 1.0 / r;
-        u[k] = rou[k] * oo;
-        v[k] = rov[k] * oo;
-        w[k] = row[k] * oo;
+        F.p[4][k] = F.p[1][k] * oo;
+        F.p[5][k] = F.p[2][k] * oo;
+        F.p[6][k] = F.p[3][k] * oo;
+        if (chl) {
+            double p[6], c[6];
+            for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
+            chl3_c_from_psi(p, c);
+            for (int q = 0; q < 6; q++) F.p[7 + q][k] = c[q];
+        }
     }
     if (k == 0) {
         const double e = __longlong_as_double((long long)sc->emax_bits);
@@ -362,6 +459,19 @@ __global__ void k3_scatter(const double *in, const int *perm, int nl, size_t n, 
 __global__ void k3_fill(size_t n, double v, double *out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) out[k] = v;
+}
+// the Cholesky state from the given c: psi from c, then c from psi (setup_flow.F90:86-117)
+__global__ void k3_chl_from_c(size_t n, Fields19 F) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double c[6], p[6];
+    for (int q = 0; q < 6; q++) c[q] = F.p[7 + q][k];
+    chl3_psi_from_c(c, p);
+    chl3_c_from_psi(p, c);
+    for (int q = 0; q < 6; q++) {
+        F.p[13 + q][k] = p[q];
+        F.p[7 + q][k] = c[q];
+    }
 }
 // hardcode_initial_conditions in 3-D: rho u = rho * u, rho v, rho w
 __global__ void k3_momentum(size_t n, const double *ro, const double *u, const double *v, const double *w, double *rou,
@@ -451,6 +561,18 @@ int derivs3(Handle *H, int b) {
     k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[4], 1, 7, A(UX), A(UY), A(UZ), A(LU));
     k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[5], 2, 7, A(VX), A(VY), A(VZ), A(LV));
     k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[6], 0, 7, A(WX), A(WY), A(WZ), A(LW));
+    if (H->cfg.form == SUNSET_FORM_CHL) {
+        // rhs.F90:186-201: full gradients of every psi component; with polymer diffusion the
+        // Laplacians of c
+        static const int cls[6] = {0, 3, 0, 0, 0, 0};
+        const bool md = H->cfg.Mdiff != 0.0;
+        for (int q = 0; q < 6; q++)
+            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[13 + q], cls[q], 7, A(CG0 + 3 * q), A(CG0 + 3 * q + 1),
+                                              A(CG0 + 3 * q + 2), nullptr);
+        if (md)
+            for (int q = 0; q < 6; q++)
+                k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], 0, nullptr, nullptr, nullptr, A(LC0 + q));
+    }
     if (H->cfg.form == SUNSET_FORM_DI) {
         // rhs_di.F90:186-194: c_xx x only, c_xy c_xz c_yz full, c_yy y only, c_zz z only; the
         // rest with full gradients, else zero (set once at allocation)
@@ -471,11 +593,12 @@ Point3 point3(Handle *H, int b, int stage) {
     P.nl = H->npfb;
     P.nz = H->nz;
     P.di = H->cfg.form == SUNSET_FORM_DI;
+    P.chl = H->cfg.form == SUNSET_FORM_CHL;
     P.full = H->cfg.di_full_gradients;
     P.md = H->cfg.Mdiff != 0.0;
     P.py = H->py;
     P.G = H->g3;
-    for (int f = 0; f < 13; f++) {
+    for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
         P.out[f] = H->f3[b ^ 1][f];
     }
@@ -501,8 +624,8 @@ int tstep3_launch(Handle *H, int b, int pid) {
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
     if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
-    if (!(H->cfg.form == SUNSET_FORM_DI || H->cfg.form == SUNSET_FORM_NEWT))
-        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers the direct and Newtonian forms");
+    if (H->cfg.form == SUNSET_FORM_LC)
+        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers the direct, Cholesky and Newtonian forms");
     if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers sPTT / Oldroyd-B, not FENE-P");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
     if (H->cfg.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero");
@@ -539,14 +662,14 @@ static int state3_alloc(Handle *H) {
     if (H->g3) return 0;
     const size_t n = n3(H);
     for (int b = 0; b < 2; b++)
-        for (int f = 0; f < 13; f++)
+        for (int f = 0; f < 19; f++)
             if (dalloc(H, &H->f3[b][f], n)) return SUNSET_ERR_NOMEM;
     for (int q = 0; q < 10; q++)
         if (dalloc(H, &H->reg3[q], n) || dalloc(H, &H->eacc3[q], n) || dalloc(H, &H->rhs3[q], n)) return SUNSET_ERR_NOMEM;
     if (dalloc(H, &H->g3, (size_t)kG3 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
     SUNSET_CUDA(H, cudaMemsetAsync(H->g3, 0, (size_t)kG3 * n * sizeof(double), H->stream));
     for (int b = 0; b < 2; b++)
-        for (int f = 7; f < 13; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
+        for (int f = 7; f < 19; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
     const unsigned nb = nblk(n);
     if (!H->partials3 && dalloc(H, &H->partials3, (size_t)nb + 16)) return SUNSET_ERR_NOMEM;
     if (!H->dsc) {
@@ -573,6 +696,11 @@ int state3_set(Handle *H, const double *const *fields10) {
         k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, n, d);
     }
     k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
+    if (H->cfg.form == SUNSET_FORM_CHL) {
+        Fields19 F19;
+        for (int q = 0; q < 19; q++) F19.p[q] = f[q];
+        k3_chl_from_c<<<nblk(n), 128, 0, st>>>(n, F19);
+    }
     SUNSET_CUDA(H, cudaGetLastError());
     DevScalars s{};
     s.dt = 1.0e-6;
@@ -588,13 +716,14 @@ int state3_set(Handle *H, const double *const *fields10) {
     return tstep3_launch(H, 0, 0);
 }
 
-// out13: ro rou rov row u v w cxx cxy cyy cxz cyz czz, reference layer-major, host memory
-int state3_get(Handle *H, double *out13) {
+// out19: ro rou rov row u v w cxx cxy cyy cxz cyz czz psixx psixy psiyy psixz psiyz psizz,
+// reference layer-major, host memory
+int state3_get(Handle *H, double *out19) {
     const size_t n = n3(H);
     cudaStream_t st = H->stream;
-    for (int f = 0; f < 13; f++) {
+    for (int f = 0; f < 19; f++) {
         k3_scatter<<<nblk(n), 128, 0, st>>>(H->f3[H->cur3][f], H->perm, H->npfb, n, H->tmp3);
-        SUNSET_CUDA(H, cudaMemcpyAsync(out13 + (size_t)f * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SUNSET_CUDA(H, cudaMemcpyAsync(out19 + (size_t)f * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, st));
         SUNSET_CUDA(H, cudaStreamSynchronize(st));
     }
     return 0;
@@ -622,7 +751,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
     const size_t n = n3(H);
     cudaStream_t st = H->stream;
     const Layer3 L = layer3(H);
-    const bool di = H->cfg.form == SUNSET_FORM_DI;
+    const bool chl = H->cfg.form == SUNSET_FORM_CHL, evolves_c = H->cfg.form != SUNSET_FORM_NEWT;
     if (mode == 0) SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
     for (int s = 0; s < nsteps; s++) {
         if (mode == 1) {
@@ -635,18 +764,21 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
             k3_point<<<nblk(n), 128, 0, st>>>(P);
             b ^= 1;
         }
-        // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694); the mass correction
+        // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694) or psi (rhs.F90:792-840);
+        // the mass correction
         static const int cls[10] = {0, 1, 2, 0, 0, 3, 0, 0, 0, 0};
-        static const int fld[10] = {0, 1, 2, 3, 7, 8, 9, 10, 11, 12};
-        for (int q = 0; q < (di ? 10 : 4); q++) {
+        const int c0 = chl ? 13 : 7;
+        const int fld[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
+        for (int q = 0; q < (evolves_c ? 10 : 4); q++) {
             double *f = H->f3[b][fld[q]];
             k3_filter_xy<<<nblk(n), 128, 0, st>>>(L, f, cls[q], H->tmp3);
             k3_filter_z<<<nblk(n), 128, 0, st>>>(L, H->tmp3, f);
         }
         k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->npfb, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
         k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
-        double *const *f = H->f3[b];
-        k3_finalize<<<nblk(n), 128, 0, st>>>(n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], H->dsc, H->cfg.vpid);
+        Fields19 F19;
+        for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, H->dsc, H->cfg.vpid);
         SUNSET_CUDA(H, cudaGetLastError());
         H->cur3 = b;
     }

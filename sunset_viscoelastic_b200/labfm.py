@@ -265,10 +265,11 @@ class Sunset:
     def state_3d(self):
         nz, _ = self.layers()
         n = self.sizes()[1] * nz
-        out = np.zeros(13 * n)
+        out = np.zeros(19 * n)
         self._chk(self.L.sunset_get_state_3d(self.h, out))
-        out = out.reshape(13, n)
-        keys = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+        out = out.reshape(19, n)
+        keys = ["ro", "rou", "rov", "row", "u", "v", "w", "cxx", "cxy", "cyy", "cxz", "cyz", "czz",
+                "psixx", "psixy", "psiyy", "psixz", "psiyz", "psizz"]
         return {k: out[i].copy() for i, k in enumerate(keys)}
 
     def rhs_3d(self):
