@@ -159,8 +159,8 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
    device time of the nsteps steps. */
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
-/* ---- 3-D (-Ddim3): direct, Cholesky (sPTT) and Newtonian forms, FP64, node sets without
-   boundary nodes ---- */
+/* ---- 3-D (-Ddim3): direct, Cholesky, log-conformation (sPTT) and Newtonian forms, FP64, node
+   sets without boundary nodes ---- */
 /* build_3rd_dimension (setup_domain.F90:435-547) and calc_fd_weights (fd.F90:27-256): after
    sunset_build_domain, the node set becomes nz layers in z over L_domain_z (the control file's
    value): dz from the mean spacing, nz = ceiling(L_domain_z/dz), at least ij_count_fd/2 + 2,
@@ -175,10 +175,11 @@ int sunset_set_state_3d(SunsetHandle *h, const double *ro, const double *u, cons
                         const double *cxx, const double *cxy, const double *cyy, const double *cxz,
                         const double *cyz, const double *czz);
 /* 19*npfb*nz: ro, rou, rov, row, u, v, w, cxx, cxy, cyy, cxz, cyz, czz, psixx, psixy, psiyy,
-   psixz, psiyz, psizz (the Cholesky factors' variables; zero in the other forms) */
+   psixz, psiyz, psizz (the Cholesky or log-conformation variables; zero otherwise) */
 int sunset_get_state_3d(SunsetHandle *h, double *out);
 /* calc_all_rhs with the dim3 terms (rhs_di.F90, rhs.F90): 10*npfb*nz: ro, rou, rov, row, xx,
-   xy, yy, xz, yz, zz (of c in the direct form, of psi in the Cholesky form) */
+   xy, yy, xz, yz, zz (of c in the direct form, of psi in the Cholesky and log-conformation
+   forms) */
 int sunset_calc_all_rhs_3d(SunsetHandle *h, double *out);
 
 /* ---- Dumps, restart, checkpoints ---- */

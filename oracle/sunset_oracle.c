@@ -2753,9 +2753,9 @@ double or_mass(OrSim *s) {
 /* =========================================================================================
  * 3-D (-Ddim3): build_3rd_dimension (setup_domain.F90:435-547), calc_fd_weights
  * (fd.F90:27-256), the z parts of derivatives.F90 (:48-63, :96-108, :145-157, :340-352,
- * :387-405, :441-453) and the dim3 branches of rhs_di.F90, rhs.F90 (Cholesky, sPTT),
- * conf_transforms.F90:27-125 and step.F90, for the direct, Cholesky and Newtonian forms on node
- * sets without boundary nodes.
+ * :387-405, :441-453) and the dim3 branches of rhs_di.F90, rhs.F90 (Cholesky) and rhs_lc.F90
+ * (log-conformation), conf_transforms.F90:27-397 and step.F90, for the direct, Cholesky,
+ * log-conformation (sPTT) and Newtonian forms on node sets without boundary nodes.
  *
  * The 3-D node set is nz copies of the 2-D one, layer-major: node k = iz*nl + i at
  * z = iz*dz.  The reference searches neighbours per layer (neighbours.F90:180-183,223-233,
@@ -2771,7 +2771,7 @@ struct Or3 {
     size_t n3;
     double dz, fdg[13], fdl[13], fdh[13];
     double *ro, *rou, *rov, *row, *u, *v, *w, *c[6]; /* n3 each; c: xx xy yy xz yz zz */
-    double *psi[6];                                  /* Cholesky: xx xy yy xz yz zz */
+    double *psi[6];                                  /* Cholesky, log-conf: xx xy yy xz yz zz */
     double time, dt, dt_cfl, dt_par;
     int itime, iRKstep;
     double emax_nm1, emax_n, emax_np1;
@@ -2823,7 +2823,7 @@ static int fd_tables(int ncfd, double dz, double L, double *g, double *g2, doubl
 }
 
 Or3 *or3_create(OrSim *s, double Lz) {
-    if (!s || !s->have_weights || s->nb != 0 || s->cfg.form == OR_FORM_LC || s->cfg.fenep || !(Lz > 0.0))
+    if (!s || !s->have_weights || s->nb != 0 || s->cfg.fenep || !(Lz > 0.0))
         return NULL;
     Or3 *o = (Or3 *)xcalloc(1, sizeof(Or3));
     o->s = s;
@@ -2975,13 +2975,142 @@ static void chl3_psi_from_c(const double *c, double *p) {
     const double zz = sqrt((c[5] - xz * xz) - yz * yz);
     p[0] = log(xx); p[1] = xy; p[2] = log(yy); p[3] = xz; p[4] = yz; p[5] = log(zz);
 }
+/* eigens (3x3 symmetric), conf_transforms.F90:218-397: closed-form eigenvalues (trigonometric
+   solution of the characteristic cubic), eigenvectors by cross products and a 2x2 rotation.
+   R column-major, R[i + 3j] = R(i+1, j+1); its columns are the eigenvectors of L[0..2]. */
+static void eigens3(double axx, double axy, double ayy, double axz, double ayz, double azz, double *L, double *R) {
+    const double onethird = 1.0 / 3.0, twothirds = 2.0 / 3.0, eps = DBL_EPSILON;
+    double a[9];
+    a[0] = axx; a[3] = axy; a[6] = axz;
+    a[1] = axy; a[4] = ayy; a[7] = ayz;
+    a[2] = axz; a[5] = ayz; a[8] = azz;
+    const double p1 = (axy * axy + axz * axz) + ayz * ayz;
+    if (p1 <= doublesmall) {
+        L[0] = axx; L[1] = ayy; L[2] = azz;
+        for (int k = 0; k < 9; k++) R[k] = 0.0;
+        R[0] = 1.0; R[4] = 1.0; R[8] = 1.0;
+        return;
+    }
+    const double q = onethird * ((axx + ayy) + azz);
+    const double p2 = (((axx - q) * (axx - q) + (ayy - q) * (ayy - q)) + (azz - q) * (azz - q)) + 2.0 * p1;
+    const double p = sqrt(p2 / 6.0);
+    const double bxx = (1.0 / p) * (axx - q), bxy = (1.0 / p) * axy, byy = (1.0 / p) * (ayy - q);
+    const double bxz = (1.0 / p) * axz, byz = (1.0 / p) * ayz, bzz = (1.0 / p) * (azz - q);
+    double detbo2 = (bxx * (byy * bzz - byz * byz) - bxy * (bxy * bzz - byz * bxz)) + bxz * (bxy * byz - byy * bxz);
+    detbo2 = 0.5 * detbo2;
+    double phi;
+    if (detbo2 <= -1.0) phi = onethird * pi;
+    else if (detbo2 >= 1.0) phi = 0.0;
+    else phi = onethird * acos(detbo2);
+    L[2] = q + (2.0 * p) * cos(phi);
+    L[0] = q + (2.0 * p) * cos(phi + twothirds * pi);
+    L[1] = (3.0 * q - L[0]) - L[2];
+#define A_(i, j) a[(i - 1) + 3 * (j - 1)]
+#define R_(i, j) R[(i - 1) + 3 * (j - 1)]
+    A_(1, 1) = A_(1, 1) - L[0]; A_(2, 2) = A_(2, 2) - L[0]; A_(3, 3) = A_(3, 3) - L[0];
+    R_(1, 1) = A_(1, 2) * A_(2, 3) - A_(1, 3) * A_(2, 2);
+    R_(2, 1) = A_(1, 3) * A_(1, 2) - A_(1, 1) * A_(2, 3);
+    R_(3, 1) = A_(1, 1) * A_(2, 2) - A_(1, 2) * A_(1, 2);
+    R_(1, 2) = A_(1, 2) * A_(3, 3) - A_(1, 3) * A_(2, 3);
+    R_(2, 2) = A_(1, 3) * A_(1, 3) - A_(1, 1) * A_(3, 3);
+    R_(3, 2) = A_(1, 1) * A_(2, 3) - A_(1, 2) * A_(1, 3);
+    R_(1, 3) = A_(2, 2) * A_(3, 3) - A_(2, 3) * A_(2, 3);
+    R_(2, 3) = A_(2, 3) * A_(1, 3) - A_(1, 2) * A_(3, 3);
+    R_(3, 3) = A_(1, 2) * A_(2, 3) - A_(2, 2) * A_(1, 3);
+    double n1 = (R_(1, 1) * R_(1, 1) + R_(2, 1) * R_(2, 1)) + R_(3, 1) * R_(3, 1);
+    double n2 = (R_(1, 2) * R_(1, 2) + R_(2, 2) * R_(2, 2)) + R_(3, 2) * R_(3, 2);
+    double n3 = (R_(1, 3) * R_(1, 3) + R_(2, 3) * R_(2, 3)) + R_(3, 3) * R_(3, 3);
+    double norm = n1;
+    int ic = 1;
+    if (n2 > norm) { ic = 2; norm = n1; } /* (the reference keeps n1 here) */
+    if (n3 > norm) ic = 3;
+    if (ic == 1) {
+        norm = sqrt(1.0 / n1);
+        R_(1, 1) = R_(1, 1) * norm; R_(2, 1) = R_(2, 1) * norm; R_(3, 1) = R_(3, 1) * norm;
+    } else if (ic == 2) {
+        norm = sqrt(1.0 / n2);
+        R_(1, 1) = R_(1, 2) * norm; R_(2, 1) = R_(2, 2) * norm; R_(3, 1) = R_(3, 2) * norm;
+    } else {
+        norm = sqrt(1.0 / n3);
+        R_(1, 1) = R_(1, 3) * norm; R_(2, 1) = R_(2, 3) * norm; R_(3, 1) = R_(3, 3) * norm;
+    }
+    if (fabs(R_(1, 1)) > fabs(R_(2, 1))) {
+        norm = sqrt(1.0 / (R_(1, 1) * R_(1, 1) + R_(3, 1) * R_(3, 1)));
+        R_(1, 2) = -R_(3, 1) * norm; R_(2, 2) = 0.0; R_(3, 2) = R_(1, 1) * norm;
+    } else {
+        norm = sqrt(1.0 / (R_(2, 1) * R_(2, 1) + R_(3, 1) * R_(3, 1)));
+        R_(1, 2) = 0.0; R_(2, 2) = R_(3, 1) * norm; R_(3, 2) = -R_(2, 1) * norm;
+    }
+    R_(1, 3) = R_(2, 1) * R_(3, 2) - R_(3, 1) * R_(2, 2);
+    R_(2, 3) = R_(3, 1) * R_(1, 2) - R_(1, 1) * R_(3, 2);
+    R_(3, 3) = R_(1, 1) * R_(2, 2) - R_(2, 1) * R_(1, 2);
+    A_(1, 1) = A_(1, 1) + L[0]; A_(2, 2) = A_(2, 2) + L[0]; A_(3, 3) = A_(3, 3) + L[0];
+    n1 = (A_(1, 1) * R_(1, 2) + A_(1, 2) * R_(2, 2)) + A_(1, 3) * R_(3, 2);
+    n2 = (A_(1, 2) * R_(1, 2) + A_(2, 2) * R_(2, 2)) + A_(2, 3) * R_(3, 2);
+    n3 = (A_(1, 3) * R_(1, 2) + A_(2, 3) * R_(2, 2)) + A_(3, 3) * R_(3, 2);
+    A_(3, 3) = (A_(1, 3) * R_(1, 3) + A_(2, 3) * R_(2, 3)) + A_(3, 3) * R_(3, 3);
+    A_(1, 3) = (A_(1, 1) * R_(1, 3) + A_(1, 2) * R_(2, 3)) + A_(1, 3) * R_(3, 3);
+    A_(2, 3) = (A_(1, 2) * R_(1, 3) + A_(2, 2) * R_(2, 3)) + A_(2, 3) * R_(3, 3);
+    n1 = ((R_(1, 2) * n1 + R_(2, 2) * n2) + R_(3, 2) * n3) - L[1];
+    n2 = (R_(1, 2) * A_(1, 3) + R_(2, 2) * A_(2, 3)) + R_(3, 2) * A_(3, 3);
+    n3 = ((R_(1, 3) * A_(1, 3) + R_(2, 3) * A_(2, 3)) + R_(3, 3) * A_(3, 3)) - L[1];
+    if (fabs(n1) >= fabs(n3)) {
+        norm = fabs(n1) > fabs(n2) ? fabs(n1) : fabs(n2);
+        if (norm > eps) {
+            if (fabs(n1) >= fabs(n2)) { n2 = n2 / n1; n1 = sqrt(1.0 / (1.0 + n2 * n2)); n2 = n2 * n1; }
+            else { n1 = n1 / n2; n2 = sqrt(1.0 / (1.0 + n1 * n1)); n1 = n1 * n2; }
+            R_(1, 2) = n2 * R_(1, 2) - n1 * R_(1, 3);
+            R_(2, 2) = n2 * R_(2, 2) - n1 * R_(2, 3);
+            R_(3, 2) = n2 * R_(3, 2) - n1 * R_(3, 3);
+        }
+    } else {
+        norm = fabs(n3) > fabs(n2) ? fabs(n3) : fabs(n2);
+        if (norm > eps) {
+            if (fabs(n3) >= fabs(n2)) { n2 = n2 / n3; n3 = sqrt(1.0 / (1.0 + n2 * n2)); n2 = n2 * n3; }
+            else { n3 = n3 / n2; n2 = sqrt(1.0 / (1.0 + n3 * n3)); n3 = n3 * n2; }
+            R_(1, 2) = n3 * R_(1, 2) - n2 * R_(1, 3);
+            R_(2, 2) = n3 * R_(2, 2) - n2 * R_(2, 3);
+            R_(3, 2) = n3 * R_(3, 2) - n2 * R_(3, 3);
+        }
+    }
+    R_(1, 3) = R_(2, 1) * R_(3, 2) - R_(3, 1) * R_(2, 2);
+    R_(2, 3) = R_(3, 1) * R_(1, 2) - R_(1, 1) * R_(3, 2);
+    R_(3, 3) = R_(1, 1) * R_(2, 2) - R_(2, 1) * R_(1, 2);
+#undef A_
+#undef R_
+}
+/* C = A B, 3x3 column-major, matmul's sum in k order */
+static void mm3(const double *A, const double *B, double *C) {
+    double t[9];
+    for (int j = 0; j < 3; j++)
+        for (int i = 0; i < 3; i++) t[i + 3 * j] = (A[i] * B[3 * j] + A[i + 3] * B[1 + 3 * j]) + A[i + 6] * B[2 + 3 * j];
+    memcpy(C, t, sizeof(t));
+}
+static void tr3(const double *A, double *T) {
+    for (int j = 0; j < 3; j++)
+        for (int i = 0; i < 3; i++) T[i + 3 * j] = A[j + 3 * i];
+}
+/* log_conf_c_from_psi / log_conf_psi_from_c in 3-D (conf_transforms.F90:127-215):
+   R f(Lambda) R^T with f = exp or log; out: xx (1,1), xy (2,1), yy (2,2), xz (1,3), yz (2,3), zz */
+static void lc3_transform(const double *in, double *out, int to_c) {
+    double L[3], R[9], RT[9], Lm[9] = {0}, M[9];
+    eigens3(in[0], in[1], in[2], in[3], in[4], in[5], L, R);
+    tr3(R, RT);
+    for (int k = 0; k < 3; k++) Lm[4 * k] = to_c ? exp(L[k]) : log(L[k]);
+    mm3(Lm, RT, M);
+    mm3(R, M, M);
+    out[0] = M[0]; out[1] = M[1]; out[2] = M[4]; out[3] = M[6]; out[4] = M[7]; out[5] = M[8];
+}
+
 static void or3_c_from_psi(Or3 *o) {
-    if (o->s->cfg.form != OR_FORM_CHL) return;
+    const int form = o->s->cfg.form;
+    if (form != OR_FORM_CHL && form != OR_FORM_LC) return;
 #pragma omp parallel for schedule(static)
     for (size_t k = 0; k < o->n3; k++) {
         double p[6], c[6];
         for (int q = 0; q < 6; q++) p[q] = o->psi[q][k];
-        chl3_c_from_psi(p, c);
+        if (form == OR_FORM_CHL) chl3_c_from_psi(p, c);
+        else lc3_transform(p, c, 1);
         for (int q = 0; q < 6; q++) o->c[q][k] = c[q];
     }
 }
@@ -2993,10 +3122,11 @@ int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, co
         o->ro[k] = ro[k]; o->u[k] = u[k]; o->v[k] = v[k]; o->w[k] = w[k];
         o->rou[k] = o->ro[k] * o->u[k]; o->rov[k] = o->ro[k] * o->v[k]; o->row[k] = o->ro[k] * o->w[k];
         for (int q = 0; q < 6; q++) o->c[q][k] = c6 ? c6[q][k] : ((q == 0 || q == 2 || q == 5) ? 1.0 : 0.0);
-        if (o->s->cfg.form == OR_FORM_CHL) {
+        if (o->s->cfg.form == OR_FORM_CHL || o->s->cfg.form == OR_FORM_LC) {
             double c[6], p[6];
             for (int q = 0; q < 6; q++) c[q] = o->c[q][k];
-            chl3_psi_from_c(c, p);
+            if (o->s->cfg.form == OR_FORM_CHL) chl3_psi_from_c(c, p);
+            else lc3_transform(c, p, 0);
             for (int q = 0; q < 6; q++) o->psi[q][k] = p[q];
         }
     }
@@ -3017,7 +3147,8 @@ int or3_get_state(Or3 *o, double *out /* 19 x n3: ro rou rov row u v w cxx cxy c
 static void rhs3(Or3 *o, double *const *r) {
     const OrSim *s = o->s;
     const size_t n = o->n3;
-    const int di = s->cfg.form == OR_FORM_DI, chl = s->cfg.form == OR_FORM_CHL, full = s->cfg.di_full_gradients;
+    const int di = s->cfg.form == OR_FORM_DI, chl = s->cfg.form == OR_FORM_CHL, islc = s->cfg.form == OR_FORM_LC;
+    const int full = di && s->cfg.di_full_gradients;
     enum { ROX, ROY, ROZ, UX, UY, UZ, VX, VY, VZ, WX, WY, WZ, LU, LV, LW, NG0 };
     double *G[NG0];
     for (int q = 0; q < NG0; q++) G[q] = zarr((int)n);
@@ -3030,12 +3161,18 @@ static void rhs3(Or3 *o, double *const *r) {
     lap3(o, o->w, 0, G[LW]);
     /* conformation gradients: c_xx x only, c_xy, c_xz, c_yz full, c_yy y only, c_zz z only
        (rhs_di.F90:186-194), the others computed only with full gradients (else zero) */
-    double *gc[6][3], *lc[6];
+    double *gc[6][3], *lc[6], *gp[6][3];
     static const int ccls[6] = {0, 3, 0, 0, 0, 0};
     static const int cmask[6] = {1, 7, 2, 7, 7, 4};
     for (int q = 0; q < 6; q++) {
-        for (int d = 0; d < 3; d++) gc[q][d] = zarr((int)n);
+        for (int d = 0; d < 3; d++) { gc[q][d] = zarr((int)n); gp[q][d] = NULL; }
         lc[q] = zarr((int)n);
+        if (islc) { /* rhs_lc.F90:184-193 (c, momentum) and :397-409 (psi, advection) */
+            for (int d = 0; d < 3; d++) gp[q][d] = zarr((int)n);
+            grad3(o, o->c[q], ccls[q], cmask[q], gc[q][0], gc[q][1], gc[q][2]);
+            grad3(o, o->psi[q], ccls[q], 7, gp[q][0], gp[q][1], gp[q][2]);
+            continue;
+        }
         if (!di && !chl) continue;
         /* Cholesky: full gradients of every psi component (rhs.F90:186-201) */
         if (chl) grad3(o, o->psi[q], ccls[q], 7, gc[q][0], gc[q][1], gc[q][2]);
@@ -3076,7 +3213,7 @@ static void rhs3(Or3 *o, double *const *r) {
             fvv = fvv + cp * ((gcxy1 + gcyy2) + gcyz3);
             fvw = fvw + cp * ((gcxz1 + gcyz2) + gczz3);
         }
-        if (di) {
+        if (di || islc) {
             fvu = fvu + cp * ((gc[0][0][k] + gc[1][1][k]) + gc[3][2][k]);
             fvv = fvv + cp * ((gc[1][0][k] + gc[2][1][k]) + gc[4][2][k]);
             fvw = fvw + cp * ((gc[3][0][k] + gc[4][1][k]) + gc[5][2][k]);
@@ -3129,6 +3266,58 @@ static void rhs3(Or3 *o, double *const *r) {
             r[9][k] = (-ad[5] + uczz) + cszz;
             continue;
         }
+        if (islc) { /* calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D) */
+            const int first = (o->itime == 1 && o->iRKstep == 1);
+            double ad[6];
+            for (int q = 0; q < 6; q++) ad[q] = -((u * gp[q][0][k] + v * gp[q][1][k]) + w * gp[q][2][k]);
+            double Lv[3], R[9], RT[9], Gm[9], T[9], M[9], B[9], Om[9], P[9], OP[9], PO[9], UC[9], Ci[9] = {0}, Rx[9];
+            eigens3(o->c[0][k], o->c[1][k], o->c[2][k], o->c[3][k], o->c[4][k], o->c[5][k], Lv, R);
+            tr3(R, RT);
+            const double tr_c = (Lv[0] + Lv[1]) + Lv[2];
+            Gm[0] = G[UX][k]; Gm[3] = G[UY][k]; Gm[6] = G[UZ][k];
+            Gm[1] = G[VX][k]; Gm[4] = G[VY][k]; Gm[7] = G[VZ][k];
+            Gm[2] = G[WX][k]; Gm[5] = G[WY][k]; Gm[8] = G[WZ][k];
+            mm3(Gm, R, T);
+            mm3(RT, T, M);
+            double oxy = (Lv[1] * M[3] + Lv[0] * M[1]);
+            if (fabs(Lv[1] - Lv[0]) <= verysmall) oxy = 0.0;
+            else oxy = oxy / (Lv[1] - Lv[0]);
+            double oxz = (Lv[2] * M[6] + Lv[0] * M[2]);
+            if (fabs(Lv[2] - Lv[0]) <= verysmall) oxz = 0.0;
+            else oxz = oxz / (Lv[2] - Lv[0]);
+            double oyz = (Lv[2] * M[7] + Lv[1] * M[5]);
+            if (fabs(Lv[2] - Lv[1]) <= verysmall) oyz = 0.0;
+            else oyz = oyz / (Lv[2] - Lv[1]);
+            M[3] = 0.0; M[1] = 0.0; M[6] = 0.0; M[2] = 0.0; M[7] = 0.0; M[5] = 0.0;
+            mm3(M, RT, T);
+            mm3(R, T, B);
+            for (int q = 0; q < 9; q++) M[q] = 0.0;
+            M[3] = oxy; M[1] = -oxy; M[6] = oxz; M[2] = -oxz; M[7] = oyz; M[5] = -oyz;
+            mm3(M, RT, T);
+            mm3(R, T, Om);
+            if (first) {
+                double GT[9];
+                tr3(Gm, GT);
+                for (int q = 0; q < 9; q++) { Om[q] = 0.0; B[q] = 0.5 * (Gm[q] + GT[q]); }
+            }
+            P[0] = o->psi[0][k]; P[3] = o->psi[1][k]; P[1] = o->psi[1][k]; P[4] = o->psi[2][k];
+            P[6] = o->psi[3][k]; P[2] = o->psi[3][k]; P[7] = o->psi[4][k]; P[5] = o->psi[4][k]; P[8] = o->psi[5][k];
+            mm3(Om, P, OP);
+            mm3(P, Om, PO);
+            for (int q = 0; q < 9; q++) UC[q] = (OP[q] - PO[q]) + 2.0 * B[q];
+            const double fR = ((1.0 - 2.0 * eps) + eps * tr_c);
+            Ci[0] = fR / Lv[0] - fR; Ci[4] = fR / Lv[1] - fR; Ci[8] = fR / Lv[2] - fR;
+            mm3(Ci, RT, T);
+            mm3(R, T, T);
+            for (int q = 0; q < 9; q++) Rx[q] = T[q] / lambda;
+            r[4][k] = (ad[0] + UC[0]) + Rx[0];
+            r[5][k] = (ad[1] + UC[3]) + Rx[3];
+            r[6][k] = (ad[2] + UC[4]) + Rx[4];
+            r[7][k] = (ad[3] + UC[6]) + Rx[6];
+            r[8][k] = (ad[4] + UC[7]) + Rx[7];
+            r[9][k] = (ad[5] + UC[8]) + Rx[8];
+            continue;
+        }
         if (!di) continue;
         /* calc_rhs_c, :415-476 */
         const double cxx = o->c[0][k], cxy = o->c[1][k], cyy = o->c[2][k], cxz = o->c[3][k], cyz = o->c[4][k], czz = o->c[5][k];
@@ -3153,7 +3342,7 @@ static void rhs3(Or3 *o, double *const *r) {
         r[9][k] = ((ad[5] + uczz) + szz) + Md * lc[5][k];
     }
     for (int q = 0; q < NG0; q++) free(G[q]);
-    for (int q = 0; q < 6; q++) { for (int d = 0; d < 3; d++) free(gc[q][d]); free(lc[q]); }
+    for (int q = 0; q < 6; q++) { for (int d = 0; d < 3; d++) { free(gc[q][d]); free(gp[q][d]); } free(lc[q]); }
 }
 
 int or3_rhs(Or3 *o, double *out /* 10 x n3 */) {
@@ -3194,7 +3383,7 @@ static void step3(Or3 *o) {
     const double dt = o->dt;
     o->emax_nm1 = o->emax_n;
     o->emax_n = o->emax_np1;
-    double **cq = s->cfg.form == OR_FORM_CHL ? o->psi : o->c; /* evolved: c (DI) or psi (Cholesky) */
+    double **cq = s->cfg.form == OR_FORM_DI ? o->c : o->psi; /* evolved: c (direct) or psi */
     double *Q[10] = {o->ro, o->rou, o->rov, o->row, cq[0], cq[1], cq[2], cq[3], cq[4], cq[5]};
     double *reg[10], *eacc[10], *r[10];
     for (int f = 0; f < 10; f++) { reg[f] = zarr((int)n); eacc[f] = zarr((int)n); r[f] = zarr((int)n); }

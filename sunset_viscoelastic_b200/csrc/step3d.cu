@@ -1,5 +1,5 @@
-// step3d.cu -- the 3-D (-Ddim3) time step of the direct, Cholesky (sPTT) and Newtonian forms
-// on node sets without boundary nodes.
+// step3d.cu -- the 3-D (-Ddim3) time step of the direct, Cholesky, log-conformation (sPTT) and
+// Newtonian forms on node sets without boundary nodes.
 //
 // The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
 // setup_domain.F90:435-547), layer-major: node k = iz*nl + i at z = iz*dz.  The reference builds
@@ -21,7 +21,7 @@ namespace sunset {
 namespace {
 
 constexpr int kMaxFd = 13;
-constexpr int kG3 = 39;  // derivative arrays, see enum G3
+constexpr int kG3 = 57;  // derivative arrays, see enum G3
 
 struct Layer3 {
     int nl, nz, ncfd;
@@ -34,8 +34,9 @@ struct Layer3 {
 // derivative arrays (each nl*nz)
 enum G3 {
     ROX, ROY, ROZ, UX, UY, UZ, VX, VY, VZ, WX, WY, WZ, LU, LV, LW,
-    CG0 = 15,  // c grads: CG0 + 3*q + d, q = xx xy yy xz yz zz, d = x y z
-    LC0 = 33   // c Laplacians: LC0 + q
+    CG0 = 15,  // c grads (Cholesky: psi grads): CG0 + 3*q + d, q = xx xy yy xz yz zz, d = x y z
+    LC0 = 33,  // c Laplacians: LC0 + q
+    PG0 = 39   // log-conformation: psi grads, PG0 + 3*q + d
 };
 
 // sign class of a field at a mirror image: 0 none, 1 like u (x mirrors), 2 like v (y
@@ -123,7 +124,7 @@ struct Point3 {
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
     const double *G;                      // kG3 derivative arrays
-    int chl;
+    int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
     double *out[19];
     double *reg[10], *eacc[10], *rhs[10];
@@ -132,6 +133,139 @@ struct Point3 {
 };
 
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// eigens (3x3 symmetric), conf_transforms.F90:218-397: closed-form eigenvalues (trigonometric
+// solution of the characteristic cubic), eigenvectors by cross products and a 2x2 rotation.
+// R column-major, R[i + 3j] = R(i+1, j+1); its columns are the eigenvectors of L[0..2].
+__device__ void eigens3(double axx, double axy, double ayy, double axz, double ayz, double azz, double *L, double *R) {
+    const double onethird = 1.0 / 3.0, twothirds = 2.0 / 3.0, eps = 2.220446049250313e-16, pi = 3.141592653589793;
+    double a[9];
+    a[0] = axx; a[3] = axy; a[6] = axz;
+    a[1] = axy; a[4] = ayy; a[7] = ayz;
+    a[2] = axz; a[5] = ayz; a[8] = azz;
+    const double p1 = (axy * axy + axz * axz) + ayz * ayz;
+    if (p1 <= 1.0e-16) {
+        L[0] = axx; L[1] = ayy; L[2] = azz;
+        for (int k = 0; k < 9; k++) R[k] = 0.0;
+        R[0] = 1.0; R[4] = 1.0; R[8] = 1.0;
+        return;
+    }
+    const double q = onethird * ((axx + ayy) + azz);
+    const double p2 = (((axx - q) * (axx - q) + (ayy - q) * (ayy - q)) + (azz - q) * (azz - q)) + 2.0 * p1;
+    const double p = sqrt(p2 / 6.0);
+    const double bxx = (1.0 / p) * (axx - q), bxy = (1.0 / p) * axy, byy = (1.0 / p) * (ayy - q);
+    const double bxz = (1.0 / p) * axz, byz = (1.0 / p) * ayz, bzz = (1.0 / p) * (azz - q);
+    double detbo2 = (bxx * (byy * bzz - byz * byz) - bxy * (bxy * bzz - byz * bxz)) + bxz * (bxy * byz - byy * bxz);
+    detbo2 = 0.5 * detbo2;
+    double phi;
+    if (detbo2 <= -1.0) phi = onethird * pi;
+    else if (detbo2 >= 1.0) phi = 0.0;
+    else phi = onethird * acos(detbo2);
+    L[2] = q + (2.0 * p) * cos(phi);
+    L[0] = q + (2.0 * p) * cos(phi + twothirds * pi);
+    L[1] = (3.0 * q - L[0]) - L[2];
+#define A_(i, j) a[(i - 1) + 3 * (j - 1)]
+#define R_(i, j) R[(i - 1) + 3 * (j - 1)]
+    A_(1, 1) = A_(1, 1) - L[0]; A_(2, 2) = A_(2, 2) - L[0]; A_(3, 3) = A_(3, 3) - L[0];
+    R_(1, 1) = A_(1, 2) * A_(2, 3) - A_(1, 3) * A_(2, 2);
+    R_(2, 1) = A_(1, 3) * A_(1, 2) - A_(1, 1) * A_(2, 3);
+    R_(3, 1) = A_(1, 1) * A_(2, 2) - A_(1, 2) * A_(1, 2);
+    R_(1, 2) = A_(1, 2) * A_(3, 3) - A_(1, 3) * A_(2, 3);
+    R_(2, 2) = A_(1, 3) * A_(1, 3) - A_(1, 1) * A_(3, 3);
+    R_(3, 2) = A_(1, 1) * A_(2, 3) - A_(1, 2) * A_(1, 3);
+    R_(1, 3) = A_(2, 2) * A_(3, 3) - A_(2, 3) * A_(2, 3);
+    R_(2, 3) = A_(2, 3) * A_(1, 3) - A_(1, 2) * A_(3, 3);
+    R_(3, 3) = A_(1, 2) * A_(2, 3) - A_(2, 2) * A_(1, 3);
+    double n1 = (R_(1, 1) * R_(1, 1) + R_(2, 1) * R_(2, 1)) + R_(3, 1) * R_(3, 1);
+    double n2 = (R_(1, 2) * R_(1, 2) + R_(2, 2) * R_(2, 2)) + R_(3, 2) * R_(3, 2);
+    double n3 = (R_(1, 3) * R_(1, 3) + R_(2, 3) * R_(2, 3)) + R_(3, 3) * R_(3, 3);
+    double norm = n1;
+    int ic = 1;
+    if (n2 > norm) { ic = 2; norm = n1; }  // (the reference keeps n1 here)
+    if (n3 > norm) ic = 3;
+    if (ic == 1) {
+        norm = sqrt(1.0 / n1);
+        R_(1, 1) = R_(1, 1) * norm; R_(2, 1) = R_(2, 1) * norm; R_(3, 1) = R_(3, 1) * norm;
+    } else if (ic == 2) {
+        norm = sqrt(1.0 / n2);
+        R_(1, 1) = R_(1, 2) * norm; R_(2, 1) = R_(2, 2) * norm; R_(3, 1) = R_(3, 2) * norm;
+    } else {
+        norm = sqrt(1.0 / n3);
+        R_(1, 1) = R_(1, 3) * norm; R_(2, 1) = R_(2, 3) * norm; R_(3, 1) = R_(3, 3) * norm;
+    }
+    if (fabs(R_(1, 1)) > fabs(R_(2, 1))) {
+        norm = sqrt(1.0 / (R_(1, 1) * R_(1, 1) + R_(3, 1) * R_(3, 1)));
+        R_(1, 2) = -R_(3, 1) * norm; R_(2, 2) = 0.0; R_(3, 2) = R_(1, 1) * norm;
+    } else {
+        norm = sqrt(1.0 / (R_(2, 1) * R_(2, 1) + R_(3, 1) * R_(3, 1)));
+        R_(1, 2) = 0.0; R_(2, 2) = R_(3, 1) * norm; R_(3, 2) = -R_(2, 1) * norm;
+    }
+    R_(1, 3) = R_(2, 1) * R_(3, 2) - R_(3, 1) * R_(2, 2);
+    R_(2, 3) = R_(3, 1) * R_(1, 2) - R_(1, 1) * R_(3, 2);
+    R_(3, 3) = R_(1, 1) * R_(2, 2) - R_(2, 1) * R_(1, 2);
+    A_(1, 1) = A_(1, 1) + L[0]; A_(2, 2) = A_(2, 2) + L[0]; A_(3, 3) = A_(3, 3) + L[0];
+    n1 = (A_(1, 1) * R_(1, 2) + A_(1, 2) * R_(2, 2)) + A_(1, 3) * R_(3, 2);
+    n2 = (A_(1, 2) * R_(1, 2) + A_(2, 2) * R_(2, 2)) + A_(2, 3) * R_(3, 2);
+    n3 = (A_(1, 3) * R_(1, 2) + A_(2, 3) * R_(2, 2)) + A_(3, 3) * R_(3, 2);
+    A_(3, 3) = (A_(1, 3) * R_(1, 3) + A_(2, 3) * R_(2, 3)) + A_(3, 3) * R_(3, 3);
+    A_(1, 3) = (A_(1, 1) * R_(1, 3) + A_(1, 2) * R_(2, 3)) + A_(1, 3) * R_(3, 3);
+    A_(2, 3) = (A_(1, 2) * R_(1, 3) + A_(2, 2) * R_(2, 3)) + A_(2, 3) * R_(3, 3);
+    n1 = ((R_(1, 2) * n1 + R_(2, 2) * n2) + R_(3, 2) * n3) - L[1];
+    n2 = (R_(1, 2) * A_(1, 3) + R_(2, 2) * A_(2, 3)) + R_(3, 2) * A_(3, 3);
+    n3 = ((R_(1, 3) * A_(1, 3) + R_(2, 3) * A_(2, 3)) + R_(3, 3) * A_(3, 3)) - L[1];
+    if (fabs(n1) >= fabs(n3)) {
+        norm = fabs(n1) > fabs(n2) ? fabs(n1) : fabs(n2);
+        if (norm > eps) {
+            if (fabs(n1) >= fabs(n2)) { n2 = n2 / n1; n1 = sqrt(1.0 / (1.0 + n2 * n2)); n2 = n2 * n1; }
+            else { n1 = n1 / n2; n2 = sqrt(1.0 / (1.0 + n1 * n1)); n1 = n1 * n2; }
+            R_(1, 2) = n2 * R_(1, 2) - n1 * R_(1, 3);
+            R_(2, 2) = n2 * R_(2, 2) - n1 * R_(2, 3);
+            R_(3, 2) = n2 * R_(3, 2) - n1 * R_(3, 3);
+        }
+    } else {
+        norm = fabs(n3) > fabs(n2) ? fabs(n3) : fabs(n2);
+        if (norm > eps) {
+            if (fabs(n3) >= fabs(n2)) { n2 = n2 / n3; n3 = sqrt(1.0 / (1.0 + n2 * n2)); n2 = n2 * n3; }
+            else { n3 = n3 / n2; n2 = sqrt(1.0 / (1.0 + n3 * n3)); n3 = n3 * n2; }
+            R_(1, 2) = n3 * R_(1, 2) - n2 * R_(1, 3);
+            R_(2, 2) = n3 * R_(2, 2) - n2 * R_(2, 3);
+            R_(3, 2) = n3 * R_(3, 2) - n2 * R_(3, 3);
+        }
+    }
+    R_(1, 3) = R_(2, 1) * R_(3, 2) - R_(3, 1) * R_(2, 2);
+    R_(2, 3) = R_(3, 1) * R_(1, 2) - R_(1, 1) * R_(3, 2);
+    R_(3, 3) = R_(1, 1) * R_(2, 2) - R_(2, 1) * R_(1, 2);
+#undef A_
+#undef R_
+}
+// C = A B, 3x3 column-major, matmul's sum in k order
+__device__ __forceinline__ void mm3(const double *A, const double *B, double *C) {
+    double t[9];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) t[i + 3 * j] = (A[i] * B[3 * j] + A[i + 3] * B[1 + 3 * j]) + A[i + 6] * B[2 + 3 * j];
+#pragma unroll
+    for (int k = 0; k < 9; k++) C[k] = t[k];
+}
+__device__ __forceinline__ void tr3(const double *A, double *T) {
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) T[i + 3 * j] = A[j + 3 * i];
+}
+// log_conf_c_from_psi / log_conf_psi_from_c in 3-D (conf_transforms.F90:127-215): R f(Lambda) R^T
+// with f = exp or log; in/out xx xy yy xz yz zz
+__device__ void lc3_transform(const double *in, double *out, bool to_c) {
+    double L[3], R[9], RT[9], Lm[9], M[9];
+    eigens3(in[0], in[1], in[2], in[3], in[4], in[5], L, R);
+    tr3(R, RT);
+    for (int k = 0; k < 9; k++) Lm[k] = 0.0;
+    for (int k = 0; k < 3; k++) Lm[4 * k] = to_c ? exp(L[k]) : log(L[k]);
+    mm3(Lm, RT, M);
+    mm3(R, M, M);
+    out[0] = M[0]; out[1] = M[1]; out[2] = M[4]; out[3] = M[6]; out[4] = M[7]; out[5] = M[8];
+}
 
 // cholesky_c_from_psi / cholesky_psi_from_c in 3-D, sPTT (conf_transforms.F90:60-71,108-121)
 __device__ __forceinline__ void chl3_c_from_psi(const double *p, double *c) {
@@ -190,7 +324,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + gcyz3);
             fvw = fvw + K.coef_polymeric * ((gcxz1 + gcyz2) + gczz3);
         }
-        if (P.di) {
+        if (P.di || P.lc) {
             fvu = fvu + K.coef_polymeric * ((g(CG0 + 0) + g(CG0 + 3 + 1)) + g(CG0 + 9 + 2));
             fvv = fvv + K.coef_polymeric * ((g(CG0 + 3 + 0) + g(CG0 + 6 + 1)) + g(CG0 + 12 + 2));
             fvw = fvw + K.coef_polymeric * ((g(CG0 + 9 + 0) + g(CG0 + 12 + 1)) + g(CG0 + 15 + 2));
@@ -248,6 +382,58 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             r[8] = (-ad[4] + ucyz) + csyz;
             r[9] = (-ad[5] + uczz) + cszz;
         }
+        if (P.lc) {  // calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D)
+            const bool first = (P.sc->itime == 1) && (P.stage == 0);
+            double ad[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) ad[q] = -((u * g(PG0 + 3 * q) + v * g(PG0 + 3 * q + 1)) + w * g(PG0 + 3 * q + 2));
+            double Lv[3], R[9], RT[9], Gm[9], T[9], M[9], B[9], Om[9], Ps[9], OP[9], PO[9], Ci[9], Rx[9];
+            eigens3(P.in[7][k], P.in[8][k], P.in[9][k], P.in[10][k], P.in[11][k], P.in[12][k], Lv, R);
+            tr3(R, RT);
+            const double tr_c = (Lv[0] + Lv[1]) + Lv[2];
+            Gm[0] = g(UX); Gm[3] = g(UY); Gm[6] = g(UZ);
+            Gm[1] = g(VX); Gm[4] = g(VY); Gm[7] = g(VZ);
+            Gm[2] = g(WX); Gm[5] = g(WY); Gm[8] = g(WZ);
+            mm3(Gm, R, T);
+            mm3(RT, T, M);
+            double oxy = (Lv[1] * M[3] + Lv[0] * M[1]);
+            if (fabs(Lv[1] - Lv[0]) <= 1.0e-30) oxy = 0.0;
+            else oxy = oxy / (Lv[1] - Lv[0]);
+            double oxz = (Lv[2] * M[6] + Lv[0] * M[2]);
+            if (fabs(Lv[2] - Lv[0]) <= 1.0e-30) oxz = 0.0;
+            else oxz = oxz / (Lv[2] - Lv[0]);
+            double oyz = (Lv[2] * M[7] + Lv[1] * M[5]);
+            if (fabs(Lv[2] - Lv[1]) <= 1.0e-30) oyz = 0.0;
+            else oyz = oyz / (Lv[2] - Lv[1]);
+            M[3] = 0.0; M[1] = 0.0; M[6] = 0.0; M[2] = 0.0; M[7] = 0.0; M[5] = 0.0;
+            mm3(M, RT, T);
+            mm3(R, T, B);
+            for (int q = 0; q < 9; q++) M[q] = 0.0;
+            M[3] = oxy; M[1] = -oxy; M[6] = oxz; M[2] = -oxz; M[7] = oyz; M[5] = -oyz;
+            mm3(M, RT, T);
+            mm3(R, T, Om);
+            if (first) {
+                double GT[9];
+                tr3(Gm, GT);
+                for (int q = 0; q < 9; q++) { Om[q] = 0.0; B[q] = 0.5 * (Gm[q] + GT[q]); }
+            }
+            Ps[0] = P.in[13][k]; Ps[3] = P.in[14][k]; Ps[1] = P.in[14][k]; Ps[4] = P.in[15][k];
+            Ps[6] = P.in[16][k]; Ps[2] = P.in[16][k]; Ps[7] = P.in[17][k]; Ps[5] = P.in[17][k]; Ps[8] = P.in[18][k];
+            mm3(Om, Ps, OP);
+            mm3(Ps, Om, PO);
+            const double fR = ((1.0 - 2.0 * K.epsPTT) + K.epsPTT * tr_c);
+            for (int q = 0; q < 9; q++) Ci[q] = 0.0;
+            Ci[0] = fR / Lv[0] - fR; Ci[4] = fR / Lv[1] - fR; Ci[8] = fR / Lv[2] - fR;
+            mm3(Ci, RT, T);
+            mm3(R, T, T);
+            for (int q = 0; q < 9; q++) Rx[q] = T[q] / K.lambda;
+            static constexpr int idx[6] = {0, 3, 4, 6, 7, 8};  // (1,1) (1,2) (2,2) (1,3) (2,3) (3,3)
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                const int e = idx[q];
+                r[4 + q] = (ad[q] + ((OP[e] - PO[e]) + 2.0 * B[e])) + Rx[e];
+            }
+        }
         if (P.di) {
             const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
                          czz = P.in[12][k];
@@ -274,12 +460,12 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
             r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
         }
-        const int nf = (P.di || P.chl) ? 10 : 4;
+        const int nf = (P.di || P.chl || P.lc) ? 10 : 4;
         if (P.stage == 4) {
             for (int q = 0; q < 10; q++) P.rhs[q][k] = r[q];
         } else {
             // evolved fields: rho, rho u, rho v, rho w, then c (direct) or psi (Cholesky)
-            const int c0 = P.chl ? 13 : 7;
+            const int c0 = (P.chl || P.lc) ? 13 : 7;
             const int src[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
             const int stage = P.stage;
             const double dt = P.sc->dt;
@@ -311,9 +497,10 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             P.out[4][k] = Un[1] * oo;
             P.out[5][k] = Un[2] * oo;
             P.out[6][k] = Un[3] * oo;
-            if (P.chl) {  // get_c_from_psi
+            if (P.chl || P.lc) {  // get_c_from_psi
                 double c[6];
-                chl3_c_from_psi(Un + 4, c);
+                if (P.chl) chl3_c_from_psi(Un + 4, c);
+                else lc3_transform(Un + 4, c, true);
                 for (int q = 0; q < 6; q++) P.out[7 + q][k] = c[q];
             }
         }
@@ -369,7 +556,7 @@ __global__ void k3_fold(const double *partials, int nblk, double *out, const dou
 struct Fields19 {
     double *p[19];
 };
-__global__ void k3_finalize(size_t n, Fields19 F, int chl, DevScalars *sc, int vpid) {
+__global__ void k3_finalize(size_t n, Fields19 F, int chl, int lc, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         const double r = F.p[0][k] - sc->dro;
@@ -378,10 +565,11 @@ __global__ void k3_finalize(size_t n, Fields19 F, int chl, DevScalars *sc, int v
         F.p[4][k] = F.p[1][k] * oo;
         F.p[5][k] = F.p[2][k] * oo;
         F.p[6][k] = F.p[3][k] * oo;
-        if (chl) {
+        if (chl || lc) {
             double p[6], c[6];
             for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
-            chl3_c_from_psi(p, c);
+            if (chl) chl3_c_from_psi(p, c);
+            else lc3_transform(p, c, true);
             for (int q = 0; q < 6; q++) F.p[7 + q][k] = c[q];
         }
     }
@@ -460,14 +648,20 @@ __global__ void k3_fill(size_t n, double v, double *out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) out[k] = v;
 }
-// the Cholesky state from the given c: psi from c, then c from psi (setup_flow.F90:86-117)
-__global__ void k3_chl_from_c(size_t n, Fields19 F) {
+// the Cholesky or log-conformation state from the given c: psi from c, then c from psi
+// (setup_flow.F90:86-117)
+__global__ void k3_psi_from_c(size_t n, Fields19 F, int lc) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double c[6], p[6];
     for (int q = 0; q < 6; q++) c[q] = F.p[7 + q][k];
-    chl3_psi_from_c(c, p);
-    chl3_c_from_psi(p, c);
+    if (lc) {
+        lc3_transform(c, p, false);
+        lc3_transform(p, c, true);
+    } else {
+        chl3_psi_from_c(c, p);
+        chl3_c_from_psi(p, c);
+    }
     for (int q = 0; q < 6; q++) {
         F.p[13 + q][k] = p[q];
         F.p[7 + q][k] = c[q];
@@ -573,6 +767,17 @@ int derivs3(Handle *H, int b) {
             for (int q = 0; q < 6; q++)
                 k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], 0, nullptr, nullptr, nullptr, A(LC0 + q));
     }
+    if (H->cfg.form == SUNSET_FORM_LC) {
+        // rhs_lc.F90:184-193: c gradients for the momentum equation (c_xx x, c_yy y, c_zz z
+        // only); :397-409: full psi gradients for the advection
+        static const int cls[6] = {0, 3, 0, 0, 0, 0}, mask[6] = {1, 7, 2, 7, 7, 4};
+        for (int q = 0; q < 6; q++) {
+            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], mask[q], A(CG0 + 3 * q), A(CG0 + 3 * q + 1),
+                                              A(CG0 + 3 * q + 2), nullptr);
+            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[13 + q], cls[q], 7, A(PG0 + 3 * q), A(PG0 + 3 * q + 1),
+                                              A(PG0 + 3 * q + 2), nullptr);
+        }
+    }
     if (H->cfg.form == SUNSET_FORM_DI) {
         // rhs_di.F90:186-194: c_xx x only, c_xy c_xz c_yz full, c_yy y only, c_zz z only; the
         // rest with full gradients, else zero (set once at allocation)
@@ -594,6 +799,7 @@ Point3 point3(Handle *H, int b, int stage) {
     P.nz = H->nz;
     P.di = H->cfg.form == SUNSET_FORM_DI;
     P.chl = H->cfg.form == SUNSET_FORM_CHL;
+    P.lc = H->cfg.form == SUNSET_FORM_LC;
     P.full = H->cfg.di_full_gradients;
     P.md = H->cfg.Mdiff != 0.0;
     P.py = H->py;
@@ -624,8 +830,6 @@ int tstep3_launch(Handle *H, int b, int pid) {
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
     if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
-    if (H->cfg.form == SUNSET_FORM_LC)
-        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers the direct, Cholesky and Newtonian forms");
     if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers sPTT / Oldroyd-B, not FENE-P");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
     if (H->cfg.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero");
@@ -696,10 +900,10 @@ int state3_set(Handle *H, const double *const *fields10) {
         k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, n, d);
     }
     k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
-    if (H->cfg.form == SUNSET_FORM_CHL) {
+    if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
         Fields19 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = f[q];
-        k3_chl_from_c<<<nblk(n), 128, 0, st>>>(n, F19);
+        k3_psi_from_c<<<nblk(n), 128, 0, st>>>(n, F19, H->cfg.form == SUNSET_FORM_LC);
     }
     SUNSET_CUDA(H, cudaGetLastError());
     DevScalars s{};
@@ -751,7 +955,8 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
     const size_t n = n3(H);
     cudaStream_t st = H->stream;
     const Layer3 L = layer3(H);
-    const bool chl = H->cfg.form == SUNSET_FORM_CHL, evolves_c = H->cfg.form != SUNSET_FORM_NEWT;
+    const bool chl = H->cfg.form == SUNSET_FORM_CHL, lc = H->cfg.form == SUNSET_FORM_LC;
+    const bool evolves_c = H->cfg.form != SUNSET_FORM_NEWT;
     if (mode == 0) SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
     for (int s = 0; s < nsteps; s++) {
         if (mode == 1) {
@@ -767,7 +972,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694) or psi (rhs.F90:792-840);
         // the mass correction
         static const int cls[10] = {0, 1, 2, 0, 0, 3, 0, 0, 0, 0};
-        const int c0 = chl ? 13 : 7;
+        const int c0 = (chl || lc) ? 13 : 7;
         const int fld[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
         for (int q = 0; q < (evolves_c ? 10 : 4); q++) {
             double *f = H->f3[b][fld[q]];
@@ -778,7 +983,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields19 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
-        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, H->dsc, H->cfg.vpid);
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->dsc, H->cfg.vpid);
         SUNSET_CUDA(H, cudaGetLastError());
         H->cur3 = b;
     }

@@ -1,6 +1,6 @@
-"""The 3-D (-Ddim3) time step on the device against the CPU restatement: the direct and
-Cholesky forms (sPTT / Oldroyd-B, with and without polymer diffusion) and the Newtonian form, on
-jittered x-y node sets stacked in z, periodic or symmetric in y.
+"""The 3-D (-Ddim3) time step on the device against the CPU restatement: the direct, Cholesky
+and log-conformation forms (sPTT / Oldroyd-B, with and without polymer diffusion) and the
+Newtonian form, on jittered x-y node sets stacked in z, periodic or symmetric in y.
 
 Reference behaviour restated (and followed by the device):
 * build_3rd_dimension (setup_domain.F90:435-547): dz from the mean spacing, nz from
@@ -12,6 +12,9 @@ Reference behaviour restated (and followed by the device):
 * rhs_di.F90 with the dim3 terms: w, rho w, c_xz, c_yz, the z parts of every gradient,
   divergence and Laplacian, the 3-D upper-convected derivative;
 * rhs.F90 (Cholesky) with the dim3 terms and the 3-D transforms of conf_transforms.F90:27-125;
+* rhs_lc.F90 (log-conformation) with the dim3 terms: the 3x3 eigen-decomposition of c
+  (conf_transforms.F90:218-397, closed form with acos and cos, so device and CPU agree to
+  rounding rather than bit for bit), the rotation rates and the 3-D transforms;
 * step.F90 with the dim3 error norms (row, xz, yz) and set_tstep with |u| including w.
 
 Tolerances as in the 2-D parity tests: state and right-hand sides within 1e-10 of their
@@ -40,6 +43,8 @@ CASES = {
     "newt-o6": ("periodic-lc-o6-262k", 20, 0.7, (1, 1), {"form": "newt"}),
     "chl-o8": ("periodic-chl-o8-1m", 20, 0.5, (1, 1), {"epsPTT": 0.25}),
     "chl-o6-mdiff-ysym": ("periodic-lc-o6-262k", 20, 0.6, (2, 2), {"form": "chl", "Mdiff": 1e-3}),
+    "lc-o6": ("periodic-lc-o6-262k", 20, 0.5, (1, 1), {}),
+    "lc-o8-oldroyd-ysym": ("periodic-chl-o8-1m", 20, 0.5, (2, 2), {"form": "lc", "epsPTT": 0.0}),
 }
 
 
