@@ -2,7 +2,11 @@
 // Newtonian forms on node sets without boundary nodes.
 //
 // The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
-// setup_domain.F90:435-547), layer-major: node k = iz*nl + i at z = iz*dz.  The reference builds
+// setup_domain.F90:435-547), layer-major in the reference (node iz*nl + i at z = iz*dz).  On the
+// device the layers are innermost: node (i, iz) sits at i*nz + iz, so a warp covers the layers of
+// one node (or a few): the node's links and weights are the same in every lane (one broadcast
+// load a link), its neighbours' values are contiguous (coalesced), and the z stencil reads
+// adjacent entries.  The C-ABI converts to and from the reference order.  The reference builds
 // the neighbour lists per layer from identical positions (neighbours.F90:180-183,223-233), so
 // every layer uses the layer's lists and LABFM weights (built once, 2-D); only the state is
 // 3-D.  z-derivatives are the periodic central differences of fd.F90 (ij_count_fd = forder+1
@@ -10,8 +14,8 @@
 // value in the same layer, u and v with the mirror's sign, w, c_xz and c_yz unchanged
 // (mirror_boundaries.F90:302-303,324-341).
 //
-// Structure, as calc_all_rhs: one gather kernel per field and derivative set (x-y LABFM sums
-// in the reference's link order, then the z stencil), then a pointwise kernel for the
+// Structure, as calc_all_rhs: one gather kernel for every derivative of every field (x-y LABFM
+// sums in the reference's link order, then the z stencils), then a pointwise kernel for the
 // right-hand side and the RK update; the filter as the x-y filter followed by the z filter of
 // its result (derivatives.F90:387-405); the mass correction and the derived fields; all FP64.
 #include "internal.cuh"
@@ -47,47 +51,97 @@ __device__ __forceinline__ double mirror_value(double x, int cls, int code) {
     return flip ? -x : x;
 }
 
-__device__ __forceinline__ size_t zlayer(const Layer3 &L, int iz, int m) {
+// layer of the m-th point of the z stencil (fd.F90:62-66, periodic)
+__device__ __forceinline__ int zlayer(const Layer3 &L, int iz, int m) {
     int l = (iz + m - L.ncfd / 2) % L.nz;
     if (l < 0) l += L.nz;
-    return (size_t)l * L.nl;
+    return l;
 }
 
-// calc_gradient / calc_gradient_only / calc_laplacian in 3-D (derivatives.F90:26-116,416-464):
-// comp bits 1 = d/dx, 2 = d/dy, 4 = d/dz; lap: the x-y Laplacian plus the z second difference.
-__global__ void k3_deriv(Layer3 L, const double *f, int cls, int comp, double *gx, double *gy, double *gz,
-                         double *lap) {
+struct Fields19 {
+    double *p[19];
+};
+
+// What one pass over a node's links gathers: per field, the G slots of its x-y sums (and z
+// stencil) and of its Laplacian (-1: not needed).
+struct FDesc {
+    int f, cls, gx, gy, gl, gz;
+};
+template <int FORM, bool MD>
+__host__ __device__ constexpr int ndesc() {
+    return FORM == SUNSET_FORM_NEWT ? 4 : FORM == SUNSET_FORM_DI ? 10 : FORM == SUNSET_FORM_CHL ? (MD ? 16 : 10) : 16;
+}
+template <int FORM, bool MD, bool FULL>
+__host__ __device__ constexpr FDesc desc3(int d) {
+    if (d == 0) return FDesc{0, 0, ROX, ROY, -1, ROZ};
+    if (d == 1) return FDesc{4, 1, UX, UY, LU, UZ};
+    if (d == 2) return FDesc{5, 2, VX, VY, LV, VZ};
+    if (d == 3) return FDesc{6, 0, WX, WY, LW, WZ};
+    const int q = (d - 4) % 6, cls = q == 1 ? 3 : 0;
+    const bool hx = q == 0 || q == 1 || q == 3 || q == 4, hy = q == 1 || q == 2 || q == 3 || q == 4;
+    const bool hz = q == 1 || q == 3 || q == 4 || q == 5;
+    if (FORM == SUNSET_FORM_DI)  // rhs_di.F90:186-194 (c_xx x, c_yy y, c_zz z only, unless full)
+        return FDesc{7 + q, cls, (FULL || hx) ? CG0 + 3 * q : -1, (FULL || hy) ? CG0 + 3 * q + 1 : -1, MD ? LC0 + q : -1,
+                     (FULL || hz) ? CG0 + 3 * q + 2 : -1};
+    if (FORM == SUNSET_FORM_CHL) {  // rhs.F90:186-201: full psi gradients; Laplacians of c
+        if (d < 10) return FDesc{13 + q, cls, CG0 + 3 * q, CG0 + 3 * q + 1, -1, CG0 + 3 * q + 2};
+        return FDesc{7 + q, cls, -1, -1, LC0 + q, -1};
+    }
+    // log-conformation, rhs_lc.F90:184-193 (c, momentum) and :397-409 (psi, advection)
+    if (d < 10) return FDesc{7 + q, cls, hx ? CG0 + 3 * q : -1, hy ? CG0 + 3 * q + 1 : -1, -1, hz ? CG0 + 3 * q + 2 : -1};
+    return FDesc{13 + q, cls, PG0 + 3 * q, PG0 + 3 * q + 1, -1, PG0 + 3 * q + 2};
+}
+
+// Every derivative the right-hand side reads, in one pass over each node's links: the x-y
+// LABFM sums of all fields (in the reference's link order, each sum as calc_gradient /
+// calc_laplacian forms it), then the z stencils.  The layers of a node share its links, so a
+// warp's link and weight loads are one broadcast each.
+template <int FORM, bool MD, bool FULL>
+__global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G) {
+    constexpr int N = ndesc<FORM, MD>();
     const size_t n = (size_t)L.nl * L.nz;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
-    const size_t off = (size_t)iz * L.nl;
-    if ((comp & 3) || lap) {
-        const long long base = L.slice_ptr[i >> 5];
-        double sx = 0.0, sy = 0.0, sl = 0.0;
-        const int cs = L.cnt_small[i];
-        for (int q = 0; q < cs; q++) {
-            const long long o = sell_at(base, q, i & 31);
-            const int l = __ldg(L.lidx + o);
-            const double pj = mirror_value(f[off + (l & kLinkMask)], cls, (int)((unsigned)l >> 30));
-            if (comp & 1) sx = sx + pj * __ldg(L.wx + o);
-            if (comp & 2) sy = sy + pj * __ldg(L.wy + o);
-            if (lap) sl = sl + pj * __ldg(L.wl + o);
-        }
-        const double p = f[k];
-        if (comp & 1) gx[k] = sx - p * L.gsx[i];
-        if (comp & 2) gy[k] = sy - p * L.gsy[i];
-        if (lap) {
-            const double r = sl - p * L.lsum[i];
-            double t = 0.0;
-            for (int m = 0; m < L.ncfd; m++) t = t + f[zlayer(L, iz, m) + i] * L.fdl[m];
-            lap[k] = r + t;
+    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
+    const size_t row = (size_t)i * L.nz;
+    double sx[N], sy[N], sl[N];
+#pragma unroll
+    for (int d = 0; d < N; d++) { sx[d] = 0.0; sy[d] = 0.0; sl[d] = 0.0; }
+    const long long base = L.slice_ptr[i >> 5];
+    const int cs = L.cnt_small[i];
+    for (int q = 0; q < cs; q++) {
+        const long long o = sell_at(base, q, i & 31);
+        const int l = __ldg(L.lidx + o);
+        const size_t pj = (size_t)(l & kLinkMask) * L.nz + iz;
+        const int code = (int)((unsigned)l >> 30);
+        const double wx = __ldg(L.wx + o), wy = __ldg(L.wy + o), wl = __ldg(L.wl + o);
+#pragma unroll
+        for (int d = 0; d < N; d++) {
+            const FDesc D = desc3<FORM, MD, FULL>(d);
+            const double v = mirror_value(F.p[D.f][pj], D.cls, code);
+            if (D.gx >= 0) sx[d] = sx[d] + v * wx;
+            if (D.gy >= 0) sy[d] = sy[d] + v * wy;
+            if (D.gl >= 0) sl[d] = sl[d] + v * wl;
         }
     }
-    if (comp & 4) {
-        double t = 0.0;
-        for (int m = 0; m < L.ncfd; m++) t = t + f[zlayer(L, iz, m) + i] * L.fdg[m];
-        gz[k] = t;
+#pragma unroll
+    for (int d = 0; d < N; d++) {
+        const FDesc D = desc3<FORM, MD, FULL>(d);
+        const double *f = F.p[D.f];
+        const double p = f[k];
+        if (D.gx >= 0) G[(size_t)D.gx * n + k] = sx[d] - p * L.gsx[i];
+        if (D.gy >= 0) G[(size_t)D.gy * n + k] = sy[d] - p * L.gsy[i];
+        if (D.gl >= 0) {
+            const double r = sl[d] - p * L.lsum[i];
+            double t = 0.0;
+            for (int m = 0; m < L.ncfd; m++) t = t + f[row + zlayer(L, iz, m)] * L.fdl[m];
+            G[(size_t)D.gl * n + k] = r + t;
+        }
+        if (D.gz >= 0) {
+            double t = 0.0;
+            for (int m = 0; m < L.ncfd; m++) t = t + f[row + zlayer(L, iz, m)] * L.fdg[m];
+            G[(size_t)D.gz * n + k] = t;
+        }
     }
 }
 
@@ -96,14 +150,13 @@ __global__ void k3_filter_xy(Layer3 L, const double *f, int cls, double *out) {
     const size_t n = (size_t)L.nl * L.nz;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
-    const size_t off = (size_t)iz * L.nl;
+    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
     const long long base = L.slice_ptr[i >> 5];
     double t = 0.0;
     for (int q = 0; q < L.cnt[i]; q++) {
         const long long o = sell_at(base, q, i & 31);
         const int l = __ldg(L.lidx + o);
-        t = t + mirror_value(f[off + (l & kLinkMask)], cls, (int)((unsigned)l >> 30)) * __ldg(L.wh + o);
+        t = t + mirror_value(f[(size_t)(l & kLinkMask) * L.nz + iz], cls, (int)((unsigned)l >> 30)) * __ldg(L.wh + o);
     }
     const double p = f[k];
     out[k] = p + (t - p * L.hsum[i]);
@@ -113,9 +166,10 @@ __global__ void k3_filter_z(Layer3 L, const double *in, double *out) {
     const size_t n = (size_t)L.nl * L.nz;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int iz = (int)(k / L.nl), i = (int)(k - (size_t)iz * L.nl);
+    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
+    const size_t row = (size_t)i * L.nz;
     double t = 0.0;
-    for (int m = 0; m < L.ncfd; m++) t = t + in[zlayer(L, iz, m) + i] * L.fdh[m];
+    for (int m = 0; m < L.ncfd; m++) t = t + in[row + zlayer(L, iz, m)] * L.fdh[m];
     out[k] = in[k] + t;
 }
 
@@ -297,7 +351,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         const StepConsts &K = P.K;
         const double *G = P.G;
         auto g = [&](int a) { return G[(size_t)a * n + k]; };
-        const int i = (int)(k % P.nl);
+        const int i = (int)(k / P.nz);
         const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
         const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
         const double tmp = ((u * g(ROX) + v * g(ROY)) + w * g(ROZ));
@@ -522,13 +576,13 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
 }
 
 // Block sums of (rho - rho_char) vol (or of vol), in a fixed tree; folded in block order.
-__global__ void k3_mass_partials(int nl, size_t n, const double *ro, const double *vol, double rho_char, int volume_only,
+__global__ void k3_mass_partials(int nz, size_t n, const double *ro, const double *vol, double rho_char, int volume_only,
                                  double *partials) {
     __shared__ double red[128];
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
     if (k < n) {
-        const double vi = vol[k % nl];
+        const double vi = vol[k / nz];
         v = volume_only ? vi : (ro[k] - rho_char) * vi;
     }
     red[threadIdx.x] = v;
@@ -553,9 +607,6 @@ __global__ void k3_fold(const double *partials, int nblk, double *out, const dou
 }
 
 // End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
-struct Fields19 {
-    double *p[19];
-};
 __global__ void k3_finalize(size_t n, Fields19 F, int chl, int lc, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
@@ -588,12 +639,12 @@ __global__ void k3_finalize(size_t n, Fields19 F, int chl, int lc, DevScalars *s
 }
 
 // set_tstep (step.F90:569-622) over the 3-D nodes: block minima as bit patterns
-__global__ void k3_tstep(int nl, size_t n, const double *u, const double *v, const double *w, const double *ro,
+__global__ void k3_tstep(int nz, size_t n, const double *u, const double *v, const double *w, const double *ro,
                          const double *sp, double csq, double visc_total, DevScalars *sc) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     double tc = 1.0e10, tp = 1.0e10;
     if (k < n) {
-        const int i = (int)(k % nl);
+        const int i = (int)(k / nz);
         const double c = sqrt(csq);
         const double um = sqrt((u[k] * u[k] + v[k] * v[k]) + w[k] * w[k]);
         tc = sp[i] / (um + c);
@@ -631,18 +682,19 @@ __global__ void k3_tstep_fold(DevScalars *sc, double L, int pid) {
     sc->dt = dt;
 }
 
-// reference layer-major arrays <-> internal layer-major arrays
-__global__ void k3_gather(const double *in, const int *perm, int nl, size_t n, double *out) {
+// reference arrays (layer-major, reference node order) <-> internal arrays (node-major, layers
+// innermost, internal node order)
+__global__ void k3_gather(const double *in, const int *perm, int nl, int nz, size_t n, double *out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const size_t iz = k / nl;
-    out[k] = in[iz * nl + perm[k - iz * nl]];
+    const size_t i = k / nz, iz = k - i * nz;
+    out[k] = in[iz * nl + perm[i]];
 }
-__global__ void k3_scatter(const double *in, const int *perm, int nl, size_t n, double *out) {
+__global__ void k3_scatter(const double *in, const int *perm, int nl, int nz, size_t n, double *out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const size_t iz = k / nl;
-    out[iz * nl + perm[k - iz * nl]] = in[k];
+    const size_t i = k / nz, iz = k - i * nz;
+    out[iz * nl + perm[i]] = in[k];
 }
 __global__ void k3_fill(size_t n, double v, double *out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -744,52 +796,26 @@ inline size_t n3(const Handle *H) { return (size_t)H->npfb * H->nz; }
 inline unsigned nblk(size_t n) { return (unsigned)((n + 127) / 128); }
 
 // all the derivatives the right-hand side reads, of buffer b
-int derivs3(Handle *H, int b) {
-    const Layer3 L = layer3(H);
+template <int FORM, bool MD, bool FULL>
+int derivs3_launch(Handle *H, int b) {
     const size_t n = n3(H);
-    double *const *f = H->f3[b];
-    double *G = H->g3;
-    auto A = [&](int a) { return G + (size_t)a * n; };
-    cudaStream_t st = H->stream;
-    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[0], 0, 7, A(ROX), A(ROY), A(ROZ), nullptr);
-    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[4], 1, 7, A(UX), A(UY), A(UZ), A(LU));
-    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[5], 2, 7, A(VX), A(VY), A(VZ), A(LV));
-    k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[6], 0, 7, A(WX), A(WY), A(WZ), A(LW));
-    if (H->cfg.form == SUNSET_FORM_CHL) {
-        // rhs.F90:186-201: full gradients of every psi component; with polymer diffusion the
-        // Laplacians of c
-        static const int cls[6] = {0, 3, 0, 0, 0, 0};
-        const bool md = H->cfg.Mdiff != 0.0;
-        for (int q = 0; q < 6; q++)
-            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[13 + q], cls[q], 7, A(CG0 + 3 * q), A(CG0 + 3 * q + 1),
-                                              A(CG0 + 3 * q + 2), nullptr);
-        if (md)
-            for (int q = 0; q < 6; q++)
-                k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], 0, nullptr, nullptr, nullptr, A(LC0 + q));
-    }
-    if (H->cfg.form == SUNSET_FORM_LC) {
-        // rhs_lc.F90:184-193: c gradients for the momentum equation (c_xx x, c_yy y, c_zz z
-        // only); :397-409: full psi gradients for the advection
-        static const int cls[6] = {0, 3, 0, 0, 0, 0}, mask[6] = {1, 7, 2, 7, 7, 4};
-        for (int q = 0; q < 6; q++) {
-            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], mask[q], A(CG0 + 3 * q), A(CG0 + 3 * q + 1),
-                                              A(CG0 + 3 * q + 2), nullptr);
-            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[13 + q], cls[q], 7, A(PG0 + 3 * q), A(PG0 + 3 * q + 1),
-                                              A(PG0 + 3 * q + 2), nullptr);
-        }
-    }
-    if (H->cfg.form == SUNSET_FORM_DI) {
-        // rhs_di.F90:186-194: c_xx x only, c_xy c_xz c_yz full, c_yy y only, c_zz z only; the
-        // rest with full gradients, else zero (set once at allocation)
-        static const int cls[6] = {0, 3, 0, 0, 0, 0}, mask[6] = {1, 7, 2, 7, 7, 4};
-        const bool md = H->cfg.Mdiff != 0.0;
-        for (int q = 0; q < 6; q++)
-            k3_deriv<<<nblk(n), 128, 0, st>>>(L, f[7 + q], cls[q], H->cfg.di_full_gradients ? 7 : mask[q],
-                                              A(CG0 + 3 * q), A(CG0 + 3 * q + 1), A(CG0 + 3 * q + 2),
-                                              md ? A(LC0 + q) : nullptr);
-    }
+    Fields19 F;
+    for (int q = 0; q < 19; q++) F.p[q] = H->f3[b][q];
+    k3_derivs<FORM, MD, FULL><<<nblk(n), 128, 0, H->stream>>>(layer3(H), F, H->g3);
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
+}
+int derivs3(Handle *H, int b) {
+    const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0;
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI:
+        if (md) return full ? derivs3_launch<SUNSET_FORM_DI, true, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, true, false>(H, b);
+        return full ? derivs3_launch<SUNSET_FORM_DI, false, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, false, false>(H, b);
+    case SUNSET_FORM_CHL:
+        return md ? derivs3_launch<SUNSET_FORM_CHL, true, false>(H, b) : derivs3_launch<SUNSET_FORM_CHL, false, false>(H, b);
+    case SUNSET_FORM_LC: return derivs3_launch<SUNSET_FORM_LC, false, false>(H, b);
+    default: return derivs3_launch<SUNSET_FORM_NEWT, false, false>(H, b);
+    }
 }
 
 Point3 point3(Handle *H, int b, int stage) {
@@ -817,7 +843,7 @@ Point3 point3(Handle *H, int b, int stage) {
 int tstep3_launch(Handle *H, int b, int pid) {
     const size_t n = n3(H);
     const double *const *f = H->f3[b];
-    k3_tstep<<<nblk(n), 128, 0, H->stream>>>(H->npfb, n, f[4], f[5], f[6], f[0], H->sp, step_consts(H->cfg, 1, 1, false, false).csq,
+    k3_tstep<<<nblk(n), 128, 0, H->stream>>>(H->nz, n, f[4], f[5], f[6], f[0], H->sp, step_consts(H->cfg, 1, 1, false, false).csq,
                                              step_consts(H->cfg, 1, 1, false, false).visc_total, H->dsc);
     k3_tstep_fold<<<1, 1, 0, H->stream>>>(H->dsc, H->cfg.L_char, pid);
     SUNSET_CUDA(H, cudaGetLastError());
@@ -897,7 +923,7 @@ int state3_set(Handle *H, const double *const *fields10) {
             continue;
         }
         SUNSET_CUDA(H, cudaMemcpyAsync(H->tmp3, fields10[q], n * sizeof(double), cudaMemcpyHostToDevice, st));
-        k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, n, d);
+        k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, H->nz, n, d);
     }
     k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
     if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
@@ -914,7 +940,7 @@ int state3_set(Handle *H, const double *const *fields10) {
     s.par_bits = 0x7ff0000000000000ull;
     SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, st));
     // sum of the 3-D nodes' volumes, for the mass correction
-    k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->npfb, n, f[0], H->vol, 1.0, 1, H->partials3);
+    k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, f[0], H->vol, 1.0, 1, H->partials3);
     k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->tv, nullptr, 1);
     SUNSET_CUDA(H, cudaGetLastError());
     return tstep3_launch(H, 0, 0);
@@ -926,7 +952,7 @@ int state3_get(Handle *H, double *out19) {
     const size_t n = n3(H);
     cudaStream_t st = H->stream;
     for (int f = 0; f < 19; f++) {
-        k3_scatter<<<nblk(n), 128, 0, st>>>(H->f3[H->cur3][f], H->perm, H->npfb, n, H->tmp3);
+        k3_scatter<<<nblk(n), 128, 0, st>>>(H->f3[H->cur3][f], H->perm, H->npfb, H->nz, n, H->tmp3);
         SUNSET_CUDA(H, cudaMemcpyAsync(out19 + (size_t)f * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, st));
         SUNSET_CUDA(H, cudaStreamSynchronize(st));
     }
@@ -941,7 +967,7 @@ int rhs3_calc(Handle *H, double *out10) {
     k3_point<<<nblk(n), 128, 0, H->stream>>>(P);
     SUNSET_CUDA(H, cudaGetLastError());
     for (int q = 0; q < 10; q++) {
-        k3_scatter<<<nblk(n), 128, 0, H->stream>>>(H->rhs3[q], H->perm, H->npfb, n, H->tmp3);
+        k3_scatter<<<nblk(n), 128, 0, H->stream>>>(H->rhs3[q], H->perm, H->npfb, H->nz, n, H->tmp3);
         SUNSET_CUDA(H, cudaMemcpyAsync(out10 + (size_t)q * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
         SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
     }
@@ -979,7 +1005,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
             k3_filter_xy<<<nblk(n), 128, 0, st>>>(L, f, cls[q], H->tmp3);
             k3_filter_z<<<nblk(n), 128, 0, st>>>(L, H->tmp3, f);
         }
-        k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->npfb, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
+        k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
         k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields19 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
