@@ -410,19 +410,38 @@ def run_3d(args, local):
     # a smooth conformation with distinct eigenvalues everywhere (the reference's closed-form 3x3
     # eigen solver has no branch for a repeated eigenvalue with nonzero off-diagonal terms)
     ro = 1.0 + 0.01 * np.cos(tp * x) * np.cos(tp * z)
-    g.set_state_3d(ro, u, v, w, 1.2 + 0.1 * np.sin(tp * z), 0.05 * np.sin(tp * x) * np.sin(tp * y),
-                   1.1 + 0.05 * np.cos(tp * y), 0.05 * np.cos(tp * z) * np.sin(tp * x), 0.03 * np.sin(tp * z),
-                   1.05 + 0.02 * np.cos(tp * x))
+    st3 = [ro, u, v, w, 1.2 + 0.1 * np.sin(tp * z), 0.05 * np.sin(tp * x) * np.sin(tp * y),
+           1.1 + 0.05 * np.cos(tp * y), 0.05 * np.cos(tp * z) * np.sin(tp * x), 0.03 * np.sin(tp * z),
+           1.05 + 0.02 * np.cos(tp * x)]
+    g.set_state_3d(*st3)
     dtc, dtp = g.set_tstep()
     dt = dt_for(wl, dtc, dtp)
     g.step(dt, args.warmup)
     ms = g.step_timed(dt, args.steps)
     n = nl * nz
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the CPU restatement on the same 3-D set, all host cores, one step (weights of the
+        # layer taken from the device build to keep the sample bounded)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.set_threads(cpu_threads())
+        lay = O.for_workload(wl, ns)
+        cnt, cs, links = g.neighbours()
+        lay.set_neighbours_weights(cnt, cs, links, g.weights())
+        o3 = O.Oracle3(lay, args.layers)
+        o3.set_state(*st3[:4], *st3[4:])
+        t0 = time.perf_counter()
+        o3.step(dt, 1)
+        el = time.perf_counter() - t0
+        cpu = {"value": n / el, "unit": "node-steps/s", "cores": cpu_threads(), "kind": "port",
+               "sample": f"1 step of the full {n}-node 3-D set (layer weights from the device build)"}
     line = {"metric": METRIC + " (3-D)", "value": n * args.steps / (ms * 1e-3), "unit": "node-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded jittered lattice, stacked in z)",
             "config": {"workload": wl.name + f"-3d-nside{args.nside}", "nodes_per_layer": nl, "layers": nz, "dz": dz,
-                       "nodes": n, "order": wl.order, "form": wl.form, "precision": "fp64"}}
+                       "nodes": n, "order": wl.order, "form": wl.form, "precision": "fp64"},
+            "cpu_baseline": cpu}
     print(json.dumps(line))
     return 0
 
