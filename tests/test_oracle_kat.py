@@ -385,3 +385,78 @@ def test_adapt_stencils_invariants():
         print(form, order, "reduced", int(np.sum(h < h0)), "of", n, "max steps", int(steps.max()),
               "max |w_lap| s^2 interior", lap.max())
         assert lap.max() < 10.0
+
+
+@pytest.mark.parametrize("form, eps", [("di", 0.25), ("chl", 0.25), ("lc", 0.0), ("newt", 0.0)])
+def test_3d_reduces_to_2d(form, eps):
+    """3-D restatement, known answer: with w = 0, c_xz = c_yz = 0, c_zz = 1 and fields that do
+    not vary in z, every layer's right-hand side is the 2-D one (the z stencils see constants;
+    rho w, c_xz and c_yz stay at rest).  The log-conformation form takes eps = 0: its 3-D sPTT
+    trace includes c_zz, the 2-D one does not (rhs_lc.F90:451-456)."""
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16, form=form, epsPTT=eps)
+    ns = wl.nodes()
+    o = O.for_workload(wl, ns, kolmogorov_forcing=0).setup()
+    o3 = O.Oracle3(o, 0.4)
+    nl = o3.nl
+    x, y = ns.x, ns.y
+    tp = 2.0 * np.pi
+    st = dict(ro=1.0 + 0.01 * np.cos(tp * x), u=np.sin(tp * x) * np.cos(tp * y), v=-np.cos(tp * x) * np.sin(tp * y),
+              cxx=1.2 + 0.1 * np.sin(tp * x), cxy=0.1 * np.cos(tp * y), cyy=1.1 + 0.05 * np.cos(tp * x), czz=np.ones(nl))
+    o.set_state(**st)
+    r2 = o.rhs()
+    T = lambda a: np.tile(a, o3.nz)
+    zero = np.zeros(o3.n)
+    o3.set_state(T(st["ro"]), T(st["u"]), T(st["v"]), zero, T(st["cxx"]), T(st["cxy"]), T(st["cyy"]), zero, zero,
+                 np.ones(o3.n))
+    r3 = o3.rhs()
+    keys = ["ro", "rou", "rov"] + ([] if form == "newt" else ["xx", "xy", "yy"])
+    for k in keys:
+        scale = max(np.abs(r2[k]).max(), 1.0)
+        e = np.abs(r3[k].reshape(o3.nz, nl) - r2[k][None, :]).max() / scale
+        assert e < 1e-9, (form, k, e)
+    for k in ["row", "xz", "yz"]:
+        assert np.abs(r3[k]).max() < 1e-9 * max(np.abs(r2["rou"]).max(), 1.0), (form, k)
+
+
+def central_first_derivative(m):
+    """Weights a_1..a_m of the central difference of 2m + 1 points for d/dz, from Taylor
+    matching in exact rationals: sum_j a_j j^(2q-1) = 1/2 for q = 1 and 0 for q = 2..m."""
+    A = [[Fraction(j) ** (2 * q - 1) for j in range(1, m + 1)] for q in range(1, m + 1)]
+    b = [Fraction(1, 2)] + [Fraction(0)] * (m - 1)
+    for c in range(m):  # Gauss-Jordan
+        r = next(r for r in range(c, m) if A[r][c] != 0)
+        A[c], A[r], b[c], b[r] = A[r], A[c], b[r], b[c]
+        for r in range(m):
+            if r != c and A[r][c] != 0:
+                f = A[r][c] / A[c][c]
+                A[r] = [x - f * y for x, y in zip(A[r], A[c])]
+                b[r] -= f * b[c]
+    return [b[j] / A[j][j] for j in range(m)]
+
+
+@pytest.mark.parametrize("wlname", ["periodic-di-o4-16k", "periodic-lc-o6-262k", "periodic-chl-o8-1m"])
+def test_3d_z_stencils(wlname):
+    """calc_fd_weights (fd.F90:27-256): the periodic z derivative is the central difference of
+    order + 1 points.  On w = sin(k z) with k = 2 pi / L_z over a uniform periodic column it
+    returns exactly cos(k z) * (2 / dz) sum_j a_j sin(j k dz) (the stencil's modified
+    wavenumber), with the a_j derived here independently of the restatement's tables.  With
+    rho = 1 and u = v = 0 the continuity right-hand side is -dw/dz."""
+    wl = dataclasses.replace(WORKLOADS[wlname], nside=12, form="newt")
+    ns = wl.nodes()
+    o = O.for_workload(wl, ns, kolmogorov_forcing=0).setup()
+    o3 = O.Oracle3(o, 1.0)
+    nl, nz, dz = o3.nl, o3.nz, o3.dz
+    m = wl.order // 2
+    assert nz >= 2 * m + 1
+    k = 2.0 * np.pi / (nz * dz)
+    z = np.repeat(np.arange(nz) * dz, nl)
+    o3.set_state(np.ones(o3.n), np.zeros(o3.n), np.zeros(o3.n), np.sin(k * z))
+    r = o3.rhs()
+    a = central_first_derivative(m)
+    kmod = 2.0 / dz * sum(float(aj) * math.sin((j + 1) * k * dz) for j, aj in enumerate(a))
+    err = np.abs(r["ro"] + kmod * np.cos(k * z)).max() / k
+    assert err < 1e-11, (wlname, err)
+    # and the truncation error has the stencil's order: (k dz)^order sized, not zero
+    assert 1e-3 * (k * dz) ** wl.order < abs(kmod - k) / k < (k * dz) ** wl.order
+    for key in ("rou", "rov", "xx", "xy", "yy"):
+        assert np.abs(r[key]).max() < 1e-12, key
