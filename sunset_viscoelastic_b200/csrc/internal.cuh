@@ -31,8 +31,13 @@ constexpr double kPi = 3.141592653589793238462643383279502884197;
 constexpr double kSs = 2.0;  // stencil support in units of h, common_parameter.F90:68
 constexpr int kSlice = 32;
 constexpr int kLinkMask = 0x3fffffff;  // low 30 bits: internal parent index
-constexpr int kTileSlices = 8;         // slices per thread block of the staged stencil kernels
+#ifndef SUNSET_TILE_SLICES
+#define SUNSET_TILE_SLICES 8
+#endif
+constexpr int kTileSlices = SUNSET_TILE_SLICES;  // slices per thread block of the staged stencil kernels
 constexpr int kTile = kTileSlices * 32;
+// per-tile partial sums live in a buffer of nodes / 128 + 1 entries
+static_assert(kTile >= 128 && kTile <= 1024, "tile of 128 to 1024 nodes");
 constexpr int kLocMask = 0x3fff;       // low 14 bits of a local link: position in the tile's halo
 
 // RK3(2)4[2R+]C, common_parameter.F90:74-94

@@ -51,11 +51,24 @@ __device__ __forceinline__ double mirror_value(double x, int cls, int code) {
     return flip ? -x : x;
 }
 
-// layer of the m-th point of the z stencil (fd.F90:62-66, periodic)
-__device__ __forceinline__ int zlayer(const Layer3 &L, int iz, int m) {
-    int l = (iz + m - L.ncfd / 2) % L.nz;
-    if (l < 0) l += L.nz;
-    return l;
+// layer l = iz + m - ncfd/2 of the m-th point of the periodic z stencil (fd.F90:62-66); the
+// offset is below nz in magnitude (layers_set keeps nz >= ncfd/2 + 2), so one wrap suffices
+__device__ __forceinline__ int zwrap(int l, int nz) {
+    l += (l < 0) ? nz : 0;
+    return (l >= nz) ? l - nz : l;
+}
+
+// thread k of the node-major layered arrays: node i, layer iz (n < 2^31, checked in layers_set)
+struct ZThread {
+    int k, i, iz;
+};
+__device__ __forceinline__ bool zthread(int nl, int nz, ZThread &t) {
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (unsigned)nl * (unsigned)nz) return false;
+    t.k = (int)k;
+    t.i = (int)(k / (unsigned)nz);
+    t.iz = (int)k - t.i * nz;
+    return true;
 }
 
 struct Fields19 {
@@ -95,84 +108,168 @@ __host__ __device__ constexpr FDesc desc3(int d) {
 // Every derivative the right-hand side reads, in one pass over each node's links: the x-y
 // LABFM sums of all fields (in the reference's link order, each sum as calc_gradient /
 // calc_laplacian forms it), then the z stencils.  The layers of a node share its links, so a
-// warp's link and weight loads are one broadcast each.
+// warp's link and weight loads are one broadcast each.  The links go in pairs whose field
+// values are all loaded before either is summed, so that a warp keeps two links' gathers in
+// flight (the sums still run in link order).
 template <int FORM, bool MD, bool FULL>
 __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G) {
     constexpr int N = ndesc<FORM, MD>();
+    constexpr int LB = 2;
+    ZThread z;
+    if (!zthread(L.nl, L.nz, z)) return;
     const size_t n = (size_t)L.nl * L.nz;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
-    const size_t row = (size_t)i * L.nz;
+    const int k = z.k, i = z.i, iz = z.iz, row = i * L.nz, h = L.ncfd / 2;
     double sx[N], sy[N], sl[N];
 #pragma unroll
     for (int d = 0; d < N; d++) { sx[d] = 0.0; sy[d] = 0.0; sl[d] = 0.0; }
     const long long base = L.slice_ptr[i >> 5];
     const int cs = L.cnt_small[i];
-#pragma unroll 4
-    for (int q = 0; q < cs; q++) {
+    int q = 0;
+    for (; q + LB <= cs; q += LB) {
+        int pj[LB], code[LB];
+        double wx[LB], wy[LB], wl[LB], v[LB][N];
+#pragma unroll
+        for (int b = 0; b < LB; b++) {
+            const long long o = sell_at(base, q + b, i & 31);
+            const int l = __ldg(L.lidx + o);
+            pj[b] = (l & kLinkMask) * L.nz + iz;
+            code[b] = (int)((unsigned)l >> 30);
+            wx[b] = __ldg(L.wx + o);
+            wy[b] = __ldg(L.wy + o);
+            wl[b] = __ldg(L.wl + o);
+        }
+#pragma unroll
+        for (int b = 0; b < LB; b++)
+#pragma unroll
+            for (int d = 0; d < N; d++) v[b][d] = F.p[desc3<FORM, MD, FULL>(d).f][pj[b]];
+#pragma unroll
+        for (int b = 0; b < LB; b++)
+#pragma unroll
+            for (int d = 0; d < N; d++) {
+                const FDesc D = desc3<FORM, MD, FULL>(d);
+                const double x = mirror_value(v[b][d], D.cls, code[b]);
+                if (D.gx >= 0) sx[d] = sx[d] + x * wx[b];
+                if (D.gy >= 0) sy[d] = sy[d] + x * wy[b];
+                if (D.gl >= 0) sl[d] = sl[d] + x * wl[b];
+            }
+    }
+    for (; q < cs; q++) {
         const long long o = sell_at(base, q, i & 31);
         const int l = __ldg(L.lidx + o);
-        const size_t pj = (size_t)(l & kLinkMask) * L.nz + iz;
+        const int pj = (l & kLinkMask) * L.nz + iz;
         const int code = (int)((unsigned)l >> 30);
         const double wx = __ldg(L.wx + o), wy = __ldg(L.wy + o), wl = __ldg(L.wl + o);
 #pragma unroll
         for (int d = 0; d < N; d++) {
             const FDesc D = desc3<FORM, MD, FULL>(d);
-            const double v = mirror_value(F.p[D.f][pj], D.cls, code);
-            if (D.gx >= 0) sx[d] = sx[d] + v * wx;
-            if (D.gy >= 0) sy[d] = sy[d] + v * wy;
-            if (D.gl >= 0) sl[d] = sl[d] + v * wl;
+            const double x = mirror_value(F.p[D.f][pj], D.cls, code);
+            if (D.gx >= 0) sx[d] = sx[d] + x * wx;
+            if (D.gy >= 0) sy[d] = sy[d] + x * wy;
+            if (D.gl >= 0) sl[d] = sl[d] + x * wl;
+        }
+    }
+    // the x-y sums in sum form; the Laplacians keep theirs for the z part
+#pragma unroll
+    for (int d = 0; d < N; d++) {
+        const FDesc D = desc3<FORM, MD, FULL>(d);
+        const double p = F.p[D.f][k];
+        if (D.gx >= 0) G[(size_t)D.gx * n + k] = sx[d] - p * L.gsx[i];
+        if (D.gy >= 0) G[(size_t)D.gy * n + k] = sy[d] - p * L.gsy[i];
+        if (D.gl >= 0) sl[d] = sl[d] - p * L.lsum[i];
+    }
+    // the z stencils, point by point over all fields (each field's sums still run in point order)
+    double tg[N], tl[N];
+#pragma unroll
+    for (int d = 0; d < N; d++) { tg[d] = 0.0; tl[d] = 0.0; }
+    for (int m = 0; m < L.ncfd; m++) {
+        const int r = row + zwrap(iz + m - h, L.nz);
+        const double cg = L.fdg[m], cl = L.fdl[m];
+#pragma unroll
+        for (int d = 0; d < N; d++) {
+            const FDesc D = desc3<FORM, MD, FULL>(d);
+            if (D.gl < 0 && D.gz < 0) continue;
+            const double fm = F.p[D.f][r];
+            if (D.gl >= 0) tl[d] = tl[d] + fm * cl;
+            if (D.gz >= 0) tg[d] = tg[d] + fm * cg;
         }
     }
 #pragma unroll
     for (int d = 0; d < N; d++) {
         const FDesc D = desc3<FORM, MD, FULL>(d);
-        const double *f = F.p[D.f];
-        const double p = f[k];
-        if (D.gx >= 0) G[(size_t)D.gx * n + k] = sx[d] - p * L.gsx[i];
-        if (D.gy >= 0) G[(size_t)D.gy * n + k] = sy[d] - p * L.gsy[i];
-        if (D.gl >= 0) {
-            const double r = sl[d] - p * L.lsum[i];
-            double t = 0.0;
-            for (int m = 0; m < L.ncfd; m++) t = t + f[row + zlayer(L, iz, m)] * L.fdl[m];
-            G[(size_t)D.gl * n + k] = r + t;
-        }
-        if (D.gz >= 0) {
-            double t = 0.0;
-            for (int m = 0; m < L.ncfd; m++) t = t + f[row + zlayer(L, iz, m)] * L.fdg[m];
-            G[(size_t)D.gz * n + k] = t;
-        }
+        if (D.gl >= 0) G[(size_t)D.gl * n + k] = sl[d] + tl[d];
+        if (D.gz >= 0) G[(size_t)D.gz * n + k] = tg[d];
     }
 }
 
-// calc_filtered_var in 3-D: the x-y filter (into out) ...
-__global__ void k3_filter_xy(Layer3 L, const double *f, int cls, double *out) {
-    const size_t n = (size_t)L.nl * L.nz;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
+// calc_filtered_var in 3-D for the NF evolved fields (ro, rou, rov, row, then the six c or psi
+// variables) in one pass over each node's links: the x-y filter of every field into its
+// scratch array ...
+struct Filter3 {
+    double *f[10];  // the fields, filtered in place
+    double *t[10];  // x-y filtered values
+};
+// sign class at mirrors of the filtered fields: rou like u, rov like v, c_xy / psi_xy like c_xy
+__host__ __device__ constexpr int filter_cls(int q) { return q == 1 ? 1 : q == 2 ? 2 : q == 5 ? 3 : 0; }
+
+template <int NF>
+__global__ void __launch_bounds__(128) k3_filter_xy(Layer3 L, Filter3 A) {
+    ZThread z;
+    if (!zthread(L.nl, L.nz, z)) return;
+    const int k = z.k, i = z.i, iz = z.iz;
     const long long base = L.slice_ptr[i >> 5];
-    double t = 0.0;
-#pragma unroll 4
-    for (int q = 0; q < L.cnt[i]; q++) {
-        const long long o = sell_at(base, q, i & 31);
-        const int l = __ldg(L.lidx + o);
-        t = t + mirror_value(f[(size_t)(l & kLinkMask) * L.nz + iz], cls, (int)((unsigned)l >> 30)) * __ldg(L.wh + o);
+    double t[NF];
+#pragma unroll
+    for (int q = 0; q < NF; q++) t[q] = 0.0;
+    const int c = L.cnt[i];
+    // links in pairs, both links' values loaded before either is summed (sums in link order)
+    int m = 0;
+    for (; m + 2 <= c; m += 2) {
+        const long long o0 = sell_at(base, m, i & 31), o1 = sell_at(base, m + 1, i & 31);
+        const int l0 = __ldg(L.lidx + o0), l1 = __ldg(L.lidx + o1);
+        const double w0 = __ldg(L.wh + o0), w1 = __ldg(L.wh + o1);
+        const int p0 = (l0 & kLinkMask) * L.nz + iz, p1 = (l1 & kLinkMask) * L.nz + iz;
+        double v0[NF], v1[NF];
+#pragma unroll
+        for (int q = 0; q < NF; q++) { v0[q] = A.f[q][p0]; v1[q] = A.f[q][p1]; }
+        const int c0 = (int)((unsigned)l0 >> 30), c1 = (int)((unsigned)l1 >> 30);
+#pragma unroll
+        for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(v0[q], filter_cls(q), c0) * w0;
+#pragma unroll
+        for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(v1[q], filter_cls(q), c1) * w1;
     }
-    const double p = f[k];
-    out[k] = p + (t - p * L.hsum[i]);
+    if (m < c) {
+        const long long o = sell_at(base, m, i & 31);
+        const int l = __ldg(L.lidx + o);
+        const int pj = (l & kLinkMask) * L.nz + iz;
+        const int code = (int)((unsigned)l >> 30);
+        const double w = __ldg(L.wh + o);
+#pragma unroll
+        for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(A.f[q][pj], filter_cls(q), code) * w;
+    }
+    const double hs = L.hsum[i];
+#pragma unroll
+    for (int q = 0; q < NF; q++) {
+        const double p = A.f[q][k];
+        A.t[q][k] = p + (t[q] - p * hs);
+    }
 }
 // ... then the z filter of that result (back into the field)
-__global__ void k3_filter_z(Layer3 L, const double *in, double *out) {
-    const size_t n = (size_t)L.nl * L.nz;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const int i = (int)(k / L.nz), iz = (int)(k - (size_t)i * L.nz);
-    const size_t row = (size_t)i * L.nz;
-    double t = 0.0;
-    for (int m = 0; m < L.ncfd; m++) t = t + in[row + zlayer(L, iz, m)] * L.fdh[m];
-    out[k] = in[k] + t;
+template <int NF>
+__global__ void __launch_bounds__(128) k3_filter_z(Layer3 L, Filter3 A) {
+    ZThread z;
+    if (!zthread(L.nl, L.nz, z)) return;
+    const int k = z.k, iz = z.iz, row = z.i * L.nz, h = L.ncfd / 2;
+    double t[NF];
+#pragma unroll
+    for (int q = 0; q < NF; q++) t[q] = 0.0;
+    for (int m = 0; m < L.ncfd; m++) {
+        const int r = row + zwrap(iz + m - h, L.nz);
+        const double c = L.fdh[m];
+#pragma unroll
+        for (int q = 0; q < NF; q++) t[q] = t[q] + A.t[q][r] * c;
+    }
+#pragma unroll
+    for (int q = 0; q < NF; q++) A.f[q][k] = A.t[q][k] + t[q];
 }
 
 struct Point3 {
@@ -353,7 +450,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         const StepConsts &K = P.K;
         const double *G = P.G;
         auto g = [&](int a) { return G[(size_t)a * n + k]; };
-        const int i = (int)(k / P.nz);
+        const int i = (int)((unsigned)k / (unsigned)P.nz);
         const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
         const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
         const double tmp = ((u * g(ROX) + v * g(ROY)) + w * g(ROZ));
@@ -646,7 +743,7 @@ __global__ void k3_tstep(int nz, size_t n, const double *u, const double *v, con
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     double tc = 1.0e10, tp = 1.0e10;
     if (k < n) {
-        const int i = (int)(k / nz);
+        const int i = (int)((unsigned)k / (unsigned)nz);
         const double c = sqrt(csq);
         const double um = sqrt((u[k] * u[k] + v[k] * v[k]) + w[k] * w[k]);
         tc = sp[i] / (um + c);
@@ -999,13 +1096,20 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         }
         // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694) or psi (rhs.F90:792-840);
         // the mass correction
-        static const int cls[10] = {0, 1, 2, 0, 0, 3, 0, 0, 0, 0};
+        // (the derivative scratch holds the x-y filtered values)
         const int c0 = (chl || lc) ? 13 : 7;
         const int fld[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
-        for (int q = 0; q < (evolves_c ? 10 : 4); q++) {
-            double *f = H->f3[b][fld[q]];
-            k3_filter_xy<<<nblk(n), 128, 0, st>>>(L, f, cls[q], H->tmp3);
-            k3_filter_z<<<nblk(n), 128, 0, st>>>(L, H->tmp3, f);
+        Filter3 FA{};
+        for (int q = 0; q < 10; q++) {
+            FA.f[q] = H->f3[b][fld[q]];
+            FA.t[q] = H->g3 + (size_t)q * n;
+        }
+        if (evolves_c) {
+            k3_filter_xy<10><<<nblk(n), 128, 0, st>>>(L, FA);
+            k3_filter_z<10><<<nblk(n), 128, 0, st>>>(L, FA);
+        } else {
+            k3_filter_xy<4><<<nblk(n), 128, 0, st>>>(L, FA);
+            k3_filter_z<4><<<nblk(n), 128, 0, st>>>(L, FA);
         }
         k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
         k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
