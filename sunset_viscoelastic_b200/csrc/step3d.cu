@@ -221,23 +221,8 @@ __global__ void __launch_bounds__(128) k3_filter_xy(Layer3 L, Filter3 A) {
 #pragma unroll
     for (int q = 0; q < NF; q++) t[q] = 0.0;
     const int c = L.cnt[i];
-    // links in pairs, both links' values loaded before either is summed (sums in link order)
-    int m = 0;
-    for (; m + 2 <= c; m += 2) {
-        const long long o0 = sell_at(base, m, i & 31), o1 = sell_at(base, m + 1, i & 31);
-        const int l0 = __ldg(L.lidx + o0), l1 = __ldg(L.lidx + o1);
-        const double w0 = __ldg(L.wh + o0), w1 = __ldg(L.wh + o1);
-        const int p0 = (l0 & kLinkMask) * L.nz + iz, p1 = (l1 & kLinkMask) * L.nz + iz;
-        double v0[NF], v1[NF];
-#pragma unroll
-        for (int q = 0; q < NF; q++) { v0[q] = A.f[q][p0]; v1[q] = A.f[q][p1]; }
-        const int c0 = (int)((unsigned)l0 >> 30), c1 = (int)((unsigned)l1 >> 30);
-#pragma unroll
-        for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(v0[q], filter_cls(q), c0) * w0;
-#pragma unroll
-        for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(v1[q], filter_cls(q), c1) * w1;
-    }
-    if (m < c) {
+#pragma unroll 4
+    for (int m = 0; m < c; m++) {
         const long long o = sell_at(base, m, i & 31);
         const int l = __ldg(L.lidx + o);
         const int pj = (l & kLinkMask) * L.nz + iz;
@@ -442,7 +427,9 @@ __device__ __forceinline__ void chl3_psi_from_c(const double *c, double *p) {
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
 // 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).
+template <int FORM>
 __global__ void __launch_bounds__(128) k3_point(Point3 P) {
+    constexpr bool kDi = FORM == SUNSET_FORM_DI, kChl = FORM == SUNSET_FORM_CHL, kLc = FORM == SUNSET_FORM_LC;
     const size_t n = (size_t)P.nl * P.nz;
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long eb = 0;
@@ -461,7 +448,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         const double tsw = ro * ((u * g(WX) + v * g(WY)) + w * g(WZ)) - w * rr;
         double fvu = K.coef_solvent * g(LU), fvv = K.coef_solvent * g(LV), fvw = K.coef_solvent * g(LW);
         auto gp = [&](int q, int d) { return g(CG0 + 3 * q + d); };  // Cholesky: psi gradients
-        if (P.chl) {  // grad c from grad psi, rhs.F90:245-262
+        if (kChl) {  // grad c from grad psi, rhs.F90:245-262
             const double pxx = P.in[13][k], pxy = P.in[14][k], pyy = P.in[15][k], pxz = P.in[16][k], pyz = P.in[17][k],
                          pzz = P.in[18][k];
             const double gcxx1 = (2.0 * exp(2.0 * pxx)) * gp(0, 0);
@@ -477,7 +464,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + gcyz3);
             fvw = fvw + K.coef_polymeric * ((gcxz1 + gcyz2) + gczz3);
         }
-        if (P.di || P.lc) {
+        if (kDi || kLc) {
             fvu = fvu + K.coef_polymeric * ((g(CG0 + 0) + g(CG0 + 3 + 1)) + g(CG0 + 9 + 2));
             fvv = fvv + K.coef_polymeric * ((g(CG0 + 3 + 0) + g(CG0 + 6 + 1)) + g(CG0 + 12 + 2));
             fvw = fvw + K.coef_polymeric * ((g(CG0 + 9 + 0) + g(CG0 + 12 + 1)) + g(CG0 + 15 + 2));
@@ -491,7 +478,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
         r[2] = ((-tsv - gpy) + bfv) + fvv;
         r[3] = ((-tsw - gpz) + bfw) + fvw;
         for (int q = 4; q < 10; q++) r[q] = 0.0;
-        if (P.chl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D)
+        if (kChl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D)
             const double ux = g(UX), uy = g(UY), uz = g(UZ), vx = g(VX), vy = g(VY), vz = g(VZ);
             const double wx = g(WX), wy = g(WY), wz = g(WZ);
             double ad[6];
@@ -535,7 +522,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             r[8] = (-ad[4] + ucyz) + csyz;
             r[9] = (-ad[5] + uczz) + cszz;
         }
-        if (P.lc) {  // calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D)
+        if (kLc) {  // calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D)
             const bool first = (P.sc->itime == 1) && (P.stage == 0);
             double ad[6];
 #pragma unroll
@@ -587,7 +574,7 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
                 r[4 + q] = (ad[q] + ((OP[e] - PO[e]) + 2.0 * B[e])) + Rx[e];
             }
         }
-        if (P.di) {
+        if (kDi) {
             const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
                          czz = P.in[12][k];
             double ad[6];
@@ -613,12 +600,12 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
             r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
         }
-        const int nf = (P.di || P.chl || P.lc) ? 10 : 4;
+        const int nf = (kDi || kChl || kLc) ? 10 : 4;
         if (P.stage == 4) {
             for (int q = 0; q < 10; q++) P.rhs[q][k] = r[q];
         } else {
             // evolved fields: rho, rho u, rho v, rho w, then c (direct) or psi (Cholesky)
-            const int c0 = (P.chl || P.lc) ? 13 : 7;
+            const int c0 = (kChl || kLc) ? 13 : 7;
             const int src[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
             const int stage = P.stage;
             const double dt = P.sc->dt;
@@ -650,9 +637,9 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             P.out[4][k] = Un[1] * oo;
             P.out[5][k] = Un[2] * oo;
             P.out[6][k] = Un[3] * oo;
-            if (P.chl || P.lc) {  // get_c_from_psi
+            if (kChl || kLc) {  // get_c_from_psi
                 double c[6];
-                if (P.chl) chl3_c_from_psi(Un + 4, c);
+                if (kChl) chl3_c_from_psi(Un + 4, c);
                 else lc3_transform(Un + 4, c, true);
                 for (int q = 0; q < 6; q++) P.out[7 + q][k] = c[q];
             }
@@ -692,8 +679,10 @@ __global__ void k3_mass_partials(int nz, size_t n, const double *ro, const doubl
     }
     if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
 }
-__global__ void k3_fold(const double *partials, int nblk, double *out, const double *divisor, int enabled) {
-    __shared__ double red[128];
+constexpr int kFoldThreads = 1024;
+__global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, int nblk, double *out, const double *divisor,
+                                                         int enabled) {
+    __shared__ double red[kFoldThreads];
     double a = 0.0;
     for (int b = threadIdx.x; b < nblk; b += blockDim.x) a = a + partials[b];
     red[threadIdx.x] = a;
@@ -939,6 +928,19 @@ Point3 point3(Handle *H, int b, int stage) {
     return P;
 }
 
+// the pointwise right-hand side and RK update of the handle's form
+int point3_launch(Handle *H, const Point3 &P, cudaStream_t st) {
+    const unsigned nb = nblk(n3(H));
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI: k3_point<SUNSET_FORM_DI><<<nb, 128, 0, st>>>(P); break;
+    case SUNSET_FORM_CHL: k3_point<SUNSET_FORM_CHL><<<nb, 128, 0, st>>>(P); break;
+    case SUNSET_FORM_LC: k3_point<SUNSET_FORM_LC><<<nb, 128, 0, st>>>(P); break;
+    default: k3_point<SUNSET_FORM_NEWT><<<nb, 128, 0, st>>>(P); break;
+    }
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
 int tstep3_launch(Handle *H, int b, int pid) {
     const size_t n = n3(H);
     const double *const *f = H->f3[b];
@@ -1040,7 +1042,7 @@ int state3_set(Handle *H, const double *const *fields10) {
     SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, &s, sizeof(s), cudaMemcpyHostToDevice, st));
     // sum of the 3-D nodes' volumes, for the mass correction
     k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, f[0], H->vol, 1.0, 1, H->partials3);
-    k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->tv, nullptr, 1);
+    k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->tv, nullptr, 1);
     SUNSET_CUDA(H, cudaGetLastError());
     return tstep3_launch(H, 0, 0);
 }
@@ -1063,7 +1065,7 @@ int rhs3_calc(Handle *H, double *out10) {
     const size_t n = n3(H);
     if (int rc = derivs3(H, H->cur3)) return rc;
     Point3 P = point3(H, H->cur3, 4);
-    k3_point<<<nblk(n), 128, 0, H->stream>>>(P);
+    if (int rc = point3_launch(H, P, H->stream)) return rc;
     SUNSET_CUDA(H, cudaGetLastError());
     for (int q = 0; q < 10; q++) {
         k3_scatter<<<nblk(n), 128, 0, H->stream>>>(H->rhs3[q], H->perm, H->npfb, H->nz, n, H->tmp3);
@@ -1091,7 +1093,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         for (int stage = 0; stage < 4; stage++) {
             if (int rc = derivs3(H, b)) return rc;
             Point3 P = point3(H, b, stage);
-            k3_point<<<nblk(n), 128, 0, st>>>(P);
+            if (int rc = point3_launch(H, P, st)) return rc;
             b ^= 1;
         }
         // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694) or psi (rhs.F90:792-840);
@@ -1112,7 +1114,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
             k3_filter_z<4><<<nblk(n), 128, 0, st>>>(L, FA);
         }
         k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
-        k3_fold<<<1, 128, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
+        k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields19 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
         k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->dsc, H->cfg.vpid);
