@@ -71,8 +71,10 @@ __device__ __forceinline__ bool zthread(int nl, int nz, ZThread &t) {
     return true;
 }
 
-struct Fields19 {
-    double *p[19];
+// the 19 state fields (ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)); slot 19 holds the
+// FENE-P function of the direct form where the gather reads it
+struct Fields3 {
+    double *p[20];
 };
 
 // What one pass over a node's links gathers: per field, the G slots of its x-y sums (and z
@@ -105,15 +107,25 @@ __host__ __device__ constexpr FDesc desc3(int d) {
     return FDesc{13 + q, cls, PG0 + 3 * q, PG0 + 3 * q + 1, -1, PG0 + 3 * q + 2};
 }
 
+// the gathered fields of a pass; with FEN (FENE-P, direct form) one more, the function
+// f = (L^2 - 3)/(L^2 - tr c) of slot 19, whose gradient goes to the slots PG0.. the direct form
+// leaves free (rhs_di.F90:198-205)
+template <int FORM, bool MD, bool FEN>
+__host__ __device__ constexpr int ndesc3() { return ndesc<FORM, MD>() + (FEN ? 1 : 0); }
+template <int FORM, bool MD, bool FULL, bool FEN>
+__host__ __device__ constexpr FDesc desc3f(int d) {
+    return (FEN && d == ndesc<FORM, MD>()) ? FDesc{19, 0, PG0, PG0 + 1, -1, PG0 + 2} : desc3<FORM, MD, FULL>(d);
+}
+
 // Every derivative the right-hand side reads, in one pass over each node's links: the x-y
 // LABFM sums of all fields (in the reference's link order, each sum as calc_gradient /
 // calc_laplacian forms it), then the z stencils.  The layers of a node share its links, so a
 // warp's link and weight loads are one broadcast each.  The links go in pairs whose field
 // values are all loaded before either is summed, so that a warp keeps two links' gathers in
 // flight (the sums still run in link order).
-template <int FORM, bool MD, bool FULL>
-__global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G) {
-    constexpr int N = ndesc<FORM, MD>();
+template <int FORM, bool MD, bool FULL, bool FEN>
+__global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields3 F, double *G) {
+    constexpr int N = ndesc3<FORM, MD, FEN>();
     constexpr int LB = 2;
     ZThread z;
     if (!zthread(L.nl, L.nz, z)) return;
@@ -141,12 +153,12 @@ __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G
 #pragma unroll
         for (int b = 0; b < LB; b++)
 #pragma unroll
-            for (int d = 0; d < N; d++) v[b][d] = F.p[desc3<FORM, MD, FULL>(d).f][pj[b]];
+            for (int d = 0; d < N; d++) v[b][d] = F.p[desc3f<FORM, MD, FULL, FEN>(d).f][pj[b]];
 #pragma unroll
         for (int b = 0; b < LB; b++)
 #pragma unroll
             for (int d = 0; d < N; d++) {
-                const FDesc D = desc3<FORM, MD, FULL>(d);
+                const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
                 const double x = mirror_value(v[b][d], D.cls, code[b]);
                 if (D.gx >= 0) sx[d] = sx[d] + x * wx[b];
                 if (D.gy >= 0) sy[d] = sy[d] + x * wy[b];
@@ -161,7 +173,7 @@ __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G
         const double wx = __ldg(L.wx + o), wy = __ldg(L.wy + o), wl = __ldg(L.wl + o);
 #pragma unroll
         for (int d = 0; d < N; d++) {
-            const FDesc D = desc3<FORM, MD, FULL>(d);
+            const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
             const double x = mirror_value(F.p[D.f][pj], D.cls, code);
             if (D.gx >= 0) sx[d] = sx[d] + x * wx;
             if (D.gy >= 0) sy[d] = sy[d] + x * wy;
@@ -171,7 +183,7 @@ __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G
     // the x-y sums in sum form; the Laplacians keep theirs for the z part
 #pragma unroll
     for (int d = 0; d < N; d++) {
-        const FDesc D = desc3<FORM, MD, FULL>(d);
+        const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
         const double p = F.p[D.f][k];
         if (D.gx >= 0) G[(size_t)D.gx * n + k] = sx[d] - p * L.gsx[i];
         if (D.gy >= 0) G[(size_t)D.gy * n + k] = sy[d] - p * L.gsy[i];
@@ -186,7 +198,7 @@ __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G
         const double cg = L.fdg[m], cl = L.fdl[m];
 #pragma unroll
         for (int d = 0; d < N; d++) {
-            const FDesc D = desc3<FORM, MD, FULL>(d);
+            const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
             if (D.gl < 0 && D.gz < 0) continue;
             const double fm = F.p[D.f][r];
             if (D.gl >= 0) tl[d] = tl[d] + fm * cl;
@@ -195,7 +207,7 @@ __global__ void __launch_bounds__(128) k3_derivs(Layer3 L, Fields19 F, double *G
     }
 #pragma unroll
     for (int d = 0; d < N; d++) {
-        const FDesc D = desc3<FORM, MD, FULL>(d);
+        const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
         if (D.gl >= 0) G[(size_t)D.gl * n + k] = sl[d] + tl[d];
         if (D.gz >= 0) G[(size_t)D.gz * n + k] = tg[d];
     }
@@ -262,6 +274,7 @@ struct Point3 {
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
     const double *G;                      // kG3 derivative arrays
+    const double *fen;                    // FENE-P function of the direct form, or null
     int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
     double *out[19];
@@ -464,7 +477,17 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             fvv = fvv + K.coef_polymeric * ((gcxy1 + gcyy2) + gcyz3);
             fvw = fvw + K.coef_polymeric * ((gcxz1 + gcyz2) + gczz3);
         }
-        if (kDi || kLc) {
+        if (kDi && P.fen) {  // FENE-P, the quotient rule (rhs_di.F90:234-245)
+            const double f1 = P.fen[k], g0 = g(PG0), g1 = g(PG0 + 1), g2 = g(PG0 + 2);
+            const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
+                         czz = P.in[12][k];
+            fvu = fvu + K.coef_polymeric * (((((g(CG0 + 0) * f1 + cxx * g0) + g(CG0 + 3 + 1) * f1) + cxy * g1) +
+                                             g(CG0 + 9 + 2) * f1) + cxz * g2);
+            fvv = fvv + K.coef_polymeric * (((((g(CG0 + 3 + 0) * f1 + cxy * g0) + g(CG0 + 6 + 1) * f1) + cyy * g1) +
+                                             g(CG0 + 12 + 2) * f1) + cyz * g2);
+            fvw = fvw + K.coef_polymeric * (((((g(CG0 + 9 + 0) * f1 + cxz * g0) + g(CG0 + 12 + 1) * f1) + cyz * g1) +
+                                             g(CG0 + 15 + 2) * f1) + czz * g2);
+        } else if (kDi || kLc) {
             fvu = fvu + K.coef_polymeric * ((g(CG0 + 0) + g(CG0 + 3 + 1)) + g(CG0 + 9 + 2));
             fvv = fvv + K.coef_polymeric * ((g(CG0 + 3 + 0) + g(CG0 + 6 + 1)) + g(CG0 + 12 + 2));
             fvw = fvw + K.coef_polymeric * ((g(CG0 + 9 + 0) + g(CG0 + 12 + 1)) + g(CG0 + 15 + 2));
@@ -588,9 +611,16 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             const double uczz = ((2.0 * wx) * cxz + (2.0 * wy) * cyz) + (2.0 * wz) * czz;
             const double ucxz = (((((ux * cxz + uy * cyz) + uz * czz) + wx * cxx) + wy * cxy) + wz * cxz);
             const double ucyz = (((((vx * cxz + vy * cyz) + vz * czz) + wx * cxy) + wy * cyy) + wz * cyz);
-            const double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
-            const double sxx = fr * (cxx - 1.0), sxy = fr * cxy, syy = fr * (cyy - 1.0);
-            const double sxz = fr * cxz, syz = fr * cyz, szz = fr * (czz - 1.0);
+            double sxx, sxy, syy, sxz, syz, szz;
+            if (P.fen) {  // FENE-P relaxation, rhs_di.F90:454-464
+                const double fr = -P.fen[k], la = K.lambda;
+                sxx = (fr * cxx + 1.0) / la; sxy = (fr * cxy) / la; syy = (fr * cyy + 1.0) / la;
+                szz = (fr * czz + 1.0) / la; sxz = (fr * cxz) / la; syz = (fr * cyz) / la;
+            } else {
+                const double fr = -(((1.0 - K.epsPTT * 2.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+                sxx = fr * (cxx - 1.0); sxy = fr * cxy; syy = fr * (cyy - 1.0);
+                sxz = fr * cxz; syz = fr * cyz; szz = fr * (czz - 1.0);
+            }
             const double Md = K.Mdiff;
             auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
             r[4] = ((ad[0] + ucxx) + sxx) + Md * lc(0);
@@ -695,7 +725,7 @@ __global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, 
 }
 
 // End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
-__global__ void k3_finalize(size_t n, Fields19 F, int chl, int lc, DevScalars *sc, int vpid) {
+__global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         const double r = F.p[0][k] - sc->dro;
@@ -790,7 +820,7 @@ __global__ void k3_fill(size_t n, double v, double *out) {
 }
 // the Cholesky or log-conformation state from the given c: psi from c, then c from psi
 // (setup_flow.F90:86-117)
-__global__ void k3_psi_from_c(size_t n, Fields19 F, int lc) {
+__global__ void k3_psi_from_c(size_t n, Fields3 F, int lc) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double c[6], p[6];
@@ -883,13 +913,23 @@ Layer3 layer3(const Handle *H) {
 inline size_t n3(const Handle *H) { return (size_t)H->npfb * H->nz; }
 inline unsigned nblk(size_t n) { return (unsigned)((n + 127) / 128); }
 
+// FENE-P function of every node-layer (rhs_di.F90:201-203), into the staging array
+__global__ void k3_fenep(unsigned n, const double *cxx, const double *cyy, const double *czz, double L2, double *f) {
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) f[k] = (L2 - 3.0) / (L2 - ((cxx[k] + cyy[k]) + czz[k]));
+}
+
 // all the derivatives the right-hand side reads, of buffer b
-template <int FORM, bool MD, bool FULL>
+template <int FORM, bool MD, bool FULL, bool FEN = false>
 int derivs3_launch(Handle *H, int b) {
     const size_t n = n3(H);
-    Fields19 F;
+    Fields3 F{};
     for (int q = 0; q < 19; q++) F.p[q] = H->f3[b][q];
-    k3_derivs<FORM, MD, FULL><<<nblk(n), 128, 0, H->stream>>>(layer3(H), F, H->g3);
+    if (FEN) {
+        k3_fenep<<<nblk(n), 128, 0, H->stream>>>((unsigned)n, H->f3[b][7], H->f3[b][9], H->f3[b][12], H->cfg.fenep_l2, H->tmp3);
+        F.p[19] = H->tmp3;
+    }
+    k3_derivs<FORM, MD, FULL, FEN><<<nblk(n), 128, 0, H->stream>>>(layer3(H), F, H->g3);
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -897,6 +937,13 @@ int derivs3(Handle *H, int b) {
     const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0;
     switch (H->cfg.form) {
     case SUNSET_FORM_DI:
+        if (H->cfg.fenep) {
+            if (md)
+                return full ? derivs3_launch<SUNSET_FORM_DI, true, true, true>(H, b)
+                            : derivs3_launch<SUNSET_FORM_DI, true, false, true>(H, b);
+            return full ? derivs3_launch<SUNSET_FORM_DI, false, true, true>(H, b)
+                        : derivs3_launch<SUNSET_FORM_DI, false, false, true>(H, b);
+        }
         if (md) return full ? derivs3_launch<SUNSET_FORM_DI, true, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, true, false>(H, b);
         return full ? derivs3_launch<SUNSET_FORM_DI, false, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, false, false>(H, b);
     case SUNSET_FORM_CHL:
@@ -918,6 +965,7 @@ Point3 point3(Handle *H, int b, int stage) {
     P.md = H->cfg.Mdiff != 0.0;
     P.py = H->py;
     P.G = H->g3;
+    P.fen = (H->cfg.form == SUNSET_FORM_DI && H->cfg.fenep) ? H->tmp3 : nullptr;
     for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
         P.out[f] = H->f3[b ^ 1][f];
@@ -957,7 +1005,8 @@ int tstep3_launch(Handle *H, int b, int pid) {
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
     if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
-    if (H->cfg.fenep) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers sPTT / Oldroyd-B, not FENE-P");
+    if (H->cfg.fenep && H->cfg.form != SUNSET_FORM_DI)
+        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers FENE-P with the direct form");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
     if (H->cfg.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero");
     const int ncfd = H->cfg.forder + 1;
@@ -1028,7 +1077,7 @@ int state3_set(Handle *H, const double *const *fields10) {
     }
     k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
     if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
-        Fields19 F19;
+        Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = f[q];
         k3_psi_from_c<<<nblk(n), 128, 0, st>>>(n, F19, H->cfg.form == SUNSET_FORM_LC);
     }
@@ -1115,7 +1164,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         }
         k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
         k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
-        Fields19 F19;
+        Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
         k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->dsc, H->cfg.vpid);
         SUNSET_CUDA(H, cudaGetLastError());

@@ -15,7 +15,10 @@ Reference behaviour restated (and followed by the device):
 * rhs_lc.F90 (log-conformation) with the dim3 terms: the 3x3 eigen-decomposition of c
   (conf_transforms.F90:218-397, closed form with acos and cos, so device and CPU agree to
   rounding rather than bit for bit), the rotation rates and the 3-D transforms;
-* step.F90 with the dim3 error norms (row, xz, yz) and set_tstep with |u| including w.
+* step.F90 with the dim3 error norms (row, xz, yz) and set_tstep with |u| including w;
+* FENE-P with the direct form (rhs_di.F90:198-245, 454-464): the function
+  f = (L^2 - 3)/(L^2 - tr c) at every node, its 3-D gradient, the quotient-rule polymer force
+  and the FENE-P relaxation.  FENE-P with the Cholesky form is outside the 3-D path and refused.
 
 Tolerances as in the 2-D parity tests: state and right-hand sides within 1e-10 of their
 terms, fields after 50 steps within 1e-8 (the mass correction and the reductions are summed in
@@ -45,6 +48,9 @@ CASES = {
     "chl-o6-mdiff-ysym": ("periodic-lc-o6-262k", 20, 0.6, (2, 2), {"form": "chl", "Mdiff": 1e-3}),
     "lc-o6": ("periodic-lc-o6-262k", 20, 0.5, (1, 1), {}),
     "lc-o8-oldroyd-ysym": ("periodic-chl-o8-1m", 20, 0.5, (2, 2), {"form": "lc", "epsPTT": 0.0}),
+    "di-o4-fenep": ("periodic-di-o4-16k", 24, 1.0, (1, 1), {"fenep": True, "fenep_l2": 30.0}),
+    "di-o6-fenep-mdiff-ysym": ("periodic-lc-o6-262k", 20, 0.6, (2, 2),
+                               {"form": "di", "fenep": True, "fenep_l2": 50.0, "Mdiff": 1e-3}),
 }
 
 
@@ -143,3 +149,15 @@ def test_steps(pair):
         e = float(np.abs(sg[k] - sr[k]).max() / max(np.abs(sr[k]).max(), 1e-300))
         assert e <= F_TOL, (k, e)
     np.testing.assert_allclose(gpu.time()["dt"], ref.time()["dt"], rtol=1e-10)
+
+
+def test_fenep_scope():
+    """FENE-P in 3-D covers the direct form; the Cholesky form is refused with a scope error."""
+    wl = dataclasses.replace(WORKLOADS["periodic-chl-o8-1m"], nside=16)
+    ns = wl.nodes()
+    kw = dict(wl.params(), fenep=True, fenep_l2=30.0)
+    gpu = labfm.Sunset(**kw)
+    gpu.build_domain(ns)
+    with pytest.raises(labfm.SunsetError, match="FENE-P"):
+        gpu.set_layers(0.5)
+    gpu.close()

@@ -387,15 +387,19 @@ def test_adapt_stencils_invariants():
         assert lap.max() < 10.0
 
 
-@pytest.mark.parametrize("form, eps", [("di", 0.25), ("chl", 0.25), ("lc", 0.0), ("newt", 0.0)])
-def test_3d_reduces_to_2d(form, eps):
+@pytest.mark.parametrize("form, eps, fenep", [("di", 0.25, False), ("chl", 0.25, False), ("lc", 0.0, False),
+                                              ("newt", 0.0, False), ("di", 0.0, True)])
+def test_3d_reduces_to_2d(form, eps, fenep):
     """3-D restatement, known answer: with w = 0, c_xz = c_yz = 0, c_zz = 1 and fields that do
     not vary in z, every layer's right-hand side is the 2-D one (the z stencils see constants;
     rho w, c_xz and c_yz stay at rest).  The log-conformation form takes eps = 0: its 3-D sPTT
-    trace includes c_zz, the 2-D one does not (rhs_lc.F90:451-456)."""
+    trace includes c_zz, the 2-D one does not (rhs_lc.F90:451-456).  FENE-P (direct form): the
+    function f and its gradient enter the momentum and the relaxation alike in 2-D and 3-D
+    (rhs_di.F90:198-245, 454-464)."""
     wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16, form=form, epsPTT=eps)
     ns = wl.nodes()
-    o = O.for_workload(wl, ns, kolmogorov_forcing=0).setup()
+    extra = dict(fenep=True, fenep_l2=30.0) if fenep else {}
+    o = O.for_workload(wl, ns, kolmogorov_forcing=0, **extra).setup()
     o3 = O.Oracle3(o, 0.4)
     nl = o3.nl
     x, y = ns.x, ns.y
@@ -409,7 +413,7 @@ def test_3d_reduces_to_2d(form, eps):
     o3.set_state(T(st["ro"]), T(st["u"]), T(st["v"]), zero, T(st["cxx"]), T(st["cxy"]), T(st["cyy"]), zero, zero,
                  np.ones(o3.n))
     r3 = o3.rhs()
-    keys = ["ro", "rou", "rov"] + ([] if form == "newt" else ["xx", "xy", "yy"])
+    keys = ["ro", "rou", "rov"] + ([] if form == "newt" else ["xx", "xy", "yy"]) + (["zz"] if fenep else [])
     for k in keys:
         scale = max(np.abs(r2[k]).max(), 1.0)
         e = np.abs(r3[k].reshape(o3.nz, nl) - r2[k][None, :]).max() / scale
