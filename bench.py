@@ -487,7 +487,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_stage (one RK stage: stencils + rhs + update)",
                 "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms, "peak_source": peak_kind,
-                "method": f"CUDA events around each of the 4 stage launches of {roof_steps} steps"}
+                "method": f"CUDA events around the 4 back-to-back stage launches of each of {roof_steps} steps, / 4"}
 
     # end to end through the C-ABI with host buffers: per step, copy the evolved fields in
     # from pinned host memory, run the step, copy them back

@@ -215,9 +215,10 @@ int sunset_save_checkpoint(SunsetHandle *h, void *buffer, size_t bytes);
 int sunset_load_checkpoint(SunsetHandle *h, const void *buffer, size_t bytes);
 
 /* Stage-kernel timing: runs `reps` fixed-dt steps at the current dt, launched kernel by
-   kernel (not as a graph) with CUDA events on the handle's stream around each RK stage
-   launch, and returns the mean stage-kernel time per launch in ms and its algorithmic
-   bytes per launch.  Advances the state by `reps` steps. */
+   kernel (not as a graph) with CUDA events on the handle's stream before the first and after
+   the last of each step's four RK stage launches (which run back to back), and returns the
+   mean stage-kernel time per launch in ms and its algorithmic bytes per launch.  Advances the
+   state by `reps` steps. */
 int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
                              double *bytes_per_launch);
 

@@ -199,6 +199,15 @@ struct LinkRing {
 #define SUNSET_RING_MIXED 4
 #endif
 __host__ __device__ constexpr int ring_depth(bool mx) { return mx ? SUNSET_RING_MIXED : SUNSET_RING_FP64; }
+// The filter streams one weight a link (20 bytes a thread and slot in FP64, 12 in FP32), so its
+// ring runs deeper for the same shared memory.
+#ifndef SUNSET_FILTER_RING_FP64
+#define SUNSET_FILTER_RING_FP64 4
+#endif
+#ifndef SUNSET_FILTER_RING_MIXED
+#define SUNSET_FILTER_RING_MIXED 8
+#endif
+__host__ __device__ constexpr int filter_ring_depth(bool mx) { return mx ? SUNSET_FILTER_RING_MIXED : SUNSET_FILTER_RING_FP64; }
 
 // Doubles of the shared-memory halo, rounded up so the ring after it is 16-byte aligned.
 __host__ __device__ inline size_t halo_doubles(int ng, int hmax) { return ((size_t)ng * hmax + 1) & ~(size_t)1; }
@@ -633,7 +642,7 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
     const Fields &F = A.in;
     const int i = blockIdx.x * kTile + threadIdx.x;
     const bool live = (i >> 5) < cK.nslices;
-    LinkRing<MX, 1, ring_depth(MX)> R;
+    LinkRing<MX, 1, filter_ring_depth(MX)> R;
     if constexpr (MX) R.src[0] = reinterpret_cast<const float2 *>(A.wh32);
     else R.src[0] = reinterpret_cast<const double2 *>(A.wh);
     R.init(smem + halo_doubles(nf, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
@@ -1180,7 +1189,8 @@ int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     const bool cf = FORM == SUNSET_FORM_CHL && H->cfg.fenep;  // Cholesky FENE-P: psizz and the conversions
     const int nf = (FORM == SUNSET_FORM_DI || cf) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
     const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) +
-                        (mx ? LinkRing<true, 1, ring_depth(true)>::bytes() : LinkRing<false, 1, ring_depth(false)>::bytes());
+                        (mx ? LinkRing<true, 1, filter_ring_depth(true)>::bytes()
+                            : LinkRing<false, 1, filter_ring_depth(false)>::bytes());
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
     if (cf) {
         if (mx) k_filter<FORM, true, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
@@ -1192,8 +1202,9 @@ int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     return 0;
 }
 
-// The kernels of one step.  stage_ev (optional, 8 events): recorded before and after each
-// of the four RK stage launches, for timing the stage kernel inside a real step sequence.
+// The kernels of one step.  stage_ev (optional, 2 events): recorded before the first and
+// after the last of the four RK stage launches, which run back to back on the stream, for
+// timing the stage kernel inside a real step sequence.
 template <int FORM>
 int launch_step_kernels(Handle *H, int from, int pid, cudaEvent_t *stage_ev) {
     const int TB = 128;
@@ -1203,9 +1214,9 @@ int launch_step_kernels(Handle *H, int from, int pid, cudaEvent_t *stage_ev) {
     int b = from;
     for (int s = 0; s < 4; s++) {
         StageArgs A = make_args(H, b, s, true);
-        if (stage_ev) SUNSET_CUDA(H, cudaEventRecord(stage_ev[2 * s], st));
+        if (stage_ev && s == 0) SUNSET_CUDA(H, cudaEventRecord(stage_ev[0], st));
         if (int rc = launch_stage_any(H, A, mx)) return rc;
-        if (stage_ev) SUNSET_CUDA(H, cudaEventRecord(stage_ev[2 * s + 1], st));
+        if (stage_ev && s == 3) SUNSET_CUDA(H, cudaEventRecord(stage_ev[1], st));
         b ^= 1;
     }
     StageArgs F = make_args(H, b, 5, true);
@@ -1427,17 +1438,17 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     if (rc) return rc;
     if (reps < 1) reps = 1;
     const bool mx = is_mx(H);
-    std::vector<cudaEvent_t> ev(8 * (size_t)reps);
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps);
     for (auto &e : ev) SUNSET_CUDA(H, cudaEventCreate(&e));
     for (int r = 0; r < reps; r++) {
-        if ((rc = launch_step(H, H->cur, 0, ev.data() + 8 * r))) break;
+        if ((rc = launch_step(H, H->cur, 0, ev.data() + 2 * r))) break;
         H->cur ^= 1;
     }
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
-    double tot = 0.0;
-    for (int k = 0; k < 4 * reps && !rc; k++) {
+    double tot = 0.0;  // the four stage launches of each step, back to back
+    for (int r = 0; r < reps && !rc; r++) {
         float t = 0.f;
-        SUNSET_CUDA(H, cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]));
+        SUNSET_CUDA(H, cudaEventElapsedTime(&t, ev[2 * r], ev[2 * r + 1]));
         tot += t;
     }
     for (auto &e : ev) cudaEventDestroy(e);
