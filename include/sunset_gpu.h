@@ -218,7 +218,8 @@ int sunset_load_checkpoint(SunsetHandle *h, const void *buffer, size_t bytes);
    kernel (not as a graph) with CUDA events on the handle's stream before the first and after
    the last of each step's four RK stage launches (which run back to back), and returns the
    mean stage-kernel time per launch in ms and its algorithmic bytes per launch.  Advances the
-   state by `reps` steps. */
+   state by `reps` steps.  On a 3-D handle it times the derivative gather of each stage
+   (events around each launch) at the current dt instead. */
 int sunset_time_stage_kernel(SunsetHandle *h, int reps, double *ms_per_launch,
                              double *bytes_per_launch);
 

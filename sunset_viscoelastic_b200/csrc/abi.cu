@@ -931,8 +931,13 @@ int sunset_load_checkpoint(SunsetHandle *sh, const void *buffer, size_t bytes) {
 int sunset_time_stage_kernel(SunsetHandle *sh, int reps, double *ms_per_launch, double *bytes_per_launch) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (reps <= 0 || !ms_per_launch || !bytes_per_launch) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
+    if (H->nz > 0) {  // 3-D: the derivative gather k3_derivs
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        if (int rc = time3_derivs(H, reps, ms_per_launch, bytes_per_launch)) return rc;
+        return check_err_flag(H);
+    }
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     return time_stage_kernel(H, reps, ms_per_launch, bytes_per_launch);
 }
 

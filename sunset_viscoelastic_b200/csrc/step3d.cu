@@ -1127,7 +1127,7 @@ int rhs3_calc(Handle *H, double *out10) {
 int tstep3(Handle *H) { return tstep3_launch(H, H->cur3, 0); }
 
 // mode 0: fixed dt; 1: set_tstep + set_tstep_PID before each step (sunset.F90:82-83)
-int step3_run(Handle *H, double dt, int nsteps, int mode) {
+int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
     const size_t n = n3(H);
     cudaStream_t st = H->stream;
     const Layer3 L = layer3(H);
@@ -1140,7 +1140,9 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         }
         int b = H->cur3;
         for (int stage = 0; stage < 4; stage++) {
+            if (ev) SUNSET_CUDA(H, cudaEventRecord(ev[8 * s + 2 * stage], st));
             if (int rc = derivs3(H, b)) return rc;
+            if (ev) SUNSET_CUDA(H, cudaEventRecord(ev[8 * s + 2 * stage + 1], st));
             Point3 P = point3(H, b, stage);
             if (int rc = point3_launch(H, P, st)) return rc;
             b ^= 1;
@@ -1171,6 +1173,71 @@ int step3_run(Handle *H, double dt, int nsteps, int mode) {
         H->cur3 = b;
     }
     return tstep3_launch(H, H->cur3, 0);
+}
+
+
+// fields read and derivative arrays written by one k3_derivs launch of the handle's form
+template <int FORM, bool MD, bool FULL, bool FEN = false>
+void derivs3_io(int &nf, int &ng) {
+    nf = ndesc3<FORM, MD, FEN>();
+    ng = 0;
+    for (int d = 0; d < nf; d++) {
+        const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
+        ng += (D.gx >= 0) + (D.gy >= 0) + (D.gl >= 0) + (D.gz >= 0);
+    }
+}
+static void derivs3_counts(const Handle *H, int &nf, int &ng) {
+    const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0, fen = H->cfg.fenep != 0;
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI:
+        if (fen) {
+            if (md) full ? derivs3_io<SUNSET_FORM_DI, true, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, true, false, true>(nf, ng);
+            else full ? derivs3_io<SUNSET_FORM_DI, false, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, false, false, true>(nf, ng);
+        } else if (md) {
+            full ? derivs3_io<SUNSET_FORM_DI, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, true, false>(nf, ng);
+        } else {
+            full ? derivs3_io<SUNSET_FORM_DI, false, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, false, false>(nf, ng);
+        }
+        break;
+    case SUNSET_FORM_CHL:
+        md ? derivs3_io<SUNSET_FORM_CHL, true, false>(nf, ng) : derivs3_io<SUNSET_FORM_CHL, false, false>(nf, ng);
+        break;
+    case SUNSET_FORM_LC: derivs3_io<SUNSET_FORM_LC, false, false>(nf, ng); break;
+    default: derivs3_io<SUNSET_FORM_NEWT, false, false>(nf, ng); break;
+    }
+}
+
+int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
+    if (reps < 1) reps = 1;
+    DevScalars s;
+    SUNSET_CUDA(H, cudaMemcpy(&s, H->dsc, sizeof(s), cudaMemcpyDeviceToHost));
+    std::vector<cudaEvent_t> ev(8 * (size_t)reps);
+    for (auto &e : ev) SUNSET_CUDA(H, cudaEventCreate(&e));
+    int rc = step3_run(H, s.dt, reps, 0, ev.data());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    double tot = 0.0;
+    for (int k = 0; k < 4 * reps && !rc; k++) {
+        float t = 0.f;
+        SUNSET_CUDA(H, cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]));
+        tot += t;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    *ms = tot / (4.0 * reps);
+    // Algorithmic bytes of one launch: every gathered field read once and every derivative
+    // array written once (8 bytes a node-layer each), the layer's small links once (a 4-byte
+    // index and three 8-byte weights; all layers share them) and the three stencil sums of
+    // each node of the layer.
+    int nf = 0, ng = 0;
+    derivs3_counts(H, nf, ng);
+    long long links = 0;
+    {
+        std::vector<int> cs(H->npfb);
+        SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int c : cs) links += c;
+    }
+    *bytes = (double)n3(H) * 8.0 * (nf + ng) + (double)links * 28.0 + (double)H->npfb * 24.0;
+    return 0;
 }
 
 }  // namespace sunset
