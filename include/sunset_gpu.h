@@ -30,6 +30,7 @@ extern "C" {
 #define SUNSET_ERR_SCOPE -4        /* configuration outside the implemented path */
 #define SUNSET_ERR_NONFINITE -5    /* NaN/Inf in the time-step error norm */
 #define SUNSET_ERR_NOMEM -6        /* device allocation failed */
+#define SUNSET_ERR_ILLCOND -7      /* a moment matrix's condition number exceeds cond_max */
 
 /* Conformation formulation (reference Makefile:71-90 ceform -> -Ddi/-Dchl/-Dlc). */
 #define SUNSET_FORM_DI 0
@@ -66,6 +67,12 @@ typedef struct {
     double u_inflow_start, u_inflow_end, ramp_time;
     int vpid;               /* -Dvpid: after every step a PID controller drives the volume-mean x
                                velocity through driving_force(1) (statistics.F90:214-303) */
+    double cond_max;        /* > 0: sunset_calc_labf_weights fails with SUNSET_ERR_ILLCOND when any
+                               node's moment matrix has sigma_max/sigma_min above it; 0: such
+                               nodes (above 1e12) are only counted, see sunset_get_conditioning.
+                               The reference inverts every nonzero sigma (svdlib.F90:283-293) */
+    int svd_max_sweeps;     /* QR sweeps per singular value before SUNSET_ERR_SVD; 0: the
+                               reference's 30 (svdlib.F90:219-222) */
 } SunsetConfig;
 
 typedef struct SunsetHandle SunsetHandle;
@@ -78,6 +85,10 @@ int sunset_create(const SunsetConfig *cfg, SunsetHandle **out);
 void sunset_destroy(SunsetHandle *h);
 const char *sunset_last_error(const SunsetHandle *h);
 int sunset_version(void);
+/* The SASS target the library's kernels were built for, as the CUDA runtime reports it for
+   one of them on `device` (cudaFuncGetAttributes binaryVersion: 100 for sm_100a), or a
+   negative SUNSET_ERR_* code.  No reference counterpart. */
+int sunset_kernel_binary_version(int device);
 
 /* setup_domain.F90:80-374 build_domain (IPART rows -> nodes, 4 FD rows per boundary node)
    + mirror_boundaries.F90:34-261 create_mirror_particles, as device-resident ghost points.
@@ -102,6 +113,12 @@ int sunset_adapt_stencils(SunsetHandle *h);
 int sunset_get_lengths(SunsetHandle *h, double *h_out, double *h_small_out);
 /* labf.F90:34-231 calc_labf_weights (+ calc_filter_weights :233-394). */
 int sunset_calc_labf_weights(SunsetHandle *h);
+/* Conditioning of the weight solves of sunset_calc_labf_weights (labf.F90:153-180, 325-388):
+   sigma_max/sigma_min of each interior node's derivative and filter moment matrix, npfb each in
+   reference order (0 for boundary nodes, which that call does not build; any pointer may be
+   NULL), the worst value, and the number of nodes above cond_max (1e12 when cond_max is 0).
+   The reference has no such output: it solves whatever it is given. */
+int sunset_get_conditioning(SunsetHandle *h, double *cond_deriv, double *cond_filter, double *worst, int *n_ill);
 /* labf.F90:505-1039 calc_boundary_weights: prunes the links of boundary nodes to their own
    layer and FD children, then FD normal and 1-D LABFM tangential operators for boundary
    nodes and FD rows 1-2, curvature and frame rotations.  A no-op without boundary nodes;
@@ -252,7 +269,8 @@ int sunset_adjoint_apply_D(SunsetHandle *h, int which, const double *gbar, doubl
    4,194,304 nodes (256 KB per GPU, held until the process exits); larger npfb returns
    SUNSET_ERR_SCOPE.  The first call on a device looks the array's address up and should
    come before any stream capture.  Work is enqueued on `stream` (NULL: the default
-   stream).  All calls share the array, so calls that overlap on the GPU race. */
+   stream); the calling thread's current device is left as it was.  All calls share the
+   array, so calls that overlap on the GPU race. */
 int sunset_kinetic_energy_noalloc(int device, int npfb, const double *ro, const double *u, const double *v,
                                   const double *vol, double *out, void *stream);
 

@@ -62,6 +62,7 @@ def lib():
         L.or_get_nodes.argtypes = [P, dp, dp, dp, dp, dp, ip, ip, ip]
         L.or_get_neighbours.argtypes = [P, ip, ip, ip]
         L.or_get_weights.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
+        L.or_get_conditioning.argtypes = [P, dp, dp]
         L.or_set_neighbours_weights.argtypes = [P, C.c_int, ip, ip, ip, dp, dp, dp, dp, dp, dp, dp]
         for name in ["or_calc_gradient", "or_calc_laplacian", "or_calc_filtered_var", "or_calc_filter_term"]:
             getattr(L, name).argtypes = [P, dp, dp]
@@ -222,6 +223,13 @@ class Oracle:
         return dict(w_grad=wg.reshape(npfb, nplink, 2), w_lap=wl.reshape(npfb, nplink),
                     w_hyp=wh.reshape(npfb, nplink), w_grad_sum=gs.reshape(npfb, 2), w_lap_sum=ls,
                     w_hyp_sum=hs, vol=vol)
+
+    def conditioning(self):
+        """sigma_max / sigma_min of each interior node's derivative and filter moment matrix."""
+        _, npfb, _, _ = self.sizes()
+        cd, cf = np.zeros(npfb), np.zeros(npfb)
+        self._chk(self.L.or_get_conditioning(self.h, cd, cf))
+        return cd, cf
 
     def set_neighbours_weights(self, cnt, cs, links, w):
         npfb, nplink = links.shape

@@ -86,6 +86,7 @@ struct OrSim {
     /* weights */
     double *w_grad, *w_lap, *w_hyp, *w_grad_sum, *w_lap_sum, *w_hyp_sum, *vol;
     double *wb_grad2, *wb_grad2_sum; /* boundary second derivatives [jj][k][3] */
+    double *cond_d, *cond_f; /* condition numbers of the derivative and filter moment matrices */
     int have_weights;
     /* fields (np) */
     double *ro, *rou, *rov, *row, *u, *v, *w, *p;
@@ -168,6 +169,7 @@ static void free_links(OrSim *s) {
     FREE(s->ij_count); FREE(s->ij_count_small); FREE(s->ij_link);
     FREE(s->w_grad); FREE(s->w_lap); FREE(s->w_hyp); FREE(s->w_grad_sum); FREE(s->w_lap_sum);
     FREE(s->w_hyp_sum); FREE(s->vol); FREE(s->wb_grad2); FREE(s->wb_grad2_sum);
+    FREE(s->cond_d); FREE(s->cond_f);
     s->have_weights = 0;
 }
 void or_destroy(OrSim *s) {
@@ -527,6 +529,20 @@ static int svd_factor(const double *amat, int n, SvdWork *sw) {
 }
 
 /* svdlib.F90:279-303: x = V diag(1/w) U^T b, skipping exactly-zero singular values. */
+/* 2-norm condition number sigma_max / sigma_min of the factored matrix (infinite when a
+   singular value is exactly zero).  The reference inverts every nonzero sigma however small
+   (svdlib.F90:283-293); this is what the library reports so that a near-singular moment
+   matrix does not pass silently. */
+static double svd_cond(const SvdWork *sw, int n) {
+    double smax = 0.0, smin = INFINITY;
+    for (int j = 0; j < n; j++) {
+        const double w = fabs(sw->w[j]);
+        smax = w > smax ? w : smax;
+        smin = w < smin ? w : smin;
+    }
+    return smin > 0.0 ? smax / smin : INFINITY;
+}
+
 static void svd_apply(const SvdWork *sw, int n, double *bvec) {
     const double *umat = sw->u, *vmat = sw->v, *W = sw->w - 1;
     double *tmp = sw->tmp - 1, *b = bvec - 1, s;
@@ -889,7 +905,9 @@ int or_get_neighbours(OrSim *s, int *ij_count, int *ij_count_small, int *ij_link
  * ------------------------------------------------------------------------------------- */
 static void alloc_weights(OrSim *s) {
     size_t nn = (size_t)s->npfb * s->nplink;
-    FREE(s->w_grad); FREE(s->w_lap); FREE(s->w_hyp); FREE(s->vol);
+    FREE(s->w_grad); FREE(s->w_lap); FREE(s->w_hyp); FREE(s->vol); FREE(s->cond_d); FREE(s->cond_f);
+    s->cond_d = (double *)xcalloc(s->npfb, sizeof(double));
+    s->cond_f = (double *)xcalloc(s->npfb, sizeof(double));
     s->w_grad = (double *)xcalloc(2 * nn, sizeof(double));
     s->w_lap = (double *)xcalloc(nn, sizeof(double));
     s->w_hyp = (double *)xcalloc(nn, sizeof(double));
@@ -943,6 +961,13 @@ static void hyp_rhs(int order, double *b, int n) {
     else { b[54] = 1.0; b[56] = 5.0; b[58] = 10.0; b[60] = 10.0; b[62] = 5.0; b[64] = 1.0; }
 }
 
+int or_get_conditioning(OrSim *s, double *cond_deriv, double *cond_filter) {
+    if (!s->cond_d) return fail(s, "weights not built");
+    if (cond_deriv) memcpy(cond_deriv, s->cond_d, sizeof(double) * s->npfb);
+    if (cond_filter) memcpy(cond_filter, s->cond_f, sizeof(double) * s->npfb);
+    return 0;
+}
+
 int or_calc_labf_weights(OrSim *s) {
     if (!s->ij_count) return fail(s, "neighbours not built");
     const int forder = s->cfg.forder, morder = s->cfg.morder;
@@ -978,6 +1003,7 @@ int or_calc_labf_weights(OrSim *s) {
                 bad = i;
                 continue;
             }
+            s->cond_d[i] = svd_cond(&sw, nG);
             svd_apply(&sw, nG, bx);
             svd_apply(&sw, nG, by);
             svd_apply(&sw, nG, bxx);
@@ -1011,6 +1037,7 @@ int or_calc_labf_weights(OrSim *s) {
                 bad = i;
                 continue;
             }
+            s->cond_f[i] = svd_cond(&sw, nF);
             svd_apply(&sw, nF, bh);
             for (int k = 0; k < s->ij_count[i]; k++) {
                 int j = lk[k];

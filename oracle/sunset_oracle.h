@@ -68,6 +68,9 @@ int or_get_nodes(OrSim *s, double *x, double *y, double *h, double *h_small, dou
 int or_find_neighbours(OrSim *s);
 int or_adapt_stencils(OrSim *s);        /* labf.F90:1079-1721, then the neighbour search again */
 int or_calc_labf_weights(OrSim *s);      /* + calc_filter_weights + calc_node_volumes */
+/* sigma_max / sigma_min of each interior node's derivative and filter moment matrices as the
+   weight build factored them (npfb each; 0 for boundary nodes, infinite for a zero sigma). */
+int or_get_conditioning(OrSim *s, double *cond_deriv, double *cond_filter);
 int or_calc_boundary_weights(OrSim *s);
 int or_calc_labf_sums(OrSim *s);
 int or_filter_coefficients(OrSim *s);

@@ -107,13 +107,25 @@ int need(Handle *H, bool ok, const char *what) {
     return 0;
 }
 
+// The device error word of the step kernels: 0 = none, 1 = the time-step error norm of a
+// step was NaN or infinite (k_finalize, k3_finalize).  No other value is ever written.
 int check_err_flag(Handle *H) {
     int e = 0;
     SUNSET_CUDA(H, cudaMemcpyAsync(&e, &H->dsc->err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
-    if (e) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite time-step error norm");
+    if (e == 1) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite time-step error norm");
+    if (e) return set_err(H, SUNSET_ERR_CUDA, "unknown device error word %d", e);
     return 0;
 }
+
+// Two CUDA events destroyed with the object, so every return path releases them.
+struct EventPair {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~EventPair() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
 
 }  // namespace
 }  // namespace sunset
@@ -123,6 +135,16 @@ using namespace sunset;
 extern "C" {
 
 int sunset_version(void) { return 1; }
+
+int sunset_kernel_binary_version(int device) {
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return SUNSET_ERR_CUDA;
+    if (device != prev && cudaSetDevice(device) != cudaSuccess) return SUNSET_ERR_CUDA;
+    cudaFuncAttributes fa{};
+    const cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)k_gather);
+    if (device != prev) cudaSetDevice(prev);
+    return e == cudaSuccess ? fa.binaryVersion : SUNSET_ERR_CUDA;
+}
 
 int sunset_create(const SunsetConfig *cfg, SunsetHandle **out) {
     if (!cfg || !out) return SUNSET_ERR_ARG;
@@ -175,6 +197,30 @@ int sunset_build_domain(SunsetHandle *sh, int nrows, const int *gi, const double
     if (H->domain_ok) return set_err(H, SUNSET_ERR_ARG, "domain already built; create a new handle");
     if (nrows <= 0 || !x || !y || !node_type || !s || !bcond) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
     if (!(xmax > xmin && ymax > ymin)) return set_err(H, SUNSET_ERR_ARG, "empty domain");
+    if (!(smax > 0.0) || !std::isfinite(smax)) return set_err(H, SUNSET_ERR_ARG, "smax must be positive");
+    for (int c = 0; c < 4; c++)
+        if (bcond[c] < 0 || bcond[c] > 3) return set_err(H, SUNSET_ERR_ARG, "bcond[%d] = %d is not 0..3", c, bcond[c]);
+    // the rows of a node file (setup_domain.F90:177-199) as the reference reads them: a row the
+    // reader would misplace or a spacing the cell list cannot hold is an error here, where the
+    // reference reads on into undefined behaviour.  Positions may lie a little outside the box
+    // (the reference's own IPART does), but not outside the tripled domain its search cells
+    // cover (neighbours.F90:84-89).
+    const double lx = xmax - xmin, ly = ymax - ymin;
+    for (int r = 0; r < nrows; r++) {
+        const int t = node_type[r];
+        if (!(t == 999 || t == 998 || (t >= 0 && t <= 2)))
+            return set_err(H, SUNSET_ERR_ARG, "row %d: node type %d is not 0, 1, 2, 998 or 999", r + 1, t);
+        if (!std::isfinite(x[r]) || !std::isfinite(y[r]) || x[r] < xmin - lx || x[r] > xmax + lx || y[r] < ymin - ly ||
+            y[r] > ymax + ly)
+            return set_err(H, SUNSET_ERR_ARG, "row %d: position (%g, %g) outside the search cells", r + 1, x[r], y[r]);
+        if (!(s[r] > 0.0) || !(s[r] <= smax))
+            return set_err(H, SUNSET_ERR_ARG, "row %d: spacing %g outside (0, smax = %g]", r + 1, s[r], smax);
+        if (t <= 2) {
+            const double rnx = nx ? nx[r] : 0.0, rny = ny ? ny[r] : 0.0;
+            if (!(std::fabs(rnx * rnx + rny * rny - 1.0) < 1e-6))
+                return set_err(H, SUNSET_ERR_ARG, "row %d: boundary node without a unit normal", r + 1);
+        }
+    }
     if (int rc = set_device(H)) return rc;
     const double hovs = hovs_for(H->cfg.forder), hovs_bound = hovs_bound_for(H->cfg.forder);
     const double hos = H->cfg.h_over_s;
@@ -309,6 +355,25 @@ int sunset_calc_labf_weights(SunsetHandle *sh) {
     H->w_ok = true;
     H->bw_ok = H->nb == 0;
     H->sums_ok = H->fc_ok = false;
+    return 0;
+}
+
+int sunset_get_conditioning(SunsetHandle *sh, double *cond_deriv, double *cond_filter, double *worst, int *n_ill) {
+    if (!sh) return SUNSET_ERR_ARG;
+    Handle *H = &sh->H;
+    if (int rc = need(H, H->cond_ok, "sunset_calc_labf_weights")) return rc;
+    if (int rc = set_device(H)) return rc;
+    const int n = H->npfb;
+    std::vector<double> t(n);
+    double *dst[2] = {cond_deriv, cond_filter};
+    const double *src[2] = {H->cond_d, H->cond_f};
+    for (int a = 0; a < 2; a++) {
+        if (!dst[a]) continue;
+        SUNSET_CUDA(H, cudaMemcpy(t.data(), src[a], n * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++) dst[a][H->h_perm[i]] = t[i];  // internal node i is reference node perm[i]
+    }
+    if (worst) *worst = H->cond_worst;
+    if (n_ill) *n_ill = H->cond_nill;
     return 0;
 }
 
@@ -636,17 +701,15 @@ int sunset_step_timed(SunsetHandle *sh, double dt, int nsteps, int mode, double 
         return rc;
     if (nsteps < 0 || (mode == 0 && !(dt > 0.0)) || mode < 0 || mode > 1 || !ms)
         return set_err(H, SUNSET_ERR_ARG, "bad dt/nsteps/mode");
-    cudaEvent_t e0, e1;
-    SUNSET_CUDA(H, cudaEventCreate(&e0));
-    SUNSET_CUDA(H, cudaEventCreate(&e1));
-    SUNSET_CUDA(H, cudaEventRecord(e0, H->stream));
+    EventPair ev;  // destroyed on every return path
+    SUNSET_CUDA(H, cudaEventCreate(&ev.e[0]));
+    SUNSET_CUDA(H, cudaEventCreate(&ev.e[1]));
+    SUNSET_CUDA(H, cudaEventRecord(ev.e[0], H->stream));
     int rc = H->nz > 0 ? step3_run(H, dt, nsteps, mode) : step_run(H, dt, nsteps, mode);
-    SUNSET_CUDA(H, cudaEventRecord(e1, H->stream));
-    SUNSET_CUDA(H, cudaEventSynchronize(e1));
+    SUNSET_CUDA(H, cudaEventRecord(ev.e[1], H->stream));
+    SUNSET_CUDA(H, cudaEventSynchronize(ev.e[1]));
     float t = 0.f;
-    SUNSET_CUDA(H, cudaEventElapsedTime(&t, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    SUNSET_CUDA(H, cudaEventElapsedTime(&t, ev.e[0], ev.e[1]));
     *ms = t;
     if (rc) return rc;
     return check_err_flag(H);
@@ -701,7 +764,9 @@ int sunset_run_host(SunsetHandle *sh, const double *state_in, double dt, int nst
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "sunset_run_host is 2-D only");
     if (!state_in || !state_out) return set_err(H, SUNSET_ERR_ARG, "null array");
+    if (nsteps < 0 || !(dt > 0.0)) return set_err(H, SUNSET_ERR_ARG, "bad dt/nsteps");
     const int n = H->npfb;
     // one copy each way through a 7 x npfb staging block (allocated on the first call), with
     // the permutation between reference and internal order done on the device
@@ -738,6 +803,7 @@ int sunset_adjoint_run(SunsetHandle *sh, double dt, int nsteps, int checkpoint_e
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "the adjoint is 2-D only");
     if (!J || !dJ_dparams) return set_err(H, SUNSET_ERR_ARG, "null output");
     if (!(dt > 0.0)) return set_err(H, SUNSET_ERR_ARG, "dt must be positive");
     const int n = H->npfb;
@@ -913,6 +979,7 @@ int sunset_checkpoint_size(SunsetHandle *sh, size_t *bytes) {
 int sunset_save_checkpoint(SunsetHandle *sh, void *buffer, size_t bytes) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
+    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "checkpoints hold 2-D states only");
     if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (!buffer || bytes < checkpoint_bytes(H)) return set_err(H, SUNSET_ERR_ARG, "checkpoint buffer too small");
     return checkpoint_save(H, buffer);
@@ -921,6 +988,7 @@ int sunset_save_checkpoint(SunsetHandle *sh, void *buffer, size_t bytes) {
 int sunset_load_checkpoint(SunsetHandle *sh, const void *buffer, size_t bytes) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
+    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "checkpoints hold 2-D states only");
     if (!buffer) return set_err(H, SUNSET_ERR_ARG, "null buffer");
     if (int rc = state_alloc(H)) return rc;
     if (int rc = checkpoint_load(H, buffer, bytes)) return rc;

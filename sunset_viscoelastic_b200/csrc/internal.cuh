@@ -39,6 +39,10 @@ constexpr int kTile = kTileSlices * 32;
 // per-tile partial sums live in a buffer of nodes / 128 + 1 entries
 static_assert(kTile >= 128 && kTile <= 1024, "tile of 128 to 1024 nodes");
 constexpr int kLocMask = 0x3fff;       // low 14 bits of a local link: position in the tile's halo
+// Condition number above which a moment matrix is counted as ill-conditioned when the run
+// sets no limit of its own (SunsetConfig::cond_max = 0): its weights lose about 12 of
+// FP64's 16 digits.
+constexpr double kCondWarn = 1.0e12;
 
 // RK3(2)4[2R+]C, common_parameter.F90:74-94
 #define SUNSET_RK_A21 (11847461282814.0 / 36547543011857.0)
@@ -192,6 +196,12 @@ struct Handle {
 
     // ---- weights (SELL, FP64) ----
     double *wx = nullptr, *wy = nullptr, *wl = nullptr, *wh = nullptr;
+    // condition numbers of each interior node's derivative / filter moment matrix (internal
+    // order), the worst one and how many exceed the limit
+    double *cond_d = nullptr, *cond_f = nullptr;
+    double cond_worst = 0.0;
+    int cond_nill = 0;
+    bool cond_ok = false;
     double *gsx = nullptr, *gsy = nullptr, *lsum = nullptr, *hsum = nullptr, *vol = nullptr;
     // mixed precision: the weights rounded to FP32 and their stencil sums (FP64 sums of
     // the rounded weights, so sum_k w_k phi_j - phi_i sum_k w_k is exactly the
@@ -289,6 +299,7 @@ int find_neighbours_device(Handle *H);
 int build_halos(Handle *H);
 int adapt_stencils_device(Handle *H);  // labf.F90:1079-1721: new h, h_small per node
 int labf_weights_device(Handle *H);
+int conditioning_check(Handle *H);
 int boundary_prune_links(Handle *H);
 int boundary_weights_device(Handle *H);
 int upload_boundary(Handle *H, const std::vector<double> &nx, const std::vector<double> &ny,

@@ -13,7 +13,13 @@
 // given it would fault or, where the GPU can reach host memory, read the wrong memory.
 // The device address is looked up once per device with cudaGetSymbolAddress, on the
 // first call made on that device (so that first call should come before any stream
-// capture), and passed to the kernels.
+// capture), and passed to the kernels.  Every call shares the array: two calls whose
+// kernels overlap on the GPU (different streams, or different host threads) race on it.
+//
+// The call leaves the calling thread's current device as it found it, and reports only
+// its own launch errors: each kernel goes through cudaLaunchKernel, whose return value is
+// that launch's status, so an error the caller left pending is neither consumed nor
+// reported here.
 #include <mutex>
 
 #include "internal.cuh"
@@ -92,7 +98,13 @@ extern "C" int sunset_kinetic_energy_noalloc(int device, int npfb, const double 
     if (npfb <= 0 || !ro || !u || !v || !vol || !out) return SUNSET_ERR_ARG;
     if (npfb > kNoAllocThreads * kNoAllocMaxBlocks) return SUNSET_ERR_SCOPE;  // beyond the static scratch
     if (device < 0 || device >= kMaxDevices) return SUNSET_ERR_ARG;
-    if (cudaSetDevice(device) != cudaSuccess) return SUNSET_ERR_CUDA;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return SUNSET_ERR_CUDA;
+    struct Restore {  // the caller's current device again on every return path
+        int dev;
+        ~Restore() { cudaSetDevice(dev); }
+    } restore{prev};
+    if (device != prev && cudaSetDevice(device) != cudaSuccess) return SUNSET_ERR_CUDA;
     double *scratch;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
@@ -104,10 +116,13 @@ extern "C" int sunset_kinetic_energy_noalloc(int device, int npfb, const double 
         scratch = g_scratch[device];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int nb = (npfb + kNoAllocThreads - 1) / kNoAllocThreads;
+    int n = npfb, nb = (npfb + kNoAllocThreads - 1) / kNoAllocThreads;
     // every partial the fold reads is written by this call first: nothing has to start at zero
-    k_ke_mass_partials<<<nb, kNoAllocThreads, 0, st>>>(npfb, ro, u, v, vol, scratch);
-    k_ke_mass_fold<<<1, kNoAllocThreads, 0, st>>>(scratch, nb, out);
-    if (cudaGetLastError() != cudaSuccess) return SUNSET_ERR_CUDA;
+    void *pa[] = {&n, &ro, &u, &v, &vol, &scratch};
+    if (cudaLaunchKernel((const void *)k_ke_mass_partials, dim3(nb), dim3(kNoAllocThreads), pa, 0, st) != cudaSuccess)
+        return SUNSET_ERR_CUDA;
+    void *fa[] = {&scratch, &nb, &out};
+    if (cudaLaunchKernel((const void *)k_ke_mass_fold, dim3(1), dim3(kNoAllocThreads), fa, 0, st) != cudaSuccess)
+        return SUNSET_ERR_CUDA;
     return SUNSET_OK;
 }

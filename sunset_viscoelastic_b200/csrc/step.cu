@@ -563,7 +563,8 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
             } else {
                 double en = 0.0, al = 0.0;
                 // Cholesky FENE-P: the conformation errors scaled by the node's 1/sqrt(f)
-                // (step.F90:442-452, applied per node; see the design notes)
+                // (step.F90:442-452 scales the running maxima by each node's factor in turn;
+                // here each node's own errors are scaled before the maximum, order-free)
                 double conf_scale = 1.0;
                 if constexpr (FORM == SUNSET_FORM_CHL && FP)
                     conf_scale = 1.0 / sqrt((cK.fenep_l2 - 3.0) / (((cK.fenep_l2 - n.cxx) - n.cyy) - n.czz));
@@ -1371,12 +1372,18 @@ int step_run(Handle *H, double dt, int nsteps, int mode) {
             if (H->graph[from]) { cudaGraphExecDestroy(H->graph[from]); H->graph[from] = nullptr; }
             cudaGraph_t g;
             SUNSET_CUDA(H, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            g = nullptr;
             int lrc = launch_step(H, from, mode);
             cudaError_t ce = cudaStreamEndCapture(st, &g);
-            if (lrc) return lrc;
-            SUNSET_CUDA(H, ce);
-            SUNSET_CUDA(H, cudaGraphInstantiate(&H->graph[from], g, 0));
+            if (lrc || ce != cudaSuccess) {  // the capture ended either way: drop what it recorded
+                if (g) cudaGraphDestroy(g);
+                if (lrc) return lrc;
+                SUNSET_CUDA(H, ce);
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&H->graph[from], g, 0);
             cudaGraphDestroy(g);
+            if (ie != cudaSuccess) H->graph[from] = nullptr;
+            SUNSET_CUDA(H, ie);
             H->graph_mode[from] = mode;
         }
         SUNSET_CUDA(H, cudaGraphLaunch(H->graph[from], st));

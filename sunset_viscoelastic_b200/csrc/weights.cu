@@ -14,6 +14,8 @@
 // applied to five right-hand sides; the filter matrix (labf.F90:258-303) is the same
 // matrix whenever h == h_small, the counts agree and the order drops agree, and is then
 // not factored again.
+#include <cmath>
+
 #include "internal.cuh"
 
 namespace sunset {
@@ -129,9 +131,10 @@ __device__ __forceinline__ void wstore(double *p, double v, int lane) {
 }
 
 // svdlib.F90:37-278 on a warp.  U (in: A, out: U) and V are column-major n x n with
-// leading dimension ld; W and rv1 are 1-based.  Returns 0 or -1 (no convergence).
+// leading dimension ld; W and rv1 are 1-based.  Returns 0 or -1 (no convergence within
+// maxits QR sweeps per singular value; the reference's limit is 30).
 template <int N>
-__device__ int svd_factor_warp(double *U, double *V, double *W, double *rv1, int ld, int lane) {
+__device__ int svd_factor_warp(double *U, double *V, double *W, double *rv1, int ld, int lane, int maxits = 30) {
     const int n = N;
 #define UM(i, j) U[((j) - 1) * ld + ((i) - 1)]
 #define VM(i, j) V[((j) - 1) * ld + ((i) - 1)]
@@ -272,7 +275,7 @@ __device__ int svd_factor_warp(double *U, double *V, double *W, double *rv1, int
                 }
                 break;
             }
-            if (its == 30) return -1;
+            if (its >= maxits) return -1;
             x = W[l];
             nm = k - 1;
             y = W[nm];
@@ -358,7 +361,24 @@ struct WArgs {
     const long long *slice_ptr;
     double *wx, *wy, *wl, *wh;
     int *err;
+    int maxits;               // QR sweeps per singular value (<= 0: the reference's 30)
+    double *cond_d, *cond_f;  // per node sigma_max / sigma_min of the two moment matrices, or null
 };
+
+// 2-norm condition number of a factored matrix, sigma_max / sigma_min over W[1..N]
+// (infinite when a singular value is exactly zero).  The reference inverts every nonzero
+// sigma however small (svdlib.F90:283-293); the library reports it instead of staying
+// silent about a near-singular stencil.
+template <int N>
+__device__ __forceinline__ double svd_cond(const double *W) {
+    double smax = 0.0, smin = INFINITY;
+    for (int j = 1; j <= N; j++) {
+        const double w = fabs(W[j]);
+        smax = w > smax ? w : smax;
+        smin = w < smin ? w : smin;
+    }
+    return smin > 0.0 ? smax / smin : INFINITY;
+}
 
 __device__ __forceinline__ long long sell_off(const long long *slice_ptr, int i, int k) {
     return sell_at(slice_ptr[i >> 5], k, i & 31);
@@ -442,10 +462,13 @@ __global__ void k_labf_weights(WArgs a) {
         assemble<ORDER>(a, i, cs, hh, U, ld, X, G, lane);
         if (a.morder >= 7 && (t == 998 || t < 0)) drop_order<n>(U, ld, 27, lane);
         if (a.morder >= 5 && (t == -1 || t == -2)) drop_order<n>(U, ld, 14, lane);
-        if (svd_factor_warp<n>(U, V, W, rv1, ld, lane)) {
+        if (svd_factor_warp<n>(U, V, W, rv1, ld, lane, a.maxits > 0 ? a.maxits : 30)) {
             if (lane == 0) atomicExch(a.err, i + 1);
             continue;
         }
+        double cond_d = 0.0;
+        if (lane == 0) cond_d = svd_cond<n>(W);
+        if (lane == 0 && a.cond_d) a.cond_d[i] = cond_d;
         for (int m = lane; m < n; m += 32) {
             bx[m] = (m == 0) ? 1.0 : 0.0;
             by[m] = (m == 1) ? 1.0 : 0.0;
@@ -492,11 +515,13 @@ __global__ void k_labf_weights(WArgs a) {
             assemble<ORDER>(a, i, cnt, hf, U, ld, X, G, lane);
             if (a.forder >= 7 && (t == 998 || t < 0)) drop_order<n>(U, ld, 27, lane);
             if (a.forder >= 5 && t == -1) drop_order<n>(U, ld, 14, lane);
-            if (svd_factor_warp<n>(U, V, W, rv1, ld, lane)) {
+            if (svd_factor_warp<n>(U, V, W, rv1, ld, lane, a.maxits > 0 ? a.maxits : 30)) {
                 if (lane == 0) atomicExch(a.err, i + 1);
                 continue;
             }
+            if (lane == 0) cond_d = svd_cond<n>(W);
         }
+        if (lane == 0 && a.cond_f) a.cond_f[i] = cond_d;
         int hord = a.forder;
         if (a.forder >= 7 && (t == 998 || t < 0)) hord = 6;
         if (a.forder >= 5 && t == -1) hord = 4;
@@ -1172,6 +1197,33 @@ int adapt_stencils_device(Handle *H) {
     return 0;
 }
 
+// Condition numbers of the moment matrices the weight build factored: the worst one and the
+// number of nodes above the limit (the configured cond_max, else kCondWarn), kept in the
+// handle.  With cond_max > 0 such a node is an error; without, it is only counted.
+int conditioning_check(Handle *H) {
+    const int n = H->npfb;
+    std::vector<double> cd(n), cf(n);
+    SUNSET_CUDA(H, cudaMemcpyAsync(cd.data(), H->cond_d, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaMemcpyAsync(cf.data(), H->cond_f, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    const double lim = H->cfg.cond_max > 0.0 ? H->cfg.cond_max : kCondWarn;
+    double worst = 0.0;
+    int nill = 0, iworst = -1;
+    for (int i = 0; i < n; i++) {
+        const double c = cd[i] > cf[i] ? cd[i] : cf[i];
+        if (c > lim) nill++;
+        if (c > worst || (std::isinf(c) && iworst < 0)) { worst = c; iworst = i; }
+    }
+    H->cond_worst = worst;
+    H->cond_nill = nill;
+    H->cond_ok = true;
+    if (H->cfg.cond_max > 0.0 && nill > 0)
+        return set_err(H, SUNSET_ERR_ILLCOND,
+                       "%d nodes have moment matrices with condition number above %g (worst %.3g at reference node %d)",
+                       nill, lim, worst, iworst >= 0 ? H->h_perm[iworst] : -1);
+    return 0;
+}
+
 int labf_weights_device(Handle *H) {
     const int n = H->npfb;
     if (H->cfg.forder != H->cfg.morder)
@@ -1190,8 +1242,11 @@ int labf_weights_device(Handle *H) {
     int *derr;
     if (dalloc(H, &derr, 1)) return SUNSET_ERR_NOMEM;
     SUNSET_CUDA(H, cudaMemsetAsync(derr, 0, sizeof(int), st));
+    if (!H->cond_d && (dalloc(H, &H->cond_d, n) || dalloc(H, &H->cond_f, n))) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->cond_d, 0, n * sizeof(double), st));
+    SUNSET_CUDA(H, cudaMemsetAsync(H->cond_f, 0, n * sizeof(double), st));
     WArgs a{n, H->cfg.morder, H->cfg.forder, H->h2, H->px, H->py, H->h, H->hs, H->ntype, H->cnt, H->cnt_small,
-            H->lpt, H->slice_ptr, H->wx, H->wy, H->wl, H->wh, derr};
+            H->lpt, H->slice_ptr, H->wx, H->wy, H->wl, H->wh, derr, H->cfg.svd_max_sweeps, H->cond_d, H->cond_f};
     int rc;
     switch (H->cfg.morder) {
     case 4: rc = launch_weights<4>(H, a); break;
@@ -1206,7 +1261,7 @@ int labf_weights_device(Handle *H) {
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
     dfree(H, derr);
     if (herr) return set_err(H, SUNSET_ERR_SVD, "SVD not converging at internal node %d (svdlib.F90:219-222)", herr - 1);
-    return 0;
+    return conditioning_check(H);
 }
 
 int boundary_prune_links(Handle *H);

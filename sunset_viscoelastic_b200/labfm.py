@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import warnings
 
 import numpy as np
 
@@ -21,6 +22,8 @@ STATE_FIELDS = ["ro", "rou", "rov", "u", "v", "psixx", "psixy", "psiyy", "psizz"
 RHS_FIELDS = ["ro", "rou", "rov", "xx", "xy", "yy", "zz"]
 # columns of a fields dump (output.F90:299-301)
 DUMP_COLUMNS = ["ro_minus_rho_char", "u", "v", "vort", "qcrit", "alpha", "cxx", "cxy", "cyy", "czz"]
+# return codes of include/sunset_gpu.h
+ERR_ARG, ERR_CUDA, ERR_SVD, ERR_SCOPE, ERR_NONFINITE, ERR_NOMEM, ERR_ILLCOND = -1, -2, -3, -4, -5, -6, -7
 
 # C-ABI symbols declared in include/sunset_gpu.h
 ABI_SYMBOLS = [
@@ -36,6 +39,7 @@ ABI_SYMBOLS = [
     "sunset_set_lengths", "sunset_get_dump", "sunset_write_dump", "sunset_set_restart", "sunset_checkpoint_size",
     "sunset_save_checkpoint", "sunset_load_checkpoint", "sunset_get_flow_control", "sunset_set_flow_control",
     "sunset_set_layers", "sunset_get_layers", "sunset_set_state_3d", "sunset_get_state_3d", "sunset_calc_all_rhs_3d",
+    "sunset_get_conditioning", "sunset_kernel_binary_version",
 ]
 
 
@@ -47,11 +51,15 @@ class SunsetConfig(C.Structure):
                 ("Mdiff", C.c_double), ("Ma", C.c_double), ("grav", C.c_double * 3), ("h_over_s", C.c_double),
                 ("device", C.c_int), ("inflow_type", C.c_int), ("inflow_velocity_control", C.c_int),
                 ("u_inflow_start", C.c_double), ("u_inflow_end", C.c_double), ("ramp_time", C.c_double),
-                ("vpid", C.c_int)]
+                ("vpid", C.c_int), ("cond_max", C.c_double), ("svd_max_sweeps", C.c_int)]
 
 
 class SunsetError(RuntimeError):
-    pass
+    """A negative SUNSET_ERR_* return code; .code holds it (None when not from a call)."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 _lib = None
@@ -101,6 +109,8 @@ def load_library(build_if_missing: bool = True):
     L.sunset_load_checkpoint.argtypes = [P, C.c_void_p, C.c_size_t]
     L.sunset_get_neighbours.argtypes = [P, ip, ip, ip]
     L.sunset_get_weights.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
+    L.sunset_get_conditioning.argtypes = [P, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.sunset_kernel_binary_version.argtypes = [C.c_int]
     for n in ["sunset_calc_gradient", "sunset_calc_laplacian", "sunset_calc_filtered_var", "sunset_calc_filter_term"]:
         getattr(L, n).argtypes = [P, dp, dp, C.c_int]
     L.sunset_set_state.argtypes = [P, dp, dp, dp, dp, dp, dp, dp]
@@ -130,7 +140,7 @@ class Sunset:
                  fenep=False, fenep_l2=1e30, Mdiff=0.0, grav=(0.0, 0.0, 0.0), mcorr=True, kolmogorov_forcing=-1,
                  di_full_gradients=True, h_over_s=0.0, L_char=1.0, U_char=1.0, precision="fp64", device=0,
                  inflow_type=1, inflow_velocity_control=0, u_inflow_start=0.0, u_inflow_end=1.0, ramp_time=1.0,
-                 vpid=False):
+                 vpid=False, cond_max=0.0, svd_max_sweeps=0):
         self.L = load_library()
         cfg = SunsetConfig()
         cfg.form = FORMS[form]
@@ -150,6 +160,7 @@ class Sunset:
         cfg.inflow_type, cfg.inflow_velocity_control = int(inflow_type), int(inflow_velocity_control)
         cfg.u_inflow_start, cfg.u_inflow_end, cfg.ramp_time = u_inflow_start, u_inflow_end, ramp_time
         cfg.vpid = int(bool(vpid))
+        cfg.cond_max, cfg.svd_max_sweeps = float(cond_max), int(svd_max_sweeps)
         self.cfg = cfg
         self.h = C.c_void_p()
         rc = self.L.sunset_create(C.byref(cfg), C.byref(self.h))
@@ -171,7 +182,7 @@ class Sunset:
 
     def _chk(self, rc):
         if rc != 0:
-            raise SunsetError(f"[{rc}] " + self.L.sunset_last_error(self.h).decode())
+            raise SunsetError(f"[{rc}] " + self.L.sunset_last_error(self.h).decode(), rc)
 
     # ---- setup_domain.F90 / neighbours.F90 / labf.F90 ----
     def build_domain(self, ns):
@@ -189,7 +200,26 @@ class Sunset:
         self._chk(self.L.sunset_find_neighbours(self.h))
 
     def calc_labf_weights(self):
+        """labf.F90:34-394.  Without a cond_max limit, nodes whose moment matrix is worse
+        conditioned than 1e12 are reported by a RuntimeWarning (the reference solves them
+        silently); with one, the call fails with SUNSET_ERR_ILLCOND."""
         self._chk(self.L.sunset_calc_labf_weights(self.h))
+        _, _, worst, n_ill = self.conditioning(arrays=False)
+        if n_ill:
+            warnings.warn(f"{n_ill} nodes have moment matrices with condition number above 1e12 "
+                          f"(worst {worst:.3g}); their weights carry few correct digits", RuntimeWarning)
+
+    def conditioning(self, arrays=True):
+        """(cond_deriv, cond_filter, worst, n_ill): sigma_max/sigma_min of each node's
+        derivative and filter moment matrix in reference order (None unless arrays), the
+        worst value, and the count above the limit."""
+        n = self.sizes()[1]
+        cd = np.zeros(n) if arrays else None
+        cf = np.zeros(n) if arrays else None
+        worst, nill = C.c_double(), C.c_int()
+        self._chk(self.L.sunset_get_conditioning(self.h, cd.ctypes.data if arrays else None,
+                                                 cf.ctypes.data if arrays else None, C.byref(worst), C.byref(nill)))
+        return cd, cf, worst.value, nill.value
 
     def calc_boundary_weights(self):
         self._chk(self.L.sunset_calc_boundary_weights(self.h))
@@ -458,7 +488,7 @@ def kinetic_energy_noalloc(device, npfb, ro_ptr, u_ptr, v_ptr, vol_ptr, out_ptr,
                                                       C.c_void_p(v_ptr), C.c_void_p(vol_ptr), C.c_void_p(out_ptr),
                                                       C.c_void_p(stream_ptr) if stream_ptr else None)
     if rc != 0:
-        raise SunsetError(f"sunset_kinetic_energy_noalloc failed with code {rc}")
+        raise SunsetError(f"sunset_kinetic_energy_noalloc failed with code {rc}", rc)
 
 
 def for_workload(wl, ns=None, precision="fp64", device=0, **over):

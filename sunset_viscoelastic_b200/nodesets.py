@@ -258,10 +258,14 @@ def read_ipart(path: str) -> NodeSet:
 
     def nxt():
         while True:
-            ln = next(it)
+            try:
+                ln = next(it)
+            except StopIteration:
+                raise ValueError(f"{path}: the file ends before the {npfb} node rows its header announces") from None
             if ln.strip():
                 return ln.split()
 
+    npfb = 0
     nb, npfb, smax, smin = nxt()
     npfb = int(npfb)
     xmin, xmax, ymin, ymax = (float(v) for v in nxt())
@@ -271,6 +275,8 @@ def read_ipart(path: str) -> NodeSet:
     for _ in range(nproc):
         nxt()
     rows = [nxt() for _ in range(npfb)]
+    if any(len(r) < 7 for r in rows):
+        raise ValueError(f"{path}: a node row has fewer than the 7 columns gi x y type nx ny s")
     a = np.array([[float(v.replace("D", "E")) for v in r] for r in rows])
     return NodeSet(x=a[:, 1], y=a[:, 2], node_type=a[:, 3].astype(np.int32), nx=a[:, 4], ny=a[:, 5],
                    s=a[:, 6], xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, bcond=bc,

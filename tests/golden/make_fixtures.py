@@ -1,7 +1,6 @@
 """Builds tests/golden/ from the reference's own fixtures.
 
-Run in a checkout where the reference is available (REFERENCE_DIR, default
-/root/reference).  Produces:
+Run with REFERENCE_DIR set to a checkout of the reference (required).  Produces:
   ipart_fixture.npz  -- the reference's IPART node set (4,056 doubly periodic nodes on
                         [-pi,pi]^2, s = 2 pi/64), converted to arrays; together with the
                         parameters of its control.in this is the only fixture the
@@ -17,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", ".."))
 from sunset_viscoelastic_b200.nodesets import read_ipart  # noqa: E402
 
-ref = os.environ.get("REFERENCE_DIR", "/root/reference")
+ref = os.environ.get("REFERENCE_DIR")
+if not ref:
+    sys.exit("set REFERENCE_DIR to a checkout of the reference (it holds IPART and control.in)")
 ns = read_ipart(os.path.join(ref, "IPART"))
 # control.in (positional, load_data.F90:53-159)
 vals = []

@@ -27,9 +27,16 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
-    # the fatbin of an nvcc -gencode arch=compute_100a,code=sm_100a build names its target
-    blob = open(labfm.library_path(), "rb").read()
-    assert b"sm_100a" in blob
+    # the build compiles every source for sm_100a SASS only (no PTX for other targets)
+    from sunset_viscoelastic_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.gpu
+def test_kernels_run_as_sm100_binaries():
+    # what the CUDA runtime reports for a kernel of the loaded library
+    lib = labfm.load_library()
+    assert lib.sunset_kernel_binary_version(0) == 100
 
 
 def test_version_and_error_paths_without_gpu():

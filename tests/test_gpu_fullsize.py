@@ -1,0 +1,205 @@
+"""Parity of the CUDA path with the CPU restatement at the full sizes of the measured
+configurations, and on the reference's own case.
+
+* periodic-di-o4-16k (128^2 nodes, order 4, direct form): weights bit-identical to the
+  restatement with the device's x^4, fields after 100 steps within 1e-8 of both
+  restatements;
+* periodic-lc-o6-262k (512^2, order 6, sPTT eps 0.25 in log-conformation form): fields after
+  200 steps within 1e-8 of the restatement with the device's x^4;
+* periodic-chl-o8-1m (1024^2, order 8, Cholesky form): gradient and Laplacian bit-identical
+  (so are the weights behind them), filter within 1e-13, fields after 5 steps within 1e-8;
+* the reference's only shipped case, its IPART node set (4,056 doubly periodic nodes) with
+  its control.in, run as the reference runs it by default: Cholesky form at order 8 with the
+  reference's own smoothing lengths adapted by adapt_stencils (sunset.F90:43-51), the
+  Kolmogorov initial condition of setup_flow.F90:224-229 (with its 1e-10 perturbation), the
+  forcing of rhs.F90:275, and the PID-controlled time step from dt = 1e-6
+  (setup_flow.F90:149, step.F90:624-682).  After 100 steps the fields match the
+  restatement within 1e-8, and the reference's Kolmogorov L2 norms (statistics.F90:552-612)
+  of the device state match the restatement's.
+
+The restatement runs on all host cores; the two larger cases take about a minute of host
+time each.
+"""
+import dataclasses
+import os
+
+import numpy as np
+import pytest
+
+from sunset_viscoelastic_b200 import labfm
+from sunset_viscoelastic_b200.nodesets import NodeSet, WORKLOADS, initial_state
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+F_TOL = 1e-8
+FIELDS = ["ro", "rou", "rov", "u", "v", "cxx", "cxy", "cyy"]
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def restatement(wl, ns, correctly_rounded=True):
+    O.set_threads(os.cpu_count() or 1)
+    O.set_pow_mode(correctly_rounded)
+    try:
+        return O.for_workload(wl, ns).setup()
+    finally:
+        O.set_pow_mode(False)
+
+
+def run_both(wl, ns, objs, nsteps):
+    st = initial_state(ns)
+    for o in objs:
+        o.set_state(**st)
+    dtc, dtp = objs[0].set_tstep()
+    for o in objs[1:]:
+        assert o.set_tstep() == (dtc, dtp)
+    dt = wl.cfl * min(dtc, dtp)
+    for o in objs:
+        o.step(dt, nsteps)
+    return [o.state() for o in objs]
+
+
+def test_direct_form_order4_full_size():
+    wl = WORKLOADS["periodic-di-o4-16k"]
+    ns = wl.nodes()
+    assert ns.n == 128 * 128
+    cr, ref = restatement(wl, ns, True), restatement(wl, ns, False)
+    gpu = labfm.for_workload(wl, ns).setup()
+    wc, wg = cr.weights(), gpu.weights()
+    for key in ["w_grad", "w_lap", "w_grad_sum", "w_lap_sum"]:
+        assert np.array_equal(wg[key], wc[key]), key
+    sc, sr, sg = run_both(wl, ns, [cr, ref, gpu], 100)
+    for k in FIELDS:
+        print(f"C1 {k}: vs restatement (device x^4) {rel(sg[k], sc[k]):.2e}, vs libm restatement {rel(sg[k], sr[k]):.2e}")
+        assert rel(sg[k], sc[k]) <= F_TOL, k
+        assert rel(sg[k], sr[k]) <= F_TOL, k
+    gpu.close()
+
+
+def test_log_conformation_order6_full_size_200_steps():
+    wl = WORKLOADS["periodic-lc-o6-262k"]
+    ns = wl.nodes()
+    assert ns.n == 512 * 512 and wl.epsPTT == 0.25 and wl.form == "lc"
+    cr = restatement(wl, ns, True)
+    gpu = labfm.for_workload(wl, ns).setup()
+    rng = np.random.default_rng(11)
+    phi = np.sin(2 * np.pi * ns.x) * np.cos(4 * np.pi * ns.y) + 0.1 * rng.standard_normal(ns.n)
+    assert np.array_equal(gpu.gradient(phi), cr.gradient(phi))
+    assert np.array_equal(gpu.laplacian(phi), cr.laplacian(phi))
+    sc, sg = run_both(wl, ns, [cr, gpu], 200)
+    for k in FIELDS + ["psixx", "psixy", "psiyy"]:
+        print(f"C2 {k} after 200 steps: {rel(sg[k], sc[k]):.2e}")
+        assert rel(sg[k], sc[k]) <= F_TOL, k
+    gpu.close()
+
+
+def test_cholesky_order8_full_size():
+    wl = WORKLOADS["periodic-chl-o8-1m"]
+    ns = wl.nodes()
+    assert ns.n == 1024 * 1024
+    cr = restatement(wl, ns, True)
+    gpu = labfm.for_workload(wl, ns).setup()
+    rng = np.random.default_rng(13)
+    phi = np.cos(2 * np.pi * ns.x) * np.sin(2 * np.pi * ns.y) + 0.1 * rng.standard_normal(ns.n)
+    g_dev, g_ref = gpu.gradient(phi), cr.gradient(phi)
+    print("C3 gradient entries differing:", int(np.sum(g_dev != g_ref)))
+    assert np.array_equal(g_dev, g_ref)
+    assert np.array_equal(gpu.laplacian(phi), cr.laplacian(phi))
+    # the filter coefficients go through cos (CUDA vs glibc): within 1e-13 of the field
+    assert np.abs(gpu.filter_term(phi) - cr.filter_term(phi)).max() <= 1e-13 * np.abs(phi).max()
+    sc, sg = run_both(wl, ns, [cr, gpu], 5)
+    for k in FIELDS + ["psixx", "psixy", "psiyy"]:
+        print(f"C3 {k} after 5 steps: {rel(sg[k], sc[k]):.2e}")
+        assert rel(sg[k], sc[k]) <= F_TOL, k
+    gpu.close()
+
+
+# ----------------------------------------------------------------------- the reference's case
+def ipart_nodes():
+    d = np.load(os.path.join(HERE, "golden", "ipart_fixture.npz"))
+    b = d["box"]
+    ns = NodeSet(x=d["x"], y=d["y"], node_type=d["node_type"], nx=d["nx"], ny=d["ny"], s=d["s"],
+                 xmin=b[0], xmax=b[1], ymin=b[2], ymax=b[3], bcond=tuple(int(v) for v in d["bcond"]), gi=d["gi"])
+    ctrl = dict(zip(["L_char", "U_char", "Re", "Wi", "beta", "epsPTT", "fenep_l2", "Mdiff", "Ma"],
+                    (float(v) for v in d["control"])))
+    return ns, ctrl
+
+
+def kolmogorov_ic(ns, Wi, Mdiff):
+    """setup_flow.F90:224-229, perturbation included."""
+    x, y = ns.x, ns.y
+    u = np.cos(y) - 0.25e-10 * (-np.sin(x / 4.0) * np.sin(y / 4.0) + 2.0 * np.cos(3.0 * x / 4.0) * np.sin(y / 2.0))
+    v = 0.25e-10 * (np.cos(x / 4.0) * np.cos(y / 4.0) - 3.0 * np.cos(3.0 * x / 4.0) * np.sin(y / 2.0))
+    cxx = 1.0 + (Wi * Wi / (1.0 + Mdiff * Wi)) * (1.0 - np.cos(2.0 * y) / (1.0 + 4.0 * Mdiff * Wi))
+    cxy = -Wi * np.sin(y) / (1.0 + Mdiff * Wi)
+    one = np.ones(ns.n)
+    return dict(ro=one, u=u, v=v, cxx=cxx, cxy=cxy, cyy=one.copy(), czz=one.copy())
+
+
+def kolmogorov_l2norm(st, y, vol, lam, exact):
+    """statistics.F90:552-612: volume-weighted L2 distances of u, v, cxx, cxy, cyy from an exact
+    state.  exact=None takes the reference's hard-coded two-mode solution (u = cos 2y,
+    cxx = 1 + 8 lam^2 sin^2 2y, cxy = -2 lam sin 2y, cyy = 1); otherwise a dict u, cxx, cxy."""
+    if exact is None:
+        exact = dict(u=np.cos(2.0 * y), cxx=1.0 + 2.0 * lam * lam * 4.0 * np.sin(2.0 * y) ** 2,
+                     cxy=-lam * 2.0 * np.sin(2.0 * y))
+    tv = vol.sum()
+    err = [st["u"] - exact["u"], st["v"], st["cxx"] - exact["cxx"], st["cxy"] - exact["cxy"], st["cyy"] - 1.0]
+    return np.array([np.sqrt(np.sum(vol * e * e) / tv) for e in err])
+
+
+def test_reference_ipart_default_run():
+    ns, c = ipart_nodes()
+    assert ns.n == 4056
+    kw = dict(form="chl", order=8, Re=c["Re"], Wi=c["Wi"], beta=c["beta"], epsPTT=c["epsPTT"], Ma=c["Ma"],
+              Mdiff=c["Mdiff"], L_char=c["L_char"], U_char=c["U_char"], kolmogorov_forcing=-1)
+    O.set_pow_mode(True)
+    try:
+        ref = O.Oracle(**kw).build_domain(ns)
+        ref.find_neighbours()
+        ref.adapt_stencils()
+        ref.calc_labf_weights()
+        ref.calc_labf_sums()
+        ref.filter_coefficients()
+    finally:
+        O.set_pow_mode(False)
+    gpu = labfm.Sunset(**kw).build_domain(ns)
+    gpu.find_neighbours()
+    gpu.adapt_stencils()
+    gpu.calc_labf_weights()
+    gpu.calc_boundary_weights()
+    gpu.calc_labf_sums()
+    gpu.filter_coefficients()
+    hr = ref.nodes()["h"][:ns.n]
+    hg, _ = gpu.lengths()
+    assert np.array_equal(hg, hr)
+    cd_r, _ = ref.conditioning()
+    cd_g, _, worst, nill = gpu.conditioning()
+    assert np.array_equal(cd_g, cd_r) and nill == 0
+    st = kolmogorov_ic(ns, c["Wi"], c["Mdiff"])
+    for o in (ref, gpu):
+        o.set_state(**st)
+        o.set_time(0.0, 1.0e-6, 0, np.array([1e-16, 1e-16, 1e-16]))  # setup_flow.F90:149-157
+        o.step(0.0, 100, pid=True)
+    tr, tg = ref.time(), gpu.time()
+    assert tg["itime"] == tr["itime"] == 100
+    assert abs(tg["dt"] - tr["dt"]) <= 1e-12 * tr["dt"]
+    sr, sg = ref.state(), gpu.state()
+    for k in FIELDS + ["psixx", "psixy", "psiyy"]:
+        print(f"IPART {k} after 100 PID steps: {rel(sg[k], sr[k]):.2e}")
+        assert rel(sg[k], sr[k]) <= F_TOL, k
+    vol = gpu.weights()["vol"]
+    lam = c["Wi"] * c["L_char"] / c["U_char"]
+    for exact in (None, dict(u=np.cos(ns.y), cxx=st["cxx"], cxy=st["cxy"])):
+        ng = kolmogorov_l2norm(sg, ns.y, vol, lam, exact)
+        nr = kolmogorov_l2norm(sr, ns.y, vol, lam, exact)
+        print("Kolmogorov L2 norms (u, v, cxx, cxy, cyy): device", ng, "restatement", nr)
+        np.testing.assert_allclose(ng, nr, rtol=1e-8, atol=1e-14)
+    # the flow stays on its steady state: the one-mode velocity error is at rounding level
+    ng1 = kolmogorov_l2norm(sg, ns.y, vol, lam, dict(u=np.cos(ns.y), cxx=st["cxx"], cxy=st["cxy"]))
+    assert ng1[0] < 1e-6 and ng1[1] < 1e-8
+    gpu.close()

@@ -464,3 +464,42 @@ def test_3d_z_stencils(wlname):
     assert 1e-3 * (k * dz) ** wl.order < abs(kmod - k) / k < (k * dz) ** wl.order
     for key in ("rou", "rov", "xx", "xy", "yy"):
         assert np.abs(r[key]).max() < 1e-12, key
+
+
+def test_conditioning_of_the_moment_matrices():
+    """The condition numbers the library reports, from the restatement's SVD: the stated
+    order-6 radius (3.2 s) leaves near-singular moment matrices (sigma_max/sigma_min above
+    1e12 at some nodes, where the reference still inverts every nonzero sigma,
+    svdlib.F90:283-293), the measured radius 4.2 s does not, and order 8 at 5.4 s sits near
+    1e10, the reference's own sensitivity at that order."""
+    worst = {}
+    for order, name, r in [(6, "periodic-lc-o6-262k", 3.2), (6, "periodic-lc-o6-262k", 4.2),
+                           (8, "periodic-chl-o8-1m", 5.4)]:
+        wl = dataclasses.replace(WORKLOADS[name], nside=48, radius_over_s=r)
+        o = O.for_workload(wl).setup()
+        cd, cf = o.conditioning()
+        assert np.all(cd >= 1.0) and np.all(cf >= 1.0)
+        worst[(order, r)] = (max(cd.max(), cf.max()), int(np.sum(np.maximum(cd, cf) > 1e12)))
+    print(worst)
+    assert worst[(6, 3.2)][1] > 0
+    assert worst[(6, 4.2)][0] < 1e8
+    assert 1e8 < worst[(8, 5.4)][0] < 1e12
+
+
+def test_truncated_node_file_is_rejected(tmp_path):
+    """A node file that ends before the rows its header announces (setup_domain.F90:93-199
+    reads npfb rows) is an error, not a shorter node set."""
+    from sunset_viscoelastic_b200.nodesets import read_ipart, write_ipart
+    ns = jittered_lattice(12)
+    p = tmp_path / "IPART"
+    write_ipart(str(p), ns)
+    back = read_ipart(str(p))
+    assert back.n == ns.n and np.array_equal(back.x, ns.x)
+    lines = p.read_text().splitlines()
+    (tmp_path / "IPART_short").write_text("\n".join(lines[:-5]) + "\n")
+    with pytest.raises(ValueError, match="ends before"):
+        read_ipart(str(tmp_path / "IPART_short"))
+    cut = lines[:-1] + [" ".join(lines[-1].split()[:4])]
+    (tmp_path / "IPART_cut").write_text("\n".join(cut) + "\n")
+    with pytest.raises(ValueError, match="7 columns"):
+        read_ipart(str(tmp_path / "IPART_cut"))
