@@ -1,11 +1,21 @@
 #!/usr/bin/env python
 """RK3 node-steps/s of the LABFM time step on B200 (one JSON line on rank 0).
 
-Workload (default): the doubly periodic 512x512 jittered node set (262,144 nodes), LABFM
-order 6, sPTT (eps=0.25) in log-conformation form, FP64 - the configuration the metric is
-quoted on.  One step = one step_rk3_4S_2R_EE: four right-hand sides with their stencils,
-the low-storage RK update with the error norm, the hyperviscous filter and the mass
-correction.  Inputs are seeded synthetic node sets (no dataset exists for this path).
+Workload (default): the doubly periodic 1024x1024 jittered node set (1,048,576 nodes), LABFM
+order 8, Oldroyd-B (Wi 2, beta 0.1) in Cholesky form - the precision configuration the metric
+compares, and the largest that fits one GPU.  The headline `value` is the FP64 drop-in; the
+line also carries
+  * `mixed`: the mixed-precision step on the same set (node-steps/s, speed-up over FP64, its
+    stage-kernel roofline, and the per-field error against the FP64 path after
+    --error-steps steps);
+  * `setup`: the device build of neighbours and weights (seconds, nodes/s) and the CPU
+    restatement's build of the same order and radius on a bounded sample of nodes;
+  * `adjoint`: the adjoint/forward cost of sunset_adjoint_run on the differentiation workload
+    (262,144 nodes, order 6, log-conformation, 200 steps, checkpoints every 20); its
+    finite-difference checks run with `--adjoint --fd-check`.
+One step = one step_rk3_4S_2R_EE: four right-hand sides with their stencils, the low-storage
+RK update with the error norm, the hyperviscous filter and the mass correction.  Inputs are
+seeded synthetic node sets (no dataset exists for this path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--precision fp64|mixed]
   python bench.py --impl reference ...   (the CPU restatement of the reference, all host cores)
@@ -30,7 +40,8 @@ sys.path.insert(0, ROOT)
 from sunset_viscoelastic_b200.nodesets import WORKLOADS  # noqa: E402
 
 METRIC = "RK3 node-steps/s"
-DEFAULT_WORKLOAD = "periodic-lc-o6-262k"
+DEFAULT_WORKLOAD = "periodic-chl-o8-1m"
+ADJOINT_WORKLOAD = "periodic-lc-o6-262k-adjoint"
 
 
 def parse():
@@ -53,6 +64,9 @@ def parse():
     p.add_argument("--checkpoint", type=int, default=20, help="--adjoint: checkpoint every N steps")
     p.add_argument("--fd-check", action="store_true",
                    help="--adjoint: check dJ/dWi, dJ/dbeta and 8 Gaussian psi0 directions by central differences")
+    p.add_argument("--no-mixed", action="store_true", help="leave out the mixed-precision block")
+    p.add_argument("--no-adjoint", action="store_true", help="leave out the adjoint cost block")
+    p.add_argument("--no-setup", action="store_true", help="leave out the setup block")
     return p.parse_args()
 
 
@@ -88,7 +102,7 @@ def dt_for(wl, dtc, dtp):
 
 
 class ClockSampler:
-    """SM clock, its maximum and the active throttle reasons, sampled every 20 ms during the
+    """SM clock, its maximum and the active throttle reasons, sampled every 5 ms during the
     timed region through NVML (read-only queries; the same counters nvidia-smi prints).
     Falls back to nvidia-smi at 200 ms where NVML is unavailable."""
 
@@ -98,7 +112,7 @@ class ClockSampler:
                   "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                   "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, cuda_device, period=0.02):
+    def __init__(self, cuda_device, period=0.005):
         self.dev = cuda_device
         self.period = period
         self.rows = []  # (sm_mhz, sm_max_mhz, reasons bitmask)
@@ -135,7 +149,7 @@ class ClockSampler:
 
             self.thread = threading.Thread(target=loop, daemon=True)
             self.thread.start()
-            self.source = "nvml 20 ms"
+            self.source = f"nvml {self.period * 1e3:g} ms"
         except Exception:
             self.out = os.path.join("/tmp", f"sunset_clocks_{os.getpid()}.csv")
             try:
@@ -229,20 +243,23 @@ ERROR_GROUPS = {"ro": ["ro"], "rou": ["rou", "rov"], "rov": ["rou", "rov"], "u":
                 "cxx": ["cxx", "cxy", "cyy"], "cxy": ["cxx", "cxy", "cyy"], "cyy": ["cxx", "cxy", "cyy"]}
 
 
-def mixed_error(wl, ns, g, dt, nsteps, device):
+def mixed_error(wl, ns, g, dt, nsteps, device, ref=None):
     """Per-field error of the mixed-precision handle g against the FP64 device path (which
     agrees with the FP64 restatement to ~1e-14 in the parity tests), both stepped nsteps
     from the initial state at the same dt.  Each field's error is relative to the magnitude
     of the quantity it is a component of (rho, the momentum or velocity vector, the
     conformation tensor): L_inf = max|d| / max_group max|f|, L_2 = ||d|| / max_group ||f||."""
     from sunset_viscoelastic_b200 import labfm
-    ref = labfm.for_workload(wl, ns, device=device).setup()
+    own = ref is None
+    if own:
+        ref = labfm.for_workload(wl, ns, device=device).setup()
     st = wl.initial(ns)
     for h in (g, ref):
         h.set_state(**st)
         h.step(dt, nsteps)
     a, b = g.state(), ref.state()
-    ref.close()
+    if own:
+        ref.close()
     linf, l2 = {}, {}
     for k, grp in ERROR_GROUPS.items():
         d = a[k] - b[k]
@@ -281,7 +298,9 @@ def run_reference(args, ws, rank):
             "cpu_baseline": {"value": value, "unit": "node-steps/s", "cores": cpu_threads(), "kind": "port",
                              "sample": f"{nsteps} RK steps of the full {nodes}-node set after {warm} warm-up steps "
                                        f"(host weight build {setup_s:.1f}s untimed)"},
-            "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "setup": {"host_s": setup_s, "host_nodes_per_s": nodes / setup_s, "cores": cpu_threads(),
+                      "what": "neighbour search, weights, sums and filter coefficients of the whole set"}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -293,32 +312,12 @@ def run_adjoint(args, local):
     import torch
     from sunset_viscoelastic_b200 import labfm
     torch.cuda.set_device(local)
-    wl = WORKLOADS[args.workload if args.workload != DEFAULT_WORKLOAD else "periodic-lc-o6-262k-adjoint"]
-    ns = wl.nodes()
+    wl = WORKLOADS[args.workload if args.workload != DEFAULT_WORKLOAD else ADJOINT_WORKLOAD]
     steps = args.steps
-    g = labfm.for_workload(wl, ns, device=local).setup()
-    st = wl.initial(ns)
-    g.set_state(**st)
-    dtc, dtp = g.set_tstep()
-    dt = dt_for(wl, dtc, dtp)
+    fwd, adj, J, dWi, dbeta, grads, g, ns, st, dt = adjoint_cost(wl, steps, args.checkpoint, args.warmup, local)
     nodes = g.sizes()[1]
-    # warm up both paths (graphs, adjoint storage), then time each from the initial state
-    g.step(dt, args.warmup)
-    g.set_state(**st)
-    g.adjoint_run(dt, steps, args.checkpoint, state_gradient=False)  # sizes the checkpoint store
-    g.set_state(**st)
-    g.synchronize()
-    t = time.perf_counter()
-    g.step(dt, steps)
-    g.synchronize()
-    fwd = time.perf_counter() - t
     g.set_state(**st)
     ms_fwd_events = g.step_timed(dt, steps)
-    g.set_state(**st)
-    g.synchronize()
-    t = time.perf_counter()
-    J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, args.checkpoint)
-    adj = time.perf_counter() - t
     line = {"metric": "adjoint/forward cost", "value": adj / fwd, "unit": "x", "higher_is_better": False,
             "n_gpus": 1, "steps": steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic (seeded jittered lattice)",
             "config": {"workload": wl.name, "nodes": nodes, "order": wl.order, "form": wl.form, "Wi": wl.Wi,
@@ -459,6 +458,89 @@ def run_3d(args, local):
     return 0
 
 
+def stage_roofline(g, wl, precision, steps):
+    """The RK stage kernel inside real steps (the same step sequence launched kernel by kernel,
+    CUDA events on the handle's stream around each step's four stage launches), against the
+    measured HBM copy bandwidth."""
+    roof_steps = max(3, min(steps, 50))
+    stage_ms, stage_bytes = g.time_stage_kernel(roof_steps)
+    peak, peak_kind = measured_peaks()
+    achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": profiled_traffic(wl.name, precision), "kernel": "k_stage (one RK stage: stencils + rhs + update)",
+            "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms, "peak_source": peak_kind,
+            "method": f"CUDA events around the 4 back-to-back stage launches of each of {roof_steps} steps, / 4"}
+
+
+def built_handle(wl, ns, precision, local):
+    """A handle through the setup calls (sunset.F90:51-60); returns it and the wall seconds of
+    the setup (neighbour search, weights, sums, filter coefficients, link streams)."""
+    from sunset_viscoelastic_b200 import labfm
+    t = time.perf_counter()
+    g = labfm.for_workload(wl, ns, precision=precision, device=local).setup()
+    g.synchronize()
+    return g, time.perf_counter() - t
+
+
+def timed_steps(g, dt, args, dist, local):
+    g.step(dt, args.warmup)
+    g.synchronize()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms = g.step_timed(dt, args.steps)
+    if dist:
+        dist.barrier()
+    return max_over_ranks(dist, ms, device=f"cuda:{local}"), clk.summary()
+
+
+def setup_block(wl, nodes, device_s):
+    """The device setup against the CPU restatement's setup (neighbour search, weights, sums,
+    filter coefficients) on a bounded sample: the same order and radius on a 192 x 192 set."""
+    import dataclasses
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(cpu_threads())
+    sub = dataclasses.replace(wl, nside=min(wl.nside, 192)) if wl.periodic else wl
+    sns = sub.nodes()
+    t = time.perf_counter()
+    o = O.for_workload(sub, sns).setup()
+    el = time.perf_counter() - t
+    del o
+    return {"device_s": device_s, "device_nodes_per_s": nodes / device_s,
+            "cpu_nodes_per_s": sns.n / el, "cpu_cores": cpu_threads(), "cpu_kind": "port",
+            "cpu_sample": f"the restatement's setup of {sns.n} nodes at the same order and radius ({el:.2f} s)",
+            "note": "wall seconds through the C-ABI setup calls, host-side link ordering included"}
+
+
+def adjoint_cost(wl, steps, checkpoint, warmup, local):
+    """(forward s, adjoint s, J, dJ/dWi, dJ/dbeta, handle, state, dt): sunset_adjoint_run from
+    the initial state against the same forward run, wall clock with the device synchronised."""
+    from sunset_viscoelastic_b200 import labfm
+    ns = wl.nodes()
+    g = labfm.for_workload(wl, ns, device=local).setup()
+    st = wl.initial(ns)
+    g.set_state(**st)
+    dtc, dtp = g.set_tstep()
+    dt = dt_for(wl, dtc, dtp)
+    # warm up both paths (graphs, adjoint storage), then time each from the initial state
+    g.step(dt, warmup)
+    g.set_state(**st)
+    g.adjoint_run(dt, steps, checkpoint, state_gradient=False)  # sizes the checkpoint store
+    g.set_state(**st)
+    g.synchronize()
+    t = time.perf_counter()
+    g.step(dt, steps)
+    g.synchronize()
+    fwd = time.perf_counter() - t
+    g.set_state(**st)
+    g.synchronize()
+    t = time.perf_counter()
+    J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, checkpoint)
+    adj = time.perf_counter() - t
+    return fwd, adj, J, dWi, dbeta, grads, g, ns, st, dt
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -469,38 +551,18 @@ def main():
     if args.layers > 0.0:
         return run_3d(args, local)
     import torch
-    from sunset_viscoelastic_b200 import labfm
     torch.cuda.set_device(local)
     dist = init_pg(ws, "nccl")
     wl = WORKLOADS[args.workload]
     ns = wl.nodes()
-    g = labfm.for_workload(wl, ns, precision=args.precision, device=local).setup()
+    g, setup_s = built_handle(wl, ns, args.precision, local)
     g.set_state(**wl.initial(ns))
     nodes = g.sizes()[1]  # npfb: the reader's node list, FD rows of boundary nodes included
     dtc, dtp = g.set_tstep()
     dt = dt_for(wl, dtc, dtp)
-    g.step(dt, args.warmup)
-    g.synchronize()
-    if dist:
-        dist.barrier()
-    with ClockSampler(local) as clk:
-        ms = g.step_timed(dt, args.steps)
-    if dist:
-        dist.barrier()
-    ms_max = max_over_ranks(dist, ms, device=f"cuda:{local}")
+    ms_max, clocks = timed_steps(g, dt, args, dist, local)
     value = ws * nodes * args.steps / (ms_max * 1e-3)
-
-    # kernel roofline: the RK stage kernel inside real steps (the same step sequence launched
-    # kernel by kernel, CUDA events on the handle's stream around every stage launch)
-    roof_steps = max(3, min(args.steps, 50))
-    stage_ms, stage_bytes = g.time_stage_kernel(roof_steps)
-    peak, peak_kind = measured_peaks()
-    achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
-    traffic = profiled_traffic(wl.name, args.precision)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_stage (one RK stage: stencils + rhs + update)",
-                "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms, "peak_source": peak_kind,
-                "method": f"CUDA events around the 4 back-to-back stage launches of each of {roof_steps} steps, / 4"}
+    roofline = stage_roofline(g, wl, args.precision, args.steps)
 
     # end to end through the C-ABI with host buffers: per step, copy the evolved fields in
     # from pinned host memory, run the step, copy them back
@@ -533,10 +595,7 @@ def main():
         el = time.perf_counter() - t
         cpu = {"value": n * k / el, "unit": "node-steps/s", "cores": cpu_threads(), "kind": "port",
                "sample": f"{k} RK steps of the full {n}-node set (weights from the device build)"}
-
-    accuracy = None
-    if args.precision == "mixed" and not args.no_error_check:
-        accuracy = mixed_error(wl, ns, g, dt, args.error_steps, local)
+        del o
 
     launches_per_step = 7
     line = {"metric": METRIC, "value": value, "unit": "node-steps/s", "n_gpus": ws, "steps": args.steps,
@@ -548,12 +607,36 @@ def main():
                        "l2": "working set larger than L2 (weights)", "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
-            "clocks": clk.summary()}
-    if accuracy is not None:
-        line["error_vs_fp64"] = accuracy
+            "clocks": clocks}
+    # the blocks below run on a single rank only (replicas have nothing more to add)
+    extra = ws == 1
+    if args.precision == "mixed" and not args.no_error_check:
+        line["error_vs_fp64"] = mixed_error(wl, ns, g, dt, args.error_steps, local)
+    if extra and args.precision == "fp64" and not args.no_mixed:
+        gm, _ = built_handle(wl, ns, "mixed", local)
+        gm.set_state(**wl.initial(ns))
+        ms_mx, clk_mx = timed_steps(gm, dt, args, None, local)
+        v_mx = nodes * args.steps / (ms_mx * 1e-3)
+        line["mixed"] = {"value": v_mx, "unit": "node-steps/s", "ms_per_step": ms_mx / args.steps,
+                         "speedup_vs_fp64": v_mx / value, "dtype": "f32+f64",
+                         "roofline": stage_roofline(gm, wl, "mixed", args.steps), "clocks": clk_mx,
+                         "gpu_launches": launches_per_step * args.steps}
+        if not args.no_error_check:
+            line["mixed"]["error_vs_fp64"] = mixed_error(wl, ns, gm, dt, args.error_steps, local, ref=g)
+        gm.close()
+    if extra and not args.no_setup:
+        line["setup"] = setup_block(wl, nodes, setup_s)
+    g.close()
+    if extra and not args.no_adjoint:
+        awl = WORKLOADS[ADJOINT_WORKLOAD]
+        fwd, adj, J, dWi, dbeta, _, ga, _, _, _ = adjoint_cost(awl, 200, 20, args.warmup, local)
+        ga.close()
+        line["adjoint"] = {"value": adj / fwd, "unit": "x (adjoint / forward wall time)", "higher_is_better": False,
+                           "workload": awl.name, "steps": 200, "checkpoint_every": 20, "forward_s": fwd,
+                           "adjoint_s": adj, "J": J, "dJ_dWi": dWi, "dJ_dbeta": dbeta,
+                           "fd_check": "python bench.py --adjoint --steps 200 --fd-check"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    g.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

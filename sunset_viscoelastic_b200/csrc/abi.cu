@@ -108,12 +108,14 @@ int need(Handle *H, bool ok, const char *what) {
 }
 
 // The device error word of the step kernels: 0 = none, 1 = the time-step error norm of a
-// step was NaN or infinite (k_finalize, k3_finalize).  No other value is ever written.
+// step was NaN or infinite (k_finalize, k3_finalize), 2 = a wait of the mixed stage kernel
+// on its link stream gave up (k_stage).  No other value is ever written.
 int check_err_flag(Handle *H) {
     int e = 0;
     SUNSET_CUDA(H, cudaMemcpyAsync(&e, &H->dsc->err, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
     SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
     if (e == 1) return set_err(H, SUNSET_ERR_NONFINITE, "non-finite time-step error norm");
+    if (e == 2) return set_err(H, SUNSET_ERR_CUDA, "a bounded wait on the stage kernel's link stream gave up");
     if (e) return set_err(H, SUNSET_ERR_CUDA, "unknown device error word %d", e);
     return 0;
 }

@@ -40,7 +40,11 @@ struct StageArgs {
     const int *halo_ptr, *halo;
     int hmax;
     const double *wx, *wy, *wl, *wh;
-    const float *wx32, *wy32, *wl32, *wh32;  // mixed precision
+    // mixed precision: the stage's packed links and their per-node scales (stream.cu), the
+    // filter's FP32 weights
+    const unsigned *pkx, *pky, *pkl;
+    const float *scx, *scy, *scl;
+    const float *wh32;
     const double *gsx, *gsy, *lsum, *hsum, *vol, *py_node;
     const int *ntype;            // node types (walls: 0)
     const double *rnx, *rny;     // wall normals into the fluid
@@ -347,14 +351,290 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Mixed-precision stage gather.
+//
+// The tile's halo is staged as FP32 offsets from a per-tile FP64 reference of each field
+// (the field's value at the tile's first halo node; zero, when the node set has mirrors, for
+// the fields a mirror link reflects), two fields to an 8-byte word, so one link's
+// neighbour values take ceil(NG/2) 8-byte shared loads.  Each thread differences them with
+// its own node's offsets and sums w_k (phi_j - phi_i) in FP32: the offsets keep the bits a
+// difference of two nearby values needs, since phi_j - ref spans a tile, not |phi|.  The
+// sums are scaled to FP64 once per node (the packed weights are integers in units of the
+// node's scale, stream.cu).
+//
+// The link stream reaches shared memory by bulk copies (the TMA engine, cp.async.bulk, from
+// this GPU's memory only, no cluster multicast): lane 0 of each warp keeps kMxDepth chunks of
+// kMxChunk link pairs of its slice in flight, each completing on an mbarrier of the warp, so
+// the link loads stay off the LSU pipe that the halo gathers keep busy.  Every wait on an
+// mbarrier is bounded: when one gives up, the kernel sets the device error word to 2, waits
+// (bounded again) for the warp's copies in flight and finishes with the sums it has; the host
+// reports the error.
+// ---------------------------------------------------------------------------------------
+#ifndef SUNSET_MX_CHUNK
+#define SUNSET_MX_CHUNK 2
+#endif
+#ifndef SUNSET_MX_DEPTH
+#define SUNSET_MX_DEPTH 2
+#endif
+constexpr int kMxChunk = SUNSET_MX_CHUNK;  // link pairs per bulk copy
+constexpr int kMxDepth = SUNSET_MX_DEPTH;  // bulk copies in flight per warp
+constexpr int kMxWaitLimit = 1 << 20;      // try_wait rounds before a wait gives up
+
+// Shared memory of the mixed stage kernel, in order: the warps' link rings (kMxDepth stages
+// of three words x kMxChunk pairs x 32 lanes, 8 bytes a lane and pair), their mbarriers, the
+// NG field references (FP64) and the halo as ceil(NG/2) arrays of float2 of hmax entries.
+__host__ __device__ constexpr size_t mx_ring_bytes() { return (size_t)kTileSlices * kMxDepth * 3 * kMxChunk * 32 * 8; }
+__host__ __device__ constexpr size_t mx_bar_bytes() { return (size_t)kTileSlices * kMxDepth * 8; }
+__host__ __device__ inline size_t mx_smem_bytes(int ng, int hmax) {
+    return mx_ring_bytes() + mx_bar_bytes() + (size_t)ng * 8 + (size_t)((ng + 1) / 2) * hmax * 8;
+}
+__device__ __forceinline__ double *mx_refs(double *smem) {
+    return reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + mx_ring_bytes() + mx_bar_bytes());
+}
+__device__ __forceinline__ float2 *mx_halo(double *smem, int ng) { return reinterpret_cast<float2 *>(mx_refs(smem) + ng); }
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// makes the barriers' initialisation visible to the bulk-copy engine
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+    for (int it = 0; it < kMxWaitLimit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// global -> this CTA's shared memory by the bulk-copy engine, completion counted on `bar`
+__device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// orders this thread's generic-proxy shared accesses before its later bulk copies
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// The xy component among the gathered fields (a mirror link flips its sign with codes 1, 2).
+__host__ __device__ constexpr bool is_xy_slot(int form, bool md, int f) {
+    return f == 4 || (form == SUNSET_FORM_LC && f == 7) || (form == SUNSET_FORM_CHL && md && f == 7);
+}
+
+// One warp's ring of packed link words (its slice's small links, pair by pair).
+struct MxRing {
+    uint2 *ring;      // kMxDepth stages of [3 words][kMxChunk pairs][32 lanes]
+    unsigned bar0;    // shared address of the warp's first mbarrier
+    const unsigned *src[3];
+    long long base;   // SELL slot of the slice's pair 0
+    int npair, nchunk;
+
+    // lane 0: bulk copies of chunk c (contiguous pair rows of 256 bytes per word array)
+    __device__ __forceinline__ void issue(int c) const {
+        const int s = c % kMxDepth;
+        const int np = min(kMxChunk, npair - c * kMxChunk);
+        const unsigned bytes = (unsigned)np * 256u, bar = bar0 + 8u * s;
+        mbar_expect_tx(bar, 3u * bytes);
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            bulk_load(smem_addr(ring + (s * 3 + a) * kMxChunk * 32), src[a] + base + (long long)c * kMxChunk * 64, bytes,
+                      bar);
+    }
+    __device__ __forceinline__ bool wait(int c) const {
+        return mbar_wait_bounded(bar0 + 8u * (c % kMxDepth), (unsigned)(c / kMxDepth) & 1u);
+    }
+};
+
+// The halo as FP32 offsets and this thread's own offsets oi (all threads of the block take
+// part; ends with a barrier).  The warp's mbarriers are initialised and its first chunks
+// started before, so the link stream flows while the halo loads.
+template <int FORM, bool MD, bool FP>
+__device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *smem, MxRing &R, bool wact,
+                                             float *oi) {
+    constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    if (wact && lane == 0) {
+        for (int s = 0; s < kMxDepth; s++) mbar_init(R.bar0 + 8u * s, 1u);
+        mbar_init_fence();
+        for (int c = 0; c < kMxDepth && c < R.nchunk; c++) R.issue(c);
+    }
+    const bool mir = cK.has_mirrors;
+    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb, hm = A.hmax;
+    const int n0 = __ldg(A.halo + hb);
+    double rf[NG];
+#pragma unroll
+    for (int f = 0; f < NG; f++)
+        rf[f] = (mir && (f == 1 || f == 2 || is_xy_slot(FORM, MD, f))) ? 0.0 : __ldg(gather_src<FORM, MD, FP>(A.in, f) + n0);
+    if (threadIdx.x == 0) {
+        double *ref = mx_refs(smem);
+#pragma unroll
+        for (int f = 0; f < NG; f++) ref[f] = rf[f];
+    }
+    float2 *hp = mx_halo(smem, NG);
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        const int node = __ldg(A.halo + hb + h);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            const float a = (float)(__ldg(gather_src<FORM, MD, FP>(A.in, 2 * p) + node) - rf[2 * p]);
+            const float b = 2 * p + 1 < NG ? (float)(__ldg(gather_src<FORM, MD, FP>(A.in, 2 * p + 1) + node) - rf[2 * p + 1])
+                                           : 0.0f;
+            hp[p * hm + h] = make_float2(a, b);
+        }
+    }
+    const int ii = i < cK.npfb ? i : 0;
+#pragma unroll
+    for (int f = 0; f < NG; f++) oi[f] = (float)(__ldg(gather_src<FORM, MD, FP>(A.in, f) + ii) - rf[f]);
+    __syncthreads();
+}
+
+// Stencil sums of node i over its small links in difference form, FP32 (see above).
+template <int FORM, bool MD, bool FP>
+__device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const double *smem, const MxRing &R,
+                                                bool wact, const float *oi, Grads &g) {
+    constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2;
+    constexpr int kFp = fp_slot(FORM, MD);
+    const int lane = threadIdx.x & 31, hm = A.hmax;
+    const float2 *hp = mx_halo(const_cast<double *>(smem), NG);
+    const bool mir = cK.has_mirrors;
+    const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
+    float s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
+    float s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
+    float s_pxx_x = 0, s_pxx_y = 0, s_pxy_x = 0, s_pxy_y = 0, s_pyy_x = 0, s_pyy_y = 0;
+    float s_lxx = 0, s_lxy = 0, s_lyy = 0;
+    float s_f_x = 0, s_f_y = 0, s_lzz = 0;
+    auto link = [&](unsigned x, unsigned y, unsigned l) {
+        const unsigned loc = (x & 63u) | ((y & 63u) << 6) | ((l & 15u) << 12);
+        const float wx = (float)((int)x >> 6), wy = (float)((int)y >> 6), wl = (float)((int)l >> 6);
+        const int j = (int)(loc & kLocMask);
+        const int code = mir ? (int)(loc >> 14) : 0;
+        float d[2 * NP];
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            const float2 v = hp[p * hm + j];
+            d[2 * p] = v.x;
+            d[2 * p + 1] = v.y;
+        }
+        // reflected fields have reference 0: the mirror value is -phi_parent
+        const float su = (code == 1 || code == 3) ? -1.0f : 1.0f, sv = (code == 2 || code == 3) ? -1.0f : 1.0f;
+        const float sxy = (code == 1 || code == 2) ? -1.0f : 1.0f;
+#pragma unroll
+        for (int f = 0; f < NG; f++) {
+            const float sg = f == 1 ? su : f == 2 ? sv : is_xy_slot(FORM, MD, f) ? sxy : 1.0f;
+            d[f] = __fmaf_rn(sg, d[f], -oi[f]);
+        }
+        s_ro_x = __fmaf_rn(wx, d[0], s_ro_x);
+        s_ro_y = __fmaf_rn(wy, d[0], s_ro_y);
+        s_u_x = __fmaf_rn(wx, d[1], s_u_x);
+        s_u_y = __fmaf_rn(wy, d[1], s_u_y);
+        s_lu = __fmaf_rn(wl, d[1], s_lu);
+        s_v_x = __fmaf_rn(wx, d[2], s_v_x);
+        s_v_y = __fmaf_rn(wy, d[2], s_v_y);
+        s_lv = __fmaf_rn(wl, d[2], s_lv);
+        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {  // c in slots 3, 4, 5
+            s_cxx_x = __fmaf_rn(wx, d[3], s_cxx_x);
+            if (full) s_cxx_y = __fmaf_rn(wy, d[3], s_cxx_y);
+            s_cxy_x = __fmaf_rn(wx, d[4], s_cxy_x);
+            s_cxy_y = __fmaf_rn(wy, d[4], s_cxy_y);
+            if (full) s_cyy_x = __fmaf_rn(wx, d[5], s_cyy_x);
+            s_cyy_y = __fmaf_rn(wy, d[5], s_cyy_y);
+        }
+        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {  // psi in slots 6-8 (LC) or 3-5 (CHL)
+            constexpr int q = FORM == SUNSET_FORM_LC ? 6 : 3;
+            s_pxx_x = __fmaf_rn(wx, d[q], s_pxx_x);
+            s_pxx_y = __fmaf_rn(wy, d[q], s_pxx_y);
+            s_pxy_x = __fmaf_rn(wx, d[q + 1], s_pxy_x);
+            s_pxy_y = __fmaf_rn(wy, d[q + 1], s_pxy_y);
+            s_pyy_x = __fmaf_rn(wx, d[q + 2], s_pyy_x);
+            s_pyy_y = __fmaf_rn(wy, d[q + 2], s_pyy_y);
+        }
+        if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) {  // c in slots 3-5 (DI) or 6-8 (CHL)
+            constexpr int q = FORM == SUNSET_FORM_DI ? 3 : 6;
+            s_lxx = __fmaf_rn(wl, d[q], s_lxx);
+            s_lxy = __fmaf_rn(wl, d[q + 1], s_lxy);
+            s_lyy = __fmaf_rn(wl, d[q + 2], s_lyy);
+        }
+        if constexpr (FP && FORM != SUNSET_FORM_NEWT) {
+            s_f_x = __fmaf_rn(wx, d[kFp], s_f_x);
+            s_f_y = __fmaf_rn(wy, d[kFp], s_f_y);
+            if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) s_lzz = __fmaf_rn(wl, d[kFp + 1], s_lzz);
+        }
+    };
+    if (wact) {
+        for (int c = 0; c < R.nchunk; c++) {
+            if (!R.wait(c)) {
+                if (lane == 0) atomicExch(&A.sc->err, 2);
+                for (int c2 = c; c2 < c + kMxDepth && c2 < R.nchunk; c2++) R.wait(c2);
+                break;
+            }
+            const int np = min(kMxChunk, R.npair - c * kMxChunk);
+            const uint2 *rs = R.ring + (c % kMxDepth) * 3 * kMxChunk * 32;
+#pragma unroll
+            for (int p = 0; p < kMxChunk; p++) {
+                if (p < np) {
+                    const uint2 X = rs[p * 32 + lane], Y = rs[(kMxChunk + p) * 32 + lane];
+                    const uint2 L = rs[(2 * kMxChunk + p) * 32 + lane];
+                    link(X.x, Y.x, L.x);
+                    link(X.y, Y.y, L.y);
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && c + kMxDepth < R.nchunk) {
+                fence_proxy_async();
+                R.issue(c + kMxDepth);
+            }
+        }
+    }
+    if (i >= cK.npfb) return;
+    const double cx = (double)A.scx[i], cy = (double)A.scy[i], cl = (double)A.scl[i];
+    g.ro_x = (double)s_ro_x * cx;
+    g.ro_y = (double)s_ro_y * cy;
+    g.u_x = (double)s_u_x * cx;
+    g.u_y = (double)s_u_y * cy;
+    g.lapu = (double)s_lu * cl;
+    g.v_x = (double)s_v_x * cx;
+    g.v_y = (double)s_v_y * cy;
+    g.lapv = (double)s_lv * cl;
+    g.cxx_x = (double)s_cxx_x * cx;
+    g.cxx_y = (double)s_cxx_y * cy;
+    g.cxy_x = (double)s_cxy_x * cx;
+    g.cxy_y = (double)s_cxy_y * cy;
+    g.cyy_x = (double)s_cyy_x * cx;
+    g.cyy_y = (double)s_cyy_y * cy;
+    g.pxx_x = (double)s_pxx_x * cx;
+    g.pxx_y = (double)s_pxx_y * cy;
+    g.pxy_x = (double)s_pxy_x * cx;
+    g.pxy_y = (double)s_pxy_y * cy;
+    g.pyy_x = (double)s_pyy_x * cx;
+    g.pyy_y = (double)s_pyy_y * cy;
+    g.lapcxx = (double)s_lxx * cl;
+    g.lapcxy = (double)s_lxy * cl;
+    g.lapcyy = (double)s_lyy * cl;
+    g.lapczz = (double)s_lzz * cl;
+    g.f_x = g.f_y = g.pzz_x = g.pzz_y = 0.0;
+    if constexpr (FP && FORM != SUNSET_FORM_NEWT) {
+        if (FORM == SUNSET_FORM_CHL) { g.pzz_x = (double)s_f_x * cx; g.pzz_y = (double)s_f_y * cy; }
+        else { g.f_x = (double)s_f_x * cx; g.f_y = (double)s_f_y * cy; }
+    }
+}
+
 // Polymer diffusion on a wall node: the transverse Laplacian of c over the node's small links
 // with the tangential second-derivative weights (calc_laplacian_transverse_only_on_bound,
 // derivatives.F90:306-358), plus the one-sided normal second derivative from its four FD rows
 // (rhs_di.F90:556-568; rhs.F90 likewise, there for c_zz too).  Links in the reference's
 // order, neighbours from the tile's shared-memory halo.
-template <int FORM, bool MD, bool FP>
-__device__ __forceinline__ void wall_conformation_laplacian(const StageArgs &A, int i, const double *sm, Grads &g) {
-    const int jj = A.bidx[i], hm = A.hmax;
+template <int FORM, bool MD, bool FP, class HV>
+__device__ __forceinline__ void wall_conformation_laplacian(const StageArgs &A, int i, HV hv, Grads &g) {
+    const int jj = A.bidx[i];
     const long long base = A.slice_ptr[i >> 5];
     const int ln = i & 31, cs = A.cnt_small[i];
     constexpr int c0 = FORM == SUNSET_FORM_DI ? 3 : 6;  // halo slots of cxx, cxy, cyy
@@ -365,13 +645,13 @@ __device__ __forceinline__ void wall_conformation_laplacian(const StageArgs &A, 
     for (int k = 0; k < cs; k++) {
         const unsigned lk = A.lloc_ref[sell_at(base, k, ln)];
         const int h = lk & kLocMask, code = lk >> 14;
-        double cxy = sm[(c0 + 1) * hm + h];
+        double cxy = hv(c0 + 1, h);
         if (code == 1 || code == 2) cxy = -cxy;
         const double wk = w[k];
-        l0 = l0 + sm[c0 * hm + h] * wk;
+        l0 = l0 + hv(c0, h) * wk;
         l1 = l1 + cxy * wk;
-        l2 = l2 + sm[(c0 + 2) * hm + h] * wk;
-        if (zz) l3 = l3 + sm[cz * hm + h] * wk;
+        l2 = l2 + hv(c0 + 2, h) * wk;
+        if (zz) l3 = l3 + hv(cz, h) * wk;
     }
     const Fields &F = A.in;
     const double ws = A.wbt_sum[jj], L = cK.L_char;
@@ -427,49 +707,73 @@ __device__ __forceinline__ void block_min_bits(unsigned long long v, unsigned lo
     }
 }
 
-// Resident blocks per SM the stage kernel is compiled for (up to 85 registers a thread):
-// the tile halo plus the link ring take 55-70 KB of shared memory on the order-6 and
-// order-8 sets, so a fourth block would not fit anyway.
+// Resident blocks per SM the stage kernel is compiled for.  FP64: up to 85 registers a
+// thread; the tile halo plus the link ring take 55-70 KB of shared memory on the order-6 and
+// order-8 sets, so a fourth block would not fit anyway.  Mixed: the FP32 halo and the
+// bulk-copy rings take 40-50 KB, and the FP32 sums fewer registers.
 #ifndef SUNSET_STAGE_BLOCKS
 #define SUNSET_STAGE_BLOCKS 3
 #endif
-__host__ __device__ constexpr int stage_min_blocks(int) { return SUNSET_STAGE_BLOCKS; }
+#ifndef SUNSET_STAGE_BLOCKS_MX
+#define SUNSET_STAGE_BLOCKS_MX 4
+#endif
+__host__ __device__ constexpr int stage_min_blocks(bool mx) { return mx ? SUNSET_STAGE_BLOCKS_MX : SUNSET_STAGE_BLOCKS; }
 
 // One RK stage (stage = 0,1,2: intermediate; 3: final; 4: right-hand side only).  One
 // block per tile of kTile nodes; the tile's halo is staged in shared memory first.
 //
-// MX (mixed precision): FP32 weights; the register S is kept as the FP32 increment
+// MX (mixed precision): packed fixed-point weights, FP32 halo offsets and FP32 sums in
+// difference form (gather_stage_mx); the register S is kept as the FP32 increment
 // D = S - U over the stage's FP64 state U (so S = U + D loses only FP32 rounding of an
 // O(dt rhs) quantity) and the error accumulator E as FP32.
 // BND: the node set has boundary nodes (walls, inflows, outflows); without them the
 // closures are compiled out, which keeps them from costing the periodic sets registers.
 template <int FORM, bool MD, bool MX, bool FP, bool BND>
-__global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageArgs A) {
+__global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs A) {
     extern __shared__ __align__(16) double smem[];
     constexpr int NG = ngather(FORM, MD, FP);
     const int i = blockIdx.x * kTile + threadIdx.x;
     bool active = (i >> 5) < cK.nslices;
-    LinkRing<MX, 3, ring_depth(MX)> R;
-    if constexpr (MX) {
-        R.src[0] = reinterpret_cast<const float2 *>(A.wx32);
-        R.src[1] = reinterpret_cast<const float2 *>(A.wy32);
-        R.src[2] = reinterpret_cast<const float2 *>(A.wl32);
-    } else {
-        R.src[0] = reinterpret_cast<const double2 *>(A.wx);
-        R.src[1] = reinterpret_cast<const double2 *>(A.wy);
-        R.src[2] = reinterpret_cast<const double2 *>(A.wl);
-    }
-    R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
-           active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
-    R.prologue();  // the first link pairs stream in while the halo is staged
-    load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD, FP>(A.in, f); });
     const int stage = A.stage;
     if (stage == 0 && i == 0) {
         A.sc->cfl_bits = 0x7ff0000000000000ull;
         A.sc->par_bits = 0x7ff0000000000000ull;
     }
     Grads g;
-    if (active) gather_stage<FORM, MD, MX, FP>(A, i, smem, R, g);
+    if constexpr (MX) {
+        const int warp = threadIdx.x >> 5, sl = blockIdx.x * kTileSlices + warp;
+        MxRing R;
+        R.ring = reinterpret_cast<uint2 *>(smem) + (size_t)warp * kMxDepth * 3 * kMxChunk * 32;
+        R.bar0 = smem_addr(reinterpret_cast<char *>(smem) + mx_ring_bytes() + (size_t)warp * kMxDepth * 8);
+        R.src[0] = A.pkx;
+        R.src[1] = A.pky;
+        R.src[2] = A.pkl;
+        R.base = active ? A.slice_ptr[sl] : 0;
+        R.npair = active ? A.slice_ws[sl] >> 1 : 0;
+        R.nchunk = (R.npair + kMxChunk - 1) / kMxChunk;
+        float oi[NG];
+        load_halo_mx<FORM, MD, FP>(A, i, smem, R, active, oi);
+        gather_stage_mx<FORM, MD, FP>(A, i, smem, R, active, oi, g);
+    } else {
+        LinkRing<false, 3, ring_depth(false)> R;
+        R.src[0] = reinterpret_cast<const double2 *>(A.wx);
+        R.src[1] = reinterpret_cast<const double2 *>(A.wy);
+        R.src[2] = reinterpret_cast<const double2 *>(A.wl);
+        R.init(smem + halo_doubles(NG, A.hmax), reinterpret_cast<const unsigned *>(A.lloc),
+               active ? (A.slice_ptr[i >> 5] >> 1) + (i & 31) : 0, active ? A.slice_ws[i >> 5] >> 1 : 0);
+        R.prologue();  // the first link pairs stream in while the halo is staged
+        load_halo<NG>(A, smem, [&](int f) { return gather_src<FORM, MD, FP>(A.in, f); });
+        if (active) gather_stage<FORM, MD, false, FP>(A, i, smem, R, g);
+    }
+    // a node's own value of gathered field f in the tile's halo slot h (wall Laplacian of c)
+    auto hv = [&](int f, int h) -> double {
+        if constexpr (MX) {
+            const float2 v = mx_halo(smem, NG)[(f >> 1) * A.hmax + h];
+            return mx_refs(smem)[f] + (double)((f & 1) ? v.y : v.x);
+        } else {
+            return smem[f * A.hmax + h];
+        }
+    };
     active = active && i < cK.npfb;
     unsigned long long emax_bits = 0;
     if constexpr (FORM == SUNSET_FORM_LC && !MX) {
@@ -496,11 +800,11 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(FORM)) k_stage(StageAr
         double uin = inout ? A.uin[jb] : 0.0;
         if (inout) {  // inflow/outflow closure in the x-y frame
             if constexpr (MD && FORM == SUNSET_FORM_CHL)  // rhs.F90:624-636: the same one-sided flux closure
-                wall_conformation_laplacian<FORM, MD, FP>(A, i, smem, g);
+                wall_conformation_laplacian<FORM, MD, FP>(A, i, hv, g);
             rhs_flow_inout(cK, n, g, ty, uin, r);
         } else if (wall) {  // wall closure; then the conformation with the rotated velocity gradient
             if constexpr (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL))
-                wall_conformation_laplacian<FORM, MD, FP>(A, i, smem, g);
+                wall_conformation_laplacian<FORM, MD, FP>(A, i, hv, g);
             const double xn = A.rnx[i], yn = A.rny[i];
             rhs_flow_wall(cK, n, g, xn, yn, r);
             const double gux = g.u_x, guy = g.u_y, gvx = g.v_x, gvy = g.v_y;
@@ -1064,12 +1368,11 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     } else {
         A.wx = H->wx; A.wy = H->wy; A.wl = H->wl; A.wh = H->wh;
     }
-    A.wx32 = H->wx32; A.wy32 = H->wy32; A.wl32 = H->wl32; A.wh32 = H->wh32;
-    if (mx) {
-        A.gsx = H->gsx32; A.gsy = H->gsy32; A.lsum = H->lsum32; A.hsum = H->hsum32;
-    } else {
-        A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum; A.hsum = H->hsum;
-    }
+    A.pkx = H->pkx; A.pky = H->pky; A.pkl = H->pkl;
+    A.scx = H->scx; A.scy = H->scy; A.scl = H->scl;
+    A.wh32 = H->wh32;
+    A.gsx = H->gsx; A.gsy = H->gsy; A.lsum = H->lsum;
+    A.hsum = mx ? H->hsum32 : H->hsum;
     A.vol = H->vol;
     A.py_node = H->py;
     A.ntype = H->ntype;
@@ -1156,8 +1459,9 @@ inline bool is_mx(const Handle *H) { return H->cfg.precision == SUNSET_MIXED; }
 
 template <int FORM, bool MD, bool FP>
 int launch_stage(Handle *H, const StageArgs &A, bool mx) {
-    const size_t smem = halo_doubles(ngather(FORM, MD, FP), H->halo_max) * sizeof(double) +
-                        (mx ? LinkRing<true, 3, ring_depth(true)>::bytes() : LinkRing<false, 3, ring_depth(false)>::bytes());
+    const size_t smem = mx ? mx_smem_bytes(ngather(FORM, MD, FP), H->halo_max)
+                           : halo_doubles(ngather(FORM, MD, FP), H->halo_max) * sizeof(double) +
+                                 LinkRing<false, 3, ring_depth(false)>::bytes();
     if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
     if (H->nb > 0) {
         if (mx) k_stage<FORM, MD, true, FP, true><<<H->ntiles, kTile, smem, H->stream>>>(A);

@@ -1,5 +1,6 @@
 // stream.cu -- the link stream of the time step: bank-aware link order, and the weights the
-// stage and filter kernels stream (FP64 copies, or FP32 for the mixed precision).
+// stage and filter kernels stream (FP64 copies, or packed fixed-point stage links and FP32
+// filter weights for the mixed precision).
 //
 // The setup, the single-operator entry points and the weight export keep the reference's
 // link order (derivatives.F90 sums over ij_link in order).  The time step sums each node's
@@ -12,13 +13,15 @@
 // bank pairs wherever a bipartite matching allows it (2.6 on that set).  Only the rounding
 // of the sums changes (relative 1e-16 a sum).
 //
-// Mixed precision: the weight solves stay FP64; the step streams the weights rounded to FP32,
-// which halves the dominant per-link traffic (26 -> 14 bytes a link with the 16-bit local
-// index), while fields, stencil arithmetic and state stay FP64.  The stencil sums sum_k w_k
-// are recomputed in FP64 from the rounded weights, so the step's sum form
-// sum_k w_k phi_j - phi_i sum_k w_k is exactly the difference form
-// sum_k w_k (phi_j - phi_i) of the rounded stencil: a constant field keeps zero derivatives
-// and the rounding never leaks a phi_i * (sum of rounding errors) term.
+// Mixed precision: the weight solves stay FP64; the stage kernel streams each link as three
+// 32-bit words, one per operator (d/dx, d/dy, Laplacian): a 26-bit two's-complement weight in
+// the upper bits, scaled by a power of two per node and operator (2^(e-25), e the exponent
+// of the node's largest |w| of that operator), and 6 bits of the link's 16-bit local index in
+// the lower bits (bits 0-5, 6-11 and 12-15 of the index in the x, y and Laplacian words).
+// That is 12 bytes a link against 26 in FP64 (16-bit index + three doubles), and the weights
+// keep 25 bits relative to the node's largest one; the stage sums in difference form,
+// sum_k w_k (phi_j - phi_i), so a constant field keeps zero derivatives whatever the rounding.
+// The filter streams its weight rounded to FP32 with the local index (6 bytes a link).
 #include <algorithm>
 #include <thread>
 #include <vector>
@@ -38,33 +41,68 @@ struct StreamArgs {
     const double *wx, *wy, *wl, *wh;
     uint16_t *lloc_s;
     double *wx_s, *wy_s, *wl_s, *wh_s;      // FP64 step
-    float *wx32, *wy32, *wl32, *wh32;       // mixed step
-    double *gsx32, *gsy32, *lsum32, *hsum32;
+    unsigned *pkx, *pky, *pkl;              // mixed step: packed stage links
+    float *scx, *scy, *scl;                 // their per-node scales
+    float *wh32;                            // mixed filter
+    double *hsum32;
 };
 
-// One thread per node: gather its links into the stream order; MX: round the weights and
-// sum the rounded weights.  Padding entries keep weight 0 and local index 0.
+constexpr int kPackBits = 26;  // bits of a packed stage weight (sign included)
+
+// Exponent e with max|w| < 2^e (0 for an all-zero operator row).
+__device__ __forceinline__ int pack_exponent(double wmax) {
+    int e = 0;
+    if (wmax > 0.0) frexp(wmax, &e);
+    return e;
+}
+// A weight as a kPackBits-bit integer in units of 2^(e - kPackBits + 1), shifted into place
+// above the 6 index bits.
+__device__ __forceinline__ unsigned pack_weight(double w, int e, unsigned idx6) {
+    const long long lim = (1ll << (kPackBits - 1)) - 1;
+    long long q = llrint(ldexp(w, kPackBits - 1 - e));
+    q = q > lim ? lim : (q < -lim ? -lim : q);
+    return ((unsigned)(int)q << 6) | (idx6 & 63u);
+}
+
+// One thread per node: gather its links into the stream order; MX: pack the stage weights
+// with the node's scales, round the filter weights to FP32 and sum those.  Padding entries
+// keep weight 0 and local index 0.
 template <bool MX>
 __global__ void k_stream_weights(StreamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.npfb) return;
     const long long base = a.slice_ptr[i >> 5];
     const int lane = i & 31;
-    double gx = 0.0, gy = 0.0, lp = 0.0, hy = 0.0;
-    for (int k = 0; k < a.slice_w[i >> 5]; k++) {
+    const int w = a.slice_w[i >> 5];
+    int ex = 0, ey = 0, el = 0;
+    if constexpr (MX) {
+        double mx = 0.0, my = 0.0, ml = 0.0;
+        for (int k = 0; k < w; k++) {
+            const int q = a.src[sell_at(base, k, lane)];
+            if (q < 0) continue;
+            mx = fmax(mx, fabs(a.wx[q]));
+            my = fmax(my, fabs(a.wy[q]));
+            ml = fmax(ml, fabs(a.wl[q]));
+        }
+        ex = pack_exponent(mx);
+        ey = pack_exponent(my);
+        el = pack_exponent(ml);
+        a.scx[i] = ldexpf(1.0f, ex - (kPackBits - 1));
+        a.scy[i] = ldexpf(1.0f, ey - (kPackBits - 1));
+        a.scl[i] = ldexpf(1.0f, el - (kPackBits - 1));
+    }
+    double hy = 0.0;
+    for (int k = 0; k < w; k++) {
         const long long o = sell_at(base, k, lane);
         const int q = a.src[o];
-        a.lloc_s[o] = q < 0 ? 0 : a.lloc[q];
+        const unsigned loc = q < 0 ? 0u : a.lloc[q];
+        a.lloc_s[o] = (uint16_t)loc;
         if constexpr (MX) {
-            const float fx = q < 0 ? 0.0f : (float)a.wx[q], fy = q < 0 ? 0.0f : (float)a.wy[q];
-            const float fl = q < 0 ? 0.0f : (float)a.wl[q], fh = q < 0 ? 0.0f : (float)a.wh[q];
-            a.wx32[o] = fx;
-            a.wy32[o] = fy;
-            a.wl32[o] = fl;
+            a.pkx[o] = pack_weight(q < 0 ? 0.0 : a.wx[q], ex, loc);
+            a.pky[o] = pack_weight(q < 0 ? 0.0 : a.wy[q], ey, loc >> 6);
+            a.pkl[o] = pack_weight(q < 0 ? 0.0 : a.wl[q], el, loc >> 12);
+            const float fh = q < 0 ? 0.0f : (float)a.wh[q];
             a.wh32[o] = fh;
-            gx = gx + (double)fx;
-            gy = gy + (double)fy;
-            lp = lp + (double)fl;
             hy = hy + (double)fh;
         } else {
             a.wx_s[o] = q < 0 ? 0.0 : a.wx[q];
@@ -73,12 +111,7 @@ __global__ void k_stream_weights(StreamArgs a) {
             a.wh_s[o] = q < 0 ? 0.0 : a.wh[q];
         }
     }
-    if constexpr (MX) {
-        a.gsx32[i] = gx;
-        a.gsy32[i] = gy;
-        a.lsum32[i] = lp;
-        a.hsum32[i] = hy;
-    }
+    if constexpr (MX) a.hsum32[i] = hy;
 }
 
 // Matching of a group of G lanes to the G bank groups (local position mod G) for one link
@@ -225,9 +258,8 @@ int make_stream_links(Handle *H) {
     if (!H->lloc_s) {
         if (dalloc(H, &H->lloc_s, L)) return SUNSET_ERR_NOMEM;
         if (mx) {
-            if (dalloc(H, &H->wx32, L) || dalloc(H, &H->wy32, L) || dalloc(H, &H->wl32, L) ||
-                dalloc(H, &H->wh32, L) || dalloc(H, &H->gsx32, n) || dalloc(H, &H->gsy32, n) ||
-                dalloc(H, &H->lsum32, n) || dalloc(H, &H->hsum32, n))
+            if (dalloc(H, &H->pkx, L) || dalloc(H, &H->pky, L) || dalloc(H, &H->pkl, L) || dalloc(H, &H->wh32, L) ||
+                dalloc(H, &H->scx, n) || dalloc(H, &H->scy, n) || dalloc(H, &H->scl, n) || dalloc(H, &H->hsum32, n))
                 return SUNSET_ERR_NOMEM;
         } else {
             if (dalloc(H, &H->wx_s, L) || dalloc(H, &H->wy_s, L) || dalloc(H, &H->wl_s, L) || dalloc(H, &H->wh_s, L))
@@ -240,8 +272,8 @@ int make_stream_links(Handle *H) {
     if (dalloc(H, &d_src, L)) return SUNSET_ERR_NOMEM;
     SUNSET_CUDA(H, cudaMemcpy(d_src, src.data(), L * sizeof(int), cudaMemcpyHostToDevice));
     StreamArgs a{n, H->slice_ptr, H->slice_w, d_src, H->lloc, H->wx, H->wy, H->wl, H->wh, H->lloc_s,
-                 H->wx_s, H->wy_s, H->wl_s, H->wh_s, H->wx32, H->wy32, H->wl32, H->wh32,
-                 H->gsx32, H->gsy32, H->lsum32, H->hsum32};
+                 H->wx_s, H->wy_s, H->wl_s, H->wh_s, H->pkx, H->pky, H->pkl, H->scx, H->scy, H->scl,
+                 H->wh32, H->hsum32};
     if (mx) k_stream_weights<true><<<(n + 255) / 256, 256, 0, H->stream>>>(a);
     else k_stream_weights<false><<<(n + 255) / 256, 256, 0, H->stream>>>(a);
     SUNSET_CUDA(H, cudaGetLastError());

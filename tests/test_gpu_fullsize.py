@@ -17,6 +17,12 @@ configurations, and on the reference's own case.
   restatement within 1e-8, and the reference's Kolmogorov L2 norms (statistics.F90:552-612)
   of the device state match the restatement's.
 
+Each field is compared with the magnitude of the quantity it is a component of (rho; the
+momentum or velocity vector; psi or the conformation tensor).  Components that vanish in the
+exact solution -- c_xy and psi_xy of a Taylor-Green flow, whose shear rate u_y + v_x is zero,
+or v of the Kolmogorov flow, which holds only its 1e-10 seed -- carry nothing but rounding,
+and a relative error against their own size would measure that rounding against itself.
+
 The restatement runs on all host cores; the two larger cases take about a minute of host
 time each.
 """
@@ -37,8 +43,19 @@ F_TOL = 1e-8
 FIELDS = ["ro", "rou", "rov", "u", "v", "cxx", "cxy", "cyy"]
 
 
+GROUP = {"ro": ["ro"], "rou": ["rou", "rov"], "rov": ["rou", "rov"], "u": ["u", "v"], "v": ["u", "v"],
+         "cxx": ["cxx", "cxy", "cyy"], "cxy": ["cxx", "cxy", "cyy"], "cyy": ["cxx", "cxy", "cyy"],
+         "psixx": ["psixx", "psixy", "psiyy"], "psixy": ["psixx", "psixy", "psiyy"],
+         "psiyy": ["psixx", "psixy", "psiyy"]}
+
+
 def rel(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def rel_field(sa, sb, k):
+    """max |a_k - b_k| over the largest magnitude of the fields in k's group (state b)."""
+    return float(np.abs(sa[k] - sb[k]).max() / max(max(np.abs(sb[f]).max() for f in GROUP[k]), 1e-300))
 
 
 def restatement(wl, ns, correctly_rounded=True):
@@ -74,9 +91,9 @@ def test_direct_form_order4_full_size():
         assert np.array_equal(wg[key], wc[key]), key
     sc, sr, sg = run_both(wl, ns, [cr, ref, gpu], 100)
     for k in FIELDS:
-        print(f"C1 {k}: vs restatement (device x^4) {rel(sg[k], sc[k]):.2e}, vs libm restatement {rel(sg[k], sr[k]):.2e}")
-        assert rel(sg[k], sc[k]) <= F_TOL, k
-        assert rel(sg[k], sr[k]) <= F_TOL, k
+        e_c, e_r = rel_field(sg, sc, k), rel_field(sg, sr, k)
+        print(f"C1 {k}: vs restatement (device x^4) {e_c:.2e}, vs libm restatement {e_r:.2e}")
+        assert e_c <= F_TOL and e_r <= F_TOL, k
     gpu.close()
 
 
@@ -92,8 +109,8 @@ def test_log_conformation_order6_full_size_200_steps():
     assert np.array_equal(gpu.laplacian(phi), cr.laplacian(phi))
     sc, sg = run_both(wl, ns, [cr, gpu], 200)
     for k in FIELDS + ["psixx", "psixy", "psiyy"]:
-        print(f"C2 {k} after 200 steps: {rel(sg[k], sc[k]):.2e}")
-        assert rel(sg[k], sc[k]) <= F_TOL, k
+        print(f"C2 {k} after 200 steps: {rel_field(sg, sc, k):.2e} (own size {rel(sg[k], sc[k]):.2e})")
+        assert rel_field(sg, sc, k) <= F_TOL, k
     gpu.close()
 
 
@@ -113,8 +130,8 @@ def test_cholesky_order8_full_size():
     assert np.abs(gpu.filter_term(phi) - cr.filter_term(phi)).max() <= 1e-13 * np.abs(phi).max()
     sc, sg = run_both(wl, ns, [cr, gpu], 5)
     for k in FIELDS + ["psixx", "psixy", "psiyy"]:
-        print(f"C3 {k} after 5 steps: {rel(sg[k], sc[k]):.2e}")
-        assert rel(sg[k], sc[k]) <= F_TOL, k
+        print(f"C3 {k} after 5 steps: {rel_field(sg, sc, k):.2e} (own size {rel(sg[k], sc[k]):.2e})")
+        assert rel_field(sg, sc, k) <= F_TOL, k
     gpu.close()
 
 
@@ -190,8 +207,8 @@ def test_reference_ipart_default_run():
     assert abs(tg["dt"] - tr["dt"]) <= 1e-12 * tr["dt"]
     sr, sg = ref.state(), gpu.state()
     for k in FIELDS + ["psixx", "psixy", "psiyy"]:
-        print(f"IPART {k} after 100 PID steps: {rel(sg[k], sr[k]):.2e}")
-        assert rel(sg[k], sr[k]) <= F_TOL, k
+        print(f"IPART {k} after 100 PID steps: {rel_field(sg, sr, k):.2e} (own size {rel(sg[k], sr[k]):.2e})")
+        assert rel_field(sg, sr, k) <= F_TOL, k
     vol = gpu.weights()["vol"]
     lam = c["Wi"] * c["L_char"] / c["U_char"]
     for exact in (None, dict(u=np.cos(ns.y), cxx=st["cxx"], cxy=st["cxy"])):
