@@ -356,8 +356,10 @@ __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const do
 //
 // The tile's halo is staged as FP32 offsets from a per-tile FP64 reference of each field
 // (the field's value at the tile's first halo node; zero, when the node set has mirrors, for
-// the fields a mirror link reflects), two fields to an 8-byte word, so one link's
-// neighbour values take ceil(NG/2) 8-byte shared loads.  Each thread differences them with
+// the fields a mirror link reflects), two fields to an 8-byte word and the words of one halo
+// node together (an odd number of words per node, so the bank-aware link order of stream.cu
+// keeps a half-warp's 8-byte loads on distinct bank pairs), so one link's neighbour values
+// take ceil(NG/2) 8-byte shared loads at one address plus constant offsets.  Each thread differences them with
 // its own node's offsets and sums w_k (phi_j - phi_i) in FP32: the offsets keep the bits a
 // difference of two nearby values needs, since phi_j - ref spans a tile, not |phi|.  The
 // sums are scaled to FP64 once per node (the packed weights are integers in units of the
@@ -386,8 +388,10 @@ constexpr int kMxWaitLimit = 1 << 20;      // try_wait rounds before a wait give
 // NG field references (FP64) and the halo as ceil(NG/2) arrays of float2 of hmax entries.
 __host__ __device__ constexpr size_t mx_ring_bytes() { return (size_t)kTileSlices * kMxDepth * 3 * kMxChunk * 32 * 8; }
 __host__ __device__ constexpr size_t mx_bar_bytes() { return (size_t)kTileSlices * kMxDepth * 8; }
+// 8-byte words a halo node takes: ceil(NG/2), made odd
+__host__ __device__ constexpr int mx_words(int ng) { return ((ng + 1) / 2) | 1; }
 __host__ __device__ inline size_t mx_smem_bytes(int ng, int hmax) {
-    return mx_ring_bytes() + mx_bar_bytes() + (size_t)ng * 8 + (size_t)((ng + 1) / 2) * hmax * 8;
+    return mx_ring_bytes() + mx_bar_bytes() + (size_t)ng * 8 + (size_t)mx_words(ng) * hmax * 8;
 }
 __device__ __forceinline__ double *mx_refs(double *smem) {
     return reinterpret_cast<double *>(reinterpret_cast<char *>(smem) + mx_ring_bytes() + mx_bar_bytes());
@@ -435,20 +439,19 @@ __host__ __device__ constexpr bool is_xy_slot(int form, bool md, int f) {
 struct MxRing {
     uint2 *ring;      // kMxDepth stages of [3 words][kMxChunk pairs][32 lanes]
     unsigned bar0;    // shared address of the warp's first mbarrier
-    const unsigned *src[3];
     long long base;   // SELL slot of the slice's pair 0
     int npair, nchunk;
 
     // lane 0: bulk copies of chunk c (contiguous pair rows of 256 bytes per word array)
-    __device__ __forceinline__ void issue(int c) const {
+    __device__ __forceinline__ void issue(const StageArgs &A, int c) const {
         const int s = c % kMxDepth;
         const int np = min(kMxChunk, npair - c * kMxChunk);
         const unsigned bytes = (unsigned)np * 256u, bar = bar0 + 8u * s;
+        const long long o = base + (long long)c * kMxChunk * 64;
         mbar_expect_tx(bar, 3u * bytes);
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-            bulk_load(smem_addr(ring + (s * 3 + a) * kMxChunk * 32), src[a] + base + (long long)c * kMxChunk * 64, bytes,
-                      bar);
+        bulk_load(smem_addr(ring + (s * 3 + 0) * kMxChunk * 32), A.pkx + o, bytes, bar);
+        bulk_load(smem_addr(ring + (s * 3 + 1) * kMxChunk * 32), A.pky + o, bytes, bar);
+        bulk_load(smem_addr(ring + (s * 3 + 2) * kMxChunk * 32), A.pkl + o, bytes, bar);
     }
     __device__ __forceinline__ bool wait(int c) const {
         return mbar_wait_bounded(bar0 + 8u * (c % kMxDepth), (unsigned)(c / kMxDepth) & 1u);
@@ -466,10 +469,10 @@ __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *
     if (wact && lane == 0) {
         for (int s = 0; s < kMxDepth; s++) mbar_init(R.bar0 + 8u * s, 1u);
         mbar_init_fence();
-        for (int c = 0; c < kMxDepth && c < R.nchunk; c++) R.issue(c);
+        for (int c = 0; c < kMxDepth && c < R.nchunk; c++) R.issue(A, c);
     }
     const bool mir = cK.has_mirrors;
-    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb, hm = A.hmax;
+    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
     const int n0 = __ldg(A.halo + hb);
     double rf[NG];
 #pragma unroll
@@ -481,6 +484,7 @@ __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *
         for (int f = 0; f < NG; f++) ref[f] = rf[f];
     }
     float2 *hp = mx_halo(smem, NG);
+    constexpr int NW = mx_words(NG);
     for (int h = threadIdx.x; h < hn; h += blockDim.x) {
         const int node = __ldg(A.halo + hb + h);
 #pragma unroll
@@ -488,7 +492,7 @@ __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *
             const float a = (float)(__ldg(gather_src<FORM, MD, FP>(A.in, 2 * p) + node) - rf[2 * p]);
             const float b = 2 * p + 1 < NG ? (float)(__ldg(gather_src<FORM, MD, FP>(A.in, 2 * p + 1) + node) - rf[2 * p + 1])
                                            : 0.0f;
-            hp[p * hm + h] = make_float2(a, b);
+            hp[h * NW + p] = make_float2(a, b);
         }
     }
     const int ii = i < cK.npfb ? i : 0;
@@ -497,15 +501,19 @@ __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *
     __syncthreads();
 }
 
-// Stencil sums of node i over its small links in difference form, FP32 (see above).
-template <int FORM, bool MD, bool FP>
+// Stencil sums of node i over its small links in difference form, FP32 (see above).  MIR:
+// the node set has mirror links (a reflected neighbour value is -phi_parent, and the
+// reflected fields have reference 0); without mirrors the signs are compiled out.
+//
+// A packed link word w (stream.cu) is the 32-bit integer 64 q + b, q the weight in units of
+// the node's scale and b six index bits: w & ~63 converted to FP32 is 64 q, w & 63 is b.
+template <int FORM, bool MD, bool FP, bool MIR>
 __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const double *smem, const MxRing &R,
                                                 bool wact, const float *oi, Grads &g) {
-    constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2;
+    constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2, NW = mx_words(NG);
     constexpr int kFp = fp_slot(FORM, MD);
-    const int lane = threadIdx.x & 31, hm = A.hmax;
+    const int lane = threadIdx.x & 31;
     const float2 *hp = mx_halo(const_cast<double *>(smem), NG);
-    const bool mir = cK.has_mirrors;
     const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
     float s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
     float s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
@@ -514,23 +522,27 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
     float s_f_x = 0, s_f_y = 0, s_lzz = 0;
     auto link = [&](unsigned x, unsigned y, unsigned l) {
         const unsigned loc = (x & 63u) | ((y & 63u) << 6) | ((l & 15u) << 12);
-        const float wx = (float)((int)x >> 6), wy = (float)((int)y >> 6), wl = (float)((int)l >> 6);
-        const int j = (int)(loc & kLocMask);
-        const int code = mir ? (int)(loc >> 14) : 0;
+        const float wx = (float)(int)(x & ~63u), wy = (float)(int)(y & ~63u), wl = (float)(int)(l & ~63u);
+        const float2 *v = hp + (loc & kLocMask) * NW;
         float d[2 * NP];
 #pragma unroll
         for (int p = 0; p < NP; p++) {
-            const float2 v = hp[p * hm + j];
-            d[2 * p] = v.x;
-            d[2 * p + 1] = v.y;
+            const float2 q = v[p];
+            d[2 * p] = q.x;
+            d[2 * p + 1] = q.y;
         }
-        // reflected fields have reference 0: the mirror value is -phi_parent
-        const float su = (code == 1 || code == 3) ? -1.0f : 1.0f, sv = (code == 2 || code == 3) ? -1.0f : 1.0f;
-        const float sxy = (code == 1 || code == 2) ? -1.0f : 1.0f;
+        if constexpr (MIR) {  // reflected fields have reference 0: the mirror value is -phi_parent
+            const unsigned code = loc >> 14;
+            const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
+            const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
 #pragma unroll
-        for (int f = 0; f < NG; f++) {
-            const float sg = f == 1 ? su : f == 2 ? sv : is_xy_slot(FORM, MD, f) ? sxy : 1.0f;
-            d[f] = __fmaf_rn(sg, d[f], -oi[f]);
+            for (int f = 0; f < NG; f++) {
+                const float sg = f == 1 ? su : f == 2 ? sv : is_xy_slot(FORM, MD, f) ? sxy : 1.0f;
+                d[f] = __fmaf_rn(sg, d[f], -oi[f]);
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < NG; f++) d[f] = __fsub_rn(d[f], oi[f]);
         }
         s_ro_x = __fmaf_rn(wx, d[0], s_ro_x);
         s_ro_y = __fmaf_rn(wy, d[0], s_ro_y);
@@ -577,12 +589,11 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
                 break;
             }
             const int np = min(kMxChunk, R.npair - c * kMxChunk);
-            const uint2 *rs = R.ring + (c % kMxDepth) * 3 * kMxChunk * 32;
+            const uint2 *rs = R.ring + (c % kMxDepth) * 3 * kMxChunk * 32 + lane;
 #pragma unroll
             for (int p = 0; p < kMxChunk; p++) {
                 if (p < np) {
-                    const uint2 X = rs[p * 32 + lane], Y = rs[(kMxChunk + p) * 32 + lane];
-                    const uint2 L = rs[(2 * kMxChunk + p) * 32 + lane];
+                    const uint2 X = rs[p * 32], Y = rs[(kMxChunk + p) * 32], L = rs[(2 * kMxChunk + p) * 32];
                     link(X.x, Y.x, L.x);
                     link(X.y, Y.y, L.y);
                 }
@@ -590,7 +601,7 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
             __syncwarp();
             if (lane == 0 && c + kMxDepth < R.nchunk) {
                 fence_proxy_async();
-                R.issue(c + kMxDepth);
+                R.issue(A, c + kMxDepth);
             }
         }
     }
@@ -745,15 +756,13 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
         MxRing R;
         R.ring = reinterpret_cast<uint2 *>(smem) + (size_t)warp * kMxDepth * 3 * kMxChunk * 32;
         R.bar0 = smem_addr(reinterpret_cast<char *>(smem) + mx_ring_bytes() + (size_t)warp * kMxDepth * 8);
-        R.src[0] = A.pkx;
-        R.src[1] = A.pky;
-        R.src[2] = A.pkl;
         R.base = active ? A.slice_ptr[sl] : 0;
         R.npair = active ? A.slice_ws[sl] >> 1 : 0;
         R.nchunk = (R.npair + kMxChunk - 1) / kMxChunk;
         float oi[NG];
         load_halo_mx<FORM, MD, FP>(A, i, smem, R, active, oi);
-        gather_stage_mx<FORM, MD, FP>(A, i, smem, R, active, oi, g);
+        if (cK.has_mirrors) gather_stage_mx<FORM, MD, FP, true>(A, i, smem, R, active, oi, g);
+        else gather_stage_mx<FORM, MD, FP, false>(A, i, smem, R, active, oi, g);
     } else {
         LinkRing<false, 3, ring_depth(false)> R;
         R.src[0] = reinterpret_cast<const double2 *>(A.wx);
@@ -768,7 +777,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
     // a node's own value of gathered field f in the tile's halo slot h (wall Laplacian of c)
     auto hv = [&](int f, int h) -> double {
         if constexpr (MX) {
-            const float2 v = mx_halo(smem, NG)[(f >> 1) * A.hmax + h];
+            const float2 v = mx_halo(smem, NG)[h * mx_words(NG) + (f >> 1)];
             return mx_refs(smem)[f] + (double)((f & 1) ? v.y : v.x);
         } else {
             return smem[f * A.hmax + h];
@@ -1045,6 +1054,185 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
         __syncthreads();
         for (int s = blockDim.x / 2; s > 0; s >>= 1) {
             if ((int)threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            A.sc->dro = cK.mcorr ? red[0] / A.sc->tv : 0.0;
+            A.sc->done_ctr = 0;
+        }
+    }
+}
+
+// The mixed-precision filter: the design of the mixed stage kernel applied to
+// filter_variables (rhs_*.F90 as above).  The tile's halo of the evolved fields as FP32
+// offsets from per-tile FP64 references (AoS words, odd count a node), the link stream (one
+// FP32 weight a link and the 16-bit local index, both in the bank-aware order) moved by bulk
+// copies, and the filter term sum_k w_k (phi_j - phi_i) summed in FP32, added to the node's
+// FP64 value.  Cholesky FENE-P converts the psi factors of J = f c to those of c in FP64
+// before the offsets are taken, and back after the filter.
+constexpr int kMxfChunk = 4;  // link pairs per bulk copy (one weight word and one index word a pair and lane)
+constexpr int kMxfDepth = 2;
+__host__ __device__ constexpr size_t mxf_ring_bytes() { return (size_t)kTileSlices * kMxfDepth * kMxfChunk * 32 * 12; }
+__host__ __device__ constexpr size_t mxf_bar_bytes() { return (size_t)kTileSlices * kMxfDepth * 8; }
+__host__ __device__ inline size_t mxf_smem_bytes(int nf, int hmax) {
+    return mxf_ring_bytes() + mxf_bar_bytes() + (size_t)mx_words(nf) * hmax * 8;
+}
+
+template <int FORM, bool FP>
+__global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
+    extern __shared__ __align__(16) double smem[];
+    constexpr bool CF = FP && FORM == SUNSET_FORM_CHL;
+    constexpr int nf = (FORM == SUNSET_FORM_DI || CF) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
+    constexpr int NP = (nf + 1) / 2, NW = mx_words(nf);
+    const Fields &F = A.in;
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sl = blockIdx.x * kTileSlices + warp;
+    const bool live = sl < cK.nslices;
+    // per warp: kMxfDepth stages of [kMxfChunk pairs][32 lanes] float2 weights, then
+    // [kMxfChunk pairs][32 lanes] index pairs
+    char *ringb = reinterpret_cast<char *>(smem) + (size_t)warp * kMxfDepth * kMxfChunk * 32 * 12;
+    const unsigned bar0 = smem_addr(reinterpret_cast<char *>(smem) + mxf_ring_bytes() + (size_t)warp * kMxfDepth * 8);
+    float2 *hp = reinterpret_cast<float2 *>(reinterpret_cast<char *>(smem) + mxf_ring_bytes() + mxf_bar_bytes());
+    const long long base = live ? A.slice_ptr[sl] : 0;
+    const int npair = live ? A.slice_w[sl] >> 1 : 0, nchunk = (npair + kMxfChunk - 1) / kMxfChunk;
+    auto issue = [&](int c) {
+        const int s = c % kMxfDepth;
+        const int np = min(kMxfChunk, npair - c * kMxfChunk);
+        const unsigned bar = bar0 + 8u * s;
+        const long long o = base + (long long)c * kMxfChunk * 64;
+        char *st = ringb + (size_t)s * kMxfChunk * 32 * 12;
+        mbar_expect_tx(bar, (unsigned)np * 384u);
+        bulk_load(smem_addr(st), A.wh32 + o, (unsigned)np * 256u, bar);
+        bulk_load(smem_addr(st + kMxfChunk * 256), A.lloc + o, (unsigned)np * 128u, bar);
+    };
+    auto wait = [&](int c) { return mbar_wait_bounded(bar0 + 8u * (c % kMxfDepth), (unsigned)(c / kMxfDepth) & 1u); };
+    if (live && lane == 0) {
+        for (int s = 0; s < kMxfDepth; s++) mbar_init(bar0 + 8u * s, 1u);
+        mbar_init_fence();
+        for (int c = 0; c < kMxfDepth && c < nchunk; c++) issue(c);
+    }
+    // halo as offsets (FENE-P Cholesky: psi of c, converted in FP64 first)
+    const bool mir = cK.has_mirrors;
+    const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
+    const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
+    const int n0 = __ldg(A.halo + hb);
+    auto values = [&](int node, double *v) {
+#pragma unroll
+        for (int f = 0; f < nf; f++) v[f] = __ldg(src[f] + node);
+        if constexpr (CF) chl_fenep_to_c_factor(cK.fenep_l2, v[3], v[4], v[5], v[6]);
+    };
+    double rf[nf];
+    values(n0, rf);
+#pragma unroll
+    for (int f = 0; f < nf; f++)
+        if (mir && (f == 1 || f == 2 || f == 4)) rf[f] = 0.0;
+    for (int h = threadIdx.x; h < hn; h += blockDim.x) {
+        double v[nf];
+        values(__ldg(A.halo + hb + h), v);
+#pragma unroll
+        for (int p = 0; p < NP; p++)
+            hp[h * NW + p] = make_float2((float)(v[2 * p] - rf[2 * p]), 2 * p + 1 < nf ? (float)(v[2 * p + 1] - rf[2 * p + 1]) : 0.0f);
+    }
+    double own[7];
+    values(i < cK.npfb ? i : 0, own);
+    float oi[nf];
+#pragma unroll
+    for (int f = 0; f < nf; f++) oi[f] = (float)(own[f] - rf[f]);
+    __syncthreads();
+    float t[nf];
+#pragma unroll
+    for (int f = 0; f < nf; f++) t[f] = 0.0f;
+    auto link = [&](unsigned loc, float w) {
+        const float2 *v = hp + (loc & kLocMask) * NW;
+        float d[2 * NP];
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            const float2 q = v[p];
+            d[2 * p] = q.x;
+            d[2 * p + 1] = q.y;
+        }
+        const unsigned code = mir ? loc >> 14 : 0u;
+        const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
+        const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
+#pragma unroll
+        for (int f = 0; f < nf; f++) {
+            const float sg = f == 1 ? su : f == 2 ? sv : f == 4 ? sxy : 1.0f;
+            t[f] = __fmaf_rn(w, __fmaf_rn(sg, d[f], -oi[f]), t[f]);
+        }
+    };
+    if (live) {
+        for (int c = 0; c < nchunk; c++) {
+            if (!wait(c)) {
+                if (lane == 0) atomicExch(&A.sc->err, 2);
+                for (int c2 = c; c2 < c + kMxfDepth && c2 < nchunk; c2++) wait(c2);
+                break;
+            }
+            const int np = min(kMxfChunk, npair - c * kMxfChunk);
+            const char *st = ringb + (size_t)(c % kMxfDepth) * kMxfChunk * 32 * 12;
+            const float2 *wv = reinterpret_cast<const float2 *>(st) + lane;
+            const unsigned *lv = reinterpret_cast<const unsigned *>(st + kMxfChunk * 256) + lane;
+#pragma unroll
+            for (int p = 0; p < kMxfChunk; p++) {
+                if (p < np) {
+                    const float2 w2 = wv[p * 32];
+                    const unsigned l2 = lv[p * 32];
+                    link(l2 & 0xffffu, w2.x);
+                    link(l2 >> 16, w2.y);
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && c + kMxfDepth < nchunk) {
+                fence_proxy_async();
+                issue(c + kMxfDepth);
+            }
+        }
+    }
+    double part = 0.0;
+    if (live && i < cK.npfb) {
+        double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
+        const bool wall = cK.has_walls && A.ntype[i] == 0;
+        double res[7];
+#pragma unroll
+        for (int f = 0; f < 7; f++) {
+            if (f < nf) {
+                double r = own[f] + (double)t[f];
+                if (wall && (f == 1 || f == 2)) r = 0.0;  // apply_time_dependent_bounds after the filter
+                res[f] = r;
+            }
+        }
+        if constexpr (CF) chl_fenep_to_j_factor(cK.fenep_l2, res[3], res[4], res[5], res[6]);
+#pragma unroll
+        for (int f = 0; f < 7; f++) {
+            if (f < nf) dst[f][i] = res[f];
+            else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = src[f][i];
+        }
+        part = (res[0] - cK.rho_char) * A.vol[i];
+    }
+    // deterministic two-level sum: fixed tree in the block, fixed order over blocks
+    __shared__ double red[kTile];
+    red[threadIdx.x] = part;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if ((int)threadIdx.x < s2) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        A.partials[blockIdx.x] = red[0];
+        __threadfence();
+        unsigned int prev = atomicAdd(&A.sc->done_ctr, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc = acc + ((volatile double *)A.partials)[b];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+            if ((int)threadIdx.x < s2) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s2];
             __syncthreads();
         }
         if (threadIdx.x == 0) {
@@ -1424,7 +1612,7 @@ int stage_smem_attributes(Handle *H, bool mx) {
 template <int FORM, bool FP>
 int filter_smem_attributes(Handle *H, bool mx) {
     SUNSET_SMEM_ATTR((k_filter<FORM, false, FP>));
-    if (mx) SUNSET_SMEM_ATTR((k_filter<FORM, true, FP>));
+    if (mx) SUNSET_SMEM_ATTR((k_filter_mx<FORM, FP>));
     return 0;
 }
 
@@ -1493,17 +1681,17 @@ template <int FORM>
 int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     const bool cf = FORM == SUNSET_FORM_CHL && H->cfg.fenep;  // Cholesky FENE-P: psizz and the conversions
     const int nf = (FORM == SUNSET_FORM_DI || cf) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
-    const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) +
-                        (mx ? LinkRing<true, 1, filter_ring_depth(true)>::bytes()
-                            : LinkRing<false, 1, filter_ring_depth(false)>::bytes());
-    if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-    if (cf) {
-        if (mx) k_filter<FORM, true, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-        else k_filter<FORM, false, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-    } else {
-        if (mx) k_filter<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-        else k_filter<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    if (mx) {
+        const size_t smem = mxf_smem_bytes(nf, H->halo_max);
+        if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
+        if (cf) k_filter_mx<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        else k_filter_mx<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        return 0;
     }
+    const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) + LinkRing<false, 1, filter_ring_depth(false)>::bytes();
+    if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
+    if (cf) k_filter<FORM, false, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+    else k_filter<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
     return 0;
 }
 
@@ -1766,12 +1954,12 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     if (rc) return rc;
     *ms = tot / (4.0 * reps);
     // Algorithmic bytes of one stage launch, averaged over the four stages: each node's
-    // small links once (16-bit local index + 3 weights of 8 bytes, 4 in the mixed path;
-    // links, not padded SELL slots), its state and derived fields read once (the halo
-    // copies of neighbours' values are re-reads), the RK registers S and E read in stages
-    // 1-3 and written in stages 0-2 (8 bytes, 4 in the mixed path), the next state with
-    // its derived fields written (conservative fields only after stage 3), and the stencil
-    // sums and ordinate read.
+    // small links once (16-bit local index + 3 weights of 8 bytes = 26 bytes; 12 in the mixed
+    // path's packed words; links, not padded SELL slots), its state and derived fields read
+    // once (the halo copies of neighbours' values are re-reads), the RK registers S and E
+    // read in stages 1-3 and written in stages 0-2 (8 bytes, 4 in the mixed path), the next
+    // state with its derived fields written (conservative fields only after stage 3), and
+    // the per-node stencil sums (mixed: weight scales) and ordinate read.
     long long links = 0;
     {
         std::vector<int> cs(H->npfb);
@@ -1783,8 +1971,8 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
     const int nread = form == SUNSET_FORM_DI ? 9 : 13;   // state + derived fields of a node
     const int nwrite = form == SUNSET_FORM_DI ? 9 : 13;  // next state + derived fields (stages 0-2)
     const double wb = mx ? 4.0 : 8.0;
-    *bytes = (double)links * (2 + 3 * wb) +
-             (double)H->npfb * (8.0 * nread + 3.0 * nf * wb + 8.0 * (3.0 * nwrite + 7.0) / 4.0 + 8.0 * 4);
+    *bytes = (double)links * (mx ? 12.0 : 2.0 + 3.0 * wb) +
+             (double)H->npfb * (8.0 * nread + 3.0 * nf * wb + 8.0 * (3.0 * nwrite + 7.0) / 4.0 + (mx ? 20.0 : 32.0));
     return 0;
 }
 

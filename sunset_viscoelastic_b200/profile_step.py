@@ -1,6 +1,9 @@
 """Driver for profiler captures of the time-step kernels.
 
-    python -m sunset_viscoelastic_b200.profile_step WORKLOAD [fp64|mixed] [STEPS]
+    python -m sunset_viscoelastic_b200.profile_step WORKLOAD [fp64|mixed] [STEPS] [NSIDE]
+
+NSIDE (periodic workloads) replaces the node set's side, for captures on a smaller set of the
+same order, radius and form.
 
 Sets the workload up (neighbours, weights, link stream), sets the initial state, runs two
 graph-launched steps, then STEPS steps launched kernel by kernel through
@@ -11,6 +14,7 @@ sunset_time_stage_kernel.  Kernel launch order after setup: the two graph steps 
 """
 from __future__ import annotations
 
+import dataclasses
 import sys
 
 from . import labfm
@@ -22,6 +26,8 @@ def main(argv=None) -> int:
     wl = WORKLOADS[argv[0]]
     precision = argv[1] if len(argv) > 1 else "fp64"
     steps = int(argv[2]) if len(argv) > 2 else 3
+    if len(argv) > 3:
+        wl = dataclasses.replace(wl, nside=int(argv[3]))
     ns = wl.nodes()
     g = labfm.for_workload(wl, ns, precision=precision).setup()
     g.set_state(**initial_state(ns))

@@ -1,9 +1,11 @@
 """Mixed precision (SUNSET_MIXED) against the FP64 restatement and the FP64 device path.
 
-The mixed step streams the FP64 weights rounded to FP32 (relative rounding 2^-24 per weight)
-with FP64 stencil sums of the rounded weights, and keeps the RK register as an FP32
-increment over the stage's FP64 state; fields, stencil arithmetic, transforms and
-reductions stay FP64.  The stated tolerance is 1e-6 relative per field after 100 steps,
+The mixed stage streams each weight as a 26-bit fixed-point number scaled per node and
+operator (rounding 2^-25 of the node's largest weight), stages the tile's neighbour values
+as FP32 offsets from a per-tile FP64 reference, sums the stencils in FP32 difference form
+sum_k w_k (phi_j - phi_i), and keeps the RK register as an FP32 increment over the stage's
+FP64 state; the state, the pointwise right-hand sides, transforms and reductions stay FP64.
+The stated tolerance is 1e-6 relative per field after 100 steps,
 with the error of field f measured against the magnitude of the quantity it is a component
 of (rho; the momentum or velocity vector; the conformation tensor):
 
@@ -97,8 +99,10 @@ def test_fields_after_100_steps(runs):
 
 
 def test_rhs(runs):
-    """calc_all_rhs of the mixed handle uses the rounded weights: within the weight rounding
-    times the stencil's conditioning of the FP64 right-hand side."""
+    """calc_all_rhs of the mixed handle uses the mixed stencils: within 1e-4 of the size of
+    the FP64 right-hand side's terms.  The viscous term dominates the difference: the FP32
+    offsets of the neighbour values round at 2^-24 of their spread over a tile, which the
+    Laplacian's O(1/s^2) weights amplify; the field tolerance after 100 steps is the gate."""
     name, wl, ns, ref, f64, mx = runs
     st = initial_state(ns)
     st["cxx"] = 1.0 + 0.3 * np.sin(2 * np.pi * ns.y) ** 2
@@ -115,7 +119,7 @@ def test_rhs(runs):
     for k in ["ro", "rou", "rov", "xx", "xy", "yy"]:
         e = np.abs(rmx[k] - r64[k]).max() / scale[k]
         print(f"{name} rhs_{k}: mixed vs FP64 {e:.2e} (of the terms' size)")
-        assert e <= 1e-5, (k, e)
+        assert e <= 1e-4, (k, e)
 
 
 def test_mixed_pid_steps():
