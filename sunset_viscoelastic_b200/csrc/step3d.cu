@@ -14,10 +14,12 @@
 // value in the same layer, u and v with the mirror's sign, w, c_xz and c_yz unchanged
 // (mirror_boundaries.F90:302-303,324-341).
 //
-// Structure, as calc_all_rhs: one gather kernel for every derivative of every field (x-y LABFM
-// sums in the reference's link order, then the z stencils), then a pointwise kernel for the
-// right-hand side and the RK update; the filter as the x-y filter followed by the z filter of
-// its result (derivatives.F90:387-405); the mass correction and the derived fields; all FP64.
+// Structure: one kernel a stage (k3_stage), as calc_all_rhs and the RK update: each node-layer
+// gathers every derivative of every field (x-y LABFM sums in the reference's link order, then
+// the z stencils) into its block's shared memory, then computes the right-hand side and the RK
+// update from there, so the derivatives never cross HBM; the filter as the x-y filter
+// followed by the z filter of its result (derivatives.F90:387-405); the mass correction and
+// the derived fields; all FP64.
 #include "internal.cuh"
 
 namespace sunset {
@@ -25,10 +27,11 @@ namespace sunset {
 namespace {
 
 constexpr int kMaxFd = 13;
-constexpr int kG3 = 57;  // derivative arrays, see enum G3
+constexpr int kG3 = 57;  // derivative slots, see enum G3
 
 struct Layer3 {
     int nl, nz, ncfd;
+    int nzc;  // > 0: blocks of (warps) nodes x 32 layers, nzc chunks of layers a node (zthread)
     const long long *slice_ptr;
     const int *cnt, *cnt_small, *lidx;
     const double *wx, *wy, *wl, *wh, *gsx, *gsy, *lsum, *hsum;
@@ -58,16 +61,29 @@ __device__ __forceinline__ int zwrap(int l, int nz) {
     return (l >= nz) ? l - nz : l;
 }
 
-// thread k of the node-major layered arrays: node i, layer iz (n < 2^31, checked in layers_set)
+// thread k of the node-major layered arrays: node i, layer iz (n < 2^31, checked in layers_set).
+// With 32 layers or more, a block takes one chunk of 32 layers of consecutive nodes, one node a
+// warp: the warp keeps its broadcast link loads and coalesced layer reads, and the block's
+// nodes, neighbours in the Morton order, share most of their neighbours' values in L1.
+// Otherwise the threads run over the node-layers in order.
 struct ZThread {
     int k, i, iz;
 };
-__device__ __forceinline__ bool zthread(int nl, int nz, ZThread &t) {
+__device__ __forceinline__ bool zthread(const Layer3 &L, ZThread &t) {
+    if (L.nzc > 0) {
+        const int grp = (int)blockIdx.x / L.nzc, zc = (int)blockIdx.x - grp * L.nzc;
+        const int i = grp * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5), iz = zc * 32 + (int)(threadIdx.x & 31);
+        if (i >= L.nl || iz >= L.nz) return false;
+        t.i = i;
+        t.iz = iz;
+        t.k = i * L.nz + iz;
+        return true;
+    }
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= (unsigned)nl * (unsigned)nz) return false;
+    if (k >= (unsigned)L.nl * (unsigned)L.nz) return false;
     t.k = (int)k;
-    t.i = (int)(k / (unsigned)nz);
-    t.iz = (int)k - t.i * nz;
+    t.i = (int)(k / (unsigned)L.nz);
+    t.iz = (int)k - t.i * L.nz;
     return true;
 }
 
@@ -128,13 +144,13 @@ __host__ __device__ constexpr FDesc desc3f(int d) {
 // and run at 4 (128 registers).
 __host__ __device__ constexpr int derivs_min_blocks(int form) { return form == SUNSET_FORM_DI ? 5 : 4; }
 
-template <int FORM, bool MD, bool FULL, bool FEN>
-__global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_derivs(Layer3 L, Fields3 F, double *G) {
+//
+// ST(slot, value) receives each derivative: a global array of the standalone gather, or the
+// fused stage kernel's shared memory.
+template <int FORM, bool MD, bool FULL, bool FEN, class ST>
+__device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, const ZThread &z, ST store) {
     constexpr int N = ndesc3<FORM, MD, FEN>();
     constexpr int LB = 2;
-    ZThread z;
-    if (!zthread(L.nl, L.nz, z)) return;
-    const size_t n = (size_t)L.nl * L.nz;
     const int k = z.k, i = z.i, iz = z.iz, row = i * L.nz, h = L.ncfd / 2;
     double sx[N], sy[N], sl[N];
 #pragma unroll
@@ -190,8 +206,8 @@ __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_derivs(Layer3
     for (int d = 0; d < N; d++) {
         const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
         const double p = F.p[D.f][k];
-        if (D.gx >= 0) G[(size_t)D.gx * n + k] = sx[d] - p * L.gsx[i];
-        if (D.gy >= 0) G[(size_t)D.gy * n + k] = sy[d] - p * L.gsy[i];
+        if (D.gx >= 0) store(D.gx, sx[d] - p * L.gsx[i]);
+        if (D.gy >= 0) store(D.gy, sy[d] - p * L.gsy[i]);
         if (D.gl >= 0) sl[d] = sl[d] - p * L.lsum[i];
     }
     // the z stencils, point by point over all fields (each field's sums still run in point order)
@@ -213,10 +229,47 @@ __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_derivs(Layer3
 #pragma unroll
     for (int d = 0; d < N; d++) {
         const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
-        if (D.gl >= 0) G[(size_t)D.gl * n + k] = sl[d] + tl[d];
-        if (D.gz >= 0) G[(size_t)D.gz * n + k] = tg[d];
+        if (D.gl >= 0) store(D.gl, sl[d] + tl[d]);
+        if (D.gz >= 0) store(D.gz, tg[d]);
     }
 }
+
+// The derivative slots a form's gather writes, numbered compactly (-1: not written; the
+// right-hand side then reads zero, as from the zeroed global arrays).
+template <int FORM, bool MD, bool FULL, bool FEN>
+__host__ __device__ constexpr int gslot(int slot) {
+    int idx = 0;
+    for (int s2 = 0; s2 < kG3; s2++) {
+        bool used = false;
+        for (int d = 0; d < ndesc3<FORM, MD, FEN>(); d++) {
+            const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
+            if (D.gx == s2 || D.gy == s2 || D.gl == s2 || D.gz == s2) used = true;
+        }
+        if (s2 == slot) return used ? idx : -1;
+        if (used) idx++;
+    }
+    return -1;
+}
+template <int FORM, bool MD, bool FULL, bool FEN>
+__host__ __device__ constexpr int ngslots() {
+    int c = 0;
+    for (int s2 = 0; s2 < kG3; s2++) c += gslot<FORM, MD, FULL, FEN>(s2) >= 0 ? 1 : 0;
+    return c;
+}
+// gslot as a table in constant memory, built at compile time: a slot index the compiler folds
+// is an immediate constant operand, one it cannot fold a single constant-bank load instead of
+// gslot's loops
+struct GTable {
+    signed char idx[kG3];
+};
+template <int FORM, bool MD, bool FULL, bool FEN>
+__host__ __device__ constexpr GTable make_gtable() {
+    GTable t{};
+    for (int a = 0; a < kG3; a++) t.idx[a] = (signed char)gslot<FORM, MD, FULL, FEN>(a);
+    return t;
+}
+template <int FORM, bool MD, bool FULL, bool FEN>
+__constant__ GTable kGTable = make_gtable<FORM, MD, FULL, FEN>();
 
 // calc_filtered_var in 3-D for the NF evolved fields (ro, rou, rov, row, then the six c or psi
 // variables) in one pass over each node's links: the x-y filter of every field into its
@@ -231,7 +284,7 @@ __host__ __device__ constexpr int filter_cls(int q) { return q == 1 ? 1 : q == 2
 template <int NF>
 __global__ void __launch_bounds__(128) k3_filter_xy(Layer3 L, Filter3 A) {
     ZThread z;
-    if (!zthread(L.nl, L.nz, z)) return;
+    if (!zthread(L, z)) return;
     const int k = z.k, i = z.i, iz = z.iz;
     const long long base = L.slice_ptr[i >> 5];
     double t[NF];
@@ -259,7 +312,7 @@ __global__ void __launch_bounds__(128) k3_filter_xy(Layer3 L, Filter3 A) {
 template <int NF>
 __global__ void __launch_bounds__(128) k3_filter_z(Layer3 L, Filter3 A) {
     ZThread z;
-    if (!zthread(L.nl, L.nz, z)) return;
+    if (!zthread(L, z)) return;
     const int k = z.k, iz = z.iz, row = z.i * L.nz, h = L.ncfd / 2;
     double t[NF];
 #pragma unroll
@@ -278,7 +331,6 @@ struct Point3 {
     StepConsts K;
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
-    const double *G;                      // kG3 derivative arrays
     const double *fen;                    // FENE-P function of the direct form, or null
     int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
@@ -445,16 +497,15 @@ __device__ __forceinline__ void chl3_psi_from_c(const double *c, double *p) {
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
 // 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).
-template <int FORM>
-__global__ void __launch_bounds__(128) k3_point(Point3 P) {
+//
+// GET(slot) returns derivative `slot` of node-layer k (global arrays, or the fused kernel's
+// shared memory); the bits of the node-layer's step error norm are returned (stage 3).
+template <int FORM, class GET>
+__device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_t k, GET g) {
     constexpr bool kDi = FORM == SUNSET_FORM_DI, kChl = FORM == SUNSET_FORM_CHL, kLc = FORM == SUNSET_FORM_LC;
-    const size_t n = (size_t)P.nl * P.nz;
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long eb = 0;
-    if (k < n) {
+    {
         const StepConsts &K = P.K;
-        const double *G = P.G;
-        auto g = [&](int a) { return G[(size_t)a * n + k]; };
         const int i = (int)((unsigned)k / (unsigned)P.nz);
         const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
         const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
@@ -680,20 +731,46 @@ __global__ void __launch_bounds__(128) k3_point(Point3 P) {
             }
         }
     }
-    if (P.stage == 3) {  // block max, then one atomic
-        __shared__ unsigned long long sm[4];
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long t = __shfl_down_sync(0xffffffffu, eb, o);
-            eb = t > eb ? t : eb;
-        }
-        if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = eb;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long m = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = sm[w] > m ? sm[w] : m;
-            if (m) atomicMax(&P.sc->emax_bits, m);
-        }
+    return eb;
+}
+
+// block maximum of the step error bits, then one atomic (stage 3; all threads of the block)
+__device__ __forceinline__ void block_emax3(unsigned long long eb, DevScalars *sc) {
+    __shared__ unsigned long long sm[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_down_sync(0xffffffffu, eb, o);
+        eb = t > eb ? t : eb;
     }
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = eb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = sm[w] > m ? sm[w] : m;
+        if (m) atomicMax(&sc->emax_bits, m);
+    }
+}
+
+// One stage fused: the derivatives of node-layer k (derivs3_body) go to this block's shared
+// memory, compact slots of 128 doubles (one per thread), and the pointwise right-hand side
+// and RK update (point3_body) read them there, so no derivative array crosses HBM.
+template <int FORM, bool MD, bool FULL, bool FEN>
+__global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_stage(Layer3 L, Fields3 F, Point3 P) {
+    constexpr int NS = ngslots<FORM, MD, FULL, FEN>();
+    __shared__ double sg[NS * 128];
+    ZThread z;
+    const bool live = zthread(L, z);
+    unsigned long long eb = 0;
+    if (live) {
+        derivs3_body<FORM, MD, FULL, FEN>(L, F, z, [&](int slot, double v) {
+            const int c = kGTable<FORM, MD, FULL, FEN>.idx[slot];
+            if (c >= 0) sg[c * 128 + threadIdx.x] = v;
+        });
+        eb = point3_body<FORM>(P, (size_t)z.k, [&](int a) {
+            const int c = kGTable<FORM, MD, FULL, FEN>.idx[a];
+            return c >= 0 ? sg[c * 128 + threadIdx.x] : 0.0;
+        });
+    }
+    if (P.stage == 3) block_emax3(eb, P.sc);
 }
 
 // Block sums of (rho - rho_char) vol (or of vol), in a fixed tree; folded in block order.
@@ -905,6 +982,7 @@ Layer3 layer3(const Handle *H) {
     L.nl = H->npfb;
     L.nz = H->nz;
     L.ncfd = H->ncfd;
+    L.nzc = H->nz >= 32 ? (H->nz + 31) / 32 : 0;
     L.slice_ptr = H->slice_ptr;
     L.cnt = H->cnt;
     L.cnt_small = H->cnt_small;
@@ -917,45 +995,16 @@ Layer3 layer3(const Handle *H) {
 
 inline size_t n3(const Handle *H) { return (size_t)H->npfb * H->nz; }
 inline unsigned nblk(size_t n) { return (unsigned)((n + 127) / 128); }
+// blocks of 128 threads over the node-layers in zthread's order
+inline unsigned zblocks(const Handle *H) {
+    if (H->nz >= 32) return (unsigned)(((H->npfb + 3) / 4) * ((H->nz + 31) / 32));
+    return nblk(n3(H));
+}
 
 // FENE-P function of every node-layer (rhs_di.F90:201-203), into the staging array
 __global__ void k3_fenep(unsigned n, const double *cxx, const double *cyy, const double *czz, double L2, double *f) {
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) f[k] = (L2 - 3.0) / (L2 - ((cxx[k] + cyy[k]) + czz[k]));
-}
-
-// all the derivatives the right-hand side reads, of buffer b
-template <int FORM, bool MD, bool FULL, bool FEN = false>
-int derivs3_launch(Handle *H, int b) {
-    const size_t n = n3(H);
-    Fields3 F{};
-    for (int q = 0; q < 19; q++) F.p[q] = H->f3[b][q];
-    if (FEN) {
-        k3_fenep<<<nblk(n), 128, 0, H->stream>>>((unsigned)n, H->f3[b][7], H->f3[b][9], H->f3[b][12], H->cfg.fenep_l2, H->tmp3);
-        F.p[19] = H->tmp3;
-    }
-    k3_derivs<FORM, MD, FULL, FEN><<<nblk(n), 128, 0, H->stream>>>(layer3(H), F, H->g3);
-    SUNSET_CUDA(H, cudaGetLastError());
-    return 0;
-}
-int derivs3(Handle *H, int b) {
-    const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0;
-    switch (H->cfg.form) {
-    case SUNSET_FORM_DI:
-        if (H->cfg.fenep) {
-            if (md)
-                return full ? derivs3_launch<SUNSET_FORM_DI, true, true, true>(H, b)
-                            : derivs3_launch<SUNSET_FORM_DI, true, false, true>(H, b);
-            return full ? derivs3_launch<SUNSET_FORM_DI, false, true, true>(H, b)
-                        : derivs3_launch<SUNSET_FORM_DI, false, false, true>(H, b);
-        }
-        if (md) return full ? derivs3_launch<SUNSET_FORM_DI, true, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, true, false>(H, b);
-        return full ? derivs3_launch<SUNSET_FORM_DI, false, true>(H, b) : derivs3_launch<SUNSET_FORM_DI, false, false>(H, b);
-    case SUNSET_FORM_CHL:
-        return md ? derivs3_launch<SUNSET_FORM_CHL, true, false>(H, b) : derivs3_launch<SUNSET_FORM_CHL, false, false>(H, b);
-    case SUNSET_FORM_LC: return derivs3_launch<SUNSET_FORM_LC, false, false>(H, b);
-    default: return derivs3_launch<SUNSET_FORM_NEWT, false, false>(H, b);
-    }
 }
 
 Point3 point3(Handle *H, int b, int stage) {
@@ -969,7 +1018,6 @@ Point3 point3(Handle *H, int b, int stage) {
     P.full = H->cfg.di_full_gradients;
     P.md = H->cfg.Mdiff != 0.0;
     P.py = H->py;
-    P.G = H->g3;
     P.fen = (H->cfg.form == SUNSET_FORM_DI && H->cfg.fenep) ? H->tmp3 : nullptr;
     for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
@@ -981,17 +1029,38 @@ Point3 point3(Handle *H, int b, int stage) {
     return P;
 }
 
-// the pointwise right-hand side and RK update of the handle's form
-int point3_launch(Handle *H, const Point3 &P, cudaStream_t st) {
-    const unsigned nb = nblk(n3(H));
-    switch (H->cfg.form) {
-    case SUNSET_FORM_DI: k3_point<SUNSET_FORM_DI><<<nb, 128, 0, st>>>(P); break;
-    case SUNSET_FORM_CHL: k3_point<SUNSET_FORM_CHL><<<nb, 128, 0, st>>>(P); break;
-    case SUNSET_FORM_LC: k3_point<SUNSET_FORM_LC><<<nb, 128, 0, st>>>(P); break;
-    default: k3_point<SUNSET_FORM_NEWT><<<nb, 128, 0, st>>>(P); break;
+// One fused stage (k3_stage) of buffer b: derivatives, right-hand side and RK update
+template <int FORM, bool MD, bool FULL, bool FEN = false>
+int stage3_launch(Handle *H, int b, int stage) {
+    const size_t n = n3(H);
+    Fields3 F{};
+    for (int q = 0; q < 19; q++) F.p[q] = H->f3[b][q];
+    if (FEN) {
+        k3_fenep<<<nblk(n), 128, 0, H->stream>>>((unsigned)n, H->f3[b][7], H->f3[b][9], H->f3[b][12], H->cfg.fenep_l2, H->tmp3);
+        F.p[19] = H->tmp3;
     }
+    k3_stage<FORM, MD, FULL, FEN><<<zblocks(H), 128, 0, H->stream>>>(layer3(H), F, point3(H, b, stage));
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
+}
+int stage3(Handle *H, int b, int stage) {
+    const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0;
+    switch (H->cfg.form) {
+    case SUNSET_FORM_DI:
+        if (H->cfg.fenep) {
+            if (md)
+                return full ? stage3_launch<SUNSET_FORM_DI, true, true, true>(H, b, stage)
+                            : stage3_launch<SUNSET_FORM_DI, true, false, true>(H, b, stage);
+            return full ? stage3_launch<SUNSET_FORM_DI, false, true, true>(H, b, stage)
+                        : stage3_launch<SUNSET_FORM_DI, false, false, true>(H, b, stage);
+        }
+        if (md) return full ? stage3_launch<SUNSET_FORM_DI, true, true>(H, b, stage) : stage3_launch<SUNSET_FORM_DI, true, false>(H, b, stage);
+        return full ? stage3_launch<SUNSET_FORM_DI, false, true>(H, b, stage) : stage3_launch<SUNSET_FORM_DI, false, false>(H, b, stage);
+    case SUNSET_FORM_CHL:
+        return md ? stage3_launch<SUNSET_FORM_CHL, true, false>(H, b, stage) : stage3_launch<SUNSET_FORM_CHL, false, false>(H, b, stage);
+    case SUNSET_FORM_LC: return stage3_launch<SUNSET_FORM_LC, false, false>(H, b, stage);
+    default: return stage3_launch<SUNSET_FORM_NEWT, false, false>(H, b, stage);
+    }
 }
 
 int tstep3_launch(Handle *H, int b, int pid) {
@@ -1051,8 +1120,8 @@ static int state3_alloc(Handle *H) {
             if (dalloc(H, &H->f3[b][f], n)) return SUNSET_ERR_NOMEM;
     for (int q = 0; q < 10; q++)
         if (dalloc(H, &H->reg3[q], n) || dalloc(H, &H->eacc3[q], n) || dalloc(H, &H->rhs3[q], n)) return SUNSET_ERR_NOMEM;
-    if (dalloc(H, &H->g3, (size_t)kG3 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
-    SUNSET_CUDA(H, cudaMemsetAsync(H->g3, 0, (size_t)kG3 * n * sizeof(double), H->stream));
+    // g3: the x-y filtered values of the ten evolved fields (the derivatives stay on chip)
+    if (dalloc(H, &H->g3, (size_t)10 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
     for (int b = 0; b < 2; b++)
         for (int f = 7; f < 19; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
     const unsigned nb = nblk(n);
@@ -1117,10 +1186,7 @@ int state3_get(Handle *H, double *out19) {
 // out10: the right-hand sides ro rou rov row xx xy yy xz yz zz, reference layer-major, host
 int rhs3_calc(Handle *H, double *out10) {
     const size_t n = n3(H);
-    if (int rc = derivs3(H, H->cur3)) return rc;
-    Point3 P = point3(H, H->cur3, 4);
-    if (int rc = point3_launch(H, P, H->stream)) return rc;
-    SUNSET_CUDA(H, cudaGetLastError());
+    if (int rc = stage3(H, H->cur3, 4)) return rc;
     for (int q = 0; q < 10; q++) {
         k3_scatter<<<nblk(n), 128, 0, H->stream>>>(H->rhs3[q], H->perm, H->npfb, H->nz, n, H->tmp3);
         SUNSET_CUDA(H, cudaMemcpyAsync(out10 + (size_t)q * n, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
@@ -1146,10 +1212,8 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
         int b = H->cur3;
         for (int stage = 0; stage < 4; stage++) {
             if (ev) SUNSET_CUDA(H, cudaEventRecord(ev[8 * s + 2 * stage], st));
-            if (int rc = derivs3(H, b)) return rc;
+            if (int rc = stage3(H, b, stage)) return rc;
             if (ev) SUNSET_CUDA(H, cudaEventRecord(ev[8 * s + 2 * stage + 1], st));
-            Point3 P = point3(H, b, stage);
-            if (int rc = point3_launch(H, P, st)) return rc;
             b ^= 1;
         }
         // filter_variables: ro rou rov row, then c (rhs_di.F90:667-694) or psi (rhs.F90:792-840);
@@ -1163,11 +1227,11 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
             FA.t[q] = H->g3 + (size_t)q * n;
         }
         if (evolves_c) {
-            k3_filter_xy<10><<<nblk(n), 128, 0, st>>>(L, FA);
-            k3_filter_z<10><<<nblk(n), 128, 0, st>>>(L, FA);
+            k3_filter_xy<10><<<zblocks(H), 128, 0, st>>>(L, FA);
+            k3_filter_z<10><<<zblocks(H), 128, 0, st>>>(L, FA);
         } else {
-            k3_filter_xy<4><<<nblk(n), 128, 0, st>>>(L, FA);
-            k3_filter_z<4><<<nblk(n), 128, 0, st>>>(L, FA);
+            k3_filter_xy<4><<<zblocks(H), 128, 0, st>>>(L, FA);
+            k3_filter_z<4><<<zblocks(H), 128, 0, st>>>(L, FA);
         }
         k3_mass_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][0], H->vol, 1.0, 0, H->partials3);
         k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
@@ -1180,37 +1244,6 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
     return tstep3_launch(H, H->cur3, 0);
 }
 
-
-// fields read and derivative arrays written by one k3_derivs launch of the handle's form
-template <int FORM, bool MD, bool FULL, bool FEN = false>
-void derivs3_io(int &nf, int &ng) {
-    nf = ndesc3<FORM, MD, FEN>();
-    ng = 0;
-    for (int d = 0; d < nf; d++) {
-        const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
-        ng += (D.gx >= 0) + (D.gy >= 0) + (D.gl >= 0) + (D.gz >= 0);
-    }
-}
-static void derivs3_counts(const Handle *H, int &nf, int &ng) {
-    const bool md = H->cfg.Mdiff != 0.0, full = H->cfg.di_full_gradients != 0, fen = H->cfg.fenep != 0;
-    switch (H->cfg.form) {
-    case SUNSET_FORM_DI:
-        if (fen) {
-            if (md) full ? derivs3_io<SUNSET_FORM_DI, true, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, true, false, true>(nf, ng);
-            else full ? derivs3_io<SUNSET_FORM_DI, false, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, false, false, true>(nf, ng);
-        } else if (md) {
-            full ? derivs3_io<SUNSET_FORM_DI, true, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, true, false>(nf, ng);
-        } else {
-            full ? derivs3_io<SUNSET_FORM_DI, false, true>(nf, ng) : derivs3_io<SUNSET_FORM_DI, false, false>(nf, ng);
-        }
-        break;
-    case SUNSET_FORM_CHL:
-        md ? derivs3_io<SUNSET_FORM_CHL, true, false>(nf, ng) : derivs3_io<SUNSET_FORM_CHL, false, false>(nf, ng);
-        break;
-    case SUNSET_FORM_LC: derivs3_io<SUNSET_FORM_LC, false, false>(nf, ng); break;
-    default: derivs3_io<SUNSET_FORM_NEWT, false, false>(nf, ng); break;
-    }
-}
 
 int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
     if (reps < 1) reps = 1;
@@ -1229,19 +1262,26 @@ int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
     for (auto &e : ev) cudaEventDestroy(e);
     if (rc) return rc;
     *ms = tot / (4.0 * reps);
-    // Algorithmic bytes of one launch: every gathered field read once and every derivative
-    // array written once (8 bytes a node-layer each), the layer's small links once (a 4-byte
-    // index and three 8-byte weights; all layers share them) and the three stencil sums of
-    // each node of the layer.
-    int nf = 0, ng = 0;
-    derivs3_counts(H, nf, ng);
+    // Algorithmic bytes of one fused stage launch (k3_stage), averaged over the four stages:
+    // the state fields the stage reads (gathered or pointwise, 8 bytes a node-layer each) once,
+    // the next state and its derived fields written once, the RK registers S and E of the ten
+    // evolved fields read in stages 1-3 and written in stages 0-2, the FENE-P function of the
+    // direct form read once, the layer's small links once (a 4-byte index and three 8-byte
+    // weights; all layers share them) with the three stencil sums and the ordinate of each
+    // node of the layer.  Neighbours' values re-read through the caches are not counted.
+    const int form = H->cfg.form;
+    const int nread = form == SUNSET_FORM_DI ? 13 : form == SUNSET_FORM_NEWT ? 7 : 19;
+    const int nwrite = form == SUNSET_FORM_DI ? 13 : form == SUNSET_FORM_NEWT ? 7 : 19;
+    const int nevo = form == SUNSET_FORM_NEWT ? 4 : 10;
     long long links = 0;
     {
         std::vector<int> cs(H->npfb);
         SUNSET_CUDA(H, cudaMemcpy(cs.data(), H->cnt_small, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
         for (int c : cs) links += c;
     }
-    *bytes = (double)n3(H) * 8.0 * (nf + ng) + (double)links * 28.0 + (double)H->npfb * 24.0;
+    const double fen = (form == SUNSET_FORM_DI && H->cfg.fenep) ? 8.0 : 0.0;
+    *bytes = (double)n3(H) * (8.0 * (nread + nwrite) + 16.0 * nevo * 6.0 / 4.0 + fen) + (double)links * 28.0 +
+             (double)H->npfb * 32.0;
     return 0;
 }
 
