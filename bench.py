@@ -472,14 +472,27 @@ def stage_roofline(g, wl, precision, steps):
             "method": f"CUDA events around the 4 back-to-back stage launches of each of {roof_steps} steps, / 4"}
 
 
-def built_handle(wl, ns, precision, local):
+def built_handle(wl, ns, precision, local, phases=None):
     """A handle through the setup calls (sunset.F90:51-60); returns it and the wall seconds of
-    the setup (neighbour search, weights, sums, filter coefficients, link streams)."""
+    the setup (neighbour search, weights, sums, filter coefficients, link streams).  phases
+    (a dict), if given, receives the seconds of each call."""
     from sunset_viscoelastic_b200 import labfm
+    t0 = time.perf_counter()
+    g = labfm.for_workload(wl, ns, precision=precision, device=local)
+    calls = [("build_domain", None), ("find_neighbours", g.find_neighbours), ("calc_labf_weights", g.calc_labf_weights),
+             ("calc_boundary_weights", g.calc_boundary_weights), ("calc_labf_sums", g.calc_labf_sums),
+             ("filter_coefficients (+ link streams)", g.filter_coefficients)]
     t = time.perf_counter()
-    g = labfm.for_workload(wl, ns, precision=precision, device=local).setup()
-    g.synchronize()
-    return g, time.perf_counter() - t
+    if phases is not None:
+        phases["build_domain"] = t - t0
+    for name, fn in calls[1:]:
+        fn()
+        g.synchronize()
+        t2 = time.perf_counter()
+        if phases is not None:
+            phases[name] = t2 - t
+        t = t2
+    return g, time.perf_counter() - t0
 
 
 def timed_steps(g, dt, args, dist, local):
@@ -494,7 +507,7 @@ def timed_steps(g, dt, args, dist, local):
     return max_over_ranks(dist, ms, device=f"cuda:{local}"), clk.summary()
 
 
-def setup_block(wl, nodes, device_s):
+def setup_block(wl, nodes, device_s, phases):
     """The device setup against the CPU restatement's setup (neighbour search, weights, sums,
     filter coefficients) on a bounded sample: the same order and radius on a 192 x 192 set."""
     import dataclasses
@@ -507,7 +520,7 @@ def setup_block(wl, nodes, device_s):
     o = O.for_workload(sub, sns).setup()
     el = time.perf_counter() - t
     del o
-    return {"device_s": device_s, "device_nodes_per_s": nodes / device_s,
+    return {"device_s": device_s, "device_nodes_per_s": nodes / device_s, "device_phases_s": phases,
             "cpu_nodes_per_s": sns.n / el, "cpu_cores": cpu_threads(), "cpu_kind": "port",
             "cpu_sample": f"the restatement's setup of {sns.n} nodes at the same order and radius ({el:.2f} s)",
             "note": "wall seconds through the C-ABI setup calls, host-side link ordering included"}
@@ -555,7 +568,8 @@ def main():
     dist = init_pg(ws, "nccl")
     wl = WORKLOADS[args.workload]
     ns = wl.nodes()
-    g, setup_s = built_handle(wl, ns, args.precision, local)
+    phases = {}
+    g, setup_s = built_handle(wl, ns, args.precision, local, phases)
     g.set_state(**wl.initial(ns))
     nodes = g.sizes()[1]  # npfb: the reader's node list, FD rows of boundary nodes included
     dtc, dtp = g.set_tstep()
@@ -625,7 +639,7 @@ def main():
             line["mixed"]["error_vs_fp64"] = mixed_error(wl, ns, gm, dt, args.error_steps, local, ref=g)
         gm.close()
     if extra and not args.no_setup:
-        line["setup"] = setup_block(wl, nodes, setup_s)
+        line["setup"] = setup_block(wl, nodes, setup_s, phases)
     g.close()
     if extra and not args.no_adjoint:
         awl = WORKLOADS[ADJOINT_WORKLOAD]

@@ -513,70 +513,53 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
     const int lane = threadIdx.x & 31;
     const float2 *hp = mx_halo(const_cast<double *>(smem), NG);
     const bool full = (FORM == SUNSET_FORM_DI) && cK.di_full;
-    float s_ro_x = 0, s_ro_y = 0, s_u_x = 0, s_u_y = 0, s_v_x = 0, s_v_y = 0, s_lu = 0, s_lv = 0;
-    float s_cxx_x = 0, s_cxx_y = 0, s_cxy_x = 0, s_cxy_y = 0, s_cyy_x = 0, s_cyy_y = 0;
-    float s_pxx_x = 0, s_pxx_y = 0, s_pxy_x = 0, s_pxy_y = 0, s_pyy_x = 0, s_pyy_y = 0;
-    float s_lxx = 0, s_lxy = 0, s_lyy = 0;
-    float s_f_x = 0, s_f_y = 0, s_lzz = 0;
+    // the x and y sums of every gathered field, two fields to a float2 (the halo's pairs), so
+    // the differences and both sums run as paired FP32 instructions (FADD2, FFMA2); the
+    // Laplacians the right-hand side reads as scalars
+    float2 ax[NP], ay[NP], noi[NP];
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+        ax[p] = make_float2(0.0f, 0.0f);
+        ay[p] = make_float2(0.0f, 0.0f);
+        noi[p] = make_float2(-oi[2 * p], 2 * p + 1 < NG ? -oi[2 * p + 1] : 0.0f);
+    }
+    float s_lu = 0, s_lv = 0, s_lxx = 0, s_lxy = 0, s_lyy = 0, s_lzz = 0;
+    auto comp = [](const float2 *a, int f) { return (f & 1) ? a[f >> 1].y : a[f >> 1].x; };
     auto link = [&](unsigned x, unsigned y, unsigned l) {
         const unsigned loc = (x & 63u) | ((y & 63u) << 6) | ((l & 15u) << 12);
         const float wx = (float)(int)(x & ~63u), wy = (float)(int)(y & ~63u), wl = (float)(int)(l & ~63u);
         const float2 *v = hp + (loc & kLocMask) * NW;
-        float d[2 * NP];
-#pragma unroll
-        for (int p = 0; p < NP; p++) {
-            const float2 q = v[p];
-            d[2 * p] = q.x;
-            d[2 * p + 1] = q.y;
-        }
+        float2 dp[NP];
         if constexpr (MIR) {  // reflected fields have reference 0: the mirror value is -phi_parent
             const unsigned code = loc >> 14;
             const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
             const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
 #pragma unroll
-            for (int f = 0; f < NG; f++) {
-                const float sg = f == 1 ? su : f == 2 ? sv : is_xy_slot(FORM, MD, f) ? sxy : 1.0f;
-                d[f] = __fmaf_rn(sg, d[f], -oi[f]);
+            for (int p = 0; p < NP; p++) {
+                const float2 q = v[p];
+                const int f0 = 2 * p, f1 = 2 * p + 1;
+                const float s0 = f0 == 1 ? su : f0 == 2 ? sv : is_xy_slot(FORM, MD, f0) ? sxy : 1.0f;
+                const float s1 = f1 == 1 ? su : f1 == 2 ? sv : is_xy_slot(FORM, MD, f1) ? sxy : 1.0f;
+                dp[p] = __ffma2_rn(make_float2(s0, s1), q, noi[p]);
             }
         } else {
 #pragma unroll
-            for (int f = 0; f < NG; f++) d[f] = __fsub_rn(d[f], oi[f]);
+            for (int p = 0; p < NP; p++) dp[p] = __fadd2_rn(v[p], noi[p]);
         }
-        s_ro_x = __fmaf_rn(wx, d[0], s_ro_x);
-        s_ro_y = __fmaf_rn(wy, d[0], s_ro_y);
-        s_u_x = __fmaf_rn(wx, d[1], s_u_x);
-        s_u_y = __fmaf_rn(wy, d[1], s_u_y);
-        s_lu = __fmaf_rn(wl, d[1], s_lu);
-        s_v_x = __fmaf_rn(wx, d[2], s_v_x);
-        s_v_y = __fmaf_rn(wy, d[2], s_v_y);
-        s_lv = __fmaf_rn(wl, d[2], s_lv);
-        if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {  // c in slots 3, 4, 5
-            s_cxx_x = __fmaf_rn(wx, d[3], s_cxx_x);
-            if (full) s_cxx_y = __fmaf_rn(wy, d[3], s_cxx_y);
-            s_cxy_x = __fmaf_rn(wx, d[4], s_cxy_x);
-            s_cxy_y = __fmaf_rn(wy, d[4], s_cxy_y);
-            if (full) s_cyy_x = __fmaf_rn(wx, d[5], s_cyy_x);
-            s_cyy_y = __fmaf_rn(wy, d[5], s_cyy_y);
+        const float2 wx2 = make_float2(wx, wx), wy2 = make_float2(wy, wy);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            ax[p] = __ffma2_rn(wx2, dp[p], ax[p]);
+            ay[p] = __ffma2_rn(wy2, dp[p], ay[p]);
         }
-        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {  // psi in slots 6-8 (LC) or 3-5 (CHL)
-            constexpr int q = FORM == SUNSET_FORM_LC ? 6 : 3;
-            s_pxx_x = __fmaf_rn(wx, d[q], s_pxx_x);
-            s_pxx_y = __fmaf_rn(wy, d[q], s_pxx_y);
-            s_pxy_x = __fmaf_rn(wx, d[q + 1], s_pxy_x);
-            s_pxy_y = __fmaf_rn(wy, d[q + 1], s_pxy_y);
-            s_pyy_x = __fmaf_rn(wx, d[q + 2], s_pyy_x);
-            s_pyy_y = __fmaf_rn(wy, d[q + 2], s_pyy_y);
-        }
+        s_lu = __fmaf_rn(wl, comp(dp, 1), s_lu);
+        s_lv = __fmaf_rn(wl, comp(dp, 2), s_lv);
         if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) {  // c in slots 3-5 (DI) or 6-8 (CHL)
             constexpr int q = FORM == SUNSET_FORM_DI ? 3 : 6;
-            s_lxx = __fmaf_rn(wl, d[q], s_lxx);
-            s_lxy = __fmaf_rn(wl, d[q + 1], s_lxy);
-            s_lyy = __fmaf_rn(wl, d[q + 2], s_lyy);
-        }
-        if constexpr (FP && FORM != SUNSET_FORM_NEWT) {
-            s_f_x = __fmaf_rn(wx, d[kFp], s_f_x);
-            s_f_y = __fmaf_rn(wy, d[kFp], s_f_y);
-            if (MD && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_CHL)) s_lzz = __fmaf_rn(wl, d[kFp + 1], s_lzz);
+            s_lxx = __fmaf_rn(wl, comp(dp, q), s_lxx);
+            s_lxy = __fmaf_rn(wl, comp(dp, q + 1), s_lxy);
+            s_lyy = __fmaf_rn(wl, comp(dp, q + 2), s_lyy);
+            if (FP) s_lzz = __fmaf_rn(wl, comp(dp, kFp + 1), s_lzz);
         }
     };
     if (wact) {
@@ -605,34 +588,43 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
     }
     if (i >= cK.npfb) return;
     const double cx = (double)A.scx[i], cy = (double)A.scy[i], cl = (double)A.scl[i];
-    g.ro_x = (double)s_ro_x * cx;
-    g.ro_y = (double)s_ro_y * cy;
-    g.u_x = (double)s_u_x * cx;
-    g.u_y = (double)s_u_y * cy;
+    auto X = [&](int f) { return (double)comp(ax, f) * cx; };
+    auto Y = [&](int f) { return (double)comp(ay, f) * cy; };
+    g.ro_x = X(0);
+    g.ro_y = Y(0);
+    g.u_x = X(1);
+    g.u_y = Y(1);
     g.lapu = (double)s_lu * cl;
-    g.v_x = (double)s_v_x * cx;
-    g.v_y = (double)s_v_y * cy;
+    g.v_x = X(2);
+    g.v_y = Y(2);
     g.lapv = (double)s_lv * cl;
-    g.cxx_x = (double)s_cxx_x * cx;
-    g.cxx_y = (double)s_cxx_y * cy;
-    g.cxy_x = (double)s_cxy_x * cx;
-    g.cxy_y = (double)s_cxy_y * cy;
-    g.cyy_x = (double)s_cyy_x * cx;
-    g.cyy_y = (double)s_cyy_y * cy;
-    g.pxx_x = (double)s_pxx_x * cx;
-    g.pxx_y = (double)s_pxx_y * cy;
-    g.pxy_x = (double)s_pxy_x * cx;
-    g.pxy_y = (double)s_pxy_y * cy;
-    g.pyy_x = (double)s_pyy_x * cx;
-    g.pyy_y = (double)s_pyy_y * cy;
+    g.cxx_x = g.cxx_y = g.cxy_x = g.cxy_y = g.cyy_x = g.cyy_y = 0.0;
+    g.pxx_x = g.pxx_y = g.pxy_x = g.pxy_y = g.pyy_x = g.pyy_y = 0.0;
+    if (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC) {  // c in slots 3, 4, 5
+        g.cxx_x = X(3);
+        g.cxx_y = full ? Y(3) : 0.0;
+        g.cxy_x = X(4);
+        g.cxy_y = Y(4);
+        g.cyy_x = full ? X(5) : 0.0;
+        g.cyy_y = Y(5);
+    }
+    if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) {  // psi in slots 6-8 (LC) or 3-5 (CHL)
+        constexpr int q = FORM == SUNSET_FORM_LC ? 6 : 3;
+        g.pxx_x = X(q);
+        g.pxx_y = Y(q);
+        g.pxy_x = X(q + 1);
+        g.pxy_y = Y(q + 1);
+        g.pyy_x = X(q + 2);
+        g.pyy_y = Y(q + 2);
+    }
     g.lapcxx = (double)s_lxx * cl;
     g.lapcxy = (double)s_lxy * cl;
     g.lapcyy = (double)s_lyy * cl;
     g.lapczz = (double)s_lzz * cl;
     g.f_x = g.f_y = g.pzz_x = g.pzz_y = 0.0;
     if constexpr (FP && FORM != SUNSET_FORM_NEWT) {
-        if (FORM == SUNSET_FORM_CHL) { g.pzz_x = (double)s_f_x * cx; g.pzz_y = (double)s_f_y * cy; }
-        else { g.f_x = (double)s_f_x * cx; g.f_y = (double)s_f_y * cy; }
+        if (FORM == SUNSET_FORM_CHL) { g.pzz_x = X(kFp); g.pzz_y = Y(kFp); }
+        else { g.f_x = X(kFp); g.f_y = Y(kFp); }
     }
 }
 
@@ -829,9 +821,9 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
             if (ty == 1) {  // inflow: no streamwise advection of psi (rhs.F90:562-564)
                 NodeState m = n;
                 m.u = 0.0;
-                rhs_c_chl(cK, m, g, r);
+                rhs_c_chl<MX>(cK, m, g, r);
             } else {
-                rhs_c_chl(cK, n, g, r);
+                rhs_c_chl<MX>(cK, n, g, r);
             }
         } else if (FORM == SUNSET_FORM_LC) {
             const bool first = (A.sc->itime == 1) && (stage == 0);
@@ -1132,29 +1124,31 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
     }
     double own[7];
     values(i < cK.npfb ? i : 0, own);
-    float oi[nf];
+    // the filter terms of field pairs (the halo's float2 words), in paired FP32 instructions
+    float2 noi[NP], tp[NP];
 #pragma unroll
-    for (int f = 0; f < nf; f++) oi[f] = (float)(own[f] - rf[f]);
+    for (int p = 0; p < NP; p++) {
+        noi[p] = make_float2(-(float)(own[2 * p] - rf[2 * p]), 2 * p + 1 < nf ? -(float)(own[2 * p + 1] - rf[2 * p + 1]) : 0.0f);
+        tp[p] = make_float2(0.0f, 0.0f);
+    }
     __syncthreads();
-    float t[nf];
-#pragma unroll
-    for (int f = 0; f < nf; f++) t[f] = 0.0f;
     auto link = [&](unsigned loc, float w) {
         const float2 *v = hp + (loc & kLocMask) * NW;
-        float d[2 * NP];
+        const float2 w2 = make_float2(w, w);
+        if (mir && (loc >> 14)) {  // a mirror image: u, v and the xy component with the mirror's sign
+            const unsigned code = loc >> 14;
+            const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
+            const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
 #pragma unroll
-        for (int p = 0; p < NP; p++) {
-            const float2 q = v[p];
-            d[2 * p] = q.x;
-            d[2 * p + 1] = q.y;
-        }
-        const unsigned code = mir ? loc >> 14 : 0u;
-        const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
-        const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
+            for (int p = 0; p < NP; p++) {
+                const int f0 = 2 * p, f1 = 2 * p + 1;
+                const float s0 = f0 == 1 ? su : f0 == 2 ? sv : f0 == 4 ? sxy : 1.0f;
+                const float s1 = f1 == 1 ? su : f1 == 2 ? sv : f1 == 4 ? sxy : 1.0f;
+                tp[p] = __ffma2_rn(w2, __ffma2_rn(make_float2(s0, s1), v[p], noi[p]), tp[p]);
+            }
+        } else {
 #pragma unroll
-        for (int f = 0; f < nf; f++) {
-            const float sg = f == 1 ? su : f == 2 ? sv : f == 4 ? sxy : 1.0f;
-            t[f] = __fmaf_rn(w, __fmaf_rn(sg, d[f], -oi[f]), t[f]);
+            for (int p = 0; p < NP; p++) tp[p] = __ffma2_rn(w2, __fadd2_rn(v[p], noi[p]), tp[p]);
         }
     };
     if (live) {
@@ -1190,7 +1184,7 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
 #pragma unroll
         for (int f = 0; f < 7; f++) {
             if (f < nf) {
-                double r = own[f] + (double)t[f];
+                double r = own[f] + (double)((f & 1) ? tp[f >> 1].y : tp[f >> 1].x);
                 if (wall && (f == 1 || f == 2)) r = 0.0;  // apply_time_dependent_bounds after the filter
                 res[f] = r;
             }
