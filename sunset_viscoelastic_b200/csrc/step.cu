@@ -1068,7 +1068,7 @@ __host__ __device__ inline size_t mxf_smem_bytes(int nf, int hmax) {
     return mxf_ring_bytes() + mxf_bar_bytes() + (size_t)mx_words(nf) * hmax * 8;
 }
 
-template <int FORM, bool FP>
+template <int FORM, bool FP, bool MIR>
 __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
     extern __shared__ __align__(16) double smem[];
     constexpr bool CF = FP && FORM == SUNSET_FORM_CHL;
@@ -1100,8 +1100,9 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
         mbar_init_fence();
         for (int c = 0; c < kMxfDepth && c < nchunk; c++) issue(c);
     }
-    // halo as offsets (FENE-P Cholesky: psi of c, converted in FP64 first)
-    const bool mir = cK.has_mirrors;
+    // halo as offsets (FENE-P Cholesky: psi of c, converted in FP64 first); MIR: the node set
+    // has mirror links, whose reflected fields have reference 0
+    constexpr bool mir = MIR;
     const double *src[7] = {F.ro, F.rou, F.rov, F.q[0], F.q[1], F.q[2], F.q[3]};
     const int hb = A.halo_ptr[blockIdx.x], hn = A.halo_ptr[blockIdx.x + 1] - hb;
     const int n0 = __ldg(A.halo + hb);
@@ -1135,7 +1136,7 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
     auto link = [&](unsigned loc, float w) {
         const float2 *v = hp + (loc & kLocMask) * NW;
         const float2 w2 = make_float2(w, w);
-        if (mir && (loc >> 14)) {  // a mirror image: u, v and the xy component with the mirror's sign
+        if (MIR && (loc >> 14)) {  // a mirror image: u, v and the xy component with the mirror's sign
             const unsigned code = loc >> 14;
             const float su = (code == 1u || code == 3u) ? -1.0f : 1.0f, sv = (code == 2u || code == 3u) ? -1.0f : 1.0f;
             const float sxy = (code == 1u || code == 2u) ? -1.0f : 1.0f;
@@ -1600,7 +1601,8 @@ int stage_smem_attributes(Handle *H, bool mx) {
 template <int FORM, bool FP>
 int filter_smem_attributes(Handle *H, bool mx) {
     SUNSET_SMEM_ATTR((k_filter<FORM, false, FP>));
-    if (mx) SUNSET_SMEM_ATTR((k_filter_mx<FORM, FP>));
+    if (mx) SUNSET_SMEM_ATTR((k_filter_mx<FORM, FP, true>));
+    if (mx) SUNSET_SMEM_ATTR((k_filter_mx<FORM, FP, false>));
     return 0;
 }
 
@@ -1672,8 +1674,13 @@ int launch_filter(Handle *H, const StageArgs &A, bool mx) {
     if (mx) {
         const size_t smem = mxf_smem_bytes(nf, H->halo_max);
         if (smem > kMaxStageSmem) return set_err(H, SUNSET_ERR_SCOPE, "tile halo too large for shared memory");
-        if (cf) k_filter_mx<FORM, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
-        else k_filter_mx<FORM, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        if (H->has_mirrors) {
+            if (cf) k_filter_mx<FORM, true, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+            else k_filter_mx<FORM, false, true><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        } else {
+            if (cf) k_filter_mx<FORM, true, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+            else k_filter_mx<FORM, false, false><<<H->ntiles, kTile, smem, H->stream>>>(A);
+        }
         return 0;
     }
     const size_t smem = halo_doubles(nf, H->halo_max) * sizeof(double) + LinkRing<false, 1, filter_ring_depth(false)>::bytes();
