@@ -847,20 +847,28 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
             for (int f = 0; f < 7; f++) Un[f] = U[f];
             if (stage < 3) {
                 const double RKa = dt * a;
+                // every register read before the first is written: the compiler cannot tell the
+                // fields' arrays apart, and would otherwise wait out each load after a store
+                double S[7], E[7];
 #pragma unroll
                 for (int f = 0; f < nf; f++) {
                     if constexpr (MX) {
-                        const double S = (stage == 0) ? U[f] : U[f] + (double)A.dreg[f][i];
-                        const double E = (stage == 0) ? 0.0 : (double)A.eacc32[f][i];
-                        Un[f] = S + RKa * rr[f];
-                        A.dreg[f][i] = (float)((S + RKb * rr[f]) - Un[f]);
-                        A.eacc32[f][i] = (float)(E + RKbmbh * rr[f]);
+                        S[f] = (stage == 0) ? U[f] : U[f] + (double)A.dreg[f][i];
+                        E[f] = (stage == 0) ? 0.0 : (double)A.eacc32[f][i];
                     } else {
-                        const double S = (stage == 0) ? U[f] : A.reg[f][i];
-                        const double E = (stage == 0) ? 0.0 : A.eacc[f][i];
-                        Un[f] = S + RKa * rr[f];
-                        A.reg[f][i] = S + RKb * rr[f];
-                        A.eacc[f][i] = E + RKbmbh * rr[f];
+                        S[f] = (stage == 0) ? U[f] : A.reg[f][i];
+                        E[f] = (stage == 0) ? 0.0 : A.eacc[f][i];
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < nf; f++) {
+                    Un[f] = S[f] + RKa * rr[f];
+                    if constexpr (MX) {
+                        A.dreg[f][i] = (float)((S[f] + RKb * rr[f]) - Un[f]);
+                        A.eacc32[f][i] = (float)(E[f] + RKbmbh * rr[f]);
+                    } else {
+                        A.reg[f][i] = S[f] + RKb * rr[f];
+                        A.eacc[f][i] = E[f] + RKbmbh * rr[f];
                     }
                 }
             } else {
@@ -913,7 +921,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
                 if (FORM == SUNSET_FORM_LC) {
                     double cxx, cxy, cyy;
                     lc_c_from_psi(Un[3], Un[4], Un[5], &cxx, &cxy, &cyy);
-                    O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = F.c[3][i];
+                    O.c[0][i] = cxx; O.c[1][i] = cxy; O.c[2][i] = cyy; O.c[3][i] = n.czz;  // carried
                 } else if (FORM == SUNSET_FORM_CHL) {
                     double cxx, cxy, cyy, czz;
                     if constexpr (FP) chl_c_from_psi_fenep(cK.fenep_l2, Un[3], Un[4], Un[5], Un[6], &cxx, &cxy, &cyy, &czz);
@@ -922,7 +930,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
                 }
                 if constexpr (FP && (FORM == SUNSET_FORM_DI || FORM == SUNSET_FORM_LC)) {
                     // DI: c is the state itself (czz = Un[6]); LC: czz is carried
-                    const double czz = FORM == SUNSET_FORM_DI ? Un[6] : F.c[3][i];
+                    const double czz = FORM == SUNSET_FORM_DI ? Un[6] : n.czz;
                     O.f[i] = fenep_f(cK.fenep_l2, FORM == SUNSET_FORM_DI ? Un[3] : O.c[0][i],
                                      FORM == SUNSET_FORM_DI ? Un[5] : O.c[2][i], czz);
                 }
@@ -997,9 +1005,11 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
             double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
             double rof = 0.0;
             const bool wall = cK.has_walls && A.ntype[i] == 0;
+            // all loads before the first store (the arrays are not known to be distinct)
             double own[7], res[7];
 #pragma unroll
-            for (int f = 0; f < 7; f++) own[f] = f < nf ? src[f][i] : 0.0;
+            for (int f = 0; f < 7; f++) own[f] = (f < nf || FORM != SUNSET_FORM_NEWT) ? src[f][i] : 0.0;
+            const double vol = A.vol[i];
             if constexpr (CF) chl_fenep_to_c_factor(cK.fenep_l2, own[3], own[4], own[5], own[6]);
 #pragma unroll
             for (int f = 0; f < 7; f++) {
@@ -1015,9 +1025,9 @@ __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
 #pragma unroll
             for (int f = 0; f < 7; f++) {
                 if (f < nf) dst[f][i] = res[f];
-                else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = src[f][i];
+                else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = own[f];  // carried through (never converted)
             }
-            part = (rof - cK.rho_char) * A.vol[i];
+            part = (rof - cK.rho_char) * vol;
         }
     }
     // deterministic two-level sum: fixed tree in the block, fixed order over blocks
@@ -1181,6 +1191,8 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
     if (live && i < cK.npfb) {
         double *dst[7] = {A.out.ro, A.out.rou, A.out.rov, A.out.q[0], A.out.q[1], A.out.q[2], A.out.q[3]};
         const bool wall = cK.has_walls && A.ntype[i] == 0;
+        // loads before the first store (the arrays are not known to be distinct)
+        const double vol = A.vol[i], carried = nf < 7 && FORM != SUNSET_FORM_NEWT ? src[6][i] : 0.0;
         double res[7];
 #pragma unroll
         for (int f = 0; f < 7; f++) {
@@ -1194,9 +1206,9 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
 #pragma unroll
         for (int f = 0; f < 7; f++) {
             if (f < nf) dst[f][i] = res[f];
-            else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = src[f][i];
+            else if (FORM != SUNSET_FORM_NEWT) dst[f][i] = carried;  // psi_zz / c_zz, nf = 6
         }
-        part = (res[0] - cK.rho_char) * A.vol[i];
+        part = (res[0] - cK.rho_char) * vol;
     }
     // deterministic two-level sum: fixed tree in the block, fixed order over blocks
     __shared__ double red[kTile];
@@ -1241,30 +1253,50 @@ __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
     double uvol = 0.0;
     if (i < cK.npfb) {
         const Fields &F = A.out;
-        double ro = F.ro[i];
+        // every load before the first store: the compiler cannot tell the field arrays apart
+        // and would otherwise wait out each load after a store
+        double ro = F.ro[i], rou = F.rou[i], rov = F.rov[i];
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        if (FORM == SUNSET_FORM_LC || FORM == SUNSET_FORM_CHL) { q0 = F.q[0][i]; q1 = F.q[1][i]; q2 = F.q[2][i]; }
+        if (FORM == SUNSET_FORM_CHL && cK.fenep) q3 = F.q[3][i];
+        // the conformation the FENE-P function reads: c itself (direct form), c_zz (carried,
+        // log-conformation); the Cholesky form's comes from psi below
+        double c0 = 0.0, c2 = 0.0, c3 = 0.0;
+        if (F.f) {
+            if (FORM != SUNSET_FORM_LC && FORM != SUNSET_FORM_CHL) { c0 = F.c[0][i]; c2 = F.c[2][i]; }
+            if (FORM != SUNSET_FORM_CHL) c3 = F.c[3][i];
+        }
+        const bool hard_in = cK.has_walls && cK.inflow_type == 1 && A.ntype[i] == 1;
+        const double uin = hard_in ? A.uin[A.bidx[i]] : 0.0;
+        const double vol = cK.vpid ? A.vol[i] : 0.0;
         if (cK.mcorr) ro = ro - dro;
         F.ro[i] = ro;
-        if (cK.has_walls && cK.inflow_type == 1 && A.ntype[i] == 1) {
+        if (hard_in) {
             // the bounds again after the filter (step.F90:498): the hard inflow's momentum
             // from the corrected density, at the step's end time (u_inflow_local unchanged)
-            F.rou[i] = A.uin[A.bidx[i]] * ro;
-            F.rov[i] = 0.0;
+            rou = uin * ro;
+            rov = 0.0;
+            F.rou[i] = rou;
+            F.rov[i] = rov;
         }
         double ooro = 1.0 / ro;
-        F.u[i] = F.rou[i] * ooro;
-        F.v[i] = F.rov[i] * ooro;
+        const double u = rou * ooro;
+        F.u[i] = u;
+        F.v[i] = rov * ooro;
         if (FORM == SUNSET_FORM_LC) {
             double cxx, cxy, cyy;
-            lc_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy);
+            lc_c_from_psi(q0, q1, q2, &cxx, &cxy, &cyy);
             F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy;
+            c0 = cxx; c2 = cyy;
         } else if (FORM == SUNSET_FORM_CHL) {
             double cxx, cxy, cyy, czz;
-            if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, F.q[0][i], F.q[1][i], F.q[2][i], F.q[3][i], &cxx, &cxy, &cyy, &czz);
-            else chl_c_from_psi(F.q[0][i], F.q[1][i], F.q[2][i], &cxx, &cxy, &cyy, &czz);
+            if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, q0, q1, q2, q3, &cxx, &cxy, &cyy, &czz);
+            else chl_c_from_psi(q0, q1, q2, &cxx, &cxy, &cyy, &czz);
             F.c[0][i] = cxx; F.c[1][i] = cxy; F.c[2][i] = cyy; F.c[3][i] = czz;
+            c0 = cxx; c2 = cyy; c3 = czz;
         }
-        if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
-        if (cK.vpid) uvol = F.u[i] * A.vol[i];
+        if (F.f) F.f[i] = fenep_f(cK.fenep_l2, c0, c2, c3);
+        if (cK.vpid) uvol = u * vol;
     }
     if (cK.vpid && advance) {
         // velocity_control with -Dvpid (statistics.F90:214-303), after the step: the volume

@@ -142,7 +142,15 @@ __host__ __device__ constexpr FDesc desc3f(int d) {
 // Minimum resident blocks a SM asked of the compiler: the direct form's gather runs fastest at
 // 5 (96 registers); the forms with 16 gathered fields lose their loads in flight at that size
 // and run at 4 (128 registers).
-__host__ __device__ constexpr int derivs_min_blocks(int form) { return form == SUNSET_FORM_DI ? 5 : 4; }
+#ifndef SUNSET_3D_BLOCKS_DI
+#define SUNSET_3D_BLOCKS_DI 5
+#endif
+#ifndef SUNSET_3D_BLOCKS
+#define SUNSET_3D_BLOCKS 4
+#endif
+__host__ __device__ constexpr int derivs_min_blocks(int form) {
+    return form == SUNSET_FORM_DI ? SUNSET_3D_BLOCKS_DI : SUNSET_3D_BLOCKS;
+}
 
 //
 // ST(slot, value) receives each derivative: a global array of the standalone gather, or the
@@ -210,11 +218,15 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
         if (D.gy >= 0) store(D.gy, sy[d] - p * L.gsy[i]);
         if (D.gl >= 0) sl[d] = sl[d] - p * L.lsum[i];
     }
-    // the z stencils, point by point over all fields (each field's sums still run in point order)
+    // the z stencils, point by point over all fields (each field's sums still run in point
+    // order); a fixed trip count with the points past ncfd cut off, so that the loads of several
+    // points can be in flight together
     double tg[N], tl[N];
 #pragma unroll
     for (int d = 0; d < N; d++) { tg[d] = 0.0; tl[d] = 0.0; }
-    for (int m = 0; m < L.ncfd; m++) {
+#pragma unroll
+    for (int m = 0; m < kMaxFd; m++) {
+        if (m >= L.ncfd) break;
         const int r = row + zwrap(iz + m - h, L.nz);
         const double cg = L.fdg[m], cl = L.fdl[m];
 #pragma unroll
@@ -301,12 +313,13 @@ __global__ void __launch_bounds__(128) k3_filter_xy(Layer3 L, Filter3 A) {
 #pragma unroll
         for (int q = 0; q < NF; q++) t[q] = t[q] + mirror_value(A.f[q][pj], filter_cls(q), code) * w;
     }
+    // the own values loaded before the first store (the arrays are not known to be distinct)
     const double hs = L.hsum[i];
+    double p[NF];
 #pragma unroll
-    for (int q = 0; q < NF; q++) {
-        const double p = A.f[q][k];
-        A.t[q][k] = p + (t[q] - p * hs);
-    }
+    for (int q = 0; q < NF; q++) p[q] = A.f[q][k];
+#pragma unroll
+    for (int q = 0; q < NF; q++) A.t[q][k] = p[q] + (t[q] - p[q] * hs);
 }
 // ... then the z filter of that result (back into the field)
 template <int NF>
@@ -314,17 +327,19 @@ __global__ void __launch_bounds__(128) k3_filter_z(Layer3 L, Filter3 A) {
     ZThread z;
     if (!zthread(L, z)) return;
     const int k = z.k, iz = z.iz, row = z.i * L.nz, h = L.ncfd / 2;
-    double t[NF];
+    double t[NF], own[NF];
 #pragma unroll
-    for (int q = 0; q < NF; q++) t[q] = 0.0;
-    for (int m = 0; m < L.ncfd; m++) {
+    for (int q = 0; q < NF; q++) { t[q] = 0.0; own[q] = A.t[q][k]; }
+#pragma unroll
+    for (int m = 0; m < kMaxFd; m++) {
+        if (m >= L.ncfd) break;
         const int r = row + zwrap(iz + m - h, L.nz);
         const double c = L.fdh[m];
 #pragma unroll
         for (int q = 0; q < NF; q++) t[q] = t[q] + A.t[q][r] * c;
     }
 #pragma unroll
-    for (int q = 0; q < NF; q++) A.f[q][k] = A.t[q][k] + t[q];
+    for (int q = 0; q < NF; q++) A.f[q][k] = own[q] + t[q];
 }
 
 struct Point3 {
@@ -702,9 +717,19 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             double Un[10];
             double en = 0.0;
             for (int q = 0; q < 10; q++) Un[q] = P.in[src[q]][k];
-            for (int q = 0; q < nf; q++) {
-                const double S = stage == 0 ? P.in[src[q]][k] : P.reg[q][k];
-                const double E = stage == 0 ? 0.0 : P.eacc[q][k];
+            // every register read before the first is written (the compiler cannot tell the
+            // arrays apart, and would otherwise wait out each load after a store)
+            double Sq[10], Eq[10];
+#pragma unroll
+            for (int q = 0; q < 10; q++) {
+                if (q >= nf) break;
+                Sq[q] = stage == 0 ? Un[q] : P.reg[q][k];
+                Eq[q] = stage == 0 ? 0.0 : P.eacc[q][k];
+            }
+#pragma unroll
+            for (int q = 0; q < 10; q++) {
+                if (q >= nf) break;
+                const double S = Sq[q], E = Eq[q];
                 if (stage < 3) {
                     Un[q] = S + (dt * a) * r[q];
                     P.reg[q][k] = S + RKb * r[q];
@@ -810,15 +835,17 @@ __global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, 
 __global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
-        const double r = F.p[0][k] - sc->dro;
+        // every load before the first store (the arrays are not known to be distinct)
+        const double r = F.p[0][k] - sc->dro, m1 = F.p[1][k], m2 = F.p[2][k], m3 = F.p[3][k];
+        double p[6], c[6];
+        if (chl || lc)
+            for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
         F.p[0][k] = r;
         const double oo = 1.0 / r;
-        F.p[4][k] = F.p[1][k] * oo;
-        F.p[5][k] = F.p[2][k] * oo;
-        F.p[6][k] = F.p[3][k] * oo;
+        F.p[4][k] = m1 * oo;
+        F.p[5][k] = m2 * oo;
+        F.p[6][k] = m3 * oo;
         if (chl || lc) {
-            double p[6], c[6];
-            for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
             if (chl) chl3_c_from_psi(p, c);
             else lc3_transform(p, c, true);
             for (int q = 0; q < 6; q++) F.p[7 + q][k] = c[q];
