@@ -176,8 +176,8 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
    device time of the nsteps steps. */
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
-/* ---- 3-D (-Ddim3): direct, Cholesky, log-conformation (sPTT) and Newtonian forms, FP64, node
-   sets without boundary nodes ---- */
+/* ---- 3-D (-Ddim3): direct, Cholesky, log-conformation (sPTT) and Newtonian forms, FENE-P with
+   the direct and Cholesky forms, FP64, node sets without boundary nodes ---- */
 /* build_3rd_dimension (setup_domain.F90:435-547) and calc_fd_weights (fd.F90:27-256): after
    sunset_build_domain, the node set becomes nz layers in z over L_domain_z (the control file's
    value): dz from the mean spacing, nz = ceiling(L_domain_z/dz), at least ij_count_fd/2 + 2,

@@ -490,8 +490,19 @@ __device__ void lc3_transform(const double *in, double *out, bool to_c) {
     out[0] = M[0]; out[1] = M[1]; out[2] = M[4]; out[3] = M[6]; out[4] = M[7]; out[5] = M[8];
 }
 
-// cholesky_c_from_psi / cholesky_psi_from_c in 3-D, sPTT (conf_transforms.F90:60-71,108-121)
-__device__ __forceinline__ void chl3_c_from_psi(const double *p, double *c) {
+// cholesky_c_from_psi / cholesky_psi_from_c in 3-D (conf_transforms.F90:28-125): sPTT, or
+// with L2 > 0 (FENE-P, :39-58 and :89-106) the factors of J = f c, f = (L^2 - 3)/(L^2 - tr c),
+// with c = J L^2 / (L^2 - 3 + tr J)
+__device__ __forceinline__ void chl3_c_from_psi(const double *p, double *c, double L2 = 0.0) {
+    if (L2 > 0.0) {
+        const double Jxx = exp(2.0 * p[0]), Jxy = exp(p[0]) * p[1], Jyy = p[1] * p[1] + exp(2.0 * p[2]);
+        const double Jzz = (exp(2.0 * p[5]) + p[3] * p[3]) + p[4] * p[4];
+        const double fq = L2 / ((((L2 - 3.0) + Jxx) + Jyy) + Jzz);
+        c[0] = Jxx * fq; c[1] = Jxy * fq; c[2] = Jyy * fq; c[5] = Jzz * fq;
+        const double Jxz = exp(p[0]) * p[3], Jyz = p[1] * p[3] + exp(p[2]) * p[4];
+        c[3] = Jxz * fq; c[4] = Jyz * fq;
+        return;
+    }
     const double e = exp(p[0]);
     c[0] = e * e;
     c[1] = exp(p[0]) * p[1];
@@ -500,14 +511,41 @@ __device__ __forceinline__ void chl3_c_from_psi(const double *p, double *c) {
     c[4] = p[1] * p[3] + exp(p[2]) * p[4];
     c[5] = (exp(2.0 * p[5]) + p[3] * p[3]) + p[4] * p[4];
 }
-__device__ __forceinline__ void chl3_psi_from_c(const double *c, double *p) {
-    const double xx = sqrt(c[0]);
-    const double xy = c[1] / (xx);
-    const double yy = (sqrt(c[2] - xy * xy));
-    const double xz = c[3] / xx;
-    const double yz = (c[4] - xy * xz) / yy;
-    const double zz = sqrt((c[5] - xz * xz) - yz * yz);
+__device__ __forceinline__ void chl3_psi_from_c(const double *c, double *p, double L2 = 0.0) {
+    double J[6];
+    const double fr = L2 > 0.0 ? (L2 - 3.0) / (L2 - ((c[0] + c[2]) + c[5])) : 1.0;
+    for (int q = 0; q < 6; q++) J[q] = L2 > 0.0 ? c[q] * fr : c[q];
+    const double xx = sqrt(J[0]);
+    const double xy = J[1] / (xx);
+    const double yy = (sqrt(J[2] - xy * xy));
+    const double xz = J[3] / xx;
+    const double yz = (J[4] - xy * xz) / yy;
+    const double zz = sqrt((J[5] - xz * xz) - yz * yz);
     p[0] = log(xx); p[1] = xy; p[2] = log(yy); p[3] = xz; p[4] = yz; p[5] = log(zz);
+}
+// filter_variables under FENE-P in 3-D, rhs.F90:816-834: the factors of J to those of c for the
+// filter; :853-868 back after it (to_c false)
+__device__ __forceinline__ void chl3_fenep_factor(double L2, double *p, bool to_c) {
+    const double trJ = ((((exp(2.0 * p[0]) + p[1] * p[1]) + exp(2.0 * p[2])) + p[3] * p[3]) + p[4] * p[4]) + exp(2.0 * p[5]);
+    double fr;
+    if (to_c) {
+        fr = (L2 * trJ) / ((L2 - 3.0) + trJ);
+        fr = (L2 - 3.0) / (L2 - fr);
+        p[0] = p[0] - log(sqrt(fr));
+        p[1] = p[1] / sqrt(fr);
+        p[2] = p[2] - log(sqrt(fr));
+        p[5] = p[5] - log(sqrt(fr));
+        p[3] = p[3] / sqrt(fr);
+        p[4] = p[4] / sqrt(fr);
+    } else {
+        fr = (L2 - 3.0) / (L2 - trJ);
+        p[0] = p[0] + log(sqrt(fr));
+        p[1] = p[1] * sqrt(fr);
+        p[2] = p[2] + log(sqrt(fr));
+        p[5] = p[5] + log(sqrt(fr));
+        p[3] = p[3] * sqrt(fr);
+        p[4] = p[4] * sqrt(fr);
+    }
 }
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
@@ -592,12 +630,30 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             const double uczz = ((wz - (uz * lxz) / lxx) - (vz * lyz) / lyy) + ((uz * lxy) * lyz) / (lxx * lyy);
             const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
                          czz = P.in[12][k];
-            const double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
             const double Md = K.Mdiff;
             auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
-            const double sxx = fr * (cxx - 1.0) + Md * lc(0), sxy = fr * cxy + Md * lc(1);
-            const double syy = fr * (cyy - 1.0) + Md * lc(2), sxz = fr * cxz + Md * lc(3);
-            const double syz = fr * cyz + Md * lc(4), szz = fr * (czz - 1.0) + Md * lc(5);
+            double sxx, sxy, syy, sxz, syz, szz;
+            if (K.fenep) {  // rhs.F90:204-209, 479-500: the factors of J = f c
+                const double L2 = K.fenep_l2, la = K.lambda;
+                const double fr = (L2 - 3.0) / (L2 - ((cxx + cyy) + czz));
+                const double srctmp =
+                    ((((((((((((2.0 * ux) * cxx + (2.0 * uy) * cxy) + (2.0 * vx) * cxy) + (2.0 * vy) * cyy) + (2.0 * uz) * cxz) +
+                           (2.0 * vz) * cyz) + (2.0 * wx) * cxz) + (2.0 * wy) * cyz) + (2.0 * wz) * czz) -
+                       (((fr * cxx + fr * cyy) + fr * czz) - 3.0) / la) +
+                      Md * ((lc(0) + lc(2)) + lc(5))));
+                const double den = ((L2 - cxx) - cyy) - czz;
+                sxx = (-(fr / la) * (fr * cxx - 1.0) + (Md * fr) * lc(0)) + ((fr * cxx) * srctmp) / den;
+                sxy = (-(fr / la) * (fr * cxy) + (Md * fr) * lc(1)) + ((fr * cxy) * srctmp) / den;
+                syy = (-(fr / la) * (fr * cyy - 1.0) + (Md * fr) * lc(2)) + ((fr * cyy) * srctmp) / den;
+                szz = (-(fr / la) * (fr * czz - 1.0) + (Md * fr) * lc(5)) + ((fr * czz) * srctmp) / den;
+                sxz = (-(fr / la) * (fr * cxz) + (Md * fr) * lc(3)) + ((fr * cxz) * srctmp) / den;
+                syz = (-(fr / la) * (fr * cyz) + (Md * fr) * lc(4)) + ((fr * cyz) * srctmp) / den;
+            } else {
+                const double fr = -(((1.0 - K.epsPTT * 3.0) + K.epsPTT * ((cxx + cyy) + czz))) / K.lambda;
+                sxx = fr * (cxx - 1.0) + Md * lc(0); sxy = fr * cxy + Md * lc(1);
+                syy = fr * (cyy - 1.0) + Md * lc(2); sxz = fr * cxz + Md * lc(3);
+                syz = fr * cyz + Md * lc(4); szz = fr * (czz - 1.0) + Md * lc(5);
+            }
             const double csxx = ((0.5 * sxx) / lxx) / lxx;
             const double csxy = sxy / lxx - ((0.5 * sxx) * lxy) / (lxx * lxx);
             const double csyy = (((0.5 * syy) / lyy) / lyy - (sxy * lxy) / ((lxx * lyy) * lyy)) +
@@ -737,7 +793,11 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                 } else {
                     Un[q] = S + RKb * r[q];
                     const double norm = q == 0 ? K.ero_norm : q < 4 ? K.erou_norm : K.exx_norm;
-                    const double t = fabs(E + RKbmbh * r[q]) * norm;
+                    double t = fabs(E + RKbmbh * r[q]) * norm;
+                    // Cholesky FENE-P (step.F90:442-452): the xx, xy, yy and zz errors scaled by
+                    // 1/sqrt(f) of the node-layer's c, each node-layer's own before the maximum
+                    if (kChl && K.fenep && (q == 4 || q == 5 || q == 6 || q == 9))
+                        t = t * (1.0 / sqrt((K.fenep_l2 - 3.0) / (((K.fenep_l2 - P.in[7][k]) - P.in[9][k]) - P.in[12][k])));
                     en = (t > en) ? t : en;
                     if (t != t) en = t;
                 }
@@ -750,7 +810,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             P.out[6][k] = Un[3] * oo;
             if (kChl || kLc) {  // get_c_from_psi
                 double c[6];
-                if (kChl) chl3_c_from_psi(Un + 4, c);
+                if (kChl) chl3_c_from_psi(Un + 4, c, K.fenep ? K.fenep_l2 : 0.0);
                 else lc3_transform(Un + 4, c, true);
                 for (int q = 0; q < 6; q++) P.out[7 + q][k] = c[q];
             }
@@ -832,7 +892,7 @@ __global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, 
 }
 
 // End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
-__global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, DevScalars *sc, int vpid) {
+__global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, double L2, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         // every load before the first store (the arrays are not known to be distinct)
@@ -846,7 +906,7 @@ __global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, DevScalars *sc
         F.p[5][k] = m2 * oo;
         F.p[6][k] = m3 * oo;
         if (chl || lc) {
-            if (chl) chl3_c_from_psi(p, c);
+            if (chl) chl3_c_from_psi(p, c, L2);
             else lc3_transform(p, c, true);
             for (int q = 0; q < 6; q++) F.p[7 + q][k] = c[q];
         }
@@ -929,7 +989,7 @@ __global__ void k3_fill(size_t n, double v, double *out) {
 }
 // the Cholesky or log-conformation state from the given c: psi from c, then c from psi
 // (setup_flow.F90:86-117)
-__global__ void k3_psi_from_c(size_t n, Fields3 F, int lc) {
+__global__ void k3_psi_from_c(size_t n, Fields3 F, int lc, double L2) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double c[6], p[6];
@@ -938,13 +998,23 @@ __global__ void k3_psi_from_c(size_t n, Fields3 F, int lc) {
         lc3_transform(c, p, false);
         lc3_transform(p, c, true);
     } else {
-        chl3_psi_from_c(c, p);
-        chl3_c_from_psi(p, c);
+        chl3_psi_from_c(c, p, L2);
+        chl3_c_from_psi(p, c, L2);
     }
     for (int q = 0; q < 6; q++) {
         F.p[13 + q][k] = p[q];
         F.p[7 + q][k] = c[q];
     }
+}
+// Cholesky FENE-P around the filter: the six psi (fields 4-9 of the filter's list) from the
+// factors of J to those of c (to_c), or back
+__global__ void k3_fenep_factors(size_t n, Filter3 A, double L2, int to_c) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double p[6];
+    for (int q = 0; q < 6; q++) p[q] = A.f[4 + q][k];
+    chl3_fenep_factor(L2, p, to_c != 0);
+    for (int q = 0; q < 6; q++) A.f[4 + q][k] = p[q];
 }
 // hardcode_initial_conditions in 3-D: rho u = rho * u, rho v, rho w
 __global__ void k3_momentum(size_t n, const double *ro, const double *u, const double *v, const double *w, double *rou,
@@ -1106,8 +1176,8 @@ int tstep3_launch(Handle *H, int b, int pid) {
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
     if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
-    if (H->cfg.fenep && H->cfg.form != SUNSET_FORM_DI)
-        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers FENE-P with the direct form");
+    if (H->cfg.fenep && H->cfg.form != SUNSET_FORM_DI && H->cfg.form != SUNSET_FORM_CHL)
+        return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers FENE-P with the direct and Cholesky forms");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
     if (H->cfg.grav[2] != 0.0) return set_err(H, SUNSET_ERR_SCOPE, "grav(3) must be zero");
     const int ncfd = H->cfg.forder + 1;
@@ -1180,7 +1250,7 @@ int state3_set(Handle *H, const double *const *fields10) {
     if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = f[q];
-        k3_psi_from_c<<<nblk(n), 128, 0, st>>>(n, F19, H->cfg.form == SUNSET_FORM_LC);
+        k3_psi_from_c<<<nblk(n), 128, 0, st>>>(n, F19, H->cfg.form == SUNSET_FORM_LC, H->cfg.fenep ? H->cfg.fenep_l2 : 0.0);
     }
     SUNSET_CUDA(H, cudaGetLastError());
     DevScalars s{};
@@ -1254,8 +1324,11 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
             FA.t[q] = H->g3 + (size_t)q * n;
         }
         if (evolves_c) {
+            const bool chlf = chl && H->cfg.fenep;  // rhs.F90:816-868: filter the factors of c
+            if (chlf) k3_fenep_factors<<<nblk(n), 128, 0, st>>>(n, FA, H->cfg.fenep_l2, 1);
             k3_filter_xy<10><<<zblocks(H), 128, 0, st>>>(L, FA);
             k3_filter_z<10><<<zblocks(H), 128, 0, st>>>(L, FA);
+            if (chlf) k3_fenep_factors<<<nblk(n), 128, 0, st>>>(n, FA, H->cfg.fenep_l2, 0);
         } else {
             k3_filter_xy<4><<<zblocks(H), 128, 0, st>>>(L, FA);
             k3_filter_z<4><<<zblocks(H), 128, 0, st>>>(L, FA);
@@ -1264,7 +1337,7 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
         k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
-        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->dsc, H->cfg.vpid);
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->cfg.fenep ? H->cfg.fenep_l2 : 0.0, H->dsc, H->cfg.vpid);
         SUNSET_CUDA(H, cudaGetLastError());
         H->cur3 = b;
     }

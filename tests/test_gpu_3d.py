@@ -51,6 +51,9 @@ CASES = {
     "di-o4-fenep": ("periodic-di-o4-16k", 24, 1.0, (1, 1), {"fenep": True, "fenep_l2": 30.0}),
     "di-o6-fenep-mdiff-ysym": ("periodic-lc-o6-262k", 20, 0.6, (2, 2),
                                {"form": "di", "fenep": True, "fenep_l2": 50.0, "Mdiff": 1e-3}),
+    "chl-o6-fenep": ("periodic-lc-o6-262k", 20, 0.6, (1, 1), {"form": "chl", "fenep": True, "fenep_l2": 50.0}),
+    "chl-o4-fenep-mdiff-ysym": ("periodic-di-o4-16k", 24, 1.0, (2, 2),
+                                {"form": "chl", "fenep": True, "fenep_l2": 30.0, "Mdiff": 1e-3}),
 }
 
 
@@ -152,8 +155,9 @@ def test_steps(pair):
 
 
 def test_fenep_scope():
-    """FENE-P in 3-D covers the direct form; the Cholesky form is refused with a scope error."""
-    wl = dataclasses.replace(WORKLOADS["periodic-chl-o8-1m"], nside=16)
+    """FENE-P in 3-D covers the direct and Cholesky forms; the log-conformation form is refused
+    with a scope error."""
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16)
     ns = wl.nodes()
     kw = dict(wl.params(), fenep=True, fenep_l2=30.0)
     gpu = labfm.Sunset(**kw)

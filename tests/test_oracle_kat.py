@@ -388,14 +388,16 @@ def test_adapt_stencils_invariants():
 
 
 @pytest.mark.parametrize("form, eps, fenep", [("di", 0.25, False), ("chl", 0.25, False), ("lc", 0.0, False),
-                                              ("newt", 0.0, False), ("di", 0.0, True)])
+                                              ("newt", 0.0, False), ("di", 0.0, True), ("chl", 0.0, True)])
 def test_3d_reduces_to_2d(form, eps, fenep):
     """3-D restatement, known answer: with w = 0, c_xz = c_yz = 0, c_zz = 1 and fields that do
     not vary in z, every layer's right-hand side is the 2-D one (the z stencils see constants;
     rho w, c_xz and c_yz stay at rest).  The log-conformation form takes eps = 0: its 3-D sPTT
     trace includes c_zz, the 2-D one does not (rhs_lc.F90:451-456).  FENE-P (direct form): the
     function f and its gradient enter the momentum and the relaxation alike in 2-D and 3-D
-    (rhs_di.F90:198-245, 454-464)."""
+    (rhs_di.F90:198-245, 454-464).  FENE-P (Cholesky form): the factors of J = f c, whose
+    source terms and transforms reduce to the 2-D ones when psi_xz = psi_yz = 0
+    (rhs.F90:479-500, conf_transforms.F90:39-58)."""
     wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16, form=form, epsPTT=eps)
     ns = wl.nodes()
     extra = dict(fenep=True, fenep_l2=30.0) if fenep else {}
