@@ -1124,10 +1124,20 @@ __global__ void k_adapt_stencils(AdaptArgs a) {
     }
 }
 
+// The largest dynamic shared memory a block may opt into on the handle's device (227 KB on
+// B200): the weight and adaptation kernels are latency-bound, one warp a node, so as many
+// warps as their per-warp matrices fit.
+int smem_optin(Handle *H, int *bytes) {
+    SUNSET_CUDA(H, cudaDeviceGetAttribute(bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
+    return 0;
+}
+
 template <int ORDER>
 int launch_weights(Handle *H, WArgs &a) {
     constexpr int per_warp = smem_doubles<ORDER>() * (int)sizeof(double);
-    int wpb = (200 * 1024) / per_warp;
+    int optin = 0;
+    if (int rc = smem_optin(H, &optin)) return rc;
+    int wpb = optin / per_warp;
     if (wpb > 16) wpb = 16;
     if (wpb < 1) wpb = 1;
     size_t smem = (size_t)wpb * per_warp;
@@ -1148,7 +1158,9 @@ template <int ORDER>
 int launch_adapt(Handle *H, AdaptArgs &a) {
     const int per_warp = (adapt_fixed_doubles<ORDER>() + 5 * a.nplink + 1) & ~1;
     const size_t per_warp_bytes = (size_t)per_warp * sizeof(double);
-    int wpb = (int)((200 * 1024) / per_warp_bytes);
+    int optin = 0;
+    if (int rc = smem_optin(H, &optin)) return rc;
+    int wpb = (int)((size_t)optin / per_warp_bytes);
     if (wpb > 16) wpb = 16;
     if (wpb < 1) return set_err(H, SUNSET_ERR_SCOPE, "neighbour lists too long for the stencil adaptation");
     a.per_warp = per_warp;
