@@ -183,6 +183,8 @@ void sunset_destroy(SunsetHandle *sh) {
     if (H->stream) cudaStreamSynchronize(H->stream);
     for (int b = 0; b < 2; b++)
         if (H->graph[b]) cudaGraphExecDestroy(H->graph[b]);
+    for (cudaGraphExec_t g : {H->adj_rec_graph, H->adj_rev_graph})
+        if (g) cudaGraphExecDestroy(g);
     for (void *p : H->allocs) cudaFree(p);
     H->allocs.clear();
     if (H->stream) cudaStreamDestroy(H->stream);

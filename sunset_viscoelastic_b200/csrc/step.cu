@@ -1487,26 +1487,47 @@ __global__ void k_set_state(int npfb, int form, const double *ro, const double *
 
 // Conservative state given directly (ro, rou, rov, q0..q3), derived fields recomputed
 // as get_velocity_from_momentum / get_c_from_psi do.
+__device__ __forceinline__ void set_conservative_node(int i, int form, double ro, double rou, double rov, double q0,
+                                                      double q1, double q2, double q3, const Fields &F) {
+    F.ro[i] = ro; F.rou[i] = rou; F.rov[i] = rov;
+    F.q[0][i] = q0; F.q[1][i] = q1; F.q[2][i] = q2; F.q[3][i] = q3;
+    double ooro = 1.0 / ro;
+    F.u[i] = rou * ooro;
+    F.v[i] = rov * ooro;
+    if (form == SUNSET_FORM_LC) {
+        double c0, c1, c2;
+        lc_c_from_psi(q0, q1, q2, &c0, &c1, &c2);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = 1.0;
+    } else if (form == SUNSET_FORM_CHL) {
+        double c0, c1, c2, c3;
+        if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, q0, q1, q2, q3, &c0, &c1, &c2, &c3);
+        else chl_c_from_psi(q0, q1, q2, &c0, &c1, &c2, &c3);
+        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
+    }
+    if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
+}
 __global__ void k_set_conservative(int npfb, int form, const double *ro, const double *rou, const double *rov,
                                    const double *q0, const double *q1, const double *q2, const double *q3, Fields F) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
-    F.ro[i] = ro[i]; F.rou[i] = rou[i]; F.rov[i] = rov[i];
-    F.q[0][i] = q0[i]; F.q[1][i] = q1[i]; F.q[2][i] = q2[i]; F.q[3][i] = q3[i];
-    double ooro = 1.0 / ro[i];
-    F.u[i] = rou[i] * ooro;
-    F.v[i] = rov[i] * ooro;
-    if (form == SUNSET_FORM_LC) {
-        double c0, c1, c2;
-        lc_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2);
-        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = 1.0;
-    } else if (form == SUNSET_FORM_CHL) {
-        double c0, c1, c2, c3;
-        if (cK.fenep) chl_c_from_psi_fenep(cK.fenep_l2, q0[i], q1[i], q2[i], q3[i], &c0, &c1, &c2, &c3);
-        else chl_c_from_psi(q0[i], q1[i], q2[i], &c0, &c1, &c2, &c3);
-        F.c[0][i] = c0; F.c[1][i] = c1; F.c[2][i] = c2; F.c[3][i] = c3;
-    }
-    if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
+    set_conservative_node(i, form, ro[i], rou[i], rov[i], q0[i], q1[i], q2[i], q3[i], F);
+}
+// The state from checkpoint *seg of the adjoint's store (7 fields of npfb doubles each a
+// checkpoint): the index is read on the device, so a captured graph serves every segment.
+__global__ void k_load_checkpoint(int npfb, int form, const double *store, const int *seg, Fields F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npfb) return;
+    const double *cp = store + (size_t)7 * npfb * (size_t)*seg;
+    const size_t n = (size_t)npfb;
+    set_conservative_node(i, form, cp[i], cp[n + i], cp[2 * n + i], cp[3 * n + i], cp[4 * n + i], cp[5 * n + i],
+                          cp[6 * n + i], F);
+}
+// Scalars set on the stream by a kernel rather than a copy from pageable host memory (which
+// the driver stages, and which can hold the host until the stream reaches it).
+__global__ void k_set_dt(DevScalars *sc, double dt) { sc->dt = dt; }
+__global__ void k_set_segment(DevScalars *sc, int *seg, int s, int itime) {
+    sc->itime = itime;
+    *seg = s;
 }
 
 __global__ void k_ke_mass(int npfb, Fields F, const double *vol, double *partials) {
@@ -1884,7 +1905,10 @@ int step_run(Handle *H, double dt, int nsteps, int mode) {
     int rc = upload_consts(H);
     if (rc) return rc;
     cudaStream_t st = H->stream;
-    if (mode == 0) SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
+    if (mode == 0) {
+        k_set_dt<<<1, 1, 0, st>>>(H->dsc, dt);
+        SUNSET_CUDA(H, cudaGetLastError());
+    }
     for (int s = 0; s < nsteps; s++) {
         int from = H->cur;
         if (!H->graph[from] || H->graph_mode[from] != mode) {
@@ -2250,13 +2274,11 @@ __device__ __forceinline__ void tile_sum2(double &a, double &b) {
 __device__ __forceinline__ void point_reverse(const RevArgs &B, int j, const double *ub, bool sbar_zero, double &t0,
                                               double &t1) {
     const int n = cK.npfb;
-    double rb[kAdjR];
+    // every load before the first store (the arrays are not known to be distinct, and each
+    // load after a store would wait out the one before)
+    double si[kAdjR];
 #pragma unroll
-    for (int f = 0; f < kAdjR; f++) {
-        const double si = sbar_zero ? 0.0 : B.sbar[f][j];
-        rb[f] = B.dt * (B.alpha * ub[f] + B.beta * si);
-        B.sbar[f][j] = ub[f] + si;
-    }
+    for (int f = 0; f < kAdjR; f++) si[f] = sbar_zero ? 0.0 : B.sbar[f][j];
     const Fields &P = B.prev;
     const double s[kAdjS] = {P.ro[j], P.rou[j], P.rov[j], P.q[0][j], P.q[1][j], P.q[2][j]};
     double g[kAdjG], gbv[kAdjG], sbv[kAdjS] = {0, 0, 0, 0, 0, 0}, tb[2] = {0.0, 0.0};
@@ -2264,6 +2286,12 @@ __device__ __forceinline__ void point_reverse(const RevArgs &B, int j, const dou
     for (int k = 0; k < kAdjG; k++) {
         g[k] = B.gprev[(size_t)k * n + j];
         gbv[k] = 0.0;
+    }
+    double rb[kAdjR];
+#pragma unroll
+    for (int f = 0; f < kAdjR; f++) {
+        rb[f] = B.dt * (B.alpha * ub[f] + B.beta * si[f]);
+        B.sbar[f][j] = ub[f] + si[f];
     }
     p_adjoint_lc(cK, s, g, B.first != 0, rb, sbv, gbv, tb);
     store_gbar(B.gb_out, n, j, gbv);
@@ -2449,9 +2477,12 @@ __global__ void __launch_bounds__(kTile, 2) k_adj_stage_lc(RevArgs B) {
         if constexpr (FUSE) {
             point_reverse(B, j, U, false, t0, t1);
         } else {
+            double sb[kAdjS];
+#pragma unroll
+            for (int f = 0; f < kAdjS; f++) sb[f] = B.sbar[f][j];
 #pragma unroll
             for (int f = 0; f < kAdjS; f++) {
-                const double x = U[f] + B.sbar[f][j];
+                const double x = U[f] + sb[f];
                 B.ua[f][j] = x;
                 if (f == 0) t0 = x;
             }
@@ -2771,6 +2802,26 @@ static int alloc_fields(Handle *H, Fields &F) {
     return 0;
 }
 
+// Captures the launches fn() makes on the handle's stream into *exec (replacing it).
+template <class FN>
+int capture_graph(Handle *H, cudaGraphExec_t *exec, FN fn) {
+    if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+    cudaGraph_t g = nullptr;
+    SUNSET_CUDA(H, cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal));
+    const int lrc = fn();
+    const cudaError_t ce = cudaStreamEndCapture(H->stream, &g);
+    if (lrc || ce != cudaSuccess) {  // the capture ended either way: drop what it recorded
+        if (g) cudaGraphDestroy(g);
+        if (lrc) return lrc;
+        SUNSET_CUDA(H, ce);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) *exec = nullptr;
+    SUNSET_CUDA(H, ie);
+    return 0;
+}
+
 int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *dtheta, double *dU0) {
     if (H->cfg.form != SUNSET_FORM_LC)
         return set_err(H, SUNSET_ERR_SCOPE, "the adjoint is built for the log-conformation form");
@@ -2818,21 +2869,27 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
         SUNSET_CUDA(H, cudaFuncSetAttribute(k_adj_filter_lc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStageSmem));
         H->adj_ready = true;
     }
+    if (!H->adj_segd && dalloc(H, &H->adj_segd, 1)) return SUNSET_ERR_NOMEM;
+    // a full segment's record and reverse sweep run as captured graphs (one launch each, so a
+    // host thread that loses its core does not leave the device idle); they hold dt and the
+    // checkpoint store, and are captured again when either changes
+    if (H->adj_graph_dt != dt || H->adj_graph_cp != H->adj_cp) {
+        for (cudaGraphExec_t *g : {&H->adj_rec_graph, &H->adj_rev_graph})
+            if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+        H->adj_graph_dt = dt;
+        H->adj_graph_cp = H->adj_cp;
+    }
     DevScalars sc0;
     SUNSET_CUDA(H, cudaMemcpyAsync(&sc0, H->dsc, sizeof(sc0), cudaMemcpyDeviceToHost, st));
     SUNSET_CUDA(H, cudaStreamSynchronize(st));
-    SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, st));
+    k_set_dt<<<1, 1, 0, st>>>(H->dsc, dt);
     const int TB = 128, nb = (n + TB - 1) / TB;
-    // Records segment sg from its checkpoint: stage inputs in adj_store[4 k + s], their stencil
-    // sums in adj_g, the state after the segment in adj_store[4 ckpt + 1].
-    auto record = [&](int sg) -> int {
-        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
+    // Records len steps of the segment whose checkpoint index and start step k_set_segment has
+    // set: stage inputs in adj_store[4 k + s], their stencil sums in adj_g, the state after the
+    // segment in adj_store[4 ckpt + 1].
+    auto record_launch = [&](int len) -> int {
         Fields &F0 = H->adj_store[0];
-        const double *cp = H->adj_cp + (size_t)7 * n * sg;
-        k_set_conservative<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, cp, cp + n, cp + 2 * (size_t)n, cp + 3 * (size_t)n,
-                                              cp + 4 * (size_t)n, cp + 5 * (size_t)n, cp + 6 * (size_t)n, F0);
-        const int it = sc0.itime + n0;
-        SUNSET_CUDA(H, cudaMemcpyAsync(&H->dsc->itime, &it, sizeof(int), cudaMemcpyHostToDevice, st));
+        k_load_checkpoint<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, H->adj_cp, H->adj_segd, F0);
         Fields &T = H->adj_store[4 * (size_t)ckpt], &X = H->adj_store[4 * (size_t)ckpt + 1];
         for (int k = 0; k < len; k++) {
             for (int s = 0; s < 4; s++) {
@@ -2846,6 +2903,15 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
             k_finalize<SUNSET_FORM_LC><<<nb, TB, 0, st>>>(Fa, 1);
         }
         SUNSET_CUDA(H, cudaGetLastError());
+        return 0;
+    };
+    auto record = [&](int sg) -> int {
+        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
+        k_set_segment<<<1, 1, 0, st>>>(H->dsc, H->adj_segd, sg, sc0.itime + n0);
+        if (len < ckpt) return record_launch(len);
+        if (!H->adj_rec_graph)
+            if (int rc = capture_graph(H, &H->adj_rec_graph, [&]() { return record_launch(ckpt); })) return rc;
+        SUNSET_CUDA(H, cudaGraphLaunch(H->adj_rec_graph, st));
         return 0;
     };
     // ---- forward with checkpoints; the last segment is recorded as it runs ----
@@ -2884,10 +2950,9 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     const double beta[4] = {SUNSET_RK_B1, SUNSET_RK_B2, SUNSET_RK_B3, 0.0};
     auto gstage = [&](int k, int s) { return H->adj_g + (size_t)(4 * k + s) * kAdjG * n; };
     auto gpair = [&](int b) { return reinterpret_cast<double2 *>(H->adj_gp[b]); };
-    for (int sg = nseg - 1; sg >= 0; sg--) {
-        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
-        if (sg + 1 < nseg)
-            if (int rc = record(sg)) return rc;
+    // reverse sweep of len steps of the segment starting at step n0 (first: the itime = 1 case
+    // of the log-conformation right-hand side may occur in it)
+    auto reverse_launch = [&](int len, int n0, bool first) -> int {
         for (int k = len - 1; k >= 0; k--) {
             // filter + mass correction reversed, then the pointwise reverse of stage 3
             B.prev = H->adj_store[4 * k + 3];
@@ -2906,7 +2971,7 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
                 B.gprev = gstage(k, s - 1);
                 B.alpha = alpha[s - 1];
                 B.beta = beta[s - 1];
-                B.first = (s == 1) && (sc0.itime + n0 + k == 1);
+                B.first = first && (s == 1) && (sc0.itime + n0 + k == 1);
                 k_adj_stage_lc<true><<<H->ntiles, kTile, smem_stage, st>>>(B);
                 cur ^= 1;
             }
@@ -2914,6 +2979,21 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
             B.gb_in = gpair(cur);
             k_adj_stage_lc<false><<<H->ntiles, kTile, smem_stage, st>>>(B);
         }
+        SUNSET_CUDA(H, cudaGetLastError());
+        return 0;
+    };
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int n0 = sg * ckpt, len = std::min(ckpt, nsteps - n0);
+        if (sg + 1 < nseg)
+            if (int rc = record(sg)) return rc;
+        const int k1 = 1 - sc0.itime - n0;  // the segment's step with itime = 1, if any
+        if (len < ckpt || (k1 >= 0 && k1 < len)) {
+            if (int rc = reverse_launch(len, n0, true)) return rc;
+            continue;
+        }
+        if (!H->adj_rev_graph)
+            if (int rc = capture_graph(H, &H->adj_rev_graph, [&]() { return reverse_launch(ckpt, 0, false); })) return rc;
+        SUNSET_CUDA(H, cudaGraphLaunch(H->adj_rev_graph, st));
     }
     SUNSET_CUDA(H, cudaGetLastError());
     k_adj_fold<<<1, 128, 0, st>>>(H->adj_tacc, H->ntiles, 2, H->adj_acc, 0);
