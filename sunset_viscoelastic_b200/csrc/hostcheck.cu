@@ -2,6 +2,8 @@
 // hand-written adjoint (adjoint.cuh), so the adjoint can be checked against finite
 // differences of the forward map without a GPU.  Built into libsunset_hostcheck.so; the time
 // step itself never calls it.
+#include <vector>
+
 #include "adjoint.cuh"
 
 extern "C" {
@@ -30,6 +32,23 @@ int sunset_hostcheck_lc(const double *par, const double *s, const double *g, int
         tbar[0] = tbar[1] = 0.0;
         sunset::p_adjoint_lc(K, s, g, first != 0, rbar, sbar, gbar, tbar);
     }
+    return 0;
+}
+
+// deal_slice_by_bank (bank_deal.cu) on one slice given as flat lists: lane r's small entries
+// are small[soff[r] .. soff[r + 1]), its other entries large[loff[r] .. loff[r + 1]); pos[e] is
+// the local position of entry e.  chosen[k * 32 + lane] for k < width (-1: padding).
+int sunset_hostcheck_deal(int group, const uint16_t *pos, const int *small, const int *soff, const int *large,
+                          const int *loff, int width, int *chosen) {
+    std::vector<int> vs[sunset::kSlice], vl[sunset::kSlice];
+    int c_s[sunset::kSlice], c[sunset::kSlice];
+    for (int r = 0; r < sunset::kSlice; r++) {
+        vs[r].assign(small + soff[r], small + soff[r + 1]);
+        vl[r].assign(large + loff[r], large + loff[r + 1]);
+        c_s[r] = (int)vs[r].size();
+        c[r] = c_s[r] + (int)vl[r].size();
+    }
+    sunset::deal_slice_by_bank(group, pos, vs, vl, c_s, c, width, chosen);
     return 0;
 }
 
