@@ -429,9 +429,9 @@ def run_3d(args, local):
     workload3 = wl.name + f"-3d-nside{args.nside}"
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": profiled_traffic(workload3, "fp64"),
-                "kernel": "k3_derivs (every derivative of a stage: x-y LABFM sums and z stencils)",
+                "kernel": "k3_stage (one fused stage: x-y LABFM sums, z stencils, right-hand side, RK update)",
                 "algorithmic_bytes_per_launch": g_bytes, "launch_ms": g_ms, "peak_source": peak_kind,
-                "method": f"CUDA events around each of the 4 gather launches of {roof_steps} steps"}
+                "method": f"CUDA events around each of the 4 stage launches of {roof_steps} steps"}
     cpu = None
     if not args.no_cpu_baseline:
         # the CPU restatement on the same 3-D set, all host cores, one step (weights of the

@@ -177,14 +177,17 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
 /* ---- 3-D (-Ddim3): direct, Cholesky, log-conformation (sPTT) and Newtonian forms, FENE-P with
-   the direct and Cholesky forms, FP64, node sets without boundary nodes ---- */
+   the direct and Cholesky forms, FP64, node sets without boundary nodes or with walls
+   (node_type 0; inflow and outflow nodes: SUNSET_ERR_SCOPE) ---- */
 /* build_3rd_dimension (setup_domain.F90:435-547) and calc_fd_weights (fd.F90:27-256): after
    sunset_build_domain, the node set becomes nz layers in z over L_domain_z (the control file's
    value): dz from the mean spacing, nz = ceiling(L_domain_z/dz), at least ij_count_fd/2 + 2,
    z-derivatives by periodic central differences of forder + 1 points.  The neighbour lists and
    weights are built for the layer (the same calls as in 2-D) and serve every layer.  Then
    sunset_set_state_3d, and sunset_step / sunset_set_tstep / sunset_get_time act on the 3-D
-   state.  Arrays are npfb*nz, layer-major (node iz*npfb + i, reference order in the layer). */
+   state.  Arrays are npfb*nz, layer-major (node iz*npfb + i, reference order in the layer).
+   Walls are walls of every layer (node_type and normals copied, :487-532): the velocity is
+   zero there and the wall branches of the right-hand sides apply, with their dim3 terms. */
 int sunset_set_layers(SunsetHandle *h, double L_domain_z);
 int sunset_get_layers(SunsetHandle *h, int *nz, double *dz);
 /* initial_solution in 3-D: rho, u, v, w and the six c components (all NULL: c = I) */

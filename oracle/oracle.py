@@ -338,15 +338,16 @@ C3_FIELDS = ["cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
 
 class Oracle3:
     """The 3-D (-Ddim3) run built on a set-up 2-D layer (direct, Cholesky, log-conformation (sPTT)
-    and Newtonian forms, FENE-P with the direct form, node sets without boundary nodes).  Arrays
-    are nl*nz, layer-major."""
+    and Newtonian forms, FENE-P with the direct and Cholesky forms, node sets without boundary
+    nodes or with walls among them).  Arrays are nl*nz, layer-major."""
 
     def __init__(self, layer: Oracle, Lz: float):
         self.layer = layer
         self.L = layer.L
         self.h = self.L.or3_create(layer.h, float(Lz))
         if not self.h:
-            raise OracleError("or3_create: needs weights, no boundary nodes, FENE-P only with the direct form")
+            raise OracleError("or3_create: needs weights, walls only among the boundary nodes, "
+                              "FENE-P only with the direct and Cholesky forms")
         nl, nz, dz = C.c_int(), C.c_int(), C.c_double()
         self.L.or3_sizes(self.h, C.byref(nl), C.byref(nz), C.byref(dz))
         self.nl, self.nz, self.dz = nl.value, nz.value, dz.value

@@ -2782,7 +2782,8 @@ double or_mass(OrSim *s) {
  * (fd.F90:27-256), the z parts of derivatives.F90 (:48-63, :96-108, :145-157, :340-352,
  * :387-405, :441-453) and the dim3 branches of rhs_di.F90, rhs.F90 (Cholesky) and rhs_lc.F90
  * (log-conformation), conf_transforms.F90:27-397 and step.F90, for the direct, Cholesky,
- * log-conformation (sPTT) and Newtonian forms on node sets without boundary nodes.
+ * log-conformation (sPTT) and Newtonian forms on node sets without boundary nodes or with walls
+ * (node_type 0) among them.
  *
  * The 3-D node set is nz copies of the 2-D one, layer-major: node k = iz*nl + i at
  * z = iz*dz.  The reference searches neighbours per layer (neighbours.F90:180-183,223-233,
@@ -2791,6 +2792,12 @@ double or_mass(OrSim *s) {
  * weights are the layer's own (the 2-D OrSim below), used with an offset of iz*nl.  Mirror
  * images take their parent's value in the same layer; u and v flip with the mirror as in 2-D,
  * w and c_xz, c_yz are copied unchanged (mirror_boundaries.F90:302-303,324-341).
+ *
+ * Walls (build_3rd_dimension copies node_type and rnorm to every layer, :487-532): a wall
+ * node's x-y operators are its boundary weights (normal and tangential derivatives), its z
+ * operators the same stencils as everywhere; its right-hand sides are the wall branches of
+ * calc_rhs_ro / calc_rhs_rovel / calc_rhs_nscbc and of the conformation equations with their
+ * dim3 terms, and apply_time_dependent_bounds holds rho u, rho v, rho w at zero there.
  * ========================================================================================= */
 struct Or3 {
     OrSim *s;                /* the layer */
@@ -2802,6 +2809,7 @@ struct Or3 {
     double time, dt, dt_cfl, dt_par;
     int itime, iRKstep;
     double emax_nm1, emax_n, emax_np1;
+    int *bidx;               /* nl: the layer node's index in boundary_list, or -1 */
     char err[256];
 };
 
@@ -2850,12 +2858,16 @@ static int fd_tables(int ncfd, double dz, double L, double *g, double *g2, doubl
 }
 
 Or3 *or3_create(OrSim *s, double Lz) {
-    if (!s || !s->have_weights || s->nb != 0 || (s->cfg.fenep && s->cfg.form != OR_FORM_DI && s->cfg.form != OR_FORM_CHL) ||
-        !(Lz > 0.0))
+    if (!s || !s->have_weights || (s->cfg.fenep && s->cfg.form != OR_FORM_DI && s->cfg.form != OR_FORM_CHL) || !(Lz > 0.0))
         return NULL;
+    for (int jj = 0; jj < s->nb; jj++) /* walls only among the boundary nodes */
+        if (s->type[s->boundary_list[jj]] != 0) return NULL;
     Or3 *o = (Or3 *)xcalloc(1, sizeof(Or3));
     o->s = s;
     o->nl = s->npfb;
+    o->bidx = (int *)xcalloc(o->nl, sizeof(int));
+    for (int i = 0; i < o->nl; i++) o->bidx[i] = -1;
+    for (int jj = 0; jj < s->nb; jj++) o->bidx[s->boundary_list[jj]] = jj;
     o->ncfd = s->cfg.forder + 1;
     /* build_3rd_dimension, :444-483 (mean_alpha = 1, one process in z) */
     double dzl = 0.0, sv = 0.0;
@@ -2873,7 +2885,7 @@ Or3 *or3_create(OrSim *s, double Lz) {
     }
     o->nz = nz;
     o->dz = dz;
-    if (fd_tables(o->ncfd, dz, L, o->fdg, o->fdl, o->fdh)) { free(o); return NULL; }
+    if (fd_tables(o->ncfd, dz, L, o->fdg, o->fdl, o->fdh)) { free(o->bidx); free(o); return NULL; }
     o->n3 = (size_t)o->nl * nz;
     double **a[] = {&o->ro, &o->rou, &o->rov, &o->row, &o->u, &o->v, &o->w, &o->c[0], &o->c[1], &o->c[2], &o->c[3], &o->c[4], &o->c[5],
                     &o->psi[0], &o->psi[1], &o->psi[2], &o->psi[3], &o->psi[4], &o->psi[5]};
@@ -2886,6 +2898,7 @@ void or3_destroy(Or3 *o) {
     double *a[] = {o->ro, o->rou, o->rov, o->row, o->u, o->v, o->w, o->c[0], o->c[1], o->c[2], o->c[3], o->c[4], o->c[5],
                    o->psi[0], o->psi[1], o->psi[2], o->psi[3], o->psi[4], o->psi[5]};
     for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) free(a[k]);
+    free(o->bidx);
     free(o);
 }
 
@@ -2956,6 +2969,39 @@ static void lap3(const Or3 *o, const double *f, int cls, double *lap) {
         double t = 0.0;
         for (int m = 0; m < o->ncfd; m++) t = t + f[zoff(o, iz, m) + i] * o->fdl[m];
         lap[k] = r + t;
+    }
+}
+/* The conformation Laplacian in 3-D: calc_laplacian_transverse_only_on_bound (:306-358), whose
+   x-y part on a wall node takes the tangential second-derivative weights (ij_wb_grad2(2,:,:)),
+   then the z stencil; on walls calc_rhs_c adds the one-sided normal second derivative over the
+   node's four FD rows, the next nodes of its layer (rhs_di.F90:553-568, rhs.F90:631-643) */
+static void lap3_conf(const Or3 *o, const double *f, int cls, double *lap) {
+    const OrSim *s = o->s;
+    const int nplink = s->nplink;
+    const double L = s->cfg.L_char;
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < o->n3; k++) {
+        const int iz = (int)(k / o->nl), i = (int)(k % o->nl);
+        const size_t off = (size_t)iz * o->nl;
+        const int jb = o->bidx[i];
+        const int *lk = s->ij_link + (size_t)i * nplink;
+        double l = 0.0, r;
+        if (jb < 0) {
+            const double *wl = s->w_lap + (size_t)i * nplink;
+            for (int q = 0; q < s->ij_count_small[i]; q++) l = l + val3(o, f, lk[q], off, cls) * wl[q];
+            r = l - f[k] * s->w_lap_sum[i];
+        } else {
+            for (int q = 0; q < s->ij_count_small[i]; q++)
+                l = l + val3(o, f, lk[q], off, cls) * s->wb_grad2[((size_t)jb * nplink + q) * 3 + 1];
+            r = l - f[k] * s->wb_grad2_sum[3 * jb + 1];
+        }
+        double t = 0.0;
+        for (int m = 0; m < o->ncfd; m++) t = t + f[zoff(o, iz, m) + i] * o->fdl[m];
+        lap[k] = r + t;
+        if (jb >= 0) {
+            const double den = ((72.0 * s->sp[i]) * s->sp[i]) * L * L;
+            lap[k] = lap[k] + (((((-415.0 * f[k]) + 576.0 * f[k + 1]) - 216.0 * f[k + 2]) + 64.0 * f[k + 3]) - 9.0 * f[k + 4]) / den;
+        }
     }
 }
 /* calc_filtered_var in 3-D (:360-405): the x-y filter, then the z filter of the result */
@@ -3189,11 +3235,24 @@ static void or3_c_from_psi(Or3 *o) {
     }
 }
 
-/* hardcode_initial_conditions in 3-D: rho, u, v, w and c given; rho u = rho * u ... */
+/* apply_time_dependent_bounds on the walls of every layer (characteristic_boundaries.F90:
+   191-257): rho u = rho v = rho w = 0 */
+static void bounds3(Or3 *o) {
+    const OrSim *s = o->s;
+    for (int iz = 0; iz < o->nz; iz++)
+        for (int jj = 0; jj < s->nb; jj++) {
+            const size_t k = (size_t)iz * o->nl + s->boundary_list[jj];
+            o->rou[k] = 0.0; o->rov[k] = 0.0; o->row[k] = 0.0;
+        }
+}
+
+/* hardcode_initial_conditions in 3-D: rho, u, v, w and c given (u, v, w zero on walls,
+   setup_flow.F90:266-280); rho u = rho * u ... */
 int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, const double *w,
                   const double *const *c6) {
     for (size_t k = 0; k < o->n3; k++) {
         o->ro[k] = ro[k]; o->u[k] = u[k]; o->v[k] = v[k]; o->w[k] = w[k];
+        if (o->bidx[k % o->nl] >= 0) { o->u[k] = 0.0; o->v[k] = 0.0; o->w[k] = 0.0; }
         o->rou[k] = o->ro[k] * o->u[k]; o->rov[k] = o->ro[k] * o->v[k]; o->row[k] = o->ro[k] * o->w[k];
         for (int q = 0; q < 6; q++) o->c[q][k] = c6 ? c6[q][k] : ((q == 0 || q == 2 || q == 5) ? 1.0 : 0.0);
         if (o->s->cfg.form == OR_FORM_CHL || o->s->cfg.form == OR_FORM_LC) {
@@ -3252,7 +3311,7 @@ static void rhs3(Or3 *o, double *const *r) {
         /* Cholesky: full gradients of every psi component (rhs.F90:186-201) */
         if (chl) grad3(o, o->psi[q], ccls[q], 7, gc[q][0], gc[q][1], gc[q][2]);
         else grad3(o, o->c[q], ccls[q], full ? 7 : cmask[q], gc[q][0], gc[q][1], gc[q][2]);
-        if (s->cfg.Mdiff != 0.0) lap3(o, o->c[q], ccls[q], lc[q]);
+        if (s->cfg.Mdiff != 0.0) lap3_conf(o, o->c[q], ccls[q], lc[q]);
     }
     /* FENE-P (direct form): the function f = (L^2 - 3)/(L^2 - tr c) at every node and its
        gradient, rhs_di.F90:198-205 */
@@ -3317,9 +3376,41 @@ static void rhs3(Or3 *o, double *const *r) {
         r[2][k] = ((-tsv - gpy) + bfv) + fvv;
         r[3][k] = ((-tsw - gpz) + bfw) + fvw;
         for (int q = 4; q < 10; q++) r[q][k] = 0.0;
-        if (chl) { /* calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D) */
-            const double ux = G[UX][k], uy = G[UY][k], uz = G[UZ][k], vx = G[VX][k], vy = G[VY][k], vz = G[VZ][k];
-            const double wx = G[WX][k], wy = G[WY][k], wz = G[WZ][k];
+        /* the x-y velocity gradients; a wall node's are in its normal-tangent frame and turn to
+           x-y for the conformation equations (rhs_di.F90:497-517, rhs.F90:586-611,
+           rhs_lc.F90:602-627; d/dz is d/dz everywhere) */
+        const int wall = o->bidx[i] >= 0;
+        double Gux = G[UX][k], Guy = G[UY][k], Gvx = G[VX][k], Gvy = G[VY][k], Gwx = G[WX][k], Gwy = G[WY][k];
+        if (wall) {
+            const double xn = s->rnx[i], yn = s->rny[i];
+            Gux = xn * G[UX][k] - yn * G[UY][k];
+            Guy = yn * G[UX][k] + xn * G[UY][k];
+            Gvx = xn * G[VX][k] - yn * G[VY][k];
+            Gvy = yn * G[VX][k] + xn * G[VY][k];
+            Gwx = xn * G[WX][k] - yn * G[WY][k];
+            Gwy = yn * G[WX][k] + xn * G[WY][k];
+            /* calc_rhs_ro's wall branch (rhs_di.F90:149-154), the wall amplitudes of
+               calc_rhs_rovel (:291-307), the isothermal wall (characteristic_boundaries.F90:27-52:
+               L5 = L1) and the update of calc_rhs_nscbc (rhs_di.F90:601-665) */
+            const double c = sqrt(csq);
+            const double un = u * xn + v * yn;
+            const double dutdt = -yn * G[UY][k] + xn * G[VY][k];
+            const double dundn = xn * G[UX][k] + yn * G[VX][k];
+            const double dutdn = -yn * G[UX][k] + xn * G[VX][k];
+            const double L1 = (0.5 * (un - c)) * (gpx - (ro * c) * dundn);
+            const double L2 = un * (G[ROX][k] - (gpx / c) / c);
+            const double L3 = un * dutdn;
+            const double L4 = un * (G[WX][k] * xn + G[WY][k] * yn);
+            const double L5 = L1;
+            const double ts = ((((c * c) * L2 + L5) + L1) / c) / c;
+            r[0][k] = (-ro * dutdt - ro * G[WZ][k]) - ts;
+            r[1][k] = (0.0 - u * ts) - (L5 - L1) / c;
+            r[2][k] = (0.0 - v * ts) - ro * L3;
+            r[3][k] = (0.0 - w * ts) - ro * L4;
+        }
+        if (chl) { /* calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D), walls :553-717 */
+            const double ux = Gux, uy = Guy, uz = G[UZ][k], vx = Gvx, vy = Gvy, vz = G[VZ][k];
+            const double wx = Gwx, wy = Gwy, wz = G[WZ][k];
             double ad[6];
             for (int q = 0; q < 6; q++) ad[q] = (u * gc[q][0][k] + v * gc[q][1][k]) + w * gc[q][2][k];
             const double lxx = exp(o->psi[0][k]), lxy = o->psi[1][k], lyy = exp(o->psi[2][k]), lzz = exp(o->psi[5][k]);
@@ -3376,7 +3467,7 @@ static void rhs3(Or3 *o, double *const *r) {
             r[9][k] = (-ad[5] + uczz) + cszz;
             continue;
         }
-        if (islc) { /* calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D) */
+        if (islc) { /* calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D), walls :564-740 */
             const int first = (o->itime == 1 && o->iRKstep == 1);
             double ad[6];
             for (int q = 0; q < 6; q++) ad[q] = -((u * gp[q][0][k] + v * gp[q][1][k]) + w * gp[q][2][k]);
@@ -3384,9 +3475,9 @@ static void rhs3(Or3 *o, double *const *r) {
             eigens3(o->c[0][k], o->c[1][k], o->c[2][k], o->c[3][k], o->c[4][k], o->c[5][k], Lv, R);
             tr3(R, RT);
             const double tr_c = (Lv[0] + Lv[1]) + Lv[2];
-            Gm[0] = G[UX][k]; Gm[3] = G[UY][k]; Gm[6] = G[UZ][k];
-            Gm[1] = G[VX][k]; Gm[4] = G[VY][k]; Gm[7] = G[VZ][k];
-            Gm[2] = G[WX][k]; Gm[5] = G[WY][k]; Gm[8] = G[WZ][k];
+            Gm[0] = Gux; Gm[3] = Guy; Gm[6] = G[UZ][k];
+            Gm[1] = Gvx; Gm[4] = Gvy; Gm[7] = G[VZ][k];
+            Gm[2] = Gwx; Gm[5] = Gwy; Gm[8] = G[WZ][k];
             mm3(Gm, R, T);
             mm3(RT, T, M);
             double oxy = (Lv[1] * M[3] + Lv[0] * M[1]);
@@ -3420,21 +3511,18 @@ static void rhs3(Or3 *o, double *const *r) {
             mm3(Ci, RT, T);
             mm3(R, T, T);
             for (int q = 0; q < 9; q++) Rx[q] = T[q] / lambda;
-            r[4][k] = (ad[0] + UC[0]) + Rx[0];
-            r[5][k] = (ad[1] + UC[3]) + Rx[3];
-            r[6][k] = (ad[2] + UC[4]) + Rx[4];
-            r[7][k] = (ad[3] + UC[6]) + Rx[6];
-            r[8][k] = (ad[4] + UC[7]) + Rx[7];
-            r[9][k] = (ad[5] + UC[8]) + Rx[8];
+            static const int e6[6] = {0, 3, 4, 6, 7, 8};
+            for (int q = 0; q < 6; q++) /* walls: without the advection (:717-726) */
+                r[4 + q][k] = wall ? UC[e6[q]] + Rx[e6[q]] : (ad[q] + UC[e6[q]]) + Rx[e6[q]];
             continue;
         }
         if (!di) continue;
-        /* calc_rhs_c, :415-476 */
+        /* calc_rhs_c, :415-476, walls :478-590 */
         const double cxx = o->c[0][k], cxy = o->c[1][k], cyy = o->c[2][k], cxz = o->c[3][k], cyz = o->c[4][k], czz = o->c[5][k];
         double ad[6];
         for (int q = 0; q < 6; q++) ad[q] = -((u * gc[q][0][k] + v * gc[q][1][k]) + w * gc[q][2][k]);
-        const double ux = G[UX][k], uy = G[UY][k], uz = G[UZ][k], vx = G[VX][k], vy = G[VY][k], vz = G[VZ][k];
-        const double wx = G[WX][k], wy = G[WY][k], wz = G[WZ][k];
+        const double ux = Gux, uy = Guy, uz = G[UZ][k], vx = Gvx, vy = Gvy, vz = G[VZ][k];
+        const double wx = Gwx, wy = Gwy, wz = G[WZ][k];
         const double ucxx = ((2.0 * ux) * cxx + (2.0 * uy) * cxy) + (2.0 * uz) * cxz;
         const double ucxy = (((((ux * cxy + uy * cyy) + uz * cyz) + vx * cxx) + vy * cxy) + vz * cxz);
         const double ucyy = ((2.0 * vx) * cxy + (2.0 * vy) * cyy) + (2.0 * vz) * cyz;
@@ -3450,6 +3538,15 @@ static void rhs3(Or3 *o, double *const *r) {
             const double fr = -(((1.0 - eps * 2.0) + eps * ((cxx + cyy) + czz))) / lambda;
             sxx = fr * (cxx - 1.0); sxy = fr * cxy; syy = fr * (cyy - 1.0);
             sxz = fr * cxz; syz = fr * cyz; szz = fr * (czz - 1.0);
+        }
+        if (wall) { /* :571-580: without the advection */
+            r[4][k] = (ucxx + sxx) + Md * lc[0][k];
+            r[5][k] = (ucxy + sxy) + Md * lc[1][k];
+            r[6][k] = (ucyy + syy) + Md * lc[2][k];
+            r[7][k] = (ucxz + sxz) + Md * lc[3][k];
+            r[8][k] = (ucyz + syz) + Md * lc[4][k];
+            r[9][k] = (uczz + szz) + Md * lc[5][k];
+            continue;
         }
         r[4][k] = ((ad[0] + ucxx) + sxx) + Md * lc[0][k];
         r[5][k] = ((ad[1] + ucxy) + sxy) + Md * lc[1][k];
@@ -3491,7 +3588,8 @@ int or3_set_tstep(Or3 *o, double *dt_cfl, double *dt_par) {
     return 0;
 }
 
-/* step_rk3_4S_2R_EE (step.F90:218-512) in 3-D, without boundary nodes */
+/* step_rk3_4S_2R_EE (step.F90:218-512) in 3-D, with apply_time_dependent_bounds after each
+   stage and around the filter (step.F90:346, 488, 498) where the node set has walls */
 static void step3(Or3 *o) {
     const OrSim *s = o->s;
     const size_t n = o->n3;
@@ -3523,6 +3621,7 @@ static void step3(Or3 *o) {
                     reg[f][k] = reg[f][k] + RKb * r[f][k];
                     eacc[f][k] = eacc[f][k] + RKbmbh * r[f][k];
                 }
+            bounds3(o);
             for (size_t k = 0; k < n; k++) { /* get_velocity_from_momentum */
                 const double oo = 1.0 / o->ro[k];
                 o->u[k] = o->rou[k] * oo; o->v[k] = o->rov[k] * oo; o->w[k] = o->row[k] * oo;
@@ -3555,6 +3654,7 @@ static void step3(Or3 *o) {
             const double econf = MAXD(en[4], MAXD(en[5], MAXD(en[6], MAXD(en[7], MAXD(en[8], en[9])))));
             o->emax_np1 = MAXD(econf, MAXD(en[0], MAXD(en[1], MAXD(en[2], MAXD(en[3], doublesmall)))));
 #undef MAXD
+            bounds3(o);
         }
     }
     /* filter_variables (rhs_di.F90:667-720): ro, rou, rov, row, then c; the mass correction */
@@ -3585,6 +3685,7 @@ static void step3(Or3 *o) {
         const double dro = tm / tv;
         for (size_t k = 0; k < n; k++) o->ro[k] = o->ro[k] - dro;
     }
+    bounds3(o);
     for (size_t k = 0; k < n; k++) {
         const double oo = 1.0 / o->ro[k];
         o->u[k] = o->rou[k] * oo; o->v[k] = o->rov[k] * oo; o->w[k] = o->row[k] * oo;

@@ -1,5 +1,5 @@
 // step3d.cu -- the 3-D (-Ddim3) time step of the direct, Cholesky, log-conformation (sPTT) and
-// Newtonian forms on node sets without boundary nodes.
+// Newtonian forms on node sets without boundary nodes or with walls (node_type 0) among them.
 //
 // The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
 // setup_domain.F90:435-547), layer-major in the reference (node iz*nl + i at z = iz*dz).  On the
@@ -20,6 +20,14 @@
 // update from there, so the derivatives never cross HBM; the filter as the x-y filter
 // followed by the z filter of its result (derivatives.F90:387-405); the mass correction and
 // the derived fields; all FP64.
+//
+// Walls: build_3rd_dimension copies node_type and the normals to every layer
+// (setup_domain.F90:487-532).  A wall node's x-y operators are its boundary weights (d/dn and
+// d/dt), so the gather is unchanged, except that its Laplacian weights are the tangential
+// second-derivative ones (calc_laplacian_transverse_only_on_bound, derivatives.F90:306-358;
+// the velocity Laplacians, which would differ, are not read on walls).  The wall branches of the
+// right-hand sides run in point3_body<FORM, true>, and apply_time_dependent_bounds holds
+// rho u, rho v, rho w at zero there after each stage and after the filter.
 #include "internal.cuh"
 
 namespace sunset {
@@ -346,6 +354,9 @@ struct Point3 {
     StepConsts K;
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
+    // walls: node types, normals into the fluid, boundary index and FD rows, spacing
+    const int *ntype, *bidx, *brow;
+    const double *rnx, *rny, *sp;
     const double *fen;                    // FENE-P function of the direct form, or null
     int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
@@ -549,17 +560,19 @@ __device__ __forceinline__ void chl3_fenep_factor(double L2, double *p, bool to_
 }
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
-// 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).
+// 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).  WALL: the node
+// set has walls, whose node-layers take the wall branches.
 //
 // GET(slot) returns derivative `slot` of node-layer k (global arrays, or the fused kernel's
 // shared memory); the bits of the node-layer's step error norm are returned (stage 3).
-template <int FORM, class GET>
+template <int FORM, bool WALL, class GET>
 __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_t k, GET g) {
     constexpr bool kDi = FORM == SUNSET_FORM_DI, kChl = FORM == SUNSET_FORM_CHL, kLc = FORM == SUNSET_FORM_LC;
     unsigned long long eb = 0;
     {
         const StepConsts &K = P.K;
         const int i = (int)((unsigned)k / (unsigned)P.nz);
+        const bool wall = WALL && P.ntype[i] == 0;
         const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
         const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
         const double tmp = ((u * g(ROX) + v * g(ROY)) + w * g(ROZ));
@@ -610,9 +623,51 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
         r[2] = ((-tsv - gpy) + bfv) + fvv;
         r[3] = ((-tsw - gpz) + bfw) + fvw;
         for (int q = 4; q < 10; q++) r[q] = 0.0;
-        if (kChl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D)
-            const double ux = g(UX), uy = g(UY), uz = g(UZ), vx = g(VX), vy = g(VY), vz = g(VZ);
-            const double wx = g(WX), wy = g(WY), wz = g(WZ);
+        // the x-y velocity gradients; a wall node's are in its normal-tangent frame and turn to
+        // x-y for the conformation equations (rhs_di.F90:497-517, rhs.F90:586-611,
+        // rhs_lc.F90:602-627; d/dz is d/dz everywhere)
+        double gux = g(UX), guy = g(UY), gvx = g(VX), gvy = g(VY), gwx = g(WX), gwy = g(WY);
+        // the conformation Laplacian on a wall adds the one-sided normal second derivative
+        // over the node's four FD rows, the next nodes of its layer (rhs_di.F90:553-568,
+        // rhs.F90:631-643)
+        auto fdrows = [&](int q) {
+            const int *rw = P.brow + 4 * P.bidx[i];
+            const int iz = (int)k - i * P.nz;
+            const double *c = P.in[7 + q];
+            const double den = (((72.0 * P.sp[i]) * P.sp[i]) * K.L_char) * K.L_char;
+            return (((((-415.0 * c[k]) + 576.0 * c[rw[0] * P.nz + iz]) - 216.0 * c[rw[1] * P.nz + iz]) +
+                     64.0 * c[rw[2] * P.nz + iz]) - 9.0 * c[rw[3] * P.nz + iz]) / den;
+        };
+        if (wall) {
+            const double xn = P.rnx[i], yn = P.rny[i];
+            gux = xn * g(UX) - yn * g(UY);
+            guy = yn * g(UX) + xn * g(UY);
+            gvx = xn * g(VX) - yn * g(VY);
+            gvy = yn * g(VX) + xn * g(VY);
+            gwx = xn * g(WX) - yn * g(WY);
+            gwy = yn * g(WX) + xn * g(WY);
+            // calc_rhs_ro's wall branch (rhs_di.F90:149-154), the wall amplitudes of
+            // calc_rhs_rovel (:291-307), the isothermal wall (characteristic_boundaries.F90:27-52:
+            // L5 = L1) and the update of calc_rhs_nscbc (rhs_di.F90:601-665)
+            const double c = sqrt(K.csq);
+            const double un = u * xn + v * yn;
+            const double dutdt = -yn * g(UY) + xn * g(VY);
+            const double dundn = xn * g(UX) + yn * g(VX);
+            const double dutdn = -yn * g(UX) + xn * g(VX);
+            const double L1 = (0.5 * (un - c)) * (gpx - (ro * c) * dundn);
+            const double L2 = un * (g(ROX) - (gpx / c) / c);
+            const double L3 = un * dutdn;
+            const double L4 = un * (g(WX) * xn + g(WY) * yn);
+            const double L5 = L1;
+            const double ts = ((((c * c) * L2 + L5) + L1) / c) / c;
+            r[0] = (-ro * dutdt - ro * g(WZ)) - ts;
+            r[1] = (0.0 - u * ts) - (L5 - L1) / c;
+            r[2] = (0.0 - v * ts) - ro * L3;
+            r[3] = (0.0 - w * ts) - ro * L4;
+        }
+        if (kChl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D), walls :553-717
+            const double ux = gux, uy = guy, uz = g(UZ), vx = gvx, vy = gvy, vz = g(VZ);
+            const double wx = gwx, wy = gwy, wz = g(WZ);
             double ad[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) ad[q] = (u * gp(q, 0) + v * gp(q, 1)) + w * gp(q, 2);
@@ -631,7 +686,11 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             const double cxx = P.in[7][k], cxy = P.in[8][k], cyy = P.in[9][k], cxz = P.in[10][k], cyz = P.in[11][k],
                          czz = P.in[12][k];
             const double Md = K.Mdiff;
-            auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
+            auto lc = [&](int q) {
+                if (!P.md) return 0.0;
+                const double x = g(LC0 + q);
+                return wall ? x + fdrows(q) : x;
+            };
             double sxx, sxy, syy, sxz, syz, szz;
             if (K.fenep) {  // rhs.F90:204-209, 479-500: the factors of J = f c
                 const double L2 = K.fenep_l2, la = K.lambda;
@@ -672,7 +731,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             r[8] = (-ad[4] + ucyz) + csyz;
             r[9] = (-ad[5] + uczz) + cszz;
         }
-        if (kLc) {  // calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D)
+        if (kLc) {  // calc_rhs_logconf, rhs_lc.F90:383-560 (sPTT, 3-D), walls :564-740
             const bool first = (P.sc->itime == 1) && (P.stage == 0);
             double ad[6];
 #pragma unroll
@@ -681,9 +740,9 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             eigens3(P.in[7][k], P.in[8][k], P.in[9][k], P.in[10][k], P.in[11][k], P.in[12][k], Lv, R);
             tr3(R, RT);
             const double tr_c = (Lv[0] + Lv[1]) + Lv[2];
-            Gm[0] = g(UX); Gm[3] = g(UY); Gm[6] = g(UZ);
-            Gm[1] = g(VX); Gm[4] = g(VY); Gm[7] = g(VZ);
-            Gm[2] = g(WX); Gm[5] = g(WY); Gm[8] = g(WZ);
+            Gm[0] = gux; Gm[3] = guy; Gm[6] = g(UZ);
+            Gm[1] = gvx; Gm[4] = gvy; Gm[7] = g(VZ);
+            Gm[2] = gwx; Gm[5] = gwy; Gm[8] = g(WZ);
             mm3(Gm, R, T);
             mm3(RT, T, M);
             double oxy = (Lv[1] * M[3] + Lv[0] * M[1]);
@@ -721,7 +780,8 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 const int e = idx[q];
-                r[4 + q] = (ad[q] + ((OP[e] - PO[e]) + 2.0 * B[e])) + Rx[e];
+                const double uc = (OP[e] - PO[e]) + 2.0 * B[e];
+                r[4 + q] = wall ? uc + Rx[e] : (ad[q] + uc) + Rx[e];  // walls: no advection (:717-726)
             }
         }
         if (kDi) {
@@ -730,8 +790,8 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             double ad[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) ad[q] = -((u * g(CG0 + 3 * q) + v * g(CG0 + 3 * q + 1)) + w * g(CG0 + 3 * q + 2));
-            const double ux = g(UX), uy = g(UY), uz = g(UZ), vx = g(VX), vy = g(VY), vz = g(VZ);
-            const double wx = g(WX), wy = g(WY), wz = g(WZ);
+            const double ux = gux, uy = guy, uz = g(UZ), vx = gvx, vy = gvy, vz = g(VZ);
+            const double wx = gwx, wy = gwy, wz = g(WZ);
             const double ucxx = ((2.0 * ux) * cxx + (2.0 * uy) * cxy) + (2.0 * uz) * cxz;
             const double ucxy = (((((ux * cxy + uy * cyy) + uz * cyz) + vx * cxx) + vy * cxy) + vz * cxz);
             const double ucyy = ((2.0 * vx) * cxy + (2.0 * vy) * cyy) + (2.0 * vz) * cyz;
@@ -749,13 +809,26 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                 sxz = fr * cxz; syz = fr * cyz; szz = fr * (czz - 1.0);
             }
             const double Md = K.Mdiff;
-            auto lc = [&](int q) { return P.md ? g(LC0 + q) : 0.0; };
-            r[4] = ((ad[0] + ucxx) + sxx) + Md * lc(0);
-            r[5] = ((ad[1] + ucxy) + sxy) + Md * lc(1);
-            r[6] = ((ad[2] + ucyy) + syy) + Md * lc(2);
-            r[7] = ((ad[3] + ucxz) + sxz) + Md * lc(3);
-            r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
-            r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
+            auto lc = [&](int q) {
+                if (!P.md) return 0.0;
+                const double x = g(LC0 + q);
+                return wall ? x + fdrows(q) : x;
+            };
+            if (wall) {  // rhs_di.F90:571-580: without the advection
+                r[4] = (ucxx + sxx) + Md * lc(0);
+                r[5] = (ucxy + sxy) + Md * lc(1);
+                r[6] = (ucyy + syy) + Md * lc(2);
+                r[7] = (ucxz + sxz) + Md * lc(3);
+                r[8] = (ucyz + syz) + Md * lc(4);
+                r[9] = (uczz + szz) + Md * lc(5);
+            } else {
+                r[4] = ((ad[0] + ucxx) + sxx) + Md * lc(0);
+                r[5] = ((ad[1] + ucxy) + sxy) + Md * lc(1);
+                r[6] = ((ad[2] + ucyy) + syy) + Md * lc(2);
+                r[7] = ((ad[3] + ucxz) + sxz) + Md * lc(3);
+                r[8] = ((ad[4] + ucyz) + syz) + Md * lc(4);
+                r[9] = ((ad[5] + uczz) + szz) + Md * lc(5);
+            }
         }
         const int nf = (kDi || kChl || kLc) ? 10 : 4;
         if (P.stage == 4) {
@@ -803,6 +876,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                 }
             }
             if (stage == 3) eb = dbits(en);
+            if (wall) { Un[1] = 0.0; Un[2] = 0.0; Un[3] = 0.0; }  // apply_time_dependent_bounds
             for (int q = 0; q < 10; q++) P.out[src[q]][k] = Un[q];
             const double oo = 1.0 / Un[0];  // get_velocity_from_momentum
             P.out[4][k] = Un[1] * oo;
@@ -838,7 +912,7 @@ __device__ __forceinline__ void block_emax3(unsigned long long eb, DevScalars *s
 // One stage fused: the derivatives of node-layer k (derivs3_body) go to this block's shared
 // memory, compact slots of 128 doubles (one per thread), and the pointwise right-hand side
 // and RK update (point3_body) read them there, so no derivative array crosses HBM.
-template <int FORM, bool MD, bool FULL, bool FEN>
+template <int FORM, bool MD, bool FULL, bool FEN, bool WALL>
 __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_stage(Layer3 L, Fields3 F, Point3 P) {
     constexpr int NS = ngslots<FORM, MD, FULL, FEN>();
     __shared__ double sg[NS * 128];
@@ -850,7 +924,7 @@ __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_stage(Layer3 
             const int c = kGTable<FORM, MD, FULL, FEN>.idx[slot];
             if (c >= 0) sg[c * 128 + threadIdx.x] = v;
         });
-        eb = point3_body<FORM>(P, (size_t)z.k, [&](int a) {
+        eb = point3_body<FORM, WALL>(P, (size_t)z.k, [&](int a) {
             const int c = kGTable<FORM, MD, FULL, FEN>.idx[a];
             return c >= 0 ? sg[c * 128 + threadIdx.x] : 0.0;
         });
@@ -891,15 +965,22 @@ __global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, 
     if (threadIdx.x == 0) *out = divisor ? (enabled ? red[0] / *divisor : 0.0) : red[0];
 }
 
-// End of step: mass correction, u, v, w from the momentum, the error-norm history and time.
-__global__ void k3_finalize(size_t n, Fields3 F, int chl, int lc, double L2, DevScalars *sc, int vpid) {
+// End of step: mass correction, apply_time_dependent_bounds on walls (ntype: node types, or
+// null without walls), u, v, w from the momentum, the error-norm history and time.
+__global__ void k3_finalize(size_t n, int nz, const int *ntype, Fields3 F, int chl, int lc, double L2, DevScalars *sc,
+                            int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         // every load before the first store (the arrays are not known to be distinct)
-        const double r = F.p[0][k] - sc->dro, m1 = F.p[1][k], m2 = F.p[2][k], m3 = F.p[3][k];
+        const double r = F.p[0][k] - sc->dro;
+        double m1 = F.p[1][k], m2 = F.p[2][k], m3 = F.p[3][k];
         double p[6], c[6];
         if (chl || lc)
             for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
+        if (ntype && ntype[(unsigned)k / (unsigned)nz] == 0) {
+            m1 = 0.0; m2 = 0.0; m3 = 0.0;
+            F.p[1][k] = 0.0; F.p[2][k] = 0.0; F.p[3][k] = 0.0;
+        }
         F.p[0][k] = r;
         const double oo = 1.0 / r;
         F.p[4][k] = m1 * oo;
@@ -1016,14 +1097,30 @@ __global__ void k3_fenep_factors(size_t n, Filter3 A, double L2, int to_c) {
     chl3_fenep_factor(L2, p, to_c != 0);
     for (int q = 0; q < 6; q++) A.f[4 + q][k] = p[q];
 }
-// hardcode_initial_conditions in 3-D: rho u = rho * u, rho v, rho w
-__global__ void k3_momentum(size_t n, const double *ro, const double *u, const double *v, const double *w, double *rou,
-                            double *rov, double *row) {
+// hardcode_initial_conditions in 3-D: u, v, w zero on walls (setup_flow.F90:266-280; ntype
+// null without walls), then rho u = rho * u, rho v, rho w
+__global__ void k3_momentum(size_t n, int nz, const int *ntype, const double *ro, double *u, double *v, double *w,
+                            double *rou, double *rov, double *row) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
+    if (ntype && ntype[(unsigned)k / (unsigned)nz] == 0) {
+        u[k] = 0.0; v[k] = 0.0; w[k] = 0.0;
+    }
     rou[k] = ro[k] * u[k];
     rov[k] = ro[k] * v[k];
     row[k] = ro[k] * w[k];
+}
+// walls: the layer's Laplacian weights and sums, each wall node's replaced by its tangential
+// second-derivative weights (reference link order, as the layer's lists) and their sum
+__global__ void k3_wall_lap_weights(int nl, const int *ntype, const int *bidx, const long long *slice_ptr,
+                                    const int *cnt_small, int nplink, const double *wbt, const double *wbt_sum,
+                                    double *wl3, double *lsum3) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nl || ntype[i] != 0) return;
+    const int jj = bidx[i];
+    const long long base = slice_ptr[i >> 5];
+    for (int q = 0; q < cnt_small[i]; q++) wl3[sell_at(base, q, i & 31)] = wbt[(size_t)jj * nplink + q];
+    lsum3[i] = wbt_sum[jj];
 }
 
 // calc_fd_weights, fd.F90:52-172, then the L_char scaling of :246-247
@@ -1084,8 +1181,8 @@ Layer3 layer3(const Handle *H) {
     L.cnt = H->cnt;
     L.cnt_small = H->cnt_small;
     L.lidx = H->lidx;
-    L.wx = H->wx; L.wy = H->wy; L.wl = H->wl; L.wh = H->wh;
-    L.gsx = H->gsx; L.gsy = H->gsy; L.lsum = H->lsum; L.hsum = H->hsum;
+    L.wx = H->wx; L.wy = H->wy; L.wl = H->nb > 0 ? H->wl3 : H->wl; L.wh = H->wh;
+    L.gsx = H->gsx; L.gsy = H->gsy; L.lsum = H->nb > 0 ? H->lsum3 : H->lsum; L.hsum = H->hsum;
     for (int m = 0; m < kMaxFd; m++) { L.fdg[m] = H->fdg[m]; L.fdl[m] = H->fdl[m]; L.fdh[m] = H->fdh[m]; }
     return L;
 }
@@ -1115,6 +1212,12 @@ Point3 point3(Handle *H, int b, int stage) {
     P.full = H->cfg.di_full_gradients;
     P.md = H->cfg.Mdiff != 0.0;
     P.py = H->py;
+    P.ntype = H->ntype;
+    P.bidx = H->bidx;
+    P.brow = H->brow;
+    P.rnx = H->rnx;
+    P.rny = H->rny;
+    P.sp = H->sp;
     P.fen = (H->cfg.form == SUNSET_FORM_DI && H->cfg.fenep) ? H->tmp3 : nullptr;
     for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
@@ -1136,7 +1239,10 @@ int stage3_launch(Handle *H, int b, int stage) {
         k3_fenep<<<nblk(n), 128, 0, H->stream>>>((unsigned)n, H->f3[b][7], H->f3[b][9], H->f3[b][12], H->cfg.fenep_l2, H->tmp3);
         F.p[19] = H->tmp3;
     }
-    k3_stage<FORM, MD, FULL, FEN><<<zblocks(H), 128, 0, H->stream>>>(layer3(H), F, point3(H, b, stage));
+    if (H->nb > 0)
+        k3_stage<FORM, MD, FULL, FEN, true><<<zblocks(H), 128, 0, H->stream>>>(layer3(H), F, point3(H, b, stage));
+    else
+        k3_stage<FORM, MD, FULL, FEN, false><<<zblocks(H), 128, 0, H->stream>>>(layer3(H), F, point3(H, b, stage));
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -1175,7 +1281,8 @@ int tstep3_launch(Handle *H, int b, int pid) {
 // ---------------------------------------------------------------------------------------
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
-    if (H->nb > 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers node sets without boundary nodes");
+    for (int t : H->h_btype)
+        if (t != 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers walls among the boundary nodes, not inflow or outflow");
     if (H->cfg.fenep && H->cfg.form != SUNSET_FORM_DI && H->cfg.form != SUNSET_FORM_CHL)
         return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers FENE-P with the direct and Cholesky forms");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
@@ -1221,6 +1328,15 @@ static int state3_alloc(Handle *H) {
     if (dalloc(H, &H->g3, (size_t)10 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
     for (int b = 0; b < 2; b++)
         for (int f = 7; f < 19; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
+    if (H->nb > 0) {  // the wall nodes' Laplacian weights of the layer (after the set-up's weights)
+        if (!H->wbt) return set_err(H, SUNSET_ERR_ARG, "call order: the set-up's weights first");
+        if (dalloc(H, &H->wl3, (size_t)H->nlinks_sell) || dalloc(H, &H->lsum3, (size_t)H->npfb)) return SUNSET_ERR_NOMEM;
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->wl3, H->wl, (size_t)H->nlinks_sell * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->lsum3, H->lsum, (size_t)H->npfb * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
+        k3_wall_lap_weights<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->ntype, H->bidx, H->slice_ptr, H->cnt_small,
+                                                                        H->nplink, H->wbt, H->wbt_sum, H->wl3, H->lsum3);
+        SUNSET_CUDA(H, cudaGetLastError());
+    }
     const unsigned nb = nblk(n);
     if (!H->partials3 && dalloc(H, &H->partials3, (size_t)nb + 16)) return SUNSET_ERR_NOMEM;
     if (!H->dsc) {
@@ -1246,7 +1362,7 @@ int state3_set(Handle *H, const double *const *fields10) {
         SUNSET_CUDA(H, cudaMemcpyAsync(H->tmp3, fields10[q], n * sizeof(double), cudaMemcpyHostToDevice, st));
         k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, H->nz, n, d);
     }
-    k3_momentum<<<nblk(n), 128, 0, st>>>(n, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
+    k3_momentum<<<nblk(n), 128, 0, st>>>(n, H->nz, H->nb > 0 ? H->ntype : nullptr, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
     if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = f[q];
@@ -1337,7 +1453,8 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
         k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
-        k3_finalize<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->cfg.fenep ? H->cfg.fenep_l2 : 0.0, H->dsc, H->cfg.vpid);
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, H->nz, H->nb > 0 ? H->ntype : nullptr, F19, chl, lc,
+                                             H->cfg.fenep ? H->cfg.fenep_l2 : 0.0, H->dsc, H->cfg.vpid);
         SUNSET_CUDA(H, cudaGetLastError());
         H->cur3 = b;
     }

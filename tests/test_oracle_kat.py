@@ -424,6 +424,56 @@ def test_3d_reduces_to_2d(form, eps, fenep):
         assert np.abs(r3[k]).max() < 1e-9 * max(np.abs(r2["rou"]).max(), 1.0), (form, k)
 
 
+@pytest.mark.parametrize("form, eps, mdiff, fenep", [("di", 0.25, 1e-3, False), ("chl", 0.25, 1e-3, False),
+                                                     ("lc", 0.0, 0.0, False), ("newt", 0.0, 0.0, False),
+                                                     ("di", 0.0, 1e-3, True), ("chl", 0.0, 1e-3, True)])
+def test_3d_walls_reduce_to_2d(form, eps, mdiff, fenep):
+    """3-D restatement with walls, known answer: on a channel (walls at y = 0 and 1, node_type
+    0) a state that does not vary in z, with w = 0, c_xz = c_yz = 0 and c_zz = 1, gives on every
+    layer the 2-D right-hand side, the wall nodes' included: the wall closure of the flow
+    (rhs_di.F90:149-154, 291-307, 601-665 with characteristic_boundaries.F90:27-52; its dim3
+    terms, rho dw/dz and L4, vanish), the conformation equations with the rotated velocity
+    gradients, and under polymer diffusion the tangential Laplacian with the one-sided normal
+    second derivative over the FD rows (rhs_di.F90:553-580, rhs.F90:631-643).  The
+    log-conformation form takes eps = 0 (its 3-D trace includes c_zz).  After a few steps
+    rho u, rho v and rho w stay zero on the walls (apply_time_dependent_bounds)."""
+    G = 8.0
+    ns = channel(24)
+    extra = dict(fenep=True, fenep_l2=30.0) if fenep else {}
+    o = O.Oracle(form=form, order=6, Re=1.0, Wi=0.5, beta=0.59, Ma=0.1, grav=(G, 0.0, 0.0), kolmogorov_forcing=0,
+                 epsPTT=eps, Mdiff=mdiff, **extra).build_domain(ns).setup()
+    o3 = O.Oracle3(o, 0.4)
+    nl = o3.nl
+    nd = o.nodes()
+    x, y, t = nd["x"][:nl], nd["y"][:nl], nd["node_type"][:nl]
+    assert np.sum(t == 0) > 0
+    st = poiseuille_state(type("P", (), {"y": y, "n": nl}), G, 1.0, 0.5)
+    st["u"] = st["u"] + 0.3 * np.sin(2 * np.pi * x) * y * (1.0 - y)
+    st["v"] = 0.2 * np.cos(2 * np.pi * x) * y * (1.0 - y)
+    st["ro"] = 1.0 + 0.01 * np.sin(2 * np.pi * x) * np.cos(np.pi * y)
+    st["cxx"] = st["cxx"] + 0.1 * np.sin(2 * np.pi * x) ** 2
+    st["cyy"] = st["cyy"] + 0.05 * np.cos(np.pi * y) ** 2
+    o.set_state(st["ro"], st["u"], st["v"], st["cxx"], st["cxy"], st["cyy"], np.ones(nl))
+    r2 = o.rhs()
+    T = lambda a: np.tile(a, o3.nz)
+    zero = np.zeros(o3.n)
+    o3.set_state(T(st["ro"]), T(st["u"]), T(st["v"]), zero, T(st["cxx"]), T(st["cxy"]), T(st["cyy"]), zero, zero,
+                 np.ones(o3.n))
+    r3 = o3.rhs()
+    keys = ["ro", "rou", "rov"] + ([] if form == "newt" else ["xx", "xy", "yy"])
+    for k in keys:
+        scale = max(np.abs(r2[k]).max(), 1.0)
+        d = np.abs(r3[k].reshape(o3.nz, nl) - r2[k][None, :])
+        assert d.max() / scale < 1e-9, (form, k, d.max() / scale)
+        assert d[:, t == 0].max() / scale < 1e-13, (form, k, "walls")
+    dc, dp = o3.set_tstep()
+    o3.step(0.3 * min(dc, dp), 3)
+    s3 = o3.state()
+    for k in ("rou", "rov", "row", "u", "v", "w"):
+        assert np.all(s3[k].reshape(o3.nz, nl)[:, t == 0] == 0.0), k
+    assert all(np.isfinite(a).all() for a in s3.values())
+
+
 def central_first_derivative(m):
     """Weights a_1..a_m of the central difference of 2m + 1 points for d/dz, from Taylor
     matching in exact rationals: sum_j a_j j^(2q-1) = 1/2 for q = 1 and 0 for q = 2..m."""
