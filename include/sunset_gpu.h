@@ -177,8 +177,8 @@ int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nste
 int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *ms);
 
 /* ---- 3-D (-Ddim3): direct, Cholesky, log-conformation (sPTT) and Newtonian forms, FENE-P with
-   the direct and Cholesky forms, FP64, node sets without boundary nodes or with walls
-   (node_type 0; inflow and outflow nodes: SUNSET_ERR_SCOPE) ---- */
+   the direct and Cholesky forms, FP64, node sets with or without boundary nodes (walls, inflow,
+   outflow), the flow-rate controller ---- */
 /* build_3rd_dimension (setup_domain.F90:435-547) and calc_fd_weights (fd.F90:27-256): after
    sunset_build_domain, the node set becomes nz layers in z over L_domain_z (the control file's
    value): dz from the mean spacing, nz = ceiling(L_domain_z/dz), at least ij_count_fd/2 + 2,
@@ -186,8 +186,10 @@ int sunset_step_timed(SunsetHandle *h, double dt, int nsteps, int mode, double *
    weights are built for the layer (the same calls as in 2-D) and serve every layer.  Then
    sunset_set_state_3d, and sunset_step / sunset_set_tstep / sunset_get_time act on the 3-D
    state.  Arrays are npfb*nz, layer-major (node iz*npfb + i, reference order in the layer).
-   Walls are walls of every layer (node_type and normals copied, :487-532): the velocity is
-   zero there and the wall branches of the right-hand sides apply, with their dim3 terms. */
+   Boundary nodes are boundary nodes of every layer (node_type and normals copied, :487-532):
+   the wall and inflow/outflow branches of the right-hand sides apply with their dim3 terms,
+   u_inflow_local is kept for every inflow node-layer, and sunset_get_flow_control /
+   sunset_set_flow_control read and set the controller of a -Dvpid run as in 2-D. */
 int sunset_set_layers(SunsetHandle *h, double L_domain_z);
 int sunset_get_layers(SunsetHandle *h, int *nz, double *dz);
 /* initial_solution in 3-D: rho, u, v, w and the six c components (all NULL: c = I) */

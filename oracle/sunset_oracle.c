@@ -2810,6 +2810,7 @@ struct Or3 {
     int itime, iRKstep;
     double emax_nm1, emax_n, emax_np1;
     int *bidx;               /* nl: the layer node's index in boundary_list, or -1 */
+    double *uin;             /* n3: u_inflow_local of each node-layer (inflow node-layers' in use) */
     char err[256];
 };
 
@@ -2860,8 +2861,6 @@ static int fd_tables(int ncfd, double dz, double L, double *g, double *g2, doubl
 Or3 *or3_create(OrSim *s, double Lz) {
     if (!s || !s->have_weights || (s->cfg.fenep && s->cfg.form != OR_FORM_DI && s->cfg.form != OR_FORM_CHL) || !(Lz > 0.0))
         return NULL;
-    for (int jj = 0; jj < s->nb; jj++) /* walls only among the boundary nodes */
-        if (s->type[s->boundary_list[jj]] != 0) return NULL;
     Or3 *o = (Or3 *)xcalloc(1, sizeof(Or3));
     o->s = s;
     o->nl = s->npfb;
@@ -2890,6 +2889,7 @@ Or3 *or3_create(OrSim *s, double Lz) {
     double **a[] = {&o->ro, &o->rou, &o->rov, &o->row, &o->u, &o->v, &o->w, &o->c[0], &o->c[1], &o->c[2], &o->c[3], &o->c[4], &o->c[5],
                     &o->psi[0], &o->psi[1], &o->psi[2], &o->psi[3], &o->psi[4], &o->psi[5]};
     for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) *a[k] = (double *)xcalloc(o->n3, sizeof(double));
+    o->uin = (double *)xcalloc(o->n3, sizeof(double));
     return o;
 }
 
@@ -2899,6 +2899,7 @@ void or3_destroy(Or3 *o) {
                    o->psi[0], o->psi[1], o->psi[2], o->psi[3], o->psi[4], o->psi[5]};
     for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) free(a[k]);
     free(o->bidx);
+    free(o->uin);
     free(o);
 }
 
@@ -3235,14 +3236,22 @@ static void or3_c_from_psi(Or3 *o) {
     }
 }
 
-/* apply_time_dependent_bounds on the walls of every layer (characteristic_boundaries.F90:
-   191-257): rho u = rho v = rho w = 0 */
+/* apply_time_dependent_bounds on every layer (characteristic_boundaries.F90:191-257) at the
+   time o->time: update_u_inflow (:262-300, the ramp while time <= ramp_time), then walls at
+   rest, and a hard inflow's momentum prescribed (rho u = u_inflow_local rho, rho v = rho w = 0) */
 static void bounds3(Or3 *o) {
     const OrSim *s = o->s;
+    const int ramp = s->cfg.inflow_velocity_control == 1 && o->time <= s->cfg.ramp_time;
+    const double um = s->cfg.u_inflow_start + ((s->cfg.u_inflow_end - s->cfg.u_inflow_start) * o->time) / s->cfg.ramp_time;
     for (int iz = 0; iz < o->nz; iz++)
         for (int jj = 0; jj < s->nb; jj++) {
-            const size_t k = (size_t)iz * o->nl + s->boundary_list[jj];
-            o->rou[k] = 0.0; o->rov[k] = 0.0; o->row[k] = 0.0;
+            const int i = s->boundary_list[jj];
+            const size_t k = (size_t)iz * o->nl + i;
+            if (s->type[i] == 1 && ramp) o->uin[k] = um;
+            if (s->type[i] == 0) { o->rou[k] = 0.0; o->rov[k] = 0.0; o->row[k] = 0.0; }
+            else if (s->type[i] == 1 && s->cfg.inflow_type == 1) {
+                o->rou[k] = o->uin[k] * o->ro[k]; o->rov[k] = 0.0; o->row[k] = 0.0;
+            }
         }
 }
 
@@ -3252,7 +3261,7 @@ int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, co
                   const double *const *c6) {
     for (size_t k = 0; k < o->n3; k++) {
         o->ro[k] = ro[k]; o->u[k] = u[k]; o->v[k] = v[k]; o->w[k] = w[k];
-        if (o->bidx[k % o->nl] >= 0) { o->u[k] = 0.0; o->v[k] = 0.0; o->w[k] = 0.0; }
+        if (o->bidx[k % o->nl] >= 0 && o->s->type[k % o->nl] == 0) { o->u[k] = 0.0; o->v[k] = 0.0; o->w[k] = 0.0; }
         o->rou[k] = o->ro[k] * o->u[k]; o->rov[k] = o->ro[k] * o->v[k]; o->row[k] = o->ro[k] * o->w[k];
         for (int q = 0; q < 6; q++) o->c[q][k] = c6 ? c6[q][k] : ((q == 0 || q == 2 || q == 5) ? 1.0 : 0.0);
         if (o->s->cfg.form == OR_FORM_CHL || o->s->cfg.form == OR_FORM_LC) {
@@ -3265,8 +3274,16 @@ int or3_set_state(Or3 *o, const double *ro, const double *u, const double *v, co
         }
     }
     or3_c_from_psi(o);
+    /* u_inflow_local (setup_flow.F90:48-50,128-138): u_char, the initial u on inflow nodes */
+    for (size_t k = 0; k < o->n3; k++) {
+        const int i = (int)(k % o->nl);
+        o->uin[k] = (o->bidx[i] >= 0 && o->s->type[i] == 1) ? o->u[k] : o->s->cfg.U_char;
+    }
     o->time = 0.0; o->itime = 0; o->dt = 1.0e-6;
     o->emax_np1 = o->emax_n = o->emax_nm1 = pid_tol;
+    /* the flow-rate controller's state (setup_flow.F90:165-169) */
+    o->s->driving_force[0] = o->s->driving_force[1] = o->s->driving_force[2] = 0.0;
+    o->s->eflow_nm1 = 1.0; o->s->sum_eflow = 0.0;
     return 0;
 }
 int or3_get_state(Or3 *o, double *out /* 19 x n3: ro rou rov row u v w cxx cxy cyy cxz cyz czz, psi x 6 */) {
@@ -3379,7 +3396,7 @@ static void rhs3(Or3 *o, double *const *r) {
         /* the x-y velocity gradients; a wall node's are in its normal-tangent frame and turn to
            x-y for the conformation equations (rhs_di.F90:497-517, rhs.F90:586-611,
            rhs_lc.F90:602-627; d/dz is d/dz everywhere) */
-        const int wall = o->bidx[i] >= 0;
+        const int ty = o->bidx[i] >= 0 ? s->type[i] : 999, wall = ty == 0, inout = ty == 1 || ty == 2;
         double Gux = G[UX][k], Guy = G[UY][k], Gvx = G[VX][k], Gvy = G[VY][k], Gwx = G[WX][k], Gwy = G[WY][k];
         if (wall) {
             const double xn = s->rnx[i], yn = s->rny[i];
@@ -3407,12 +3424,62 @@ static void rhs3(Or3 *o, double *const *r) {
             r[1][k] = (0.0 - u * ts) - (L5 - L1) / c;
             r[2][k] = (0.0 - v * ts) - ro * L3;
             r[3][k] = (0.0 - w * ts) - ro * L4;
+        } else if (inout) {
+            /* inflow (node_type 1) and outflow (2) in the x-y frame: calc_rhs_ro's in/out branch
+               (rhs_di.F90:155-157), the amplitudes and the transverse, viscous and body-force
+               terms of calc_rhs_rovel (:311-359; no Kolmogorov forcing), the closure of
+               characteristic_boundaries.F90 for the node's type (soft :54-80, hard :82-110,
+               inflow-outflow :112-150, outflow :152-189) and calc_rhs_nscbc (:601-665) */
+            const double c = sqrt(csq), p = csq * ro, uinf = o->uin[k];
+            const double nscbc = 2.87e-1, Lx = (s->xmax - s->xmin) * s->cfg.L_char, pin = s->rho_char * s->csq;
+            const double rro = ((-v * G[ROY][k] - ro * G[VY][k]) - w * G[ROZ][k]) - ro * G[WZ][k];
+            double L1 = (0.5 * (u - c)) * (gpx - (ro * c) * G[UX][k]);
+            double L2 = u * (G[ROX][k] - (gpx / c) / c);
+            double L3 = u * G[VX][k];
+            double L4 = u * G[WX][k];
+            double L5 = (0.5 * (u + c)) * (gpx + (ro * c) * G[UX][k]);
+            const double bu = ro * (g[0] + df[0]), bv = ro * (g[1] + df[1]), bw = ro * (g[2] + df[2]);
+            const double rou = ((-(v * G[UY][k]) - w * G[UZ][k]) + fvu) + bu;
+            const double rov = (((-(v * G[VY][k]) - w * G[VZ][k]) - gpy) + fvv) + bv;
+            const double row = (((-(v * G[WY][k]) - w * G[WZ][k]) - gpz) + fvw) + bw;
+            if (ty == 1) {
+                if (s->cfg.inflow_type == 1) {
+                    L2 = 0.0; L3 = 0.0; L4 = 0.0; L5 = L1;
+                } else if (s->cfg.inflow_type == 2) {
+                    if (u > 0.0) {
+                        L2 = 0.0;
+                        L3 = ((v * nscbc) * c) / Lx;
+                        L4 = ((w * nscbc) * c) / Lx;
+                        L5 = ((((((u - uinf) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx;
+                    } else {
+                        L2 = 0.0;
+                        L5 = (((((p - pin) * nscbc) * c) * 1.0) / 2.0) / Lx;
+                    }
+                } else {
+                    L2 = 0.0;
+                    L3 = (((((v * nscbc) * c) / Lx) - v * G[VY][k]) - w * G[VZ][k]) - gpy / ro;
+                    L4 = ((w * nscbc) * c) / Lx + row;
+                    L5 = (((((((u - uinf) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx -
+                          0.5 * (((v * gpy) + (p * G[VY][k])) + (((ro * c) * v) * G[UY][k]))) -
+                         0.5 * (((w * gpz) + (p * G[WZ][k])) + (((ro * c) * w) * G[UZ][k]));
+                }
+            } else {
+                if (u < c) L1 = (((((p - pin) * nscbc) * c) * 1.0) / 2.0) / Lx;
+                L2 = 0.0;
+                if (u <= 0.0) { L2 = 0.0; L3 = 0.0; L4 = 0.0; }
+            }
+            const double ts = ((((c * c) * L2 + L5) + L1) / c) / c;
+            r[0][k] = rro - ts;
+            r[1][k] = (rou - u * ts) - (L5 - L1) / c;
+            r[2][k] = (rov - v * ts) - ro * L3;
+            r[3][k] = (row - w * ts) - ro * L4;
         }
         if (chl) { /* calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D), walls :553-717 */
             const double ux = Gux, uy = Guy, uz = G[UZ][k], vx = Gvx, vy = Gvy, vz = G[VZ][k];
             const double wx = Gwx, wy = Gwy, wz = G[WZ][k];
             double ad[6];
-            for (int q = 0; q < 6; q++) ad[q] = (u * gc[q][0][k] + v * gc[q][1][k]) + w * gc[q][2][k];
+            const double ua = ty == 1 ? 0.0 : u; /* inflow: no streamwise advection (rhs.F90:562-564) */
+            for (int q = 0; q < 6; q++) ad[q] = (ua * gc[q][0][k] + v * gc[q][1][k]) + w * gc[q][2][k];
             const double lxx = exp(o->psi[0][k]), lxy = o->psi[1][k], lyy = exp(o->psi[2][k]), lzz = exp(o->psi[5][k]);
             const double lxz = o->psi[3][k], lyz = o->psi[4][k];
             double ucxx = (ux + (uy * lxy) / lxx);
@@ -3539,6 +3606,7 @@ static void rhs3(Or3 *o, double *const *r) {
             sxx = fr * (cxx - 1.0); sxy = fr * cxy; syy = fr * (cyy - 1.0);
             sxz = fr * cxz; syz = fr * cyz; szz = fr * (czz - 1.0);
         }
+        if (inout) continue; /* :582-590: zero on inflow and outflow nodes (to be completed there) */
         if (wall) { /* :571-580: without the advection */
             r[4][k] = (ucxx + sxx) + Md * lc[0][k];
             r[5][k] = (ucxy + sxy) + Md * lc[1][k];
@@ -3576,7 +3644,7 @@ int or3_set_tstep(Or3 *o, double *dt_cfl, double *dt_par) {
         const int i = (int)(k % o->nl);
         const double c = sqrt(s->csq);
         const double um = sqrt((o->u[k] * o->u[k] + o->v[k] * o->v[k]) + o->w[k] * o->w[k]);
-        const double t = s->sp[i] / (um + c);
+        const double t = (o->bidx[i] >= 0 && s->type[i] == 2) ? (0.8 * s->sp[i]) / (um + c) : s->sp[i] / (um + c);
         dcfl = (t < dcfl) ? t : dcfl;
         const double tv = ((s->sp[i] * s->sp[i]) * o->ro[k]) / s->visc_total;
         dvisc = (tv < dvisc) ? tv : dvisc;
@@ -3694,6 +3762,30 @@ static void step3(Or3 *o) {
     for (int f = 0; f < 10; f++) { free(reg[f]); free(eacc[f]); free(r[f]); }
 }
 
+/* velocity_control with -Dvpid in 3-D (statistics.F90:214-303): dV = vol dz, summed over the
+   node-layers in order (the reference's OpenMP reduction has no fixed order) */
+static void velocity_control3(Or3 *o) {
+    OrSim *s = o->s;
+    double tot_vol = 0.0, tot_u = 0.0;
+    for (size_t k = 0; k < o->n3; k++) {
+        const double dvi = s->vol[k % o->nl] * o->dz;
+        tot_vol = tot_vol + dvi;
+        tot_u = tot_u + o->u[k] * dvi;
+    }
+    tot_u = tot_u / tot_vol;
+    const double Lx = (s->xmax - s->xmin) * s->cfg.L_char, Ly = (s->ymax - s->ymin) * s->cfg.L_char;
+    const double eflow_n = 1.0 - (tot_u * tot_vol) / (Ly * Lx);
+    s->sum_eflow = s->sum_eflow + eflow_n * o->dt;
+    const double deflowdt = (eflow_n - s->eflow_nm1) / o->dt;
+    const double facA = ((((0.5 * 0.5) * 0.5) * 1.0) * 2.0) * 2.0;
+    const double facB = facA / 0.4, facC = facA * 0.02;
+    double df = ((facA * eflow_n) + facB * s->sum_eflow) + facC * deflowdt;
+    df = (500.0 < df) ? 500.0 : df;
+    df = (-500.0 > df) ? -500.0 : df;
+    s->driving_force[0] = df;
+    s->eflow_nm1 = eflow_n;
+}
+
 int or3_step(Or3 *o, double dt, int nsteps, int pid) {
     for (int q = 0; q < nsteps; q++) {
         if (pid) {
@@ -3712,6 +3804,10 @@ int or3_step(Or3 *o, double dt, int nsteps, int pid) {
         }
         step3(o);
         o->itime++;
+        /* statistics_control after the step: the controller with -Dvpid, else the driving force
+           zeroed (statistics.F90:80-90,288) */
+        if (o->s->cfg.vpid) velocity_control3(o);
+        else o->s->driving_force[0] = o->s->driving_force[1] = o->s->driving_force[2] = 0.0;
     }
     return 0;
 }

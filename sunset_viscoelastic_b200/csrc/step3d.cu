@@ -1,5 +1,5 @@
 // step3d.cu -- the 3-D (-Ddim3) time step of the direct, Cholesky, log-conformation (sPTT) and
-// Newtonian forms on node sets without boundary nodes or with walls (node_type 0) among them.
+// Newtonian forms on node sets with or without boundary nodes (walls, inflow, outflow).
 //
 // The 3-D node set is nz copies of the 2-D one in z (build_3rd_dimension,
 // setup_domain.F90:435-547), layer-major in the reference (node iz*nl + i at z = iz*dz).  On the
@@ -21,14 +21,16 @@
 // followed by the z filter of its result (derivatives.F90:387-405); the mass correction and
 // the derived fields; all FP64.
 //
-// Walls: build_3rd_dimension copies node_type and the normals to every layer
-// (setup_domain.F90:487-532).  A wall node's x-y operators are its boundary weights (d/dn and
-// d/dt), so the gather is unchanged, except that its Laplacian weights are the tangential
-// second-derivative ones (calc_laplacian_transverse_only_on_bound, derivatives.F90:306-358;
-// the velocity Laplacians, which would differ, are not read on walls).  The wall branches of the
-// right-hand sides run in point3_body<FORM, true>, and apply_time_dependent_bounds holds
-// rho u, rho v, rho w at zero there after each stage and after the filter.
+// Boundary nodes: build_3rd_dimension copies node_type and the normals to every layer
+// (setup_domain.F90:487-532).  A boundary node's x-y operators are its boundary weights (on
+// walls d/dn and d/dt; on inflow and outflow nodes d/dx and d/dy), so the gather is unchanged,
+// except that the conformation Laplacian there takes the tangential second-derivative weights
+// (calc_laplacian_transverse_only_on_bound, derivatives.F90:306-358).  The boundary branches of
+// the right-hand sides run in point3_body<FORM, true>, and apply_time_dependent_bounds after
+// each stage and after the filter holds rho u, rho v, rho w at zero on walls and prescribes a
+// hard inflow's momentum, with u_inflow_local on its ramp.
 #include "internal.cuh"
+#include "physics.cuh"
 
 namespace sunset {
 
@@ -43,6 +45,7 @@ struct Layer3 {
     const long long *slice_ptr;
     const int *cnt, *cnt_small, *lidx;
     const double *wx, *wy, *wl, *wh, *gsx, *gsy, *lsum, *hsum;
+    const double *wlc, *lsumc;  // with boundary nodes: the conformation Laplacian's weights and sums
     double fdg[kMaxFd], fdl[kMaxFd], fdh[kMaxFd];
 };
 
@@ -163,10 +166,13 @@ __host__ __device__ constexpr int derivs_min_blocks(int form) {
 //
 // ST(slot, value) receives each derivative: a global array of the standalone gather, or the
 // fused stage kernel's shared memory.
-template <int FORM, bool MD, bool FULL, bool FEN, class ST>
+// BND: the node set has boundary nodes, whose conformation Laplacians (fields 7-12) take the
+// weights wlc and sums lsumc.
+template <int FORM, bool MD, bool FULL, bool FEN, bool BND, class ST>
 __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, const ZThread &z, ST store) {
     constexpr int N = ndesc3<FORM, MD, FEN>();
     constexpr int LB = 2;
+    constexpr bool kCL = BND && MD;
     const int k = z.k, i = z.i, iz = z.iz, row = i * L.nz, h = L.ncfd / 2;
     double sx[N], sy[N], sl[N];
 #pragma unroll
@@ -176,7 +182,7 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
     int q = 0;
     for (; q + LB <= cs; q += LB) {
         int pj[LB], code[LB];
-        double wx[LB], wy[LB], wl[LB], v[LB][N];
+        double wx[LB], wy[LB], wl[LB], wc[LB], v[LB][N];
 #pragma unroll
         for (int b = 0; b < LB; b++) {
             const long long o = sell_at(base, q + b, i & 31);
@@ -186,6 +192,7 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
             wx[b] = __ldg(L.wx + o);
             wy[b] = __ldg(L.wy + o);
             wl[b] = __ldg(L.wl + o);
+            wc[b] = kCL ? __ldg(L.wlc + o) : 0.0;
         }
 #pragma unroll
         for (int b = 0; b < LB; b++)
@@ -199,7 +206,7 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
                 const double x = mirror_value(v[b][d], D.cls, code[b]);
                 if (D.gx >= 0) sx[d] = sx[d] + x * wx[b];
                 if (D.gy >= 0) sy[d] = sy[d] + x * wy[b];
-                if (D.gl >= 0) sl[d] = sl[d] + x * wl[b];
+                if (D.gl >= 0) sl[d] = sl[d] + x * ((kCL && D.f >= 7) ? wc[b] : wl[b]);
             }
     }
     for (; q < cs; q++) {
@@ -208,13 +215,14 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
         const int pj = (l & kLinkMask) * L.nz + iz;
         const int code = (int)((unsigned)l >> 30);
         const double wx = __ldg(L.wx + o), wy = __ldg(L.wy + o), wl = __ldg(L.wl + o);
+        const double wc = kCL ? __ldg(L.wlc + o) : 0.0;
 #pragma unroll
         for (int d = 0; d < N; d++) {
             const FDesc D = desc3f<FORM, MD, FULL, FEN>(d);
             const double x = mirror_value(F.p[D.f][pj], D.cls, code);
             if (D.gx >= 0) sx[d] = sx[d] + x * wx;
             if (D.gy >= 0) sy[d] = sy[d] + x * wy;
-            if (D.gl >= 0) sl[d] = sl[d] + x * wl;
+            if (D.gl >= 0) sl[d] = sl[d] + x * ((kCL && D.f >= 7) ? wc : wl);
         }
     }
     // the x-y sums in sum form; the Laplacians keep theirs for the z part
@@ -224,7 +232,7 @@ __device__ __forceinline__ void derivs3_body(const Layer3 &L, const Fields3 &F, 
         const double p = F.p[D.f][k];
         if (D.gx >= 0) store(D.gx, sx[d] - p * L.gsx[i]);
         if (D.gy >= 0) store(D.gy, sy[d] - p * L.gsy[i]);
-        if (D.gl >= 0) sl[d] = sl[d] - p * L.lsum[i];
+        if (D.gl >= 0) sl[d] = sl[d] - p * ((kCL && D.f >= 7) ? L.lsumc[i] : L.lsum[i]);
     }
     // the z stencils, point by point over all fields (each field's sums still run in point
     // order); a fixed trip count with the points past ncfd cut off, so that the loads of several
@@ -354,9 +362,11 @@ struct Point3 {
     StepConsts K;
     int nl, nz, di, full, md;
     const double *py;                     // node ordinate (Kolmogorov forcing)
-    // walls: node types, normals into the fluid, boundary index and FD rows, spacing
+    // boundary nodes: node types, normals into the fluid, boundary index and FD rows, spacing;
+    // u_inflow_local of every node-layer
     const int *ntype, *bidx, *brow;
     const double *rnx, *rny, *sp;
+    double *uin;
     const double *fen;                    // FENE-P function of the direct form, or null
     int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
@@ -560,19 +570,21 @@ __device__ __forceinline__ void chl3_fenep_factor(double L2, double *p, bool to_
 }
 
 // calc_rhs_ro, calc_rhs_rovel and calc_rhs_c with the dim3 terms (rhs_di.F90:119-139,
-// 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).  WALL: the node
-// set has walls, whose node-layers take the wall branches.
+// 215-275, 415-476), then the stage's RK update (step.F90:285-343, 366-483).  BND: the node
+// set has boundary nodes, whose node-layers take the wall or inflow/outflow branches.
 //
 // GET(slot) returns derivative `slot` of node-layer k (global arrays, or the fused kernel's
 // shared memory); the bits of the node-layer's step error norm are returned (stage 3).
-template <int FORM, bool WALL, class GET>
+template <int FORM, bool BND, class GET>
 __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_t k, GET g) {
     constexpr bool kDi = FORM == SUNSET_FORM_DI, kChl = FORM == SUNSET_FORM_CHL, kLc = FORM == SUNSET_FORM_LC;
     unsigned long long eb = 0;
     {
         const StepConsts &K = P.K;
         const int i = (int)((unsigned)k / (unsigned)P.nz);
-        const bool wall = WALL && P.ntype[i] == 0;
+        const int ty = BND ? P.ntype[i] : 999;
+        const bool wall = ty == 0, inout = ty == 1 || ty == 2;
+        double uin = inout ? P.uin[k] : 0.0;
         const double ro = P.in[0][k], u = P.in[4][k], v = P.in[5][k], w = P.in[6][k];
         const double gpx = K.csq * g(ROX), gpy = K.csq * g(ROY), gpz = K.csq * g(ROZ);
         const double tmp = ((u * g(ROX) + v * g(ROY)) + w * g(ROZ));
@@ -627,9 +639,9 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
         // x-y for the conformation equations (rhs_di.F90:497-517, rhs.F90:586-611,
         // rhs_lc.F90:602-627; d/dz is d/dz everywhere)
         double gux = g(UX), guy = g(UY), gvx = g(VX), gvy = g(VY), gwx = g(WX), gwy = g(WY);
-        // the conformation Laplacian on a wall adds the one-sided normal second derivative
-        // over the node's four FD rows, the next nodes of its layer (rhs_di.F90:553-568,
-        // rhs.F90:631-643)
+        // the conformation Laplacian on a wall (and in the Cholesky form on every boundary
+        // node) adds the one-sided normal second derivative over the node's four FD rows, the
+        // next nodes of its layer (rhs_di.F90:553-568, rhs.F90:631-643)
         auto fdrows = [&](int q) {
             const int *rw = P.brow + 4 * P.bidx[i];
             const int iz = (int)k - i * P.nz;
@@ -664,13 +676,62 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             r[1] = (0.0 - u * ts) - (L5 - L1) / c;
             r[2] = (0.0 - v * ts) - ro * L3;
             r[3] = (0.0 - w * ts) - ro * L4;
+        } else if (inout) {
+            // inflow (node_type 1) and outflow (2) in the x-y frame: calc_rhs_ro's in/out branch
+            // (rhs_di.F90:155-157), the amplitudes and the transverse, viscous and body-force
+            // terms of calc_rhs_rovel (:311-359; no Kolmogorov forcing), the closure of
+            // characteristic_boundaries.F90 for the node's type (soft :54-80, hard :82-110,
+            // inflow-outflow :112-150, outflow :152-189) and calc_rhs_nscbc (:601-665)
+            const double c = sqrt(K.csq), p = K.csq * ro, nscbc = K.nscbc, Lx = K.Lx;
+            const double rro = ((-v * g(ROY) - ro * g(VY)) - w * g(ROZ)) - ro * g(WZ);
+            double L1 = (0.5 * (u - c)) * (gpx - (ro * c) * g(UX));
+            double L2 = u * (g(ROX) - (gpx / c) / c);
+            double L3 = u * g(VX);
+            double L4 = u * g(WX);
+            double L5 = (0.5 * (u + c)) * (gpx + (ro * c) * g(UX));
+            const double bu = ro * (K.grav0 + P.sc->df), bv = ro * (K.grav1 + 0.0), bw = ro * (0.0 + 0.0);
+            const double rou = ((-(v * g(UY)) - w * g(UZ)) + fvu) + bu;
+            const double rov = (((-(v * g(VY)) - w * g(VZ)) - gpy) + fvv) + bv;
+            const double row = (((-(v * g(WY)) - w * g(WZ)) - gpz) + fvw) + bw;
+            if (ty == 1) {
+                if (K.inflow_type == 1) {
+                    L2 = 0.0; L3 = 0.0; L4 = 0.0; L5 = L1;
+                } else if (K.inflow_type == 2) {
+                    if (u > 0.0) {
+                        L2 = 0.0;
+                        L3 = ((v * nscbc) * c) / Lx;
+                        L4 = ((w * nscbc) * c) / Lx;
+                        L5 = ((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx;
+                    } else {
+                        L2 = 0.0;
+                        L5 = (((((p - K.p_in) * nscbc) * c) * 1.0) / 2.0) / Lx;
+                    }
+                } else {
+                    L2 = 0.0;
+                    L3 = (((((v * nscbc) * c) / Lx) - v * g(VY)) - w * g(VZ)) - gpy / ro;
+                    L4 = ((w * nscbc) * c) / Lx + row;
+                    L5 = (((((((u - uin) * nscbc) * (1.0 - u / c)) * c) * c) * 1.0) / Lx -
+                          0.5 * (((v * gpy) + (p * g(VY))) + (((ro * c) * v) * g(UY)))) -
+                         0.5 * (((w * gpz) + (p * g(WZ))) + (((ro * c) * w) * g(UZ)));
+                }
+            } else {
+                if (u < c) L1 = (((((p - K.p_out) * nscbc) * c) * 1.0) / 2.0) / Lx;
+                L2 = 0.0;
+                if (u <= 0.0) { L2 = 0.0; L3 = 0.0; L4 = 0.0; }
+            }
+            const double ts = ((((c * c) * L2 + L5) + L1) / c) / c;
+            r[0] = rro - ts;
+            r[1] = (rou - u * ts) - (L5 - L1) / c;
+            r[2] = (rov - v * ts) - ro * L3;
+            r[3] = (row - w * ts) - ro * L4;
         }
         if (kChl) {  // calc_rhs_cholesky, rhs.F90:421-556 (sPTT, 3-D), walls :553-717
             const double ux = gux, uy = guy, uz = g(UZ), vx = gvx, vy = gvy, vz = g(VZ);
             const double wx = gwx, wy = gwy, wz = g(WZ);
             double ad[6];
+            const double ua = ty == 1 ? 0.0 : u;  // inflow: no streamwise advection (rhs.F90:562-564)
 #pragma unroll
-            for (int q = 0; q < 6; q++) ad[q] = (u * gp(q, 0) + v * gp(q, 1)) + w * gp(q, 2);
+            for (int q = 0; q < 6; q++) ad[q] = (ua * gp(q, 0) + v * gp(q, 1)) + w * gp(q, 2);
             const double lxx = exp(P.in[13][k]), lxy = P.in[14][k], lyy = exp(P.in[15][k]), lzz = exp(P.in[18][k]);
             const double lxz = P.in[16][k], lyz = P.in[17][k];
             double ucxx = (ux + (uy * lxy) / lxx);
@@ -689,7 +750,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             auto lc = [&](int q) {
                 if (!P.md) return 0.0;
                 const double x = g(LC0 + q);
-                return wall ? x + fdrows(q) : x;
+                return (wall || inout) ? x + fdrows(q) : x;
             };
             double sxx, sxy, syy, sxz, syz, szz;
             if (K.fenep) {  // rhs.F90:204-209, 479-500: the factors of J = f c
@@ -814,7 +875,9 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                 const double x = g(LC0 + q);
                 return wall ? x + fdrows(q) : x;
             };
-            if (wall) {  // rhs_di.F90:571-580: without the advection
+            if (inout) {  // :582-590: zero on inflow and outflow nodes (to be completed there)
+                for (int q = 4; q < 10; q++) r[q] = 0.0;
+            } else if (wall) {  // rhs_di.F90:571-580: without the advection
                 r[4] = (ucxx + sxx) + Md * lc(0);
                 r[5] = (ucxy + sxy) + Md * lc(1);
                 r[6] = (ucyy + syy) + Md * lc(2);
@@ -876,7 +939,16 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                 }
             }
             if (stage == 3) eb = dbits(en);
-            if (wall) { Un[1] = 0.0; Un[2] = 0.0; Un[3] = 0.0; }  // apply_time_dependent_bounds
+            // apply_time_dependent_bounds (characteristic_boundaries.F90:191-257) at the stage's
+            // time time0 + c_s dt: walls at rest; on inflow node-layers u_inflow_local follows
+            // its ramp, and a hard inflow prescribes the momentum
+            if (wall) { Un[1] = 0.0; Un[2] = 0.0; Un[3] = 0.0; }
+            if (ty == 1) {
+                const double cs = stage == 0 ? 0.0 : stage == 1 ? SUNSET_RK_A21 : stage == 2 ? (SUNSET_RK_A32 + SUNSET_RK_B1) : 1.0;
+                uin = inflow_velocity(K, P.sc->time + dt * cs, uin);
+                P.uin[k] = uin;
+                if (K.inflow_type == 1) { Un[1] = uin * Un[0]; Un[2] = 0.0; Un[3] = 0.0; }
+            }
             for (int q = 0; q < 10; q++) P.out[src[q]][k] = Un[q];
             const double oo = 1.0 / Un[0];  // get_velocity_from_momentum
             P.out[4][k] = Un[1] * oo;
@@ -912,7 +984,7 @@ __device__ __forceinline__ void block_emax3(unsigned long long eb, DevScalars *s
 // One stage fused: the derivatives of node-layer k (derivs3_body) go to this block's shared
 // memory, compact slots of 128 doubles (one per thread), and the pointwise right-hand side
 // and RK update (point3_body) read them there, so no derivative array crosses HBM.
-template <int FORM, bool MD, bool FULL, bool FEN, bool WALL>
+template <int FORM, bool MD, bool FULL, bool FEN, bool BND>
 __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_stage(Layer3 L, Fields3 F, Point3 P) {
     constexpr int NS = ngslots<FORM, MD, FULL, FEN>();
     __shared__ double sg[NS * 128];
@@ -920,11 +992,11 @@ __global__ void __launch_bounds__(128, derivs_min_blocks(FORM)) k3_stage(Layer3 
     const bool live = zthread(L, z);
     unsigned long long eb = 0;
     if (live) {
-        derivs3_body<FORM, MD, FULL, FEN>(L, F, z, [&](int slot, double v) {
+        derivs3_body<FORM, MD, FULL, FEN, BND>(L, F, z, [&](int slot, double v) {
             const int c = kGTable<FORM, MD, FULL, FEN>.idx[slot];
             if (c >= 0) sg[c * 128 + threadIdx.x] = v;
         });
-        eb = point3_body<FORM, WALL>(P, (size_t)z.k, [&](int a) {
+        eb = point3_body<FORM, BND>(P, (size_t)z.k, [&](int a) {
             const int c = kGTable<FORM, MD, FULL, FEN>.idx[a];
             return c >= 0 ? sg[c * 128 + threadIdx.x] : 0.0;
         });
@@ -965,10 +1037,72 @@ __global__ void __launch_bounds__(kFoldThreads) k3_fold(const double *partials, 
     if (threadIdx.x == 0) *out = divisor ? (enabled ? red[0] / *divisor : 0.0) : red[0];
 }
 
-// End of step: mass correction, apply_time_dependent_bounds on walls (ntype: node types, or
-// null without walls), u, v, w from the momentum, the error-norm history and time.
-__global__ void k3_finalize(size_t n, int nz, const int *ntype, Fields3 F, int chl, int lc, double L2, DevScalars *sc,
-                            int vpid) {
+// velocity_control with -Dvpid in 3-D (statistics.F90:214-303, dV = vol dz): block sums of
+// u dV and of dV (a fixed tree), then the fold and the PID update of driving_force(1)
+__global__ void k3_flow_partials(int nz, size_t n, const double *u, const double *vol, double dz, double *pu,
+                                 double *pv) {
+    __shared__ double ru[128], rv[128];
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double a = 0.0, b = 0.0;
+    if (k < n) {
+        b = vol[k / nz] * dz;
+        a = u[k] * b;
+    }
+    ru[threadIdx.x] = a;
+    rv[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            ru[threadIdx.x] = ru[threadIdx.x] + ru[threadIdx.x + s];
+            rv[threadIdx.x] = rv[threadIdx.x] + rv[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        pu[blockIdx.x] = ru[0];
+        pv[blockIdx.x] = rv[0];
+    }
+}
+constexpr int kFlowThreads = 1024;
+__global__ void __launch_bounds__(kFlowThreads) k3_velocity_control(const double *pu, const double *pv, int nblk, double Lx,
+                                                                     double Ly, DevScalars *sc) {
+    __shared__ double ru[kFlowThreads], rv[kFlowThreads];
+    double a = 0.0, b = 0.0;
+    for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
+        a = a + pu[q];
+        b = b + pv[q];
+    }
+    ru[threadIdx.x] = a;
+    rv[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            ru[threadIdx.x] = ru[threadIdx.x] + ru[threadIdx.x + s];
+            rv[threadIdx.x] = rv[threadIdx.x] + rv[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double tot_vol = rv[0], dt = sc->dt;
+        const double tot_u = ru[0] / tot_vol;
+        const double eflow_n = 1.0 - (tot_u * tot_vol) / (Ly * Lx);
+        sc->sum_eflow = sc->sum_eflow + eflow_n * dt;
+        const double deflowdt = (eflow_n - sc->eflow_nm1) / dt;
+        const double facA = ((((0.5 * 0.5) * 0.5) * 1.0) * 2.0) * 2.0;
+        const double facB = facA / 0.4, facC = facA * 0.02;
+        double df = ((facA * eflow_n) + facB * sc->sum_eflow) + facC * deflowdt;
+        df = (500.0 < df) ? 500.0 : df;
+        df = (-500.0 > df) ? -500.0 : df;
+        sc->df = df;
+        sc->eflow_nm1 = eflow_n;
+    }
+}
+
+// End of step: mass correction, apply_time_dependent_bounds (ntype: node types, or null without
+// boundary nodes: walls at rest, a hard inflow's momentum from u_inflow_local), u, v, w from the
+// momentum, the error-norm history and time.
+__global__ void k3_finalize(size_t n, int nz, const int *ntype, const double *uin, int hard_in, Fields3 F, int chl, int lc,
+                            double L2, DevScalars *sc, int vpid) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
         // every load before the first store (the arrays are not known to be distinct)
@@ -977,9 +1111,14 @@ __global__ void k3_finalize(size_t n, int nz, const int *ntype, Fields3 F, int c
         double p[6], c[6];
         if (chl || lc)
             for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
-        if (ntype && ntype[(unsigned)k / (unsigned)nz] == 0) {
+        const int ty = ntype ? ntype[(unsigned)k / (unsigned)nz] : 999;
+        if (ty == 0) {
             m1 = 0.0; m2 = 0.0; m3 = 0.0;
-            F.p[1][k] = 0.0; F.p[2][k] = 0.0; F.p[3][k] = 0.0;
+        } else if (ty == 1 && hard_in) {  // the hard inflow's momentum from the corrected density
+            m1 = uin[k] * r; m2 = 0.0; m3 = 0.0;
+        }
+        if (ty == 0 || (ty == 1 && hard_in)) {
+            F.p[1][k] = m1; F.p[2][k] = m2; F.p[3][k] = m3;
         }
         F.p[0][k] = r;
         const double oo = 1.0 / r;
@@ -1007,15 +1146,15 @@ __global__ void k3_finalize(size_t n, int nz, const int *ntype, Fields3 F, int c
 }
 
 // set_tstep (step.F90:569-622) over the 3-D nodes: block minima as bit patterns
-__global__ void k3_tstep(int nz, size_t n, const double *u, const double *v, const double *w, const double *ro,
-                         const double *sp, double csq, double visc_total, DevScalars *sc) {
+__global__ void k3_tstep(int nz, size_t n, const int *ntype, const double *u, const double *v, const double *w,
+                         const double *ro, const double *sp, double csq, double visc_total, DevScalars *sc) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     double tc = 1.0e10, tp = 1.0e10;
     if (k < n) {
         const int i = (int)((unsigned)k / (unsigned)nz);
         const double c = sqrt(csq);
         const double um = sqrt((u[k] * u[k] + v[k] * v[k]) + w[k] * w[k]);
-        tc = sp[i] / (um + c);
+        tc = (ntype && ntype[i] == 2) ? (0.8 * sp[i]) / (um + c) : sp[i] / (um + c);  // outflow: 0.8
         tp = ((sp[i] * sp[i]) * ro[k]) / visc_total;
     }
     unsigned long long bc = dbits(tc), bp = dbits(tp);
@@ -1110,14 +1249,23 @@ __global__ void k3_momentum(size_t n, int nz, const int *ntype, const double *ro
     rov[k] = ro[k] * v[k];
     row[k] = ro[k] * w[k];
 }
-// walls: the layer's Laplacian weights and sums, each wall node's replaced by its tangential
-// second-derivative weights (reference link order, as the layer's lists) and their sum
-__global__ void k3_wall_lap_weights(int nl, const int *ntype, const int *bidx, const long long *slice_ptr,
-                                    const int *cnt_small, int nplink, const double *wbt, const double *wbt_sum,
-                                    double *wl3, double *lsum3) {
+// u_inflow_local of the initial state (setup_flow.F90:48-50,128-138): u on inflow node-layers,
+// u_char elsewhere
+__global__ void k3_init_uin(size_t n, int nz, const int *ntype, const double *u, double uchar, double *uin) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uin[k] = ntype[(unsigned)k / (unsigned)nz] == 1 ? u[k] : uchar;
+}
+// boundary nodes: the layer's Laplacian weights and sums, each boundary node's replaced by its
+// tangential second-derivative weights (reference link order, as the layer's lists) and their
+// sum: the conformation Laplacian's
+__global__ void k3_boundary_lap_weights(int nl, const int *bidx, const long long *slice_ptr,
+                                        const int *cnt_small, int nplink, const double *wbt, const double *wbt_sum,
+                                        double *wl3, double *lsum3) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nl || ntype[i] != 0) return;
-    const int jj = bidx[i];
+    if (i >= nl) return;
+    const int jj = bidx[i];  // -1 off the boundary (FD rows carry negative node types)
+    if (jj < 0) return;
     const long long base = slice_ptr[i >> 5];
     for (int q = 0; q < cnt_small[i]; q++) wl3[sell_at(base, q, i & 31)] = wbt[(size_t)jj * nplink + q];
     lsum3[i] = wbt_sum[jj];
@@ -1181,8 +1329,10 @@ Layer3 layer3(const Handle *H) {
     L.cnt = H->cnt;
     L.cnt_small = H->cnt_small;
     L.lidx = H->lidx;
-    L.wx = H->wx; L.wy = H->wy; L.wl = H->nb > 0 ? H->wl3 : H->wl; L.wh = H->wh;
-    L.gsx = H->gsx; L.gsy = H->gsy; L.lsum = H->nb > 0 ? H->lsum3 : H->lsum; L.hsum = H->hsum;
+    L.wx = H->wx; L.wy = H->wy; L.wl = H->wl; L.wh = H->wh;
+    L.gsx = H->gsx; L.gsy = H->gsy; L.lsum = H->lsum; L.hsum = H->hsum;
+    L.wlc = H->wl3;
+    L.lsumc = H->lsum3;
     for (int m = 0; m < kMaxFd; m++) { L.fdg[m] = H->fdg[m]; L.fdl[m] = H->fdl[m]; L.fdh[m] = H->fdh[m]; }
     return L;
 }
@@ -1218,6 +1368,7 @@ Point3 point3(Handle *H, int b, int stage) {
     P.rnx = H->rnx;
     P.rny = H->rny;
     P.sp = H->sp;
+    P.uin = H->uin3;
     P.fen = (H->cfg.form == SUNSET_FORM_DI && H->cfg.fenep) ? H->tmp3 : nullptr;
     for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
@@ -1269,7 +1420,7 @@ int stage3(Handle *H, int b, int stage) {
 int tstep3_launch(Handle *H, int b, int pid) {
     const size_t n = n3(H);
     const double *const *f = H->f3[b];
-    k3_tstep<<<nblk(n), 128, 0, H->stream>>>(H->nz, n, f[4], f[5], f[6], f[0], H->sp, step_consts(H->cfg, 1, 1, false, false).csq,
+    k3_tstep<<<nblk(n), 128, 0, H->stream>>>(H->nz, n, H->nb > 0 ? H->ntype : nullptr, f[4], f[5], f[6], f[0], H->sp, step_consts(H->cfg, 1, 1, false, false).csq,
                                              step_consts(H->cfg, 1, 1, false, false).visc_total, H->dsc);
     k3_tstep_fold<<<1, 1, 0, H->stream>>>(H->dsc, H->cfg.L_char, pid);
     SUNSET_CUDA(H, cudaGetLastError());
@@ -1281,8 +1432,6 @@ int tstep3_launch(Handle *H, int b, int pid) {
 // ---------------------------------------------------------------------------------------
 int layers_set(Handle *H, double Lz) {
     if (!(Lz > 0.0)) return set_err(H, SUNSET_ERR_ARG, "L_domain_z must be positive");
-    for (int t : H->h_btype)
-        if (t != 0) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers walls among the boundary nodes, not inflow or outflow");
     if (H->cfg.fenep && H->cfg.form != SUNSET_FORM_DI && H->cfg.form != SUNSET_FORM_CHL)
         return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path covers FENE-P with the direct and Cholesky forms");
     if (H->cfg.precision != SUNSET_FP64) return set_err(H, SUNSET_ERR_SCOPE, "the 3-D path runs in FP64");
@@ -1328,17 +1477,19 @@ static int state3_alloc(Handle *H) {
     if (dalloc(H, &H->g3, (size_t)10 * n) || dalloc(H, &H->tmp3, n)) return SUNSET_ERR_NOMEM;
     for (int b = 0; b < 2; b++)
         for (int f = 7; f < 19; f++) SUNSET_CUDA(H, cudaMemsetAsync(H->f3[b][f], 0, n * sizeof(double), H->stream));
-    if (H->nb > 0) {  // the wall nodes' Laplacian weights of the layer (after the set-up's weights)
+    if (H->nb > 0) {  // the boundary nodes' Laplacian weights of the layer (after the set-up's weights)
         if (!H->wbt) return set_err(H, SUNSET_ERR_ARG, "call order: the set-up's weights first");
-        if (dalloc(H, &H->wl3, (size_t)H->nlinks_sell) || dalloc(H, &H->lsum3, (size_t)H->npfb)) return SUNSET_ERR_NOMEM;
+        if (dalloc(H, &H->wl3, (size_t)H->nlinks_sell) || dalloc(H, &H->lsum3, (size_t)H->npfb) || dalloc(H, &H->uin3, n))
+            return SUNSET_ERR_NOMEM;
         SUNSET_CUDA(H, cudaMemcpyAsync(H->wl3, H->wl, (size_t)H->nlinks_sell * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
         SUNSET_CUDA(H, cudaMemcpyAsync(H->lsum3, H->lsum, (size_t)H->npfb * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
-        k3_wall_lap_weights<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->ntype, H->bidx, H->slice_ptr, H->cnt_small,
+        k3_boundary_lap_weights<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->bidx, H->slice_ptr, H->cnt_small,
                                                                         H->nplink, H->wbt, H->wbt_sum, H->wl3, H->lsum3);
         SUNSET_CUDA(H, cudaGetLastError());
     }
     const unsigned nb = nblk(n);
-    if (!H->partials3 && dalloc(H, &H->partials3, (size_t)nb + 16)) return SUNSET_ERR_NOMEM;
+    // block partials: the mass sums, and the controller's two sums (from nb + 16 on)
+    if (!H->partials3 && dalloc(H, &H->partials3, 3 * ((size_t)nb + 16))) return SUNSET_ERR_NOMEM;
     if (!H->dsc) {
         if (dalloc(H, &H->dsc, 1)) return SUNSET_ERR_NOMEM;
     }
@@ -1363,6 +1514,7 @@ int state3_set(Handle *H, const double *const *fields10) {
         k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, H->nz, n, d);
     }
     k3_momentum<<<nblk(n), 128, 0, st>>>(n, H->nz, H->nb > 0 ? H->ntype : nullptr, f[0], f[4], f[5], f[6], f[1], f[2], f[3]);
+    if (H->nb > 0) k3_init_uin<<<nblk(n), 128, 0, st>>>(n, H->nz, H->ntype, f[4], H->cfg.U_char, H->uin3);
     if (H->cfg.form == SUNSET_FORM_CHL || H->cfg.form == SUNSET_FORM_LC) {
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = f[q];
@@ -1453,8 +1605,16 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
         k3_fold<<<1, kFoldThreads, 0, st>>>(H->partials3, (int)nblk(n), &H->dsc->dro, &H->dsc->tv, H->cfg.mcorr);
         Fields3 F19;
         for (int q = 0; q < 19; q++) F19.p[q] = H->f3[b][q];
-        k3_finalize<<<nblk(n), 128, 0, st>>>(n, H->nz, H->nb > 0 ? H->ntype : nullptr, F19, chl, lc,
+        k3_finalize<<<nblk(n), 128, 0, st>>>(n, H->nz, H->nb > 0 ? H->ntype : nullptr, H->uin3, H->cfg.inflow_type == 1, F19, chl, lc,
                                              H->cfg.fenep ? H->cfg.fenep_l2 : 0.0, H->dsc, H->cfg.vpid);
+        if (H->cfg.vpid) {  // statistics_control after the step (sunset.F90:104)
+            const size_t off = nblk(n) + 16;
+            k3_flow_partials<<<nblk(n), 128, 0, st>>>(H->nz, n, H->f3[b][4], H->vol, H->dz, H->partials3 + off,
+                                                      H->partials3 + 2 * off);
+            const double L = H->cfg.L_char;
+            k3_velocity_control<<<1, kFlowThreads, 0, st>>>(H->partials3 + off, H->partials3 + 2 * off, (int)nblk(n),
+                                                          (H->xmax - H->xmin) * L, (H->ymax - H->ymin) * L, H->dsc);
+        }
         SUNSET_CUDA(H, cudaGetLastError());
         H->cur3 = b;
     }

@@ -154,6 +154,49 @@ def test_steps(pair):
     np.testing.assert_allclose(gpu.time()["dt"], ref.time()["dt"], rtol=1e-10)
 
 
+def test_velocity_control_3d():
+    """velocity_control with -Dvpid in 3-D (statistics.F90:214-303): after every step the volume
+    sums over the node-layers with dV = vol dz drive driving_force(1) by the PID law, and the
+    body force of the next step carries it.  Device against the restatement over 20 steps: the
+    controller's state (summed in a fixed tree on the device, in node order on the CPU) and the
+    fields."""
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=24)
+    ns = wl.nodes()
+    kw = dict(wl.params(), vpid=True, kolmogorov_forcing=0)
+    O.set_pow_mode(True)
+    try:
+        layer = O.Oracle(**kw)
+        layer.build_domain(ns)
+        layer.setup()
+    finally:
+        O.set_pow_mode(False)
+    ref = O.Oracle3(layer, 1.0)
+    gpu = labfm.Sunset(**kw)
+    gpu.build_domain(ns)
+    nz, dz = gpu.set_layers(1.0)
+    gpu.setup()
+    nd = layer.nodes()
+    nl = ref.nl
+    st = state3(np.tile(nd["x"][:nl], nz), np.tile(nd["y"][:nl], nz), np.repeat(np.arange(nz) * dz, nl))
+    c = {k: st[k] for k in ["cxx", "cxy", "cyy", "cxz", "cyz", "czz"]}
+    ref.set_state(st["ro"], st["u"], st["v"], st["w"], **c)
+    gpu.set_state_3d(st["ro"], st["u"], st["v"], st["w"], **c)
+    dcr, dpr = ref.set_tstep()
+    gpu.set_tstep()
+    for o in (ref, gpu):
+        o.step(0.3 * min(dcr, dpr), 20)
+    fr, fg = layer.flow_control(), gpu.flow_control()
+    print("3-D controller:", fr, fg)
+    assert abs(fr["driving_force"][0]) > 1e-3
+    np.testing.assert_allclose(fg["driving_force"][0], fr["driving_force"][0], rtol=1e-9)
+    np.testing.assert_allclose([fg["eflow_nm1"], fg["sum_eflow"]], [fr["eflow_nm1"], fr["sum_eflow"]], rtol=1e-9)
+    sr, sg = ref.state(), gpu.state_3d()
+    for k in ["ro", "rou", "rov", "row", "cxx", "czz"]:
+        e = float(np.abs(sg[k] - sr[k]).max() / max(np.abs(sr[k]).max(), 1e-300))
+        assert e <= F_TOL, (k, e)
+    gpu.close()
+
+
 def test_fenep_scope():
     """FENE-P in 3-D covers the direct and Cholesky forms; the log-conformation form is refused
     with a scope error."""

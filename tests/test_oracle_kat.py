@@ -17,8 +17,8 @@ from fractions import Fraction
 import numpy as np
 import pytest
 
-from sunset_viscoelastic_b200.nodesets import (NodeSet, WORKLOADS, channel, initial_state, jittered_lattice,
-                                               poiseuille_state)
+from sunset_viscoelastic_b200.nodesets import (NodeSet, WORKLOADS, channel, inflow_channel, inflow_state, initial_state,
+                                               jittered_lattice, poiseuille_state)
 import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -472,6 +472,48 @@ def test_3d_walls_reduce_to_2d(form, eps, mdiff, fenep):
     for k in ("rou", "rov", "row", "u", "v", "w"):
         assert np.all(s3[k].reshape(o3.nz, nl)[:, t == 0] == 0.0), k
     assert all(np.isfinite(a).all() for a in s3.values())
+
+
+@pytest.mark.parametrize("form, itype, extra", [("di", 0, {}), ("di", 1, {}), ("lc", 2, {}), ("chl", 0, {"Mdiff": 1e-3}),
+                                                ("chl", 1, {})])
+def test_3d_inout_reduces_to_2d(form, itype, extra):
+    """3-D restatement with inflow and outflow nodes, known answer: on the inflow channel a state
+    that does not vary in z, with w = 0, c_xz = c_yz = 0 and c_zz = 1, gives on every layer the
+    2-D right-hand sides, the inflow and outflow node-layers' included (rhs_di.F90:155-157,
+    311-359, characteristic_boundaries.F90:54-189 and calc_rhs_nscbc with their dim3 terms, which
+    vanish here; the Cholesky form's inflow advection and one-sided flux closure,
+    rhs.F90:558-643).  The log-conformation form takes eps = 0 (its 3-D trace includes c_zz)."""
+    ns = inflow_channel(24, ybc=1)
+    order = {"di": 4, "lc": 6, "chl": 8}[form]
+    kw = dict(Re=10.0, Wi=0.5, beta=0.59, Ma=0.1, kolmogorov_forcing=0, form=form, order=order, inflow_type=itype,
+              epsPTT=0.0, **extra)
+    o = O.Oracle(**kw).build_domain(ns).setup()
+    o3 = O.Oracle3(o, 0.4)
+    nl = o3.nl
+    nd = o.nodes()
+    t = nd["node_type"][:nl]
+    assert np.sum(t == 1) > 0 and np.sum(t == 2) > 0
+    st = inflow_state(type("R", (), {"x": nd["x"][:nl], "y": nd["y"][:nl]}))
+    o.set_state(**st)
+    r2 = o.rhs()
+    T = lambda a: np.tile(a, o3.nz)
+    zero = np.zeros(o3.n)
+    o3.set_state(T(st["ro"]), T(st["u"]), T(st["v"]), zero, T(st["cxx"]), T(st["cxy"]), T(st["cyy"]), zero, zero,
+                 np.ones(o3.n))
+    r3 = o3.rhs()
+    io = (t == 1) | (t == 2)
+    for k in ["ro", "rou", "rov"] + ([] if form == "di" else ["xx", "xy", "yy"]):
+        scale = max(np.abs(r2[k]).max(), 1.0)
+        d = np.abs(r3[k].reshape(o3.nz, nl) - r2[k][None, :])
+        assert d.max() / scale < 1e-9, (form, k, d.max() / scale)
+        assert d[:, io].max() / scale < 1e-11, (form, k, "inflow/outflow")
+    dc, dp = o3.set_tstep()
+    o3.step(0.3 * min(dc, dp), 3)
+    s3 = o3.state()
+    assert all(np.isfinite(a).all() for a in s3.values())
+    if itype == 1:  # hard inflow: v = w = 0 there
+        for k in ("rov", "row"):
+            assert np.all(s3[k].reshape(o3.nz, nl)[:, t == 1] == 0.0), k
 
 
 def central_first_derivative(m):
