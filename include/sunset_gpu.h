@@ -162,7 +162,8 @@ int sunset_step(SunsetHandle *h, double dt, int nsteps, int mode);
 /* time, dt, itime, emax(3) = {emax_nm1, emax_n, emax_np1} */
 int sunset_get_time(SunsetHandle *h, double *time, double *dt, int *itime, double *emax);
 int sunset_set_time(SunsetHandle *h, double time, double dt, int itime, const double *emax);
-/* sum 0.5 rho |u|^2 vol and sum rho vol over the interior nodes */
+/* sum 0.5 rho |u|^2 dV and sum rho dV over the interior nodes (mass_and_energy_check,
+   statistics.F90:305-330): dV = vol in 2-D, vol dz over the node-layers of a 3-D handle */
 int sunset_kinetic_energy(SunsetHandle *h, double *ke);
 int sunset_mass(SunsetHandle *h, double *mass);
 int sunset_synchronize(SunsetHandle *h);
@@ -209,19 +210,24 @@ int sunset_calc_all_rhs_3d(SunsetHandle *h, double *out);
    (rho - rho_char, u, v, vorticity, Q criterion, alpha_out = the node's error norm of the
    last step, cxx, cxy, cyy, czz; vorticity and Q rotated on walls as :229-241), and the
    header's 9 values (eflow_nm1, sum_eflow, driving_force(3) of the flow-rate controller,
-   emax_np1, emax_n, emax_nm1, dt). */
+   emax_np1, emax_n, emax_nm1, dt).  On a 3-D handle the -Dallout dump of :296-299, 13*npfb*nz
+   over every node-layer, layer-major: rho - rho_char, u, v, w, |vorticity| (3-D gradient;
+   on walls as :226-235), Q (never set by the reference in 3-D: 0), alpha_out, cxx, cxy, cyy,
+   cxz, cyz, czz. */
 int sunset_get_dump(SunsetHandle *h, double *columns, double *header);
 /* The same as files in the reference's layout: <directory>/fields_10000_<n_out>, with
    <directory>/nodes_10000 (output_nodes, output.F90:421-476: global index, x, y, s, h,
    h_small, node type) when n_out == 1, and a line "time 2 npfb n_out 1" appended to
-   <directory>/time.out.  Readable by the reference's restart loader and vtk_conv. */
+   <directory>/time.out.  Readable by the reference's restart loader and vtk_conv.  3-D: the
+   13-column rows of every node-layer, nodes with z and the layer offset of the global index
+   (setup_domain.F90:520-535), "time 3 npfb*nz n_out 1". */
 int sunset_write_dump(SunsetHandle *h, const char *directory, int n_out, double time);
 /* Restart (-Drestart): setup_domain.F90:206-242 loads h and h_small from the nodes file
    before the neighbour search (adapt_stencils is skipped); load_restart_file,
    setup_flow.F90:448-552, sets rho, u, v and c (psi formed from c) and the error-norm history
    and dt and the flow-rate controller's state from a fields dump (columns and header as
    sunset_get_dump returns them; driving_force(2:3) must be zero).  Time and step count
-   restart at 0, as there. */
+   restart at 0, as there.  On a 3-D handle from the 13 columns (:505-509: rho, u, v, w, c). */
 int sunset_set_lengths(SunsetHandle *h, const double *h_lengths, const double *h_small);
 int sunset_set_restart(SunsetHandle *h, const double *columns, const double *header);
 /* The flow-rate controller's state (common_vars.F90:82, statistics.F90:214-303): eflow_nm1,
@@ -231,7 +237,9 @@ int sunset_set_flow_control(SunsetHandle *h, const double *in);
 /* Binary checkpoint of the device state between steps (no counterpart in the reference):
    the fields, the step's scalars (time, dt, step count, error-norm history) and the per-node
    error, bit for bit, into a caller buffer of sunset_checkpoint_size bytes.  Loading it into
-   a handle built on the same node set and configuration resumes the run exactly. */
+   a handle built on the same node set and configuration resumes the run exactly.  A 3-D
+   handle's checkpoint holds the 19 fields of every node-layer, the node-layers' step error and
+   u_inflow_local, and loads only into a handle with the same layers. */
 int sunset_checkpoint_size(SunsetHandle *h, size_t *bytes);
 int sunset_save_checkpoint(SunsetHandle *h, void *buffer, size_t bytes);
 int sunset_load_checkpoint(SunsetHandle *h, const void *buffer, size_t bytes);

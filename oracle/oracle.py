@@ -100,6 +100,11 @@ def lib():
         L.or3_set_tstep.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.or3_step.argtypes = [P, C.c_double, C.c_int, C.c_int]
         L.or3_get_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), dp]
+        L.or3_kinetic_energy.restype = C.c_double
+        L.or3_kinetic_energy.argtypes = [P]
+        L.or3_mass.restype = C.c_double
+        L.or3_mass.argtypes = [P]
+        L.or3_get_dump.argtypes = [P, dp, dp]
         _lib = L
     return _lib
 
@@ -395,3 +400,17 @@ class Oracle3:
         em = np.zeros(3)
         self.L.or3_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it), em)
         return dict(time=t.value, dt=dt.value, itime=it.value, emax=em)
+
+    def kinetic_energy(self):
+        return float(self.L.or3_kinetic_energy(self.h))
+
+    def mass(self):
+        return float(self.L.or3_mass(self.h))
+
+    def dump(self):
+        """output_layer's 13 columns of every node-layer (layer-major) and the 9 header values."""
+        out, hd = np.zeros(13 * self.n), np.zeros(9)
+        self.L.or3_get_dump(self.h, out, hd)
+        keys = ["ro_minus_rho_char", "u", "v", "w", "vort", "qcrit", "alpha", "cxx", "cxy", "cyy", "cxz", "cyz", "czz"]
+        out = out.reshape(13, self.n)
+        return {k: out[i].copy() for i, k in enumerate(keys)}, hd

@@ -2811,6 +2811,7 @@ struct Or3 {
     double emax_nm1, emax_n, emax_np1;
     int *bidx;               /* nl: the layer node's index in boundary_list, or -1 */
     double *uin;             /* n3: u_inflow_local of each node-layer (inflow node-layers' in use) */
+    double *alpha;           /* n3: the last step's error of each node-layer (alpha_out) */
     char err[256];
 };
 
@@ -2890,6 +2891,7 @@ Or3 *or3_create(OrSim *s, double Lz) {
                     &o->psi[0], &o->psi[1], &o->psi[2], &o->psi[3], &o->psi[4], &o->psi[5]};
     for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) *a[k] = (double *)xcalloc(o->n3, sizeof(double));
     o->uin = (double *)xcalloc(o->n3, sizeof(double));
+    o->alpha = (double *)xcalloc(o->n3, sizeof(double));
     return o;
 }
 
@@ -2900,6 +2902,7 @@ void or3_destroy(Or3 *o) {
     for (size_t k = 0; k < sizeof(a) / sizeof(a[0]); k++) free(a[k]);
     free(o->bidx);
     free(o->uin);
+    free(o->alpha);
     free(o);
 }
 
@@ -3709,13 +3712,16 @@ static void step3(Or3 *o) {
                     const double L2 = s->cfg.fenep_l2;
                     sc = 1.0 / sqrt((L2 - 3.0) / (((L2 - o->c[0][k]) - o->c[2][k]) - o->c[5][k]));
                 }
+                double al = 0.0; /* alpha_out (step.F90:456-458): rho, rho u, rho v, xx, xy, yy */
                 for (int f = 0; f < nf; f++) {
                     Q[f][k] = reg[f][k] + RKb * r[f][k];
                     eacc[f][k] = eacc[f][k] + RKbmbh * r[f][k];
                     double t = fabs(eacc[f][k]) * norms[f];
+                    if (f != 3 && f < 7) al = (t > al) ? t : al;
                     if (f == 4 || f == 5 || f == 6 || f == 9) t = t * sc;
                     en[f] = (t > en[f]) ? t : en[f];
                 }
+                o->alpha[k] = al;
             }
 #define MAXD(x, y) ((x) > (y) ? (x) : (y))
             /* :475-483 (xx xy yy xz yz zz; ro rou rov row) */
@@ -3810,6 +3816,56 @@ int or3_step(Or3 *o, double dt, int nsteps, int pid) {
         else o->s->driving_force[0] = o->s->driving_force[1] = o->s->driving_force[2] = 0.0;
     }
     return 0;
+}
+
+/* output_layer in 3-D with -Dallout (output.F90:184-310): 13 columns a node-layer, layer-major:
+   rho - rho_char, u, v, w, |vorticity| (walls: the turned gradients of :226-235), Q (never set
+   in 3-D by the reference: 0 here), alpha_out, c xx xy yy xz yz zz; the header's 9 values */
+int or3_get_dump(Or3 *o, double *out, double *header) {
+    const OrSim *s = o->s;
+    const size_t n = o->n3;
+    double *G[9];
+    for (int q = 0; q < 9; q++) G[q] = zarr((int)n);
+    grad3(o, o->u, 1, 7, G[0], G[1], G[2]);
+    grad3(o, o->v, 2, 7, G[3], G[4], G[5]);
+    grad3(o, o->w, 0, 7, G[6], G[7], G[8]);
+    for (size_t k = 0; k < n; k++) {
+        const int i = (int)(k % o->nl);
+        const double ux = G[0][k], uy = G[1][k], uz = G[2][k], vx = G[3][k], vy = G[4][k], vz = G[5][k];
+        const double wx = G[6][k], wy = G[7][k];
+        double a, b, c;
+        if (o->bidx[i] >= 0 && s->type[i] == 0) {
+            const double xn = s->rnx[i], yn = s->rny[i];
+            a = wy - (xn * vz - yn * uz);
+            b = (xn * uz + yn * vz) - wx;
+            c = (((xn * vx) - yn * ux) - xn * uy) - yn * vy;
+        } else {
+            a = wy - vz;
+            b = uz - wx;
+            c = vx - uy;
+        }
+        const double col[13] = {-s->rho_char + o->ro[k], o->u[k], o->v[k], o->w[k], sqrt((a * a + b * b) + c * c), 0.0, o->alpha[k],
+                                o->c[0][k], o->c[1][k], o->c[2][k], o->c[3][k], o->c[4][k], o->c[5][k]};
+        for (int q = 0; q < 13; q++) out[(size_t)q * n + k] = col[q];
+    }
+    for (int q = 0; q < 9; q++) free(G[q]);
+    const double hd[9] = {s->eflow_nm1, s->sum_eflow, s->driving_force[0], 0.0, 0.0, o->emax_np1, o->emax_n, o->emax_nm1, o->dt};
+    for (int q = 0; q < 9; q++) header[q] = hd[q];
+    return 0;
+}
+
+/* mass_and_energy_check in 3-D (statistics.F90:305-330): dV = vol dz, node-layers in order */
+double or3_kinetic_energy(Or3 *o) {
+    double ke = 0.0;
+    for (size_t k = 0; k < o->n3; k++)
+        ke = ke + ((0.5 * o->ro[k]) * ((o->u[k] * o->u[k] + o->v[k] * o->v[k]) + o->w[k] * o->w[k])) *
+                      (o->s->vol[k % o->nl] * o->dz);
+    return ke;
+}
+double or3_mass(Or3 *o) {
+    double m = 0.0;
+    for (size_t k = 0; k < o->n3; k++) m = m + o->ro[k] * (o->s->vol[k % o->nl] * o->dz);
+    return m;
 }
 
 int or3_get_time(Or3 *o, double *time, double *dt, int *itime, double *emax) {

@@ -745,15 +745,29 @@ int sunset_set_time(SunsetHandle *sh, double time, double dt, int itime, const d
     return 0;
 }
 
+// mass_and_energy_check (statistics.F90:305-330): over the 2-D state, or the 3-D one with
+// dV = vol dz
 int sunset_kinetic_energy(SunsetHandle *sh, double *ke) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
+    if (!ke) return set_err(H, SUNSET_ERR_ARG, "null pointer");
+    if (H->nz > 0) {
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        return ke_mass3(H, ke, nullptr);
+    }
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     return reduce_ke_mass(H, ke, nullptr);
 }
 
 int sunset_mass(SunsetHandle *sh, double *mass) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
+    if (!mass) return set_err(H, SUNSET_ERR_ARG, "null pointer");
+    if (H->nz > 0) {
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        return ke_mass3(H, nullptr, mass);
+    }
+    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     return reduce_ke_mass(H, nullptr, mass);
 }
 
@@ -846,15 +860,26 @@ int sunset_set_lengths(SunsetHandle *sh, const double *h, const double *h_small)
 int sunset_get_dump(SunsetHandle *sh, double *columns, double *header) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (!columns || !header) return set_err(H, SUNSET_ERR_ARG, "null array");
-    const int n = H->npfb;
-    double *cols = nullptr;
-    if (dalloc(H, &cols, 10 * (size_t)n)) return SUNSET_ERR_NOMEM;
-    int rc = dump_columns(H, cols);
-    for (int f = 0; f < 10 && !rc; f++) rc = to_reference(H, cols + (size_t)f * n, SUNSET_PTR_HOST, columns + (size_t)f * n);
-    dfree(H, cols);
-    if (rc) return rc;
+    if (H->nz > 0) {  // 13 columns over every node-layer, layer-major (output.F90:296-299, -Dallout)
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        const size_t n = (size_t)H->npfb * H->nz;
+        double *cols = nullptr;
+        if (dalloc(H, &cols, 13 * n)) return SUNSET_ERR_NOMEM;
+        int rc = dump3_columns(H, cols);
+        for (int f = 0; f < 13 && !rc; f++) rc = state3_column_to_host(H, cols + (size_t)f * n, columns + (size_t)f * n);
+        dfree(H, cols);
+        if (rc) return rc;
+    } else {
+        if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
+        const int n = H->npfb;
+        double *cols = nullptr;
+        if (dalloc(H, &cols, 10 * (size_t)n)) return SUNSET_ERR_NOMEM;
+        int rc = dump_columns(H, cols);
+        for (int f = 0; f < 10 && !rc; f++) rc = to_reference(H, cols + (size_t)f * n, SUNSET_PTR_HOST, columns + (size_t)f * n);
+        dfree(H, cols);
+        if (rc) return rc;
+    }
     DevScalars sc;
     SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
     // eflow_nm1, sum_eflow, driving_force(3) (only its x component is ever set), emax_np1,
@@ -868,25 +893,49 @@ int sunset_write_dump(SunsetHandle *sh, const char *directory, int n_out, double
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (!directory || n_out < 0) return set_err(H, SUNSET_ERR_ARG, "bad arguments");
-    const int n = H->npfb;
-    std::vector<double> cols(10 * (size_t)n), hd(9);
+    const int nz = H->nz > 0 ? H->nz : 1, ncol = H->nz > 0 ? 13 : 10;
+    const long long n = (long long)H->npfb * nz;  // rows: the nodes, or every node-layer in 3-D
+    std::vector<double> cols(ncol * (size_t)n), hd(9);
     if (int rc = sunset_get_dump(sh, cols.data(), hd.data())) return rc;
     const std::string dir(directory);
     const std::string fname = dir + "/fields_10000_" + std::to_string(n_out);
     FILE *f = fopen(fname.c_str(), "w");
     if (!f) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", fname.c_str());
     // output.F90:272-310, list-directed layout
-    fprintf(f, " !! header !!\n %d\n", n);
+    fprintf(f, " !! header !!\n %lld\n", n);
     fprintf(f, " %.17E %.17E %.17E %.17E %.17E\n", hd[0], hd[1], hd[2], hd[3], hd[4]);
     fprintf(f, " %.17E %.17E %.17E %.17E\n", hd[5], hd[6], hd[7], hd[8]);
     fprintf(f, " !! end header !!\n");
-    for (int i = 0; i < n; i++) {
-        for (int c = 0; c < 10; c++) fprintf(f, " %.17E", cols[(size_t)c * n + i]);
+    for (long long i = 0; i < n; i++) {
+        for (int c = 0; c < ncol; c++) fprintf(f, " %.17E", cols[(size_t)c * n + i]);
         fputc('\n', f);
     }
     const bool ok = fclose(f) == 0;
     if (!ok) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", fname.c_str());
-    if (n_out == 1) {  // output_nodes, output.F90:421-476
+    if (n_out == 1 && H->nz > 0) {  // output_nodes in 3-D: gi + layer offset, x, y, z, s, h, h_small, type
+        const int nl = H->npfb;
+        std::vector<double> x(nl), y(nl), sp(nl), hv(nl), hsv(nl);
+        std::vector<int> t(nl);
+        SUNSET_CUDA(H, cudaMemcpy(x.data(), H->px, nl * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(y.data(), H->py, nl * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(sp.data(), H->sp, nl * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(hv.data(), H->h, nl * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(hsv.data(), H->hs, nl * sizeof(double), cudaMemcpyDeviceToHost));
+        SUNSET_CUDA(H, cudaMemcpy(t.data(), H->ntype, nl * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int> at(nl);
+        for (int i = 0; i < nl; i++) at[H->h_perm[i]] = i;
+        const std::string nname = dir + "/nodes_10000";
+        FILE *g = fopen(nname.c_str(), "w");
+        if (!g) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", nname.c_str());
+        fprintf(g, " %lld\n", n);
+        for (int iz = 0; iz < H->nz; iz++)  // setup_domain.F90:520-535
+            for (int r = 0; r < nl; r++) {
+                const int i = at[r];
+                fprintf(g, " %lld %.17E %.17E %.17E %.17E %.17E %.17E %d\n", (long long)H->h_gi[r] + (long long)iz * nl, x[i],
+                        y[i], (double)iz * H->dz, sp[i], hv[i], hsv[i], t[i]);
+            }
+        if (fclose(g) != 0) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", nname.c_str());
+    } else if (n_out == 1) {  // output_nodes, output.F90:421-476
         std::vector<double> x(n), y(n), sp(n), hv(n), hsv(n);
         std::vector<int> t(n);
         SUNSET_CUDA(H, cudaMemcpy(x.data(), H->px, n * sizeof(double), cudaMemcpyDeviceToHost));
@@ -910,7 +959,7 @@ int sunset_write_dump(SunsetHandle *sh, const char *directory, int n_out, double
     const std::string tname = dir + "/time.out";  // unit 21: time, dims, npfb, n_out, nprocs
     FILE *tf = fopen(tname.c_str(), "a");
     if (!tf) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", tname.c_str());
-    fprintf(tf, " %.17E 2 %d %d 1\n", time, n, n_out);
+    fprintf(tf, " %.17E %d %lld %d 1\n", time, H->nz > 0 ? 3 : 2, n, n_out);
     if (fclose(tf) != 0) return set_err(H, SUNSET_ERR_ARG, "cannot write %s", tname.c_str());
     return 0;
 }
@@ -920,15 +969,24 @@ int sunset_set_restart(SunsetHandle *sh, const double *columns, const double *he
     if (int rc = op_common(sh, &H)) return rc;
     if (!columns || !header) return set_err(H, SUNSET_ERR_ARG, "null array");
     if (header[3] != 0.0 || header[4] != 0.0)
-        return set_err(H, SUNSET_ERR_SCOPE, "driving_force(2:3) must be zero on this 2-D path");
-    const int n = H->npfb;
-    // load_restart_file, setup_flow.F90:448-552: rho = (rho - rho_char) + rho_char, u, v, c
-    std::vector<double> ro(n);
-    for (int i = 0; i < n; i++) ro[i] = columns[i] + 1.0;
+        return set_err(H, SUNSET_ERR_SCOPE, "driving_force(2:3) must be zero (the controller drives x only)");
     const double *c = columns;
-    if (int rc = sunset_set_state(sh, ro.data(), c + n, c + 2 * (size_t)n, c + 6 * (size_t)n, c + 7 * (size_t)n,
-                                  c + 8 * (size_t)n, c + 9 * (size_t)n))
-        return rc;
+    if (H->nz > 0) {  // load_restart_file in 3-D (setup_flow.F90:505-509): 13 columns a node-layer
+        const size_t n = (size_t)H->npfb * H->nz;
+        std::vector<double> ro(n);
+        for (size_t k = 0; k < n; k++) ro[k] = c[k] + 1.0;
+        if (int rc = sunset_set_state_3d(sh, ro.data(), c + n, c + 2 * n, c + 3 * n, c + 7 * n, c + 8 * n, c + 9 * n,
+                                         c + 10 * n, c + 11 * n, c + 12 * n))
+            return rc;
+    } else {
+        const int n = H->npfb;
+        // load_restart_file, setup_flow.F90:448-552: rho = (rho - rho_char) + rho_char, u, v, c
+        std::vector<double> ro(n);
+        for (int i = 0; i < n; i++) ro[i] = columns[i] + 1.0;
+        if (int rc = sunset_set_state(sh, ro.data(), c + n, c + 2 * (size_t)n, c + 6 * (size_t)n, c + 7 * (size_t)n,
+                                      c + 8 * (size_t)n, c + 9 * (size_t)n))
+            return rc;
+    }
     DevScalars sc;
     SUNSET_CUDA(H, cudaMemcpy(&sc, H->dsc, sizeof(sc), cudaMemcpyDeviceToHost));
     sc.eflow_nm1 = header[0];
@@ -978,14 +1036,18 @@ int sunset_checkpoint_size(SunsetHandle *sh, size_t *bytes) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
     if (!bytes) return set_err(H, SUNSET_ERR_ARG, "null pointer");
-    *bytes = checkpoint_bytes(H);
+    *bytes = H->nz > 0 ? checkpoint3_bytes(H) : checkpoint_bytes(H);
     return 0;
 }
 
 int sunset_save_checkpoint(SunsetHandle *sh, void *buffer, size_t bytes) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "checkpoints hold 2-D states only");
+    if (H->nz > 0) {
+        if (int rc = need(H, H->state3_ok, "sunset_set_state_3d")) return rc;
+        if (!buffer || bytes < checkpoint3_bytes(H)) return set_err(H, SUNSET_ERR_ARG, "checkpoint buffer too small");
+        return checkpoint3_save(H, buffer);
+    }
     if (int rc = need(H, H->state_ok, "sunset_set_state")) return rc;
     if (!buffer || bytes < checkpoint_bytes(H)) return set_err(H, SUNSET_ERR_ARG, "checkpoint buffer too small");
     return checkpoint_save(H, buffer);
@@ -994,8 +1056,12 @@ int sunset_save_checkpoint(SunsetHandle *sh, void *buffer, size_t bytes) {
 int sunset_load_checkpoint(SunsetHandle *sh, const void *buffer, size_t bytes) {
     Handle *H;
     if (int rc = op_common(sh, &H)) return rc;
-    if (H->nz > 0) return set_err(H, SUNSET_ERR_SCOPE, "checkpoints hold 2-D states only");
     if (!buffer) return set_err(H, SUNSET_ERR_ARG, "null buffer");
+    if (H->nz > 0) {
+        if (int rc = checkpoint3_load(H, buffer, bytes)) return rc;
+        H->state3_ok = true;
+        return 0;
+    }
     if (int rc = state_alloc(H)) return rc;
     if (int rc = checkpoint_load(H, buffer, bytes)) return rc;
     H->state_ok = true;

@@ -29,6 +29,8 @@
 // the right-hand sides run in point3_body<FORM, true>, and apply_time_dependent_bounds after
 // each stage and after the filter holds rho u, rho v, rho w at zero on walls and prescribes a
 // hard inflow's momentum, with u_inflow_local on its ramp.
+#include <cstring>
+
 #include "internal.cuh"
 #include "physics.cuh"
 
@@ -367,6 +369,7 @@ struct Point3 {
     const int *ntype, *bidx, *brow;
     const double *rnx, *rny, *sp;
     double *uin;
+    double *alpha;  // stage 3: each node-layer's step error (alpha_out, step.F90:456-458)
     const double *fen;                    // FENE-P function of the direct form, or null
     int chl, lc;
     const double *in[19];                 // ro rou rov row u v w cxx cxy cyy cxz cyz czz psi(6)
@@ -907,7 +910,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
             const double bh = stage == 0 ? SUNSET_RK_BH1 : stage == 1 ? SUNSET_RK_BH2 : stage == 2 ? SUNSET_RK_BH3 : SUNSET_RK_BH4;
             const double RKb = dt * b, RKbmbh = dt * (b - bh);
             double Un[10];
-            double en = 0.0;
+            double en = 0.0, al = 0.0;
             for (int q = 0; q < 10; q++) Un[q] = P.in[src[q]][k];
             // every register read before the first is written (the compiler cannot tell the
             // arrays apart, and would otherwise wait out each load after a store)
@@ -930,6 +933,7 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                     Un[q] = S + RKb * r[q];
                     const double norm = q == 0 ? K.ero_norm : q < 4 ? K.erou_norm : K.exx_norm;
                     double t = fabs(E + RKbmbh * r[q]) * norm;
+                    if (q != 3 && q < 7) al = (t > al) ? t : al;  // alpha_out: rho, momentum x y, xx xy yy
                     // Cholesky FENE-P (step.F90:442-452): the xx, xy, yy and zz errors scaled by
                     // 1/sqrt(f) of the node-layer's c, each node-layer's own before the maximum
                     if (kChl && K.fenep && (q == 4 || q == 5 || q == 6 || q == 9))
@@ -938,7 +942,10 @@ __device__ __forceinline__ unsigned long long point3_body(const Point3 &P, size_
                     if (t != t) en = t;
                 }
             }
-            if (stage == 3) eb = dbits(en);
+            if (stage == 3) {
+                eb = dbits(en);
+                P.alpha[k] = al;
+            }
             // apply_time_dependent_bounds (characteristic_boundaries.F90:191-257) at the stage's
             // time time0 + c_s dt: walls at rest; on inflow node-layers u_inflow_local follows
             // its ramp, and a hard inflow prescribes the momentum
@@ -1369,6 +1376,7 @@ Point3 point3(Handle *H, int b, int stage) {
     P.rny = H->rny;
     P.sp = H->sp;
     P.uin = H->uin3;
+    P.alpha = H->alpha3;
     P.fen = (H->cfg.form == SUNSET_FORM_DI && H->cfg.fenep) ? H->tmp3 : nullptr;
     for (int f = 0; f < 19; f++) {
         P.in[f] = H->f3[b][f];
@@ -1465,9 +1473,11 @@ int layers_set(Handle *H, double Lz) {
     return 0;
 }
 
-static int state3_alloc(Handle *H) {
+int state3_alloc(Handle *H) {
     if (H->g3) return 0;
     const size_t n = n3(H);
+    if (dalloc(H, &H->alpha3, n)) return SUNSET_ERR_NOMEM;
+    SUNSET_CUDA(H, cudaMemsetAsync(H->alpha3, 0, n * sizeof(double), H->stream));
     for (int b = 0; b < 2; b++)
         for (int f = 0; f < 19; f++)
             if (dalloc(H, &H->f3[b][f], n)) return SUNSET_ERR_NOMEM;
@@ -1548,6 +1558,16 @@ int state3_get(Handle *H, double *out19) {
     return 0;
 }
 
+// one internal node-layer array to the reference's layer-major order, in host memory
+int state3_column_to_host(Handle *H, const double *dev, double *host) {
+    const size_t n = n3(H);
+    k3_scatter<<<nblk(n), 128, 0, H->stream>>>(dev, H->perm, H->npfb, H->nz, n, H->tmp3);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaMemcpyAsync(host, H->tmp3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
 // out10: the right-hand sides ro rou rov row xx xy yy xz yz zz, reference layer-major, host
 int rhs3_calc(Handle *H, double *out10) {
     const size_t n = n3(H);
@@ -1622,6 +1642,182 @@ int step3_run(Handle *H, double dt, int nsteps, int mode, cudaEvent_t *ev) {
 }
 
 
+// The 13 columns of the 3-D fields dump (output_layer, output.F90:184-310 with -Dallout, every
+// node-layer): rho - rho_char, u, v, w, the vorticity magnitude from the 3-D velocity gradient
+// (calc_gradient: the layer's x-y weights, on walls in the normal-tangent frame and turned
+// there as :226-235 does, and the z stencil), Q (which the reference never sets in 3-D: 0),
+// alpha_out, then c xx xy yy xz yz zz.  Internal order, one column after another.
+__global__ void k3_dump(Layer3 L, Fields3 F, const int *ntype, const double *rnx, const double *rny, const double *alpha,
+                        double rho_char, double *out) {
+    const size_t n = (size_t)L.nl * L.nz;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = (int)((unsigned)k / (unsigned)L.nz), iz = (int)k - i * L.nz, row = i * L.nz, h = L.ncfd / 2;
+    const double *fu = F.p[4], *fv = F.p[5], *fw = F.p[6];
+    double g[3][3];  // [u v w][x y z]
+    const double *ff[3] = {fu, fv, fw};
+    const int cls[3] = {1, 2, 0};
+    const long long base = L.slice_ptr[i >> 5];
+    for (int f = 0; f < 3; f++) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int q = 0; q < L.cnt_small[i]; q++) {
+            const long long o = sell_at(base, q, i & 31);
+            const int l = L.lidx[o];
+            const double x = mirror_value(ff[f][(l & kLinkMask) * L.nz + iz], cls[f], (int)((unsigned)l >> 30));
+            sx = sx + x * L.wx[o];
+            sy = sy + x * L.wy[o];
+        }
+        for (int m = 0; m < L.ncfd; m++) sz = sz + ff[f][row + zwrap(iz + m - h, L.nz)] * L.fdg[m];
+        g[f][0] = sx - ff[f][k] * L.gsx[i];
+        g[f][1] = sy - ff[f][k] * L.gsy[i];
+        g[f][2] = sz;
+    }
+    double a, b, c;
+    if (ntype && ntype[i] == 0) {
+        const double xn = rnx[i], yn = rny[i];
+        a = g[2][1] - (xn * g[1][2] - yn * g[0][2]);
+        b = (xn * g[0][2] + yn * g[1][2]) - g[2][0];
+        c = (((xn * g[1][0]) - yn * g[0][0]) - xn * g[0][1]) - yn * g[1][1];
+    } else {
+        a = g[2][1] - g[1][2];
+        b = g[0][2] - g[2][0];
+        c = g[1][0] - g[0][1];
+    }
+    const double vort = sqrt((a * a + b * b) + c * c);
+    const double col[13] = {-rho_char + F.p[0][k], fu[k], fv[k], fw[k], vort, 0.0, alpha[k],
+                            F.p[7][k], F.p[8][k], F.p[9][k], F.p[10][k], F.p[11][k], F.p[12][k]};
+    for (int q = 0; q < 13; q++) out[(size_t)q * n + k] = col[q];
+}
+int dump3_columns(Handle *H, double *out13) {
+    const size_t n = n3(H);
+    Fields3 F{};
+    for (int q = 0; q < 19; q++) F.p[q] = H->f3[H->cur3][q];
+    k3_dump<<<nblk(n), 128, 0, H->stream>>>(layer3(H), F, H->nb > 0 ? H->ntype : nullptr, H->rnx, H->rny, H->alpha3, 1.0,
+                                            out13);
+    SUNSET_CUDA(H, cudaGetLastError());
+    return 0;
+}
+
+// Checkpoint of a 3-D handle: the 19 fields of the current buffer, the step's scalars, the
+// node-layers' step error and (with boundary nodes) u_inflow_local, in the internal order,
+// behind a header that names the configuration, the layers and the node set's fingerprint.
+namespace {
+struct Checkpoint3Header {
+    char magic[8];
+    int version, npfb, nz, form, fenep, nb;
+    double dz, xsum, ysum;
+};
+}  // namespace
+size_t checkpoint3_bytes(const Handle *H) {
+    return sizeof(Checkpoint3Header) + sizeof(DevScalars) + (20 + (H->nb > 0 ? 1 : 0)) * n3(H) * sizeof(double);
+}
+static int checkpoint3_header(Handle *H, Checkpoint3Header &hd) {
+    memset(&hd, 0, sizeof(hd));
+    memcpy(hd.magic, "SUNSET3D", 8);
+    hd.version = 1;
+    hd.npfb = H->npfb;
+    hd.nz = H->nz;
+    hd.form = H->cfg.form;
+    hd.fenep = H->cfg.fenep;
+    hd.nb = H->nb;
+    hd.dz = H->dz;
+    std::vector<double> x(H->npfb), y(H->npfb);
+    SUNSET_CUDA(H, cudaMemcpy(x.data(), H->px, H->npfb * sizeof(double), cudaMemcpyDeviceToHost));
+    SUNSET_CUDA(H, cudaMemcpy(y.data(), H->py, H->npfb * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < H->npfb; i++) { hd.xsum = hd.xsum + x[i]; hd.ysum = hd.ysum + y[i]; }
+    return 0;
+}
+int checkpoint3_save(Handle *H, void *buf) {
+    Checkpoint3Header hd;
+    if (int rc = checkpoint3_header(H, hd)) return rc;
+    const size_t n = n3(H);
+    char *p = static_cast<char *>(buf);
+    memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    SUNSET_CUDA(H, cudaMemcpyAsync(p, H->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, H->stream));
+    p += sizeof(DevScalars);
+    for (int f = 0; f < 19; f++, p += n * sizeof(double))
+        SUNSET_CUDA(H, cudaMemcpyAsync(p, H->f3[H->cur3][f], n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaMemcpyAsync(p, H->alpha3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    p += n * sizeof(double);
+    if (H->nb > 0) SUNSET_CUDA(H, cudaMemcpyAsync(p, H->uin3, n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+int checkpoint3_load(Handle *H, const void *buf, size_t bytes) {
+    if (bytes != checkpoint3_bytes(H))
+        return set_err(H, SUNSET_ERR_ARG, "checkpoint of %zu bytes, expected %zu", bytes, checkpoint3_bytes(H));
+    Checkpoint3Header mine, hd;
+    if (int rc = checkpoint3_header(H, mine)) return rc;
+    const char *p = static_cast<const char *>(buf);
+    memcpy(&hd, p, sizeof(hd));
+    if (memcmp(hd.magic, mine.magic, 8) != 0 || hd.version != mine.version || hd.npfb != mine.npfb || hd.nz != mine.nz ||
+        hd.form != mine.form || hd.fenep != mine.fenep || hd.nb != mine.nb || hd.dz != mine.dz || hd.xsum != mine.xsum ||
+        hd.ysum != mine.ysum)
+        return set_err(H, SUNSET_ERR_ARG, "checkpoint written for another configuration, layering or node set");
+    if (int rc = state3_alloc(H)) return rc;
+    const size_t n = n3(H);
+    p += sizeof(hd);
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->dsc, p, sizeof(DevScalars), cudaMemcpyHostToDevice, H->stream));
+    p += sizeof(DevScalars);
+    H->cur3 = 0;
+    for (int f = 0; f < 19; f++, p += n * sizeof(double))
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->f3[0][f], p, n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    SUNSET_CUDA(H, cudaMemcpyAsync(H->alpha3, p, n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    p += n * sizeof(double);
+    if (H->nb > 0) SUNSET_CUDA(H, cudaMemcpyAsync(H->uin3, p, n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    // the mass correction's total volume, as sunset_set_state_3d leaves it
+    k3_mass_partials<<<nblk(n), 128, 0, H->stream>>>(H->nz, n, H->f3[0][0], H->vol, 1.0, 1, H->partials3);
+    k3_fold<<<1, kFoldThreads, 0, H->stream>>>(H->partials3, (int)nblk(n), &H->dsc->tv, nullptr, 1);
+    SUNSET_CUDA(H, cudaGetLastError());
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    return 0;
+}
+
+// Kinetic energy and mass of the 3-D state (mass_and_energy_check, statistics.F90:305-330, with
+// dV = vol dz): block sums in a fixed tree, the blocks summed in order on the host.
+__global__ void k3_ke_mass(int nz, size_t n, const double *ro, const double *u, const double *v, const double *w,
+                           const double *vol, double dz, double *pk, double *pm) {
+    __shared__ double s1[128], s2[128];
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0, m = 0.0;
+    if (k < n) {
+        const double dv = vol[k / nz] * dz;
+        ke = ((0.5 * ro[k]) * ((u[k] * u[k] + v[k] * v[k]) + w[k] * w[k])) * dv;
+        m = ro[k] * dv;
+    }
+    s1[threadIdx.x] = ke;
+    s2[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+            s2[threadIdx.x] = s2[threadIdx.x] + s2[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        pk[blockIdx.x] = s1[0];
+        pm[blockIdx.x] = s2[0];
+    }
+}
+int ke_mass3(Handle *H, double *ke, double *mass) {
+    const size_t n = n3(H);
+    const unsigned nb = nblk(n), off = nb + 16;
+    const double *const *f = H->f3[H->cur3];
+    k3_ke_mass<<<nb, 128, 0, H->stream>>>(H->nz, n, f[0], f[4], f[5], f[6], H->vol, H->dz, H->partials3, H->partials3 + off);
+    SUNSET_CUDA(H, cudaGetLastError());
+    std::vector<double> pk(nb), pm(nb);
+    SUNSET_CUDA(H, cudaMemcpyAsync(pk.data(), H->partials3, nb * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaMemcpyAsync(pm.data(), H->partials3 + off, nb * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+    SUNSET_CUDA(H, cudaStreamSynchronize(H->stream));
+    double a = 0.0, b = 0.0;
+    for (unsigned q = 0; q < nb; q++) { a += pk[q]; b += pm[q]; }
+    if (ke) *ke = a;
+    if (mass) *mass = b;
+    return 0;
+}
+
 int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
     if (reps < 1) reps = 1;
     DevScalars s;
@@ -1642,7 +1838,8 @@ int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
     // Algorithmic bytes of one fused stage launch (k3_stage), averaged over the four stages:
     // the state fields the stage reads (gathered or pointwise, 8 bytes a node-layer each) once,
     // the next state and its derived fields written once, the RK registers S and E of the ten
-    // evolved fields read in stages 1-3 and written in stages 0-2, the FENE-P function of the
+    // evolved fields read in stages 1-3 and written in stages 0-2, the step error of each
+    // node-layer written by the final stage, the FENE-P function of the
     // direct form read once, the layer's small links once (a 4-byte index and three 8-byte
     // weights; all layers share them) with the three stencil sums and the ordinate of each
     // node of the layer.  Neighbours' values re-read through the caches are not counted.
@@ -1657,7 +1854,7 @@ int time3_derivs(Handle *H, int reps, double *ms, double *bytes) {
         for (int c : cs) links += c;
     }
     const double fen = (form == SUNSET_FORM_DI && H->cfg.fenep) ? 8.0 : 0.0;
-    *bytes = (double)n3(H) * (8.0 * (nread + nwrite) + 16.0 * nevo * 6.0 / 4.0 + fen) + (double)links * 28.0 +
+    *bytes = (double)n3(H) * (8.0 * (nread + nwrite) + 16.0 * nevo * 6.0 / 4.0 + 8.0 / 4.0 + fen) + (double)links * 28.0 +
              (double)H->npfb * 32.0;
     return 0;
 }

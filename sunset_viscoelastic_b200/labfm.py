@@ -22,6 +22,9 @@ STATE_FIELDS = ["ro", "rou", "rov", "u", "v", "psixx", "psixy", "psiyy", "psizz"
 RHS_FIELDS = ["ro", "rou", "rov", "xx", "xy", "yy", "zz"]
 # columns of a fields dump (output.F90:299-301)
 DUMP_COLUMNS = ["ro_minus_rho_char", "u", "v", "vort", "qcrit", "alpha", "cxx", "cxy", "cyy", "czz"]
+# the 3-D dump (output.F90:296-299): every node-layer, layer-major
+DUMP_COLUMNS_3D = ["ro_minus_rho_char", "u", "v", "w", "vort", "qcrit", "alpha", "cxx", "cxy", "cyy", "cxz", "cyz",
+                   "czz"]
 # return codes of include/sunset_gpu.h
 ERR_ARG, ERR_CUDA, ERR_SVD, ERR_SCOPE, ERR_NONFINITE, ERR_NOMEM, ERR_ILLCOND = -1, -2, -3, -4, -5, -6, -7
 
@@ -256,21 +259,28 @@ class Sunset:
         f = lambda a: np.ascontiguousarray(a, np.float64)
         self._chk(self.L.sunset_set_lengths(self.h, f(h), f(h_small)))
 
-    def dump(self):
-        """(columns dict of output_layer's 10 columns, header array of 9) in reference order."""
+    def _dump_layout(self):
+        nz, _ = self.layers()
         n = self.sizes()[1]
-        cols, hd = np.zeros(10 * n), np.zeros(9)
+        return (DUMP_COLUMNS_3D, n * nz) if nz > 0 else (DUMP_COLUMNS, n)
+
+    def dump(self):
+        """(columns dict of output_layer's columns, header array of 9) in reference order: 10
+        columns a node, or on a 3-D handle 13 a node-layer."""
+        keys, n = self._dump_layout()
+        cols, hd = np.zeros(len(keys) * n), np.zeros(9)
         self._chk(self.L.sunset_get_dump(self.h, cols, hd))
-        cols = cols.reshape(10, n)
-        return {k: cols[i].copy() for i, k in enumerate(DUMP_COLUMNS)}, hd
+        cols = cols.reshape(len(keys), n)
+        return {k: cols[i].copy() for i, k in enumerate(keys)}, hd
 
     def write_dump(self, directory, n_out, time=0.0):
         self._chk(self.L.sunset_write_dump(self.h, str(directory).encode(), int(n_out), float(time)))
 
     def set_restart(self, columns, header):
-        """load_restart_file from dump columns (dict or 10 x npfb array) and header."""
+        """load_restart_file from dump columns (dict, or the columns x rows array of dump()) and
+        header."""
         if isinstance(columns, dict):
-            columns = np.stack([columns[k] for k in DUMP_COLUMNS])
+            columns = np.stack([columns[k] for k in self._dump_layout()[0]])
         self._chk(self.L.sunset_set_restart(self.h, np.ascontiguousarray(columns, np.float64).ravel(),
                                             np.ascontiguousarray(header, np.float64)))
 

@@ -144,6 +144,9 @@ def test_steps(pair):
     tr, tg = ref.time(), gpu.time()
     np.testing.assert_allclose(tg["time"], tr["time"], rtol=1e-14)
     np.testing.assert_allclose(tg["emax"], tr["emax"], rtol=1e-6)
+    # mass_and_energy_check with dV = vol dz (the device sums in a fixed tree)
+    np.testing.assert_allclose(gpu.kinetic_energy(), ref.kinetic_energy(), rtol=1e-11)
+    np.testing.assert_allclose(gpu.mass(), ref.mass(), rtol=1e-13)
     # PID-controlled steps (set_tstep + set_tstep_PID before each)
     for o in (ref, gpu):
         o.step(0.0, 10, pid=True)

@@ -153,7 +153,10 @@ def test_call_order_and_3d_scope():
     assert code_of(g.calc_labf_weights) == labfm.ERR_ARG    # before find_neighbours
     g.setup()
     assert code_of(g.step, 1e-5, 1) == labfm.ERR_ARG        # before set_state
+    assert code_of(g.kinetic_energy) == labfm.ERR_ARG       # no state to reduce yet
+    assert code_of(g.mass) == labfm.ERR_ARG
     g.set_layers(0.25)
-    assert code_of(g.load_checkpoint, b"\0" * 64) == labfm.ERR_SCOPE
-    assert code_of(g.save_checkpoint) == labfm.ERR_SCOPE
+    assert code_of(g.kinetic_energy) == labfm.ERR_ARG       # a 3-D handle: before set_state_3d
+    assert code_of(g.load_checkpoint, b"\0" * 64) == labfm.ERR_ARG   # not a 3-D checkpoint of this size
+    assert code_of(g.save_checkpoint) == labfm.ERR_ARG      # nothing to save before set_state_3d
     g.close()
