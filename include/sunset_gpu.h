@@ -170,7 +170,9 @@ int sunset_synchronize(SunsetHandle *h);
 
 /* Host-buffer round trip, the drop-in use from a host code that owns the fields: copy the
    evolved variables in from host arrays (pinned for full speed), run nsteps, copy them
-   back.  7*npfb in reference order: ro rou rov q_xx q_xy q_yy q_zz, q = c (DI) or psi. */
+   back.  7*npfb in reference order: ro rou rov q_xx q_xy q_yy q_zz, q = c (DI) or psi.  On a
+   3-D handle 10*npfb*nz, layer-major: ro rou rov row q_xx q_xy q_yy q_xz q_yz q_zz (the first 4
+   for the Newtonian form). */
 int sunset_run_host(SunsetHandle *h, const double *state_in, double dt, int nsteps, double *state_out);
 
 /* sunset_step with the steps bracketed by CUDA events on the handle's stream: *ms is the

@@ -1558,6 +1558,51 @@ int state3_get(Handle *H, double *out19) {
     return 0;
 }
 
+// u, v, w from the momentum and c from psi (get_velocity_from_momentum, get_c_from_psi,
+// step.F90:514-567) after the evolved fields were set
+__global__ void k3_derive(size_t n, Fields3 F, int chl, int lc, double L2) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double oo = 1.0 / F.p[0][k];
+    const double m1 = F.p[1][k], m2 = F.p[2][k], m3 = F.p[3][k];
+    double p[6], c[6];
+    if (chl || lc)
+        for (int q = 0; q < 6; q++) p[q] = F.p[13 + q][k];
+    F.p[4][k] = m1 * oo;
+    F.p[5][k] = m2 * oo;
+    F.p[6][k] = m3 * oo;
+    if (chl || lc) {
+        if (chl) chl3_c_from_psi(p, c, L2);
+        else lc3_transform(p, c, true);
+        for (int q = 0; q < 6; q++) F.p[7 + q][k] = c[q];
+    }
+}
+
+// The host-buffer round trip on a 3-D handle: the ten evolved fields (rho, rho u, rho v, rho w,
+// then c in the direct form or psi) of every node-layer, layer-major, in from host memory; nsteps
+// fixed-dt steps; the same fields back out.
+int run_host3(Handle *H, const double *state_in, double dt, int nsteps, double *state_out) {
+    const size_t n = n3(H);
+    cudaStream_t st = H->stream;
+    const bool chl = H->cfg.form == SUNSET_FORM_CHL, lc = H->cfg.form == SUNSET_FORM_LC;
+    const int c0 = (chl || lc) ? 13 : 7;
+    const int fld[10] = {0, 1, 2, 3, c0, c0 + 1, c0 + 2, c0 + 3, c0 + 4, c0 + 5};
+    const int nf = H->cfg.form == SUNSET_FORM_NEWT ? 4 : 10;
+    double *const *f = H->f3[H->cur3];
+    for (int q = 0; q < nf; q++) {
+        SUNSET_CUDA(H, cudaMemcpyAsync(H->tmp3, state_in + (size_t)q * n, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        k3_gather<<<nblk(n), 128, 0, st>>>(H->tmp3, H->perm, H->npfb, H->nz, n, f[fld[q]]);
+    }
+    Fields3 F19;
+    for (int q = 0; q < 19; q++) F19.p[q] = f[q];
+    k3_derive<<<nblk(n), 128, 0, st>>>(n, F19, chl, lc, H->cfg.fenep ? H->cfg.fenep_l2 : 0.0);
+    SUNSET_CUDA(H, cudaGetLastError());
+    if (int rc = step3_run(H, dt, nsteps, 0)) return rc;
+    for (int q = 0; q < nf; q++)
+        if (int rc = state3_column_to_host(H, H->f3[H->cur3][fld[q]], state_out + (size_t)q * n)) return rc;
+    return 0;
+}
+
 // one internal node-layer array to the reference's layer-major order, in host memory
 int state3_column_to_host(Handle *H, const double *dev, double *host) {
     const size_t n = n3(H);

@@ -457,7 +457,8 @@ class Sunset:
         self._chk(self.L.sunset_synchronize(self.h))
 
     def run_host(self, state_in_ptr, dt, nsteps, state_out_ptr):
-        """Host-buffer round trip (7*npfb doubles in and out, pointers to pinned memory)."""
+        """Host-buffer round trip (7*npfb doubles in and out, or 10*npfb*nz on a 3-D handle;
+        pointers to pinned memory)."""
         self._chk(self.L.sunset_run_host(self.h, C.c_void_p(state_in_ptr), float(dt), int(nsteps),
                                          C.c_void_p(state_out_ptr)))
 

@@ -28,6 +28,7 @@ import dataclasses
 
 import numpy as np
 import pytest
+import torch
 
 from sunset_viscoelastic_b200 import labfm
 from sunset_viscoelastic_b200.nodesets import WORKLOADS
@@ -198,6 +199,52 @@ def test_velocity_control_3d():
         e = float(np.abs(sg[k] - sr[k]).max() / max(np.abs(sr[k]).max(), 1e-300))
         assert e <= F_TOL, (k, e)
     gpu.close()
+
+
+def test_run_host_3d():
+    """The host-buffer round trip on a 3-D handle (the evolved fields of every node-layer in,
+    nsteps fixed-dt steps, out) against the same steps on a handle stepped in place."""
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=24)
+    ns = wl.nodes()
+    kw = dict(wl.params(), form="chl", epsPTT=0.25)
+    handles = []
+    for _ in range(2):
+        g = labfm.Sunset(**kw)
+        g.build_domain(ns)
+        nz, dz = g.set_layers(1.0)
+        g.setup()
+        handles.append(g)
+    a, b = handles
+    nl = a.sizes()[1]
+    O.set_pow_mode(True)
+    try:
+        layer = O.Oracle(**kw)
+        layer.build_domain(ns)
+        layer.setup()
+    finally:
+        O.set_pow_mode(False)
+    nd = layer.nodes()
+    st = state3(np.tile(nd["x"][:nl], nz), np.tile(nd["y"][:nl], nz), np.repeat(np.arange(nz) * dz, nl))
+    c = {k: st[k] for k in ["cxx", "cxy", "cyy", "cxz", "cyz", "czz"]}
+    for g in (a, b):
+        g.set_state_3d(st["ro"], st["u"], st["v"], st["w"], **c)
+    s0 = a.state_3d()
+    keys = ["ro", "rou", "rov", "row", "psixx", "psixy", "psiyy", "psixz", "psiyz", "psizz"]
+    pin = torch.from_numpy(np.concatenate([s0[k] for k in keys])).pin_memory()
+    pout = torch.zeros_like(pin).pin_memory()
+    dc, dp = a.set_tstep()
+    dt = 0.3 * min(dc, dp)
+    a.step(dt, 10)
+    b.run_host(pin.data_ptr(), dt, 10, pout.data_ptr())
+    sa = a.state_3d()
+    out = pout.numpy().reshape(10, -1)
+    for q, k in enumerate(keys):
+        e = float(np.abs(out[q] - sa[k]).max() / max(np.abs(sa[k]).max(), 1e-300))
+        assert e <= 1e-12, (k, e)
+    sb = b.state_3d()
+    assert np.array_equal(sb["rou"], out[1])
+    for g in handles:
+        g.close()
 
 
 def test_fenep_scope():
