@@ -527,9 +527,11 @@ def setup_block(wl, nodes, device_s, phases):
             "note": "wall seconds through the C-ABI setup calls, host-side link ordering included"}
 
 
-def adjoint_cost(wl, steps, checkpoint, warmup, local):
+def adjoint_cost(wl, steps, checkpoint, warmup, local, reps=3):
     """(forward s, adjoint s, J, dJ/dWi, dJ/dbeta, handle, state, dt): sunset_adjoint_run from
-    the initial state against the same forward run, wall clock with the device synchronised."""
+    the initial state against the same forward run, wall clock with the device synchronised;
+    each the median of `reps` runs from the initial state (the host's launch loop of a
+    0.1-0.5 s run varies by several per cent between runs)."""
     from sunset_viscoelastic_b200 import labfm
     ns = wl.nodes()
     g = labfm.for_workload(wl, ns, device=local).setup()
@@ -541,18 +543,20 @@ def adjoint_cost(wl, steps, checkpoint, warmup, local):
     g.step(dt, warmup)
     g.set_state(**st)
     g.adjoint_run(dt, steps, checkpoint, state_gradient=False)  # sizes the checkpoint store
-    g.set_state(**st)
-    g.synchronize()
-    t = time.perf_counter()
-    g.step(dt, steps)
-    g.synchronize()
-    fwd = time.perf_counter() - t
-    g.set_state(**st)
-    g.synchronize()
-    t = time.perf_counter()
-    J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, checkpoint)
-    adj = time.perf_counter() - t
-    return fwd, adj, J, dWi, dbeta, grads, g, ns, st, dt
+    fwds, adjs = [], []
+    for _ in range(max(1, reps)):
+        g.set_state(**st)
+        g.synchronize()
+        t = time.perf_counter()
+        g.step(dt, steps)
+        g.synchronize()
+        fwds.append(time.perf_counter() - t)
+        g.set_state(**st)
+        g.synchronize()
+        t = time.perf_counter()
+        J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, checkpoint)
+        adjs.append(time.perf_counter() - t)
+    return float(np.median(fwds)), float(np.median(adjs)), J, dWi, dbeta, grads, g, ns, st, dt
 
 
 def main():
