@@ -544,18 +544,21 @@ def adjoint_cost(wl, steps, checkpoint, warmup, local, reps=3):
     g.set_state(**st)
     g.adjoint_run(dt, steps, checkpoint, state_gradient=False)  # sizes the checkpoint store
     fwds, adjs = [], []
-    for _ in range(max(1, reps)):
-        g.set_state(**st)
-        g.synchronize()
-        t = time.perf_counter()
-        g.step(dt, steps)
-        g.synchronize()
-        fwds.append(time.perf_counter() - t)
-        g.set_state(**st)
-        g.synchronize()
-        t = time.perf_counter()
-        J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, checkpoint)
-        adjs.append(time.perf_counter() - t)
+    with ClockSampler(local) as clk:
+        for _ in range(max(1, reps)):
+            g.set_state(**st)
+            g.synchronize()
+            t = time.perf_counter()
+            g.step(dt, steps)
+            g.synchronize()
+            fwds.append(time.perf_counter() - t)
+            g.set_state(**st)
+            g.synchronize()
+            t = time.perf_counter()
+            J, (dWi, dbeta), grads = g.adjoint_run(dt, steps, checkpoint)
+            adjs.append(time.perf_counter() - t)
+    adjoint_cost.clocks = clk.summary()
+    adjoint_cost.samples = {"forward_s": fwds, "adjoint_s": adjs}
     return float(np.median(fwds)), float(np.median(adjs)), J, dWi, dbeta, grads, g, ns, st, dt
 
 
@@ -652,7 +655,8 @@ def main():
         ga.close()
         line["adjoint"] = {"value": adj / fwd, "unit": "x (adjoint / forward wall time)", "higher_is_better": False,
                            "workload": awl.name, "steps": 200, "checkpoint_every": 20, "forward_s": fwd,
-                           "adjoint_s": adj, "J": J, "dJ_dWi": dWi, "dJ_dbeta": dbeta,
+                           "adjoint_s": adj, "samples": adjoint_cost.samples, "clocks": adjoint_cost.clocks,
+                           "J": J, "dJ_dWi": dWi, "dJ_dbeta": dbeta,
                            "fd_check": "python bench.py --adjoint --steps 200 --fd-check"}
         # the same run with every step's stages recorded in HBM (one segment, about 52 GB at
         # 262,144 nodes): no forward recomputation
