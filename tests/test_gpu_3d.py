@@ -18,7 +18,12 @@ Reference behaviour restated (and followed by the device):
 * step.F90 with the dim3 error norms (row, xz, yz) and set_tstep with |u| including w;
 * FENE-P with the direct form (rhs_di.F90:198-245, 454-464): the function
   f = (L^2 - 3)/(L^2 - tr c) at every node, its 3-D gradient, the quotient-rule polymer force
-  and the FENE-P relaxation.  FENE-P with the Cholesky form is outside the 3-D path and refused.
+  and the FENE-P relaxation; FENE-P with the Cholesky form (rhs.F90:204-209, 479-500: the
+  factors of J = f c); FENE-P with the log-conformation form is refused (its 3-D branch reads
+  values the reference never sets);
+* the flow-rate controller with dV = vol dz, kinetic energy and mass, and the host-buffer
+  round trip on a 3-D handle.  Walls, inflow and outflow, output, restart and checkpoints have
+  their own files (test_gpu_3d_walls.py, test_gpu_3d_inout.py, test_gpu_3d_output.py).
 
 Tolerances as in the 2-D parity tests: state and right-hand sides within 1e-10 of their
 terms, fields after 50 steps within 1e-8 (the mass correction and the reductions are summed in
