@@ -11,11 +11,8 @@
  *
  * All functions return 0 on success or a negative SUNSET_ERR_* code; the message is
  * available from sunset_last_error().  Nothing aborts the host process.  A handle owns
- * one CUDA stream; calls on one handle must not overlap.  Distinct handles are independent
- * where their configurations agree (SunsetConfig and node set); the 2-D time step reads its
- * constants from one constant bank of the library, uploaded on the calling handle's stream,
- * so handles with different configurations are driven from one host thread at a time (the
- * stepping and operator calls return after their device work, host pointers given).
+ * one CUDA stream; calls on one handle must not overlap, distinct handles are independent
+ * (every kernel takes its run's constants as a launch parameter).
  */
 #ifndef SUNSET_GPU_H
 #define SUNSET_GPU_H

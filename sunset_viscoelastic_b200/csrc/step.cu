@@ -30,9 +30,9 @@ namespace sunset {
 
 namespace {
 
-__constant__ StepConsts cK;
 
 struct StageArgs {
+    StepConsts K;  // the run's constants (load_data.F90:131-148), a kernel parameter of every launch
     const long long *slice_ptr;
     const int *slice_ws, *slice_w;
     const int *lidx;
@@ -247,6 +247,7 @@ __host__ __device__ inline size_t halo_doubles(int ng, int hmax) { return ((size
 // below evaluates the difference form sum_k w_k (phi_j - phi_i) of the rounded stencil.
 template <int FORM, bool MD, bool MX, bool FP, class RING>
 __device__ __forceinline__ void gather_stage(const StageArgs &A, int i, const double *sm, RING &R, Grads &g) {
+    const StepConsts &cK = A.K;
     const int hm = A.hmax;
     const int npair = R.npair;
     const Fields &F = A.in;
@@ -492,6 +493,7 @@ struct MxRing {
 template <int FORM, bool MD, bool FP>
 __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *smem, MxRing &R, bool wact,
                                              float *oi) {
+    const StepConsts &cK = A.K;
     constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2;
     const int lane = threadIdx.x & 31;
     if (wact && lane == 0) {
@@ -539,6 +541,7 @@ __device__ __forceinline__ void load_halo_mx(const StageArgs &A, int i, double *
 template <int FORM, bool MD, bool FP, bool MIR>
 __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const double *smem, const MxRing &R,
                                                 bool wact, const float *oi, Grads &g) {
+    const StepConsts &cK = A.K;
     constexpr int NG = ngather(FORM, MD, FP), NP = (NG + 1) / 2, NW = mx_words(NG);
     constexpr int kFp = fp_slot(FORM, MD);
     const int lane = threadIdx.x & 31;
@@ -666,6 +669,7 @@ __device__ __forceinline__ void gather_stage_mx(const StageArgs &A, int i, const
 // order, neighbours from the tile's shared-memory halo.
 template <int FORM, bool MD, bool FP, class HV>
 __device__ __forceinline__ void wall_conformation_laplacian(const StageArgs &A, int i, HV hv, Grads &g) {
+    const StepConsts &cK = A.K;
     const int jj = A.bidx[i];
     const long long base = A.slice_ptr[i >> 5];
     const int ln = i & 31, cs = A.cnt_small[i];
@@ -762,6 +766,7 @@ __host__ __device__ constexpr int stage_min_blocks(bool mx) { return mx ? SUNSET
 // closures are compiled out, which keeps them from costing the periodic sets registers.
 template <int FORM, bool MD, bool MX, bool FP, bool BND>
 __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs A) {
+    const StepConsts &cK = A.K;
     extern __shared__ __align__(16) double smem[];
     constexpr int NG = ngather(FORM, MD, FP);
     const int i = blockIdx.x * kTile + threadIdx.x;
@@ -979,6 +984,7 @@ __global__ void __launch_bounds__(kTile, stage_min_blocks(MX)) k_stage(StageArgs
 // the halo, in registers for the node itself.
 template <int FORM, bool MX, bool FP = false>
 __global__ void __launch_bounds__(kTile, 4) k_filter(StageArgs A) {
+    const StepConsts &cK = A.K;
     extern __shared__ __align__(16) double smem[];
     constexpr bool CF = FP && FORM == SUNSET_FORM_CHL;
     constexpr int nf = (FORM == SUNSET_FORM_DI || CF) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
@@ -1111,6 +1117,7 @@ __host__ __device__ inline size_t mxf_smem_bytes(int nf, int hmax) {
 
 template <int FORM, bool FP, bool MIR>
 __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
+    const StepConsts &cK = A.K;
     extern __shared__ __align__(16) double smem[];
     constexpr bool CF = FP && FORM == SUNSET_FORM_CHL;
     constexpr int nf = (FORM == SUNSET_FORM_DI || CF) ? 7 : (FORM == SUNSET_FORM_NEWT ? 3 : 6);
@@ -1279,6 +1286,7 @@ __global__ void __launch_bounds__(kTile, 4) k_filter_mx(StageArgs A) {
 // bookkeeping (error-norm history, time, itime).
 template <int FORM>
 __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
+    const StepConsts &cK = A.K;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double dro = A.sc->dro;
     double uvol = 0.0;
@@ -1396,7 +1404,7 @@ __global__ void __launch_bounds__(128) k_finalize(StageArgs A, int advance) {
 // set_tstep (step.F90:569-622) over the current state: block minima of s/(|u|+c) and
 // s^2 rho/mu, folded into dt_cfl and dt_parabolic by k_pid / the host.
 __global__ void __launch_bounds__(128) k_tstep(const double *u, const double *v, const double *ro, const double *sp,
-                                                const int *ntype, int npfb, DevScalars *sc) {
+                                                const int *ntype, int npfb, DevScalars *sc, StepConsts cK) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double tc = 1.0e10, tp = 1.0e10;
     if (i < npfb) {
@@ -1410,7 +1418,7 @@ __global__ void __launch_bounds__(128) k_tstep(const double *u, const double *v,
 }
 
 // set_tstep_PID, step.F90:624-682.
-__global__ void k_pid(DevScalars *sc) {
+__global__ void k_pid(DevScalars *sc, StepConsts cK) {
     double dcfl = __longlong_as_double((long long)sc->cfl_bits);
     double dvisc = __longlong_as_double((long long)sc->par_bits);
     sc->dt_cfl = (1.0 * dcfl) * cK.L_char;
@@ -1429,7 +1437,7 @@ __global__ void k_pid(DevScalars *sc) {
     sc->par_bits = 0x7ff0000000000000ull;
 }
 
-__global__ void k_tstep_fold(DevScalars *sc) {
+__global__ void k_tstep_fold(DevScalars *sc, StepConsts cK) {
     double dcfl = __longlong_as_double((long long)sc->cfl_bits);
     double dvisc = __longlong_as_double((long long)sc->par_bits);
     sc->dt_cfl = (1.0 * dcfl) * cK.L_char;
@@ -1440,6 +1448,7 @@ __global__ void k_tstep_fold(DevScalars *sc) {
 // Single operators of the C-ABI (derivatives.F90), on a field in internal order.
 // ---------------------------------------------------------------------------------------
 __global__ void k_op_grad_lap(StageArgs A, const double *phi, double *gx, double *gy, double *lap) {
+    const StepConsts &cK = A.K;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if ((i >> 5) >= cK.nslices) return;
     const long long base = A.slice_ptr[i >> 5];
@@ -1461,6 +1470,7 @@ __global__ void k_op_grad_lap(StageArgs A, const double *phi, double *gx, double
 }
 
 __global__ void k_op_filter(StageArgs A, const double *phi, double *out, int term_only) {
+    const StepConsts &cK = A.K;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if ((i >> 5) >= cK.nslices) return;
     const long long base = A.slice_ptr[i >> 5];
@@ -1480,7 +1490,7 @@ __global__ void k_op_filter(StageArgs A, const double *phi, double *out, int ter
 // Wall nodes get zero velocity (setup_flow.F90:266-280).
 __global__ void k_set_state(int npfb, int form, const double *ro, const double *u, const double *v,
                             const double *cxx, const double *cxy, const double *cyy, const double *czz,
-                            const int *ntype, int has_walls, Fields F) {
+                            const int *ntype, int has_walls, Fields F, StepConsts cK) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
     double r = ro[i];
@@ -1519,7 +1529,8 @@ __global__ void k_set_state(int npfb, int form, const double *ro, const double *
 // Conservative state given directly (ro, rou, rov, q0..q3), derived fields recomputed
 // as get_velocity_from_momentum / get_c_from_psi do.
 __device__ __forceinline__ void set_conservative_node(int i, int form, double ro, double rou, double rov, double q0,
-                                                      double q1, double q2, double q3, const Fields &F) {
+                                                      double q1, double q2, double q3, const Fields &F,
+                                                      const StepConsts &cK) {
     F.ro[i] = ro; F.rou[i] = rou; F.rov[i] = rov;
     F.q[0][i] = q0; F.q[1][i] = q1; F.q[2][i] = q2; F.q[3][i] = q3;
     double ooro = 1.0 / ro;
@@ -1538,20 +1549,21 @@ __device__ __forceinline__ void set_conservative_node(int i, int form, double ro
     if (F.f) F.f[i] = fenep_f(cK.fenep_l2, F.c[0][i], F.c[2][i], F.c[3][i]);
 }
 __global__ void k_set_conservative(int npfb, int form, const double *ro, const double *rou, const double *rov,
-                                   const double *q0, const double *q1, const double *q2, const double *q3, Fields F) {
+                                   const double *q0, const double *q1, const double *q2, const double *q3, Fields F,
+                                   StepConsts cK) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
-    set_conservative_node(i, form, ro[i], rou[i], rov[i], q0[i], q1[i], q2[i], q3[i], F);
+    set_conservative_node(i, form, ro[i], rou[i], rov[i], q0[i], q1[i], q2[i], q3[i], F, cK);
 }
 // The state from checkpoint *seg of the adjoint's store (7 fields of npfb doubles each a
 // checkpoint): the index is read on the device, so a captured graph serves every segment.
-__global__ void k_load_checkpoint(int npfb, int form, const double *store, const int *seg, Fields F) {
+__global__ void k_load_checkpoint(int npfb, int form, const double *store, const int *seg, Fields F, StepConsts cK) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npfb) return;
     const double *cp = store + (size_t)7 * npfb * (size_t)*seg;
     const size_t n = (size_t)npfb;
     set_conservative_node(i, form, cp[i], cp[n + i], cp[2 * n + i], cp[3 * n + i], cp[4 * n + i], cp[5 * n + i],
-                          cp[6 * n + i], F);
+                          cp[6 * n + i], F, cK);
 }
 // Scalars set on the stream by a kernel rather than a copy from pageable host memory (which
 // the driver stages, and which can hold the host until the stream reaches it).
@@ -1613,9 +1625,16 @@ __global__ void k_fold_partials(const double *partials, int n, double *out) {
 // Kernel arguments over buffer `from`.  step: the time step's link stream (bank-aware order;
 // FP32 weights with their own sums in mixed precision); otherwise the reference-order FP64
 // arrays of the single-operator entry points.
+// The run's constants, passed to every kernel that reads them as a kernel parameter (so that
+// handles of different configurations never share them).
+StepConsts consts_of(const Handle *H) {
+    return step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, H->nb > 0, H->xmax - H->xmin, H->ymax - H->ymin);
+}
+
 StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     const bool mx = step && H->cfg.precision == SUNSET_MIXED;
     StageArgs A{};
+    A.K = consts_of(H);
     A.slice_ptr = H->slice_ptr;
     A.slice_ws = H->slice_ws;
     A.slice_w = H->slice_w;
@@ -1661,12 +1680,7 @@ StageArgs make_args(Handle *H, int from, int stage, bool step = false) {
     return A;
 }
 
-int upload_consts(Handle *H) {
-    const StepConsts K = step_consts(H->cfg, H->npfb, H->nslices, H->has_mirrors, H->nb > 0, H->xmax - H->xmin,
-                                     H->ymax - H->ymin);
-    SUNSET_CUDA(H, cudaMemcpyToSymbolAsync(cK, &K, sizeof(K), 0, cudaMemcpyHostToDevice, H->stream));
-    return 0;
-}
+int upload_consts(Handle *) { return 0; }
 
 constexpr size_t kMaxStageSmem = 200 * 1024;
 
@@ -1782,7 +1796,7 @@ int launch_step_kernels(Handle *H, int from, int pid, cudaEvent_t *stage_ev) {
     const int TB = 128;
     cudaStream_t st = H->stream;
     const bool mx = is_mx(H);
-    if (pid) k_pid<<<1, 1, 0, st>>>(H->dsc);
+    if (pid) k_pid<<<1, 1, 0, st>>>(H->dsc, consts_of(H));
     int b = from;
     for (int s = 0; s < 4; s++) {
         StageArgs A = make_args(H, b, s, true);
@@ -1797,7 +1811,7 @@ int launch_step_kernels(Handle *H, int from, int pid, cudaEvent_t *stage_ev) {
     StageArgs Z = make_args(H, b ^ 1, 5, true);  // in = filter input, out = filtered buffer
     const int fb = (H->npfb + TB - 1) / TB;
     k_finalize<FORM><<<fb, TB, 0, st>>>(Z, 1);
-    k_tstep<<<fb, TB, 0, st>>>(H->buf[b].u, H->buf[b].v, H->buf[b].ro, H->sp, H->ntype, H->npfb, H->dsc);
+    k_tstep<<<fb, TB, 0, st>>>(H->buf[b].u, H->buf[b].v, H->buf[b].ro, H->sp, H->ntype, H->npfb, H->dsc, consts_of(H));
     return 0;
 }
 
@@ -1893,7 +1907,7 @@ int state_set_device(Handle *H, const double *ro, const double *u, const double 
     if (rc) return rc;
     H->cur = 0;
     k_set_state<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, ro, u, v, cxx, cxy, cyy, czz,
-                                                              H->ntype, H->nb > 0, H->buf[0]);
+                                                              H->ntype, H->nb > 0, H->buf[0], consts_of(H));
     SUNSET_CUDA(H, cudaGetLastError());
     rc = init_scalars(H);
     if (rc) return rc;
@@ -1905,7 +1919,8 @@ int state_set_conservative_device(Handle *H, const double *const *f7) {
     int rc = upload_consts(H);
     if (rc) return rc;
     k_set_conservative<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(H->npfb, H->cfg.form, f7[0], f7[1], f7[2],
-                                                                     f7[3], f7[4], f7[5], f7[6], H->buf[H->cur]);
+                                                                     f7[3], f7[4], f7[5], f7[6], H->buf[H->cur],
+                                                                     consts_of(H));
     SUNSET_CUDA(H, cudaGetLastError());
     if (!H->uin_set) return init_inflow(H);
     return 0;
@@ -1917,8 +1932,8 @@ int set_tstep_device(Handle *H) {
     unsigned long long inf = 0x7ff0000000000000ull;
     SUNSET_CUDA(H, cudaMemcpyAsync(&sc->cfl_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, H->stream));
     SUNSET_CUDA(H, cudaMemcpyAsync(&sc->par_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, H->stream));
-    k_tstep<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(F.u, F.v, F.ro, H->sp, H->ntype, H->npfb, sc);
-    k_tstep_fold<<<1, 1, 0, H->stream>>>(sc);
+    k_tstep<<<(H->npfb + 127) / 128, 128, 0, H->stream>>>(F.u, F.v, F.ro, H->sp, H->ntype, H->npfb, sc, consts_of(H));
+    k_tstep_fold<<<1, 1, 0, H->stream>>>(sc, consts_of(H));
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -2067,7 +2082,7 @@ int time_stage_kernel(Handle *H, int reps, double *ms, double *bytes) {
 namespace {
 __global__ void k_dump(int n, Fields F, const double *gux, const double *guy, const double *gvx, const double *gvy,
                        const int *ntype, const double *rnx, const double *rny, int has_walls, const double *alpha,
-                       double *out) {
+                       double *out, StepConsts cK) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double ux = gux[i], uy = guy[i], vx = gvx[i], vy = gvy[i];
@@ -2099,7 +2114,7 @@ int dump_columns(Handle *H, double *out) {
     if (int rc = op_gradient(H, F.u, g, g + n)) return rc;
     if (int rc = op_gradient(H, F.v, g + 2 * (size_t)n, g + 3 * (size_t)n)) return rc;
     k_dump<<<(n + 127) / 128, 128, 0, H->stream>>>(n, F, g, g + n, g + 2 * (size_t)n, g + 3 * (size_t)n, H->ntype,
-                                                   H->rnx, H->rny, H->nb > 0, H->alpha, out);
+                                                   H->rnx, H->rny, H->nb > 0, H->alpha, out, consts_of(H));
     SUNSET_CUDA(H, cudaGetLastError());
     return 0;
 }
@@ -2240,6 +2255,7 @@ struct AdjArgs {
 
 // Kernels of the reverse sweep.
 struct RevArgs {
+    StepConsts K;               // the run's constants
     const long long *sptr;      // reverse link streams: slice starts (links)
     const int *sw, *sws;        // slice widths: all links (filter), small links (stage stencils)
     const uint16_t *locs, *locf;  // halo position | reflection code << 14: stage, filter order
@@ -2304,6 +2320,7 @@ __device__ __forceinline__ void tile_sum2(double &a, double &b) {
 // adjoint.cuh's reverse of the right-hand side at the recorded state and stencil sums.
 __device__ __forceinline__ void point_reverse(const RevArgs &B, int j, const double *ub, bool sbar_zero, double &t0,
                                               double &t1) {
+    const StepConsts &cK = B.K;
     const int n = cK.npfb;
     // every load before the first store (the arrays are not known to be distinct, and each
     // load after a store would wait out the one before)
@@ -2361,6 +2378,7 @@ __host__ __device__ inline size_t rev_filter_smem(int hmax) {
 // U4_bar_j = Uf_bar_j (1 - hsum_j) + sum over reverse links w_ij Uf_bar_i, whose rho part
 // is (filter^T rho_bar)_j - tvol_j sum(rho_bar) / sum(vol).
 __global__ void __launch_bounds__(kTile, 2) k_adj_filter_lc(RevArgs B) {
+    const StepConsts &cK = B.K;
     extern __shared__ __align__(16) double smem[];
     const int n = cK.npfb;
     const int j = blockIdx.x * kTile + threadIdx.x;
@@ -2425,6 +2443,7 @@ __global__ void __launch_bounds__(kTile, 2) k_adj_filter_lc(RevArgs B) {
 // otherwise (s = 0) U_bar_0 + S_bar_0 is the adjoint of the step's input.
 template <bool FUSE>
 __global__ void __launch_bounds__(kTile, 2) k_adj_stage_lc(RevArgs B) {
+    const StepConsts &cK = B.K;
     extern __shared__ __align__(16) double smem[];
     const int n = cK.npfb;
     const int j = blockIdx.x * kTile + threadIdx.x;
@@ -2532,6 +2551,7 @@ __global__ void __launch_bounds__(kTile, 2) k_adj_stage_lc(RevArgs B) {
 
 // Adjoint of J = sum 1/2 rho |u|^2 vol at the final state, and its per-tile sums of rho_bar.
 __global__ void __launch_bounds__(kTile) k_adj_objective(Fields F, const double *vol, RevArgs B) {
+    const StepConsts &cK = B.K;
     const int i = blockIdx.x * kTile + threadIdx.x;
     double r = 0.0, dummy = 0.0;
     if (i < cK.npfb) {
@@ -2799,6 +2819,7 @@ static int adjoint_build_stream(Handle *H) {
 
 static RevArgs rev_args(Handle *H) {
     RevArgs B{};
+    B.K = consts_of(H);
     B.sptr = H->rv_sptr; B.sw = H->rv_sw; B.sws = H->rv_sws;
     B.locs = H->rv_loc_s; B.locf = H->rv_loc_f;
     B.hptr = H->rv_hptr; B.halo = H->rv_halo; B.hmax = H->rv_hmax;
@@ -2920,7 +2941,7 @@ int adjoint_run(Handle *H, double dt, int nsteps, int ckpt, double *J, double *d
     // segment in adj_store[4 ckpt + 1].
     auto record_launch = [&](int len) -> int {
         Fields &F0 = H->adj_store[0];
-        k_load_checkpoint<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, H->adj_cp, H->adj_segd, F0);
+        k_load_checkpoint<<<nb, TB, 0, st>>>(n, SUNSET_FORM_LC, H->adj_cp, H->adj_segd, F0, consts_of(H));
         Fields &T = H->adj_store[4 * (size_t)ckpt], &X = H->adj_store[4 * (size_t)ckpt + 1];
         for (int k = 0; k < len; k++) {
             for (int s = 0; s < 4; s++) {
