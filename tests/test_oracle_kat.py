@@ -516,6 +516,40 @@ def test_3d_inout_reduces_to_2d(form, itype, extra):
             assert np.all(s3[k].reshape(o3.nz, nl)[:, t == 1] == 0.0), k
 
 
+def test_3d_output_reduces_to_2d():
+    """3-D output quantities, known answer: for a state that does not vary in z with w = 0, the
+    3-D dump's vorticity magnitude (output.F90:212-216) is |dv/dx - du/dy| of the layer (the z
+    stencils see constants), its state columns repeat the layer's on every layer, and the 3-D
+    kinetic energy and mass with dV = vol dz (statistics.F90:305-330) are nz dz times the
+    layer's."""
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=16)
+    ns = wl.nodes()
+    o = O.for_workload(wl, ns, kolmogorov_forcing=0).setup()
+    o3 = O.Oracle3(o, 0.4)
+    nl, nz, dz = o3.nl, o3.nz, o3.dz
+    x, y = ns.x, ns.y
+    tp = 2.0 * np.pi
+    st = dict(ro=1.0 + 0.01 * np.cos(tp * x), u=np.sin(tp * x) * np.cos(tp * y), v=-np.cos(tp * x) * np.sin(tp * y),
+              cxx=1.2 + 0.1 * np.sin(tp * x), cxy=0.1 * np.cos(tp * y), cyy=1.1 + 0.05 * np.cos(tp * x), czz=np.ones(nl))
+    o.set_state(**st)
+    gu, gv = o.gradient(st["u"]), o.gradient(st["v"])
+    vort2 = np.abs(gv[:, 0] - gu[:, 1])
+    T = lambda a: np.tile(a, nz)
+    zero = np.zeros(o3.n)
+    o3.set_state(T(st["ro"]), T(st["u"]), T(st["v"]), zero, T(st["cxx"]), T(st["cxy"]), T(st["cyy"]), zero, zero,
+                 np.ones(o3.n))
+    cols, hd = o3.dump()
+    scale = np.abs(vort2).max()
+    assert np.abs(cols["vort"].reshape(nz, nl) - vort2[None, :]).max() < 1e-9 * scale
+    for k, ref in (("u", st["u"]), ("v", st["v"])):
+        assert np.array_equal(cols[k].reshape(nz, nl), np.tile(ref, (nz, 1))), k
+    # c passes through psi and back (the 3x3 eigen solution): equal to rounding
+    np.testing.assert_allclose(cols["cxx"].reshape(nz, nl), np.tile(st["cxx"], (nz, 1)), rtol=1e-12)
+    assert np.all(cols["w"] == 0.0) and np.all(cols["qcrit"] == 0.0)
+    np.testing.assert_allclose(o3.kinetic_energy(), nz * dz * o.kinetic_energy(), rtol=1e-12)
+    np.testing.assert_allclose(o3.mass(), nz * dz * o.mass(), rtol=1e-12)
+
+
 def central_first_derivative(m):
     """Weights a_1..a_m of the central difference of 2m + 1 points for d/dz, from Taylor
     matching in exact rationals: sum_j a_j j^(2q-1) = 1/2 for q = 1 and 0 for q = 2..m."""
