@@ -546,6 +546,37 @@ def test_shear_wave_decays_at_the_viscous_rate(order, tol):
     assert abs(amp - exact) < tol * (1.0 - exact), (order, amp, exact)
 
 
+@pytest.mark.parametrize("form", ["di", "chl", "lc"])
+def test_relaxation_at_rest_is_exponential(form):
+    """Known answer in time for the conformation equation: at rest with a uniform c0, the
+    Oldroyd-B relaxation dc/dt = -(c - I)/lambda (rhs_di.F90:454-476, and the same relaxation
+    through the Cholesky and log-conformation variables, rhs.F90:462-547, rhs_lc.F90:519-545)
+    gives c(t) = I + (c0 - I) exp(-t/lambda), lambda = Wi L/U (load_data.F90:131-138).  Each form
+    integrates it with RK3 in its own variables; c after 60 steps agrees with the exponential to
+    1e-9 and the flow stays at rest."""
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=24)
+    ns = wl.nodes()
+    Wi = 0.5
+    o = O.for_workload(wl, ns, form=form, kolmogorov_forcing=0, Wi=Wi, epsPTT=0.0, Mdiff=0.0).setup()
+    n = o.sizes()[1]
+    c0 = dict(cxx=1.5, cxy=0.2, cyy=1.2, czz=1.3)
+    one = np.ones(n)
+    o.set_state(one, np.zeros(n), np.zeros(n), c0["cxx"] * one, c0["cxy"] * one, c0["cyy"] * one, c0["czz"] * one)
+    dtc, dtp = o.set_tstep()
+    dt = 0.3 * min(dtc, dtp)
+    steps = 60
+    o.step(dt, steps)
+    st = o.state()
+    decay = math.exp(-dt * steps / Wi)
+    assert 1.0 - decay > 0.02
+    for k, v in c0.items():
+        if k == "czz" and form != "di":
+            continue  # c_zz is not evolved by the Cholesky and log-conformation forms in 2-D
+        exact = (1.0 if k != "cxy" else 0.0) + (v - (1.0 if k != "cxy" else 0.0)) * decay
+        assert np.abs(st[k] - exact).max() < 1e-9, (form, k, np.abs(st[k] - exact).max())
+    assert np.abs(st["u"]).max() < 1e-12 and np.abs(st["v"]).max() < 1e-12
+
+
 def test_3d_output_reduces_to_2d():
     """3-D output quantities, known answer: for a state that does not vary in z with w = 0, the
     3-D dump's vorticity magnitude (output.F90:212-216) is |dv/dx - du/dy| of the layer (the z
