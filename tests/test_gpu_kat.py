@@ -1,0 +1,103 @@
+"""Known answers in time on the device, independent of the restatement.
+
+* The shear wave u = sin(2 pi y), v = 0, rho = 1 solves the compressible momentum equation
+  exactly (no advection, no pressure gradient, divergence free) and decays as exp(-nu k^2 t),
+  nu = mu_solvent / rho (load_data.F90:131-138), k = 2 pi.  The device's Newtonian step on a
+  jittered periodic set (32 nodes a wavelength) follows it within the error of the stencils,
+  the hyperviscous filter and RK3: after 20 steps the amplitude's error, relative to the decayed
+  amount, is below 2e-2, 5e-4 and 2e-5 at orders 4, 6 and 8.
+* At rest with a uniform conformation c0, the Oldroyd-B relaxation dc/dt = -(c - I)/lambda
+  (rhs_di.F90:454-476; through the Cholesky and log-conformation variables rhs.F90:462-547 and
+  rhs_lc.F90:519-545) gives c(t) = I + (c0 - I) exp(-t/lambda), lambda = Wi L/U.  Each form
+  integrates it in its own variables, in 2-D and on a 3-D layered set (every component,
+  c_xz and c_yz included); after 60 steps c agrees with the exponential to 1e-9 and the flow
+  stays at rest.
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+
+from sunset_viscoelastic_b200 import labfm
+from sunset_viscoelastic_b200.nodesets import WORKLOADS
+
+pytestmark = pytest.mark.gpu
+
+C0 = dict(cxx=1.5, cxy=0.2, cyy=1.2, cxz=0.1, cyz=0.05, czz=1.3)
+IDENT = dict(cxx=1.0, cxy=0.0, cyy=1.0, cxz=0.0, cyz=0.0, czz=1.0)
+
+
+@pytest.mark.parametrize("order, tol", [(4, 2e-2), (6, 5e-4), (8, 2e-5)])
+def test_shear_wave_decays_at_the_viscous_rate(order, tol):
+    name = {4: "periodic-di-o4-16k", 6: "periodic-lc-o6-262k", 8: "periodic-chl-o8-1m"}[order]
+    wl = dataclasses.replace(WORKLOADS[name], nside=32)
+    ns = wl.nodes()
+    g = labfm.for_workload(wl, ns, form="newt", kolmogorov_forcing=0, Re=1.0, beta=0.5).setup()
+    n = g.sizes()[1]
+    assert n == ns.n
+    shape = np.sin(2.0 * np.pi * ns.y)
+    one = np.ones(n)
+    g.set_state(one, shape.copy(), np.zeros(n), one, np.zeros(n), one, one)
+    dt = 0.3 * min(g.set_tstep())
+    steps = 20
+    g.step(dt, steps)
+    u = g.state()["u"]
+    amp = float(u @ shape / (shape @ shape))
+    exact = math.exp(-0.5 * (2.0 * np.pi) ** 2 * dt * steps)  # nu = beta * visc_total / rho = 0.5
+    print(f"order {order}: amplitude {amp:.12f}, exact {exact:.12f}, "
+          f"error / decay {abs(amp - exact) / (1.0 - exact):.2e}")
+    assert 1.0 - exact > 0.01
+    assert abs(amp - exact) < tol * (1.0 - exact), (order, amp, exact)
+    g.close()
+
+
+def check_relaxation(st, dt, steps, Wi, keys):
+    decay = math.exp(-dt * steps / Wi)
+    assert 1.0 - decay > 0.02
+    for k in keys:
+        exact = IDENT[k] + (C0[k] - IDENT[k]) * decay
+        e = float(np.abs(st[k] - exact).max())
+        print(f"{k}: {e:.2e}")
+        assert e < 1e-9, (k, e)
+
+
+@pytest.mark.parametrize("form", ["di", "chl", "lc"])
+def test_relaxation_at_rest_2d(form):
+    wl = dataclasses.replace(WORKLOADS["periodic-lc-o6-262k"], nside=24)
+    ns = wl.nodes()
+    Wi = 0.5
+    g = labfm.for_workload(wl, ns, form=form, kolmogorov_forcing=0, Wi=Wi, epsPTT=0.0, Mdiff=0.0).setup()
+    n = g.sizes()[1]
+    one = np.ones(n)
+    g.set_state(one, np.zeros(n), np.zeros(n), C0["cxx"] * one, C0["cxy"] * one, C0["cyy"] * one, C0["czz"] * one)
+    dt = 0.3 * min(g.set_tstep())
+    g.step(dt, 60)
+    st = g.state()
+    # c_zz is evolved in 2-D by the direct form only
+    check_relaxation(st, dt, 60, Wi, ["cxx", "cxy", "cyy"] + (["czz"] if form == "di" else []))
+    assert np.abs(st["u"]).max() < 1e-12 and np.abs(st["v"]).max() < 1e-12
+    g.close()
+
+
+@pytest.mark.parametrize("form", ["di", "chl", "lc"])
+def test_relaxation_at_rest_3d(form):
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=24)
+    ns = wl.nodes()
+    Wi = 0.5
+    kw = dict(wl.params(), form=form, kolmogorov_forcing=0, Wi=Wi, epsPTT=0.0, Mdiff=0.0)
+    g = labfm.Sunset(**kw)
+    g.build_domain(ns)
+    nz, _ = g.set_layers(0.25)
+    g.setup()
+    m = g.sizes()[1] * nz
+    one = np.ones(m)
+    z = np.zeros(m)
+    g.set_state_3d(one, z, z, z, **{k: C0[k] * one for k in C0})
+    dt = 0.3 * min(g.set_tstep())
+    g.step(dt, 60)
+    st = g.state_3d()
+    check_relaxation(st, dt, 60, Wi, list(C0))
+    for k in ("u", "v", "w"):
+        assert np.abs(st[k]).max() < 1e-12, k
+    g.close()
