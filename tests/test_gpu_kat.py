@@ -5,7 +5,9 @@
   nu = mu_solvent / rho (load_data.F90:131-138), k = 2 pi.  The device's Newtonian step on a
   jittered periodic set (32 nodes a wavelength) follows it within the error of the stencils,
   the hyperviscous filter and RK3: after 20 steps the amplitude's error, relative to the decayed
-  amount, is below 2e-2, 5e-4 and 2e-5 at orders 4, 6 and 8.
+  amount, is below 2e-2, 5e-4 and 2e-5 at orders 4, 6 and 8.  The same wave across the layers,
+  u = sin(2 pi z / Lz), decays through the z finite-difference stencils (fd.F90:27-256) and the
+  z filter alone: below 5e-2, 1e-3 and 2e-5.
 * At rest with a uniform conformation c0, the Oldroyd-B relaxation dc/dt = -(c - I)/lambda
   (rhs_di.F90:454-476; through the Cholesky and log-conformation variables rhs.F90:462-547 and
   rhs_lc.F90:519-545) gives c(t) = I + (c0 - I) exp(-t/lambda), lambda = Wi L/U.  Each form
@@ -49,6 +51,35 @@ def test_shear_wave_decays_at_the_viscous_rate(order, tol):
           f"error / decay {abs(amp - exact) / (1.0 - exact):.2e}")
     assert 1.0 - exact > 0.01
     assert abs(amp - exact) < tol * (1.0 - exact), (order, amp, exact)
+    g.close()
+
+
+@pytest.mark.parametrize("order, tol", [(4, 5e-2), (6, 1e-3), (8, 2e-5)])
+def test_shear_wave_in_z_decays_at_the_viscous_rate(order, tol):
+    """u = sin(2 pi z / Lz) on a layered set (Lz = 1, dz = 0.04) decays as exp(-nu k^2 t),
+    k = 2 pi / Lz, through the z stencils and the z filter alone; after 20 steps the amplitude's
+    error relative to the decay is below 5e-2, 1e-3 and 2e-5 at orders 4, 6 and 8."""
+    name = {4: "periodic-di-o4-16k", 6: "periodic-lc-o6-262k", 8: "periodic-chl-o8-1m"}[order]
+    wl = dataclasses.replace(WORKLOADS[name], nside=24)
+    g = labfm.Sunset(**dict(wl.params(), form="newt", kolmogorov_forcing=0, Re=1.0, beta=0.5))
+    g.build_domain(wl.nodes())
+    nz, dz = g.set_layers(1.0)
+    g.setup()
+    nl = g.sizes()[1]
+    Lz = nz * dz
+    shape = np.sin(2.0 * np.pi * np.repeat(np.arange(nz) * dz, nl) / Lz)
+    z = np.zeros(nl * nz)
+    g.set_state_3d(np.ones(nl * nz), shape.copy(), z, z)
+    dt = 0.3 * min(g.set_tstep())
+    g.step(dt, 20)
+    st = g.state_3d()
+    amp = float(st["u"] @ shape / (shape @ shape))
+    exact = math.exp(-0.5 * (2.0 * np.pi / Lz) ** 2 * dt * 20)
+    print(f"z order {order}: nz {nz}, amplitude {amp:.12f}, exact {exact:.12f}, "
+          f"error / decay {abs(amp - exact) / (1.0 - exact):.2e}")
+    assert 1.0 - exact > 0.01
+    assert abs(amp - exact) < tol * (1.0 - exact), (order, amp, exact)
+    assert np.abs(st["v"]).max() < 1e-13 and np.abs(st["w"]).max() < 1e-13
     g.close()
 
 
