@@ -608,6 +608,38 @@ def test_relaxation_at_rest_is_exponential(form):
     assert np.abs(st["u"]).max() < 1e-12 and np.abs(st["v"]).max() < 1e-12
 
 
+@pytest.mark.parametrize("form", ["di", "chl", "lc"])
+def test_relaxation_at_rest_3d_is_exponential(form):
+    """The relaxation at rest on a 3-D layered set, every component of c (c_xz, c_yz and c_zz
+    included) evolved by each form in its own 3-D variables (rhs_di.F90:450-476 with the dim3
+    terms; rhs.F90:500-547; rhs_lc.F90:519-545): c = I + (c0 - I) exp(-t/lambda) to 1e-9 after
+    60 steps, the flow at rest."""
+    wl = dataclasses.replace(WORKLOADS["periodic-di-o4-16k"], nside=24)
+    Wi = 0.5
+    kw = dict(wl.params(), form=form, kolmogorov_forcing=0, Wi=Wi, epsPTT=0.0, Mdiff=0.0)
+    O.set_pow_mode(True)
+    try:
+        layer = O.Oracle(**kw).build_domain(wl.nodes()).setup()
+    finally:
+        O.set_pow_mode(False)
+    r = O.Oracle3(layer, 0.25)
+    m = r.nl * r.nz
+    c0 = dict(cxx=1.5, cxy=0.2, cyy=1.2, cxz=0.1, cyz=0.05, czz=1.3)
+    ident = dict(cxx=1.0, cxy=0.0, cyy=1.0, cxz=0.0, cyz=0.0, czz=1.0)
+    one, z = np.ones(m), np.zeros(m)
+    r.set_state(one, z, z, z, **{k: c0[k] * one for k in c0})
+    dt = 0.3 * min(r.set_tstep())
+    r.step(dt, 60)
+    st = r.state()
+    decay = math.exp(-dt * 60 / Wi)
+    assert 1.0 - decay > 0.02
+    for k in c0:
+        e = float(np.abs(st[k] - (ident[k] + (c0[k] - ident[k]) * decay)).max())
+        assert e < 1e-9, (form, k, e)
+    for k in ("rou", "rov", "row"):
+        assert np.abs(st[k]).max() < 1e-12, k
+
+
 def test_3d_output_reduces_to_2d():
     """3-D output quantities, known answer: for a state that does not vary in z with w = 0, the
     3-D dump's vorticity magnitude (output.F90:212-216) is |dv/dx - du/dy| of the layer (the z
